@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark of the PathTracer hot path on one B200 (or N replicas).
+
+Workload (default): the 1920x1080 "heightfield_soup_1080p" scene -- a
+1024x1024 fBm heightfield (2,093,058 triangles) plus 200,000 random triangles
+and 64 emissive triangles, 256 random StandardMaterials, a 1024x512
+procedural sky env map -- rendered by VBufferRT + PathTracer at 64 samples per
+pixel (4 frames of 16 spp, the reference's per-frame maximum), 8 bounces,
+NEE + MIS (balance heuristic), Power emissive sampler, LogLuv per-sample
+colour.  One step = one 64-spp frame = 132.7 M paths.
+
+Prints one JSON line (rank 0).  `--impl reference` times the CPU restatement
+of the same path (the reference's GPU path needs DXR/Vulkan, unavailable on
+this box) on a bounded crop of the same workload using all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FRAMES_PER_STEP = 4
+SPP_PER_FRAME = 16
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="heightfield_soup_1080p")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the cpu_baseline sample")
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sms, maxs, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                maxs.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": max(maxs) if maxs else None,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def algorithmic_bytes(c: dict, pixels: int) -> int:
+    """Algorithmic bytes of one PathTracer launch from its event counts:
+    80 B per compressed 8-wide node visit, 48 B per triangle record tested,
+    268 B of shading data per hit (indices, 3 packed vertices, instance,
+    material blob), 76 B per emissive light sample, 144 B per env-map
+    importance sample, 48 B per bilinear env-map evaluation, 4 B per env pdf,
+    plus 16 B V-buffer read and 16 B colour write per pixel."""
+    return (80 * c["node_visits"] + 48 * c["tri_tests"] + 268 * c["hits"] + 76 * c["light_samples"]
+            + 144 * c["env_samples"] + 48 * c["env_evals"] + 4 * c["env_pdfs"] + 32 * pixels)
+
+
+def load_traffic(workload: str):
+    """Per-launch DRAM bytes of the path-tracer kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / f"path_tracer_kernel_{workload}.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("dram_bytes_per_launch")
+        except (ValueError, OSError):
+            return None
+    return None
+
+
+def cpu_baseline(workload_name: str, seconds: float):
+    """Times the CPU oracle (FP32 PathTracer restatement) on a crop of the workload
+    on all host cores.  Returns (Mpaths/s, cores, sample description)."""
+    import numpy as np
+    from falcor_b200.scene import WORKLOADS, make_host_scene
+    from oracle import ffi as orc
+    from tests import helpers as H
+    w = WORKLOADS[workload_name]
+    host = make_host_scene(w)
+    osc = H.oracle_scene(host)
+    cores = os.cpu_count() or 1
+    vb = osc.vbuffer(w.width, w.height, threads=cores)
+    # Calibrate on a small crop, then size the sample to ~`seconds` of work.
+    cx, cy = w.width // 2 - 16, w.height // 2 - 16
+    params = H.pt_params(w.width, w.height, SPP_PER_FRAME, seed=0, max_bounces=w.max_bounces, sampler=2, color_format=1)
+    _, _, cnt, dt = osc.path_tracer(vb, params, threads=cores, rect=(cx, cy, cx + 32, cy + 32))
+    rate = max(cnt.paths, 1) / max(dt, 1e-6)
+    side = int(min(max(32, (rate * seconds / SPP_PER_FRAME) ** 0.5), 512))
+    side -= side % 16
+    x0, y0 = max(0, w.width // 2 - side // 2), max(0, w.height // 2 - side // 2)
+    _, _, cnt, dt = osc.path_tracer(vb, params, threads=cores, rect=(x0, y0, x0 + side, y0 + side))
+    # Background pixels also count as paths in the workload's unit (they are written per sample).
+    bg = int(np.sum(vb[y0:y0 + side, x0:x0 + side, 0] == 0)) * SPP_PER_FRAME
+    paths = cnt.paths + bg
+    desc = (f"{side}x{side} crop at the frame centre, {SPP_PER_FRAME} spp, {w.max_bounces} bounces, FP32 CPU oracle "
+            f"(-O3 -ffp-contract=off), {paths} paths in {dt:.2f} s")
+    return paths / dt / 1e6, cores, desc
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    value, cores, desc = cpu_baseline(args.workload, args.cpu_seconds / max(args.steps, 1))
+    vals = [value]
+    for _ in range(max(args.steps - 1, 0)):
+        v, _, _ = cpu_baseline(args.workload, args.cpu_seconds / max(args.steps, 1))
+        vals.append(v)
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": "Mpaths/s (PathTracer forward, NEE+MIS)", "value": round(v, 4), "unit": "Mpaths/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic procedural scene",
+            "config": {"workload": args.workload},
+            "cpu_baseline": {"value": round(v, 4), "unit": "Mpaths/s", "cores": cores, "kind": "port", "sample": desc},
+            "e2e": {"value": round(v, 4), "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference GPU path (Slang on DXR/Vulkan RT) unavailable on this box; CPU restatement timed instead"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+
+    from falcor_b200 import build
+    build.build()
+    from falcor_b200.scene import WORKLOADS, Scene, make_host_scene
+    from falcor_b200.passes import PathTracer, VBufferRT
+
+    w = WORKLOADS[args.workload]
+    host = make_host_scene(w)
+    scene = Scene(host)
+    W, Hh = w.width, w.height
+    vb = VBufferRT()
+    vb.set_scene(scene)
+    pt = PathTracer({"samplesPerPixel": SPP_PER_FRAME, "maxSurfaceBounces": w.max_bounces,
+                     "maxDiffuseBounces": w.max_bounces, "maxSpecularBounces": w.max_bounces,
+                     "emissiveSampler": "Power", "colorFormat": "LogLuvHDR", "misHeuristic": "Balance"})
+    pt.set_scene(scene)
+    vbuf = torch.zeros((Hh, W, 4), dtype=torch.int32, device=dev)
+    frame = torch.zeros((Hh, W, 4), dtype=torch.float32, device=dev)
+    accum = torch.zeros((Hh, W, 4), dtype=torch.float32, device=dev)
+    # L2 flush buffer (larger than the 126 MB L2), written between steps.
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    kernel_ms = []
+
+    def step(timed_kernels: bool):
+        vb.execute({"vbuffer": vbuf})
+        accum.zero_()
+        for f in range(FRAMES_PER_STEP):
+            pt.set_properties({"fixedSeed": f})
+            if timed_kernels:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            pt.execute({"vbuffer": vbuf, "color": frame})
+            if timed_kernels:
+                e1.record(stream)
+                kernel_ms.append((e0, e1))
+            accum.add_(frame)
+        accum.mul_(1.0 / FRAMES_PER_STEP)
+
+    for _ in range(args.warmup):
+        step(False)
+        flush.fill_(1.0)
+    torch.cuda.synchronize()
+    counters = pt.counters()  # counts of the last PathTracer launch
+    paths_per_step = W * Hh * SPP_PER_FRAME * FRAMES_PER_STEP
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        step(True)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += s0.elapsed_time(s1)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = paths_per_step * world / (ms_per_step / 1e3) / 1e6
+
+    kms = [a.elapsed_time(b) for a, b in kernel_ms]
+    k_avg_ms = sum(kms) / len(kms)
+    alg = algorithmic_bytes(counters, W * Hh)
+    hbm, peak_kind = peaks()
+    achieved = alg / (k_avg_ms / 1e3) / 1e9
+    rays_per_step = counters["rays"] * FRAMES_PER_STEP
+
+    # End to end through the public API: per step the camera is re-sent from host
+    # memory, the frame is rendered, and the resolved image is read back into pinned host memory.
+    host_img = torch.empty((Hh, W, 4), dtype=torch.float32, pin_memory=True)
+    cam = torch.tensor(list(host.camera_data().posW) + list(host.camera_data().cameraU) + list(host.camera_data().cameraV)
+                       + list(host.camera_data().cameraW) + [0.0, 0.0, 0.0, 0.0], dtype=torch.float32).pin_memory()
+    cam_dev = torch.empty_like(cam, device=dev)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e2e_steps = max(2, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        cam_dev.copy_(cam, non_blocking=True)
+        step(False)
+        host_img.copy_(accum, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = paths_per_step * world / e2e_s / 1e6
+
+    st = pt.stats()
+    line = {
+        "metric": "Mpaths/s (PathTracer forward, NEE+MIS)", "value": round(value, 3), "unit": "Mpaths/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic procedural scene (seeded), no dataset",
+        "config": {"workload": w.name, "resolution": [W, Hh], "spp": SPP_PER_FRAME * FRAMES_PER_STEP,
+                   "frames_per_step": FRAMES_PER_STEP, "max_bounces": w.max_bounces,
+                   "triangles": scene.info.triangle_count, "emissive_triangles": scene.info.emissive_triangle_count,
+                   "bvh_nodes": scene.info.bvh_node_count, "bvh_build_s": round(scene.info.bvh_build_seconds, 3),
+                   "parallelism": f"replicas x{world}", "l2_flush": "256 MB buffer written before every timed step"},
+        "mrays_per_s": round(rays_per_step * world / (ms_per_step / 1e3) / 1e6, 3),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "traffic": load_traffic(w.name), "peak_kind": peak_kind,
+                     "kernel": "path_tracer_kernel", "kernel_ms": round(k_avg_ms, 3),
+                     "algorithmic_bytes_per_launch": alg},
+        "e2e": {"value": round(e2e_value, 3), "unit": "Mpaths/s", "h2d_bytes_per_step": cam.numel() * 4,
+                "d2h_bytes_per_step": host_img.numel() * 4},
+        "gpu_launches": args.steps * (1 + FRAMES_PER_STEP),
+        "clocks": clk,
+        "counters_last_launch": counters,
+        "device_error": st.device_error,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, desc = cpu_baseline(w.name, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpaths/s", "cores": cores, "kind": "port", "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

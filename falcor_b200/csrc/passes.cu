@@ -1,0 +1,416 @@
+// passes.cu -- render-pass objects of the C-ABI: properties with the
+// reference names and defaults, channel reflection, and execute().
+//
+//   MinimalPathTracer  RenderPasses/MinimalPathTracer/MinimalPathTracer.cpp:60-200
+//   PathTracer         RenderPasses/PathTracer/PathTracer.cpp:155-415,1329-1598
+//   VBufferRT          RenderPasses/GBuffer/VBuffer/VBufferRT.cpp
+//   WARDiffPathTracer  RenderPasses/WARDiffPathTracer/WARDiffPathTracer.cpp:53-144 (adjoint.cu)
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <sstream>
+#include <string>
+
+#include "kernels.cuh"
+#include "passes.h"
+#include "scene_device.h"
+
+namespace fpt {
+
+namespace {
+
+struct ChannelSpec { const char* name; const char* desc; bool input; bool optional; const char* format; };
+
+const ChannelSpec kMinimalChannels[] = {
+    {"vbuffer", "Visibility buffer in packed format", true, false, "PackedHitInfo"},
+    {"viewW", "World-space view direction (xyz float format)", true, true, "RGBA32Float"},
+    {"color", "Output color (sum of direct and indirect)", false, false, "RGBA32Float"},
+};
+const ChannelSpec kPathTracerChannels[] = {
+    {"vbuffer", "Visibility buffer in packed format", true, false, "PackedHitInfo"},
+    {"mvec", "Motion vector buffer (float format)", true, true, "RG32Float"},
+    {"viewW", "World-space view direction (xyz float format)", true, true, "RGBA32Float"},
+    {"sampleCount", "Sample count buffer (integer format)", true, true, "R8Uint"},
+    {"color", "Output color (linear)", false, true, "RGBA32Float"},
+    {"albedo", "Output albedo (linear)", false, true, "RGBA8Unorm"},
+    {"specularAlbedo", "Output specular albedo (linear)", false, true, "RGBA8Unorm"},
+    {"indirectAlbedo", "Output indirect albedo (linear)", false, true, "RGBA8Unorm"},
+    {"guideNormal", "Output guide normal (linear)", false, true, "RGBA16Float"},
+    {"reflectionPosW", "Output reflection pos (world space)", false, true, "RGBA32Float"},
+    {"rayCount", "Per-pixel ray count", false, true, "R32Uint"},
+    {"pathLength", "Per-pixel path length", false, true, "R32Uint"},
+};
+const ChannelSpec kVBufferChannels[] = {
+    {"vbuffer", "Visibility buffer in packed format", false, false, "PackedHitInfo"},
+};
+const ChannelSpec kWARDiffChannels[] = {
+    {"color", "Output color (linear)", false, false, "RGBA32Float"},
+    {"dColor", "Output gradient of color w.r.t. the debug variable", false, true, "RGBA32Float"},
+};
+
+void set_defaults(fpt_pass& p) {
+    auto& d = p.props;
+    if (p.type == "MinimalPathTracer") {
+        d["maxBounces"] = PropValue::num(3);
+        d["computeDirect"] = PropValue::num(1);
+        d["useImportanceSampling"] = PropValue::num(1);
+        d["diffuseBrdf"] = PropValue::str("Frostbite");
+    } else if (p.type == "PathTracer") {
+        d["samplesPerPixel"] = PropValue::num(1);
+        d["maxSurfaceBounces"] = PropValue::num(0);
+        d["maxDiffuseBounces"] = PropValue::num(3);
+        d["maxSpecularBounces"] = PropValue::num(3);
+        d["maxTransmissionBounces"] = PropValue::num(10);
+        d["sampleGenerator"] = PropValue::num(0);
+        d["fixedSeed"] = PropValue::num(1);
+        d["useBSDFSampling"] = PropValue::num(1);
+        d["useRussianRoulette"] = PropValue::num(0);
+        d["useNEE"] = PropValue::num(1);
+        d["useMIS"] = PropValue::num(1);
+        d["misHeuristic"] = PropValue::str("Balance");
+        d["misPowerExponent"] = PropValue::num(2);
+        d["emissiveSampler"] = PropValue::str("LightBVH");
+        d["useRTXDI"] = PropValue::num(0);
+        d["useAlphaTest"] = PropValue::num(1);
+        d["adjustShadingNormals"] = PropValue::num(0);
+        d["maxNestedMaterials"] = PropValue::num(2);
+        d["useLightsInDielectricVolumes"] = PropValue::num(0);
+        d["disableCaustics"] = PropValue::num(0);
+        d["specularRoughnessThreshold"] = PropValue::num(0.25);
+        d["primaryLodMode"] = PropValue::str("Mip0");
+        d["lodBias"] = PropValue::num(0);
+        d["useNRDDemodulation"] = PropValue::num(1);
+        d["useSER"] = PropValue::num(1);
+        d["outputSize"] = PropValue::str("Default");
+        d["colorFormat"] = PropValue::str("LogLuvHDR");
+        d["diffuseBrdf"] = PropValue::str("Frostbite");
+    } else if (p.type == "VBufferRT") {
+        d["samplePattern"] = PropValue::str("Center");
+        d["useAlphaTest"] = PropValue::num(1);
+    } else if (p.type == "WARDiffPathTracer") {
+        d["samplesPerPixel"] = PropValue::num(1);
+        d["maxBounces"] = PropValue::num(0);
+        d["diffMode"] = PropValue::str("Primal");
+        d["diffVarName"] = PropValue::str("");
+        d["sampleGenerator"] = PropValue::num(1);
+        d["fixedSeed"] = PropValue::num(1);
+        d["useBSDFSampling"] = PropValue::num(1);
+        d["useNEE"] = PropValue::num(1);
+        d["useMIS"] = PropValue::num(1);
+        d["useWAR"] = PropValue::num(1);
+        d["auxSampleCount"] = PropValue::num(16);
+        d["Log10vMFConcentration"] = PropValue::num(5);
+        d["Log10vMFConcentrationScreen"] = PropValue::num(5);
+        d["boundaryTermBeta"] = PropValue::num(0.01);
+        d["useAntitheticSampling"] = PropValue::num(1);
+        d["diffuseBrdf"] = PropValue::str("Frostbite");
+        d["replayMode"] = PropValue::str("Replay");
+    }
+}
+
+const std::map<std::string, int> kMISHeuristics = {{"Balance", 0}, {"PowerTwo", 1}, {"PowerExp", 2}};
+const std::map<std::string, int> kEmissiveSamplers = {{"Uniform", 0}, {"LightBVH", 1}, {"Power", 2}};
+const std::map<std::string, int> kColorFormats = {{"RGBA32F", 0}, {"LogLuvHDR", 1}};
+const std::map<std::string, int> kDiffModes = {{"Primal", 0}, {"BackwardDiff", 1}, {"ForwardDiffDebug", 2}, {"BackwardDiffDebug", 3}};
+
+std::string json_escape(const std::string& s) {
+    std::string o;
+    for (char c : s) {
+        if (c == '"' || c == '\\') o += '\\';
+        o += c;
+    }
+    return o;
+}
+
+fpt_status write_json(const std::string& s, char* buf, size_t cap) {
+    if (!buf || cap < s.size() + 1) return set_error(FPT_ERR_INVALID_ARG, "buffer too small for JSON (" + std::to_string(s.size() + 1) + " bytes)");
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return FPT_OK;
+}
+
+}  // namespace
+}  // namespace fpt
+
+double fpt_pass::num(const std::string& k) const {
+    auto it = props.find(k);
+    return it == props.end() ? 0.0 : it->second.n;
+}
+std::string fpt_pass::str(const std::string& k) const {
+    auto it = props.find(k);
+    return it == props.end() ? std::string() : it->second.s;
+}
+
+namespace fpt {
+
+fpt_status ensure_scratch(fpt_pass& p) {
+    if (p.scratch) return FPT_OK;
+    if (cudaMalloc(&p.scratch, kScratchBytes) != cudaSuccess) return set_error(FPT_ERR_OOM, "cudaMalloc pass scratch");
+    cudaMemset(p.scratch, 0, kScratchBytes);
+    return FPT_OK;
+}
+
+fpt_status check_device_error(fpt_pass& p, cudaStream_t st) {
+    (void)st;
+    return FPT_OK;
+}
+
+// Fills the PathTracer parameters after PathTracer::validateOptions (PathTracer.cpp:370-415).
+void path_tracer_params(fpt_pass& p, FrameParams& fp) {
+    fp.spp = uint32_t(std::clamp(p.num("samplesPerPixel"), 1.0, 16.0));
+    auto clampB = [](double v) { return uint32_t(std::clamp(v, 0.0, 254.0)); };
+    fp.maxDiffuseBounces = clampB(p.num("maxDiffuseBounces"));
+    fp.maxSpecularBounces = clampB(p.num("maxSpecularBounces"));
+    fp.maxTransmissionBounces = clampB(p.num("maxTransmissionBounces"));
+    fp.maxSurfaceBounces = std::max(clampB(p.num("maxSurfaceBounces")),
+                                    std::max(fp.maxDiffuseBounces, std::max(fp.maxSpecularBounces, fp.maxTransmissionBounces)));
+    fp.sampleGenerator = uint32_t(p.num("sampleGenerator")) == 1 ? 1u : 0u;
+    fp.useBSDFSampling = p.num("useBSDFSampling") != 0;
+    fp.useNEE = p.num("useNEE") != 0;
+    fp.useMIS = p.num("useMIS") != 0;
+    auto mh = kMISHeuristics.find(p.str("misHeuristic"));
+    fp.misHeuristic = mh == kMISHeuristics.end() ? 0u : uint32_t(mh->second);
+    fp.misPowerExponent = float(p.num("misPowerExponent"));
+    auto es = kEmissiveSamplers.find(p.str("emissiveSampler"));
+    int sampler = es == kEmissiveSamplers.end() ? 1 : es->second;
+    if (sampler == 1) {
+        if (!p.warnedLightBVH) {
+            log_warning("PathTracer: emissiveSampler 'LightBVH' is not implemented; using 'Power'");
+            p.warnedLightBVH = true;
+        }
+        sampler = 2;
+    }
+    fp.emissiveSampler = uint32_t(sampler);
+    fp.specularRoughnessThreshold = float(std::clamp(p.num("specularRoughnessThreshold"), 0.0, 1.0));
+    auto cf = kColorFormats.find(p.str("colorFormat"));
+    fp.colorFormat = cf == kColorFormats.end() ? 1u : uint32_t(cf->second);
+    fp.seed = p.useFixedSeed ? uint32_t(p.num("fixedSeed")) : p.frameCount;
+    fp.lambert = p.str("diffuseBrdf") == "Lambert";
+}
+
+}  // namespace fpt
+
+using namespace fpt;
+
+extern "C" {
+
+FPT_API fpt_status fpt_pass_create(const char* type_name, fpt_pass** out) {
+    if (!type_name || !out) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_create: null argument");
+    std::string t(type_name);
+    if (t != "MinimalPathTracer" && t != "PathTracer" && t != "VBufferRT" && t != "WARDiffPathTracer")
+        return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_create: unknown render pass type '" + t + "'");
+    auto* p = new fpt_pass();
+    p->type = t;
+    set_defaults(*p);
+    *out = p;
+    return FPT_OK;
+}
+
+FPT_API void fpt_pass_destroy(fpt_pass* pass) {
+    if (!pass) return;
+    if (pass->scratch) cudaFree(pass->scratch);
+    if (pass->adjointScratch) cudaFree(pass->adjointScratch);
+    delete pass;
+}
+
+FPT_API fpt_status fpt_pass_set_property_int(fpt_pass* pass, const char* key, int64_t value) {
+    return fpt_pass_set_property_float(pass, key, double(value));
+}
+
+FPT_API fpt_status fpt_pass_set_property_float(fpt_pass* pass, const char* key, double value) {
+    if (!pass || !key) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_property: null argument");
+    auto it = pass->props.find(key);
+    if (it == pass->props.end()) {
+        log_warning("Unknown property '" + std::string(key) + "' in " + pass->type + " properties.");
+        return FPT_OK;
+    }
+    if (it->second.isString) {
+        // Enum-valued properties also accept their integer value.
+        const std::map<std::string, int>* m = nullptr;
+        std::string k(key);
+        if (k == "misHeuristic") m = &kMISHeuristics;
+        else if (k == "emissiveSampler") m = &kEmissiveSamplers;
+        else if (k == "colorFormat") m = &kColorFormats;
+        else if (k == "diffMode") m = &kDiffModes;
+        if (!m) return set_error(FPT_ERR_INVALID_ARG, "property '" + k + "' expects a string");
+        for (auto& kv : *m)
+            if (kv.second == int(value)) { it->second.s = kv.first; return FPT_OK; }
+        return set_error(FPT_ERR_INVALID_ARG, "invalid value for property '" + k + "'");
+    }
+    if (std::string(key) == "fixedSeed") pass->useFixedSeed = true;
+    it->second.n = value;
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_pass_set_property_string(fpt_pass* pass, const char* key, const char* value) {
+    if (!pass || !key || !value) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_property_string: null argument");
+    auto it = pass->props.find(key);
+    if (it == pass->props.end()) {
+        log_warning("Unknown property '" + std::string(key) + "' in " + pass->type + " properties.");
+        return FPT_OK;
+    }
+    if (!it->second.isString) return set_error(FPT_ERR_INVALID_ARG, "property '" + std::string(key) + "' expects a number");
+    std::string k(key), v(value);
+    const std::map<std::string, int>* m = nullptr;
+    if (k == "misHeuristic") m = &kMISHeuristics;
+    else if (k == "emissiveSampler") m = &kEmissiveSamplers;
+    else if (k == "colorFormat") m = &kColorFormats;
+    else if (k == "diffMode") m = &kDiffModes;
+    if (m && m->find(v) == m->end()) return set_error(FPT_ERR_INVALID_ARG, "invalid value '" + v + "' for property '" + k + "'");
+    if (k == "diffuseBrdf" && v != "Frostbite" && v != "Lambert")
+        return set_error(FPT_ERR_INVALID_ARG, "diffuseBrdf must be 'Frostbite' or 'Lambert'");
+    it->second.s = v;
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_pass_get_properties_json(const fpt_pass* pass, char* buf, size_t cap) {
+    if (!pass) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_get_properties_json: null pass");
+    std::ostringstream os;
+    os << "{";
+    bool first = true;
+    for (auto& kv : pass->props) {
+        if (!first) os << ", ";
+        first = false;
+        os << "\"" << json_escape(kv.first) << "\": ";
+        if (kv.second.isString) os << "\"" << json_escape(kv.second.s) << "\"";
+        else {
+            char tmp[64];
+            std::snprintf(tmp, sizeof(tmp), "%.17g", kv.second.n);
+            os << tmp;
+        }
+    }
+    os << "}";
+    return write_json(os.str(), buf, cap);
+}
+
+FPT_API fpt_status fpt_pass_reflect_json(const fpt_pass* pass, char* buf, size_t cap) {
+    if (!pass) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_reflect_json: null pass");
+    const ChannelSpec* ch = nullptr;
+    size_t n = 0;
+    if (pass->type == "MinimalPathTracer") { ch = kMinimalChannels; n = sizeof(kMinimalChannels) / sizeof(ChannelSpec); }
+    else if (pass->type == "PathTracer") { ch = kPathTracerChannels; n = sizeof(kPathTracerChannels) / sizeof(ChannelSpec); }
+    else if (pass->type == "VBufferRT") { ch = kVBufferChannels; n = sizeof(kVBufferChannels) / sizeof(ChannelSpec); }
+    else { ch = kWARDiffChannels; n = sizeof(kWARDiffChannels) / sizeof(ChannelSpec); }
+    std::ostringstream os;
+    os << "{\"inputs\": [";
+    bool first = true;
+    for (size_t i = 0; i < n; i++) {
+        if (!ch[i].input) continue;
+        os << (first ? "" : ", ") << "{\"name\": \"" << ch[i].name << "\", \"desc\": \"" << ch[i].desc << "\", \"optional\": "
+           << (ch[i].optional ? "true" : "false") << ", \"format\": \"" << ch[i].format << "\"}";
+        first = false;
+    }
+    os << "], \"outputs\": [";
+    first = true;
+    for (size_t i = 0; i < n; i++) {
+        if (ch[i].input) continue;
+        os << (first ? "" : ", ") << "{\"name\": \"" << ch[i].name << "\", \"desc\": \"" << ch[i].desc << "\", \"optional\": "
+           << (ch[i].optional ? "true" : "false") << ", \"format\": \"" << ch[i].format << "\"}";
+        first = false;
+    }
+    os << "]}";
+    return write_json(os.str(), buf, cap);
+}
+
+FPT_API fpt_status fpt_pass_set_scene(fpt_pass* pass, fpt_scene* scene) {
+    if (!pass) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_scene: null pass");
+    pass->scene = scene;
+    pass->frameCount = 0;
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void* stream) {
+    if (!pass || !io) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_execute: null argument");
+    if (!pass->scene) return set_error(FPT_ERR_NO_SCENE, pass->type + ": no scene set");
+    if (io->width == 0 || io->height == 0 || io->width > 16384 || io->height > 16384)
+        return set_error(FPT_ERR_INVALID_ARG, pass->type + ": invalid frame size");
+    if (pass->type == "PathTracer" && (io->width > 4096 || io->height > 4096))
+        return set_error(FPT_ERR_INVALID_ARG, "PathTracer: frame dimension exceeds kMaxFrameDimension (4096)");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    fpt_status s = ensure_scratch(*pass);
+    if (s != FPT_OK) return s;
+    const DevScene& ds = pass->scene->dev;
+    FrameParams fp;
+    std::memset(&fp, 0, sizeof(fp));
+    fp.width = io->width;
+    fp.height = io->height;
+    fp.frameIndex = io->frame_index;
+    fp.prngDimension = io->prng_dimension;
+    fp.vbuffer = reinterpret_cast<const uint4*>(io->vbuffer);
+    fp.color = reinterpret_cast<float4*>(io->color);
+    fp.rayCount = io->ray_count;
+    fp.pathLength = io->path_length;
+    fp.sampleColor = io->sample_color;
+    fp.vbufferOut = reinterpret_cast<uint4*>(io->vbuffer_out);
+    fp.counters = reinterpret_cast<unsigned long long*>(pass->scratch);
+    fp.workCounter = reinterpret_cast<uint32_t*>(static_cast<char*>(pass->scratch) + kWorkCounterOffset);
+    fp.workItems = io->width * io->height;
+    cudaError_t e = cudaMemsetAsync(pass->scratch, 0, kNumCounters * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, cudaGetErrorString(e));
+    pass->launches = 1;
+    if (pass->type == "VBufferRT") {
+        if (!io->vbuffer_out) return set_error(FPT_ERR_INVALID_ARG, "VBufferRT: output 'vbuffer' not connected");
+        e = launch_vbuffer(ds, fp, st);
+    } else if (pass->type == "MinimalPathTracer") {
+        if (!io->vbuffer || !io->color) return set_error(FPT_ERR_INVALID_ARG, "MinimalPathTracer: 'vbuffer' and 'color' are required");
+        fp.maxBounces = uint32_t(std::max(0.0, pass->num("maxBounces")));
+        fp.computeDirect = pass->num("computeDirect") != 0;
+        fp.useImportanceSampling = pass->num("useImportanceSampling") != 0;
+        fp.lambert = pass->str("diffuseBrdf") == "Lambert";
+        fp.frameIndex = io->frame_index;
+        e = launch_minimal_pt(ds, fp, st);
+    } else if (pass->type == "PathTracer") {
+        if (!io->vbuffer || !io->color) return set_error(FPT_ERR_INVALID_ARG, "PathTracer: 'vbuffer' and 'color' are required");
+        path_tracer_params(*pass, fp);
+        pass->launches = 2;
+        e = launch_path_tracer(ds, fp, st);
+        pass->frameCount++;
+    } else {
+        return wardiff_execute(*pass, io, nullptr, nullptr, st);
+    }
+    if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, pass->type + ": kernel launch failed: " + cudaGetErrorString(e));
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_pass_backward(fpt_pass* pass, const fpt_frame_io* io, const float* dLdI, const fpt_grad_buffers* grads,
+                                     void* stream) {
+    if (!pass || !io || !dLdI || !grads) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_backward: null argument");
+    if (pass->type != "WARDiffPathTracer") return set_error(FPT_ERR_UNSUPPORTED, "fpt_pass_backward: only WARDiffPathTracer is differentiable");
+    if (!pass->scene) return set_error(FPT_ERR_NO_SCENE, "WARDiffPathTracer: no scene set");
+    fpt_status s = ensure_scratch(*pass);
+    if (s != FPT_OK) return s;
+    return wardiff_execute(*pass, io, dLdI, grads, static_cast<cudaStream_t>(stream));
+}
+
+FPT_API fpt_status fpt_pass_get_stats(fpt_pass* pass, fpt_pass_stats* out, void* stream) {
+    if (!pass || !out) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_get_stats: null argument");
+    std::memset(out, 0, sizeof(*out));
+    if (!pass->scratch || !pass->scene) return FPT_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned long long c[2] = {0, 0};
+    uint32_t err = 0;
+    cudaError_t e = cudaMemcpyAsync(c, pass->scratch, 16, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&err, pass->scene->dev.errorWord, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, cudaGetErrorString(e));
+    out->paths = c[0];
+    out->rays = c[1];
+    out->device_error = err;
+    out->kernel_launches = pass->launches;
+    return err ? set_error(FPT_ERR_DEVICE, "device error word 0x" + std::to_string(err)) : FPT_OK;
+}
+
+FPT_API fpt_status fpt_pass_get_counters(fpt_pass* pass, uint64_t* out, uint32_t count, void* stream) {
+    if (!pass || !out) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_get_counters: null argument");
+    const uint32_t n = std::min<uint32_t>(count, uint32_t(kNumCounters));
+    std::memset(out, 0, size_t(count) * sizeof(uint64_t));
+    if (!pass->scratch) return FPT_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(out, pass->scratch, size_t(n) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, cudaGetErrorString(e));
+    return FPT_OK;
+}
+
+}  // extern "C"

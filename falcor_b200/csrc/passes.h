@@ -1,0 +1,44 @@
+// passes.h -- the render-pass object behind the fpt_pass handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+
+#include "common.h"
+
+namespace fpt {
+
+struct PropValue {
+    double n = 0.0;
+    std::string s;
+    bool isString = false;
+    static PropValue num(double v) { PropValue p; p.n = v; return p; }
+    static PropValue str(const std::string& v) { PropValue p; p.s = v; p.isString = true; return p; }
+};
+
+}  // namespace fpt
+
+struct fpt_pass {
+    std::string type;
+    std::map<std::string, fpt::PropValue> props;
+    fpt_scene* scene = nullptr;
+    void* scratch = nullptr;          // counters (16 B) + work counter (4 B)
+    void* adjointScratch = nullptr;   // checkpointed path vertices (adjoint)
+    size_t adjointScratchBytes = 0;
+    uint32_t frameCount = 0;
+    bool useFixedSeed = false;
+    bool warnedLightBVH = false;
+    uint32_t launches = 0;
+
+    double num(const std::string& k) const;
+    std::string str(const std::string& k) const;
+};
+
+namespace fpt {
+fpt_status ensure_scratch(fpt_pass& p);
+// WARDiffPathTracer primal (dLdI == nullptr) or adjoint.
+fpt_status wardiff_execute(fpt_pass& p, const fpt_frame_io* io, const float* dLdI, const fpt_grad_buffers* grads,
+                           cudaStream_t st);
+}  // namespace fpt

@@ -1,0 +1,31 @@
+// scene_device.h -- the device scene object behind the fpt_scene handle.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "device_scene.cuh"
+
+namespace fpt {
+
+struct DeviceBuffers {
+    std::vector<void*> ptrs;
+    size_t bytes = 0;
+    DeviceBuffers() = default;
+    DeviceBuffers(const DeviceBuffers&) = delete;
+    DeviceBuffers& operator=(const DeviceBuffers&) = delete;
+    ~DeviceBuffers();
+};
+
+fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out);
+
+}  // namespace fpt
+
+struct fpt_scene {
+    fpt::DevScene dev;
+    fpt::DeviceBuffers buffers;
+    fpt::BVH8 bvh;                    // host copy of the acceleration structure
+    std::vector<uint32_t> aliasTable; // host copy of the alias table
+    float aliasWeightSum = 0.f;
+    fpt_scene_info info{};
+};

@@ -1,0 +1,187 @@
+"""Render passes with Falcor's RenderPass interface (RenderGraph/RenderPass.h).
+
+``RenderPass.create(type, props)`` mirrors ``RenderPass::create`` by name
+(RenderGraph/RenderPass.cpp:53-60) for the passes of the hot path:
+``MinimalPathTracer``, ``PathTracer``, ``WARDiffPathTracer`` and the
+``VBufferRT`` that feeds them.  Properties use the reference names and
+defaults; unknown keys are warned about and ignored.  ``execute`` takes a
+``RenderData``-like mapping from channel names to CUDA tensors and runs on the
+current torch stream.  All work goes through libfpt.so; there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+from typing import Any, Mapping
+
+from . import _ffi
+from ._ffi import check, lib
+from .scene import Scene
+
+
+def _ptr(t) -> int | None:
+    if t is None:
+        return None
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("render pass channels must be CUDA tensors")
+    if not t.is_contiguous():
+        raise ValueError("render pass channels must be contiguous")
+    return t.data_ptr()
+
+
+def _stream() -> int:
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+class RenderPass:
+    """A render pass object backed by an fpt_pass handle."""
+
+    TYPES = ("MinimalPathTracer", "PathTracer", "VBufferRT", "WARDiffPathTracer")
+
+    def __init__(self, type_name: str, props: Mapping[str, Any] | None = None):
+        h = C.c_void_p()
+        check(lib().fpt_pass_create(type_name.encode(), C.byref(h)))
+        self._h = h
+        self.type = type_name
+        self.scene: Scene | None = None
+        if props:
+            self.set_properties(props)
+
+    @classmethod
+    def create(cls, type_name: str, props: Mapping[str, Any] | None = None) -> "RenderPass":
+        cls_map = {"MinimalPathTracer": MinimalPathTracer, "PathTracer": PathTracer, "VBufferRT": VBufferRT,
+                   "WARDiffPathTracer": WARDiffPathTracer}
+        if type_name not in cls_map:
+            raise ValueError(f"unknown render pass type '{type_name}'")
+        return cls_map[type_name](props)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().fpt_pass_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # Properties (Utils/Properties.h).
+    def set_properties(self, props: Mapping[str, Any]) -> None:
+        for k, v in props.items():
+            key = k.encode()
+            if isinstance(v, str):
+                check(lib().fpt_pass_set_property_string(self._h, key, v.encode()))
+            elif isinstance(v, bool):
+                check(lib().fpt_pass_set_property_int(self._h, key, int(v)))
+            elif isinstance(v, int):
+                check(lib().fpt_pass_set_property_int(self._h, key, v))
+            elif isinstance(v, float):
+                check(lib().fpt_pass_set_property_float(self._h, key, v))
+            elif hasattr(v, "name"):  # enum-like
+                check(lib().fpt_pass_set_property_string(self._h, key, str(v.name).encode()))
+            else:
+                raise TypeError(f"unsupported property type for '{k}': {type(v)}")
+
+    setProperties = set_properties
+
+    @property
+    def properties(self) -> dict:
+        buf = C.create_string_buffer(8192)
+        check(lib().fpt_pass_get_properties_json(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    getProperties = properties
+
+    def reflect(self) -> dict:
+        buf = C.create_string_buffer(8192)
+        check(lib().fpt_pass_reflect_json(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    def set_scene(self, scene: Scene | None) -> None:
+        self.scene = scene
+        check(lib().fpt_pass_set_scene(self._h, scene.handle if scene else None))
+
+    setScene = set_scene
+
+    def _io(self, rd: Mapping[str, Any], width: int, height: int, frame: int, prng_dim: int = 0,
+            sample_color=None) -> _ffi.fpt_frame_io:
+        io = _ffi.fpt_frame_io()
+        io.width, io.height = width, height
+        io.frame_index = frame
+        io.prng_dimension = prng_dim
+        io.vbuffer = _ptr(rd.get("vbuffer")) if self.type != "VBufferRT" else None
+        io.color = _ptr(rd.get("color"))
+        io.ray_count = _ptr(rd.get("rayCount"))
+        io.path_length = _ptr(rd.get("pathLength"))
+        io.d_color = _ptr(rd.get("dColor"))
+        io.vbuffer_out = _ptr(rd.get("vbuffer")) if self.type == "VBufferRT" else None
+        io.sample_color = _ptr(sample_color)
+        return io
+
+    def execute(self, render_data: Mapping[str, Any], frame: int = 0, prng_dimension: int = 0, sample_color=None) -> None:
+        """RenderPass::execute: render into the output channels of `render_data`."""
+        some = next((t for t in render_data.values() if t is not None), None)
+        if some is None:
+            raise ValueError("render_data has no channels")
+        height, width = int(some.shape[0]), int(some.shape[1])
+        io = self._io(render_data, width, height, frame, prng_dimension, sample_color)
+        check(lib().fpt_pass_execute(self._h, C.byref(io), C.c_void_p(_stream())))
+
+    def stats(self) -> _ffi.fpt_pass_stats:
+        s = _ffi.fpt_pass_stats()
+        check(lib().fpt_pass_get_stats(self._h, C.byref(s), C.c_void_p(_stream())))
+        return s
+
+    COUNTER_NAMES = ("paths", "rays", "closest_rays", "shadow_rays", "node_visits", "tri_tests", "hits",
+                     "light_samples", "env_samples", "env_evals", "env_pdfs")
+
+    def counters(self) -> dict:
+        """Event counters of the last execute (PixelStats equivalent)."""
+        arr = (C.c_uint64 * len(self.COUNTER_NAMES))()
+        check(lib().fpt_pass_get_counters(self._h, arr, len(arr), C.c_void_p(_stream())))
+        return dict(zip(self.COUNTER_NAMES, [int(x) for x in arr]))
+
+
+class VBufferRT(RenderPass):
+    def __init__(self, props=None):
+        super().__init__("VBufferRT", props)
+
+
+class MinimalPathTracer(RenderPass):
+    def __init__(self, props=None):
+        super().__init__("MinimalPathTracer", props)
+
+
+class PathTracer(RenderPass):
+    def __init__(self, props=None):
+        super().__init__("PathTracer", props)
+
+    def reset(self) -> None:
+        """PathTracer::reset (PathTracer.cpp:198-214): restart the frame counter."""
+        if self.scene is not None:
+            self.set_scene(self.scene)
+
+    @property
+    def fixedSeed(self) -> int:
+        return int(self.properties["fixedSeed"])
+
+    @fixedSeed.setter
+    def fixedSeed(self, v: int) -> None:
+        self.set_properties({"fixedSeed": int(v)})
+
+
+class WARDiffPathTracer(RenderPass):
+    def __init__(self, props=None):
+        super().__init__("WARDiffPathTracer", props)
+
+    def backward(self, render_data: Mapping[str, Any], dLdI, material_grad=None, position_grad=None, frame: int = 0) -> None:
+        some = next((t for t in render_data.values() if t is not None), dLdI)
+        height, width = int(some.shape[0]), int(some.shape[1])
+        io = self._io(render_data, width, height, frame)
+        g = _ffi.fpt_grad_buffers()
+        g.material = _ptr(material_grad)
+        g.mesh_position = _ptr(position_grad)
+        g.material_dim = material_grad.numel() if material_grad is not None else 0
+        g.position_dim = position_grad.numel() if position_grad is not None else 0
+        check(lib().fpt_pass_backward(self._h, C.byref(io), C.c_void_p(_ptr(dLdI)), C.byref(g), C.c_void_p(_stream())))

@@ -1,0 +1,152 @@
+"""Scenes: procedural host scenes (the synthetic workloads) and device scenes.
+
+``HostScene`` owns a scene description in host memory (the SceneBuilder
+inputs: vertices, indices, geometry instances, StandardMaterials, camera,
+optional lat-long env map).  ``Scene`` uploads one to the current CUDA device:
+it builds the compressed 8-wide BVH, the light collection with its alias table
+and the env-map importance map (Scene + SceneBuilder + LightCollection +
+EmissivePowerSampler + EnvMapSampler of the reference).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import check, lib
+
+# fpt_procedural_kind
+BOX_ICOSPHERE = 0
+HEIGHTFIELD_SOUP = 1
+DISPLACED_SPHERE = 2
+RANDOM_SOUP = 3
+DISPLACED_GRID = 4
+
+
+class HostScene:
+    """A scene description in host memory (library-owned when procedural)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        self.desc = lib().fpt_scene_host_desc(handle).contents
+
+    @staticmethod
+    def procedural(kind: int, seed: int = 0, grid_res: int = 0, soup_triangles: int = 0, material_count: int = 0,
+                   emissive_count: int = 0, sphere_subdiv: int = 0, envmap: tuple[int, int] | None = None,
+                   aspect_ratio: float = 0.0) -> "HostScene":
+        p = _ffi.fpt_procedural_params(kind=kind, seed=seed, grid_res=grid_res, soup_triangles=soup_triangles,
+                                       material_count=material_count, emissive_count=emissive_count,
+                                       sphere_subdiv=sphere_subdiv, envmap_width=envmap[0] if envmap else 0,
+                                       envmap_height=envmap[1] if envmap else 0, lambert=0, aspect_ratio=aspect_ratio)
+        h = C.c_void_p()
+        check(lib().fpt_procedural_scene(C.byref(p), C.byref(h)))
+        return HostScene(h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().fpt_scene_host_free(self._h)
+            self._h = None
+
+    # numpy views (valid while this object lives)
+    @property
+    def vertices(self) -> np.ndarray:
+        d = self.desc
+        return np.ctypeslib.as_array(C.cast(d.vertices, C.POINTER(C.c_float)), shape=(d.vertex_count, 12))
+
+    @property
+    def indices(self) -> np.ndarray:
+        d = self.desc
+        return np.ctypeslib.as_array(d.indices, shape=(d.index_count,))
+
+    @property
+    def instances(self) -> np.ndarray:
+        d = self.desc
+        return np.ctypeslib.as_array(C.cast(d.instances, C.POINTER(C.c_uint32)), shape=(d.instance_count, 5))
+
+    @property
+    def materials(self) -> np.ndarray:
+        d = self.desc
+        return np.ctypeslib.as_array(C.cast(d.materials, C.POINTER(C.c_float)), shape=(d.material_count, 19))
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.instances[:, 2].sum()) if self.desc.instance_count else 0
+
+    def camera_data(self) -> _ffi.fpt_camera_data:
+        cd = _ffi.fpt_camera_data()
+        check(lib().fpt_camera_compute(C.byref(self.desc.camera), C.byref(cd)))
+        return cd
+
+    def hit_bits(self) -> _ffi.fpt_hitinfo_bits:
+        b = _ffi.fpt_hitinfo_bits()
+        check(lib().fpt_hitinfo_compute_bits(C.byref(self.desc), C.byref(b)))
+        return b
+
+
+class Scene:
+    """A scene resident on the current CUDA device (fpt_scene)."""
+
+    def __init__(self, host: HostScene):
+        self.host = host
+        h = C.c_void_p()
+        check(lib().fpt_scene_create(C.byref(host.desc), C.byref(h)))
+        self._h = h
+        self.info = _ffi.fpt_scene_info()
+        check(lib().fpt_scene_get_info(self._h, C.byref(self.info)))
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().fpt_scene_destroy(self._h)
+            self._h = None
+
+    def bvh(self) -> tuple[np.ndarray, np.ndarray]:
+        """Host copies of the 8-wide BVH nodes (80 B each) and triangle records (48 B each)."""
+        v = _ffi.fpt_bvh_view()
+        check(lib().fpt_scene_get_bvh(self._h, C.byref(v)))
+        nodes = np.ctypeslib.as_array(C.cast(v.nodes, C.POINTER(C.c_uint8)), shape=(v.node_count * 80,)).copy()
+        tris = np.ctypeslib.as_array(C.cast(v.tris, C.POINTER(C.c_uint8)), shape=(v.tri_count * 48,)).copy()
+        return nodes.reshape(-1, 80), tris.reshape(-1, 48)
+
+    def alias_table(self) -> tuple[np.ndarray, float]:
+        n = self.info.emissive_triangle_count
+        out = np.zeros(2 * max(n, 1), dtype=np.uint32)
+        inv = C.c_float()
+        check(lib().fpt_scene_get_alias_table(self._h, out.ctypes.data_as(C.POINTER(C.c_uint32)), n, C.byref(inv)))
+        return out[: 2 * n], float(inv.value)
+
+
+@dataclass(frozen=True)
+class Workload:
+    """A named synthetic workload: scene parameters plus frame settings."""
+    name: str
+    kind: int
+    width: int
+    height: int
+    spp: int
+    max_bounces: int
+    params: dict
+
+
+# The synthetic workloads (procedural scenes; no dataset is involved).
+WORKLOADS = {
+    "box_icosphere_256": Workload("box_icosphere_256", BOX_ICOSPHERE, 256, 256, 1, 3,
+                                  dict(seed=0, sphere_subdiv=4, aspect_ratio=1.0)),
+    "heightfield_soup_1080p": Workload("heightfield_soup_1080p", HEIGHTFIELD_SOUP, 1920, 1080, 64, 8,
+                                       dict(seed=1, grid_res=1024, soup_triangles=200000, material_count=256,
+                                            emissive_count=64, envmap=(1024, 512), aspect_ratio=1920 / 1080)),
+    "displaced_sphere_512": Workload("displaced_sphere_512", DISPLACED_SPHERE, 512, 512, 16, 4,
+                                     dict(seed=3, material_count=256, sphere_subdiv=142, emissive_count=8,
+                                          envmap=(256, 128), aspect_ratio=1.0)),
+}
+
+
+def make_host_scene(w: Workload, **overrides) -> HostScene:
+    params = dict(w.params)
+    params.update(overrides)
+    return HostScene.procedural(w.kind, **params)

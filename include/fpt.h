@@ -1,0 +1,351 @@
+/*
+ * fpt.h -- C-ABI of the B200-native Falcor path-tracing hot path.
+ *
+ * Plain C structs, caller-owned device memory for frame I/O, stream-ordered
+ * execution, integer status codes and no exceptions across the boundary.
+ * Streams are passed as `void*` (a cudaStream_t; NULL = legacy default
+ * stream) so that FFI callers (ctypes, cgo, JNI) need no CUDA headers.
+ *
+ * Each entry point names the reference interface it replaces.  Paths are
+ * relative to the Falcor 8.0 source tree.
+ */
+#ifndef FPT_H
+#define FPT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define FPT_API __declspec(dllexport)
+#else
+#define FPT_API __attribute__((visibility("default")))
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes.  Replaces FALCOR_THROW (Core/Error.h:106-123): every error  */
+/* is returned, and the message is available from fpt_last_error().         */
+/* ------------------------------------------------------------------------ */
+typedef enum fpt_status {
+    FPT_OK = 0,
+    FPT_ERR_INVALID_ARG = 1,   /* bad pointer, size or property value         */
+    FPT_ERR_CUDA = 2,          /* a CUDA runtime call failed                  */
+    FPT_ERR_OOM = 3,           /* device allocation failed                    */
+    FPT_ERR_NO_SCENE = 4,      /* pass executed without a scene               */
+    FPT_ERR_UNSUPPORTED = 5,   /* feature outside the implemented subset      */
+    FPT_ERR_DEVICE = 6,        /* a kernel raised its device error word       */
+    FPT_ERR_TIMEOUT = 7,       /* a bounded device loop gave up               */
+    FPT_ERR_NO_DEVICE = 8      /* no CUDA device / extension not usable       */
+} fpt_status;
+
+/* Device error word bits written by kernels (never a trap). */
+#define FPT_DEVERR_STACK_OVERFLOW 0x1u /* traversal stack overflow            */
+#define FPT_DEVERR_BAD_INDEX      0x2u /* out-of-range node/triangle index     */
+#define FPT_DEVERR_NAN            0x4u /* NaN radiance written                 */
+#define FPT_DEVERR_TIMEOUT        0x8u /* persistent loop hit its deadline     */
+#define FPT_DEVERR_QUEUE          0x10u /* work-queue bound exceeded           */
+
+/* ------------------------------------------------------------------------ */
+/* Scene description (host memory).  Mirrors the SceneBuilder inputs of the  */
+/* triangle-mesh subset: StaticVertexData (Scene/SceneTypes.slang:217-224),  */
+/* GeometryInstanceData (SceneTypes.slang:106-120), BasicMaterialData        */
+/* (Scene/Material/BasicMaterialData.slang:48-88) and CameraData             */
+/* (Scene/Camera/CameraData.slang:40-75).  Geometry is static and already in */
+/* world space (Scene.cpp:2986-2990 pre-transforms static meshes).           */
+/* ------------------------------------------------------------------------ */
+typedef struct fpt_vertex {
+    float position[3];
+    float normal[3];
+    float tangent[4];   /* xyz + sign w; w == 0 marks "no tangent"           */
+    float texcoord[2];
+} fpt_vertex;           /* 48 B, StaticVertexData without curveRadius        */
+
+#define FPT_INSTANCE_FRONT_FACE_CW 0x8u /* MeshFlags::IsFrontFaceCW          */
+
+typedef struct fpt_geometry_instance {
+    uint32_t vb_offset;      /* first vertex of the mesh                      */
+    uint32_t ib_offset;      /* first index (in uint32 units) of the mesh     */
+    uint32_t triangle_count;
+    uint32_t material_id;
+    uint32_t flags;          /* FPT_INSTANCE_*                                */
+} fpt_geometry_instance;
+
+#define FPT_MATERIAL_DOUBLE_SIDED 0x1u
+#define FPT_MATERIAL_THIN_SURFACE 0x2u
+
+typedef struct fpt_material {     /* StandardMaterial, MetalRough model       */
+    float base_color[4];          /* rgb + opacity; stored as fp16 on device  */
+    float specular[4];            /* occlusion, roughness, metallic, unused   */
+    float emissive[3];
+    float emissive_factor;
+    float ior;                    /* stored as fp16 in the material header    */
+    float specular_transmission;
+    float diffuse_transmission;
+    float transmission[3];
+    uint32_t flags;               /* FPT_MATERIAL_*                           */
+} fpt_material;
+
+typedef struct fpt_camera {       /* Camera properties (Camera.cpp)           */
+    float position[3];
+    float target[3];
+    float up[3];
+    float focal_length;           /* mm; 0 means FOV 0                        */
+    float frame_height;           /* mm                                       */
+    float aspect_ratio;
+    float near_z, far_z;
+    float focal_distance;
+    float jitter_x, jitter_y;
+} fpt_camera;
+
+typedef struct fpt_camera_data {  /* ray-tracing subset of CameraData        */
+    float posW[3];
+    float cameraU[3];
+    float cameraV[3];
+    float cameraW[3];
+    float nearZ, farZ;
+    float jitterX, jitterY;
+} fpt_camera_data;
+
+typedef struct fpt_envmap_desc {  /* EnvMap (Scene/Lights/EnvMap.slang)      */
+    uint32_t width, height;       /* lat-long RGB32F texels                    */
+    const float* rgb;             /* width*height*3 floats, row-major          */
+    float tint[3];
+    float intensity;
+} fpt_envmap_desc;
+
+typedef struct fpt_scene_desc {
+    const fpt_vertex* vertices;
+    uint32_t vertex_count;
+    const uint32_t* indices;      /* local (per-mesh) vertex indices          */
+    uint32_t index_count;
+    const fpt_geometry_instance* instances;
+    uint32_t instance_count;
+    const fpt_material* materials;
+    uint32_t material_count;
+    fpt_camera camera;
+    const fpt_envmap_desc* envmap; /* NULL: no environment light              */
+} fpt_scene_desc;
+
+/* Procedural synthetic scenes (the benchmark workloads). */
+typedef enum fpt_procedural_kind {
+    FPT_SCENE_BOX_ICOSPHERE = 0,  /* 12 quads + emissive ceiling + icosphere   */
+    FPT_SCENE_HEIGHTFIELD_SOUP = 1, /* fBm grid + random triangles + envmap    */
+    FPT_SCENE_DISPLACED_SPHERE = 2, /* displaced sphere, per-face materials    */
+    FPT_SCENE_RANDOM_SOUP = 3,    /* random triangle soup + emitters + envmap  */
+    FPT_SCENE_DISPLACED_GRID = 4  /* displaced grid + emitters + envmap        */
+} fpt_procedural_kind;
+
+typedef struct fpt_procedural_params {
+    uint32_t kind;                /* fpt_procedural_kind                       */
+    uint32_t seed;
+    uint32_t grid_res;            /* heightfield / grid vertices per side      */
+    uint32_t soup_triangles;      /* random triangles                          */
+    uint32_t material_count;
+    uint32_t emissive_count;      /* emissive triangles                        */
+    uint32_t sphere_subdiv;       /* icosphere subdivision / sphere tessellation */
+    uint32_t envmap_width, envmap_height; /* 0: no envmap                      */
+    uint32_t lambert;             /* reserved                                  */
+    float aspect_ratio;           /* camera aspect (frame width / height)      */
+} fpt_procedural_params;
+
+/* Opaque handles. */
+typedef struct fpt_scene fpt_scene;
+typedef struct fpt_pass fpt_pass;
+typedef struct fpt_batch fpt_batch;
+typedef struct fpt_scene_host fpt_scene_host;
+
+/* ------------------------------------------------------------------------ */
+/* Library / device.                                                         */
+/* ------------------------------------------------------------------------ */
+FPT_API const char* fpt_version(void);
+/* Last error message of the calling thread (empty string if none). */
+FPT_API const char* fpt_last_error(void);
+/* Number of visible CUDA devices with compute capability 10.x (0 if none). */
+FPT_API int fpt_device_count(void);
+
+/* ------------------------------------------------------------------------ */
+/* Host-side scene tools (no GPU needed).                                   */
+/* ------------------------------------------------------------------------ */
+/* Generates a procedural scene into library-owned host memory.
+ * Replaces scene import through SceneBuilder (Scene/SceneBuilder.cpp) for the
+ * synthetic benchmark scenes. */
+FPT_API fpt_status fpt_procedural_scene(const fpt_procedural_params* params,
+                                        fpt_scene_host** out);
+FPT_API const fpt_scene_desc* fpt_scene_host_desc(const fpt_scene_host* h);
+FPT_API void fpt_scene_host_free(fpt_scene_host* h);
+
+/* Camera::calculateCameraParameters ray-tracing vectors
+ * (Scene/Camera/Camera.cpp:112-195). */
+FPT_API fpt_status fpt_camera_compute(const fpt_camera* cam, fpt_camera_data* out);
+
+/* HitInfo bit allocation (Scene/HitInfo.cpp:52-108) for a scene
+ * description: type, instance-ID and primitive-index bits of the
+ * uncompressed 128-bit PackedHitInfo header. */
+typedef struct fpt_hitinfo_bits {
+    uint32_t type_bits, instance_id_bits, primitive_index_bits;
+} fpt_hitinfo_bits;
+FPT_API fpt_status fpt_hitinfo_compute_bits(const fpt_scene_desc* desc, fpt_hitinfo_bits* out);
+
+/* Host copies of the device-side acceleration structure, for tests and for
+ * the oracle's node/triangle visit counts.  `nodes` is an array of 80-byte
+ * compressed 8-wide nodes, `tris` an array of 48-byte triangle records. */
+typedef struct fpt_bvh_view {
+    const void* nodes;
+    uint32_t node_count;
+    const void* tris;
+    uint32_t tri_count;
+    float scene_lo[3], scene_hi[3];
+} fpt_bvh_view;
+
+/* Host-only build of the same compressed 8-wide BVH that fpt_scene_create
+ * uploads (no GPU needed).  The reference has no software triangle BVH:
+ * this replaces the driver-built BLAS/TLAS (Scene::buildBlas Scene.cpp:3376). */
+typedef struct fpt_bvh fpt_bvh;
+FPT_API fpt_status fpt_bvh_build(const fpt_scene_desc* desc, fpt_bvh** out);
+FPT_API fpt_status fpt_bvh_get_view(const fpt_bvh* bvh, fpt_bvh_view* out, uint32_t* max_depth, double* build_seconds);
+FPT_API void fpt_bvh_free(fpt_bvh* bvh);
+
+/* ------------------------------------------------------------------------ */
+/* Device scene.  Replaces Scene + its DXR BLAS/TLAS build                   */
+/* (Scene::buildBlas Scene.cpp:3376, buildTlas Scene.h:1176) and the         */
+/* LightCollection / EmissivePowerSampler / EnvMapSampler setup             */
+/* (LightCollection.cpp, EmissivePowerSampler.cpp:86-175,                   */
+/* EnvMapSampler.cpp:38-80).  Synchronous on the current device.            */
+/* ------------------------------------------------------------------------ */
+FPT_API fpt_status fpt_scene_create(const fpt_scene_desc* desc, fpt_scene** out);
+FPT_API void fpt_scene_destroy(fpt_scene* scene);
+
+typedef struct fpt_scene_info {
+    uint32_t triangle_count;
+    uint32_t instance_count;
+    uint32_t material_count;
+    uint32_t emissive_triangle_count;
+    uint32_t bvh_node_count;
+    uint32_t has_envmap;
+    fpt_hitinfo_bits hit_bits;
+    double bvh_build_seconds;
+    uint64_t device_bytes;
+    fpt_camera_data camera;
+} fpt_scene_info;
+FPT_API fpt_status fpt_scene_get_info(const fpt_scene* scene, fpt_scene_info* out);
+/* Host view of the scene's BVH (valid until the scene is destroyed). */
+FPT_API fpt_status fpt_scene_get_bvh(const fpt_scene* scene, fpt_bvh_view* out);
+/* Host copy of the emissive alias table (uint2 per emissive triangle) and
+ * the reciprocal weight sum (EmissivePowerSampler::bindShaderData). */
+FPT_API fpt_status fpt_scene_get_alias_table(const fpt_scene* scene, uint32_t* out_pairs,
+                                             uint32_t capacity, float* inv_weight_sum);
+
+/* ------------------------------------------------------------------------ */
+/* Render passes.  Replaces the RenderPass plugins                            */
+/*   MinimalPathTracer (RenderPasses/MinimalPathTracer/MinimalPathTracer.cpp) */
+/*   PathTracer        (RenderPasses/PathTracer/PathTracer.cpp)               */
+/*   WARDiffPathTracer (RenderPasses/WARDiffPathTracer/WARDiffPathTracer.cpp) */
+/*   VBufferRT         (RenderPasses/GBuffer/VBuffer/VBufferRT.cpp)          */
+/* created by name as RenderPass::create (RenderGraph/RenderPass.cpp:53-60). */
+/* ------------------------------------------------------------------------ */
+FPT_API fpt_status fpt_pass_create(const char* type_name, fpt_pass** out);
+FPT_API void fpt_pass_destroy(fpt_pass* pass);
+
+/* Properties (Utils/Properties.h): same names and defaults as the reference
+ * passes.  Unknown keys are logged as warnings and ignored, never an error
+ * (MinimalPathTracer.cpp:86, PathTracer.cpp:366). */
+FPT_API fpt_status fpt_pass_set_property_int(fpt_pass* pass, const char* key, int64_t value);
+FPT_API fpt_status fpt_pass_set_property_float(fpt_pass* pass, const char* key, double value);
+FPT_API fpt_status fpt_pass_set_property_string(fpt_pass* pass, const char* key, const char* value);
+/* Serialises the current properties as a JSON object into buf (NUL-terminated).
+ * Returns FPT_ERR_INVALID_ARG if capacity is too small. */
+FPT_API fpt_status fpt_pass_get_properties_json(const fpt_pass* pass, char* buf, size_t capacity);
+/* Input/output channel list (RenderPass::reflect) as JSON. */
+FPT_API fpt_status fpt_pass_reflect_json(const fpt_pass* pass, char* buf, size_t capacity);
+
+/* RenderPass::setScene (RenderGraph/RenderPass.h:218). */
+FPT_API fpt_status fpt_pass_set_scene(fpt_pass* pass, fpt_scene* scene);
+
+/* Per-frame I/O (RenderData channels).  All pointers are caller-owned device
+ * memory; NULL marks an unconnected optional channel. */
+typedef struct fpt_frame_io {
+    uint32_t width, height;
+    uint32_t frame_index;        /* gFrameCount / params.frameCount           */
+    uint32_t prng_dimension;     /* kRenderPassPRNGDimension                  */
+    const uint32_t* vbuffer;     /* in  "vbuffer": PackedHitInfo uint4/pixel   */
+    float* color;                /* out "color": RGBA32F                      */
+    uint32_t* ray_count;         /* out "rayCount": R32Uint                   */
+    uint32_t* path_length;       /* out "pathLength": R32Uint                 */
+    float* d_color;              /* out "dColor" (WARDiffPathTracer)          */
+    uint32_t* vbuffer_out;       /* out "vbuffer" of VBufferRT                */
+    float* sample_color;         /* out, optional: per-sample RGB radiance
+                                    (3 floats, pixel-major, spp per pixel),
+                                    before the per-sample colour format      */
+} fpt_frame_io;
+
+/* RenderPass::execute (RenderGraph/RenderPass.h:184). */
+FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void* stream);
+
+/* Gradient buffers (DiffRendering/SceneGradients.cpp:42-206): caller-owned
+ * device arrays, accumulated into (not cleared). */
+typedef struct fpt_grad_buffers {
+    float* material;             /* material_count * 20 floats
+                                    (DiffMaterialData layout), or NULL       */
+    float* mesh_position;        /* vertex_count * 3 floats, or NULL          */
+    uint32_t material_dim;       /* number of floats in `material`            */
+    uint32_t position_dim;       /* number of floats in `mesh_position`       */
+} fpt_grad_buffers;
+
+/* bwd_diff(tracePaths) of WARDiffPathTracer.rt.slang:167-180 by path replay:
+ * dLdI is a caller-owned device array of float3 per pixel. */
+FPT_API fpt_status fpt_pass_backward(fpt_pass* pass, const fpt_frame_io* io,
+                                     const float* dLdI, const fpt_grad_buffers* grads,
+                                     void* stream);
+
+/* Device counters of the last execute (rays traced, paths, error word). */
+typedef struct fpt_pass_stats {
+    uint64_t paths;
+    uint64_t rays;
+    uint32_t device_error;
+    uint32_t kernel_launches;
+} fpt_pass_stats;
+FPT_API fpt_status fpt_pass_get_stats(fpt_pass* pass, fpt_pass_stats* out, void* stream);
+
+/* Event counters of the last execute, the PixelStats equivalent
+ * (Rendering/Utils/PixelStats.h:47): [0] paths, [1] rays, [2] closest-hit
+ * rays, [3] visibility rays, [4] BVH node visits, [5] triangle tests,
+ * [6] shaded hits, [7] emissive light samples, [8] env-map importance
+ * samples, [9] env-map evaluations, [10] env-map pdf evaluations. */
+#define FPT_NUM_COUNTERS 11
+FPT_API fpt_status fpt_pass_get_counters(fpt_pass* pass, uint64_t* out, uint32_t count, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Batched uneven forward: many render requests in one persistent launch    */
+/* captured as a CUDA graph.  No reference counterpart (the reference       */
+/* renders one graph execution per request); each request is a PathTracer  */
+/* execute with its own scene, resolution, spp, bounce limit and seed.     */
+/* ------------------------------------------------------------------------ */
+typedef struct fpt_batch_request {
+    fpt_scene* scene;
+    uint32_t width, height;
+    uint32_t spp;
+    uint32_t max_bounces;
+    uint32_t seed;
+    float* color;                /* RGBA32F output, caller-owned device memory */
+} fpt_batch_request;
+
+FPT_API fpt_status fpt_batch_create(fpt_batch** out);
+FPT_API void fpt_batch_destroy(fpt_batch* batch);
+FPT_API fpt_status fpt_batch_add(fpt_batch* batch, const fpt_batch_request* req);
+/* Tuning: block size and queue chunk (0 = autotuned value). */
+FPT_API fpt_status fpt_batch_set_tuning(fpt_batch* batch, uint32_t block_size, uint32_t chunk);
+/* Runs the autotuner over block size and chunk on the current requests. */
+FPT_API fpt_status fpt_batch_autotune(fpt_batch* batch, void* stream);
+/* One persistent launch over all requests (graph-captured on first call). */
+FPT_API fpt_status fpt_batch_launch(fpt_batch* batch, void* stream);
+/* The same requests as one plain launch per request, for comparison. */
+FPT_API fpt_status fpt_batch_launch_sequential(fpt_batch* batch, void* stream);
+FPT_API fpt_status fpt_batch_get_stats(fpt_batch* batch, fpt_pass_stats* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FPT_H */

@@ -1,0 +1,160 @@
+"""ctypes loader of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
+the checker and by bench.py's cpu_baseline / reference legs.  The product
+package (falcor_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ORACLE_DIR = Path(__file__).resolve().parent
+LIB_PATH = ORACLE_DIR / "_build" / "liboracle.so"
+
+u32 = C.c_uint32
+_P = C.c_void_p
+
+
+class MinimalPTParams(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("frameCount", u32), ("prngDimension", u32), ("maxBounces", u32),
+                ("computeDirect", u32), ("useImportanceSampling", u32), ("lambert", u32)]
+
+
+class PathTracerParams(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("samplesPerPixel", u32), ("maxSurfaceBounces", u32),
+                ("maxDiffuseBounces", u32), ("maxSpecularBounces", u32), ("maxTransmissionBounces", u32),
+                ("sampleGenerator", u32), ("useBSDFSampling", u32), ("useNEE", u32), ("useMIS", u32),
+                ("misHeuristic", u32), ("misPowerExponent", C.c_float), ("emissiveSampler", u32),
+                ("specularRoughnessThreshold", C.c_float), ("colorFormat", u32), ("seed", u32), ("lambert", u32)]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [("triangle_count", u32), ("instance_count", u32), ("emissive_count", u32), ("active_emissive_count", u32),
+                ("type_bits", u32), ("instance_id_bits", u32), ("primitive_index_bits", u32), ("has_env", u32),
+                ("alias_weight_sum", C.c_float), ("imp_dim", u32), ("imp_base_mip", u32)]
+
+
+class Counters(C.Structure):
+    _fields_ = [("paths", C.c_uint64), ("rays", C.c_uint64), ("closest", C.c_uint64), ("shadow", C.c_uint64),
+                ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64)]
+
+
+_lib = None
+
+
+def build() -> Path:
+    """Builds liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        l = C.CDLL(str(LIB_PATH))
+        l.orc_scene_create.restype = _P
+        l.orc_scene_create.argtypes = [_P, _P]
+        l.orc_scene_destroy.argtypes = [_P]
+        l.orc_scene_get_info.argtypes = [_P, C.POINTER(SceneInfo)]
+        l.orc_scene_get_lights.argtypes = [_P, _P, _P, _P]
+        l.orc_scene_get_importance.argtypes = [_P, u32, _P]
+        l.orc_vbuffer.argtypes = [_P, u32, u32, _P, u32]
+        l.orc_trace_closest.argtypes = [_P, u32, _P, _P, _P, _P, _P, _P, C.c_int]
+        l.orc_trace_visibility.argtypes = [_P, u32, _P, _P, _P, _P]
+        l.orc_minimal_pt.restype = C.c_double
+        l.orc_minimal_pt.argtypes = [_P, C.POINTER(MinimalPTParams), _P, _P, _P, C.c_int, u32, u32, u32, u32, u32]
+        l.orc_path_tracer.restype = C.c_double
+        l.orc_path_tracer.argtypes = [_P, C.POINTER(PathTracerParams), _P, _P, _P, C.c_int, u32, u32, u32, u32, u32,
+                                      C.POINTER(Counters)]
+        for n in ("orc_xoshiro", "orc_lcg"):
+            getattr(l, n).argtypes = [_P, u32, u32, _P]
+        l.orc_splitmix.argtypes = [_P, u32, u32, _P]
+        l.orc_jenkins.argtypes = [_P, u32, _P]
+        l.orc_bit_interleave.argtypes = [_P, u32, _P]
+        l.orc_compute_ray_origin.argtypes = [_P, _P, u32, _P]
+        l.orc_sample_generator.argtypes = [C.c_int, _P, _P, _P, u32, u32, _P]
+        l.orc_f32tof16.argtypes = [_P, u32, _P]
+        l.orc_f16tof32.argtypes = [_P, u32, _P]
+        l.orc_logluv.argtypes = [_P, u32, _P, _P]
+        l.orc_intersect_triangle.restype = u32
+        l.orc_intersect_triangle.argtypes = [_P, _P, _P, _P, _P]
+        l.orc_bsdf_sample.argtypes = [_P, C.c_int, u32, _P, _P, u32, _P, _P, _P, _P, _P, _P, _P]
+        _lib = l
+    return _lib
+
+
+def ptr(a: np.ndarray) -> C.c_void_p:
+    assert a.flags["C_CONTIGUOUS"]
+    return C.c_void_p(a.ctypes.data)
+
+
+class OracleScene:
+    """The oracle's copy of a scene, built from the same host description."""
+
+    def __init__(self, desc_ptr, camera_data):
+        self._h = lib().orc_scene_create(C.cast(desc_ptr, _P), C.cast(C.pointer(camera_data), _P))
+        if not self._h:
+            raise RuntimeError("oracle scene creation failed")
+        self.info = SceneInfo()
+        lib().orc_scene_get_info(self._h, C.byref(self.info))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_scene_destroy(self._h)
+            self._h = None
+
+    def vbuffer(self, w: int, h: int, threads: int = 0) -> np.ndarray:
+        out = np.zeros((h, w, 4), dtype=np.uint32)
+        lib().orc_vbuffer(self._h, w, h, ptr(out), threads)
+        return out
+
+    def trace_closest(self, o: np.ndarray, d: np.ndarray, tmin: np.ndarray, tmax: np.ndarray, brute: bool = False):
+        n = o.shape[0]
+        o = np.ascontiguousarray(o, dtype=np.float32)
+        d = np.ascontiguousarray(d, dtype=np.float32)
+        tmin = np.ascontiguousarray(tmin, dtype=np.float32)
+        tmax = np.ascontiguousarray(tmax, dtype=np.float32)
+        out = np.zeros((n, 4), dtype=np.uint32)
+        t = np.zeros(n, dtype=np.float32)
+        lib().orc_trace_closest(self._h, n, ptr(o), ptr(d), ptr(tmin), ptr(tmax), ptr(out), ptr(t), int(brute))
+        return out, t
+
+    def minimal_pt(self, vbuffer: np.ndarray, params: MinimalPTParams, fp64: bool = False, threads: int = 0, rect=None):
+        h, w = vbuffer.shape[:2]
+        out = np.zeros((h, w, 4), dtype=np.float32)
+        rays = np.zeros((h, w), dtype=np.uint32)
+        x0, y0, x1, y1 = rect if rect else (0, 0, w, h)
+        dt = lib().orc_minimal_pt(self._h, C.byref(params), ptr(np.ascontiguousarray(vbuffer)), ptr(out), ptr(rays),
+                                  int(fp64), threads, x0, y0, x1, y1)
+        return out, rays, dt
+
+    def path_tracer(self, vbuffer: np.ndarray, params: PathTracerParams, fp64: bool = False, threads: int = 0, rect=None,
+                    samples: bool = False):
+        h, w = vbuffer.shape[:2]
+        out = np.zeros((h, w, 4), dtype=np.float32)
+        smp = np.zeros((h, w, params.samplesPerPixel, 3), dtype=np.float32) if samples else None
+        cnt = Counters()
+        x0, y0, x1, y1 = rect if rect else (0, 0, w, h)
+        dt = lib().orc_path_tracer(self._h, C.byref(params), ptr(np.ascontiguousarray(vbuffer)), ptr(out),
+                                   ptr(smp) if smp is not None else None, int(fp64), threads, x0, y0, x1, y1, C.byref(cnt))
+        return out, smp, cnt, dt
+
+    def lights(self):
+        n = self.info.emissive_count
+        alias = np.zeros(2 * max(n, 1), dtype=np.uint32)
+        flux = np.zeros(max(n, 1), dtype=np.float32)
+        area = np.zeros(max(n, 1), dtype=np.float32)
+        lib().orc_scene_get_lights(self._h, ptr(alias), ptr(flux), ptr(area))
+        return alias[: 2 * n], flux[:n], area[:n]
+
+    def importance(self, mip: int = 0) -> np.ndarray:
+        d = self.info.imp_dim >> mip
+        out = np.zeros((d, d), dtype=np.float32)
+        lib().orc_scene_get_importance(self._h, mip, ptr(out))
+        return out

@@ -1,0 +1,256 @@
+// oracle_capi.cpp -- C entry points of the CPU oracle, loaded with ctypes by
+// the tests, by smoke() and by bench.py's cpu_baseline leg.
+//
+// TEST INFRASTRUCTURE ONLY (see oracle_math.h): nothing in the product path
+// links or loads this library.
+#include <chrono>
+#include <cstdio>
+#include <exception>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "oracle_render.h"
+
+using namespace orc;
+
+namespace {
+thread_local std::string g_err;
+}
+
+extern "C" {
+
+const char* orc_last_error() { return g_err.c_str(); }
+
+void* orc_scene_create(const fpt_scene_desc* d, const fpt_camera_data* cam) {
+    try {
+        return new Scene(d, cam);
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+void orc_scene_destroy(void* s) { delete static_cast<Scene*>(s); }
+
+struct orc_scene_info {
+    uint32_t triangle_count, instance_count, emissive_count, active_emissive_count;
+    uint32_t type_bits, instance_id_bits, primitive_index_bits, has_env;
+    float alias_weight_sum;
+    uint32_t imp_dim, imp_base_mip;
+};
+void orc_scene_get_info(const void* sp, orc_scene_info* out) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    out->triangle_count = uint32_t(s.triInstance.size());
+    out->instance_count = uint32_t(s.instances.size());
+    out->emissive_count = uint32_t(s.emissive.size());
+    out->active_emissive_count = uint32_t(s.activeTriangles.size());
+    out->type_bits = s.hitBits.type_bits;
+    out->instance_id_bits = s.hitBits.instance_id_bits;
+    out->primitive_index_bits = s.hitBits.primitive_index_bits;
+    out->has_env = s.hasEnv ? 1u : 0u;
+    out->alias_weight_sum = s.aliasWeightSum;
+    out->imp_dim = s.impDim;
+    out->imp_base_mip = s.impBaseMip;
+}
+// Alias table (2 uints per emissive triangle) and per-triangle flux.
+void orc_scene_get_lights(const void* sp, uint32_t* alias, float* flux, float* area) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    for (size_t i = 0; i < s.emissive.size(); i++) {
+        if (alias) { alias[2 * i] = s.aliasTable[2 * i]; alias[2 * i + 1] = s.aliasTable[2 * i + 1]; }
+        if (flux) flux[i] = s.emissive[i].flux;
+        if (area) area[i] = s.emissive[i].area;
+    }
+}
+// Importance map mip (dim >> mip)^2 floats.
+void orc_scene_get_importance(const void* sp, uint32_t mip, float* out) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    if (mip >= s.impMips.size()) return;
+    std::copy(s.impMips[mip].begin(), s.impMips[mip].end(), out);
+}
+
+void orc_vbuffer(const void* sp, uint32_t W, uint32_t H, uint32_t* out, uint32_t threads) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    parallel_tiles(0, 0, W, H, threads, [&](uint32_t x, uint32_t y, uint32_t) { render_vbuffer_pixel(s, W, H, x, y, out); });
+}
+
+// Per-ray closest hits: origins/dirs n*3 floats; out n*4 uint32 PackedHitInfo +
+// tOut n floats.  brute != 0 tests every triangle.
+void orc_trace_closest(const void* sp, uint32_t n, const float* o, const float* d, const float* tmin, const float* tmax,
+                       uint32_t* out, float* tOut, int brute) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    for (uint32_t i = 0; i < n; i++) {
+        V3<float> oo(o[3 * i], o[3 * i + 1], o[3 * i + 2]), dd(d[3 * i], d[3 * i + 1], d[3 * i + 2]);
+        Hit h = brute ? s.traceClosestBrute(oo, dd, tmin[i], tmax[i]) : s.traceClosest(oo, dd, tmin[i], tmax[i], nullptr);
+        pack_hit(s.hitBits, h, out + 4 * size_t(i));
+        if (tOut) tOut[i] = h.valid ? h.t : -1.f;
+    }
+}
+void orc_trace_visibility(const void* sp, uint32_t n, const float* o, const float* d, const float* tmax, uint32_t* out) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    for (uint32_t i = 0; i < n; i++) {
+        V3<float> oo(o[3 * i], o[3 * i + 1], o[3 * i + 2]), dd(d[3 * i], d[3 * i + 1], d[3 * i + 2]);
+        out[i] = s.traceVisibility(oo, dd, 0.f, tmax[i], nullptr) ? 1u : 0u;
+    }
+}
+
+// MinimalPathTracer over the rectangle [x0,x1)x[y0,y1) of a W x H frame.
+// out: RGBA32F for the full frame (only the rectangle is written).
+double orc_minimal_pt(const void* sp, const MinimalPTParams* p, const uint32_t* vbuffer, float* out, uint32_t* rays,
+                      int fp64, uint32_t threads, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    auto t0 = std::chrono::steady_clock::now();
+    parallel_tiles(x0, y0, x1, y1, threads, [&](uint32_t x, uint32_t y, uint32_t) {
+        size_t i = size_t(y) * p->width + x;
+        uint32_t r = 0;
+        float* o = out + 4 * i;
+        if (fp64) {
+            V3<double> c = minimal_pt_pixel<double>(s, *p, x, y, vbuffer + 4 * i, &r);
+            o[0] = float(c.x); o[1] = float(c.y); o[2] = float(c.z);
+        } else {
+            V3<float> c = minimal_pt_pixel<float>(s, *p, x, y, vbuffer + 4 * i, &r);
+            o[0] = c.x; o[1] = c.y; o[2] = c.z;
+        }
+        o[3] = 1.f;
+        if (rays) rays[i] = r;
+    });
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+struct orc_counters { uint64_t paths, rays, closest, shadow, node_visits, tri_tests; };
+
+// PathTracer over a rectangle.  color: RGBA32F full frame; samples (optional):
+// per pixel spp*3 floats, pixel-major over the full frame.
+double orc_path_tracer(const void* sp, const PathTracerParams* p, const uint32_t* vbuffer, float* color, float* samples,
+                       int fp64, uint32_t threads, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, orc_counters* cnt) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    uint32_t nthreads = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
+    std::vector<PathCounters> pcs(nthreads);
+    auto t0 = std::chrono::steady_clock::now();
+    parallel_tiles(x0, y0, x1, y1, nthreads, [&](uint32_t x, uint32_t y, uint32_t tid) {
+        size_t i = size_t(y) * p->width + x;
+        float* so = samples ? samples + i * size_t(p->samplesPerPixel) * 3 : nullptr;
+        if (fp64) path_tracer_pixel<double>(s, *p, x, y, vbuffer + 4 * i, so, color + 4 * i, &pcs[tid]);
+        else path_tracer_pixel<float>(s, *p, x, y, vbuffer + 4 * i, so, color + 4 * i, &pcs[tid]);
+    });
+    double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (cnt) {
+        *cnt = orc_counters{0, 0, 0, 0, 0, 0};
+        for (auto& c : pcs) {
+            cnt->paths += c.paths; cnt->rays += c.rays; cnt->closest += c.tc.closest; cnt->shadow += c.tc.shadow;
+            cnt->node_visits += c.tc.nodeVisits; cnt->tri_tests += c.tc.triTests;
+        }
+    }
+    return dt;
+}
+
+// ----- Known-answer helpers (RNG, hashing, packing, ray offsets) ---------------
+void orc_xoshiro(const uint32_t* seeds, uint32_t n, uint32_t dims, uint32_t* out) {
+    for (uint32_t i = 0; i < n; i++) {
+        Xoshiro128 r{{seeds[4 * i], seeds[4 * i + 1], seeds[4 * i + 2], seeds[4 * i + 3]}};
+        for (uint32_t j = 0; j < dims; j++) out[size_t(j) * n + i] = r.next();
+    }
+}
+void orc_splitmix(const uint32_t* seeds, uint32_t n, uint32_t dims, uint64_t* out) {
+    for (uint32_t i = 0; i < n; i++) {
+        SplitMix64 r = SplitMix64::create(seeds[2 * i], seeds[2 * i + 1]);
+        for (uint32_t j = 0; j < dims; j++) out[size_t(j) * n + i] = r.next64();
+    }
+}
+void orc_lcg(const uint32_t* seeds, uint32_t n, uint32_t dims, uint32_t* out) {
+    for (uint32_t i = 0; i < n; i++) {
+        LCG r{seeds[i]};
+        for (uint32_t j = 0; j < dims; j++) out[size_t(j) * n + i] = r.next();
+    }
+}
+void orc_jenkins(const uint32_t* in, uint32_t n, uint32_t* out) { for (uint32_t i = 0; i < n; i++) out[i] = jenkins_hash(in[i]); }
+// Mirrors the five outputs of BitTricksTests.cs.slang:testBitInterleave.
+void orc_bit_interleave(const uint32_t* data, uint32_t n, uint32_t* out) {
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t d = data[i];
+        uint32_t bx = d & 0xffffu, by = d >> 16;
+        uint32_t inter = interleave_32bit(bx, by);
+        out[5 * i + 0] = interleave_32bit(bx ^ 0xbeef0000u, by ^ 0xbeef0000u);
+        out[5 * i + 1] = interleave_16bit(bx ^ 0xbeefed00u, by ^ 0xbeefed00u);
+        uint32_t x, y;
+        deinterleave_16bit(inter & 0x0000ffffu, x, y);
+        out[5 * i + 2] = (y << 16) | x;
+        deinterleave_8bit(inter & 0x000000ffu, x, y);
+        out[5 * i + 3] = (y << 16) | x;
+        deinterleave_2x8bit(inter & 0x00ff00ffu, x, y);
+        uint32_t tx = ((x >> 8) & 0x0f00u) | (x & 0xfu), ty = ((y >> 8) & 0x0f00u) | (y & 0xfu);
+        out[5 * i + 4] = (ty << 16) | tx;
+    }
+}
+void orc_compute_ray_origin(const float* pos, const float* nrm, uint32_t n, float* out) {
+    for (uint32_t i = 0; i < n; i++) {
+        V3<float> r = compute_ray_origin(V3<float>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]),
+                                         V3<float>(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]));
+        out[3 * i] = r.x; out[3 * i + 1] = r.y; out[3 * i + 2] = r.z;
+    }
+}
+// First `dims` raw 32-bit outputs of a sample generator per (pixel, sampleNumber).
+void orc_sample_generator(int kind, const uint32_t* px, const uint32_t* py, const uint32_t* sn, uint32_t n, uint32_t dims,
+                          uint32_t* out) {
+    for (uint32_t i = 0; i < n; i++) {
+        if (kind == 1) {
+            UniformSG g(px[i], py[i], sn[i]);
+            for (uint32_t j = 0; j < dims; j++) out[size_t(i) * dims + j] = g.next();
+        } else {
+            TinyUniformSG g(px[i], py[i], sn[i]);
+            for (uint32_t j = 0; j < dims; j++) out[size_t(i) * dims + j] = g.next();
+        }
+    }
+}
+void orc_f32tof16(const float* in, uint32_t n, uint16_t* out) { for (uint32_t i = 0; i < n; i++) out[i] = f32tof16_host(in[i]); }
+void orc_f16tof32(const uint16_t* in, uint32_t n, float* out) { for (uint32_t i = 0; i < n; i++) out[i] = f16tof32(in[i]); }
+void orc_logluv(const float* rgb, uint32_t n, uint32_t* enc, float* dec) {
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t e = encode_logluv_hdr(V3<float>(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2]));
+        enc[i] = e;
+        V3<float> d = decode_logluv_hdr(e);
+        dec[3 * i] = d.x; dec[3 * i + 1] = d.y; dec[3 * i + 2] = d.z;
+    }
+}
+uint32_t orc_intersect_triangle(const float* ro, const float* rd, const float* v, float* bary, float* t) {
+    V3<float> vv[3] = {V3<float>(v[0], v[1], v[2]), V3<float>(v[3], v[4], v[5]), V3<float>(v[6], v[7], v[8])};
+    V3<float> b;
+    bool hit = intersect_ray_triangle(V3<float>(ro[0], ro[1], ro[2]), V3<float>(rd[0], rd[1], rd[2]), vv, b, *t);
+    bary[0] = b.x; bary[1] = b.y; bary[2] = b.z;
+    return hit ? 1u : 0u;
+}
+
+// StandardBSDF in the local frame, for sampling/pdf consistency tests.
+// data: diffuse[3], specular[3], roughness, metallic, eta, diffTrans, specTrans.
+// For each of n inputs: wi (3 floats), u (4 random uint32 words used as the
+// sample generator stream).  Outputs wo, weight, pdf, lobe, valid, plus
+// eval(wi, wo) and evalPdf(wi, wo) of the sampled direction.
+struct ListSG {
+    const uint32_t* w; uint32_t i = 0, n;
+    uint32_t next() { return i < n ? w[i++] : 0u; }
+};
+void orc_bsdf_sample(const float* data, int lambert, uint32_t n, const float* wi, const uint32_t* words, uint32_t nwords,
+                     float* wo, float* weight, float* pdf, uint32_t* lobe, uint32_t* valid, float* evalOut, float* pdfOut) {
+    BSDFData<float> d;
+    d.diffuse = V3<float>(data[0], data[1], data[2]);
+    d.specular = V3<float>(data[3], data[4], data[5]);
+    d.roughness = data[6]; d.metallic = data[7]; d.eta = data[8]; d.diffuseTransmission = data[9]; d.specularTransmission = data[10];
+    d.transmission = V3<float>(1.f);
+    for (uint32_t i = 0; i < n; i++) {
+        V3<float> w(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+        StandardBSDF<float> b(w, d, false, LOBE_ALL, lambert != 0);
+        ListSG sg{words + size_t(i) * nwords, 0, nwords};
+        V3<float> o, wt;
+        float pd;
+        uint32_t lb;
+        bool ok = b.sample(w, o, pd, wt, lb, sg);
+        wo[3 * i] = o.x; wo[3 * i + 1] = o.y; wo[3 * i + 2] = o.z;
+        weight[3 * i] = wt.x; weight[3 * i + 1] = wt.y; weight[3 * i + 2] = wt.z;
+        pdf[i] = pd; lobe[i] = lb; valid[i] = ok ? 1u : 0u;
+        V3<float> e = b.eval(w, o);
+        evalOut[3 * i] = e.x; evalOut[3 * i + 1] = e.y; evalOut[3 * i + 2] = e.z;
+        pdfOut[i] = b.eval_pdf(w, o);
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,132 @@
+// oracle_scene.h -- the oracle's own copy of the scene as the reference shaders
+// see it: packed vertices, fp16-quantised materials, the emissive light
+// collection, the power-sampler alias table and the env-map importance map,
+// plus a simple binary BVH used only to find closest hits quickly.
+//
+// TEST INFRASTRUCTURE ONLY (see oracle_math.h).
+#pragma once
+
+#include <vector>
+#include <cstdint>
+#include "oracle_math.h"
+#include "../include/fpt.h"
+
+namespace orc {
+
+// PackedStaticVertexData (Scene/SceneTypes.slang:226-294), host pack + device unpack.
+struct PackedVertex {
+    float pos[3];
+    uint32_t nxy;        // fp16 normal.x | normal.y << 16
+    uint32_t nz_tw;      // fp16 normal.z | fp16 tangent sign << 16
+    uint32_t tangentOct; // encodeNormal2x16(tangent.xyz)
+    float uv[2];
+};
+
+struct StaticVertex {  // StaticVertexData after unpack()
+    V3<float> position, normal;
+    float tangent[4];
+    V2<float> uv;
+};
+
+// BasicMaterialData fields used by StandardMaterial (fp16 where the reference stores fp16).
+struct Material {
+    float baseColor[4];  // fp16-quantised
+    float specular[4];   // fp16-quantised: occlusion, roughness, metallic
+    float emissive[3];
+    float emissiveFactor;
+    float ior;           // fp16-quantised (MaterialHeader IoR)
+    float specTrans, diffTrans;  // fp16-quantised
+    float transmission[3];       // fp16-quantised
+    bool doubleSided, thinSurface;
+    uint32_t activeLobes;
+    bool emissiveNonZero;
+};
+
+// EmissiveTriangle after PackedEmissiveTriangle::unpack (LightCollectionShared.slang:41-135).
+struct EmissiveTri {
+    V3<float> posW[3];
+    V2<float> uv[3];     // fp16-quantised
+    V3<float> normal;    // decoded from the 2x16 octahedral encoding
+    float area;
+    uint32_t materialID;
+    float flux;          // FinalizeIntegration.cs.slang:103-111
+    V3<float> averageRadiance;
+};
+
+struct Hit {
+    bool valid = false;
+    uint32_t instanceID = 0, primitiveIndex = 0, globalTri = 0;
+    float baryX = 0, baryY = 0;  // DXR-style barycentrics (weights of v1, v2)
+    float t = 0;
+};
+
+struct TraceCounters {
+    uint64_t closest = 0, shadow = 0, nodeVisits = 0, triTests = 0;
+};
+
+class Scene {
+public:
+    Scene(const fpt_scene_desc* d, const fpt_camera_data* cam, uint32_t aliasSeedDefault = 1);
+
+    // geometry
+    std::vector<PackedVertex> vertices;
+    std::vector<uint32_t> indices;
+    std::vector<fpt_geometry_instance> instances;
+    std::vector<uint32_t> triInstance, triPrim;     // global triangle -> (instance, primitive)
+    std::vector<uint32_t> instanceTriOffset;        // instance -> first global triangle
+    std::vector<V3<float>> triV;                    // 3 world-space positions per global triangle
+    std::vector<Material> materials;
+    fpt_camera_data camera;
+    fpt_hitinfo_bits hitBits;
+
+    // lights
+    std::vector<EmissiveTri> emissive;
+    std::vector<uint32_t> instanceEmissiveOffset;   // perMeshInstanceOffset, 0xffffffff if none
+    std::vector<uint32_t> activeTriangles;
+    std::vector<uint32_t> aliasTable;               // 2 uints per emissive triangle
+    float aliasWeightSum = 0.f;
+
+    // environment
+    bool hasEnv = false;
+    uint32_t envW = 0, envH = 0;
+    std::vector<float> envRGB;
+    float envScale[3] = {1, 1, 1};                  // intensity * tint
+    uint32_t impDim = 0, impBaseMip = 0;
+    std::vector<std::vector<float>> impMips;        // mip 0 = impDim^2
+
+    // helpers
+    StaticVertex getVertex(uint32_t globalIndex) const;
+    void getTriangleVertexIndices(uint32_t instanceID, uint32_t prim, uint32_t idx[3]) const;
+    uint32_t emissiveIndex(uint32_t instanceID, uint32_t prim) const {
+        uint32_t o = instanceEmissiveOffset[instanceID];
+        return o == 0xffffffffu ? 0xffffffffu : o + prim;
+    }
+    V3<float> envEval(V3<float> dir) const;         // EnvMap::eval (bilinear, wrap u, clamp v)
+    V3<double> envEvalD(V3<double> dir) const;
+
+    // traversal
+    Hit traceClosest(V3<float> o, V3<float> d, float tMin, float tMax, TraceCounters* c) const;
+    bool traceVisibility(V3<float> o, V3<float> d, float tMin, float tMax, TraceCounters* c) const;
+    Hit traceClosestD(V3<double> o, V3<double> d, double tMin, double tMax) const;
+    bool traceVisibilityD(V3<double> o, V3<double> d, double tMin, double tMax) const;
+
+    // brute-force closest hit over all triangles (for traversal tests)
+    Hit traceClosestBrute(V3<float> o, V3<float> d, float tMin, float tMax) const;
+
+private:
+    struct Node { float lo[3], hi[3]; uint32_t left, right, first, count; };
+    std::vector<Node> nodes;
+    std::vector<uint32_t> order;
+    void buildBVH();
+    void buildLights(uint32_t aliasSeed);
+    void buildEnv(const fpt_envmap_desc* env);
+    template <class R> Hit traceImpl(V3<R> o, V3<R> d, R tMin, R tMax, bool anyHit, TraceCounters* c) const;
+};
+
+// Packs one vertex like PackedStaticVertexData::pack on the host.
+PackedVertex pack_vertex(const fpt_vertex& v);
+
+// EmissivePowerSampler::generateAliasTable (EmissivePowerSampler.cpp:86-175).
+void generate_alias_table(std::vector<float> weights, std::vector<uint32_t>& table, float& weightSum);
+
+}  // namespace orc

@@ -1,0 +1,86 @@
+"""The C-ABI library loads and exports every entry point include/fpt.h declares
+(no GPU needed: nothing here launches device work)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "fpt.h").read_text()
+    return sorted(set(re.findall(r"FPT_API\s+[^;(]*?\b(fpt_\w+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "fpt_pass_execute" in syms and "fpt_scene_create" in syms and "fpt_pass_backward" in syms
+    assert len(syms) >= 30
+
+
+def test_library_exports_every_declared_symbol(fpt):
+    from falcor_b200 import _ffi
+    missing = [s for s in declared_symbols() if not hasattr(fpt, s)]
+    assert not missing, missing
+    # The ctypes signature table covers the same set.
+    assert sorted(_ffi.SIGNATURES) == declared_symbols()
+
+
+def test_version_and_errors(fpt):
+    assert b"sm_100a" in fpt.fpt_version()
+    h = C.c_void_p()
+    st = fpt.fpt_pass_create(b"NoSuchPass", C.byref(h))
+    assert st == 1 and b"NoSuchPass" in fpt.fpt_last_error()
+
+
+def test_pass_properties_defaults_and_unknown_keys(fpt):
+    from falcor_b200.passes import RenderPass
+    pt = RenderPass.create("PathTracer")
+    p = pt.properties
+    # PathTracer.h:130-170 defaults.
+    assert p["samplesPerPixel"] == 1 and p["maxDiffuseBounces"] == 3 and p["maxSpecularBounces"] == 3
+    assert p["maxTransmissionBounces"] == 10 and p["useNEE"] == 1 and p["useMIS"] == 1
+    assert p["misHeuristic"] == "Balance" and p["emissiveSampler"] == "LightBVH" and p["colorFormat"] == "LogLuvHDR"
+    assert abs(p["specularRoughnessThreshold"] - 0.25) < 1e-12
+    pt.set_properties({"samplesPerPixel": 4, "emissiveSampler": "Power", "noSuchKey": 3})  # unknown: warning only
+    assert pt.properties["samplesPerPixel"] == 4 and pt.properties["emissiveSampler"] == "Power"
+    mpt = RenderPass.create("MinimalPathTracer")
+    assert mpt.properties["maxBounces"] == 3 and mpt.properties["computeDirect"] == 1
+    war = RenderPass.create("WARDiffPathTracer")
+    q = war.properties
+    assert q["auxSampleCount"] == 16 and q["Log10vMFConcentration"] == 5 and q["useAntitheticSampling"] == 1
+    assert abs(q["boundaryTermBeta"] - 0.01) < 1e-12
+
+
+def test_reflect_channels(fpt):
+    from falcor_b200.passes import RenderPass
+    r = RenderPass.create("MinimalPathTracer").reflect()
+    assert [c["name"] for c in r["inputs"]] == ["vbuffer", "viewW"]
+    assert [c["name"] for c in r["outputs"]] == ["color"]
+    r = RenderPass.create("PathTracer").reflect()
+    outs = [c["name"] for c in r["outputs"]]
+    assert "color" in outs and "rayCount" in outs and "pathLength" in outs
+    r = RenderPass.create("WARDiffPathTracer").reflect()
+    assert [c["name"] for c in r["outputs"]] == ["color", "dColor"]
+
+
+def test_procedural_scenes_and_camera(fpt):
+    from falcor_b200.scene import HostScene, BOX_ICOSPHERE, HEIGHTFIELD_SOUP
+    s = HostScene.procedural(BOX_ICOSPHERE, seed=0, sphere_subdiv=4, aspect_ratio=1.0)
+    assert s.triangle_count == 24 + 2 + 5120
+    assert s.desc.instance_count == 14 and s.desc.material_count == 14
+    bits = s.hit_bits()
+    # HitInfo.cpp:52-108: 7 hit types -> 3 bits, 14 instances -> 4 bits, 5120 triangles -> 13 bits.
+    assert (bits.type_bits, bits.instance_id_bits, bits.primitive_index_bits) == (3, 4, 13)
+    cd = s.camera_data()
+    W = np.array(cd.cameraW)
+    assert abs(np.linalg.norm(W) - 10000.0) < 1e-2  # focalDistance default
+    V = np.array(cd.cameraV)
+    # vlen = focalDistance * tan(fovY / 2) with fovY = 45 degrees
+    assert abs(np.linalg.norm(V) - 10000.0 * np.tan(np.radians(22.5))) < 1.0
+    h = HostScene.procedural(HEIGHTFIELD_SOUP, seed=1, grid_res=64, soup_triangles=1000, material_count=16,
+                             emissive_count=8, envmap=(64, 32), aspect_ratio=16 / 9)
+    assert h.triangle_count == 2 * 63 * 63 + 1000 + 8
+    assert h.desc.envmap and h.desc.envmap.contents.width == 64
