@@ -12,6 +12,7 @@
 // lane loops over the pixel's samples, so lanes of a warp stay in the same
 // trace/shade loop while their paths have different lengths.
 #include "kernels.cuh"
+#include "path_logic.cuh"
 
 namespace fpt {
 
@@ -22,32 +23,6 @@ namespace {
 constexpr int kVBufferBlock = 128;
 constexpr int kMinimalBlock = 128;
 constexpr int kPathBlock = 128;
-
-// Per-thread event counts, reduced per warp and added to the pass's device
-// counters once per thread: [0] paths, [1] rays, [2] closest-hit rays,
-// [3] visibility rays, [4] BVH node visits, [5] triangle tests, [6] shaded
-// hits, [7] emissive light samples, [8] env-map importance samples,
-// [9] env-map evaluations, [10] env-map pdf evaluations.
-struct Counters {
-    uint32_t v[kNumCounters] = {0};
-    FPT_D void trace(bool shadow, const TraceStats& ts) {
-        v[1]++;
-        v[shadow ? 3 : 2]++;
-        v[4] += ts.nodes;
-        v[5] += ts.tris;
-    }
-};
-
-FPT_D void flush_counters(unsigned long long* out, const Counters& c) {
-    if (!out) return;
-#pragma unroll
-    for (int i = 0; i < kNumCounters; i++) {
-        unsigned long long x = c.v[i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if ((threadIdx.x & 31) == 0 && x) atomicAdd(out + i, x);
-    }
-}
 
 // ---------------------------------------------------------------------------
 // VBufferRT.
@@ -149,273 +124,146 @@ __global__ void __launch_bounds__(kMinimalBlock) minimal_pt_kernel(DevScene s, F
     flush_counters(p.counters, cnt);
 }
 
-// ---------------------------------------------------------------------------
-// PathTracer.
-// ---------------------------------------------------------------------------
-constexpr uint32_t PF_ACTIVE = 0x1, PF_TRANSMISSION = 0x4, PF_SPECULAR = 0x8, PF_DELTA = 0x10;
-constexpr uint32_t PF_LIGHT_UPPER = 0x40, PF_LIGHT_LOWER = 0x80;
+// Per-lane state of the path-tracer state machine.
+enum LaneState : uint32_t { LS_FETCH = 0, LS_SHADE = 1, LS_TRACE = 2, LS_MISS = 3, LS_DONE = 4 };
 
-FPT_D float eval_mis(const FrameParams& p, float p0, float p1) {
-    if (p.misHeuristic == 0) { const float q0 = p0, q1 = p1; return q0 / (q0 + q1); }
-    if (p.misHeuristic == 1) { const float q0 = p0 * p0, q1 = p1 * p1; return q0 / (q0 + q1); }
-    const float q0 = powf(p0, p.misPowerExponent), q1 = powf(p1, p.misPowerExponent);
-    return q0 / (q0 + q1);
-}
-
-template <class SG>
-struct PathState {
-    uint32_t flags, bounces, vertexIndex;
-    float3 origin, dir, normal, thp, L;
-    float pdf;
-    HitRec hit;
-    SG sg;
-    FPT_D bool has(uint32_t f) const { return (flags & f) != 0; }
-    FPT_D void set(uint32_t f, bool v) { flags = v ? (flags | f) : (flags & ~f); }
-    FPT_D uint32_t getBounces(int t) const { return (bounces >> (t * 8)) & 0xffu; }
-    FPT_D bool isLightSampled() const { return (flags & (PF_LIGHT_UPPER | PF_LIGHT_LOWER)) != 0; }
-    FPT_D bool isLightSamplable() const { return !has(PF_DELTA); }
-};
-
-FPT_D bool finished_surface_bounces(const FrameParams& p, uint32_t bounces) {
-    const uint32_t d = bounces & 0xffu, sp = (bounces >> 8) & 0xffu, tr = (bounces >> 16) & 0xffu;
-    return (d + sp + tr > p.maxSurfaceBounces) || (d > p.maxDiffuseBounces) || (sp > p.maxSpecularBounces) ||
-           (tr > p.maxTransmissionBounces);
-}
-
-// generateLightSample (PathTracer.slang:705-738) for env + emissive lights.
-template <class SG>
-FPT_D bool generate_light_sample(const DevScene& s, const FrameParams& p, const ShadingData& sd, bool upper, bool lower,
-                                 SG& sg, float3& Li, float& lpdf, float3& lorigin, float3& ldir, float& ldist, Counters& cnt) {
-    const bool useEnv = s.hasEnv != 0, useEm = s.hasEmissive != 0;
-    float pr0 = useEnv ? 1.f : 0.f, pr1 = useEm ? 1.f : 0.f;
-    const float sum = pr0 + pr1;
-    if (sum != 0.f) { const float inv = 1.f / sum; pr0 *= inv; pr1 *= inv; }
-    float u = next1D(sg);
-    uint32_t lightType;
-    float selPdf;
-    if (u < pr0) { lightType = 0; selPdf = pr0; }
-    else {
-        u -= pr0;
-        if (u < pr1) { lightType = 1; selPdf = pr1; }
-        else return false;
-    }
-    bool valid = false;
-    if (useEnv && lightType == 0) {
-        float3 dir, Le;
-        float epdf;
-        env_sample(s, next2D(sg), dir, epdf, Le);
-        cnt.v[8]++;
-        Li = epdf > 0.f ? Le / epdf : f3(0.f);
-        lpdf = epdf;
-        lorigin = compute_ray_origin(sd.posW, dot(sd.faceN, dir) >= 0.f ? sd.faceN : -sd.faceN);
-        ldist = 1e30f;
-        ldir = dir;
-        valid = any_pos(Li);
-    }
-    if (useEm && lightType == 1) {
-        TriLightSample tls;
-        cnt.v[7]++;
-        if (emissive_sample(s, p.emissiveSampler, sd.posW, sg, tls)) {
-            Li = tls.pdf > 0.f ? tls.Le / tls.pdf : f3(0.f);
-            lpdf = tls.pdf;
-            const float3 lightPos = compute_ray_origin(tls.posW, tls.normalW);
-            const float3 toL0 = lightPos - sd.posW;
-            lorigin = compute_ray_origin(sd.posW, dot(sd.faceN, toL0) >= 0.f ? sd.faceN : -sd.faceN);
-            const float3 toLight = lightPos - lorigin;
-            ldist = length(toLight);
-            ldir = normalize(toLight);
-            valid = any_pos(Li);
-        }
-    }
-    if (!valid) return false;
-    const float NdotL = dot(sd_oriented_face_n(sd), ldir);
-    if ((!upper && NdotL >= -kMinCosTheta) || (!lower && NdotL <= kMinCosTheta)) return false;
-    lpdf *= selPdf;
-    Li = Li / selPdf;
-    return true;
-}
-
-// PathTracer::handleHit (PathTracer.slang:821-1066).
-template <class SG, bool HAS_T>
-FPT_D void pt_handle_hit(const DevScene& s, const FrameParams& p, PathState<SG>& path, uint2* stack, Counters& cnt) {
-    const bool isPrimaryHit = path.vertexIndex == 1;
-    const bool useEnv = s.hasEnv != 0, useEm = s.hasEmissive != 0;
-    const ShadingData sd = load_shading_data(s, path.hit, path.dir);
-    cnt.v[6]++;
-    const MaterialInstance<HAS_T> mi = material_instance<HAS_T>(s, sd, p.lambert != 0);
-    const float roughness = mi.propRoughness();
-    const bool isLightSamplable = path.isLightSamplable();
-    const bool computeEmissive =
-        isPrimaryHit || (useEm && (!p.useNEE || p.useMIS || !path.isLightSampled() || !isLightSamplable));
-    if (computeEmissive && any_pos(mi.emission)) {
-        float misWeight = 1.f;
-        if (useEm && p.useNEE && p.useMIS && !isPrimaryHit && path.isLightSampled() && isLightSamplable) {
-            const uint32_t off = __ldg(s.instEmissiveOffset + path.hit.instanceID);
-            const uint32_t triIdx = off == 0xffffffffu ? 0xffffffffu : off + path.hit.primIndex;
-            const float emissiveSel = (useEnv && useEm) ? 0.5f : 1.f;
-            const float lightPdf = emissiveSel * emissive_eval_pdf(s, p.emissiveSampler, path.origin, triIdx, sd.posW, sd_oriented_face_n(sd));
-            misWeight = eval_mis(p, path.pdf, lightPdf);
-        }
-        path.L += path.thp * (misWeight * mi.emission);
-    }
-    if (finished_surface_bounces(p, path.bounces)) { path.set(PF_ACTIVE, false); return; }
-    path.origin = sd_ray_origin(sd);
-    const uint32_t lobeTypes = mi.lobeTypes();
-    const bool applyNEE = p.useNEE && (lobeTypes & L_NON_DELTA) != 0;
-    path.set(PF_LIGHT_UPPER | PF_LIGHT_LOWER, false);
-    if (applyNEE) {
-        const bool upper = (lobeTypes & L_NON_DELTA_R) != 0, lower = (lobeTypes & L_NON_DELTA_T) != 0;
-        float3 Li, lorigin, ldir;
-        float lpdf, ldist;
-        const bool validSample = generate_light_sample(s, p, sd, upper, lower, path.sg, Li, lpdf, lorigin, ldir, ldist, cnt);
-        path.set(PF_LIGHT_UPPER, upper);
-        path.set(PF_LIGHT_LOWER, lower);
-        if (validSample) {
-            if (p.useMIS) {
-                const float scatterPdf = mi.evalPdf(sd, ldir, p.useBSDFSampling != 0);
-                Li *= eval_mis(p, lpdf, scatterPdf);
-            }
-            const float3 Lr = mi.eval(sd, ldir) * Li;
-            if (any_pos(Lr)) {
-                HitRec sh;
-                TraceStats ts;
-                trace_bvh<true>(s, lorigin, ldir, 0.f, ldist, sh, stack, kPathBlock, &ts);
-                cnt.trace(true, ts);
-                if (!sh.valid) path.L += path.thp * Lr;
-            }
-        }
-    }
-    // generateScatterRay (PathTracer.slang:385-513).
-    float3 wo, w;
-    float bpdf;
-    uint32_t lobe;
-    bool valid = mi.sample(sd, path.sg, wo, w, bpdf, lobe, p.useBSDFSampling != 0);
-    if (valid) {
-        path.dir = wo;
-        path.thp *= w;
-        path.pdf = bpdf;
-        path.set(PF_TRANSMISSION | PF_SPECULAR | PF_DELTA, false);
-        if (lobe & L_REFLECTION) {
-            const bool isDiffuse = (lobe & L_DIFF_R) || roughness > p.specularRoughnessThreshold;
-            if (isDiffuse) path.bounces += 1u;
-            else { path.bounces += 1u << 8; path.set(PF_SPECULAR, true); }
-        }
-        if (lobe & L_DELTA) path.set(PF_DELTA, true);
-        if (lobe & L_TRANSMISSION) {
-            path.bounces += 1u << 16;
-            path.set(PF_TRANSMISSION, true);
-            path.origin = sd_ray_origin(sd, false);
-        }
-        path.normal = sd_oriented_face_n(sd);
-        valid = any_pos(path.thp);
-    }
-    if (p.useNEE && !p.useMIS && finished_surface_bounces(p, path.bounces) && path.isLightSamplable()) valid = false;
-    if (!valid) path.set(PF_ACTIVE, false);
-}
-
-// PathTracer::handleMiss (PathTracer.slang:1071-1157).
-template <class SG>
-FPT_D void pt_handle_miss(const DevScene& s, const FrameParams& p, PathState<SG>& path, Counters& cnt) {
-    const bool useEnv = s.hasEnv != 0, useEm = s.hasEmissive != 0;
-    const bool isLightSamplable = path.isLightSamplable();
-    const bool computeEnv = useEnv && (!p.useNEE || p.useMIS || !path.isLightSampled() || !isLightSamplable);
-    if (computeEnv) {
-        float misWeight = 1.f;
-        if (p.useNEE && p.useMIS && path.isLightSampled() && isLightSamplable) {
-            const float envSel = (useEnv && useEm) ? 0.5f : 1.f;
-            const float lightPdf = envSel * env_eval_pdf(s, path.dir);
-            cnt.v[10]++;
-            misWeight = eval_mis(p, path.pdf, lightPdf);
-        }
-        path.L += path.thp * (misWeight * env_eval(s, path.dir));
-        cnt.v[9]++;
-    }
-    path.set(PF_ACTIVE, false);
-}
-
-template <class SG, bool HAS_T>
-FPT_D float3 pt_trace_path(const DevScene& s, const FrameParams& p, uint32_t x, uint32_t y, uint32_t sampleIdx,
-                           const HitRec& primary, float3 primaryDir, uint2* stack, Counters& cnt, uint32_t& rays) {
-    PathState<SG> path;
-    path.sg.init(x, y, p.seed * p.spp + sampleIdx);
-    path.flags = PF_ACTIVE;
-    path.bounces = 0;
-    path.thp = f3(1.f);
-    path.L = f3(0.f);
-    path.pdf = 0.f;
-    path.normal = f3(0.f);
-    path.origin = load3(s.camera.posW);
-    path.dir = primaryDir;
-    path.hit = primary;
-    path.vertexIndex = 1;
-    pt_handle_hit<SG, HAS_T>(s, p, path, stack, cnt);
-    while (path.has(PF_ACTIVE)) {
-        path.vertexIndex++;
-        rays++;
-        HitRec h;
-        TraceStats ts;
-        trace_bvh<false>(s, path.origin, path.dir, 0.f, 1e30f, h, stack, kPathBlock, &ts);
-        cnt.trace(false, ts);
-        if (h.valid) {
-            path.hit = h;
-            pt_handle_hit<SG, HAS_T>(s, p, path, stack, cnt);
-        } else {
-            pt_handle_miss<SG>(s, p, path, cnt);
-        }
-    }
-    cnt.v[0]++;
-    return path.L;
-}
-
+// Persistent path tracer.  Each lane owns one pixel at a time and runs its
+// spp samples one after the other (TracePass.rt.slang:490-506); a lane that
+// finishes its pixel fetches the next one with a warp-aggregated atomic, so
+// lanes regenerate work independently.  Every loop iteration has one
+// traversal call site (a visibility ray pending from NEE, else the extension
+// ray) followed by one shading call site (handleHit or handleMiss), which
+// keeps the warp converged in both phases and the kernel small.
 template <class SG, bool HAS_T>
 __global__ void __launch_bounds__(kPathBlock) path_tracer_kernel(DevScene s, FrameParams p) {
     __shared__ uint2 stackMem[kStackSize * kPathBlock];
     uint2* stack = stackMem + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t laneMaskLt = (1u << lane) - 1u;
+    const uint32_t spp = p.spp;
     Counters cnt;
+    uint32_t state = LS_FETCH;
+    uint32_t idx = 0, x = 0, y = 0, sampleIdx = 0, rays = 0;
+    float3 primaryDir = f3(0.f), color = f3(0.f);
+    HitRec primary;
+    primary.valid = false;
+    PathState<SG> path;
+    path.flags = 0;
+    path.shadowPending = false;
     for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(p.workCounter, 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= p.workItems) break;
-        const uint32_t idx = base + lane;
-        if (idx < p.workItems) {
-            const uint32_t x = idx % p.width, y = idx / p.width;
+        // (1) Work fetch for lanes without a pixel.  Background pixels are
+        // written right away (GeneratePaths::writeBackground).
+        for (;;) {
+            const bool need = state == LS_FETCH;
+            const uint32_t mask = __ballot_sync(0xffffffffu, need);
+            if (mask == 0) break;
+            const int leader = __ffs(mask) - 1;
+            uint32_t base = 0;
+            if (int(lane) == leader) base = atomicAdd(p.workCounter, uint32_t(__popc(mask)));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (!need) continue;
+            idx = base + uint32_t(__popc(mask & laneMaskLt));
+            if (idx >= p.workItems) { state = LS_DONE; continue; }
+            x = idx % p.width;
+            y = idx / p.width;
             float tMin, tMax;
-            const float3 primaryDir = camera_ray_dir(s.camera, x, y, p.width, p.height, tMin, tMax);
-            HitRec hit;
-            const bool isHit = unpack_hit(s.bits, __ldg(p.vbuffer + idx), hit);
-            const uint32_t spp = p.spp;
-            float3 color = f3(0.f);
-            uint32_t rays = 0;
-            if (!isHit) {
-                // GeneratePaths::writeBackground (GeneratePaths.cs.slang:208-245).
+            primaryDir = camera_ray_dir(s.camera, x, y, p.width, p.height, tMin, tMax);
+            color = f3(0.f);
+            rays = 0;
+            sampleIdx = 0;
+            if (unpack_hit(s.bits, __ldg(p.vbuffer + idx), primary)) {
+                state = LS_SHADE;  // primary hit of sample 0
+                path.sg.init(x, y, p.seed * spp);
+                path.flags = PF_ACTIVE;
+                path.bounces = 0;
+                path.thp = f3(1.f);
+                path.L = f3(0.f);
+                path.pdf = 0.f;
+                path.normal = f3(0.f);
+                path.origin = load3(s.camera.posW);
+                path.dir = primaryDir;
+                path.hit = primary;
+                path.vertexIndex = 1;
+                path.shadowPending = false;
+            } else {
                 const float3 bg = s.hasEnv ? env_eval(s, primaryDir) : f3(0.f);
                 if (s.hasEnv) cnt.v[9]++;
+                float3 c = f3(0.f);
                 for (uint32_t i = 0; i < spp; i++) {
                     if (p.sampleColor) {
                         float* o = p.sampleColor + (size_t(idx) * spp + i) * 3;
                         o[0] = bg.x; o[1] = bg.y; o[2] = bg.z;
                     }
-                    color += (spp != 1 && p.colorFormat == 1) ? decode_logluv_hdr(encode_logluv_hdr(bg)) : bg;
+                    c += (spp != 1 && p.colorFormat == 1) ? decode_logluv_hdr(encode_logluv_hdr(bg)) : bg;
                 }
-            } else {
-                for (uint32_t i = 0; i < spp; i++) {
-                    const float3 L = (p.sampleGenerator == 0)
-                                         ? pt_trace_path<TinyUniformSG, HAS_T>(s, p, x, y, i, hit, primaryDir, stack, cnt, rays)
-                                         : pt_trace_path<UniformSG, HAS_T>(s, p, x, y, i, hit, primaryDir, stack, cnt, rays);
-                    if (p.sampleColor) {
-                        float* o = p.sampleColor + (size_t(idx) * spp + i) * 3;
-                        o[0] = L.x; o[1] = L.y; o[2] = L.z;
-                    }
-                    color += (spp != 1 && p.colorFormat == 1) ? decode_logluv_hdr(encode_logluv_hdr(L)) : L;
-                }
+                const float3 out = spp == 1 ? c : c * (1.f / float(spp));
+                p.color[idx] = make_float4(out.x, out.y, out.z, 1.f);
+                if (p.rayCount) p.rayCount[idx] = 0;
+                // stays LS_FETCH
             }
-            // ResolvePass (ResolvePass.cs.slang:80-101); 1 spp writes the colour directly.
-            const float3 out = spp == 1 ? color : color * (1.f / float(spp));
-            if (!isfinite(out.x) || !isfinite(out.y) || !isfinite(out.z)) atomicOr(s.errorWord, FPT_DEVERR_NAN);
-            p.color[idx] = make_float4(out.x, out.y, out.z, 1.f);
-            if (p.rayCount) p.rayCount[idx] = rays;
+        }
+        if (__all_sync(0xffffffffu, state == LS_DONE)) break;
+
+        // (2) Traversal: the pending visibility ray, else the extension ray.
+        if (state == LS_TRACE) {
+            const bool shadow = path.shadowPending;
+            HitRec h;
+            TraceStats ts;
+            if (shadow) trace_bvh<true>(s, path.sOrigin, path.sDir, 0.f, path.sDist, h, stack, kPathBlock, &ts);
+            else trace_bvh<false>(s, path.origin, path.dir, 0.f, 1e30f, h, stack, kPathBlock, &ts);
+            cnt.trace(shadow, ts);
+            rays++;
+            if (shadow) {
+                path.shadowPending = false;
+                if (!h.valid) path.L += path.sLr;
+                // The extension ray is traced on the next iteration (if the path continues).
+            } else {
+                path.vertexIndex++;
+                if (h.valid) { path.hit = h; state = LS_SHADE; }
+                else state = LS_MISS;
+            }
+        }
+
+        // (3) Shading: handleHit / handleMiss.
+        if (state == LS_SHADE) pt_handle_hit<SG, HAS_T>(s, p, path, cnt);
+        else if (state == LS_MISS) pt_handle_miss<SG>(s, p, path, cnt);
+        if (state == LS_SHADE || state == LS_MISS || state == LS_TRACE) {
+            if (path.has(PF_ACTIVE) || path.shadowPending) {
+                state = LS_TRACE;
+            } else {
+                // Sample finished (writeOutput + ResolvePass accumulation).
+                cnt.v[0]++;
+                const float3 L = path.L;
+                if (p.sampleColor) {
+                    float* o = p.sampleColor + (size_t(idx) * spp + sampleIdx) * 3;
+                    o[0] = L.x; o[1] = L.y; o[2] = L.z;
+                }
+                color += (spp != 1 && p.colorFormat == 1) ? decode_logluv_hdr(encode_logluv_hdr(L)) : L;
+                sampleIdx++;
+                if (sampleIdx < spp) {
+                    path.sg.init(x, y, p.seed * spp + sampleIdx);
+                    path.flags = PF_ACTIVE;
+                    path.bounces = 0;
+                    path.thp = f3(1.f);
+                    path.L = f3(0.f);
+                    path.pdf = 0.f;
+                    path.normal = f3(0.f);
+                    path.origin = load3(s.camera.posW);
+                    path.dir = primaryDir;
+                    path.hit = primary;
+                    path.vertexIndex = 1;
+                    path.shadowPending = false;
+                    state = LS_SHADE;
+                    // The primary hit of the next sample is shaded on the next iteration.
+                    continue;
+                }
+                // ResolvePass (ResolvePass.cs.slang:80-101); 1 spp writes the colour directly.
+                const float3 out = spp == 1 ? color : color * (1.f / float(spp));
+                if (!isfinite(out.x) || !isfinite(out.y) || !isfinite(out.z)) atomicOr(s.errorWord, FPT_DEVERR_NAN);
+                p.color[idx] = make_float4(out.x, out.y, out.z, 1.f);
+                if (p.rayCount) p.rayCount[idx] = rays;
+                state = LS_FETCH;
+            }
         }
     }
     flush_counters(p.counters, cnt);
@@ -459,8 +307,14 @@ cudaError_t launch_path_tracer(const DevScene& s, const FrameParams& p, cudaStre
     cudaError_t e = cudaMemsetAsync(p.workCounter, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     const int blocks = path_tracer_grid_blocks(kPathBlock);
-    if (s.hasTransmission) path_tracer_kernel<TinyUniformSG, true><<<blocks, kPathBlock, 0, st>>>(s, p);
-    else path_tracer_kernel<TinyUniformSG, false><<<blocks, kPathBlock, 0, st>>>(s, p);
+    const bool uniform = p.sampleGenerator == 1;
+    if (s.hasTransmission) {
+        if (uniform) path_tracer_kernel<UniformSG, true><<<blocks, kPathBlock, 0, st>>>(s, p);
+        else path_tracer_kernel<TinyUniformSG, true><<<blocks, kPathBlock, 0, st>>>(s, p);
+    } else {
+        if (uniform) path_tracer_kernel<UniformSG, false><<<blocks, kPathBlock, 0, st>>>(s, p);
+        else path_tracer_kernel<TinyUniformSG, false><<<blocks, kPathBlock, 0, st>>>(s, p);
+    }
     return cudaGetLastError();
 }
 

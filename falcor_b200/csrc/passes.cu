@@ -86,6 +86,10 @@ void set_defaults(fpt_pass& p) {
         d["outputSize"] = PropValue::str("Default");
         d["colorFormat"] = PropValue::str("LogLuvHDR");
         d["diffuseBrdf"] = PropValue::str("Frostbite");
+        // Scheduling of this implementation (no reference counterpart):
+        // "Wavefront" (default) or "Megakernel"; paths in flight per wave.
+        d["scheduler"] = PropValue::str("Wavefront");
+        d["wavefrontCapacity"] = PropValue::num(1 << 23);
     } else if (p.type == "VBufferRT") {
         d["samplePattern"] = PropValue::str("Center");
         d["useAlphaTest"] = PropValue::num(1);
@@ -260,6 +264,8 @@ FPT_API fpt_status fpt_pass_set_property_string(fpt_pass* pass, const char* key,
     if (m && m->find(v) == m->end()) return set_error(FPT_ERR_INVALID_ARG, "invalid value '" + v + "' for property '" + k + "'");
     if (k == "diffuseBrdf" && v != "Frostbite" && v != "Lambert")
         return set_error(FPT_ERR_INVALID_ARG, "diffuseBrdf must be 'Frostbite' or 'Lambert'");
+    if (k == "scheduler" && v != "Wavefront" && v != "Megakernel")
+        return set_error(FPT_ERR_INVALID_ARG, "scheduler must be 'Wavefront' or 'Megakernel'");
     it->second.s = v;
     return FPT_OK;
 }
@@ -363,8 +369,18 @@ FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void
     } else if (pass->type == "PathTracer") {
         if (!io->vbuffer || !io->color) return set_error(FPT_ERR_INVALID_ARG, "PathTracer: 'vbuffer' and 'color' are required");
         path_tracer_params(*pass, fp);
-        pass->launches = 2;
-        e = launch_path_tracer(ds, fp, st);
+        if (pass->str("scheduler") == "Megakernel") {
+            pass->launches = 2;
+            e = launch_path_tracer(ds, fp, st);
+        } else {
+            const uint32_t cap = uint32_t(std::max(1.0, pass->num("wavefrontCapacity")));
+            e = pass->wavefront.ensure(std::max<uint32_t>(cap, fp.spp));
+            if (e != cudaSuccess) return set_error(FPT_ERR_OOM, std::string("PathTracer: wavefront buffers: ") + cudaGetErrorString(e));
+            e = launch_path_tracer_wavefront(ds, fp, pass->wavefront, st);
+            const uint32_t wavePixels = std::max<uint32_t>(1, std::min<uint32_t>(fp.width * fp.height, pass->wavefront.capacity / fp.spp));
+            const uint32_t waves = (fp.width * fp.height + wavePixels - 1) / wavePixels;
+            pass->launches = waves * (4 * (fp.maxSurfaceBounces + 2) + 3);
+        }
         pass->frameCount++;
     } else {
         return wardiff_execute(*pass, io, nullptr, nullptr, st);

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "common.h"
+#include "wavefront.h"
 
 namespace fpt {
 
@@ -31,6 +32,7 @@ struct fpt_pass {
     bool useFixedSeed = false;
     bool warnedLightBVH = false;
     uint32_t launches = 0;
+    fpt::WavefrontBuffers wavefront;  // path state of the wavefront scheduler
 
     double num(const std::string& k) const;
     std::string str(const std::string& k) const;

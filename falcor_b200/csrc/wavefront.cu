@@ -1,0 +1,359 @@
+// wavefront.cu -- wavefront PathTracer for sm_100a.
+//
+// The frame's (pixel, sample) paths are processed in waves of up to
+// `capacity` paths whose state lives in structure-of-arrays buffers.  Each
+// bounce runs three small kernels over compacted queues of path indices:
+//   shade   handleHit / handleMiss (PathTracer.slang:821-1157): emission with
+//           MIS, NEE light sample, BSDF sample; pushes the visibility ray to
+//           the shadow queue and the continuing path to the extension queue
+//   shadow  any-hit traversal of the NEE rays; adds thp * Lr when visible
+//   extend  closest-hit traversal of the continuing paths
+// Queue pushes are warp-aggregated (ballot + one atomic per warp), so every
+// kernel runs on dense, converged warps.  A resolve kernel sums the samples
+// of each pixel in sample order with the per-sample colour format
+// (ResolvePass.cs.slang:80-101), and a generate kernel seeds the wave
+// (PathTracer.slang:273-301, GeneratePaths.cs.slang:93-256).
+#include <algorithm>
+
+#include "kernels.cuh"
+#include "path_logic.cuh"
+#include "wavefront.h"
+
+namespace fpt {
+
+using namespace dev;
+
+namespace {
+
+constexpr int kTraceBlock = 128;
+constexpr int kShadeBlock = 128;
+
+// Counts: [0] shade queue, [1] extension queue, [2] shadow queue.
+struct WaveParams {
+    uint32_t waveFirstPixel;   // first pixel of the wave
+    uint32_t wavePixels;       // pixels in the wave
+    uint32_t wavePaths;        // wavePixels * spp
+    uint32_t* counts;
+    const uint32_t* shadeQueue;
+    uint32_t* extQueue;
+    uint32_t* shadowQueue;
+};
+
+struct SoA {
+    float4* originPdf;    // origin.xyz, pdf
+    float4* dirV;         // dir.xyz, flags | vertexIndex << 16 (bits)
+    float4* thpB;         // thp.xyz, bounce counters (bits)
+    float4* L;            // L.xyz, -
+    uint4* sg;            // sample generator state
+    uint4* hit;           // instanceID, primIndex, baryX, baryY
+    float4* sOrigin;      // shadow origin, distance
+    float4* sDir;         // shadow direction, -
+    float4* sLr;          // shadow contribution thp * Lr
+    float* sampleL;       // per-path radiance (3 floats), wave slot order
+};
+
+template <class SG> FPT_D void store_sg(uint4& o, const SG& g);
+template <class SG> FPT_D void load_sg(const uint4& i, SG& g);
+template <> FPT_D void store_sg<TinyUniformSG>(uint4& o, const TinyUniformSG& g) { o = make_uint4(g.state, 0, 0, 0); }
+template <> FPT_D void load_sg<TinyUniformSG>(const uint4& i, TinyUniformSG& g) { g.state = i.x; }
+template <> FPT_D void store_sg<UniformSG>(uint4& o, const UniformSG& g) { o = make_uint4(g.s0, g.s1, g.s2, g.s3); }
+template <> FPT_D void load_sg<UniformSG>(const uint4& i, UniformSG& g) { g.s0 = i.x; g.s1 = i.y; g.s2 = i.z; g.s3 = i.w; }
+
+template <class SG>
+FPT_D void load_path(const SoA& w, uint32_t i, PathState<SG>& path) {
+    const float4 a = w.originPdf[i], b = w.dirV[i], c = w.thpB[i], d = w.L[i];
+    path.origin = make_float3(a.x, a.y, a.z);
+    path.pdf = a.w;
+    path.dir = make_float3(b.x, b.y, b.z);
+    const uint32_t fv = __float_as_uint(b.w);
+    path.flags = fv & 0xffffu;
+    path.vertexIndex = fv >> 16;
+    path.thp = make_float3(c.x, c.y, c.z);
+    path.bounces = __float_as_uint(c.w);
+    path.L = make_float3(d.x, d.y, d.z);
+    load_sg(w.sg[i], path.sg);
+    const uint4 h = w.hit[i];
+    path.hit.instanceID = h.x;
+    path.hit.primIndex = h.y;
+    path.hit.baryX = __uint_as_float(h.z);
+    path.hit.baryY = __uint_as_float(h.w);
+    path.hit.valid = true;
+    path.normal = f3(0.f);
+    path.shadowPending = false;
+}
+
+template <class SG>
+FPT_D void store_path(const SoA& w, uint32_t i, const PathState<SG>& path) {
+    w.originPdf[i] = make_float4(path.origin.x, path.origin.y, path.origin.z, path.pdf);
+    w.dirV[i] = make_float4(path.dir.x, path.dir.y, path.dir.z, __uint_as_float((path.flags & 0xffffu) | (path.vertexIndex << 16)));
+    w.thpB[i] = make_float4(path.thp.x, path.thp.y, path.thp.z, __uint_as_float(path.bounces));
+    w.L[i] = make_float4(path.L.x, path.L.y, path.L.z, 0.f);
+    store_sg(w.sg[i], path.sg);
+}
+
+// Warp-aggregated push of `item` onto queue q (count at *cnt).
+FPT_D void push(bool pred, uint32_t item, uint32_t* q, uint32_t* cnt) {
+    const uint32_t mask = __ballot_sync(__activemask(), pred);
+    if (mask == 0) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (int(lane) == leader) base = atomicAdd(cnt, uint32_t(__popc(mask)));
+    base = __shfl_sync(__activemask(), base, leader);
+    if (pred) q[base + uint32_t(__popc(mask & ((1u << lane) - 1u)))] = item;
+}
+
+// Seeds a wave: slot i <-> (pixel waveFirstPixel + i % wavePixels, sample i / wavePixels).
+// Background pixels write their samples directly; hit pixels enter the shade queue.
+template <class SG>
+__global__ void __launch_bounds__(kShadeBlock) wf_generate(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    Counters cnt;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i - threadIdx.x < wp.wavePaths; i += gridDim.x * blockDim.x) {
+        bool enqueue = false;
+        if (i < wp.wavePaths) {
+            const uint32_t pixIn = i % wp.wavePixels, sample = i / wp.wavePixels;
+            const uint32_t pix = wp.waveFirstPixel + pixIn;
+            const uint32_t x = pix % p.width, y = pix / p.width;
+            float tMin, tMax;
+            const float3 dir = camera_ray_dir(s.camera, x, y, p.width, p.height, tMin, tMax);
+            HitRec hit;
+            if (unpack_hit(s.bits, __ldg(p.vbuffer + pix), hit)) {
+                PathState<SG> path;
+                path.sg.init(x, y, p.seed * p.spp + sample);
+                path.flags = PF_ACTIVE | 0x2u;  // active, hit (primary hit from the V-buffer)
+                path.vertexIndex = 1;
+                path.bounces = 0;
+                path.thp = f3(1.f);
+                path.L = f3(0.f);
+                path.pdf = 0.f;
+                path.origin = load3(s.camera.posW);
+                path.dir = dir;
+                store_path(w, i, path);
+                w.hit[i] = make_uint4(hit.instanceID, hit.primIndex, __float_as_uint(hit.baryX), __float_as_uint(hit.baryY));
+                enqueue = true;
+            } else {
+                const float3 bg = s.hasEnv ? env_eval(s, dir) : f3(0.f);
+                if (s.hasEnv) cnt.v[9]++;
+                float* o = w.sampleL + size_t(i) * 3;
+                o[0] = bg.x; o[1] = bg.y; o[2] = bg.z;
+            }
+        }
+        push(enqueue, i, const_cast<uint32_t*>(wp.shadeQueue), wp.counts + 0);
+    }
+    flush_counters(p.counters, cnt);
+}
+
+// handleHit / handleMiss for every path of the shade queue.  The hit flag of
+// a path is PF_HIT (0x2) in its flags.
+template <class SG, bool HAS_T>
+__global__ void __launch_bounds__(kShadeBlock) wf_shade(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    Counters cnt;
+    const uint32_t n = wp.counts[0];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k - threadIdx.x < n; k += gridDim.x * blockDim.x) {
+        bool ext = false, shadow = false;
+        uint32_t i = 0;
+        if (k < n) {
+            i = wp.shadeQueue[k];
+            PathState<SG> path;
+            load_path(w, i, path);
+            if (path.flags & 0x2u) pt_handle_hit<SG, HAS_T>(s, p, path, cnt);
+            else pt_handle_miss<SG>(s, p, path, cnt);
+            shadow = path.shadowPending;
+            if (shadow) {
+                w.sOrigin[i] = make_float4(path.sOrigin.x, path.sOrigin.y, path.sOrigin.z, path.sDist);
+                w.sDir[i] = make_float4(path.sDir.x, path.sDir.y, path.sDir.z, 0.f);
+                w.sLr[i] = make_float4(path.sLr.x, path.sLr.y, path.sLr.z, 0.f);
+            }
+            ext = path.has(PF_ACTIVE);
+            store_path(w, i, path);
+            if (!ext) cnt.v[0]++;
+        }
+        push(shadow, i, wp.shadowQueue, wp.counts + 2);
+        push(ext, i, wp.extQueue, wp.counts + 1);
+    }
+    flush_counters(p.counters, cnt);
+}
+
+// Visibility rays: L += thp * Lr when unoccluded.
+__global__ void __launch_bounds__(kTraceBlock) wf_shadow(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    __shared__ uint2 stackMem[kStackSize * kTraceBlock];
+    uint2* stack = stackMem + threadIdx.x;
+    Counters cnt;
+    const uint32_t n = wp.counts[2];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = wp.shadowQueue[k];
+        const float4 o = w.sOrigin[i], d = w.sDir[i];
+        HitRec h;
+        TraceStats ts;
+        trace_bvh<true>(s, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), 0.f, o.w, h, stack, kTraceBlock, &ts);
+        cnt.trace(true, ts);
+        if (!h.valid) {
+            const float4 lr = w.sLr[i];
+            float4 L = w.L[i];
+            L.x += lr.x; L.y += lr.y; L.z += lr.z;
+            w.L[i] = L;
+        }
+    }
+    flush_counters(p.counters, cnt);
+}
+
+// Extension rays: closest hit; the path re-enters the shade queue.
+__global__ void __launch_bounds__(kTraceBlock) wf_extend(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    __shared__ uint2 stackMem[kStackSize * kTraceBlock];
+    uint2* stack = stackMem + threadIdx.x;
+    Counters cnt;
+    const uint32_t n = wp.counts[1];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = wp.extQueue[k];
+        const float4 o = w.originPdf[i], d = w.dirV[i];
+        HitRec h;
+        TraceStats ts;
+        trace_bvh<false>(s, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), 0.f, 1e30f, h, stack, kTraceBlock, &ts);
+        cnt.trace(false, ts);
+        uint32_t fv = __float_as_uint(d.w);
+        fv += 1u << 16;  // vertexIndex++
+        if (h.valid) {
+            fv |= 0x2u;
+            w.hit[i] = make_uint4(h.instanceID, h.primIndex, __float_as_uint(h.baryX), __float_as_uint(h.baryY));
+        } else {
+            fv &= ~0x2u;
+        }
+        w.dirV[i] = make_float4(d.x, d.y, d.z, __uint_as_float(fv));
+    }
+    flush_counters(p.counters, cnt);
+}
+
+// Finished paths keep their radiance in L; copy it into the per-sample buffer.
+__global__ void wf_collect(FrameParams p, WaveParams wp, SoA w, const uint32_t* hitPixelFlags) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePaths; i += gridDim.x * blockDim.x) {
+        const uint32_t pix = wp.waveFirstPixel + i % wp.wavePixels;
+        if (!(__ldg(p.vbuffer + pix).x)) continue;  // background: written by wf_generate
+        const float4 L = w.L[i];
+        float* o = w.sampleL + size_t(i) * 3;
+        o[0] = L.x; o[1] = L.y; o[2] = L.z;
+    }
+}
+
+// ResolvePass: per-pixel average of the per-sample colours in sample order.
+__global__ void wf_resolve(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < wp.wavePixels; j += gridDim.x * blockDim.x) {
+        const uint32_t pix = wp.waveFirstPixel + j;
+        float3 c = f3(0.f);
+        for (uint32_t smp = 0; smp < p.spp; smp++) {
+            const float* q = w.sampleL + (size_t(smp) * wp.wavePixels + j) * 3;
+            const float3 L = make_float3(q[0], q[1], q[2]);
+            if (p.sampleColor) {
+                float* o = p.sampleColor + (size_t(pix) * p.spp + smp) * 3;
+                o[0] = L.x; o[1] = L.y; o[2] = L.z;
+            }
+            c += (p.spp != 1 && p.colorFormat == 1) ? decode_logluv_hdr(encode_logluv_hdr(L)) : L;
+        }
+        const float3 out = p.spp == 1 ? c : c * (1.f / float(p.spp));
+        if (!isfinite(out.x) || !isfinite(out.y) || !isfinite(out.z)) atomicOr(s.errorWord, FPT_DEVERR_NAN);
+        p.color[pix] = make_float4(out.x, out.y, out.z, 1.f);
+    }
+}
+
+// Moves the extension queue into the shade queue for the next bounce.
+__global__ void wf_advance(WaveParams wp) {
+    wp.counts[0] = wp.counts[1];
+    wp.counts[1] = 0;
+    wp.counts[2] = 0;
+}
+
+int blocks_for(const void* kernel, int block) {
+    int perSM = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, block, 0);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(1, perSM) * sms;
+}
+
+template <class SG, bool HAS_T>
+cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st) {
+    SoA w;
+    w.originPdf = b.f4(0); w.dirV = b.f4(1); w.thpB = b.f4(2); w.L = b.f4(3);
+    w.sg = reinterpret_cast<uint4*>(b.f4(4)); w.hit = reinterpret_cast<uint4*>(b.f4(5));
+    w.sOrigin = b.f4(6); w.sDir = b.f4(7); w.sLr = b.f4(8);
+    w.sampleL = b.sampleL;
+    const uint32_t pixels = p.width * p.height;
+    const uint32_t wavePixels = std::max<uint32_t>(1, std::min<uint32_t>(pixels, b.capacity / p.spp));
+    static int gShade = 0, gTrace = 0, gGen = 0;
+    if (!gShade) {
+        gShade = blocks_for(reinterpret_cast<const void*>(wf_shade<SG, HAS_T>), kShadeBlock);
+        gTrace = blocks_for(reinterpret_cast<const void*>(wf_extend), kTraceBlock);
+        gGen = blocks_for(reinterpret_cast<const void*>(wf_generate<SG>), kShadeBlock);
+    }
+    const uint32_t maxIter = p.maxSurfaceBounces + 2;
+    for (uint32_t first = 0; first < pixels; first += wavePixels) {
+        WaveParams wp;
+        wp.waveFirstPixel = first;
+        wp.wavePixels = std::min(wavePixels, pixels - first);
+        wp.wavePaths = wp.wavePixels * p.spp;
+        wp.counts = b.counts;
+        cudaError_t e = cudaMemsetAsync(b.counts, 0, 4 * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return e;
+        uint32_t* qa = b.queueA;
+        uint32_t* qb = b.queueB;
+        wp.shadeQueue = qa;
+        wp.extQueue = qb;
+        wp.shadowQueue = b.shadowQueue;
+        const int genBlocks = std::min<int>(gGen, int((wp.wavePaths + kShadeBlock - 1) / kShadeBlock));
+        wf_generate<SG><<<genBlocks, kShadeBlock, 0, st>>>(s, p, wp, w);
+        for (uint32_t it = 0; it < maxIter; it++) {
+            wf_shade<SG, HAS_T><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
+            wf_shadow<<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
+            wf_extend<<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
+            wf_advance<<<1, 1, 0, st>>>(wp);
+            std::swap(qa, qb);
+            wp.shadeQueue = qa;
+            wp.extQueue = qb;
+        }
+        wf_collect<<<gGen, 256, 0, st>>>(p, wp, w, nullptr);
+        wf_resolve<<<(wp.wavePixels + 255) / 256, 256, 0, st>>>(s, p, wp, w);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t WavefrontBuffers::ensure(uint32_t cap) {
+    if (capacity >= cap && base) return cudaSuccess;
+    release();
+    const size_t f4Bytes = size_t(cap) * sizeof(float4);
+    const size_t bytes = kFloat4Arrays * f4Bytes + size_t(cap) * 3 * sizeof(float) + 3 * size_t(cap) * sizeof(uint32_t) + 256;
+    cudaError_t e = cudaMalloc(&base, bytes);
+    if (e != cudaSuccess) { base = nullptr; return e; }
+    capacity = cap;
+    char* q = static_cast<char*>(base);
+    arrays = reinterpret_cast<float4*>(q);
+    q += kFloat4Arrays * f4Bytes;
+    sampleL = reinterpret_cast<float*>(q);
+    q += size_t(cap) * 3 * sizeof(float);
+    queueA = reinterpret_cast<uint32_t*>(q);
+    q += size_t(cap) * sizeof(uint32_t);
+    queueB = reinterpret_cast<uint32_t*>(q);
+    q += size_t(cap) * sizeof(uint32_t);
+    shadowQueue = reinterpret_cast<uint32_t*>(q);
+    q += size_t(cap) * sizeof(uint32_t);
+    counts = reinterpret_cast<uint32_t*>(q);
+    bytesAllocated = bytes;
+    return cudaSuccess;
+}
+
+void WavefrontBuffers::release() {
+    if (base) cudaFree(base);
+    base = nullptr;
+    capacity = 0;
+}
+
+cudaError_t launch_path_tracer_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st) {
+    const bool uniform = p.sampleGenerator == 1;
+    if (s.hasTransmission) return uniform ? run_wavefront<UniformSG, true>(s, p, b, st) : run_wavefront<TinyUniformSG, true>(s, p, b, st);
+    return uniform ? run_wavefront<UniformSG, false>(s, p, b, st) : run_wavefront<TinyUniformSG, false>(s, p, b, st);
+}
+
+}  // namespace fpt

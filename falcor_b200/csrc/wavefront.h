@@ -1,0 +1,31 @@
+// wavefront.h -- path-state buffers and launcher of the wavefront PathTracer.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace fpt {
+
+// Structure-of-arrays path state for `capacity` paths in flight, allocated
+// once per pass and reused by every frame (scratch owned by the pass).
+struct WavefrontBuffers {
+    static constexpr int kFloat4Arrays = 9;
+    void* base = nullptr;
+    uint32_t capacity = 0;
+    size_t bytesAllocated = 0;
+    float4* arrays = nullptr;      // kFloat4Arrays x capacity float4
+    float* sampleL = nullptr;      // 3 floats per path
+    uint32_t* queueA = nullptr;
+    uint32_t* queueB = nullptr;
+    uint32_t* shadowQueue = nullptr;
+    uint32_t* counts = nullptr;    // [0] shade, [1] extension, [2] shadow
+    float4* f4(int k) const { return arrays + size_t(k) * capacity; }
+    cudaError_t ensure(uint32_t capacity);
+    void release();
+    ~WavefrontBuffers() { release(); }
+};
+
+cudaError_t launch_path_tracer_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st);
+
+}  // namespace fpt
