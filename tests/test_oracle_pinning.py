@@ -1,0 +1,84 @@
+"""The oracle is pinned against the reference's own known-answer tests.
+
+oracle/_ref/kat_runner is built (by __graft_entry__.build() or
+`make -f ref.mk` in oracle/) from the reference's unit-test sources
+(Tests/Sampling/PseudorandomTests.cpp, Tests/Utils/HashUtilsTests.cpp,
+Tests/Utils/BitTricksTests.cpp, Tests/Utils/GeometryHelpersTests.cpp) and the
+reference's Utils/Math/Float16.cpp; the tests' Slang programs are replaced by
+the oracle, so the reference's own EXPECT_EQ checks judge the oracle.
+"""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+RUNNER = ROOT / "oracle" / "_ref" / "kat_runner"
+REF = Path("/root/reference/Source")
+
+
+def _runner():
+    if not RUNNER.exists():
+        if not REF.exists():
+            pytest.skip("reference sources absent and kat_runner not built")
+        subprocess.run(["make", "-s", "-f", "ref.mk"], cwd=ROOT / "oracle", check=True)
+    return RUNNER
+
+
+def test_reference_known_answer_tests_pass_against_oracle():
+    out = subprocess.run([str(_runner())], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    lines = {l.split()[1]: l.split()[0] for l in out.stdout.splitlines() if l[:4] in ("PASS", "FAIL", "SKIP")}
+    for name in ("XoshiroPRNG", "SplitMixPRNG", "LCGPRNG", "JenkinsHash_CompareToCPU", "BitInterleave",
+                 "ComputeRayOrigin", "Float16Conversions"):
+        assert lines.get(name) == "PASS", (name, out.stdout)
+
+
+def test_sample_generator_streams(oracle):
+    """UniformSampleGenerator / TinyUniformSampleGenerator seeding restated in numpy
+    from UniformSampleGenerator.slang:53-71 and TinyUniformSampleGenerator.slang:58-63."""
+    import ctypes as C
+    lib = oracle.lib()
+    n, dims = 64, 8
+    rng = np.random.default_rng(0)
+    px = rng.integers(0, 4096, n, dtype=np.uint32)
+    py = rng.integers(0, 4096, n, dtype=np.uint32)
+    sn = rng.integers(0, 1 << 20, n, dtype=np.uint32)
+    out = np.zeros((n, dims), dtype=np.uint32)
+    lib.orc_sample_generator(1, oracle.ptr(px), oracle.ptr(py), oracle.ptr(sn), n, dims, oracle.ptr(out))
+
+    def interleave(x, y):
+        r = 0
+        for i in range(16):
+            r |= ((int(x) >> i) & 1) << (2 * i)
+            r |= ((int(y) >> i) & 1) << (2 * i + 1)
+        return r
+    M64 = (1 << 64) - 1
+    for k in range(n):
+        st = (int(sn[k]) << 32) | interleave(px[k], py[k])
+        vals = []
+        for _ in range(2):
+            st = (st + 0x9E3779B97F4A7C15) & M64
+            z = st
+            z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
+            z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
+            vals.append(z ^ (z >> 31))
+        s = [vals[0] & 0xffffffff, vals[0] >> 32, vals[1] & 0xffffffff, vals[1] >> 32]
+        rot = lambda x, r: ((x << r) | (x >> (32 - r))) & 0xffffffff
+        for j in range(dims):
+            res = (rot((s[0] * 5) & 0xffffffff, 7) * 9) & 0xffffffff
+            t = (s[1] << 9) & 0xffffffff
+            s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3]; s[2] ^= t; s[3] = rot(s[3], 11)
+            assert out[k, j] == res
+    lib.orc_sample_generator(0, oracle.ptr(px), oracle.ptr(py), oracle.ptr(sn), n, dims, oracle.ptr(out))
+    for k in range(n):
+        v0, v1, sm = interleave(px[k], py[k]), int(sn[k]), 0
+        for _ in range(16):
+            sm = (sm + 0x9e3779b9) & 0xffffffff
+            v0 = (v0 + ((((v1 << 4) + 0xa341316c) ^ (v1 + sm) ^ ((v1 >> 5) + 0xc8013ea4)) & 0xffffffff)) & 0xffffffff
+            v1 = (v1 + ((((v0 << 4) + 0xad90777d) ^ (v0 + sm) ^ ((v0 >> 5) + 0x7e95761e)) & 0xffffffff)) & 0xffffffff
+        st = v0
+        for j in range(dims):
+            st = (1664525 * st + 1013904223) & 0xffffffff
+            assert out[k, j] == st
