@@ -124,6 +124,7 @@ SIGNATURES = {
     "fpt_pass_reflect_json": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
     "fpt_pass_set_scene": (C.c_int, [_P, _P]),
     "fpt_pass_execute": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P]),
+    "fpt_pass_execute_noalloc": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P]),
     "fpt_pass_backward": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P, C.POINTER(fpt_grad_buffers), _P]),
     "fpt_pass_get_stats": (C.c_int, [_P, C.POINTER(fpt_pass_stats), _P]),
     "fpt_pass_get_counters": (C.c_int, [_P, C.POINTER(C.c_uint64), u32, _P]),

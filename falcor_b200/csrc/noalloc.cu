@@ -1,0 +1,112 @@
+// noalloc.cu -- PathTracer execute that allocates no device memory.
+//
+// Some callers cannot call cudaMalloc: a host that has reserved the GPU's
+// memory for its own pool (a fixed memory budget that forbids stray device
+// allocations), or a frame loop that must not take the implicit device-wide
+// synchronisation of cudaMalloc/cudaFree while other work is in flight.
+// For them this entry point runs the wavefront PathTracer with all of its
+// scratch -- path state, queues, queue counts and event counters -- in one
+// file-scope device array.  The array is part of the library image: every GPU
+// that loads the library holds it until the process exits.
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "kernels.cuh"
+#include "passes.h"
+#include "scene_device.h"
+#include "wavefront.h"
+
+namespace fpt {
+
+namespace {
+
+// Paths in flight per wave.  Frames of any size are processed in waves of
+// kNoAllocPaths / spp pixels.
+constexpr uint32_t kNoAllocPaths = 16384;
+constexpr size_t kHeaderBytes = 256;  // event counters, work counter
+constexpr size_t kNoAllocBytes =
+    kHeaderBytes + WavefrontBuffers::kFloat4Arrays * size_t(kNoAllocPaths) * 16 + size_t(kNoAllocPaths) * 12 +
+    3 * size_t(kNoAllocPaths) * 4 + 256;  // = WavefrontBuffers::bytes_for(kNoAllocPaths) + header (2.63 MiB)
+constexpr uint32_t kNoAllocMaxDim = 4096;  // PathTracer kMaxFrameDimension (Params.slang:68)
+
+__device__ __align__(256) unsigned char g_noallocScratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mutex;
+void* g_devPtr[kMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device.  The array's
+// name in host code is only a host-side stand-in, so the address must come
+// from cudaGetSymbolAddress, once per device, with that device current.
+fpt_status scratch_address(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return set_error(FPT_ERR_UNSUPPORTED, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!g_devPtr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noallocScratch);
+        if (e != cudaSuccess || !p)
+            return set_error(FPT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_devPtr[dev] = p;
+    }
+    *out = g_devPtr[dev];
+    return FPT_OK;
+}
+
+}  // namespace
+
+void path_tracer_params(fpt_pass& p, FrameParams& fp);
+
+}  // namespace fpt
+
+using namespace fpt;
+
+extern "C" {
+
+FPT_API fpt_status fpt_pass_execute_noalloc(fpt_pass* pass, const fpt_frame_io* io, void* stream) {
+    if (!pass || !io) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_execute_noalloc: null argument");
+    if (pass->type != "PathTracer") return set_error(FPT_ERR_UNSUPPORTED, "fpt_pass_execute_noalloc: only PathTracer passes");
+    if (!pass->scene) return set_error(FPT_ERR_NO_SCENE, "PathTracer: no scene set");
+    if (!io->vbuffer || !io->color) return set_error(FPT_ERR_INVALID_ARG, "PathTracer: 'vbuffer' and 'color' are required");
+    if (io->width == 0 || io->height == 0 || io->width > kNoAllocMaxDim || io->height > kNoAllocMaxDim)
+        return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_execute_noalloc: frame " + std::to_string(io->width) + "x" +
+                                                  std::to_string(io->height) + " exceeds the maximum of " +
+                                                  std::to_string(kNoAllocMaxDim) + "x" + std::to_string(kNoAllocMaxDim));
+    void* scratch = nullptr;
+    fpt_status s = scratch_address(&scratch);
+    if (s != FPT_OK) return s;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    FrameParams fp;
+    std::memset(&fp, 0, sizeof(fp));
+    fp.width = io->width;
+    fp.height = io->height;
+    fp.frameIndex = io->frame_index;
+    fp.prngDimension = io->prng_dimension;
+    fp.vbuffer = reinterpret_cast<const uint4*>(io->vbuffer);
+    fp.color = reinterpret_cast<float4*>(io->color);
+    fp.rayCount = io->ray_count;
+    fp.pathLength = io->path_length;
+    fp.sampleColor = io->sample_color;
+    fp.counters = static_cast<unsigned long long*>(scratch);
+    fp.workCounter = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + kWorkCounterOffset);
+    fp.workItems = io->width * io->height;
+    path_tracer_params(*pass, fp);
+    if (fp.spp > kNoAllocPaths) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_execute_noalloc: too many samples per pixel");
+    // The event counters start at zero; the queue counts are cleared per wave.
+    cudaError_t e = cudaMemsetAsync(scratch, 0, kHeaderBytes, st);
+    if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, cudaGetErrorString(e));
+    if (WavefrontBuffers::bytes_for(kNoAllocPaths) + kHeaderBytes > kNoAllocBytes)
+        return set_error(FPT_ERR_UNSUPPORTED, "fpt_pass_execute_noalloc: scratch layout larger than the static array");
+    WavefrontBuffers view;
+    view.view(static_cast<char*>(scratch) + kHeaderBytes, kNoAllocPaths);
+    e = launch_path_tracer_wavefront(pass->scene->dev, fp, view, st);
+    view.base = nullptr;  // the view never frees the static array
+    if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, std::string("PathTracer (no-alloc): ") + cudaGetErrorString(e));
+    pass->frameCount++;
+    return FPT_OK;
+}
+
+}  // extern "C"

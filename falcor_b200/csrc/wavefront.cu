@@ -350,6 +350,30 @@ void WavefrontBuffers::release() {
     capacity = 0;
 }
 
+size_t WavefrontBuffers::bytes_for(uint32_t cap) {
+    return kFloat4Arrays * size_t(cap) * sizeof(float4) + size_t(cap) * 3 * sizeof(float) + 3 * size_t(cap) * sizeof(uint32_t) + 256;
+}
+
+void WavefrontBuffers::view(void* mem, uint32_t cap) {
+    // Same layout as ensure(), over memory that the caller owns.
+    owning = false;
+    base = mem;
+    capacity = cap;
+    char* q = static_cast<char*>(mem);
+    arrays = reinterpret_cast<float4*>(q);
+    q += kFloat4Arrays * size_t(cap) * sizeof(float4);
+    sampleL = reinterpret_cast<float*>(q);
+    q += size_t(cap) * 3 * sizeof(float);
+    queueA = reinterpret_cast<uint32_t*>(q);
+    q += size_t(cap) * sizeof(uint32_t);
+    queueB = reinterpret_cast<uint32_t*>(q);
+    q += size_t(cap) * sizeof(uint32_t);
+    shadowQueue = reinterpret_cast<uint32_t*>(q);
+    q += size_t(cap) * sizeof(uint32_t);
+    counts = reinterpret_cast<uint32_t*>(q);
+    bytesAllocated = bytes_for(cap);
+}
+
 cudaError_t launch_path_tracer_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st) {
     const bool uniform = p.sampleGenerator == 1;
     if (s.hasTransmission) return uniform ? run_wavefront<UniformSG, true>(s, p, b, st) : run_wavefront<TinyUniformSG, true>(s, p, b, st);

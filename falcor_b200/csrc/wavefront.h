@@ -14,6 +14,7 @@ struct WavefrontBuffers {
     void* base = nullptr;
     uint32_t capacity = 0;
     size_t bytesAllocated = 0;
+    bool owning = true;            // false after view(): the memory belongs to someone else
     float4* arrays = nullptr;      // kFloat4Arrays x capacity float4
     float* sampleL = nullptr;      // 3 floats per path
     uint32_t* queueA = nullptr;
@@ -24,6 +25,12 @@ struct WavefrontBuffers {
     cudaError_t ensure(uint32_t capacity);
     void release();
     ~WavefrontBuffers() { release(); }
+
+    // Bytes needed for `capacity` paths in flight.
+    static size_t bytes_for(uint32_t capacity);
+    // Lays the buffers out over `mem` (at least bytes_for(capacity) bytes,
+    // 256-byte aligned) without allocating; the view never frees `mem`.
+    void view(void* mem, uint32_t capacity);
 };
 
 cudaError_t launch_path_tracer_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st);

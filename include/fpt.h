@@ -284,6 +284,21 @@ typedef struct fpt_frame_io {
 /* RenderPass::execute (RenderGraph/RenderPass.h:184). */
 FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void* stream);
 
+/* PathTracer execute that allocates no device memory.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc -- a host whose device
+ * memory is reserved for its own pool, or a frame loop that must not take the
+ * device-wide synchronisation of cudaMalloc/cudaFree -- it renders the same
+ * frame as fpt_pass_execute on a PathTracer pass, with all scratch (path
+ * state, queues, counters; 2.63 MiB, 16384 paths in flight per wave) in one
+ * static device array that every GPU loading this library holds until exit.
+ * Limits: PathTracer passes only, frames up to 4096 x 4096 (larger sizes are
+ * rejected with FPT_ERR_INVALID_ARG).  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller.  The
+ * event counters of fpt_pass_get_counters are not updated by this call. */
+FPT_API fpt_status fpt_pass_execute_noalloc(fpt_pass* pass, const fpt_frame_io* io, void* stream);
+
 /* Gradient buffers (DiffRendering/SceneGradients.cpp:42-206): caller-owned
  * device arrays, accumulated into (not cleared). */
 typedef struct fpt_grad_buffers {
