@@ -42,6 +42,8 @@ def parse_args():
     ap.add_argument("--workload", default="heightfield_soup_1080p")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the cpu_baseline sample")
+    ap.add_argument("--resolution", default=None, help="WxH override of the workload's frame size (small profiling cases)")
+    ap.add_argument("--frames-per-step", type=int, default=FRAMES_PER_STEP, help="16-spp frames per step")
     return ap.parse_args()
 
 
@@ -116,12 +118,25 @@ def algorithmic_bytes(c: dict, pixels: int) -> int:
             + 144 * c["env_samples"] + 48 * c["env_evals"] + 4 * c["env_pdfs"] + 32 * pixels)
 
 
-def load_traffic(workload: str):
-    """Per-launch DRAM bytes of the path-tracer kernel from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / f"path_tracer_kernel_{workload}.json"
+def category_bytes(c: dict, pixels: int) -> dict:
+    """Algorithmic bytes of one frame split by wavefront kernel category."""
+    ext_nodes = c["node_visits"] - c["shadow_node_visits"]
+    ext_tris = c["tri_tests"] - c["shadow_tri_tests"]
+    return {
+        "extend": 80 * ext_nodes + 48 * ext_tris,
+        "shadow": 80 * c["shadow_node_visits"] + 48 * c["shadow_tri_tests"],
+        "shade": 268 * c["hits"] + 76 * c["light_samples"] + 144 * c["env_samples"] + 48 * c["env_evals"] + 4 * c["env_pdfs"],
+        "resolve": 32 * pixels,
+    }
+
+
+def load_traffic(workload: str, kernel: str):
+    """Per-launch DRAM bytes (read + write) of a wavefront kernel, from the committed
+    ncu summary profiles/traffic_<workload>.json, if present."""
+    p = ROOT / "profiles" / f"traffic_{workload}.json"
     if p.exists():
         try:
-            return json.loads(p.read_text()).get("dram_bytes_per_launch")
+            return json.loads(p.read_text()).get(f"wf_{kernel}", {}).get("dram_bytes_per_launch")
         except (ValueError, OSError):
             return None
     return None
@@ -195,12 +210,16 @@ def main():
     from falcor_b200 import build
     build.build()
     from falcor_b200.scene import WORKLOADS, Scene, make_host_scene
+    from falcor_b200 import _ffi
     from falcor_b200.passes import PathTracer, VBufferRT
 
     w = WORKLOADS[args.workload]
     host = make_host_scene(w)
     scene = Scene(host)
     W, Hh = w.width, w.height
+    if args.resolution:
+        W, Hh = (int(x) for x in args.resolution.lower().split("x"))
+    frames = args.frames_per_step
     vb = VBufferRT()
     vb.set_scene(scene)
     pt = PathTracer({"samplesPerPixel": SPP_PER_FRAME, "maxSurfaceBounces": w.max_bounces,
@@ -213,34 +232,30 @@ def main():
     # L2 flush buffer (larger than the 126 MB L2), written between steps.
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream()
-    kernel_ms = []
 
     def step(timed_kernels: bool):
         vb.execute({"vbuffer": vbuf})
         accum.zero_()
-        for f in range(FRAMES_PER_STEP):
-            pt.set_properties({"fixedSeed": f})
-            if timed_kernels:
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
+        for f in range(frames):
+            # profileKernels: the library brackets each wavefront kernel launch
+            # with CUDA events on this stream (fpt_pass_get_kernel_times).
+            pt.set_properties({"fixedSeed": f, "profileKernels": int(timed_kernels)})
             pt.execute({"vbuffer": vbuf, "color": frame})
-            if timed_kernels:
-                e1.record(stream)
-                kernel_ms.append((e0, e1))
             accum.add_(frame)
-        accum.mul_(1.0 / FRAMES_PER_STEP)
+        accum.mul_(1.0 / frames)
 
     for _ in range(args.warmup):
         step(False)
         flush.fill_(1.0)
     torch.cuda.synchronize()
     counters = pt.counters()  # counts of the last PathTracer launch
-    paths_per_step = W * Hh * SPP_PER_FRAME * FRAMES_PER_STEP
+    paths_per_step = W * Hh * SPP_PER_FRAME * frames
 
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(local_rank)
+    pt.kernel_times(reset=True)
     clocks.start()
     total_ms = 0.0
     for _ in range(args.steps):
@@ -261,26 +276,33 @@ def main():
     ms_per_step = total_ms / args.steps
     value = paths_per_step * world / (ms_per_step / 1e3) / 1e6
 
-    kms = [a.elapsed_time(b) for a, b in kernel_ms]
-    k_avg_ms = sum(kms) / len(kms)
-    alg = algorithmic_bytes(counters, W * Hh)
+    ktimes = pt.kernel_times(reset=True)  # {category: (ms total, launches)} over the timed steps
+    frames_timed = args.steps * frames
+    cat_bytes = category_bytes(counters, W * Hh)
     hbm, peak_kind = peaks()
-    achieved = alg / (k_avg_ms / 1e3) / 1e9
-    rays_per_step = counters["rays"] * FRAMES_PER_STEP
+    dominant = max(("extend", "shadow", "shade"), key=lambda k: ktimes[k][0])
+    dom_ms, dom_launches = ktimes[dominant]
+    dom_bytes_per_launch = cat_bytes[dominant] * frames_timed / max(dom_launches, 1)
+    achieved = cat_bytes[dominant] * frames_timed / (dom_ms / 1e3) / 1e9
+    breakdown = {k: {"ms_per_frame": round(ktimes[k][0] / frames_timed, 3), "launches_per_frame": ktimes[k][1] / frames_timed,
+                     "algorithmic_GBps": round(cat_bytes[k] * frames_timed / max(ktimes[k][0], 1e-9) / 1e6, 2) if k in cat_bytes else None}
+                 for k in ktimes}
+    alg = algorithmic_bytes(counters, W * Hh)
+    rays_per_step = counters["rays"] * frames
 
-    # End to end through the public API: per step the camera is re-sent from host
-    # memory, the frame is rendered, and the resolved image is read back into pinned host memory.
+    # End to end through the public API: per step the host camera is handed to
+    # the scene (fpt_scene_set_camera; it reaches the device in the launch
+    # parameters), the frame is rendered, and the resolved image is read back
+    # into pinned host memory.
     host_img = torch.empty((Hh, W, 4), dtype=torch.float32, pin_memory=True)
-    cam = torch.tensor(list(host.camera_data().posW) + list(host.camera_data().cameraU) + list(host.camera_data().cameraV)
-                       + list(host.camera_data().cameraW) + [0.0, 0.0, 0.0, 0.0], dtype=torch.float32).pin_memory()
-    cam_dev = torch.empty_like(cam, device=dev)
+    cam = _ffi.fpt_camera.from_buffer_copy(host.desc.camera)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     e2e_steps = max(2, args.steps // 2)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        cam_dev.copy_(cam, non_blocking=True)
+        scene.set_camera(cam)
         step(False)
         host_img.copy_(accum, non_blocking=True)
         torch.cuda.synchronize()
@@ -297,19 +319,20 @@ def main():
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic procedural scene (seeded), no dataset",
-        "config": {"workload": w.name, "resolution": [W, Hh], "spp": SPP_PER_FRAME * FRAMES_PER_STEP,
-                   "frames_per_step": FRAMES_PER_STEP, "max_bounces": w.max_bounces,
+        "config": {"workload": w.name, "resolution": [W, Hh], "spp": SPP_PER_FRAME * frames,
+                   "frames_per_step": frames, "max_bounces": w.max_bounces,
                    "triangles": scene.info.triangle_count, "emissive_triangles": scene.info.emissive_triangle_count,
                    "bvh_nodes": scene.info.bvh_node_count, "bvh_build_s": round(scene.info.bvh_build_seconds, 3),
                    "parallelism": f"replicas x{world}", "l2_flush": "256 MB buffer written before every timed step"},
         "mrays_per_s": round(rays_per_step * world / (ms_per_step / 1e3) / 1e6, 3),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
-                     "frac": round(achieved / hbm, 4), "traffic": load_traffic(w.name), "peak_kind": peak_kind,
-                     "kernel": "path_tracer_kernel", "kernel_ms": round(k_avg_ms, 3),
-                     "algorithmic_bytes_per_launch": alg},
-        "e2e": {"value": round(e2e_value, 3), "unit": "Mpaths/s", "h2d_bytes_per_step": cam.numel() * 4,
+                     "frac": round(achieved / hbm, 4), "traffic": None if args.resolution else load_traffic(w.name, dominant), "peak_kind": peak_kind,
+                     "kernel": f"wf_{dominant}", "kernel_ms_per_launch": round(dom_ms / max(dom_launches, 1), 4),
+                     "algorithmic_bytes_per_launch": int(dom_bytes_per_launch),
+                     "frame_algorithmic_bytes": alg, "breakdown": breakdown},
+        "e2e": {"value": round(e2e_value, 3), "unit": "Mpaths/s", "h2d_bytes_per_step": C.sizeof(cam),
                 "d2h_bytes_per_step": host_img.numel() * 4},
-        "gpu_launches": args.steps * (1 + FRAMES_PER_STEP),
+        "gpu_launches": args.steps * (1 + frames * int(st.kernel_launches)),
         "clocks": clk,
         "counters_last_launch": counters,
         "device_error": st.device_error,

@@ -113,6 +113,7 @@ SIGNATURES = {
     "fpt_scene_create": (C.c_int, [C.POINTER(fpt_scene_desc), C.POINTER(_P)]),
     "fpt_scene_destroy": (None, [_P]),
     "fpt_scene_get_info": (C.c_int, [_P, C.POINTER(fpt_scene_info)]),
+    "fpt_scene_set_camera": (C.c_int, [_P, C.POINTER(fpt_camera)]),
     "fpt_scene_get_bvh": (C.c_int, [_P, C.POINTER(fpt_bvh_view)]),
     "fpt_scene_get_alias_table": (C.c_int, [_P, C.POINTER(u32), u32, C.POINTER(f32)]),
     "fpt_pass_create": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
@@ -128,6 +129,7 @@ SIGNATURES = {
     "fpt_pass_backward": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P, C.POINTER(fpt_grad_buffers), _P]),
     "fpt_pass_get_stats": (C.c_int, [_P, C.POINTER(fpt_pass_stats), _P]),
     "fpt_pass_get_counters": (C.c_int, [_P, C.POINTER(C.c_uint64), u32, _P]),
+    "fpt_pass_get_kernel_times": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_uint64), u32, C.c_int]),
     "fpt_batch_create": (C.c_int, [C.POINTER(_P)]),
     "fpt_batch_destroy": (None, [_P]),
     "fpt_batch_add": (C.c_int, [_P, C.POINTER(fpt_batch_request)]),
@@ -162,6 +164,18 @@ def lib() -> C.CDLL:
             fn.argtypes = args
         _lib = l
     return _lib
+
+
+def release(fn_name: str, handle) -> None:
+    """Frees a handle from a finaliser; a no-op once the library or the
+    interpreter is being torn down (module globals may already be None)."""
+    l = _lib
+    if l is None or handle is None:
+        return
+    try:
+        getattr(l, fn_name)(handle)
+    except Exception:
+        pass
 
 
 def check(status: int) -> None:

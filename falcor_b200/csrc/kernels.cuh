@@ -8,7 +8,7 @@
 
 namespace fpt {
 
-constexpr int kNumCounters = 11;       // see Counters in kernels.cu
+constexpr int kNumCounters = 13;       // see Counters in path_logic.cuh
 constexpr size_t kWorkCounterOffset = 128;  // byte offset of the work counter in the pass scratch
 constexpr size_t kScratchBytes = 256;
 

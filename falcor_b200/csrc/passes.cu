@@ -90,6 +90,8 @@ void set_defaults(fpt_pass& p) {
         // "Wavefront" (default) or "Megakernel"; paths in flight per wave.
         d["scheduler"] = PropValue::str("Wavefront");
         d["wavefrontCapacity"] = PropValue::num(1 << 23);
+        // CUDA-event timing of each wavefront kernel category (fpt_pass_get_kernel_times).
+        d["profileKernels"] = PropValue::num(0);
     } else if (p.type == "VBufferRT") {
         d["samplePattern"] = PropValue::str("Center");
         d["useAlphaTest"] = PropValue::num(1);
@@ -376,7 +378,8 @@ FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void
             const uint32_t cap = uint32_t(std::max(1.0, pass->num("wavefrontCapacity")));
             e = pass->wavefront.ensure(std::max<uint32_t>(cap, fp.spp));
             if (e != cudaSuccess) return set_error(FPT_ERR_OOM, std::string("PathTracer: wavefront buffers: ") + cudaGetErrorString(e));
-            e = launch_path_tracer_wavefront(ds, fp, pass->wavefront, st);
+            pass->timer.enabled = pass->num("profileKernels") != 0;
+            e = launch_path_tracer_wavefront(ds, fp, pass->wavefront, st, &pass->timer);
             const uint32_t wavePixels = std::max<uint32_t>(1, std::min<uint32_t>(fp.width * fp.height, pass->wavefront.capacity / fp.spp));
             const uint32_t waves = (fp.width * fp.height + wavePixels - 1) / wavePixels;
             pass->launches = waves * (4 * (fp.maxSurfaceBounces + 2) + 3);
@@ -415,6 +418,18 @@ FPT_API fpt_status fpt_pass_get_stats(fpt_pass* pass, fpt_pass_stats* out, void*
     out->device_error = err;
     out->kernel_launches = pass->launches;
     return err ? set_error(FPT_ERR_DEVICE, "device error word 0x" + std::to_string(err)) : FPT_OK;
+}
+
+FPT_API fpt_status fpt_pass_get_kernel_times(fpt_pass* pass, double* ms, uint64_t* launches, uint32_t count, int reset) {
+    if (!pass || !ms || !launches) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_get_kernel_times: null argument");
+    cudaError_t e = pass->timer.collect();
+    if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, cudaGetErrorString(e));
+    for (uint32_t i = 0; i < count; i++) {
+        ms[i] = i < uint32_t(KC_COUNT) ? pass->timer.ms[i] : 0.0;
+        launches[i] = i < uint32_t(KC_COUNT) ? pass->timer.launches[i] : 0;
+    }
+    if (reset) pass->timer.reset();
+    return FPT_OK;
 }
 
 FPT_API fpt_status fpt_pass_get_counters(fpt_pass* pass, uint64_t* out, uint32_t count, void* stream) {

@@ -33,6 +33,7 @@ struct fpt_pass {
     bool warnedLightBVH = false;
     uint32_t launches = 0;
     fpt::WavefrontBuffers wavefront;  // path state of the wavefront scheduler
+    fpt::KernelTimer timer;           // per-category kernel timing ("profileKernels")
 
     double num(const std::string& k) const;
     std::string str(const std::string& k) const;

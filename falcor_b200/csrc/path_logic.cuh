@@ -12,7 +12,8 @@ namespace dev {
 // counters once per thread: [0] paths, [1] rays, [2] closest-hit rays,
 // [3] visibility rays, [4] BVH node visits, [5] triangle tests, [6] shaded
 // hits, [7] emissive light samples, [8] env-map importance samples,
-// [9] env-map evaluations, [10] env-map pdf evaluations.
+// [9] env-map evaluations, [10] env-map pdf evaluations, [11] node visits and
+// [12] triangle tests of visibility rays (included in [4] and [5]).
 struct Counters {
     uint32_t v[kNumCounters] = {0};
     FPT_D void trace(bool shadow, const TraceStats& ts) {
@@ -20,6 +21,10 @@ struct Counters {
         v[shadow ? 3 : 2]++;
         v[4] += ts.nodes;
         v[5] += ts.tris;
+        if (shadow) {
+            v[11] += ts.nodes;
+            v[12] += ts.tris;
+        }
     }
 };
 

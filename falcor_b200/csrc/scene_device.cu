@@ -372,6 +372,13 @@ FPT_API fpt_status fpt_scene_get_info(const fpt_scene* scene, fpt_scene_info* ou
     return FPT_OK;
 }
 
+FPT_API fpt_status fpt_scene_set_camera(fpt_scene* scene, const fpt_camera* camera) {
+    if (!scene || !camera) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_camera: null argument");
+    compute_camera(*camera, scene->info.camera);
+    scene->dev.camera = scene->info.camera;
+    return FPT_OK;
+}
+
 FPT_API fpt_status fpt_scene_get_bvh(const fpt_scene* scene, fpt_bvh_view* out) {
     if (!scene || !out) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_get_bvh: null argument");
     out->nodes = scene->bvh.nodes.data();

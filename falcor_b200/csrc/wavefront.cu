@@ -271,7 +271,9 @@ int blocks_for(const void* kernel, int block) {
 }
 
 template <class SG, bool HAS_T>
-cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st) {
+cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st, KernelTimer* kt) {
+    auto T0 = [&](int cat) { if (kt && kt->enabled) kt->begin(cat, st); };
+    auto T1 = [&]() { if (kt && kt->enabled) kt->end(st); };
     SoA w;
     w.originPdf = b.f4(0); w.dirV = b.f4(1); w.thpB = b.f4(2); w.L = b.f4(3);
     w.sg = reinterpret_cast<uint4*>(b.f4(4)); w.hit = reinterpret_cast<uint4*>(b.f4(5));
@@ -300,18 +302,28 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
         wp.extQueue = qb;
         wp.shadowQueue = b.shadowQueue;
         const int genBlocks = std::min<int>(gGen, int((wp.wavePaths + kShadeBlock - 1) / kShadeBlock));
+        T0(KC_GENERATE);
         wf_generate<SG><<<genBlocks, kShadeBlock, 0, st>>>(s, p, wp, w);
+        T1();
         for (uint32_t it = 0; it < maxIter; it++) {
+            T0(KC_SHADE);
             wf_shade<SG, HAS_T><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
+            T1();
+            T0(KC_SHADOW);
             wf_shadow<<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
+            T1();
+            T0(KC_EXTEND);
             wf_extend<<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
+            T1();
             wf_advance<<<1, 1, 0, st>>>(wp);
             std::swap(qa, qb);
             wp.shadeQueue = qa;
             wp.extQueue = qb;
         }
+        T0(KC_RESOLVE);
         wf_collect<<<gGen, 256, 0, st>>>(p, wp, w, nullptr);
         wf_resolve<<<(wp.wavePixels + 255) / 256, 256, 0, st>>>(s, p, wp, w);
+        T1();
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -374,10 +386,57 @@ void WavefrontBuffers::view(void* mem, uint32_t cap) {
     bytesAllocated = bytes_for(cap);
 }
 
-cudaError_t launch_path_tracer_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st) {
+cudaError_t launch_path_tracer_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st,
+                                         KernelTimer* kt) {
     const bool uniform = p.sampleGenerator == 1;
-    if (s.hasTransmission) return uniform ? run_wavefront<UniformSG, true>(s, p, b, st) : run_wavefront<TinyUniformSG, true>(s, p, b, st);
-    return uniform ? run_wavefront<UniformSG, false>(s, p, b, st) : run_wavefront<TinyUniformSG, false>(s, p, b, st);
+    if (s.hasTransmission)
+        return uniform ? run_wavefront<UniformSG, true>(s, p, b, st, kt) : run_wavefront<TinyUniformSG, true>(s, p, b, st, kt);
+    return uniform ? run_wavefront<UniformSG, false>(s, p, b, st, kt) : run_wavefront<TinyUniformSG, false>(s, p, b, st, kt);
+}
+
+void KernelTimer::begin(int cat, cudaStream_t st) {
+    if (used + 2 > events.size()) {
+        const size_t grow = std::max<size_t>(64, events.size());
+        for (size_t i = 0; i < grow; i++) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) { enabled = false; return; }
+            events.push_back(e);
+        }
+    }
+    pendingCat.push_back(cat);
+    cudaEventRecord(events[used], st);
+}
+
+void KernelTimer::end(cudaStream_t st) {
+    if (!enabled || pendingCat.empty() || used + 1 >= events.size()) return;
+    cudaEventRecord(events[used + 1], st);
+    used += 2;
+}
+
+cudaError_t KernelTimer::collect() {
+    const size_t pairs = std::min(used / 2, pendingCat.size());
+    for (size_t k = 0; k < pairs; k++) {
+        cudaError_t e = cudaEventSynchronize(events[k * 2 + 1]);
+        if (e != cudaSuccess) return e;
+        float t = 0.f;
+        e = cudaEventElapsedTime(&t, events[k * 2], events[k * 2 + 1]);
+        if (e != cudaSuccess) return e;
+        ms[pendingCat[k]] += t;
+        launches[pendingCat[k]] += 1;
+    }
+    used = 0;
+    pendingCat.clear();
+    return cudaSuccess;
+}
+
+void KernelTimer::reset() {
+    used = 0;
+    pendingCat.clear();
+    for (int i = 0; i < KC_COUNT; i++) { ms[i] = 0; launches[i] = 0; }
+}
+
+KernelTimer::~KernelTimer() {
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
 }
 
 }  // namespace fpt

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "kernels.cuh"
 
 namespace fpt {
@@ -33,6 +35,27 @@ struct WavefrontBuffers {
     void view(void* mem, uint32_t capacity);
 };
 
-cudaError_t launch_path_tracer_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st);
+// Kernel categories timed by KernelTimer.
+enum KernelCategory { KC_GENERATE = 0, KC_SHADE = 1, KC_SHADOW = 2, KC_EXTEND = 3, KC_RESOLVE = 4, KC_COUNT = 5 };
+
+// Optional CUDA-event timing of each kernel launch, by category (the
+// equivalent of Falcor's FALCOR_PROFILE scopes, Utils/Timing/Profiler.h).
+struct KernelTimer {
+    bool enabled = false;
+    std::vector<cudaEvent_t> events;   // pool, reused
+    std::vector<int> pendingCat;       // category of each recorded pair
+    size_t used = 0;                   // events in use (pairs * 2)
+    double ms[KC_COUNT] = {0};
+    uint64_t launches[KC_COUNT] = {0};
+    void begin(int cat, cudaStream_t st);
+    void end(cudaStream_t st);
+    // Waits for the recorded events and folds them into ms/launches.
+    cudaError_t collect();
+    void reset();
+    ~KernelTimer();
+};
+
+cudaError_t launch_path_tracer_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st,
+                                         KernelTimer* timer = nullptr);
 
 }  // namespace fpt

@@ -59,7 +59,7 @@ class RenderPass:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().fpt_pass_destroy(self._h)
+            _ffi.release("fpt_pass_destroy", self._h)
             self._h = None
 
     @property
@@ -134,7 +134,16 @@ class RenderPass:
         return s
 
     COUNTER_NAMES = ("paths", "rays", "closest_rays", "shadow_rays", "node_visits", "tri_tests", "hits",
-                     "light_samples", "env_samples", "env_evals", "env_pdfs")
+                     "light_samples", "env_samples", "env_evals", "env_pdfs", "shadow_node_visits", "shadow_tri_tests")
+    KERNEL_CATEGORIES = ("generate", "shade", "shadow", "extend", "resolve")
+
+    def kernel_times(self, reset: bool = True) -> dict:
+        """GPU ms and launches per wavefront kernel category (needs profileKernels=1)."""
+        n = len(self.KERNEL_CATEGORIES)
+        ms = (C.c_double * n)()
+        la = (C.c_uint64 * n)()
+        check(lib().fpt_pass_get_kernel_times(self._h, ms, la, n, int(reset)))
+        return {k: (float(ms[i]), int(la[i])) for i, k in enumerate(self.KERNEL_CATEGORIES)}
 
     def counters(self) -> dict:
         """Event counters of the last execute (PixelStats equivalent)."""

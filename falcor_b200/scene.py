@@ -46,7 +46,7 @@ class HostScene:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().fpt_scene_host_free(self._h)
+            _ffi.release("fpt_scene_host_free", self._h)
             self._h = None
 
     # numpy views (valid while this object lives)
@@ -102,8 +102,13 @@ class Scene:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().fpt_scene_destroy(self._h)
+            _ffi.release("fpt_scene_destroy", self._h)
             self._h = None
+
+    def set_camera(self, camera: _ffi.fpt_camera) -> None:
+        """Replaces the camera for the next frames (fpt_scene_set_camera)."""
+        check(lib().fpt_scene_set_camera(self._h, C.byref(camera)))
+        check(lib().fpt_scene_get_info(self._h, C.byref(self.info)))
 
     def bvh(self) -> tuple[np.ndarray, np.ndarray]:
         """Host copies of the 8-wide BVH nodes (80 B each) and triangle records (48 B each)."""

@@ -231,6 +231,10 @@ typedef struct fpt_scene_info {
     fpt_camera_data camera;
 } fpt_scene_info;
 FPT_API fpt_status fpt_scene_get_info(const fpt_scene* scene, fpt_scene_info* out);
+/* Replaces the scene camera (Camera::setPosition/setTarget/setUpVector/
+ * setFocalLength, Scene/Camera/Camera.h:76-152, applied at the next frame).
+ * The camera travels to the device with the next launch's parameters. */
+FPT_API fpt_status fpt_scene_set_camera(fpt_scene* scene, const fpt_camera* camera);
 /* Host view of the scene's BVH (valid until the scene is destroyed). */
 FPT_API fpt_status fpt_scene_get_bvh(const fpt_scene* scene, fpt_bvh_view* out);
 /* Host copy of the emissive alias table (uint2 per emissive triangle) and
@@ -329,8 +333,15 @@ FPT_API fpt_status fpt_pass_get_stats(fpt_pass* pass, fpt_pass_stats* out, void*
  * rays, [3] visibility rays, [4] BVH node visits, [5] triangle tests,
  * [6] shaded hits, [7] emissive light samples, [8] env-map importance
  * samples, [9] env-map evaluations, [10] env-map pdf evaluations. */
-#define FPT_NUM_COUNTERS 11
+#define FPT_NUM_COUNTERS 13   /* [11] node visits and [12] triangle tests of visibility rays */
 FPT_API fpt_status fpt_pass_get_counters(fpt_pass* pass, uint64_t* out, uint32_t count, void* stream);
+
+/* GPU time per kernel category of the wavefront PathTracer, measured with CUDA
+ * events on the pass's stream when the pass property "profileKernels" is 1
+ * (the FALCOR_PROFILE scopes of Utils/Timing/Profiler.h:288-311):
+ * [0] generate, [1] shade, [2] visibility traversal, [3] extension traversal,
+ * [4] resolve.  Waits for the recorded events; `reset` clears the totals. */
+FPT_API fpt_status fpt_pass_get_kernel_times(fpt_pass* pass, double* ms, uint64_t* launches, uint32_t count, int reset);
 
 /* ------------------------------------------------------------------------ */
 /* Batched uneven forward: many render requests in one persistent launch    */
