@@ -144,7 +144,9 @@ def load_traffic(workload: str, kernel: str):
 
 def cpu_baseline(workload_name: str, seconds: float):
     """Times the CPU oracle (FP32 PathTracer restatement) on a crop of the workload
-    on all host cores.  Returns (Mpaths/s, cores, sample description)."""
+    on all host cores: a square crop at the frame centre (side <= 1024) rendered
+    at 16 spp for as many frames (seeds 0, 1, ...) as fill about `seconds`.
+    Returns (Mpaths/s, cores, sample description)."""
     import numpy as np
     from falcor_b200.scene import WORKLOADS, make_host_scene
     from oracle import ffi as orc
@@ -155,20 +157,26 @@ def cpu_baseline(workload_name: str, seconds: float):
     cores = os.cpu_count() or 1
     vb = osc.vbuffer(w.width, w.height, threads=cores)
     # Calibrate on a small crop, then size the sample to ~`seconds` of work.
-    cx, cy = w.width // 2 - 16, w.height // 2 - 16
+    cx, cy = w.width // 2 - 64, w.height // 2 - 64
     params = H.pt_params(w.width, w.height, SPP_PER_FRAME, seed=0, max_bounces=w.max_bounces, sampler=2, color_format=1)
-    _, _, cnt, dt = osc.path_tracer(vb, params, threads=cores, rect=(cx, cy, cx + 32, cy + 32))
+    _, _, cnt, dt = osc.path_tracer(vb, params, threads=cores, rect=(cx, cy, cx + 128, cy + 128))
     rate = max(cnt.paths, 1) / max(dt, 1e-6)
-    side = int(min(max(32, (rate * seconds / SPP_PER_FRAME) ** 0.5), 512))
+    target = rate * seconds
+    side = int(min(max(32, (target / SPP_PER_FRAME) ** 0.5), 1024, w.width, w.height))
     side -= side % 16
+    frames = max(1, int(round(target / (side * side * SPP_PER_FRAME))))
     x0, y0 = max(0, w.width // 2 - side // 2), max(0, w.height // 2 - side // 2)
-    _, _, cnt, dt = osc.path_tracer(vb, params, threads=cores, rect=(x0, y0, x0 + side, y0 + side))
     # Background pixels also count as paths in the workload's unit (they are written per sample).
     bg = int(np.sum(vb[y0:y0 + side, x0:x0 + side, 0] == 0)) * SPP_PER_FRAME
-    paths = cnt.paths + bg
-    desc = (f"{side}x{side} crop at the frame centre, {SPP_PER_FRAME} spp, {w.max_bounces} bounces, FP32 CPU oracle "
-            f"(-O3 -ffp-contract=off), {paths} paths in {dt:.2f} s")
-    return paths / dt / 1e6, cores, desc
+    paths, total = 0, 0.0
+    for f in range(frames):
+        params.seed = f
+        _, _, cnt, dt = osc.path_tracer(vb, params, threads=cores, rect=(x0, y0, x0 + side, y0 + side))
+        paths += cnt.paths + bg
+        total += dt
+    desc = (f"{side}x{side} crop at the frame centre, {frames} frame(s) of {SPP_PER_FRAME} spp, {w.max_bounces} bounces, "
+            f"FP32 CPU oracle (-O3 -ffp-contract=off), {paths} paths in {total:.2f} s")
+    return paths / total / 1e6, cores, desc
 
 
 def run_reference(args):

@@ -33,6 +33,7 @@ struct DevScene {
     fpt_hitinfo_bits bits;
     uint32_t hasEnv, hasEmissive, hasTransmission;
     uint32_t nodeCount, triCount;
+    uint32_t bvhDepth;                // levels of the 8-wide tree (root = 1)
     uint32_t* errorWord;              // device error word (FPT_DEVERR_*)
 };
 
@@ -98,162 +99,298 @@ FPT_D bool intersect_triangle(const RayShear& rs, float3 o, float3 v0, float3 v1
     return true;
 }
 
-// Conservative ray/box slab test: the computed entry/exit distances carry a
-// relative error of a few ulps, so the interval is widened by 2^-19 of its
-// magnitude before it is compared; no box that the ray touches is culled.
-FPT_D float widen_lo(float t) { return t - fabsf(t) * 1.9073486e-6f; }
-FPT_D float widen_hi(float t) { return t + fabsf(t) * 1.9073486e-6f; }
+// ---------------------------------------------------------------------------
+// Compressed 8-wide BVH traversal.
+//
+// Child boxes are stored as 8-bit offsets q from a per-node origin p with a
+// power-of-two scale s per axis; the builder guarantees that
+// fma(q, s, p) rounded to float encloses each child box.  The slab distance of
+// a plane is evaluated as one FMA, t = q * (s * inv) + (p - o) * inv, where
+// s * inv is exact (s is a power of two).  The rounding of p - o, of the
+// products and of the FMA, the rounding of the decoded plane and of 1/d are
+// each below 2^-24 of one of |p| * |inv|, |p - o| * |inv|, 255 s |inv| or |t|;
+// the entry and exit distances of every axis are therefore moved outward by
+// eps = 2^-18 (|p| + 2 |p - o| + 512 s) |inv| before the comparison, so no box
+// that the ray touches is culled.  (Scene coordinates are limited to
+// |x| <= 1e15 so that none of these terms overflows.)
+// ---------------------------------------------------------------------------
+struct TraceStats {
+    uint32_t nodes = 0, tris = 0;
+};
+
+// Per-ray constants of the traversal.
+struct TraceRay {
+    float3 o, d;
+    float ix, iy, iz;
+    uint32_t octinv;  // bit a set when d[a] < 0
+    float tMin;
+    RayShear rs;
+};
+
+FPT_D TraceRay make_trace_ray(float3 o, float3 d, float tMin) {
+    TraceRay r;
+    r.o = o;
+    r.d = d;
+    r.ix = 1.f / (fabsf(d.x) > 1e-20f ? d.x : copysignf(1e-20f, d.x));
+    r.iy = 1.f / (fabsf(d.y) > 1e-20f ? d.y : copysignf(1e-20f, d.y));
+    r.iz = 1.f / (fabsf(d.z) > 1e-20f ? d.z : copysignf(1e-20f, d.z));
+    r.octinv = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+    r.tMin = tMin;
+    r.rs = make_shear(d);
+    return r;
+}
+
+enum : uint32_t { kTraceRunning = 0, kTraceDone = 1, kTraceAnyHit = 2, kTraceError = 3 };
+constexpr uint32_t kTriGroupFlag = 0x80000000u;  // stack entry holds a triangle group
+
+// Resumable traversal state.  The current node group (gBase, gHits, gImask)
+// holds the not yet visited children of the last visited node, as bits in
+// octant order (bit i is child slot i ^ octinv); the triangle group
+// (tBase, tHits) holds the leaf triangles still to be tested.
+struct TraceState {
+    float tBest;
+    uint32_t bestTri, bestInst, bestPrim;
+    float bestU, bestV;
+    uint32_t gBase, gHits, gImask;
+    uint32_t tBase, tHits;
+    int sp;
+    uint32_t visits, triTests;
+    uint32_t status;
+};
+
+FPT_D void trace_init(const TraceRay& r, float tMax, TraceState& t) {
+    t.tBest = tMax;
+    t.bestTri = 0xffffffffu;
+    t.bestInst = t.bestPrim = 0;
+    t.bestU = t.bestV = 0.f;
+    // Pseudo group whose only member is the root (node 0 in slot 0).
+    t.gBase = 0;
+    t.gHits = 1u << r.octinv;
+    t.gImask = 1u;
+    t.tBase = t.tHits = 0;
+    t.sp = 0;
+    t.visits = t.triTests = 0;
+    t.status = kTraceRunning;
+}
+
+// Byte k (0..3) of w as an exact float: 0x4B0000qq is 2^23 + qq.
+FPT_D float quant_to_float(uint32_t w, uint32_t k) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | k)) - 8388608.f;
+}
+
+// Moves bit k of an 8-bit mask to bit k ^ o.
+FPT_D uint32_t octant_permute(uint32_t m, uint32_t o) {
+    if (o & 1u) m = ((m & 0x55u) << 1) | ((m >> 1) & 0x55u);
+    if (o & 2u) m = ((m & 0x33u) << 2) | ((m >> 2) & 0x33u);
+    if (o & 4u) m = ((m & 0x0fu) << 4) | ((m >> 4) & 0x0fu);
+    return m;
+}
+
+struct AxisPlanes {
+    uint32_t n0, n1, f0, f1;  // near / far quantised planes of slots 0-3, 4-7
+    float si, bn, bf;         // s * inv, (p - o) * inv - eps, (p - o) * inv + eps
+};
+
+FPT_D AxisPlanes axis_planes(float p, float s, float o, float inv, uint32_t lo0, uint32_t lo1, uint32_t hi0, uint32_t hi1,
+                             bool flip) {
+    AxisPlanes a;
+    a.n0 = flip ? hi0 : lo0;
+    a.n1 = flip ? hi1 : lo1;
+    a.f0 = flip ? lo0 : hi0;
+    a.f1 = flip ? lo1 : hi1;
+    const float base = p - o;
+    const float bi = base * inv;
+    const float eps = (fabsf(p) + 2.f * fabsf(base) + 512.f * s) * fabsf(inv) * 3.8146973e-6f;  // 2^-18
+    a.si = s * inv;
+    a.bn = bi - eps;
+    a.bf = bi + eps;
+    return a;
+}
+
+// Visits one node: tests its 8 child boxes against [tMin, tBest].  Returns
+// the hit internal children as a group (octant order) and the triangles of
+// the hit leaf children as a bit mask relative to the node's triangle base.
+FPT_D void visit_node(const DevScene& s, const TraceRay& r, float tBest, uint32_t nodeIdx, uint32_t& innerHits,
+                      uint32_t& childBase, uint32_t& imask, uint32_t& triBase, uint32_t& triHits) {
+    const uint4* np = s.nodes + size_t(nodeIdx) * 5;
+    const uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+    const uint32_t ew = w0.w;
+    const float sx = __uint_as_float((ew & 0xffu) << 23);
+    const float sy = __uint_as_float(((ew >> 8) & 0xffu) << 23);
+    const float sz = __uint_as_float(((ew >> 16) & 0xffu) << 23);
+    imask = ew >> 24;
+    childBase = w1.x;
+    triBase = w1.y;
+    // Quantised planes: lo x = w2.xy, lo y = w2.zw, lo z = w3.xy, hi x = w3.zw,
+    // hi y = w4.xy, hi z = w4.zw (slots 0-3 in the first word, 4-7 in the second).
+    const AxisPlanes X = axis_planes(__uint_as_float(w0.x), sx, r.o.x, r.ix, w2.x, w2.y, w3.z, w3.w, (r.octinv & 1u) != 0);
+    const AxisPlanes Y = axis_planes(__uint_as_float(w0.y), sy, r.o.y, r.iy, w2.z, w2.w, w4.x, w4.y, (r.octinv & 2u) != 0);
+    const AxisPlanes Z = axis_planes(__uint_as_float(w0.z), sz, r.o.z, r.iz, w3.x, w3.y, w4.z, w4.w, (r.octinv & 4u) != 0);
+    uint32_t hits = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < 8; k++) {
+        const uint32_t b = k & 3u;
+        const float tnx = fmaf(quant_to_float(k < 4 ? X.n0 : X.n1, b), X.si, X.bn);
+        const float tfx = fmaf(quant_to_float(k < 4 ? X.f0 : X.f1, b), X.si, X.bf);
+        const float tny = fmaf(quant_to_float(k < 4 ? Y.n0 : Y.n1, b), Y.si, Y.bn);
+        const float tfy = fmaf(quant_to_float(k < 4 ? Y.f0 : Y.f1, b), Y.si, Y.bf);
+        const float tnz = fmaf(quant_to_float(k < 4 ? Z.n0 : Z.n1, b), Z.si, Z.bn);
+        const float tfz = fmaf(quant_to_float(k < 4 ? Z.f0 : Z.f1, b), Z.si, Z.bf);
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tMin));
+        const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tBest));
+        hits |= (tn <= tf) ? (1u << k) : 0u;
+    }
+    // Empty slots hold the inverted box [p + 255 s, p], which no ray enters
+    // (and whose meta byte is 0, so a hit would add nothing).
+    innerHits = octant_permute(hits & imask, r.octinv);
+    uint32_t leaves = hits & ~imask;
+    triHits = 0;
+    while (leaves) {
+        const uint32_t k = uint32_t(__ffs(leaves) - 1);
+        leaves &= leaves - 1u;
+        const uint32_t m = __byte_perm(w1.z, w1.w, k) & 0xffu;  // (count << 5) | offset
+        triHits |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+    }
+}
+
+// One traversal iteration: visit the next node of the current group (if
+// any), then test the pending leaf triangles, then pop the stack when the
+// group is exhausted.  `postponeLimit` > 0 lets a lane push its triangle
+// group onto the stack and keep visiting nodes when fewer than
+// kPostponeLanes lanes of its warp have triangles to test; it is the stack
+// depth below which this is allowed (stack size minus tree depth, so that
+// node groups always fit).  Postponing is off by default: on the 2.3 M
+// triangle heightfield workload it cost 3 % (8 lanes) with dynamic ray fetch.
+#ifndef FPT_POSTPONE_LANES
+#define FPT_POSTPONE_LANES 0
+#endif
+constexpr int kPostponeLanes = FPT_POSTPONE_LANES;
+
+template <bool ANY>
+FPT_D void trace_step(const DevScene& s, const TraceRay& r, TraceState& t, uint2* stack, uint32_t stride, int postponeLimit) {
+    if (t.gHits) {
+        const uint32_t i = uint32_t(__ffs(t.gHits) - 1);
+        t.gHits &= t.gHits - 1u;
+        const uint32_t slot = i ^ r.octinv;
+        const uint32_t nodeIdx = t.gBase + __popc(t.gImask & ((1u << slot) - 1u));
+        t.visits++;
+        // A well-formed tree visits each node at most once per ray; guard
+        // against corrupted input so that the loop always terminates.
+        if (nodeIdx >= s.nodeCount || t.visits > s.nodeCount) {
+            atomicOr(s.errorWord, FPT_DEVERR_BAD_INDEX);
+            t.status = kTraceError;
+            return;
+        }
+        uint32_t innerHits, childBase, imask, triBase, triHits;
+        visit_node(s, r, t.tBest, nodeIdx, innerHits, childBase, imask, triBase, triHits);
+        if (t.gHits) {
+            if (t.sp >= kStackSize) {
+                atomicOr(s.errorWord, FPT_DEVERR_STACK_OVERFLOW);
+                t.status = kTraceError;
+                return;
+            }
+            stack[size_t(t.sp) * stride] = make_uint2(t.gBase, t.gHits | (t.gImask << 8));
+            t.sp++;
+        }
+        t.gBase = childBase;
+        t.gHits = innerHits;
+        t.gImask = imask;
+        t.tBase = triBase;
+        t.tHits = triHits;
+    }
+    while (t.tHits) {
+        if (postponeLimit > 0 && t.gHits && t.sp < postponeLimit && __popc(__activemask()) < kPostponeLanes) {
+            stack[size_t(t.sp) * stride] = make_uint2(t.tBase | kTriGroupFlag, t.tHits);
+            t.sp++;
+            t.tHits = 0;
+            break;
+        }
+        const uint32_t b = uint32_t(__ffs(t.tHits) - 1);
+        t.tHits &= t.tHits - 1u;
+        const uint32_t ti = t.tBase + b;
+        if (ti >= s.triCount) {
+            atomicOr(s.errorWord, FPT_DEVERR_BAD_INDEX);
+            continue;
+        }
+        const float4* tp = s.tris + size_t(ti) * 3;
+        const float4 a = __ldg(tp), bb = __ldg(tp + 1), c = __ldg(tp + 2);
+        t.triTests++;
+        float th, u, v;
+        if (!intersect_triangle(r.rs, r.o, make_float3(a.x, a.y, a.z), make_float3(bb.x, bb.y, bb.z), make_float3(c.x, c.y, c.z),
+                                th, u, v))
+            continue;
+        if (!(th >= r.tMin && th <= t.tBest)) continue;
+        const uint32_t g = __float_as_uint(a.w);
+        if (th == t.tBest && g > t.bestTri) continue;
+        if (ANY) {
+            t.status = kTraceAnyHit;
+            return;
+        }
+        t.tBest = th;
+        t.bestTri = g;
+        t.bestInst = __float_as_uint(bb.w);
+        t.bestPrim = __float_as_uint(c.w);
+        t.bestU = u;
+        t.bestV = v;
+    }
+    if (t.gHits == 0 && t.tHits == 0) {
+        if (t.sp == 0) {
+            t.status = kTraceDone;
+            return;
+        }
+        t.sp--;
+        const uint2 e = stack[size_t(t.sp) * stride];
+        if (e.x & kTriGroupFlag) {
+            t.tBase = e.x & ~kTriGroupFlag;
+            t.tHits = e.y;
+        } else {
+            t.gBase = e.x;
+            t.gHits = e.y & 0xffu;
+            t.gImask = e.y >> 8;
+        }
+    }
+}
+
+FPT_D void trace_result(const TraceState& t, HitRec& hit) {
+    hit.valid = false;
+    if (t.status == kTraceAnyHit) {
+        hit.valid = true;
+        return;
+    }
+    if (t.status == kTraceDone && t.bestTri != 0xffffffffu) {
+        hit.valid = true;
+        hit.globalTri = t.bestTri;
+        hit.instanceID = t.bestInst;
+        hit.primIndex = t.bestPrim;
+        hit.baryX = t.bestU;
+        hit.baryY = t.bestV;
+        hit.t = t.tBest;
+    }
+}
 
 // Traces one ray through the compressed 8-wide BVH.
 //   ANY = false: closest hit in [tMin, tMax]; ties on t resolve to the
 //                smaller global triangle index.
 //   ANY = true : first hit in [tMin, tMax] (visibility rays).
 // `stack` is this thread's slice of the block's shared-memory stack, strided
-// by `stride` entries.  Returns false and sets FPT_DEVERR_STACK_OVERFLOW if the
-// stack would overflow (the ray is then treated as a miss).
-struct TraceStats {
-    uint32_t nodes = 0, tris = 0;
-};
-
+// by `stride` entries.  Returns false (and the ray counts as a miss) when the
+// traversal stopped on an error, which is also recorded in the error word.
 template <bool ANY>
 FPT_D bool trace_bvh(const DevScene& s, float3 o, float3 d, float tMin, float tMax, HitRec& hit, uint2* stack,
                      uint32_t stride, TraceStats* ts = nullptr) {
     hit.valid = false;
     if (s.nodeCount == 0) return true;
-    const RayShear rs = make_shear(d);
-    const float ix = 1.f / (fabsf(d.x) > 1e-20f ? d.x : copysignf(1e-20f, d.x));
-    const float iy = 1.f / (fabsf(d.y) > 1e-20f ? d.y : copysignf(1e-20f, d.y));
-    const float iz = 1.f / (fabsf(d.z) > 1e-20f ? d.z : copysignf(1e-20f, d.z));
-    const uint32_t octinv = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
-    float tBest = tMax;
-    uint32_t bestTri = 0xffffffffu, bestInst = 0, bestPrim = 0;
-    float bestU = 0.f, bestV = 0.f;
-
-    int sp = 0;
-    uint32_t nodeIdx = 0;
-    bool haveNode = true;
-    uint32_t gBase = 0, gHits = 0, gImask = 0;
-    uint32_t visits = 0, triTests = 0;
-    for (;;) {
-        uint32_t tBase = 0, tHits = 0;
-        if (haveNode) {
-            haveNode = false;
-            visits++;
-            // A well-formed tree visits each node at most once per ray; guard
-            // against corrupted input so that the loop always terminates.
-            if (nodeIdx >= s.nodeCount || visits > s.nodeCount) {
-                atomicOr(s.errorWord, FPT_DEVERR_BAD_INDEX);
-                break;
-            }
-            const uint4* np = s.nodes + size_t(nodeIdx) * 5;
-            const uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
-            const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
-            const uint32_t ew = w0.w;
-            const float sx = __uint_as_float((ew & 0xffu) << 23);
-            const float sy = __uint_as_float(((ew >> 8) & 0xffu) << 23);
-            const float sz = __uint_as_float(((ew >> 16) & 0xffu) << 23);
-            const uint32_t imask = ew >> 24;
-            const uint32_t childBase = w1.x, triBase = w1.y;
-            const uint32_t meta[2] = {w1.z, w1.w};
-            const uint32_t qlx[2] = {w2.x, w2.y}, qly[2] = {w2.z, w2.w}, qlz[2] = {w3.x, w3.y};
-            const uint32_t qhx[2] = {w3.z, w3.w}, qhy[2] = {w4.x, w4.y}, qhz[2] = {w4.z, w4.w};
-            uint32_t innerHits = 0;
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const int wi = k >> 2, sh = (k & 3) * 8;
-                const uint32_t m = (meta[wi] >> sh) & 0xffu;
-                const bool internal = (imask >> k) & 1u;
-                if (!internal && m == 0u) continue;
-                const float lox = fmaf(float((qlx[wi] >> sh) & 0xffu), sx, px);
-                const float loy = fmaf(float((qly[wi] >> sh) & 0xffu), sy, py);
-                const float loz = fmaf(float((qlz[wi] >> sh) & 0xffu), sz, pz);
-                const float hix = fmaf(float((qhx[wi] >> sh) & 0xffu), sx, px);
-                const float hiy = fmaf(float((qhy[wi] >> sh) & 0xffu), sy, py);
-                const float hiz = fmaf(float((qhz[wi] >> sh) & 0xffu), sz, pz);
-                const float t0x = ((octinv & 1u) ? hix : lox) - o.x, t1x = ((octinv & 1u) ? lox : hix) - o.x;
-                const float t0y = ((octinv & 2u) ? hiy : loy) - o.y, t1y = ((octinv & 2u) ? loy : hiy) - o.y;
-                const float t0z = ((octinv & 4u) ? hiz : loz) - o.z, t1z = ((octinv & 4u) ? loz : hiz) - o.z;
-                const float tn = fmaxf(fmaxf(t0x * ix, t0y * iy), fmaxf(t0z * iz, tMin));
-                const float tf = fminf(fminf(t1x * ix, t1y * iy), fminf(t1z * iz, tBest));
-                if (!(widen_lo(tn) <= widen_hi(tf))) continue;
-                if (internal) {
-                    innerHits |= 1u << (k ^ octinv);
-                } else {
-                    const uint32_t cnt = m >> 5, off = m & 31u;
-                    tHits |= ((1u << cnt) - 1u) << off;
-                }
-            }
-            tBase = triBase;
-            if (gHits) {
-                if (sp >= kStackSize) {
-                    atomicOr(s.errorWord, FPT_DEVERR_STACK_OVERFLOW);
-                    if (ts) { ts->nodes += visits; ts->tris += triTests; }
-                    return false;
-                }
-                stack[size_t(sp) * stride] = make_uint2(gBase, gHits | (gImask << 8));
-                sp++;
-            }
-            gBase = childBase;
-            gHits = innerHits;
-            gImask = imask;
-        }
-        // Leaf triangles of the node just visited.
-        while (tHits) {
-            const int b = __ffs(tHits) - 1;
-            tHits &= tHits - 1u;
-            if (tBase + uint32_t(b) >= s.triCount) {
-                atomicOr(s.errorWord, FPT_DEVERR_BAD_INDEX);
-                continue;
-            }
-            const float4* tp = s.tris + size_t(tBase + uint32_t(b)) * 3;
-            const float4 a = __ldg(tp), bb = __ldg(tp + 1), c = __ldg(tp + 2);
-            triTests++;
-            float t, u, v;
-            if (!intersect_triangle(rs, o, make_float3(a.x, a.y, a.z), make_float3(bb.x, bb.y, bb.z), make_float3(c.x, c.y, c.z), t, u, v))
-                continue;
-            if (!(t >= tMin && t <= tBest)) continue;
-            const uint32_t g = __float_as_uint(a.w);
-            if (t == tBest && g > bestTri) continue;
-            if (ANY) {
-                hit.valid = true;
-                if (ts) { ts->nodes += visits; ts->tris += triTests; }
-                return true;
-            }
-            tBest = t;
-            bestTri = g;
-            bestInst = __float_as_uint(bb.w);
-            bestPrim = __float_as_uint(c.w);
-            bestU = u;
-            bestV = v;
-        }
-        // Next node: nearest remaining child of the current group, else pop.
-        if (gHits == 0) {
-            if (sp == 0) break;
-            sp--;
-            const uint2 e = stack[size_t(sp) * stride];
-            gBase = e.x;
-            gHits = e.y & 0xffu;
-            gImask = e.y >> 8;
-        }
-        const int i = __ffs(gHits) - 1;
-        gHits &= gHits - 1u;
-        const uint32_t slot = uint32_t(i) ^ octinv;
-        nodeIdx = gBase + __popc(gImask & ((1u << slot) - 1u));
-        haveNode = true;
+    const TraceRay r = make_trace_ray(o, d, tMin);
+    TraceState t;
+    trace_init(r, tMax, t);
+    while (t.status == kTraceRunning) trace_step<ANY>(s, r, t, stack, stride, 0);
+    if (ts) {
+        ts->nodes += t.visits;
+        ts->tris += t.triTests;
     }
-    if (ts) { ts->nodes += visits; ts->tris += triTests; }
-    if (bestTri != 0xffffffffu) {
-        hit.valid = true;
-        hit.globalTri = bestTri;
-        hit.instanceID = bestInst;
-        hit.primIndex = bestPrim;
-        hit.baryX = bestU;
-        hit.baryY = bestV;
-        hit.t = tBest;
-    }
-    return true;
+    trace_result(t, hit);
+    return t.status != kTraceError;
 }
-
 // ---------------------------------------------------------------------------
 // HitInfo packing (Scene/HitInfo.slang:457-487), uncompressed uint4.
 // ---------------------------------------------------------------------------

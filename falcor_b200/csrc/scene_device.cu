@@ -134,6 +134,15 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
     if (d.index_count && !d.indices) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: indices is NULL");
     if (d.instance_count && !d.instances) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: instances is NULL");
     if (d.material_count == 0 || !d.materials) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: no materials");
+    // The traversal's conservative box test needs |coordinate| * |1/d| to
+    // stay finite (|1/d| <= 1e20): positions are limited to |x| <= 1e15.
+    for (uint32_t i = 0; i < d.vertex_count; i++)
+        for (int a = 0; a < 3; a++) {
+            const float x = d.vertices[i].position[a];
+            if (!(std::fabs(x) <= 1e15f))
+                return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: vertex " + std::to_string(i) +
+                                                          " has a non-finite or out-of-range (|x| > 1e15) position");
+        }
     auto sc = std::make_unique<fpt_scene>();
     fpt_scene& s = *sc;
     compute_camera(d.camera, s.info.camera);
@@ -284,6 +293,7 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
     ds.hasTransmission = hasTransmission ? 1u : 0u;
     ds.nodeCount = uint32_t(s.bvh.nodes.size());
     ds.triCount = total;
+    ds.bvhDepth = s.bvh.maxDepth;
     ds.camera = s.info.camera;
     ds.bits = s.info.hit_bits;
 

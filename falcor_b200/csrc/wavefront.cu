@@ -28,7 +28,9 @@ namespace {
 constexpr int kTraceBlock = 128;
 constexpr int kShadeBlock = 128;
 
-// Counts: [0] shade queue, [1] extension queue, [2] shadow queue.
+// Counts: [0] shade queue, [1] extension queue, [2] shadow queue, [4] and [5]
+// the fetch counters of the extension and visibility ray kernels.
+constexpr int kFetchExtend = 4, kFetchShadow = 5, kNumWaveCounts = 8;
 struct WaveParams {
     uint32_t waveFirstPixel;   // first pixel of the wave
     uint32_t wavePixels;       // pixels in the wave
@@ -175,52 +177,114 @@ __global__ void __launch_bounds__(kShadeBlock) wf_shade(DevScene s, FrameParams 
 }
 
 // Visibility rays: L += thp * Lr when unoccluded.
-__global__ void __launch_bounds__(kTraceBlock) wf_shadow(DevScene s, FrameParams p, WaveParams wp, SoA w) {
-    __shared__ uint2 stackMem[kStackSize * kTraceBlock];
-    uint2* stack = stackMem + threadIdx.x;
+// Ray tracing kernels (visibility and extension rays) with per-lane dynamic
+// ray fetch: each warp takes chunks of kFetchChunk queue entries with one
+// atomic and hands them to its idle lanes, and a lane whose ray has finished
+// takes the next one as soon as fewer than kRefillBelow lanes of its warp are
+// still tracing.  The traversal itself advances one node visit per step, so
+// rays of very different lengths share a warp without leaving most of its
+// lanes idle until the longest ray is done.
+#ifndef FPT_REFILL_BELOW
+#define FPT_REFILL_BELOW 24
+#endif
+#ifndef FPT_TRACE_MIN_BLOCKS
+#define FPT_TRACE_MIN_BLOCKS 6
+#endif
+constexpr uint32_t kFetchChunk = 128;
+constexpr int kRefillBelow = FPT_REFILL_BELOW;
+
+template <bool SHADOW>
+FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams& wp, const SoA& w, uint2* stack) {
+    const uint32_t lane = threadIdx.x & 31u;
     Counters cnt;
-    const uint32_t n = wp.counts[2];
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t i = wp.shadowQueue[k];
-        const float4 o = w.sOrigin[i], d = w.sDir[i];
-        HitRec h;
-        TraceStats ts;
-        trace_bvh<true>(s, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), 0.f, o.w, h, stack, kTraceBlock, &ts);
-        cnt.trace(true, ts);
-        if (!h.valid) {
-            const float4 lr = w.sLr[i];
-            float4 L = w.L[i];
-            L.x += lr.x; L.y += lr.y; L.z += lr.z;
-            w.L[i] = L;
+    const uint32_t n = wp.counts[SHADOW ? 2 : 1];
+    uint32_t* fetch = wp.counts + (SHADOW ? kFetchShadow : kFetchExtend);
+    const uint32_t* queue = SHADOW ? wp.shadowQueue : wp.extQueue;
+    const int postponeLimit = kStackSize - int(s.bvhDepth);
+    uint32_t chunkNext = 0, chunkEnd = 0;  // warp-uniform
+    bool drained = n == 0 || s.nodeCount == 0;
+    bool active = false;
+    uint32_t path = 0, fv = 0;
+    TraceRay r;
+    TraceState t;
+    for (;;) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (idle && !drained) {
+            if (chunkNext >= chunkEnd) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(fetch, kFetchChunk);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base >= n) drained = true;
+                else { chunkNext = base; chunkEnd = min(base + kFetchChunk, n); }
+            }
+            if (!drained) {
+                const uint32_t avail = chunkEnd - chunkNext;
+                const uint32_t rank = __popc(idle & ((1u << lane) - 1u));
+                if (!active && rank < avail) {
+                    path = queue[chunkNext + rank];
+                    float4 o, d;
+                    if (SHADOW) { o = w.sOrigin[path]; d = w.sDir[path]; }
+                    else { o = w.originPdf[path]; d = w.dirV[path]; }
+                    fv = __float_as_uint(d.w);
+                    r = make_trace_ray(make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), 0.f);
+                    trace_init(r, SHADOW ? o.w : 1e30f, t);
+                    active = true;
+                }
+                chunkNext += min(avail, uint32_t(__popc(idle)));
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0) break;
+        for (;;) {
+            if (active) {
+                trace_step<SHADOW>(s, r, t, stack, kTraceBlock, postponeLimit);
+                if (t.status != kTraceRunning) {
+                    active = false;
+                    cnt.v[1]++;
+                    cnt.v[SHADOW ? 3 : 2]++;
+                    cnt.v[4] += t.visits;
+                    cnt.v[5] += t.triTests;
+                    if (SHADOW) { cnt.v[11] += t.visits; cnt.v[12] += t.triTests; }
+                    HitRec h;
+                    trace_result(t, h);
+                    if (SHADOW) {
+                        if (!h.valid && t.status != kTraceError) {
+                            const float4 lr = w.sLr[path];
+                            float4 L = w.L[path];
+                            L.x += lr.x; L.y += lr.y; L.z += lr.z;
+                            w.L[path] = L;
+                        }
+                    } else {
+                        uint32_t f = fv + (1u << 16);  // vertexIndex++
+                        if (h.valid) {
+                            f |= 0x2u;
+                            w.hit[path] = make_uint4(h.instanceID, h.primIndex, __float_as_uint(h.baryX), __float_as_uint(h.baryY));
+                        } else {
+                            f &= ~0x2u;
+                        }
+                        float4 d = w.dirV[path];
+                        d.w = __uint_as_float(f);
+                        w.dirV[path] = d;
+                    }
+                }
+            }
+            const uint32_t a = __ballot_sync(0xffffffffu, active);
+            if (a == 0) break;
+            if (!drained && __popc(a) < kRefillBelow) break;
         }
     }
     flush_counters(p.counters, cnt);
 }
 
-// Extension rays: closest hit; the path re-enters the shade queue.
-__global__ void __launch_bounds__(kTraceBlock) wf_extend(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+// Visibility rays of the NEE samples: any hit; adds thp * Lr when unoccluded.
+__global__ void __launch_bounds__(kTraceBlock, FPT_TRACE_MIN_BLOCKS) wf_shadow(DevScene s, FrameParams p, WaveParams wp, SoA w) {
     __shared__ uint2 stackMem[kStackSize * kTraceBlock];
-    uint2* stack = stackMem + threadIdx.x;
-    Counters cnt;
-    const uint32_t n = wp.counts[1];
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t i = wp.extQueue[k];
-        const float4 o = w.originPdf[i], d = w.dirV[i];
-        HitRec h;
-        TraceStats ts;
-        trace_bvh<false>(s, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), 0.f, 1e30f, h, stack, kTraceBlock, &ts);
-        cnt.trace(false, ts);
-        uint32_t fv = __float_as_uint(d.w);
-        fv += 1u << 16;  // vertexIndex++
-        if (h.valid) {
-            fv |= 0x2u;
-            w.hit[i] = make_uint4(h.instanceID, h.primIndex, __float_as_uint(h.baryX), __float_as_uint(h.baryY));
-        } else {
-            fv &= ~0x2u;
-        }
-        w.dirV[i] = make_float4(d.x, d.y, d.z, __uint_as_float(fv));
-    }
-    flush_counters(p.counters, cnt);
+    trace_queue<true>(s, p, wp, w, stackMem + threadIdx.x);
+}
+
+// Extension rays: closest hit; the path re-enters the shade queue.
+__global__ void __launch_bounds__(kTraceBlock, FPT_TRACE_MIN_BLOCKS) wf_extend(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    __shared__ uint2 stackMem[kStackSize * kTraceBlock];
+    trace_queue<false>(s, p, wp, w, stackMem + threadIdx.x);
 }
 
 // Finished paths keep their radiance in L; copy it into the per-sample buffer.
@@ -259,6 +323,8 @@ __global__ void wf_advance(WaveParams wp) {
     wp.counts[0] = wp.counts[1];
     wp.counts[1] = 0;
     wp.counts[2] = 0;
+    wp.counts[kFetchExtend] = 0;
+    wp.counts[kFetchShadow] = 0;
 }
 
 int blocks_for(const void* kernel, int block) {
@@ -294,7 +360,7 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
         wp.wavePixels = std::min(wavePixels, pixels - first);
         wp.wavePaths = wp.wavePixels * p.spp;
         wp.counts = b.counts;
-        cudaError_t e = cudaMemsetAsync(b.counts, 0, 4 * sizeof(uint32_t), st);
+        cudaError_t e = cudaMemsetAsync(b.counts, 0, kNumWaveCounts * sizeof(uint32_t), st);
         if (e != cudaSuccess) return e;
         uint32_t* qa = b.queueA;
         uint32_t* qb = b.queueB;
