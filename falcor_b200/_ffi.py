@@ -83,6 +83,10 @@ class fpt_grad_buffers(C.Structure):
     _fields_ = [("material", C.c_void_p), ("mesh_position", C.c_void_p), ("material_dim", u32), ("position_dim", u32)]
 
 
+class fpt_grad_config(C.Structure):
+    _fields_ = [("grad_type", u32), ("dim", u32), ("hash_size", u32)]
+
+
 class fpt_pass_stats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("rays", C.c_uint64), ("device_error", u32), ("kernel_launches", u32)]
 
@@ -114,6 +118,8 @@ SIGNATURES = {
     "fpt_scene_destroy": (None, [_P]),
     "fpt_scene_get_info": (C.c_int, [_P, C.POINTER(fpt_scene_info)]),
     "fpt_scene_set_camera": (C.c_int, [_P, C.POINTER(fpt_camera)]),
+    "fpt_scene_get_material_params": (C.c_int, [_P, C.POINTER(u32), u32, C.POINTER(C.c_float)]),
+    "fpt_scene_set_material_params": (C.c_int, [_P, C.POINTER(u32), u32, C.POINTER(C.c_float)]),
     "fpt_scene_get_bvh": (C.c_int, [_P, C.POINTER(fpt_bvh_view)]),
     "fpt_scene_get_alias_table": (C.c_int, [_P, C.POINTER(u32), u32, C.POINTER(f32)]),
     "fpt_pass_create": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
@@ -127,6 +133,13 @@ SIGNATURES = {
     "fpt_pass_execute": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P]),
     "fpt_pass_execute_noalloc": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P]),
     "fpt_pass_backward": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P, C.POINTER(fpt_grad_buffers), _P]),
+    "fpt_scene_gradients_create": (C.c_int, [C.POINTER(fpt_grad_config), u32, C.POINTER(_P)]),
+    "fpt_scene_gradients_destroy": (None, [_P]),
+    "fpt_scene_gradients_clear": (C.c_int, [_P, u32, _P]),
+    "fpt_scene_gradients_aggregate": (C.c_int, [_P, u32, _P]),
+    "fpt_scene_gradients_get": (C.c_int, [_P, u32, C.POINTER(C.POINTER(C.c_float)), C.POINTER(u32), C.POINTER(u32)]),
+    "fpt_pass_set_scene_gradients": (C.c_int, [_P, _P]),
+    "fpt_pass_set_dLdI": (C.c_int, [_P, _P]),
     "fpt_pass_get_stats": (C.c_int, [_P, C.POINTER(fpt_pass_stats), _P]),
     "fpt_pass_get_counters": (C.c_int, [_P, C.POINTER(C.c_uint64), u32, _P]),
     "fpt_pass_get_kernel_times": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_uint64), u32, C.c_int]),

@@ -88,6 +88,16 @@ FPT_D float3 decode_normal2x16(uint32_t p) { return oct_to_ndir_snorm(unpack_sno
 // ---------------------------------------------------------------------------
 // Pseudorandom generators and sample generators (Utils/Sampling/...).
 // ---------------------------------------------------------------------------
+// jenkinsHash (Utils/Math/HashUtils.slang:41-50): Bob Jenkins' 32-bit integer hash.
+FPT_D uint32_t jenkins_hash(uint32_t a) {
+    a = (a + 0x7ed55d16u) + (a << 12);
+    a = (a ^ 0xc761c23cu) ^ (a >> 19);
+    a = (a + 0x165667b1u) + (a << 5);
+    a = (a + 0xd3a2646cu) ^ (a << 9);
+    a = (a + 0xfd7046c5u) + (a << 3);
+    a = (a ^ 0xb55a4f09u) ^ (a >> 16);
+    return a;
+}
 FPT_D uint32_t interleave_32bit(uint32_t vx, uint32_t vy) {
     uint32_t x = vx & 0x0000ffffu;
     x = (x | (x << 8)) & 0x00FF00FFu;

@@ -16,6 +16,7 @@
 #include "kernels.cuh"
 #include "passes.h"
 #include "scene_device.h"
+#include "wardiff.h"
 
 namespace fpt {
 
@@ -98,9 +99,9 @@ void set_defaults(fpt_pass& p) {
     } else if (p.type == "WARDiffPathTracer") {
         d["samplesPerPixel"] = PropValue::num(1);
         d["maxBounces"] = PropValue::num(0);
-        d["diffMode"] = PropValue::str("Primal");
+        d["diffMode"] = PropValue::str("ForwardDiffDebug");
         d["diffVarName"] = PropValue::str("");
-        d["sampleGenerator"] = PropValue::num(1);
+        d["sampleGenerator"] = PropValue::num(0);
         d["fixedSeed"] = PropValue::num(1);
         d["useBSDFSampling"] = PropValue::num(1);
         d["useNEE"] = PropValue::num(1);
@@ -112,7 +113,10 @@ void set_defaults(fpt_pass& p) {
         d["boundaryTermBeta"] = PropValue::num(0.01);
         d["useAntitheticSampling"] = PropValue::num(1);
         d["diffuseBrdf"] = PropValue::str("Frostbite");
-        d["replayMode"] = PropValue::str("Replay");
+        // WARDiffPathTracerParams.runBackward (Params.slang:51) and the mesh of
+        // InverseOptimizationParams (set_mesh_to_optimize).
+        d["runBackward"] = PropValue::num(1);
+        d["meshToOptimize"] = PropValue::num(0);
     }
 }
 
@@ -400,6 +404,20 @@ FPT_API fpt_status fpt_pass_backward(fpt_pass* pass, const fpt_frame_io* io, con
     fpt_status s = ensure_scratch(*pass);
     if (s != FPT_OK) return s;
     return wardiff_execute(*pass, io, dLdI, grads, static_cast<cudaStream_t>(stream));
+}
+
+FPT_API fpt_status fpt_pass_set_scene_gradients(fpt_pass* pass, fpt_scene_gradients* grads) {
+    if (!pass) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_scene_gradients: null pass");
+    if (pass->type != "WARDiffPathTracer") return set_error(FPT_ERR_UNSUPPORTED, "scene_gradients: only WARDiffPathTracer has scene gradients");
+    pass->sceneGradients = grads;
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_pass_set_dLdI(fpt_pass* pass, const float* dLdI) {
+    if (!pass) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_dLdI: null pass");
+    if (pass->type != "WARDiffPathTracer") return set_error(FPT_ERR_UNSUPPORTED, "dL_dI: only WARDiffPathTracer takes dL_dI");
+    pass->dLdI = dLdI;
+    return FPT_OK;
 }
 
 FPT_API fpt_status fpt_pass_get_stats(fpt_pass* pass, fpt_pass_stats* out, void* stream) {

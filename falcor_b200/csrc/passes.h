@@ -34,6 +34,8 @@ struct fpt_pass {
     uint32_t launches = 0;
     fpt::WavefrontBuffers wavefront;  // path state of the wavefront scheduler
     fpt::KernelTimer timer;           // per-category kernel timing ("profileKernels")
+    fpt_scene_gradients* sceneGradients = nullptr;  // WARDiffPathTracer::scene_gradients (not owned)
+    const float* dLdI = nullptr;                    // WARDiffPathTracer::dL_dI (device, float3 per pixel)
 
     double num(const std::string& k) const;
     std::string str(const std::string& k) const;

@@ -126,6 +126,22 @@ DeviceBuffers::~DeviceBuffers() {
     for (void* p : ptrs) cudaFree(p);
 }
 
+// BasicMaterialData packing of a StandardMaterial (fp16 fields quantised on
+// the host like Falcor's float16_t, Utils/Math/Float16.cpp:56-169).
+DevMaterial pack_material(const fpt_material& s0) {
+    DevMaterial o;
+    std::memset(&o, 0, sizeof(o));
+    for (int k = 0; k < 4; k++) { o.baseColor[k] = f32_to_f16_host(s0.base_color[k]); o.specular[k] = f32_to_f16_host(s0.specular[k]); }
+    for (int k = 0; k < 3; k++) { o.emissive[k] = s0.emissive[k]; o.transmission[k] = f32_to_f16_host(s0.transmission[k]); }
+    o.emissiveFactor = s0.emissive_factor;
+    o.ior = f32_to_f16_host(s0.ior);
+    o.specTrans = f32_to_f16_host(s0.specular_transmission);
+    o.diffTrans = f32_to_f16_host(s0.diffuse_transmission);
+    o.flags = uint16_t((s0.flags & FPT_MATERIAL_DOUBLE_SIDED ? 1u : 0u) | (s0.flags & FPT_MATERIAL_THIN_SURFACE ? 2u : 0u));
+    o.activeLobes = 0xff;
+    return o;
+}
+
 fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
     int devCount = 0;
     if (cudaGetDeviceCount(&devCount) != cudaSuccess || devCount == 0)
@@ -204,18 +220,11 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
         inst[i] = DevInstance{d.instances[i].vb_offset, d.instances[i].ib_offset, d.instances[i].material_id, d.instances[i].flags};
     std::vector<DevMaterial> mats(d.material_count);
     std::vector<bool> emissiveMat(d.material_count, false);
+    s.materials.assign(d.materials, d.materials + d.material_count);
     for (uint32_t m = 0; m < d.material_count; m++) {
         const fpt_material& s0 = d.materials[m];
         DevMaterial& o = mats[m];
-        std::memset(&o, 0, sizeof(o));
-        for (int k = 0; k < 4; k++) { o.baseColor[k] = f32_to_f16_host(s0.base_color[k]); o.specular[k] = f32_to_f16_host(s0.specular[k]); }
-        for (int k = 0; k < 3; k++) { o.emissive[k] = s0.emissive[k]; o.transmission[k] = f32_to_f16_host(s0.transmission[k]); }
-        o.emissiveFactor = s0.emissive_factor;
-        o.ior = f32_to_f16_host(s0.ior);
-        o.specTrans = f32_to_f16_host(s0.specular_transmission);
-        o.diffTrans = f32_to_f16_host(s0.diffuse_transmission);
-        o.flags = uint16_t((s0.flags & FPT_MATERIAL_DOUBLE_SIDED ? 1u : 0u) | (s0.flags & FPT_MATERIAL_THIN_SURFACE ? 2u : 0u));
-        o.activeLobes = 0xff;
+        o = pack_material(s0);
         if (f16_to_f32_host(o.specTrans) > 0.f || f16_to_f32_host(o.diffTrans) > 0.f) hasTransmission = true;
         emissiveMat[m] = (s0.emissive[0] * s0.emissive_factor > 0.f) || (s0.emissive[1] * s0.emissive_factor > 0.f) ||
                          (s0.emissive[2] * s0.emissive_factor > 0.f);
@@ -386,6 +395,60 @@ FPT_API fpt_status fpt_scene_set_camera(fpt_scene* scene, const fpt_camera* came
     if (!scene || !camera) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_camera: null argument");
     compute_camera(*camera, scene->info.camera);
     scene->dev.camera = scene->info.camera;
+    return FPT_OK;
+}
+
+// Serialized material parameters (Scene/Material/StandardMaterialParamLayout.slang:32-42,
+// Material::serializeParams / deserializeParams): baseColor 0-2, metallic 3,
+// roughness 4, ior 5, transmissionColor 6-8, diffuseTransmission 9,
+// specularTransmission 10, emissiveColor 11-13, emissiveFactor 14, 15-19 unused.
+FPT_API fpt_status fpt_scene_get_material_params(const fpt_scene* scene, const uint32_t* ids, uint32_t count, float* params) {
+    if (!scene || (count && (!ids || !params))) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_get_material_params: null argument");
+    for (uint32_t i = 0; i < count; i++) {
+        if (ids[i] >= scene->materials.size()) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_get_material_params: material ID out of range");
+        const fpt_material& m = scene->materials[ids[i]];
+        float* o = params + size_t(i) * 20;
+        std::memset(o, 0, 20 * sizeof(float));
+        for (int k = 0; k < 3; k++) { o[k] = m.base_color[k]; o[6 + k] = m.transmission[k]; o[11 + k] = m.emissive[k]; }
+        o[3] = m.specular[2];
+        o[4] = m.specular[1];
+        o[5] = m.ior;
+        o[9] = m.diffuse_transmission;
+        o[10] = m.specular_transmission;
+        o[14] = m.emissive_factor;
+    }
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_scene_set_material_params(fpt_scene* scene, const uint32_t* ids, uint32_t count, const float* params) {
+    if (!scene || (count && (!ids || !params))) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_material_params: null argument");
+    for (uint32_t i = 0; i < count; i++)
+        if (ids[i] >= scene->materials.size()) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_material_params: material ID out of range");
+    std::vector<fpt_material> next = scene->materials;
+    for (uint32_t i = 0; i < count; i++) {
+        fpt_material& m = next[ids[i]];
+        const float* v = params + size_t(i) * 20;
+        for (int k = 0; k < 3; k++) { m.base_color[k] = v[k]; m.transmission[k] = v[6 + k]; }
+        m.specular[2] = v[3];
+        m.specular[1] = v[4];
+        m.ior = v[5];
+        m.diffuse_transmission = v[9];
+        m.specular_transmission = v[10];
+        const fpt_material& cur = scene->materials[ids[i]];
+        if (v[11] != cur.emissive[0] || v[12] != cur.emissive[1] || v[13] != cur.emissive[2] || v[14] != cur.emissive_factor)
+            return set_error(FPT_ERR_UNSUPPORTED, "fpt_scene_set_material_params: emissive parameters are fixed (the light collection is not rebuilt)");
+    }
+    bool hasTransmission = false;
+    for (uint32_t i = 0; i < count; i++) {
+        const DevMaterial dm = pack_material(next[ids[i]]);
+        if (cudaMemcpy(const_cast<DevMaterial*>(scene->dev.materials) + ids[i], &dm, sizeof(dm), cudaMemcpyHostToDevice) != cudaSuccess)
+            return set_error(FPT_ERR_CUDA, "fpt_scene_set_material_params: upload failed");
+    }
+    for (const fpt_material& m : next)
+        if (f16_to_f32_host(f32_to_f16_host(m.specular_transmission)) > 0.f || f16_to_f32_host(f32_to_f16_host(m.diffuse_transmission)) > 0.f)
+            hasTransmission = true;
+    scene->materials.swap(next);
+    scene->dev.hasTransmission = hasTransmission ? 1u : 0u;
     return FPT_OK;
 }
 

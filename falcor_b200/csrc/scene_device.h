@@ -18,6 +18,7 @@ struct DeviceBuffers {
 };
 
 fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out);
+DevMaterial pack_material(const fpt_material& m);
 
 }  // namespace fpt
 
@@ -26,6 +27,7 @@ struct fpt_scene {
     fpt::DeviceBuffers buffers;
     fpt::BVH8 bvh;                    // host copy of the acceleration structure
     std::vector<uint32_t> aliasTable; // host copy of the alias table
+    std::vector<fpt_material> materials;  // host copy of the material parameters
     float aliasWeightSum = 0.f;
     fpt_scene_info info{};
 };

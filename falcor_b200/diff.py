@@ -1,0 +1,173 @@
+"""Differentiable rendering: SceneGradients and the torch autograd bridge.
+
+``SceneGradients`` mirrors DiffRendering/SceneGradients.cpp:188-206
+(``create``, ``clear_grads``, ``aggregate_grads``, ``clear_all_grads``,
+``aggregate_all_grads``, ``get_grad_types``, ``get_grads_buffer``) over the
+fpt_scene_gradients handle; ``GradientType`` and ``GradConfig`` follow
+DiffRendering/SharedTypes.slang:53-71.  ``WARDiffRender`` is a
+``torch.autograd.Function`` whose forward renders the WARDiffPathTracer primal
+with the given material parameters and whose backward runs the adjoint of the
+same frame (same sample seed) into flat gradient tensors.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass
+
+from . import _ffi
+from ._ffi import check, lib
+
+
+class GradientType(enum.IntEnum):
+    Material = 0
+    MeshPosition = 1
+    MeshNormal = 2
+    MeshTangent = 3
+
+
+@dataclass
+class GradConfig:
+    grad_type: GradientType
+    dim: int
+    hash_size: int
+
+
+class _DeviceView:
+    """__cuda_array_interface__ view of a device float buffer (zero copy)."""
+
+    def __init__(self, ptr: int, n: int, owner):
+        self._owner = owner
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (ptr, False), "version": 3}
+
+
+def _stream() -> int:
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+class SceneGradients:
+    def __init__(self, configs):
+        arr = (_ffi.fpt_grad_config * len(configs))()
+        for i, c in enumerate(configs):
+            arr[i].grad_type, arr[i].dim, arr[i].hash_size = int(c.grad_type), int(c.dim), int(c.hash_size)
+        h = C.c_void_p()
+        check(lib().fpt_scene_gradients_create(arr, len(configs), C.byref(h)))
+        self._h = h
+        self._types = [GradientType(int(c.grad_type)) for c in configs]
+
+    @classmethod
+    def create(cls, device=None, grad_config_list=()):
+        return cls(list(grad_config_list))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            try:
+                _ffi.release("fpt_scene_gradients_destroy", self._h)
+            except Exception:  # interpreter shutdown
+                pass
+            self._h = None
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def clear_grads(self, render_context=None, grad_type: GradientType = GradientType.Material) -> None:
+        check(lib().fpt_scene_gradients_clear(self._h, int(grad_type), C.c_void_p(_stream())))
+
+    def aggregate_grads(self, render_context=None, grad_type: GradientType = GradientType.Material) -> None:
+        check(lib().fpt_scene_gradients_aggregate(self._h, int(grad_type), C.c_void_p(_stream())))
+
+    def clear_all_grads(self, render_context=None) -> None:
+        for t in self._types:
+            self.clear_grads(render_context, t)
+
+    def aggregate_all_grads(self, render_context=None) -> None:
+        for t in self._types:
+            self.aggregate_grads(render_context, t)
+
+    def get_grad_types(self) -> list:
+        return list(self._types)
+
+    def get_grads_buffer(self, grad_type: GradientType):
+        """The aggregated gradient buffer as a zero-copy CUDA tensor view."""
+        import torch
+        ptr = C.POINTER(C.c_float)()
+        dim, hs = C.c_uint32(), C.c_uint32()
+        check(lib().fpt_scene_gradients_get(self._h, int(grad_type), C.byref(ptr), C.byref(dim), C.byref(hs)))
+        if not ptr:
+            raise ValueError(f"gradient type {GradientType(int(grad_type)).name} is not configured")
+        addr = C.cast(ptr, C.c_void_p).value
+        return torch.as_tensor(_DeviceView(addr, dim.value, self), device="cuda")
+
+
+def _autograd():
+    import torch
+
+    class WARDiffRender(torch.autograd.Function):
+        """image = render(material_params); d image -> d material_params (and
+        d positions of the pass's mesh, returned through ``position_grad``).
+
+        forward(ctx, material_params [M, 20] float32 CUDA, renderer, frame_seed)
+        """
+
+        @staticmethod
+        def forward(ctx, material_params, renderer, frame_seed):
+            renderer.set_material_params(material_params)
+            img = renderer.render(frame_seed)
+            ctx.renderer = renderer
+            ctx.frame_seed = frame_seed
+            ctx.shape = material_params.shape
+            return img
+
+        @staticmethod
+        def backward(ctx, grad_img):
+            gm, _ = ctx.renderer.gradients(grad_img, ctx.frame_seed)
+            return gm.view(ctx.shape), None, None
+
+    return WARDiffRender
+
+
+def war_diff_render(material_params, renderer, frame_seed: int):
+    """Differentiable WARDiffPathTracer render (see ``WARDiffRender``)."""
+    return _autograd().apply(material_params, renderer, frame_seed)
+
+
+class DiffRenderer:
+    """Renders one scene with a WARDiffPathTracer pass at a fixed resolution and
+    exposes primal / gradient calls for ``war_diff_render``."""
+
+    def __init__(self, scene, width: int, height: int, props=None, mesh_id: int | None = None):
+        import torch
+        from .passes import WARDiffPathTracer
+        self.scene = scene
+        self.width, self.height = width, height
+        p = {"diffMode": "BackwardDiff", "maxBounces": 4, "useWAR": False}
+        if props:
+            p.update(props)
+        self.pt = WARDiffPathTracer(p)
+        self.pt.set_scene(scene)
+        if mesh_id is not None:
+            self.pt.set_mesh_to_optimize(mesh_id)
+        self.mesh_id = mesh_id
+        self.material_count = scene.info.material_count
+        self.position_grad = None
+        self.color = torch.zeros((height, width, 4), dtype=torch.float32, device="cuda")
+
+    def set_material_params(self, params) -> None:
+        self.scene.set_material_params(list(range(params.shape[0])), params.detach().reshape(-1, 20).cpu().numpy())
+
+    def render(self, frame_seed: int):
+        self.pt.set_properties({"fixedSeed": int(frame_seed), "runBackward": 0})
+        self.pt.execute({"color": self.color})
+        return self.color[..., :3].clone()
+
+    def gradients(self, grad_img, frame_seed: int, position_dim: int = 0):
+        import torch
+        self.pt.set_properties({"fixedSeed": int(frame_seed)})
+        gm = torch.zeros(self.material_count * 20, dtype=torch.float32, device="cuda")
+        gp = torch.zeros(max(position_dim, 1), dtype=torch.float32, device="cuda") if position_dim else None
+        dLdI = grad_img[..., :3].contiguous().float()
+        self.pt.backward({"color": self.color}, dLdI, material_grad=gm, position_grad=gp)
+        self.position_grad = gp
+        return gm, gp

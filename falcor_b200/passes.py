@@ -59,7 +59,10 @@ class RenderPass:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            _ffi.release("fpt_pass_destroy", self._h)
+            try:
+                _ffi.release("fpt_pass_destroy", self._h)
+            except Exception:  # interpreter shutdown
+                pass
             self._h = None
 
     @property
@@ -181,10 +184,46 @@ class PathTracer(RenderPass):
 
 
 class WARDiffPathTracer(RenderPass):
+    """WARDiffPathTracer (RenderPasses/WARDiffPathTracer/WARDiffPathTracer.cpp:697-715):
+    ``scene_gradients``, ``run_backward``, ``dL_dI``, ``set_mesh_to_optimize``."""
+
     def __init__(self, props=None):
         super().__init__("WARDiffPathTracer", props)
+        self._scene_gradients = None
+        self._dLdI = None
+
+    @property
+    def scene_gradients(self):
+        return self._scene_gradients
+
+    @scene_gradients.setter
+    def scene_gradients(self, g) -> None:
+        check(lib().fpt_pass_set_scene_gradients(self._h, g.handle if g is not None else None))
+        self._scene_gradients = g
+
+    @property
+    def run_backward(self) -> int:
+        return int(self.properties["runBackward"])
+
+    @run_backward.setter
+    def run_backward(self, v: int) -> None:
+        self.set_properties({"runBackward": int(v)})
+
+    @property
+    def dL_dI(self):
+        return self._dLdI
+
+    @dL_dI.setter
+    def dL_dI(self, t) -> None:
+        """dL/dI as a contiguous CUDA float32 tensor of H x W x 3 (float3 per pixel)."""
+        check(lib().fpt_pass_set_dLdI(self._h, C.c_void_p(_ptr(t)) if t is not None else None))
+        self._dLdI = t
+
+    def set_mesh_to_optimize(self, mesh_id: int) -> None:
+        self.set_properties({"meshToOptimize": int(mesh_id)})
 
     def backward(self, render_data: Mapping[str, Any], dLdI, material_grad=None, position_grad=None, frame: int = 0) -> None:
+        """Adjoint of one frame into flat gradient tensors (fpt_pass_backward)."""
         some = next((t for t in render_data.values() if t is not None), dLdI)
         height, width = int(some.shape[0]), int(some.shape[1])
         io = self._io(render_data, width, height, frame)

@@ -46,7 +46,10 @@ class HostScene:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            _ffi.release("fpt_scene_host_free", self._h)
+            try:
+                _ffi.release("fpt_scene_host_free", self._h)
+            except Exception:  # interpreter shutdown
+                pass
             self._h = None
 
     # numpy views (valid while this object lives)
@@ -102,13 +105,31 @@ class Scene:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            _ffi.release("fpt_scene_destroy", self._h)
+            try:
+                _ffi.release("fpt_scene_destroy", self._h)
+            except Exception:  # interpreter shutdown
+                pass
             self._h = None
 
     def set_camera(self, camera: _ffi.fpt_camera) -> None:
         """Replaces the camera for the next frames (fpt_scene_set_camera)."""
         check(lib().fpt_scene_set_camera(self._h, C.byref(camera)))
         check(lib().fpt_scene_get_info(self._h, C.byref(self.info)))
+
+    def get_material_params(self, ids) -> np.ndarray:
+        """Scene::getMaterialParams: 20 floats per material (serialized layout)."""
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        out = np.zeros((len(ids), 20), dtype=np.float32)
+        check(lib().fpt_scene_get_material_params(self._h, ids.ctypes.data_as(C.POINTER(C.c_uint32)), len(ids),
+                                                  out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
+    def set_material_params(self, ids, params) -> None:
+        """Scene::setMaterialParams (emissive parameters must stay unchanged)."""
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        params = np.ascontiguousarray(params, dtype=np.float32).reshape(len(ids), 20)
+        check(lib().fpt_scene_set_material_params(self._h, ids.ctypes.data_as(C.POINTER(C.c_uint32)), len(ids),
+                                                  params.ctypes.data_as(C.POINTER(C.c_float))))
 
     def bvh(self) -> tuple[np.ndarray, np.ndarray]:
         """Host copies of the 8-wide BVH nodes (80 B each) and triangle records (48 B each)."""

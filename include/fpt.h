@@ -235,6 +235,14 @@ FPT_API fpt_status fpt_scene_get_info(const fpt_scene* scene, fpt_scene_info* ou
  * setFocalLength, Scene/Camera/Camera.h:76-152, applied at the next frame).
  * The camera travels to the device with the next launch's parameters. */
 FPT_API fpt_status fpt_scene_set_camera(fpt_scene* scene, const fpt_camera* camera);
+/* Scene::getMaterialParams / setMaterialParams (Scene.cpp:4426-4470): 20
+ * floats per material in the serialized StandardMaterial layout (baseColor
+ * 0-2, metallic 3, roughness 4, ior 5, transmissionColor 6-8,
+ * diffuseTransmission 9, specularTransmission 10, emissiveColor 11-13,
+ * emissiveFactor 14).  Host arrays.  Emissive parameters cannot be changed
+ * (FPT_ERR_UNSUPPORTED): the light collection is built once per scene. */
+FPT_API fpt_status fpt_scene_get_material_params(const fpt_scene* scene, const uint32_t* ids, uint32_t count, float* params);
+FPT_API fpt_status fpt_scene_set_material_params(fpt_scene* scene, const uint32_t* ids, uint32_t count, const float* params);
 /* Host view of the scene's BVH (valid until the scene is destroyed). */
 FPT_API fpt_status fpt_scene_get_bvh(const fpt_scene* scene, fpt_bvh_view* out);
 /* Host copy of the emissive alias table (uint2 per emissive triangle) and
@@ -313,11 +321,53 @@ typedef struct fpt_grad_buffers {
     uint32_t position_dim;       /* number of floats in `mesh_position`       */
 } fpt_grad_buffers;
 
-/* bwd_diff(tracePaths) of WARDiffPathTracer.rt.slang:167-180 by path replay:
- * dLdI is a caller-owned device array of float3 per pixel. */
+/* bwd_diff(tracePaths) of WARDiffPathTracer.rt.slang:167-180 into caller-owned
+ * flat buffers (no hashing): the path is re-traced with the same samples and
+ * its vertices are swept backwards.  dLdI is a caller-owned device array of
+ * float3 per pixel.  Equivalent to an execute with runBackward = 1 followed by
+ * aggregation, for callers that keep gradients in their own tensors. */
 FPT_API fpt_status fpt_pass_backward(fpt_pass* pass, const fpt_frame_io* io,
                                      const float* dLdI, const fpt_grad_buffers* grads,
                                      void* stream);
+
+/* SceneGradients (DiffRendering/SceneGradients.h:40-120, .cpp:42-206):
+ * gradient types as in DiffRendering/SharedTypes.slang:53-71. */
+typedef enum fpt_gradient_type {
+    FPT_GRAD_MATERIAL = 0,       /* materialID * 20 + StandardMaterialParamLayout offset */
+    FPT_GRAD_MESH_POSITION = 1,  /* localVertex * 3 + axis of the optimised mesh          */
+    FPT_GRAD_MESH_NORMAL = 2,    /* accepted; the adjoint produces no normal gradients   */
+    FPT_GRAD_MESH_TANGENT = 3,   /* accepted; the adjoint produces no tangent gradients  */
+    FPT_GRAD_TYPE_COUNT = 4
+} fpt_gradient_type;
+
+/* GradConfig(grad_type, dim, hash_size) (SceneGradients.cpp:188-196). */
+typedef struct fpt_grad_config {
+    uint32_t grad_type;
+    uint32_t dim;
+    uint32_t hash_size;
+} fpt_grad_config;
+
+typedef struct fpt_scene_gradients fpt_scene_gradients;
+
+/* SceneGradients::create: device buffers of dim floats and dim * hash_size
+ * scratch floats per configured type. */
+FPT_API fpt_status fpt_scene_gradients_create(const fpt_grad_config* configs, uint32_t count,
+                                              fpt_scene_gradients** out);
+FPT_API void fpt_scene_gradients_destroy(fpt_scene_gradients* grads);
+/* clearGrads (SceneGradients.cpp:110-118): zero scratch and result. */
+FPT_API fpt_status fpt_scene_gradients_clear(fpt_scene_gradients* grads, uint32_t grad_type, void* stream);
+/* aggregateGrads (SceneGradients.cpp:120-135, AggregateGradients.cs.slang:50-73):
+ * result[i] += sum over hash rows of scratch[row][i]. */
+FPT_API fpt_status fpt_scene_gradients_aggregate(fpt_scene_gradients* grads, uint32_t grad_type, void* stream);
+/* getGradsBuffer: device pointer of the result (valid until destroy). */
+FPT_API fpt_status fpt_scene_gradients_get(const fpt_scene_gradients* grads, uint32_t grad_type, float** out,
+                                           uint32_t* dim, uint32_t* hash_size);
+/* WARDiffPathTracer::setSceneGradients / setdLdI (WARDiffPathTracer.cpp:697-715):
+ * with diffMode "BackwardDiff" and property runBackward = 1, fpt_pass_execute
+ * scatters the gradients of the frame into the scene gradients' scratch
+ * buffers; dLdI is a device array of float3 per pixel.  Not owned. */
+FPT_API fpt_status fpt_pass_set_scene_gradients(fpt_pass* pass, fpt_scene_gradients* grads);
+FPT_API fpt_status fpt_pass_set_dLdI(fpt_pass* pass, const float* dLdI);
 
 /* Device counters of the last execute (rays traced, paths, error word). */
 typedef struct fpt_pass_stats {

@@ -32,6 +32,11 @@ class PathTracerParams(C.Structure):
                 ("specularRoughnessThreshold", C.c_float), ("colorFormat", u32), ("seed", u32), ("lambert", u32)]
 
 
+class WarDiffParams(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("maxBounces", u32), ("useBSDFSampling", u32), ("useNEE", u32),
+                ("useMIS", u32), ("useAntithetic", u32), ("seed", u32), ("lambert", u32), ("meshID", u32)]
+
+
 class SceneInfo(C.Structure):
     _fields_ = [("triangle_count", u32), ("instance_count", u32), ("emissive_count", u32), ("active_emissive_count", u32),
                 ("type_bits", u32), ("instance_id_bits", u32), ("primitive_index_bits", u32), ("has_env", u32),
@@ -72,6 +77,9 @@ def lib() -> C.CDLL:
         l.orc_path_tracer.restype = C.c_double
         l.orc_path_tracer.argtypes = [_P, C.POINTER(PathTracerParams), _P, _P, _P, C.c_int, u32, u32, u32, u32, u32,
                                       C.POINTER(Counters)]
+        l.orc_wardiff.restype = C.c_double
+        l.orc_wardiff.argtypes = [_P, C.POINTER(WarDiffParams), C.c_int, C.c_int, _P, u32, _P, u32, C.c_double, _P, _P, _P,
+                                  _P, u32, u32, u32, u32, u32, C.POINTER(C.c_uint64)]
         for n in ("orc_xoshiro", "orc_lcg"):
             getattr(l, n).argtypes = [_P, u32, u32, _P]
         l.orc_splitmix.argtypes = [_P, u32, u32, _P]
@@ -144,6 +152,34 @@ class OracleScene:
         dt = lib().orc_path_tracer(self._h, C.byref(params), ptr(np.ascontiguousarray(vbuffer)), ptr(out),
                                    ptr(smp) if smp is not None else None, int(fp64), threads, x0, y0, x1, y1, C.byref(cnt))
         return out, smp, cnt, dt
+
+    def wardiff(self, params: WarDiffParams, mode: int = 0, dLdI=None, mat_tangents=None, pos_tangents=None, eps: float = 0.0,
+                threads: int = 0, rect=None):
+        """WARDiffPathTracer restatement.  mode 0: FP32 primal; 1: forward-mode
+        derivatives along the rows of mat_tangents / pos_tangents (K <= 4) ->
+        sum over pixels of dLdI . dL/dv_k; 2: radiance with the parameters offset
+        by eps * (row 0) (FP64), for finite differences.
+        Returns (color RGBA32F, grads[K] or None, perturbed radiance or None, rays, seconds)."""
+        w, h = params.width, params.height
+        color = np.zeros((h, w, 4), dtype=np.float32)
+        K = 0
+        mt = pt = None
+        if mat_tangents is not None:
+            mt = np.ascontiguousarray(np.atleast_2d(mat_tangents), dtype=np.float64)
+            K = mt.shape[0]
+        if pos_tangents is not None:
+            pt = np.ascontiguousarray(np.atleast_2d(pos_tangents), dtype=np.float64)
+            K = max(K, pt.shape[0])
+        grads = np.zeros(4, dtype=np.float64)
+        pert = np.zeros((h, w, 3), dtype=np.float64) if mode == 2 else None
+        g = np.ascontiguousarray(dLdI, dtype=np.float32) if dLdI is not None else None
+        x0, y0, x1, y1 = rect if rect else (0, 0, w, h)
+        rays = C.c_uint64()
+        dt = lib().orc_wardiff(self._h, C.byref(params), mode, K, ptr(mt) if mt is not None else None,
+                               mt.shape[1] if mt is not None else 0, ptr(pt) if pt is not None else None,
+                               pt.shape[1] if pt is not None else 0, eps, ptr(g) if g is not None else None, ptr(color),
+                               ptr(grads), ptr(pert) if pert is not None else None, threads, x0, y0, x1, y1, C.byref(rays))
+        return color, (grads[:K] if mode == 1 else None), pert, int(rays.value), dt
 
     def lights(self):
         n = self.info.emissive_count

@@ -253,4 +253,43 @@ void orc_bsdf_sample(const float* data, int lambert, uint32_t n, const float* wi
     }
 }
 
+
+// WARDiffPathTracer over a rectangle (one path per pixel).  color: RGBA32F full
+// frame (optional); dLdI: 3 floats per pixel, pixel-major (mode 1); grads: K
+// doubles, sum over the rectangle of dLdI . dL/dv_k (mode 1); pert: 3 doubles
+// per pixel of the perturbed radiance (mode 2).
+double orc_wardiff(const void* sp, const WarDiffParams* p, int mode, int K, const double* matTangents, uint32_t matDim,
+                   const double* posTangents, uint32_t posDim, double eps, const float* dLdI, float* color, double* grads,
+                   double* pert, uint32_t threads, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, uint64_t* rays) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    WarSeeds seeds;
+    seeds.K = K;
+    seeds.mat = matTangents;
+    seeds.matDim = matDim;
+    seeds.pos = posTangents;
+    seeds.posDim = posDim;
+    seeds.meshID = p->meshID;
+    seeds.eps = eps;
+    uint32_t nthreads = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
+    std::vector<std::vector<double>> acc(nthreads, std::vector<double>(4, 0.0));
+    std::vector<WarCounters> wcs(nthreads);
+    auto t0 = std::chrono::steady_clock::now();
+    parallel_tiles(x0, y0, x1, y1, nthreads, [&](uint32_t x, uint32_t y, uint32_t tid) {
+        size_t i = size_t(y) * p->width + x;
+        wardiff_pixel(s, *p, seeds, mode, x, y, dLdI ? dLdI + 3 * i : nullptr, color ? color + 4 * i : nullptr,
+                      acc[tid].data(), pert ? pert + 3 * i : nullptr, &wcs[tid]);
+    });
+    double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (grads)
+        for (int k = 0; k < K && k < 4; k++) {
+            grads[k] = 0;
+            for (auto& a : acc) grads[k] += a[k];
+        }
+    if (rays) {
+        *rays = 0;
+        for (auto& c : wcs) *rays += c.rays;
+    }
+    return dt;
+}
+
 }  // extern "C"

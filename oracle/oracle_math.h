@@ -19,6 +19,8 @@
 #include <algorithm>
 #include <limits>
 
+#include "oracle_dual.h"
+
 namespace orc {
 
 // ---------------------------------------------------------------------------

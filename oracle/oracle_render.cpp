@@ -754,6 +754,8 @@ void path_tracer_pixel(const Scene& s, const PathTracerParams& p, uint32_t x, ui
     colorOut[0] = float(out.x); colorOut[1] = float(out.y); colorOut[2] = float(out.z); colorOut[3] = 1.f;
 }
 
+#include "oracle_wardiff.inl"
+
 template V3<float> minimal_pt_pixel<float>(const Scene&, const MinimalPTParams&, uint32_t, uint32_t, const uint32_t*, uint32_t*);
 template V3<double> minimal_pt_pixel<double>(const Scene&, const MinimalPTParams&, uint32_t, uint32_t, const uint32_t*, uint32_t*);
 template void path_tracer_pixel<float>(const Scene&, const PathTracerParams&, uint32_t, uint32_t, const uint32_t*, float*, float*, PathCounters*);

@@ -38,6 +38,35 @@ struct PathCounters {
     TraceCounters tc;
 };
 
+// WARDiffPathTracer (oracle_wardiff.inl).
+struct WarDiffParams {           // WARDiffPathTracer static + runtime parameters
+    uint32_t width, height;
+    uint32_t maxBounces;         // default 0
+    uint32_t useBSDFSampling, useNEE, useMIS;
+    uint32_t useAntithetic;      // default 1
+    uint32_t seed;               // frame seed (fixedSeed or frame count)
+    uint32_t lambert;
+    uint32_t meshID;             // mesh whose vertex positions are differentiated
+};
+
+struct WarSeeds {
+    int K = 0;                       // number of seeded directions
+    const double* mat = nullptr;     // K x matDim tangents of material parameters (materialID * 20 + offset)
+    uint32_t matDim = 0;
+    const double* pos = nullptr;     // K x posDim tangents of the positions of mesh `meshID` (localVertex * 3 + axis)
+    uint32_t posDim = 0;
+    uint32_t meshID = 0xffffffffu;
+    double eps = 0;                  // Shadow: perturbation scale
+};
+
+struct WarCounters { uint64_t rays = 0, hits = 0; };
+
+// mode 0: FP32 primal into colorOut (RGBA); 1: forward-mode derivatives along
+// the K <= 4 seeded directions, gradAcc[k] += dLdI . dL/dv_k; 2: the path with
+// the seeded parameters offset by eps * v_0, perturbed radiance into pertOut (FP64).
+void wardiff_pixel(const Scene& s, const WarDiffParams& p, const WarSeeds& seeds, int mode, uint32_t x, uint32_t y,
+                   const float* dLdI, float* colorOut, double* gradAcc, double* pertOut, WarCounters* wc);
+
 void pack_hit(const fpt_hitinfo_bits& b, const Hit& h, uint32_t out[4]);
 Hit unpack_hit(const fpt_hitinfo_bits& b, const uint32_t in[4]);
 

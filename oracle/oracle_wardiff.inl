@@ -1,0 +1,351 @@
+// oracle_wardiff.inl -- CPU restatement of the WARDiffPathTracer primal and of
+// its derivative with respect to material parameters and mesh vertex
+// positions, included by oracle_render.cpp.
+//
+// TEST INFRASTRUCTURE ONLY (see oracle_math.h).
+//
+// The path (RenderPasses/WARDiffPathTracer/WARDiffPathTracer.rt.slang:75-143,
+// PTUtils.slang:97-341) is written once over two types: V (float) for every
+// non-differentiable quantity -- sampling, traversal, shading frames, MIS
+// weights -- and R for the differentiable ones -- throughput, radiance, the
+// hit position of AttachToRay intersections and the material parameters read
+// through GradientIOWrapper.  R = float is the FP32 parity oracle; R = Dual<N>
+// gives forward-mode derivatives along N seeded parameter directions; R =
+// Shadow gives the same path with the seeded parameters perturbed, for finite
+// differences that keep every non-differentiable decision fixed.
+//
+// Differentiability follows the Slang sources:
+//  * mi.sample, generateEmissiveSample, evalMIS, getProperties (emission) and
+//    the light sampler are not differentiable (PTUtils.slang:177-207,
+//    StandardMaterialInstance.slang:92-160); mi.evalAD is
+//    (StandardMaterialInstance.slang:75-89) through StandardBSDFData, whose
+//    lobe probabilities are detached (StandardBSDF.slang:174-184).
+//  * computeBarycentrics is not [Differentiable]
+//    (Utils/Geometry/GeometryHelpers.slang:465-482), so the AttachToRay hit
+//    position is sum(v_i * b_i) with b detached (DiffSceneQuery.slang:195-219);
+//    the interpolated normal and tangent come from vertex attributes that carry
+//    no position derivative (DiffSceneIO.slang:145-258).
+//  * computeRayOrigin passes the position derivative through unchanged
+//    (GeometryHelpers.slang:70-83).
+//  * The Gaussian pixel-filter ratio and the area-to-solid-angle ratio are
+//    x / detach(x) (WARDiffPathTracer.rt.slang:92-93, PTUtils.slang:238):
+//    value 1, derivative dx / x.
+// The warped-area reparameterisation (useWAR) leaves every value unchanged (its
+// weight is det(I + infinitesimal J) = 1 and its direction offset is an
+// infinitesimal, WarpedAreaReparam.slang:226-263) and is not restated here:
+// this oracle covers the primal and the interior (useWAR = false) gradients.
+
+template <class R> struct Seed;
+template <> struct Seed<float> {
+    static float mat(const WarSeeds&, uint32_t, float v) { return v; }
+    static float pos(const WarSeeds&, uint32_t, float v) { return v; }
+};
+template <int N> struct Seed<Dual<N>> {
+    static Dual<N> get(const double* t, uint32_t dim, int K, uint32_t idx, float v) {
+        Dual<N> r{double(v)};
+        if (t && idx < dim)
+            for (int k = 0; k < N && k < K; k++) r.d[k] = t[size_t(k) * dim + idx];
+        return r;
+    }
+    static Dual<N> mat(const WarSeeds& s, uint32_t idx, float v) { return get(s.mat, s.matDim, s.K, idx, v); }
+    static Dual<N> pos(const WarSeeds& s, uint32_t idx, float v) { return get(s.pos, s.posDim, s.K, idx, v); }
+};
+template <> struct Seed<Shadow> {
+    static Shadow get(const double* t, uint32_t dim, double eps, uint32_t idx, float v) {
+        double p = double(v);
+        if (t && idx < dim) p += eps * t[idx];
+        return Shadow(double(v), p);
+    }
+    static Shadow mat(const WarSeeds& s, uint32_t idx, float v) { return get(s.mat, s.matDim, s.eps, idx, v); }
+    static Shadow pos(const WarSeeds& s, uint32_t idx, float v) { return get(s.pos, s.posDim, s.eps, idx, v); }
+};
+
+template <class R> static V3<R> lift3(const V3<float>& a) { return V3<R>(R(a.x), R(a.y), R(a.z)); }
+template <class R> static V3<float> val3(const V3<R>& a) { return V3<float>(float(a.x), float(a.y), float(a.z)); }
+
+// Intersection recomputed from the hit triangle (DiffSceneQuery.slang:148-219).
+template <class R> struct WarIsect {
+    uint32_t instanceID, primIndex;
+    float b[3];                  // computeBarycentrics of the ray/plane point
+    V3<R> posW;                  // sum(v_i * b_i)
+    V3<float> normalW, tangentW; // interpolated vertex normal / tangent (unnormalised)
+    uint32_t localIdx[3];        // vertex indices within the mesh
+};
+
+// computeRayDistanceToTriangle (GeometryHelpers.slang:442-457).
+static float war_ray_distance(const V3<float> v[3], V3<float> o, V3<float> d) {
+    V3<float> e1 = v[1] - v[0], e2 = v[2] - v[0];
+    V3<float> pvec = cross(d, e2);
+    float det = dot(e1, pvec);
+    V3<float> tvec = o - v[0];
+    V3<float> qvec = cross(tvec, e1);
+    return dot(e2, qvec) / det;
+}
+// computeBarycentrics (GeometryHelpers.slang:465-482).
+static void war_barycentrics(const V3<float> v[3], V3<float> p, float b[3]) {
+    V3<float> e0 = v[0] - p, e1 = v[1] - p, e2 = v[2] - p;
+    float a0 = length(cross(e1, e2));
+    float a1 = length(cross(e2, e0));
+    float a2 = length(cross(e0, e1));
+    float area = a0 + a1 + a2;
+    b[0] = a0 / area;
+    b[1] = a1 / area;
+    b[2] = a2 / area;
+}
+
+template <class R>
+static WarIsect<R> war_intersection(const Scene& s, const WarSeeds& seeds, const Hit& h, V3<float> o, V3<float> d) {
+    WarIsect<R> is;
+    is.instanceID = h.instanceID;
+    is.primIndex = h.primitiveIndex;
+    uint32_t idx[3];
+    s.getTriangleVertexIndices(h.instanceID, h.primitiveIndex, idx);
+    const uint32_t vb = s.instances[h.instanceID].vb_offset;
+    StaticVertex sv[3] = {s.getVertex(idx[0]), s.getVertex(idx[1]), s.getVertex(idx[2])};
+    V3<float> v[3] = {sv[0].position, sv[1].position, sv[2].position};
+    const float t = war_ray_distance(v, o, d);
+    V3<float> p = o + d * t;
+    war_barycentrics(v, p, is.b);
+    const bool seeded = h.instanceID == seeds.meshID;
+    V3<R> vr[3];
+    for (int i = 0; i < 3; i++) {
+        is.localIdx[i] = idx[i] - vb;
+        for (int a = 0; a < 3; a++)
+            vr[i][a] = seeded ? Seed<R>::pos(seeds, is.localIdx[i] * 3 + a, v[i][a]) : R(v[i][a]);
+    }
+    is.posW = vr[0] * R(is.b[0]) + vr[1] * R(is.b[1]) + vr[2] * R(is.b[2]);
+    // loadVertexNormalsW / loadVertexTangentsW (identity world matrices).
+    V3<float> n[3], tg[3];
+    for (int i = 0; i < 3; i++) {
+        n[i] = normalize(sv[i].normal);
+        tg[i] = normalize(V3<float>(sv[i].tangent[0], sv[i].tangent[1], sv[i].tangent[2]));
+    }
+    is.normalW = n[0] * is.b[0] + n[1] * is.b[1] + n[2] * is.b[2];
+    is.tangentW = tg[0] * is.b[0] + tg[1] * is.b[1] + tg[2] * is.b[2];
+    return is;
+}
+
+// Material instance built through GradientIOWrapper.getFloat
+// (StandardMaterial.slang:135-250); R carries the seeded derivatives.
+template <class R>
+static MaterialInstance<R> war_material(const Scene& s, const WarSeeds& seeds, const ShadingData<float>& sd, bool lambert) {
+    const Material& m = s.materials[sd.materialID];
+    const uint32_t base = sd.materialID * 20u;
+    MaterialInstance<R> mi;
+    mi.lambert = lambert;
+    mi.thin = m.thinSurface;
+    mi.activeLobes = m.activeLobes;
+    BSDFData<R>& d = mi.data;
+    R IoR = Seed<R>::mat(seeds, base + 5, m.ior);
+    d.eta = sd.frontFacing ? (R(1) / IoR) : (IoR / R(1));
+    d.diffuseTransmission = Seed<R>::mat(seeds, base + 9, m.diffTrans);
+    d.specularTransmission = Seed<R>::mat(seeds, base + 10, m.specTrans);
+    d.transmission = V3<R>(R(0));
+    if (d.diffuseTransmission > R(0) || d.specularTransmission > R(0))
+        d.transmission = V3<R>(Seed<R>::mat(seeds, base + 6, m.transmission[0]), Seed<R>::mat(seeds, base + 7, m.transmission[1]),
+                               Seed<R>::mat(seeds, base + 8, m.transmission[2]));
+    R f = (IoR - R(1)) / (IoR + R(1));
+    R F0 = f * f;
+    V3<R> baseColor(Seed<R>::mat(seeds, base + 0, m.baseColor[0]), Seed<R>::mat(seeds, base + 1, m.baseColor[1]),
+                    Seed<R>::mat(seeds, base + 2, m.baseColor[2]));
+    R roughness = Seed<R>::mat(seeds, base + 4, m.specular[1]);
+    R metallic = Seed<R>::mat(seeds, base + 3, m.specular[2]);
+    d.diffuse = lerp(baseColor, V3<R>(R(0)), metallic);
+    d.specular = lerp(V3<R>(F0), baseColor, metallic);
+    d.roughness = roughness;
+    d.metallic = metallic;
+    mi.T = lift3<R>(sd.T); mi.B = lift3<R>(sd.B); mi.N = lift3<R>(sd.N);
+    if (!sd.frontFacing && m.doubleSided) mi.N = -mi.N;  // flipShadingNormal
+    mi.emission = V3<R>(R(0));
+    if (sd.frontFacing) mi.emission = V3<R>(R(m.emissive[0]), R(m.emissive[1]), R(m.emissive[2])) * R(m.emissiveFactor);
+    return mi;
+}
+
+template <class R> static ShadingData<R> sd_lift(const ShadingData<float>& a) {
+    ShadingData<R> r;
+    r.posW = lift3<R>(a.posW); r.V = lift3<R>(a.V); r.T = lift3<R>(a.T); r.B = lift3<R>(a.B); r.N = lift3<R>(a.N);
+    r.faceN = lift3<R>(a.faceN);
+    r.uv = V2<R>(R(a.uv.x), R(a.uv.y));
+    for (int k = 0; k < 4; k++) r.tangentW[k] = R(a.tangentW[k]);
+    r.frontFacing = a.frontFacing;
+    r.materialID = a.materialID;
+    r.IoR = R(a.IoR);
+    return r;
+}
+
+// evalMIS, power-two heuristic (PTUtils.slang:87-93).
+static float war_mis(float n0, float p0, float n1, float p1) {
+    float q0 = (n0 * p0) * (n0 * p0);
+    float q1 = (n1 * p1) * (n1 * p1);
+    return q0 / (q0 + q1);
+}
+
+template <class R> struct WarPath {
+    V3<R> radiance, thp;
+    uint32_t length = 0;
+    bool terminated = false;
+    V3<float> normal;
+    float pdf = 0;
+};
+
+template <class R>
+static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSeeds& seeds, uint32_t x, uint32_t y,
+                            WarCounters* wc) {
+    const uint32_t frameSeed = p.seed;
+    UniformSG sg(x, y, frameSeed / 2);
+    next2D<float>(sg);
+    next2D<float>(sg);
+    next2D<float>(sg);
+    V2<float> pixelf(float(x) + 0.5f, float(y) + 0.5f);
+    V2<float> u = next2D<float>(sg);
+    // sampleGaussian (WARDiffPathTracer.rt.slang:59-62), sigma 0.5.
+    const float sigma = 0.5f;
+    const float r = std::sqrt(-2.f * std::log(u.x));
+    const float ang = 6.28318530717958647692f * u.y;
+    V2<float> jitter((r * std::cos(ang)) * sigma, (r * std::sin(ang)) * sigma);
+    if (p.useAntithetic && frameSeed % 2 == 0) jitter = V2<float>(-jitter.x, -jitter.y);
+    V2<float> pix = pixelf + jitter;
+
+    WarPath<R> path;
+    path.radiance = V3<R>(R(0));
+    path.thp = V3<R>(R(1));
+    path.normal = V3<float>(0.f);
+    // The pixel-filter ratio w / detach(w) has value 1; its derivative only
+    // exists through the warped screen sample (useWAR), not restated here.
+
+    // computeCameraRayDirection (DiffSceneQuery.slang:314-323).
+    const fpt_camera_data& c = s.camera;
+    V2<float> q(pix.x / float(p.width), pix.y / float(p.height));
+    V2<float> ndc(2.f * q.x + -1.f, -2.f * q.y + 1.f);
+    V3<float> dirU = ndc.x * V3<float>(c.cameraU[0], c.cameraU[1], c.cameraU[2]) + ndc.y * V3<float>(c.cameraV[0], c.cameraV[1], c.cameraV[2]) +
+                     V3<float>(c.cameraW[0], c.cameraW[1], c.cameraW[2]);
+    float len = length(dirU);
+    V3<float> rayDir = len > 0.f ? dirU / len : V3<float>(0.f);
+    V3<float> rayOrigin(c.posW[0], c.posW[1], c.posW[2]);
+
+    if (wc) wc->rays++;
+    Hit h = s.traceClosest(rayOrigin, rayDir, 0.f, std::numeric_limits<float>::max(), nullptr);
+    if (!h.valid) return path.radiance;
+    WarIsect<R> is = war_intersection<R>(s, seeds, h, rayOrigin, rayDir);
+
+    const bool useEmissive = !s.emissive.empty();
+    for (;;) {
+        // handleHit (PTUtils.slang:253-341).
+        if (wc) wc->hits++;
+        Hit th;
+        th.valid = true;
+        th.instanceID = is.instanceID;
+        th.primitiveIndex = is.primIndex;
+        th.baryX = is.b[1];
+        th.baryY = is.b[2];
+        ShadingData<float> sd = load_shading_data<float>(s, th, rayDir);
+        {
+            // loadShadingData: sd.frame = createSafe(isect.normalW, float4(isect.tangentW, v.tangentW.w)).
+            uint32_t vi[3];
+            s.getTriangleVertexIndices(is.instanceID, is.primIndex, vi);
+            const float bw[3] = {1.f - is.b[1] - is.b[2], is.b[1], is.b[2]};
+            float tw = s.getVertex(vi[0]).tangent[3] * bw[0];
+            tw += s.getVertex(vi[1]).tangent[3] * bw[1];
+            tw += s.getVertex(vi[2]).tangent[3] * bw[2];
+            tw = sgn(tw);
+            sd.N = normalize(is.normalW);
+            const V3<float> tg = is.tangentW;
+            const float NdotT = dot(tg, sd.N);
+            const bool nonParallel = std::fabs(NdotT) < 0.9999f;
+            const bool nonZero = dot(tg, tg) > 0.f;
+            const bool valid = std::fabs(tw) == 1.f && nonZero && nonParallel;
+            if (valid) {
+                sd.T = normalize(tg - sd.N * NdotT);
+                sd.B = cross(sd.N, sd.T) * tw;
+            } else {
+                sd.T = perp_stark(sd.N);
+                sd.B = cross(sd.N, sd.T);
+            }
+        }
+        const MaterialInstance<float> miV = war_material<float>(s, WarSeeds(), sd, p.lambert != 0);
+        const MaterialInstance<R> miR = war_material<R>(s, seeds, sd, p.lambert != 0);
+        const ShadingData<R> sdR = sd_lift<R>(sd);
+
+        const bool isPrimaryHit = path.length == 0;
+        const bool computeEmissive = isPrimaryHit || (useEmissive && (!p.useNEE || p.useMIS));
+        if (computeEmissive && any_pos(miV.emission)) {
+            float misWeight = 1.f;
+            if (!isPrimaryHit && useEmissive && p.useNEE && p.useMIS) {
+                const uint32_t tri = s.emissiveIndex(is.instanceID, is.primIndex);
+                const float lightPdf = emissive_eval_pdf<float>(s, 0, rayOrigin, tri, sd.posW, sd.orientedFaceN());
+                misWeight = war_mis(1.f, path.pdf, 1.f, lightPdf);
+            }
+            path.radiance += (path.thp * lift3<R>(miV.emission)) * R(misWeight);
+        }
+        if (path.length >= p.maxBounces + 1) { path.terminated = true; break; }
+
+        if (p.useNEE && useEmissive) {
+            // generateEmissiveSample (PTUtils.slang:177-207), not differentiable.
+            TriLightSample<float> tls;
+            const V3<float> posV = val3(is.posW);
+            if (emissive_sample_light<float>(s, 0, posV, sg, tls)) {
+                V3<float> Li = tls.pdf > 0.f ? tls.Le / tls.pdf : V3<float>(0.f);
+                V3<float> lightPos = compute_ray_origin(tls.posW, tls.normalW);
+                V3<float> origin = compute_ray_origin(posV, is.normalW);
+                V3<float> toLight = lightPos - origin;
+                float distance = length(toLight);
+                V3<float> ldir = normalize(toLight);
+                if (any_pos(Li)) {
+                    if (wc) wc->rays++;
+                    const bool visible = s.traceVisibility(origin, ldir, 0.f, distance, nullptr);
+                    if (visible) {
+                        // computeNEE (PTUtils.slang:211-249).
+                        V3<R> wo = lift3<R>(tls.posW) - is.posW;
+                        R dist = length(wo);
+                        wo /= dist;
+                        V3<R> thp = path.thp;
+                        R a2s = (dist * dist) / dot(lift3<R>(tls.normalW), -wo);
+                        V3<R> bsdfValue = miR.eval(sdR, wo);
+                        V3<R> weight = ((lift3<R>(Li) * bsdfValue) * a2s) / detach(a2s);
+                        if (p.useMIS) {
+                            const float scatterPdf = miV.evalPdf(sd, ldir, p.useBSDFSampling != 0);
+                            weight *= R(war_mis(1.f, tls.pdf, 1.f, scatterPdf));
+                        }
+                        path.radiance += thp * weight;
+                    }
+                }
+            }
+        }
+
+        // generateScatterRay (PTUtils.slang:136-172).
+        BSDFSampleOut<float> bs;
+        if (!(miV.sample(sd, sg, bs, p.useBSDFSampling != 0) && bs.pdf > 0.f)) { path.terminated = true; break; }
+        rayDir = bs.wo;
+        rayOrigin = compute_ray_origin(val3(is.posW), sd.frontFacing ? sd.faceN : -sd.faceN);
+        V3<R> bsdfWeight = miR.eval(sdR, lift3<R>(bs.wo)) / R(bs.pdf);
+        path.thp *= bsdfWeight;
+        path.normal = sd.orientedFaceN();
+        path.pdf = bs.pdf;
+        if (!any_pos(path.thp)) { path.terminated = true; break; }
+        path.length++;
+
+        if (wc) wc->rays++;
+        h = s.traceClosest(rayOrigin, rayDir, 0.f, std::numeric_limits<float>::max(), nullptr);
+        if (!h.valid) break;
+        is = war_intersection<R>(s, seeds, h, rayOrigin, rayDir);
+    }
+    return path.radiance;
+}
+
+void wardiff_pixel(const Scene& s, const WarDiffParams& p, const WarSeeds& seeds, int mode, uint32_t x, uint32_t y,
+                   const float* dLdI, float* colorOut, double* gradAcc, double* pertOut, WarCounters* wc) {
+    if (mode == 0) {
+        V3<float> L = war_trace_path<float>(s, p, seeds, x, y, wc);
+        if (colorOut) { colorOut[0] = L.x; colorOut[1] = L.y; colorOut[2] = L.z; colorOut[3] = 1.f; }
+    } else if (mode == 1) {
+        V3<Dual<4>> L = war_trace_path<Dual<4>>(s, p, seeds, x, y, wc);
+        if (colorOut) { colorOut[0] = float(L.x.v); colorOut[1] = float(L.y.v); colorOut[2] = float(L.z.v); colorOut[3] = 1.f; }
+        if (gradAcc && dLdI)
+            for (int k = 0; k < 4 && k < seeds.K; k++)
+                gradAcc[k] += double(dLdI[0]) * L.x.d[k] + double(dLdI[1]) * L.y.d[k] + double(dLdI[2]) * L.z.d[k];
+    } else {
+        V3<Shadow> L = war_trace_path<Shadow>(s, p, seeds, x, y, wc);
+        if (pertOut) { pertOut[0] = L.x.p; pertOut[1] = L.y.p; pertOut[2] = L.z.p; }
+        if (colorOut) { colorOut[0] = float(L.x.b); colorOut[1] = float(L.y.b); colorOut[2] = float(L.z.b); colorOut[3] = 1.f; }
+    }
+}
