@@ -117,6 +117,9 @@ void set_defaults(fpt_pass& p) {
         // InverseOptimizationParams (set_mesh_to_optimize).
         d["runBackward"] = PropValue::num(1);
         d["meshToOptimize"] = PropValue::num(0);
+        // "Wavefront" (default) or "Megakernel" (one thread per pixel); paths per wave.
+        d["scheduler"] = PropValue::str("Wavefront");
+        d["wavefrontCapacity"] = PropValue::num(1 << 22);
     }
 }
 

@@ -1,0 +1,434 @@
+// war_wavefront.cu -- wavefront scheduler of the WARDiffPathTracer primal
+// and adjoint (the default; the per-pixel megakernel in wardiff.cu is the
+// "Megakernel" scheduler).
+//
+// The frame's paths (one per pixel, WARDiffPathTracer.rt.slang:115-143) run in
+// waves whose state lives in the structure-of-arrays buffers of the PathTracer
+// wavefront.  Per bounce:
+//   extend    closest-hit traversal with dynamic ray fetch (shared with the PathTracer)
+//   shade     handleHit (PTUtils.slang:253-341): emission, the uniform light
+//             sample, the scatter sample; pushes the visibility ray and the
+//             continuing path
+//   shadow    any-hit traversal; adds thp * weight when unoccluded
+//   nee_grad  (adjoint) applies the NEE gradients of the visible samples
+// The adjoint re-traces the frame from its seeds (path replay: the primal
+// stores nothing).  The shade kernel writes, per path vertex, the record the
+// scatter term needs (local directions, throughput, pdf, BSDF weight and the
+// vertex's radiance increments); after the last bounce a sweep kernel walks
+// each path's records backwards with the throughput adjoint
+//     A_k = dLdI * e_k + A_{k+1} * w_k,   dS/df_k(ws) = A_{k+1} * thp_k / pdf_k.
+// The NEE term's adjoint is dLdI itself, so its gradients are formed in the
+// shade kernel and applied when the visibility ray finds the light unoccluded.
+#include <algorithm>
+
+#include "passes.h"
+#include "scene_device.h"
+#include "war_common.cuh"
+#include "war_wavefront.h"
+#include "wavefront_common.cuh"
+
+namespace fpt {
+
+namespace {
+
+// Adjoint scratch layout (float4 arrays of `capacity` entries):
+//   pending NEE gradients: 7 arrays, records: kRecArrays per vertex.
+constexpr int kNeeArrays = 7;
+constexpr int kRecArrays = 5;
+
+struct WarWave {
+    uint32_t waveFirstPixel, wavePixels, capacity;
+    float4* nee;        // kNeeArrays x capacity
+    float4* rec;        // maxVertices x kRecArrays x capacity
+    uint32_t* nv;       // records per path
+    uint32_t maxVertices;
+};
+
+FPT_D float4& nee_at(const WarWave& ww, int j, uint32_t i) { return ww.nee[size_t(j) * ww.capacity + i]; }
+FPT_D float4& rec_at(const WarWave& ww, uint32_t k, int j, uint32_t i) {
+    return ww.rec[(size_t(k) * kRecArrays + j) * ww.capacity + i];
+}
+
+// Seeds the wave: camera ray of pixel waveFirstPixel + i (tracePaths,
+// WARDiffPathTracer.rt.slang:115-143 and tracePath :75-112).
+template <bool BWD>
+__global__ void __launch_bounds__(kShadeBlock) ww_generate(DevScene s, WarParams p, WaveParams wp, SoA w, WarWave ww) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePixels; i += gridDim.x * blockDim.x) {
+        const uint32_t pid = wp.waveFirstPixel + i;
+        const uint32_t x = pid % p.width, y = pid / p.width;
+        UniformSG sg;
+        sg.init(x, y, p.frameSeed / 2);
+        next2D(sg);
+        next2D(sg);
+        next2D(sg);
+        const float2 u = next2D(sg);
+        const float r = sqrtf(-2.f * logf(u.x));
+        const float ang = 6.28318530717958647692f * u.y;
+        float jx = (r * cosf(ang)) * 0.5f, jy = (r * sinf(ang)) * 0.5f;
+        if (p.useAntithetic && p.frameSeed % 2 == 0) { jx = -jx; jy = -jy; }
+        const float px = (float(x) + 0.5f) + jx, py = (float(y) + 0.5f) + jy;
+        const float qx = px / float(p.width), qy = py / float(p.height);
+        const float ndcx = 2.f * qx + -1.f, ndcy = -2.f * qy + 1.f;
+        const float3 dirU = load3(s.camera.cameraU) * ndcx + load3(s.camera.cameraV) * ndcy + load3(s.camera.cameraW);
+        const float len = length(dirU);
+        const float3 d = len > 0.f ? dirU / len : f3(0.f);
+        const float3 o = load3(s.camera.posW);
+        w.originPdf[i] = make_float4(o.x, o.y, o.z, 0.f);
+        w.dirV[i] = make_float4(d.x, d.y, d.z, __uint_as_float(PF_ACTIVE));
+        w.thpB[i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(0u));
+        w.L[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        store_sg(w.sg[i], sg);
+        wp.extQueue[i] = i;
+        if (BWD) ww.nv[i] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        wp.counts[1] = wp.wavePixels;
+        if (p.counters) {
+            atomicAdd(p.counters + 0, (unsigned long long)wp.wavePixels);
+        }
+    }
+}
+
+// handleHit for every path of the shade queue whose extension ray hit.
+template <bool HAS_T, bool BWD>
+__global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p, WaveParams wp, SoA w, WarWave ww) {
+    Counters cnt;
+    const bool useEmissive = s.hasEmissive != 0 && s.activeCount > 0;
+    const uint32_t n = wp.counts[0];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = wp.shadeQueue[k];
+        const float4 od = w.originPdf[i], dv = w.dirV[i];
+        const uint32_t fv = __float_as_uint(dv.w);
+        if (!(fv & 0x2u)) continue;  // the extension ray missed: the path is done (no environment light)
+        const uint32_t pid = wp.waveFirstPixel + i;
+        float3 rayOrigin = make_float3(od.x, od.y, od.z), rayDir = make_float3(dv.x, dv.y, dv.z);
+        const float pathPdf = od.w;
+        const float4 tb = w.thpB[i];
+        float3 thp = make_float3(tb.x, tb.y, tb.z);
+        uint32_t pathLen = __float_as_uint(tb.w);
+        float4 Lr = w.L[i];
+        float3 radiance = make_float3(Lr.x, Lr.y, Lr.z);
+        UniformSG sg;
+        load_sg(w.sg[i], sg);
+        const uint4 hr = w.hit[i];
+        HitRec h;
+        h.instanceID = hr.x;
+        h.primIndex = hr.y;
+        h.baryX = __uint_as_float(hr.z);
+        h.baryY = __uint_as_float(hr.w);
+        h.valid = true;
+        cnt.v[6]++;
+        const WarIsect is = war_intersect(s, h, rayOrigin, rayDir);
+        const ShadingData sd = war_shading_data(s, is, rayDir);
+        const MaterialInstance<HAS_T> mi = material_instance<HAS_T>(s, sd, p.lambert != 0);
+        float3 g = f3(0.f), e = f3(0.f);
+        uint32_t vk = 0;
+        if (BWD) {
+            g = make_float3(p.dLdI[3 * size_t(pid)], p.dLdI[3 * size_t(pid) + 1], p.dLdI[3 * size_t(pid) + 2]);
+            vk = ww.nv[i];
+            ww.nv[i] = vk + 1;
+            rec_at(ww, vk, 0, i) = make_float4(0.f, 0.f, 0.f, 1.f);  // wiL, pdf
+            rec_at(ww, vk, 1, i) = make_float4(0.f, 0.f, 0.f, __uint_as_float(sd.materialID));
+            rec_at(ww, vk, 2, i) = make_float4(thp.x, thp.y, thp.z, __uint_as_float(sd.frontFacing ? 1u : 0u));
+            rec_at(ww, vk, 3, i) = make_float4(0.f, 0.f, 0.f, 0.f);  // bw
+        }
+        const bool isPrimaryHit = pathLen == 0;
+        const bool computeEmissive = isPrimaryHit || (useEmissive && (!p.useNEE || p.useMIS));
+        if (computeEmissive && any_pos(mi.emission)) {
+            float misWeight = 1.f;
+            if (!isPrimaryHit && useEmissive && p.useNEE && p.useMIS) {
+                const uint32_t off = __ldg(s.instEmissiveOffset + is.inst);
+                const uint32_t tri = off == 0xffffffffu ? 0xffffffffu : off + is.prim;
+                const float lightPdf = emissive_eval_pdf(s, 0, rayOrigin, tri, sd.posW, sd_oriented_face_n(sd));
+                misWeight = war_mis(1.f, pathPdf, 1.f, lightPdf);
+            }
+            radiance += (thp * mi.emission) * misWeight;
+            if (BWD) e += mi.emission * misWeight;
+        }
+        bool cont = false, shadowRay = false;
+        if (pathLen < p.maxBounces + 1) {
+            if (p.useNEE && useEmissive) {
+                TriLightSample tls;
+                cnt.v[7]++;
+                if (emissive_sample(s, 0, is.posW, sg, tls)) {
+                    const float3 Li = tls.pdf > 0.f ? tls.Le / tls.pdf : f3(0.f);
+                    const float3 lightPos = compute_ray_origin(tls.posW, tls.normalW);
+                    const float3 origin = compute_ray_origin(is.posW, is.normalW);
+                    const float3 toLight = lightPos - origin;
+                    const float distance = length(toLight);
+                    const float3 ldir = normalize(toLight);
+                    if (any_pos(Li)) {
+                        // computeNEE (PTUtils.slang:211-249); applied if the light is visible.
+                        float3 wo = tls.posW - is.posW;
+                        const float dist = length(wo);
+                        wo /= dist;
+                        const float a2s = (dist * dist) / dot(tls.normalW, -wo);
+                        const float3 bsdfValue = mi.eval(sd, wo);
+                        float3 weight = ((Li * bsdfValue) * a2s) / a2s;
+                        float mis = 1.f;
+                        if (p.useMIS) {
+                            const float scatterPdf = mi.evalPdf(sd, ldir, p.useBSDFSampling != 0);
+                            mis = war_mis(1.f, tls.pdf, 1.f, scatterPdf);
+                            weight *= mis;
+                        }
+                        const float3 contrib = thp * weight;
+                        w.sOrigin[i] = make_float4(origin.x, origin.y, origin.z, distance);
+                        w.sDir[i] = make_float4(ldir.x, ldir.y, ldir.z, 0.f);
+                        w.sLr[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
+                        shadowRay = true;
+                        if (BWD) {
+                            float G[11];
+#pragma unroll
+                            for (int q = 0; q < 11; q++) G[q] = 0.f;
+                            float3 dP = f3(0.f);
+                            const float3 wiL = mi.toLocal(sd.V), woL = mi.toLocal(wo);
+                            if (mi.valid_hemisphere(sd, wiL, woL, wo)) {
+                                const MatParams mp = load_mat_params(s, sd.materialID);
+                                const DV3<14> J = eval_jacobian<14, HAS_T>(mi, mp, sd.frontFacing, wiL, woL);
+                                const float3 Gf = ((g * thp) * Li) * mis;
+#pragma unroll
+                                for (int q = 0; q < 11; q++) G[q] = Gf.x * J.x.d[q] + Gf.y * J.y.d[q] + Gf.z * J.z.d[q];
+                                if (p.gradPos && is.inst == p.meshID) {
+                                    const float3 gL = make_float3(Gf.x * J.x.d[11] + Gf.y * J.y.d[11] + Gf.z * J.z.d[11],
+                                                                  Gf.x * J.x.d[12] + Gf.y * J.y.d[12] + Gf.z * J.z.d[12],
+                                                                  Gf.x * J.x.d[13] + Gf.y * J.y.d[13] + Gf.z * J.z.d[13]);
+                                    const float3 gwo = mi.T * gL.x + mi.B * gL.y + mi.N * gL.z;
+                                    const float gRatio = dot(Gf, make_float3(J.x.v, J.y.v, J.z.v));
+                                    const float nlwo = dot(tls.normalW, wo);
+                                    dP = (gwo - wo * dot(wo, gwo)) * (-1.f / dist);
+                                    dP += (wo * (-3.f / dist) + tls.normalW * (1.f / (dist * nlwo))) * gRatio;
+                                }
+                            }
+                            const bool posGrad = p.gradPos && is.inst == p.meshID;
+                            nee_at(ww, 0, i) = make_float4(G[0], G[1], G[2], G[3]);
+                            nee_at(ww, 1, i) = make_float4(G[4], G[5], G[6], G[7]);
+                            nee_at(ww, 2, i) = make_float4(G[8], G[9], G[10], __uint_as_float(sd.materialID));
+                            nee_at(ww, 3, i) = make_float4(dP.x, dP.y, dP.z, __uint_as_float(posGrad ? 1u : 0u));
+                            nee_at(ww, 4, i) = make_float4(is.b[0], is.b[1], is.b[2], __uint_as_float(is.local[0]));
+                            nee_at(ww, 5, i) = make_float4(__uint_as_float(is.local[1]), __uint_as_float(is.local[2]), 0.f, 0.f);
+                            nee_at(ww, 6, i) = make_float4(weight.x, weight.y, weight.z, 0.f);
+                        }
+                    }
+                }
+            }
+            // generateScatterRay (PTUtils.slang:136-172).
+            float3 wo, wgt;
+            float pdf;
+            uint32_t lobe;
+            if (mi.sample(sd, sg, wo, wgt, pdf, lobe, p.useBSDFSampling != 0) && pdf > 0.f) {
+                rayDir = wo;
+                rayOrigin = compute_ray_origin(is.posW, sd.frontFacing ? sd.faceN : -sd.faceN);
+                const float3 bsdfWeight = mi.eval(sd, wo) / pdf;
+                if (BWD) {
+                    const float3 wiL = mi.toLocal(sd.V), wsL = mi.toLocal(wo);
+                    const bool valid = mi.valid_hemisphere(sd, wiL, wsL, wo);
+                    rec_at(ww, vk, 0, i) = make_float4(wiL.x, wiL.y, wiL.z, pdf);
+                    rec_at(ww, vk, 1, i) = make_float4(wsL.x, wsL.y, wsL.z, __uint_as_float(sd.materialID));
+                    rec_at(ww, vk, 2, i) = make_float4(thp.x, thp.y, thp.z,
+                                                       __uint_as_float((sd.frontFacing ? 1u : 0u) | (valid ? 2u : 0u)));
+                    rec_at(ww, vk, 3, i) = make_float4(bsdfWeight.x, bsdfWeight.y, bsdfWeight.z, 0.f);
+                }
+                thp *= bsdfWeight;
+                if (any_pos(thp)) {
+                    pathLen++;
+                    cont = true;
+                }
+                w.originPdf[i] = make_float4(rayOrigin.x, rayOrigin.y, rayOrigin.z, pdf);
+                w.dirV[i] = make_float4(rayDir.x, rayDir.y, rayDir.z, __uint_as_float(fv & ~0x2u));
+            }
+        }
+        push(shadowRay, i, wp.shadowQueue, wp.counts + 2);
+        if (BWD) rec_at(ww, vk, 4, i) = make_float4(e.x, e.y, e.z, 0.f);
+        if (BWD && vk + 1 >= ww.maxVertices) cont = false;  // guarded by the host
+        w.thpB[i] = make_float4(thp.x, thp.y, thp.z, __uint_as_float(pathLen));
+        w.L[i] = make_float4(radiance.x, radiance.y, radiance.z, 0.f);
+        store_sg(w.sg[i], sg);
+        push(cont, i, wp.extQueue, wp.counts + 1);
+    }
+    flush_counters(p.counters, cnt);
+}
+
+// Applies the NEE gradients of the samples whose visibility ray found the
+// light unoccluded (sLr.w set by the shadow kernel) and adds the NEE weight to
+// the vertex's radiance increment.
+__global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(WarParams p, WaveParams wp, SoA w, WarWave ww) {
+    const uint32_t n = wp.counts[2];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = wp.shadowQueue[k];
+        if (w.sLr[i].w != 1.f) continue;
+        const uint32_t pid = wp.waveFirstPixel + i;
+        const float4 a = nee_at(ww, 0, i), b = nee_at(ww, 1, i), c = nee_at(ww, 2, i);
+        const float G[11] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z};
+        const uint32_t matID = __float_as_uint(c.w);
+        if (p.gradMat && matID * kMatParams + 11 <= p.matDim) {
+            float* gm = p.gradMat + size_t(war_hash(pid, p.matHash)) * p.matDim + matID * kMatParams;
+#pragma unroll
+            for (int q = 0; q < 11; q++)
+                if (G[q] != 0.f) atomicAdd(gm + q, G[q]);
+        }
+        const float4 d = nee_at(ww, 3, i);
+        if (p.gradPos && __float_as_uint(d.w)) {
+            const float4 bb = nee_at(ww, 4, i), ll = nee_at(ww, 5, i);
+            const float bw[3] = {bb.x, bb.y, bb.z};
+            const uint32_t loc[3] = {__float_as_uint(bb.w), __float_as_uint(ll.x), __float_as_uint(ll.y)};
+            float* gp = p.gradPos + size_t(war_hash(pid, p.posHash)) * p.posDim;
+#pragma unroll
+            for (int v = 0; v < 3; v++) {
+                const uint32_t o = loc[v] * 3;
+                if (o + 3 > p.posDim) continue;
+                atomicAdd(gp + o, bw[v] * d.x);
+                atomicAdd(gp + o + 1, bw[v] * d.y);
+                atomicAdd(gp + o + 2, bw[v] * d.z);
+            }
+        }
+        const float4 wt = nee_at(ww, 6, i);
+        const uint32_t vk = ww.nv[i] - 1;
+        float4& e = rec_at(ww, vk, 4, i);
+        e.x += wt.x;
+        e.y += wt.y;
+        e.z += wt.z;
+    }
+}
+
+// Reverse sweep over each path's scatter records.
+template <bool HAS_T>
+__global__ void __launch_bounds__(kShadeBlock) ww_sweep(DevScene s, WarParams p, WaveParams wp, WarWave ww) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePixels; i += gridDim.x * blockDim.x) {
+        const uint32_t pid = wp.waveFirstPixel + i;
+        const float3 g = make_float3(p.dLdI[3 * size_t(pid)], p.dLdI[3 * size_t(pid) + 1], p.dLdI[3 * size_t(pid) + 2]);
+        const uint32_t hash = war_hash(pid, p.matHash);
+        float3 A = f3(0.f);
+        for (int k = int(ww.nv[i]) - 1; k >= 0; k--) {
+            const float4 r0 = rec_at(ww, k, 0, i), r1 = rec_at(ww, k, 1, i), r2 = rec_at(ww, k, 2, i);
+            const float4 r3 = rec_at(ww, k, 3, i), r4 = rec_at(ww, k, 4, i);
+            const uint32_t flags = __float_as_uint(r2.w);
+            const float3 thp = make_float3(r2.x, r2.y, r2.z);
+            if ((flags & 2u) && (A.x != 0.f || A.y != 0.f || A.z != 0.f)) {
+                const uint32_t matID = __float_as_uint(r1.w);
+                const MatParams mp = load_mat_params(s, matID);
+                ShadingData sd;
+                sd.frontFacing = (flags & 1u) != 0;
+                sd.materialID = matID;
+                const MaterialInstance<HAS_T> mi = material_instance<HAS_T>(s, sd, p.lambert != 0);
+                const DV3<11> J = eval_jacobian<11, HAS_T>(mi, mp, sd.frontFacing, make_float3(r0.x, r0.y, r0.z),
+                                                          make_float3(r1.x, r1.y, r1.z));
+                const float3 Gs = (A * thp) / r0.w;
+                add_material_grads<11>(p, hash, matID, J, Gs);
+            }
+            A = A * make_float3(r3.x, r3.y, r3.z) + g * make_float3(r4.x, r4.y, r4.z);
+        }
+    }
+}
+
+__global__ void ww_resolve(WarParams p, WaveParams wp, SoA w) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePixels; i += gridDim.x * blockDim.x) {
+        const float4 L = w.L[i];
+        p.color[wp.waveFirstPixel + i] = make_float4(L.x, L.y, L.z, 1.f);
+    }
+}
+
+__global__ void ww_advance(WaveParams wp) {
+    wp.counts[0] = wp.counts[1];
+    wp.counts[1] = 0;
+    wp.counts[2] = 0;
+    wp.counts[kFetchExtend] = 0;
+    wp.counts[kFetchShadow] = 0;
+}
+
+__global__ void __launch_bounds__(kTraceBlock, FPT_TRACE_MIN_BLOCKS) ww_extend(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    __shared__ uint2 stackMem[kStackSize * kTraceBlock];
+    trace_queue<false>(s, p, wp, w, stackMem + threadIdx.x);
+}
+template <bool MARK>
+__global__ void __launch_bounds__(kTraceBlock, FPT_TRACE_MIN_BLOCKS) ww_shadow(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    __shared__ uint2 stackMem[kStackSize * kTraceBlock];
+    trace_queue<true, MARK>(s, p, wp, w, stackMem + threadIdx.x);
+}
+
+template <bool HAS_T, bool BWD>
+cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adj, cudaStream_t st,
+                              uint32_t& launches) {
+    SoA w;
+    w.originPdf = b.f4(0); w.dirV = b.f4(1); w.thpB = b.f4(2); w.L = b.f4(3);
+    w.sg = reinterpret_cast<uint4*>(b.f4(4)); w.hit = reinterpret_cast<uint4*>(b.f4(5));
+    w.sOrigin = b.f4(6); w.sDir = b.f4(7); w.sLr = b.f4(8);
+    w.sampleL = b.sampleL;
+    WarWave ww{};
+    ww.capacity = b.capacity;
+    ww.maxVertices = p.maxBounces + 2;
+    if (BWD) {
+        char* q = static_cast<char*>(adj);
+        ww.nee = reinterpret_cast<float4*>(q);
+        q += size_t(kNeeArrays) * b.capacity * sizeof(float4);
+        ww.rec = reinterpret_cast<float4*>(q);
+        q += size_t(ww.maxVertices) * kRecArrays * b.capacity * sizeof(float4);
+        ww.nv = reinterpret_cast<uint32_t*>(q);
+    }
+    // Trace kernels read the ray counters through FrameParams.
+    FrameParams fp{};
+    fp.counters = p.counters;
+    static int gShade = 0, gTrace = 0, gSweep = 0;
+    if (!gShade) {
+        gShade = blocks_for(reinterpret_cast<const void*>(ww_shade<HAS_T, BWD>), kShadeBlock);
+        gTrace = blocks_for(reinterpret_cast<const void*>(ww_extend), kTraceBlock);
+        gSweep = BWD ? blocks_for(reinterpret_cast<const void*>(ww_sweep<HAS_T>), kShadeBlock) : 1;
+    }
+    const uint32_t pixels = p.width * p.height;
+    const uint32_t maxIter = p.maxBounces + 2;
+    launches = 0;
+    for (uint32_t first = 0; first < pixels; first += b.capacity) {
+        WaveParams wp;
+        wp.waveFirstPixel = first;
+        wp.wavePixels = std::min(b.capacity, pixels - first);
+        wp.wavePaths = wp.wavePixels;
+        wp.counts = b.counts;
+        cudaError_t e = cudaMemsetAsync(b.counts, 0, kNumWaveCounts * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return e;
+        uint32_t* qa = b.queueA;
+        uint32_t* qb = b.queueB;
+        wp.shadeQueue = qa;
+        wp.extQueue = qb;
+        wp.shadowQueue = b.shadowQueue;
+        const int genBlocks = std::min<int>(gShade, int((wp.wavePixels + kShadeBlock - 1) / kShadeBlock));
+        ww_generate<BWD><<<genBlocks, kShadeBlock, 0, st>>>(s, p, wp, w, ww);
+        launches++;
+        for (uint32_t it = 0; it < maxIter; it++) {
+            ww_extend<<<gTrace, kTraceBlock, 0, st>>>(s, fp, wp, w);
+            ww_advance<<<1, 1, 0, st>>>(wp);
+            std::swap(qa, qb);
+            wp.shadeQueue = qa;
+            wp.extQueue = qb;
+            ww_shade<HAS_T, BWD><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w, ww);
+            ww_shadow<BWD><<<gTrace, kTraceBlock, 0, st>>>(s, fp, wp, w);
+            launches += 4;
+            if (BWD) {
+                ww_nee_grad<<<gShade, kShadeBlock, 0, st>>>(p, wp, w, ww);
+                launches++;
+            }
+        }
+        if (BWD) ww_sweep<HAS_T><<<std::min<int>(gSweep, int((wp.wavePixels + kShadeBlock - 1) / kShadeBlock)), kShadeBlock, 0, st>>>(s, p, wp, ww);
+        else ww_resolve<<<(wp.wavePixels + 255) / 256, 256, 0, st>>>(p, wp, w);
+        launches++;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces) {
+    const size_t maxVertices = size_t(maxBounces) + 2;
+    return (size_t(kNeeArrays) + maxVertices * kRecArrays) * capacity * sizeof(float4) + size_t(capacity) * sizeof(uint32_t);
+}
+
+cudaError_t launch_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adjointScratch, bool backward,
+                                 cudaStream_t st, uint32_t& launches) {
+    if (s.hasTransmission)
+        return backward ? run_war_wavefront<true, true>(s, p, b, adjointScratch, st, launches)
+                        : run_war_wavefront<true, false>(s, p, b, adjointScratch, st, launches);
+    return backward ? run_war_wavefront<false, true>(s, p, b, adjointScratch, st, launches)
+                    : run_war_wavefront<false, false>(s, p, b, adjointScratch, st, launches);
+}
+
+}  // namespace fpt

@@ -1,0 +1,32 @@
+// war_wavefront.h -- launch parameters of the WARDiffPathTracer kernels and
+// the wavefront launcher (war_wavefront.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device_scene.cuh"
+#include "wavefront.h"
+
+namespace fpt {
+
+struct WarParams {
+    uint32_t width, height, maxBounces;
+    uint32_t useBSDFSampling, useNEE, useMIS, useAntithetic;
+    uint32_t frameSeed, lambert, meshID;
+    float4* color;               // primal output
+    const float* dLdI;           // float3 per pixel (adjoint)
+    float* gradMat;              // [hash][matDim]
+    uint32_t matDim, matHash;
+    float* gradPos;              // [hash][posDim]
+    uint32_t posDim, posHash;
+    unsigned long long* counters;  // [0] paths, [1] rays
+};
+
+// Bytes of adjoint scratch (pending NEE gradients + per-vertex records) for a
+// wave of `capacity` paths.
+size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces);
+// Primal (backward = false) or adjoint of one frame; `launches` counts kernels.
+cudaError_t launch_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adjointScratch, bool backward,
+                                 cudaStream_t st, uint32_t& launches);
+
+}  // namespace fpt

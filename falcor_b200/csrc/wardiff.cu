@@ -36,6 +36,7 @@
 #include "passes.h"
 #include "scene_device.h"
 #include "wardiff.h"
+#include "war_common.cuh"
 
 namespace fpt {
 
@@ -44,165 +45,6 @@ using namespace dev;
 namespace {
 
 constexpr int kWarBlock = 128;
-constexpr int kMaxWarVertices = 16;   // maxBounces <= 14 in the adjoint
-constexpr uint32_t kMatParams = 20;   // DiffMaterialData::kMaterialParamCount
-
-struct WarParams {
-    uint32_t width, height, maxBounces;
-    uint32_t useBSDFSampling, useNEE, useMIS, useAntithetic;
-    uint32_t frameSeed, lambert, meshID;
-    float4* color;               // primal output
-    const float* dLdI;           // float3 per pixel (adjoint)
-    float* gradMat;              // [hash][matDim]
-    uint32_t matDim, matHash;
-    float* gradPos;              // [hash][posDim]
-    uint32_t posDim, posHash;
-    unsigned long long* counters;  // [0] paths, [1] rays
-};
-
-// Intersection recomputed from the hit triangle (DiffSceneQuery.slang:148-219).
-struct WarIsect {
-    uint32_t inst, prim;
-    float b[3];
-    float3 posW;
-    float3 normalW, tangentW;    // interpolated, unnormalised
-    float tw;                    // sign of the interpolated tangent w
-    uint32_t local[3];           // vertex indices within the mesh
-};
-
-FPT_D float war_ray_distance(float3 v0, float3 v1, float3 v2, float3 o, float3 d) {
-    const float3 e1 = v1 - v0, e2 = v2 - v0;
-    const float3 pvec = cross(d, e2);
-    const float det = dot(e1, pvec);
-    const float3 tvec = o - v0;
-    const float3 qvec = cross(tvec, e1);
-    return dot(e2, qvec) / det;
-}
-
-FPT_D WarIsect war_intersect(const DevScene& s, const HitRec& h, float3 o, float3 d) {
-    WarIsect is;
-    is.inst = h.instanceID;
-    is.prim = h.primIndex;
-    const DevInstance inst = s.instances[h.instanceID];
-    const uint32_t* ip = s.indices + inst.ibOffset + h.primIndex * 3;
-    is.local[0] = __ldg(ip);
-    is.local[1] = __ldg(ip + 1);
-    is.local[2] = __ldg(ip + 2);
-    const PackedVertex pv0 = load_vertex(s.vertices, is.local[0] + inst.vbOffset);
-    const PackedVertex pv1 = load_vertex(s.vertices, is.local[1] + inst.vbOffset);
-    const PackedVertex pv2 = load_vertex(s.vertices, is.local[2] + inst.vbOffset);
-    float3 v0, v1, v2, n0, n1, n2;
-    unpack_vertex(pv0, v0, n0);
-    unpack_vertex(pv1, v1, n1);
-    unpack_vertex(pv2, v2, n2);
-    // computeBarycentrics of the ray/triangle-plane point (GeometryHelpers.slang:442-482).
-    const float t = war_ray_distance(v0, v1, v2, o, d);
-    const float3 p = o + d * t;
-    const float3 e0 = v0 - p, e1 = v1 - p, e2 = v2 - p;
-    const float a0 = length(cross(e1, e2));
-    const float a1 = length(cross(e2, e0));
-    const float a2 = length(cross(e0, e1));
-    const float area = a0 + a1 + a2;
-    is.b[0] = a0 / area;
-    is.b[1] = a1 / area;
-    is.b[2] = a2 / area;
-    is.posW = v0 * is.b[0] + v1 * is.b[1] + v2 * is.b[2];
-    // loadVertexNormalsW / loadVertexTangentsW (DiffSceneIO.slang:145-258), identity world matrices.
-    n0 = normalize(n0); n1 = normalize(n1); n2 = normalize(n2);
-    const float3 t0 = normalize(decode_normal2x16(pv0.tangentOct)), t1 = normalize(decode_normal2x16(pv1.tangentOct)),
-                 t2 = normalize(decode_normal2x16(pv2.tangentOct));
-    is.normalW = n0 * is.b[0] + n1 * is.b[1] + n2 * is.b[2];
-    is.tangentW = t0 * is.b[0] + t1 * is.b[1] + t2 * is.b[2];
-    // VertexData.tangentW.w with the TriangleHit barycentric weights (Scene.slang:452-455).
-    const float w0 = sgn(f16(pv0.nz_tw >> 16)), w1 = sgn(f16(pv1.nz_tw >> 16)), w2 = sgn(f16(pv2.nz_tw >> 16));
-    const float bx = is.b[1], by = is.b[2];
-    float tw = w0 * (1.f - bx - by);
-    tw += w1 * bx;
-    tw += w2 * by;
-    is.tw = sgn(tw);
-    return is;
-}
-
-// loadShadingData (PTUtils.slang:97-123): the vertex data of the hit with
-// sd.frame = ShadingFrame::createSafe(isect.normalW, float4(isect.tangentW, v.tangentW.w)).
-FPT_D ShadingData war_shading_data(const DevScene& s, const WarIsect& is, float3 rayDir) {
-    HitRec th;
-    th.instanceID = is.inst;
-    th.primIndex = is.prim;
-    th.globalTri = 0;
-    th.baryX = is.b[1];
-    th.baryY = is.b[2];
-    th.t = 0.f;
-    th.valid = true;
-    ShadingData sd = load_shading_data(s, th, rayDir);
-    sd.N = normalize(is.normalW);
-    const float3 tg = is.tangentW;
-    const float NdotT = dot(tg, sd.N);
-    const bool valid = fabsf(is.tw) == 1.f && dot(tg, tg) > 0.f && fabsf(NdotT) < 0.9999f;
-    if (valid) {
-        sd.T = normalize(tg - sd.N * NdotT);
-        sd.B = cross(sd.N, sd.T) * is.tw;
-    } else {
-        sd.T = perp_stark(sd.N);
-        sd.B = cross(sd.N, sd.T);
-    }
-    return sd;
-}
-
-// evalMIS, power-two heuristic (PTUtils.slang:87-93).
-FPT_D float war_mis(float n0, float p0, float n1, float p1) {
-    const float q0 = (n0 * p0) * (n0 * p0);
-    const float q1 = (n1 * p1) * (n1 * p1);
-    return q0 / (q0 + q1);
-}
-
-// Raw material parameters (StandardMaterialParamLayout order) of a material.
-struct MatParams {
-    float3 baseColor, transmission;
-    float metallic, roughness, ior, diffTrans, specTrans;
-};
-FPT_D MatParams load_mat_params(const DevScene& s, uint32_t id) {
-    const uint4* mp = reinterpret_cast<const uint4*>(s.materials + id);
-    const uint4 m0 = __ldg(mp), m2 = __ldg(mp + 2);
-    MatParams m;
-    m.baseColor = make_float3(f16(m0.x & 0xffffu), f16(m0.x >> 16), f16(m0.y & 0xffffu));
-    m.roughness = f16(m0.z >> 16);
-    m.metallic = f16(m0.w & 0xffffu);
-    m.ior = f16(m2.x & 0xffffu);
-    m.specTrans = f16(m2.x >> 16);
-    m.diffTrans = f16(m2.y & 0xffffu);
-    m.transmission = make_float3(f16(m2.y >> 16), f16(m2.z & 0xffffu), f16(m2.z >> 16));
-    return m;
-}
-
-// Jacobian of one evalAD with respect to the 11 material parameters (slots
-// 0-10) and, for N = 14, the local outgoing direction (slots 11-13).
-template <int N, bool HAS_T>
-FPT_D DV3<N> eval_jacobian(const MaterialInstance<HAS_T>& mi, const MatParams& mp, bool frontFacing, float3 wiL, float3 woL) {
-    const StandardBSDF<HAS_T> b = mi.bsdf(wiL);
-    const DBSDFData<N> d = diff_bsdf_data<N>(mp.baseColor, mp.metallic, mp.roughness, mp.ior, mp.transmission, mp.diffTrans,
-                                             mp.specTrans, frontFacing);
-    const DV3<N> wi = dv3c<N>(wiL);
-    const DV3<N> wo = dv3(dvar<N>(woL.x, 11), dvar<N>(woL.y, 12), dvar<N>(woL.z, 13));
-    return diff_bsdf_eval<N>(d, wi, wo, mi.thin, mi.activeLobes, mi.lambert, b.pDR, HAS_T ? b.pDT : 0.f, b.pSR,
-                             HAS_T ? b.pST : 0.f);
-}
-
-FPT_D uint32_t war_hash(uint32_t pixelID, uint32_t hashSize) { return jenkins_hash(pixelID) % hashSize; }
-
-// Adds sum_c G_c * J_c[i] for the 11 material parameters.
-template <int N>
-FPT_D void add_material_grads(const WarParams& p, uint32_t hash, uint32_t matID, const DV3<N>& J, float3 G) {
-    if (!p.gradMat) return;
-    const uint32_t base = matID * kMatParams;
-    if (base + 11 > p.matDim) return;
-    float* g = p.gradMat + size_t(hash) * p.matDim + base;
-#pragma unroll
-    for (int i = 0; i < 11; i++) {
-        const float v = G.x * J.x.d[i] + G.y * J.y.d[i] + G.z * J.z.d[i];
-        if (v != 0.f) atomicAdd(g + i, v);
-    }
-}
 
 struct WarVertex {
     float3 wiL, wsL, thp, bw, e;
@@ -547,14 +389,37 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
     cudaError_t e = cudaMemsetAsync(pass.scratch, 0, kNumCounters * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, "WARDiffPathTracer: counter reset failed");
     const bool hasT = scene->dev.hasTransmission != 0;
+    const bool wavefront = pass.str("scheduler") != "Megakernel";
+    if (backward || wavefront) {
+        if (p.maxBounces + 2 > uint32_t(kMaxWarVertices))
+            return set_error(FPT_ERR_UNSUPPORTED, "WARDiffPathTracer: the adjoint supports maxBounces <= 14");
+    }
     if (!backward) {
         if (!io->color) return set_error(FPT_ERR_INVALID_ARG, "WARDiffPathTracer: 'color' is required");
         p.color = reinterpret_cast<float4*>(io->color);
         if (io->d_color) cudaMemsetAsync(io->d_color, 0, size_t(p.width) * p.height * 16, st);
-        e = hasT ? launch_war<true, false>(scene->dev, p, st) : launch_war<false, false>(scene->dev, p, st);
+    }
+    if (wavefront) {
+        const uint32_t pixels = p.width * p.height;
+        const uint32_t cap = std::min<uint32_t>(pixels, uint32_t(std::max(1.0, pass.num("wavefrontCapacity"))));
+        e = pass.wavefront.ensure(cap);
+        if (e != cudaSuccess) return set_error(FPT_ERR_OOM, std::string("WARDiffPathTracer: wavefront buffers: ") + cudaGetErrorString(e));
+        if (backward) {
+            const size_t need = war_adjoint_bytes(pass.wavefront.capacity, p.maxBounces);
+            if (pass.adjointScratchBytes < need) {
+                if (pass.adjointScratch) cudaFree(pass.adjointScratch);
+                pass.adjointScratch = nullptr;
+                pass.adjointScratchBytes = 0;
+                if (cudaMalloc(&pass.adjointScratch, need) != cudaSuccess)
+                    return set_error(FPT_ERR_OOM, "WARDiffPathTracer: adjoint scratch allocation failed");
+                pass.adjointScratchBytes = need;
+            }
+        }
+    }
+    if (!backward) {
+        if (wavefront) e = launch_war_wavefront(scene->dev, p, pass.wavefront, nullptr, false, st, pass.launches);
+        else e = hasT ? launch_war<true, false>(scene->dev, p, st) : launch_war<false, false>(scene->dev, p, st);
     } else {
-        if (p.maxBounces + 2 > uint32_t(kMaxWarVertices))
-            return set_error(FPT_ERR_UNSUPPORTED, "WARDiffPathTracer: the adjoint supports maxBounces <= 14");
         if (direct) {
             p.dLdI = dLdI;
             p.gradMat = grads->material;
@@ -573,9 +438,12 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
             if (gm.active) { p.gradMat = gm.tmp; p.matDim = gm.dim; p.matHash = gm.hash; }
             if (gp.active) { p.gradPos = gp.tmp; p.posDim = gp.dim; p.posHash = gp.hash; }
         }
-        e = hasT ? launch_war<true, true>(scene->dev, p, st) : launch_war<false, true>(scene->dev, p, st);
+        p.matHash = std::max(p.matHash, 1u);
+        p.posHash = std::max(p.posHash, 1u);
+        if (wavefront) e = launch_war_wavefront(scene->dev, p, pass.wavefront, pass.adjointScratch, true, st, pass.launches);
+        else e = hasT ? launch_war<true, true>(scene->dev, p, st) : launch_war<false, true>(scene->dev, p, st);
     }
-    pass.launches = 1;
+    if (!wavefront) pass.launches = 1;
     pass.frameCount++;
     if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, std::string("WARDiffPathTracer: kernel launch failed: ") + cudaGetErrorString(e));
     return FPT_OK;

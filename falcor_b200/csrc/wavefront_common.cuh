@@ -1,0 +1,205 @@
+// wavefront_common.cuh -- structure-of-arrays path state, warp-aggregated
+// queues and the dynamic-fetch ray tracing loop shared by the wavefront
+// PathTracer (wavefront.cu) and the wavefront WARDiffPathTracer
+// (war_wavefront.cu).  Everything here has internal linkage per translation
+// unit.
+#pragma once
+
+#include "kernels.cuh"
+#include "path_logic.cuh"
+
+namespace fpt {
+namespace {
+
+using namespace dev;
+
+constexpr int kTraceBlock = 128;
+constexpr int kShadeBlock = 128;
+
+// Counts: [0] shade queue, [1] extension queue, [2] shadow queue, [4] and [5]
+// the fetch counters of the extension and visibility ray kernels.
+constexpr int kFetchExtend = 4, kFetchShadow = 5, kNumWaveCounts = 8;
+struct WaveParams {
+    uint32_t waveFirstPixel;   // first pixel of the wave
+    uint32_t wavePixels;       // pixels in the wave
+    uint32_t wavePaths;        // wavePixels * spp
+    uint32_t* counts;
+    const uint32_t* shadeQueue;
+    uint32_t* extQueue;
+    uint32_t* shadowQueue;
+};
+
+struct SoA {
+    float4* originPdf;    // origin.xyz, pdf
+    float4* dirV;         // dir.xyz, flags | vertexIndex << 16 (bits)
+    float4* thpB;         // thp.xyz, bounce counters (bits)
+    float4* L;            // L.xyz, -
+    uint4* sg;            // sample generator state
+    uint4* hit;           // instanceID, primIndex, baryX, baryY
+    float4* sOrigin;      // shadow origin, distance
+    float4* sDir;         // shadow direction, -
+    float4* sLr;          // shadow contribution thp * Lr
+    float* sampleL;       // per-path radiance (3 floats), wave slot order
+};
+
+template <class SG> FPT_D void store_sg(uint4& o, const SG& g);
+template <class SG> FPT_D void load_sg(const uint4& i, SG& g);
+template <> FPT_D void store_sg<TinyUniformSG>(uint4& o, const TinyUniformSG& g) { o = make_uint4(g.state, 0, 0, 0); }
+template <> FPT_D void load_sg<TinyUniformSG>(const uint4& i, TinyUniformSG& g) { g.state = i.x; }
+template <> FPT_D void store_sg<UniformSG>(uint4& o, const UniformSG& g) { o = make_uint4(g.s0, g.s1, g.s2, g.s3); }
+template <> FPT_D void load_sg<UniformSG>(const uint4& i, UniformSG& g) { g.s0 = i.x; g.s1 = i.y; g.s2 = i.z; g.s3 = i.w; }
+
+template <class SG>
+FPT_D void load_path(const SoA& w, uint32_t i, PathState<SG>& path) {
+    const float4 a = w.originPdf[i], b = w.dirV[i], c = w.thpB[i], d = w.L[i];
+    path.origin = make_float3(a.x, a.y, a.z);
+    path.pdf = a.w;
+    path.dir = make_float3(b.x, b.y, b.z);
+    const uint32_t fv = __float_as_uint(b.w);
+    path.flags = fv & 0xffffu;
+    path.vertexIndex = fv >> 16;
+    path.thp = make_float3(c.x, c.y, c.z);
+    path.bounces = __float_as_uint(c.w);
+    path.L = make_float3(d.x, d.y, d.z);
+    load_sg(w.sg[i], path.sg);
+    const uint4 h = w.hit[i];
+    path.hit.instanceID = h.x;
+    path.hit.primIndex = h.y;
+    path.hit.baryX = __uint_as_float(h.z);
+    path.hit.baryY = __uint_as_float(h.w);
+    path.hit.valid = true;
+    path.normal = f3(0.f);
+    path.shadowPending = false;
+}
+
+template <class SG>
+FPT_D void store_path(const SoA& w, uint32_t i, const PathState<SG>& path) {
+    w.originPdf[i] = make_float4(path.origin.x, path.origin.y, path.origin.z, path.pdf);
+    w.dirV[i] = make_float4(path.dir.x, path.dir.y, path.dir.z, __uint_as_float((path.flags & 0xffffu) | (path.vertexIndex << 16)));
+    w.thpB[i] = make_float4(path.thp.x, path.thp.y, path.thp.z, __uint_as_float(path.bounces));
+    w.L[i] = make_float4(path.L.x, path.L.y, path.L.z, 0.f);
+    store_sg(w.sg[i], path.sg);
+}
+
+// Warp-aggregated push of `item` onto queue q (count at *cnt).
+FPT_D void push(bool pred, uint32_t item, uint32_t* q, uint32_t* cnt) {
+    const uint32_t mask = __ballot_sync(__activemask(), pred);
+    if (mask == 0) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (int(lane) == leader) base = atomicAdd(cnt, uint32_t(__popc(mask)));
+    base = __shfl_sync(__activemask(), base, leader);
+    if (pred) q[base + uint32_t(__popc(mask & ((1u << lane) - 1u)))] = item;
+}
+
+// Ray tracing kernels (visibility and extension rays) with per-lane dynamic
+// ray fetch: each warp takes chunks of kFetchChunk queue entries with one
+// atomic and hands them to its idle lanes, and a lane whose ray has finished
+// takes the next one as soon as fewer than kRefillBelow lanes of its warp are
+// still tracing.  The traversal itself advances one node visit per step, so
+// rays of very different lengths share a warp without leaving most of its
+// lanes idle until the longest ray is done.
+#ifndef FPT_REFILL_BELOW
+#define FPT_REFILL_BELOW 24
+#endif
+#ifndef FPT_TRACE_MIN_BLOCKS
+#define FPT_TRACE_MIN_BLOCKS 6
+#endif
+constexpr uint32_t kFetchChunk = 128;
+constexpr int kRefillBelow = FPT_REFILL_BELOW;
+
+template <bool SHADOW, bool MARK_VISIBLE = false>
+FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams& wp, const SoA& w, uint2* stack) {
+    const uint32_t lane = threadIdx.x & 31u;
+    Counters cnt;
+    const uint32_t n = wp.counts[SHADOW ? 2 : 1];
+    uint32_t* fetch = wp.counts + (SHADOW ? kFetchShadow : kFetchExtend);
+    const uint32_t* queue = SHADOW ? wp.shadowQueue : wp.extQueue;
+    const int postponeLimit = kStackSize - int(s.bvhDepth);
+    uint32_t chunkNext = 0, chunkEnd = 0;  // warp-uniform
+    bool drained = n == 0 || s.nodeCount == 0;
+    bool active = false;
+    uint32_t path = 0, fv = 0;
+    TraceRay r;
+    TraceState t;
+    for (;;) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (idle && !drained) {
+            if (chunkNext >= chunkEnd) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(fetch, kFetchChunk);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base >= n) drained = true;
+                else { chunkNext = base; chunkEnd = min(base + kFetchChunk, n); }
+            }
+            if (!drained) {
+                const uint32_t avail = chunkEnd - chunkNext;
+                const uint32_t rank = __popc(idle & ((1u << lane) - 1u));
+                if (!active && rank < avail) {
+                    path = queue[chunkNext + rank];
+                    float4 o, d;
+                    if (SHADOW) { o = w.sOrigin[path]; d = w.sDir[path]; }
+                    else { o = w.originPdf[path]; d = w.dirV[path]; }
+                    fv = __float_as_uint(d.w);
+                    r = make_trace_ray(make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), 0.f);
+                    trace_init(r, SHADOW ? o.w : 1e30f, t);
+                    active = true;
+                }
+                chunkNext += min(avail, uint32_t(__popc(idle)));
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0) break;
+        for (;;) {
+            if (active) {
+                trace_step<SHADOW>(s, r, t, stack, kTraceBlock, postponeLimit);
+                if (t.status != kTraceRunning) {
+                    active = false;
+                    cnt.v[1]++;
+                    cnt.v[SHADOW ? 3 : 2]++;
+                    cnt.v[4] += t.visits;
+                    cnt.v[5] += t.triTests;
+                    if (SHADOW) { cnt.v[11] += t.visits; cnt.v[12] += t.triTests; }
+                    HitRec h;
+                    trace_result(t, h);
+                    if (SHADOW) {
+                        if (!h.valid && t.status != kTraceError) {
+                            const float4 lr = w.sLr[path];
+                            float4 L = w.L[path];
+                            L.x += lr.x; L.y += lr.y; L.z += lr.z;
+                            w.L[path] = L;
+                            if (MARK_VISIBLE) w.sLr[path].w = 1.f;  // read by the adjoint's NEE-gradient kernel
+                        }
+                    } else {
+                        uint32_t f = fv + (1u << 16);  // vertexIndex++
+                        if (h.valid) {
+                            f |= 0x2u;
+                            w.hit[path] = make_uint4(h.instanceID, h.primIndex, __float_as_uint(h.baryX), __float_as_uint(h.baryY));
+                        } else {
+                            f &= ~0x2u;
+                        }
+                        float4 d = w.dirV[path];
+                        d.w = __uint_as_float(f);
+                        w.dirV[path] = d;
+                    }
+                }
+            }
+            const uint32_t a = __ballot_sync(0xffffffffu, active);
+            if (a == 0) break;
+            if (!drained && __popc(a) < kRefillBelow) break;
+        }
+    }
+    flush_counters(p.counters, cnt);
+}
+
+inline int blocks_for(const void* kernel, int block) {
+    int perSM = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, block, 0);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(1, perSM) * sms;
+}
+
+}  // namespace
+}  // namespace fpt

@@ -24,8 +24,9 @@ def war_params(w, h, seed=3, max_bounces=2, mesh=0):
                          seed=seed, lambert=0, meshID=mesh)
 
 
-def war_props(max_bounces=2, seed=3, mesh=0, mode="BackwardDiff"):
-    return {"diffMode": mode, "maxBounces": max_bounces, "fixedSeed": seed, "useWAR": False, "meshToOptimize": mesh}
+def war_props(max_bounces=2, seed=3, mesh=0, mode="BackwardDiff", scheduler="Wavefront"):
+    return {"diffMode": mode, "maxBounces": max_bounces, "fixedSeed": seed, "useWAR": False, "meshToOptimize": mesh,
+            "scheduler": scheduler}
 
 
 def mesh_vertex_count(host, mesh):
@@ -91,8 +92,9 @@ def gpu_scene(host):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("scheduler", ["Wavefront", "Megakernel"])
 @pytest.mark.parametrize("scene", ["box", "heightfield"])
-def test_primal_matches_oracle(fpt, oracle, scene):
+def test_primal_matches_oracle(fpt, oracle, scene, scheduler):
     import torch
     from falcor_b200.passes import WARDiffPathTracer
     host = H.box_icosphere(3) if scene == "box" else H.small_heightfield(materials=16, emitters=16)
@@ -101,7 +103,7 @@ def test_primal_matches_oracle(fpt, oracle, scene):
     for seed in (2, 3):
         ref, _, _, _, _ = osc.wardiff(war_params(W, Hh, seed=seed, max_bounces=3), mode=0)
         s = gpu_scene(host)
-        pt = WARDiffPathTracer(war_props(max_bounces=3, seed=seed, mode="Primal"))
+        pt = WARDiffPathTracer(war_props(max_bounces=3, seed=seed, mode="Primal", scheduler=scheduler))
         pt.set_scene(s)
         out = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
         pt.execute({"color": out})
@@ -113,8 +115,9 @@ def test_primal_matches_oracle(fpt, oracle, scene):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("scheduler", ["Wavefront", "Megakernel"])
 @pytest.mark.parametrize("scene", ["box", "heightfield"])
-def test_adjoint_matches_oracle_forward_mode(fpt, oracle, scene):
+def test_adjoint_matches_oracle_forward_mode(fpt, oracle, scene, scheduler):
     import torch
     from falcor_b200.passes import WARDiffPathTracer
     host = H.box_icosphere(3) if scene == "box" else H.small_heightfield(materials=16, emitters=16)
@@ -128,7 +131,7 @@ def test_adjoint_matches_oracle_forward_mode(fpt, oracle, scene):
     _, gp_ref, _, _, _ = osc.wardiff(war_params(W, Hh, mesh=mesh), mode=1, dLdI=dLdI, pos_tangents=P)
 
     s = gpu_scene(host)
-    pt = WARDiffPathTracer(war_props(mesh=mesh))
+    pt = WARDiffPathTracer(war_props(mesh=mesh, scheduler=scheduler))
     pt.set_scene(s)
     color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
     gm = torch.zeros(T.shape[1], dtype=torch.float32, device="cuda")
