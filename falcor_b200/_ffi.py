@@ -147,6 +147,7 @@ SIGNATURES = {
     "fpt_batch_destroy": (None, [_P]),
     "fpt_batch_add": (C.c_int, [_P, C.POINTER(fpt_batch_request)]),
     "fpt_batch_set_tuning": (C.c_int, [_P, u32, u32]),
+    "fpt_batch_get_tuning": (C.c_int, [_P, C.POINTER(u32), C.POINTER(u32)]),
     "fpt_batch_autotune": (C.c_int, [_P, _P]),
     "fpt_batch_launch": (C.c_int, [_P, _P]),
     "fpt_batch_launch_sequential": (C.c_int, [_P, _P]),

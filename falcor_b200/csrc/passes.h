@@ -43,6 +43,8 @@ struct fpt_pass {
 
 namespace fpt {
 fpt_status ensure_scratch(fpt_pass& p);
+// PathTracer properties -> kernel parameters (PathTracer.cpp:253-415 parsing and validation).
+void path_tracer_params(fpt_pass& p, FrameParams& fp);
 // WARDiffPathTracer primal (dLdI == nullptr) or adjoint.
 fpt_status wardiff_execute(fpt_pass& p, const fpt_frame_io* io, const float* dLdI, const fpt_grad_buffers* grads,
                            cudaStream_t st);

@@ -14,6 +14,7 @@
 // (ResolvePass.cs.slang:80-101), and a generate kernel seeds the wave
 // (PathTracer.slang:273-301, GeneratePaths.cs.slang:93-256).
 #include <algorithm>
+#include <cstring>
 
 #include "kernels.cuh"
 #include "path_logic.cuh"
@@ -26,39 +27,69 @@ using namespace dev;
 
 namespace {
 
-// Seeds a wave: slot i <-> (pixel waveFirstPixel + i % wavePixels, sample i / wavePixels).
-// Background pixels write their samples directly; hit pixels enter the shade queue.
+// Seeds one slot: (pixel pix, sample) of a frame.  Background pixels write
+// their samples directly; returns true for hit pixels (shade queue).
 template <class SG>
+FPT_D bool generate_slot(const DevScene& s, const FrameParams& p, const SoA& w, uint32_t i, uint32_t pix, uint32_t sample,
+                         Counters& cnt) {
+    const uint32_t x = pix % p.width, y = pix / p.width;
+    float tMin, tMax;
+    const float3 dir = camera_ray_dir(s.camera, x, y, p.width, p.height, tMin, tMax);
+    HitRec hit;
+    if (unpack_hit(s.bits, __ldg(p.vbuffer + pix), hit)) {
+        PathState<SG> path;
+        path.sg.init(x, y, p.seed * p.spp + sample);
+        path.flags = PF_ACTIVE | 0x2u;  // active, hit (primary hit from the V-buffer)
+        path.vertexIndex = 1;
+        path.bounces = 0;
+        path.thp = f3(1.f);
+        path.L = f3(0.f);
+        path.pdf = 0.f;
+        path.origin = load3(s.camera.posW);
+        path.dir = dir;
+        store_path(w, i, path);
+        w.hit[i] = make_uint4(hit.instanceID, hit.primIndex, __float_as_uint(hit.baryX), __float_as_uint(hit.baryY));
+        return true;
+    }
+    const float3 bg = s.hasEnv ? env_eval(s, dir) : f3(0.f);
+    if (s.hasEnv) cnt.v[9]++;
+    float* o = w.sampleL + size_t(i) * 3;
+    o[0] = bg.x; o[1] = bg.y; o[2] = bg.z;
+    return false;
+}
+
+// Tile of slot (or resolved pixel) `x` of a batched wave: the last tile whose
+// offset is <= x (tiles are in slot order).
+template <bool PIXELS>
+FPT_D uint32_t find_tile(const WaveParams& wp, uint32_t x) {
+    uint32_t lo = 0, hi = wp.tileCount;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t off = PIXELS ? wp.tiles[mid].pixelOffset : wp.tiles[mid].slotOffset;
+        if (off <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Seeds a wave.  Single frame: slot i <-> (pixel waveFirstPixel + i % wavePixels,
+// sample i / wavePixels).  Batched (MULTI): slot i of tile t <-> (pixel
+// firstPixel + j % numPixels, sample j / numPixels), j = i - slotOffset.
+template <class SG, bool MULTI>
 __global__ void __launch_bounds__(kShadeBlock) wf_generate(DevScene s, FrameParams p, WaveParams wp, SoA w) {
     Counters cnt;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i - threadIdx.x < wp.wavePaths; i += gridDim.x * blockDim.x) {
         bool enqueue = false;
         if (i < wp.wavePaths) {
-            const uint32_t pixIn = i % wp.wavePixels, sample = i / wp.wavePixels;
-            const uint32_t pix = wp.waveFirstPixel + pixIn;
-            const uint32_t x = pix % p.width, y = pix / p.width;
-            float tMin, tMax;
-            const float3 dir = camera_ray_dir(s.camera, x, y, p.width, p.height, tMin, tMax);
-            HitRec hit;
-            if (unpack_hit(s.bits, __ldg(p.vbuffer + pix), hit)) {
-                PathState<SG> path;
-                path.sg.init(x, y, p.seed * p.spp + sample);
-                path.flags = PF_ACTIVE | 0x2u;  // active, hit (primary hit from the V-buffer)
-                path.vertexIndex = 1;
-                path.bounces = 0;
-                path.thp = f3(1.f);
-                path.L = f3(0.f);
-                path.pdf = 0.f;
-                path.origin = load3(s.camera.posW);
-                path.dir = dir;
-                store_path(w, i, path);
-                w.hit[i] = make_uint4(hit.instanceID, hit.primIndex, __float_as_uint(hit.baryX), __float_as_uint(hit.baryY));
-                enqueue = true;
+            if (MULTI) {
+                const uint32_t t = find_tile<false>(wp, i);
+                wp.slotTile[i] = t;
+                const BatchTile tile = wp.tiles[t];
+                const uint32_t j = i - tile.slotOffset;
+                enqueue = generate_slot<SG>(wp.scenes[tile.req], wp.frames[tile.req], w, i, tile.firstPixel + j % tile.numPixels,
+                                            j / tile.numPixels, cnt);
             } else {
-                const float3 bg = s.hasEnv ? env_eval(s, dir) : f3(0.f);
-                if (s.hasEnv) cnt.v[9]++;
-                float* o = w.sampleL + size_t(i) * 3;
-                o[0] = bg.x; o[1] = bg.y; o[2] = bg.z;
+                enqueue = generate_slot<SG>(s, p, w, i, wp.waveFirstPixel + i % wp.wavePixels, i / wp.wavePixels, cnt);
             }
         }
         push(enqueue, i, const_cast<uint32_t*>(wp.shadeQueue), wp.counts + 0);
@@ -66,9 +97,26 @@ __global__ void __launch_bounds__(kShadeBlock) wf_generate(DevScene s, FramePara
     flush_counters(p.counters, cnt);
 }
 
+template <class SG, bool HAS_T>
+FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uint32_t i, bool& ext, bool& shadow, Counters& cnt) {
+    PathState<SG> path;
+    load_path(w, i, path);
+    if (path.flags & 0x2u) pt_handle_hit<SG, HAS_T>(s, p, path, cnt);
+    else pt_handle_miss<SG>(s, p, path, cnt);
+    shadow = path.shadowPending;
+    if (shadow) {
+        w.sOrigin[i] = make_float4(path.sOrigin.x, path.sOrigin.y, path.sOrigin.z, path.sDist);
+        w.sDir[i] = make_float4(path.sDir.x, path.sDir.y, path.sDir.z, 0.f);
+        w.sLr[i] = make_float4(path.sLr.x, path.sLr.y, path.sLr.z, 0.f);
+    }
+    ext = path.has(PF_ACTIVE);
+    store_path(w, i, path);
+    if (!ext) cnt.v[0]++;
+}
+
 // handleHit / handleMiss for every path of the shade queue.  The hit flag of
 // a path is PF_HIT (0x2) in its flags.
-template <class SG, bool HAS_T>
+template <class SG, bool HAS_T, bool MULTI>
 __global__ void __launch_bounds__(kShadeBlock) wf_shade(DevScene s, FrameParams p, WaveParams wp, SoA w) {
     Counters cnt;
     const uint32_t n = wp.counts[0];
@@ -77,19 +125,12 @@ __global__ void __launch_bounds__(kShadeBlock) wf_shade(DevScene s, FrameParams 
         uint32_t i = 0;
         if (k < n) {
             i = wp.shadeQueue[k];
-            PathState<SG> path;
-            load_path(w, i, path);
-            if (path.flags & 0x2u) pt_handle_hit<SG, HAS_T>(s, p, path, cnt);
-            else pt_handle_miss<SG>(s, p, path, cnt);
-            shadow = path.shadowPending;
-            if (shadow) {
-                w.sOrigin[i] = make_float4(path.sOrigin.x, path.sOrigin.y, path.sOrigin.z, path.sDist);
-                w.sDir[i] = make_float4(path.sDir.x, path.sDir.y, path.sDir.z, 0.f);
-                w.sLr[i] = make_float4(path.sLr.x, path.sLr.y, path.sLr.z, 0.f);
+            if (MULTI) {
+                const uint32_t r = slot_request(wp, i);
+                shade_slot<SG, HAS_T>(wp.scenes[r], wp.frames[r], w, i, ext, shadow, cnt);
+            } else {
+                shade_slot<SG, HAS_T>(s, p, w, i, ext, shadow, cnt);
             }
-            ext = path.has(PF_ACTIVE);
-            store_path(w, i, path);
-            if (!ext) cnt.v[0]++;
         }
         push(shadow, i, wp.shadowQueue, wp.counts + 2);
         push(ext, i, wp.extQueue, wp.counts + 1);
@@ -109,11 +150,28 @@ __global__ void __launch_bounds__(kTraceBlock, FPT_TRACE_MIN_BLOCKS) wf_extend(D
     trace_queue<false>(s, p, wp, w, stackMem + threadIdx.x);
 }
 
+// Batched waves: each ray traced in its own request's scene.
+__global__ void __launch_bounds__(kTraceBlock, FPT_TRACE_MIN_BLOCKS) wf_shadow_batch(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    __shared__ uint2 stackMem[kStackSize * kTraceBlock];
+    trace_queue<true, false, true>(s, p, wp, w, stackMem + threadIdx.x);
+}
+__global__ void __launch_bounds__(kTraceBlock, FPT_TRACE_MIN_BLOCKS) wf_extend_batch(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    __shared__ uint2 stackMem[kStackSize * kTraceBlock];
+    trace_queue<false, false, true>(s, p, wp, w, stackMem + threadIdx.x);
+}
+
 // Finished paths keep their radiance in L; copy it into the per-sample buffer.
-__global__ void wf_collect(FrameParams p, WaveParams wp, SoA w, const uint32_t* hitPixelFlags) {
+template <bool MULTI>
+__global__ void wf_collect(FrameParams p, WaveParams wp, SoA w) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePaths; i += gridDim.x * blockDim.x) {
-        const uint32_t pix = wp.waveFirstPixel + i % wp.wavePixels;
-        if (!(__ldg(p.vbuffer + pix).x)) continue;  // background: written by wf_generate
+        if (MULTI) {
+            const BatchTile tile = wp.tiles[wp.slotTile[i]];
+            const uint32_t pix = tile.firstPixel + (i - tile.slotOffset) % tile.numPixels;
+            if (!(__ldg(wp.frames[tile.req].vbuffer + pix).x)) continue;
+        } else {
+            const uint32_t pix = wp.waveFirstPixel + i % wp.wavePixels;
+            if (!(__ldg(p.vbuffer + pix).x)) continue;  // background: written by wf_generate
+        }
         const float4 L = w.L[i];
         float* o = w.sampleL + size_t(i) * 3;
         o[0] = L.x; o[1] = L.y; o[2] = L.z;
@@ -121,22 +179,34 @@ __global__ void wf_collect(FrameParams p, WaveParams wp, SoA w, const uint32_t* 
 }
 
 // ResolvePass: per-pixel average of the per-sample colours in sample order.
+FPT_D void resolve_pixel(const DevScene& s, const FrameParams& p, const SoA& w, uint32_t pix, uint32_t slot0, uint32_t stride) {
+    float3 c = f3(0.f);
+    for (uint32_t smp = 0; smp < p.spp; smp++) {
+        const float* q = w.sampleL + (size_t(smp) * stride + slot0) * 3;
+        const float3 L = make_float3(q[0], q[1], q[2]);
+        if (p.sampleColor) {
+            float* o = p.sampleColor + (size_t(pix) * p.spp + smp) * 3;
+            o[0] = L.x; o[1] = L.y; o[2] = L.z;
+        }
+        c += (p.spp != 1 && p.colorFormat == 1) ? decode_logluv_hdr(encode_logluv_hdr(L)) : L;
+    }
+    const float3 out = p.spp == 1 ? c : c * (1.f / float(p.spp));
+    if (!isfinite(out.x) || !isfinite(out.y) || !isfinite(out.z)) atomicOr(s.errorWord, FPT_DEVERR_NAN);
+    p.color[pix] = make_float4(out.x, out.y, out.z, 1.f);
+}
+
+template <bool MULTI>
 __global__ void wf_resolve(DevScene s, FrameParams p, WaveParams wp, SoA w) {
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < wp.wavePixels; j += gridDim.x * blockDim.x) {
-        const uint32_t pix = wp.waveFirstPixel + j;
-        float3 c = f3(0.f);
-        for (uint32_t smp = 0; smp < p.spp; smp++) {
-            const float* q = w.sampleL + (size_t(smp) * wp.wavePixels + j) * 3;
-            const float3 L = make_float3(q[0], q[1], q[2]);
-            if (p.sampleColor) {
-                float* o = p.sampleColor + (size_t(pix) * p.spp + smp) * 3;
-                o[0] = L.x; o[1] = L.y; o[2] = L.z;
-            }
-            c += (p.spp != 1 && p.colorFormat == 1) ? decode_logluv_hdr(encode_logluv_hdr(L)) : L;
+        if (MULTI) {
+            const BatchTile tile = wp.tiles[find_tile<true>(wp, j)];
+            const uint32_t jt = j - tile.pixelOffset;
+            // Slot of (pixel jt, sample smp) = slotOffset + smp * numPixels + jt.
+            resolve_pixel(wp.scenes[tile.req], wp.frames[tile.req], w, tile.firstPixel + jt,
+                          tile.slotOffset + jt - 0u, tile.numPixels);
+        } else {
+            resolve_pixel(s, p, w, wp.waveFirstPixel + j, j, wp.wavePixels);
         }
-        const float3 out = p.spp == 1 ? c : c * (1.f / float(p.spp));
-        if (!isfinite(out.x) || !isfinite(out.y) || !isfinite(out.z)) atomicOr(s.errorWord, FPT_DEVERR_NAN);
-        p.color[pix] = make_float4(out.x, out.y, out.z, 1.f);
     }
 }
 
@@ -162,13 +232,13 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
     const uint32_t wavePixels = std::max<uint32_t>(1, std::min<uint32_t>(pixels, b.capacity / p.spp));
     static int gShade = 0, gTrace = 0, gGen = 0;
     if (!gShade) {
-        gShade = blocks_for(reinterpret_cast<const void*>(wf_shade<SG, HAS_T>), kShadeBlock);
+        gShade = blocks_for(reinterpret_cast<const void*>(wf_shade<SG, HAS_T, false>), kShadeBlock);
         gTrace = blocks_for(reinterpret_cast<const void*>(wf_extend), kTraceBlock);
-        gGen = blocks_for(reinterpret_cast<const void*>(wf_generate<SG>), kShadeBlock);
+        gGen = blocks_for(reinterpret_cast<const void*>(wf_generate<SG, false>), kShadeBlock);
     }
     const uint32_t maxIter = p.maxSurfaceBounces + 2;
     for (uint32_t first = 0; first < pixels; first += wavePixels) {
-        WaveParams wp;
+        WaveParams wp{};
         wp.waveFirstPixel = first;
         wp.wavePixels = std::min(wavePixels, pixels - first);
         wp.wavePaths = wp.wavePixels * p.spp;
@@ -182,11 +252,11 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
         wp.shadowQueue = b.shadowQueue;
         const int genBlocks = std::min<int>(gGen, int((wp.wavePaths + kShadeBlock - 1) / kShadeBlock));
         T0(KC_GENERATE);
-        wf_generate<SG><<<genBlocks, kShadeBlock, 0, st>>>(s, p, wp, w);
+        wf_generate<SG, false><<<genBlocks, kShadeBlock, 0, st>>>(s, p, wp, w);
         T1();
         for (uint32_t it = 0; it < maxIter; it++) {
             T0(KC_SHADE);
-            wf_shade<SG, HAS_T><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
+            wf_shade<SG, HAS_T, false><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
             T1();
             T0(KC_SHADOW);
             wf_shadow<<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
@@ -200,8 +270,8 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
             wp.extQueue = qb;
         }
         T0(KC_RESOLVE);
-        wf_collect<<<gGen, 256, 0, st>>>(p, wp, w, nullptr);
-        wf_resolve<<<(wp.wavePixels + 255) / 256, 256, 0, st>>>(s, p, wp, w);
+        wf_collect<false><<<gGen, 256, 0, st>>>(p, wp, w);
+        wf_resolve<false><<<(wp.wavePixels + 255) / 256, 256, 0, st>>>(s, p, wp, w);
         T1();
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -209,7 +279,79 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
     return cudaSuccess;
 }
 
+// All waves of a batch (one stream-ordered sequence; the caller captures it
+// in a CUDA graph).
+template <class SG, bool HAS_T>
+cudaError_t run_batch(const BatchDevice& bd, const std::vector<BatchWave>& waves, WavefrontBuffers& b, int shadeScale,
+                      cudaStream_t st, uint32_t& launches) {
+    SoA w;
+    w.originPdf = b.f4(0); w.dirV = b.f4(1); w.thpB = b.f4(2); w.L = b.f4(3);
+    w.sg = reinterpret_cast<uint4*>(b.f4(4)); w.hit = reinterpret_cast<uint4*>(b.f4(5));
+    w.sOrigin = b.f4(6); w.sDir = b.f4(7); w.sLr = b.f4(8);
+    w.sampleL = b.sampleL;
+    DevScene none;
+    std::memset(&none, 0, sizeof(none));
+    FrameParams fp;
+    std::memset(&fp, 0, sizeof(fp));
+    fp.counters = bd.counters;
+    static int gShade = 0, gTrace = 0, gGen = 0;
+    if (!gShade) {
+        gShade = blocks_for(reinterpret_cast<const void*>(wf_shade<SG, HAS_T, true>), kShadeBlock);
+        gTrace = blocks_for(reinterpret_cast<const void*>(wf_extend_batch), kTraceBlock);
+        gGen = blocks_for(reinterpret_cast<const void*>(wf_generate<SG, true>), kShadeBlock);
+    }
+    const int shadeBlocks = gShade * std::max(1, shadeScale);
+    launches = 0;
+    for (const BatchWave& wv : waves) {
+        WaveParams wp{};
+        wp.waveFirstPixel = 0;
+        wp.wavePixels = wv.pixels;
+        wp.wavePaths = wv.paths;
+        wp.counts = b.counts;
+        wp.scenes = bd.scenes;
+        wp.frames = bd.frames;
+        wp.tiles = bd.tiles + wv.firstTile;
+        wp.tileCount = wv.tileCount;
+        wp.slotTile = bd.slotTile;
+        cudaError_t e = cudaMemsetAsync(b.counts, 0, kNumWaveCounts * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return e;
+        uint32_t* qa = b.queueA;
+        uint32_t* qb = b.queueB;
+        wp.shadeQueue = qa;
+        wp.extQueue = qb;
+        wp.shadowQueue = b.shadowQueue;
+        const int genBlocks = std::min<int>(gGen, int((wp.wavePaths + kShadeBlock - 1) / kShadeBlock));
+        wf_generate<SG, true><<<genBlocks, kShadeBlock, 0, st>>>(none, fp, wp, w);
+        launches++;
+        for (uint32_t it = 0; it < wv.maxIter; it++) {
+            wf_shade<SG, HAS_T, true><<<shadeBlocks, kShadeBlock, 0, st>>>(none, fp, wp, w);
+            wf_shadow_batch<<<gTrace, kTraceBlock, 0, st>>>(none, fp, wp, w);
+            wf_extend_batch<<<gTrace, kTraceBlock, 0, st>>>(none, fp, wp, w);
+            wf_advance<<<1, 1, 0, st>>>(wp);
+            launches += 4;
+            std::swap(qa, qb);
+            wp.shadeQueue = qa;
+            wp.extQueue = qb;
+        }
+        wf_collect<true><<<gGen, 256, 0, st>>>(fp, wp, w);
+        wf_resolve<true><<<(wp.wavePixels + 255) / 256, 256, 0, st>>>(none, fp, wp, w);
+        launches += 2;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 }  // namespace
+
+cudaError_t launch_batch_wavefront(const BatchDevice& bd, const std::vector<BatchWave>& waves, bool uniformSG, bool hasT,
+                                   WavefrontBuffers& b, int shadeScale, cudaStream_t st, uint32_t& launches) {
+    if (uniformSG)
+        return hasT ? run_batch<UniformSG, true>(bd, waves, b, shadeScale, st, launches)
+                    : run_batch<UniformSG, false>(bd, waves, b, shadeScale, st, launches);
+    return hasT ? run_batch<TinyUniformSG, true>(bd, waves, b, shadeScale, st, launches)
+                : run_batch<TinyUniformSG, false>(bd, waves, b, shadeScale, st, launches);
+}
 
 cudaError_t WavefrontBuffers::ensure(uint32_t cap) {
     if (capacity >= cap && base) return cudaSuccess;

@@ -58,4 +58,28 @@ struct KernelTimer {
 cudaError_t launch_path_tracer_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st,
                                          KernelTimer* timer = nullptr);
 
+// Batched PathTracer: one wave holds whole pixel tiles of several requests.
+// Tile t covers pixels [firstPixel, firstPixel + numPixels) of request `req`,
+// all `spp` samples, at wave slots [slotOffset, slotOffset + numPixels * spp)
+// (sample-major) and resolved pixels [pixelOffset, pixelOffset + numPixels).
+struct BatchTile {
+    uint32_t req, firstPixel, numPixels, slotOffset, pixelOffset, spp;
+};
+struct BatchWave {
+    uint32_t firstTile, tileCount, paths, pixels, maxIter;
+};
+// Device arrays of a batch: per-request scenes and frame parameters, all
+// tiles, and a per-slot tile index (capacity entries).
+struct BatchDevice {
+    const DevScene* scenes = nullptr;
+    const FrameParams* frames = nullptr;
+    const BatchTile* tiles = nullptr;
+    uint32_t* slotTile = nullptr;
+    unsigned long long* counters = nullptr;
+};
+// Enqueues every wave of the batch (uniform sample generator type and
+// transmission variant across requests); shadeScale multiplies the shade grid.
+cudaError_t launch_batch_wavefront(const BatchDevice& bd, const std::vector<BatchWave>& waves, bool uniformSG, bool hasT,
+                                   WavefrontBuffers& b, int shadeScale, cudaStream_t st, uint32_t& launches);
+
 }  // namespace fpt

@@ -27,7 +27,16 @@ struct WaveParams {
     const uint32_t* shadeQueue;
     uint32_t* extQueue;
     uint32_t* shadowQueue;
+    // Batched waves only: per-request scenes/frames, this wave's tiles, slot -> tile.
+    const DevScene* scenes;
+    const FrameParams* frames;
+    const BatchTile* tiles;
+    uint32_t tileCount;
+    uint32_t* slotTile;
 };
+
+// Request of wave slot i in a batched wave.
+FPT_D uint32_t slot_request(const WaveParams& wp, uint32_t i) { return wp.tiles[wp.slotTile[i]].req; }
 
 struct SoA {
     float4* originPdf;    // origin.xyz, pdf
@@ -109,18 +118,20 @@ FPT_D void push(bool pred, uint32_t item, uint32_t* q, uint32_t* cnt) {
 constexpr uint32_t kFetchChunk = 128;
 constexpr int kRefillBelow = FPT_REFILL_BELOW;
 
-template <bool SHADOW, bool MARK_VISIBLE = false>
+// MULTI: rays of a batched wave, each traced in its own request's scene.
+template <bool SHADOW, bool MARK_VISIBLE = false, bool MULTI = false>
 FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams& wp, const SoA& w, uint2* stack) {
     const uint32_t lane = threadIdx.x & 31u;
     Counters cnt;
     const uint32_t n = wp.counts[SHADOW ? 2 : 1];
     uint32_t* fetch = wp.counts + (SHADOW ? kFetchShadow : kFetchExtend);
     const uint32_t* queue = SHADOW ? wp.shadowQueue : wp.extQueue;
-    const int postponeLimit = kStackSize - int(s.bvhDepth);
+    const int postponeLimit = MULTI ? 0 : kStackSize - int(s.bvhDepth);
     uint32_t chunkNext = 0, chunkEnd = 0;  // warp-uniform
-    bool drained = n == 0 || s.nodeCount == 0;
+    bool drained = n == 0 || (!MULTI && s.nodeCount == 0);
     bool active = false;
     uint32_t path = 0, fv = 0;
+    const DevScene* S = nullptr;  // MULTI: this lane's scene
     TraceRay r;
     TraceState t;
     for (;;) {
@@ -144,6 +155,10 @@ FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams
                     fv = __float_as_uint(d.w);
                     r = make_trace_ray(make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), 0.f);
                     trace_init(r, SHADOW ? o.w : 1e30f, t);
+                    if (MULTI) {
+                        S = wp.scenes + slot_request(wp, path);
+                        if (S->nodeCount == 0) t.status = kTraceDone;  // empty scene: a miss
+                    }
                     active = true;
                 }
                 chunkNext += min(avail, uint32_t(__popc(idle)));
@@ -152,7 +167,11 @@ FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams
         if (__ballot_sync(0xffffffffu, active) == 0) break;
         for (;;) {
             if (active) {
-                trace_step<SHADOW>(s, r, t, stack, kTraceBlock, postponeLimit);
+                if (MULTI) {
+                    if (t.status == kTraceRunning) trace_step<SHADOW>(*S, r, t, stack, kTraceBlock, 0);
+                } else {
+                    trace_step<SHADOW>(s, r, t, stack, kTraceBlock, postponeLimit);
+                }
                 if (t.status != kTraceRunning) {
                     active = false;
                     cnt.v[1]++;

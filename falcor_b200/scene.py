@@ -176,3 +176,28 @@ def make_host_scene(w: Workload, **overrides) -> HostScene:
     params = dict(w.params)
     params.update(overrides)
     return HostScene.procedural(w.kind, **params)
+
+
+# Batched uneven forward workload: 8 procedural scenes of 10k to 1M triangles
+# (random soups and displaced grids, 256 materials, 64 emitters) and 64 requests
+# with resolution from {128, 256, 512, 1024}^2, spp from {1, 4, 16, 32} and a
+# bounce limit from 2..8, drawn with a seeded generator (expected 2.9e8 paths).
+BATCH_SCENE_TRIANGLES = (10_000, 19_307, 37_276, 71_969, 138_950, 268_270, 517_947, 1_000_000)
+
+
+def batch_scene_params(i: int) -> tuple[int, dict]:
+    tris = BATCH_SCENE_TRIANGLES[i]
+    if i % 2 == 0:
+        return RANDOM_SOUP, dict(seed=100 + i, soup_triangles=tris, material_count=256, emissive_count=64, aspect_ratio=1.0)
+    res = int(round((tris / 2) ** 0.5)) + 1  # 2 (res - 1)^2 triangles
+    return DISPLACED_GRID, dict(seed=100 + i, grid_res=res, material_count=256, emissive_count=64, aspect_ratio=1.0)
+
+
+def batch_requests(count: int = 64, seed: int = 4) -> list[tuple[int, int, int, int, int]]:
+    """(scene index, width, height, spp, max bounces) per request."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        res = int(rng.choice([128, 256, 512, 1024]))
+        out.append((int(rng.integers(0, 8)), res, res, int(rng.choice([1, 4, 16, 32])), int(rng.integers(2, 9))))
+    return out

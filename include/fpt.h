@@ -411,13 +411,19 @@ typedef struct fpt_batch_request {
 FPT_API fpt_status fpt_batch_create(fpt_batch** out);
 FPT_API void fpt_batch_destroy(fpt_batch* batch);
 FPT_API fpt_status fpt_batch_add(fpt_batch* batch, const fpt_batch_request* req);
-/* Tuning: block size and queue chunk (0 = autotuned value). */
-FPT_API fpt_status fpt_batch_set_tuning(fpt_batch* batch, uint32_t block_size, uint32_t chunk);
-/* Runs the autotuner over block size and chunk on the current requests. */
+/* Tuning: paths in flight per wave (the queue depth) and a multiplier of the
+ * occupancy-sized shade grid; 0 keeps the current value. */
+FPT_API fpt_status fpt_batch_set_tuning(fpt_batch* batch, uint32_t wave_capacity, uint32_t shade_grid_scale);
+FPT_API fpt_status fpt_batch_get_tuning(const fpt_batch* batch, uint32_t* wave_capacity, uint32_t* shade_grid_scale);
+/* Times the batched launch over wave capacities 2^20..2^23 and shade grid
+ * scales 1, 2 on the current requests and keeps the fastest. */
 FPT_API fpt_status fpt_batch_autotune(fpt_batch* batch, void* stream);
-/* One persistent launch over all requests (graph-captured on first call). */
+/* All requests as one CUDA graph (built on first call, relaunched after):
+ * V-buffers, then waves that pack whole pixel tiles of several requests
+ * through the wavefront kernels, then the per-request frame averages. */
 FPT_API fpt_status fpt_batch_launch(fpt_batch* batch, void* stream);
-/* The same requests as one plain launch per request, for comparison. */
+/* The same requests as one plain launch per request (VBufferRT, then the
+ * PathTracer per frame of <= 16 spp), for comparison; identical images. */
 FPT_API fpt_status fpt_batch_launch_sequential(fpt_batch* batch, void* stream);
 FPT_API fpt_status fpt_batch_get_stats(fpt_batch* batch, fpt_pass_stats* out, void* stream);
 
