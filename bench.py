@@ -26,6 +26,8 @@ import threading
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -44,6 +46,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the cpu_baseline sample")
     ap.add_argument("--resolution", default=None, help="WxH override of the workload's frame size (small profiling cases)")
     ap.add_argument("--frames-per-step", type=int, default=FRAMES_PER_STEP, help="16-spp frames per step")
+    ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched secondary metrics")
     return ap.parse_args()
 
 
@@ -177,6 +180,89 @@ def cpu_baseline(workload_name: str, seconds: float):
     desc = (f"{side}x{side} crop at the frame centre, {frames} frame(s) of {SPP_PER_FRAME} spp, {w.max_bounces} bounces, "
             f"FP32 CPU oracle (-O3 -ffp-contract=off), {paths} paths in {total:.2f} s")
     return paths / total / 1e6, cores, desc
+
+
+def _time_ms(fn, reps: int) -> float:
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def adjoint_bench(dev) -> dict:
+    """WARDiffPathTracer forward + adjoint on the displaced-sphere workload:
+    512 x 512, one path per pixel per frame, 16 frames per step, maxBounces 4,
+    gradients of 256 x 20 material parameters and of every vertex position
+    (20k-triangle sphere in 256 patches; the environment map is dropped:
+    WARDiff has no environment light)."""
+    import torch
+    from falcor_b200.scene import WORKLOADS, Scene, make_host_scene
+    from falcor_b200.passes import WARDiffPathTracer
+    w = WORKLOADS["displaced_sphere_512"]
+    host = make_host_scene(w, envmap=None)
+    scene = Scene(host)
+    W, Hh, frames = 512, 512, 16
+    nv = host.desc.vertex_count  # positions of every mesh (meshToOptimize = -1)
+    pt = WARDiffPathTracer({"diffMode": "BackwardDiff", "maxBounces": w.max_bounces, "useWAR": False, "runBackward": 0,
+                            "meshToOptimize": -1})
+    pt.set_scene(scene)
+    color = torch.zeros((Hh, W, 4), dtype=torch.float32, device=dev)
+    g = torch.Generator(device=dev).manual_seed(0)
+    dLdI = torch.randn((Hh, W, 3), dtype=torch.float32, device=dev, generator=g)
+    gm = torch.zeros(host.desc.material_count * 20, dtype=torch.float32, device=dev)
+    gp = torch.zeros(nv * 3, dtype=torch.float32, device=dev)
+
+    def fwd():
+        for f in range(frames):
+            pt.set_properties({"fixedSeed": f})
+            pt.execute({"color": color})
+
+    def bwd():
+        for f in range(frames):
+            pt.set_properties({"fixedSeed": f})
+            pt.backward({"color": color}, dLdI, material_grad=gm, position_grad=gp)
+
+    for _ in range(2):
+        fwd()
+        bwd()
+    t_fwd = _time_ms(fwd, 3)
+    t_bwd = _time_ms(bwd, 3)
+    paths = W * Hh * frames
+    return {"workload": "displaced_sphere 512x512, 16 frames x 1 spp, maxBounces 4, material + position gradients",
+            "unit": "Mpaths/s", "forward": round(paths / t_fwd / 1e3, 2), "adjoint": round(paths / t_bwd / 1e3, 2),
+            "fwd_plus_adjoint": round(paths / (t_fwd + t_bwd) / 1e3, 2), "ms_forward": round(t_fwd, 3),
+            "ms_adjoint": round(t_bwd, 3), "triangles": scene.info.triangle_count, "gradient_dims": [gm.numel(), gp.numel()]}
+
+
+def batched_bench(dev) -> dict:
+    """Batched uneven forward: 64 requests over 8 procedural scenes of 10k-1M
+    triangles (one CUDA graph, autotuned) vs one plain launch per request."""
+    import torch
+    from falcor_b200.batch import Batch
+    from falcor_b200.scene import HostScene, Scene, batch_requests, batch_scene_params
+    hosts = [HostScene.procedural(batch_scene_params(i)[0], **batch_scene_params(i)[1]) for i in range(8)]
+    scenes = [Scene(h) for h in hosts]
+    b = Batch()
+    for i, (si, wdt, hgt, spp, mb) in enumerate(batch_requests()):
+        b.add(scenes[si], wdt, hgt, spp, mb, seed=i)
+    paths = b.total_paths
+    b.launch_sequential()
+    t_seq = _time_ms(b.launch_sequential, 2)
+    tuning = b.autotune()
+    b.launch()
+    t_bat = _time_ms(b.launch, 3)
+    st = b.stats()
+    return {"workload": "64 requests, 8 scenes of 10k-1M triangles, res {128..1024}^2, spp {1,4,16,32}, bounces 2-8",
+            "unit": "Mpaths/s", "paths_per_launch": paths, "batched": round(paths / t_bat / 1e3, 2),
+            "sequential": round(paths / t_seq / 1e3, 2), "speedup": round(t_seq / t_bat, 3),
+            "ms_batched": round(t_bat, 2), "ms_sequential": round(t_seq, 2),
+            "tuning": {"wave_capacity": tuning[0], "shade_grid_scale": tuning[1]},
+            "graph_kernel_launches": int(st.kernel_launches), "device_error": int(st.device_error)}
 
 
 def run_reference(args):
@@ -345,6 +431,10 @@ def main():
         "counters_last_launch": counters,
         "device_error": st.device_error,
     }
+    if not args.no_extras:
+        # Secondary metrics of the same run (every rank does its own replica).
+        line["adjoint"] = adjoint_bench(dev)
+        line["batched"] = batched_bench(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, desc = cpu_baseline(w.name, args.cpu_seconds)
         line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpaths/s", "cores": cores, "kind": "port", "sample": desc}

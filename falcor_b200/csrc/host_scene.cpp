@@ -411,8 +411,9 @@ fpt_scene_host* build_heightfield_soup(const fpt_procedural_params& p) {
     return h;
 }
 
-// Displaced UV sphere split into `bands` latitude bands (one instance and
-// material each).  sphere_subdiv = segments around (rings = segments / 2).
+// Displaced UV sphere split into up to 16 x 16 latitude/longitude patches,
+// one instance and one material each (256 materials for the default 142 x 71
+// grid).  sphere_subdiv = segments around (rings = segments / 2).
 fpt_scene_host* build_displaced_sphere(const fpt_procedural_params& p) {
     auto* h = new fpt_scene_host();
     std::mt19937_64 rng(p.seed);
@@ -422,30 +423,30 @@ fpt_scene_host* build_displaced_sphere(const fpt_procedural_params& p) {
     Noise noise(p.seed + 7);
     const uint32_t seg = p.sphere_subdiv ? p.sphere_subdiv : 142;
     const uint32_t rings = seg / 2;
-    // One mesh: positions on a displaced sphere of radius 0.6.
-    Mesh all;
     auto disp = [&](float th, float ph) { return 0.6f + 0.05f * noise.fbm(3.f * ph, 3.f * th, 4); };
-    for (uint32_t r = 0; r <= rings; r++)
-        for (uint32_t s = 0; s <= seg; s++) {
-            float th = 3.14159265f * float(r) / float(rings), ph = 2.f * 3.14159265f * float(s % seg) / float(seg);
-            float d[3] = {std::sin(th) * std::cos(ph), std::cos(th), std::sin(th) * std::sin(ph)};
-            float rad = disp(th, ph);
-            for (int k = 0; k < 3; k++) { all.pos.push_back(rad * d[k]); all.nrm.push_back(d[k]); }
+    auto vertex = [&](uint32_t r, uint32_t sIdx, Mesh& m) {
+        const float th = 3.14159265f * float(r) / float(rings), ph = 2.f * 3.14159265f * float(sIdx % seg) / float(seg);
+        const float d[3] = {std::sin(th) * std::cos(ph), std::cos(th), std::sin(th) * std::sin(ph)};
+        const float rad = disp(th, ph);
+        for (int k = 0; k < 3; k++) { m.pos.push_back(rad * d[k]); m.nrm.push_back(d[k]); }
+    };
+    const uint32_t pr = std::min<uint32_t>(16, rings), ps = std::min<uint32_t>(16, seg);
+    uint32_t patch = 0;
+    for (uint32_t a = 0; a < pr; a++)
+        for (uint32_t c = 0; c < ps; c++, patch++) {
+            const uint32_t r0 = rings * a / pr, r1 = rings * (a + 1) / pr, s0 = seg * c / ps, s1 = seg * (c + 1) / ps;
+            Mesh m;
+            const uint32_t cols = s1 - s0 + 1;
+            for (uint32_t r = r0; r <= r1; r++)
+                for (uint32_t sIdx = s0; sIdx <= s1; sIdx++) vertex(r, sIdx, m);
+            for (uint32_t r = 0; r < r1 - r0; r++)
+                for (uint32_t q = 0; q < s1 - s0; q++) {
+                    const uint32_t v00 = r * cols + q, v01 = v00 + 1, v10 = v00 + cols, v11 = v10 + 1;
+                    if (r + r0 != 0) { uint32_t t[3] = {v00, v01, v10}; m.idx.insert(m.idx.end(), t, t + 3); }
+                    if (r + r0 + 1 != rings) { uint32_t t[3] = {v01, v11, v10}; m.idx.insert(m.idx.end(), t, t + 3); }
+                }
+            if (!m.idx.empty()) add_instance(*h, m, patch % nmat);
         }
-    const uint32_t bands = std::min<uint32_t>(nmat, rings);
-    for (uint32_t b = 0; b < bands; b++) {
-        uint32_t r0 = rings * b / bands, r1 = rings * (b + 1) / bands;
-        Mesh m;
-        m.pos.assign(all.pos.begin() + size_t(r0) * (seg + 1) * 3, all.pos.begin() + size_t(r1 + 1) * (seg + 1) * 3);
-        m.nrm.assign(all.nrm.begin() + size_t(r0) * (seg + 1) * 3, all.nrm.begin() + size_t(r1 + 1) * (seg + 1) * 3);
-        for (uint32_t r = 0; r < r1 - r0; r++)
-            for (uint32_t s = 0; s < seg; s++) {
-                uint32_t a = r * (seg + 1) + s, bb = a + 1, c = a + seg + 1, d = c + 1;
-                if (r + r0 != 0) { uint32_t t[3] = {a, bb, c}; m.idx.insert(m.idx.end(), t, t + 3); }
-                if (r + r0 + 1 != rings) { uint32_t t[3] = {bb, d, c}; m.idx.insert(m.idx.end(), t, t + 3); }
-            }
-        add_instance(*h, m, b % nmat);
-    }
     // Two emissive quads as area lights.
     const float elo[3] = {-0.8f, 1.3f, -0.8f}, ehi[3] = {0.8f, 1.5f, 0.8f};
     add_emitters(*h, rng, p.emissive_count ? p.emissive_count : 8, elo, ehi, 0.3f, 0.6f, 20.f, 60.f);

@@ -28,7 +28,16 @@ struct WarIsect {
     float3 normalW, tangentW;    // interpolated, unnormalised
     float tw;                    // sign of the interpolated tangent w
     uint32_t local[3];           // vertex indices within the mesh
+    uint32_t vbOffset;           // first vertex of the mesh in the scene's vertex buffer
 };
+
+// Mesh-position gradient target: one mesh (InverseOptimizationParams.meshID),
+// or every mesh with scene-global vertex indices when meshID is kAllMeshes.
+constexpr uint32_t kAllMeshes = 0xffffffffu;
+FPT_D bool war_pos_target(uint32_t meshID, const WarIsect& is) { return meshID == kAllMeshes || is.inst == meshID; }
+FPT_D uint32_t war_pos_index(uint32_t meshID, const WarIsect& is, int v) {
+    return (meshID == kAllMeshes ? is.vbOffset + is.local[v] : is.local[v]) * 3u;
+}
 
 FPT_D float war_ray_distance(float3 v0, float3 v1, float3 v2, float3 o, float3 d) {
     const float3 e1 = v1 - v0, e2 = v2 - v0;
@@ -48,6 +57,7 @@ FPT_D WarIsect war_intersect(const DevScene& s, const HitRec& h, float3 o, float
     is.local[0] = __ldg(ip);
     is.local[1] = __ldg(ip + 1);
     is.local[2] = __ldg(ip + 2);
+    is.vbOffset = inst.vbOffset;
     const PackedVertex pv0 = load_vertex(s.vertices, is.local[0] + inst.vbOffset);
     const PackedVertex pv1 = load_vertex(s.vertices, is.local[1] + inst.vbOffset);
     const PackedVertex pv2 = load_vertex(s.vertices, is.local[2] + inst.vbOffset);

@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
                                 const float3 Gf = ((g * thp) * Li) * mis;
 #pragma unroll
                                 for (int q = 0; q < 11; q++) G[q] = Gf.x * J.x.d[q] + Gf.y * J.y.d[q] + Gf.z * J.z.d[q];
-                                if (p.gradPos && is.inst == p.meshID) {
+                                if (p.gradPos && war_pos_target(p.meshID, is)) {
                                     const float3 gL = make_float3(Gf.x * J.x.d[11] + Gf.y * J.y.d[11] + Gf.z * J.z.d[11],
                                                                   Gf.x * J.x.d[12] + Gf.y * J.y.d[12] + Gf.z * J.z.d[12],
                                                                   Gf.x * J.x.d[13] + Gf.y * J.y.d[13] + Gf.z * J.z.d[13]);
@@ -199,13 +199,14 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
                                     dP += (wo * (-3.f / dist) + tls.normalW * (1.f / (dist * nlwo))) * gRatio;
                                 }
                             }
-                            const bool posGrad = p.gradPos && is.inst == p.meshID;
+                            const bool posGrad = p.gradPos && war_pos_target(p.meshID, is);
                             nee_at(ww, 0, i) = make_float4(G[0], G[1], G[2], G[3]);
                             nee_at(ww, 1, i) = make_float4(G[4], G[5], G[6], G[7]);
                             nee_at(ww, 2, i) = make_float4(G[8], G[9], G[10], __uint_as_float(sd.materialID));
                             nee_at(ww, 3, i) = make_float4(dP.x, dP.y, dP.z, __uint_as_float(posGrad ? 1u : 0u));
-                            nee_at(ww, 4, i) = make_float4(is.b[0], is.b[1], is.b[2], __uint_as_float(is.local[0]));
-                            nee_at(ww, 5, i) = make_float4(__uint_as_float(is.local[1]), __uint_as_float(is.local[2]), 0.f, 0.f);
+                            nee_at(ww, 4, i) = make_float4(is.b[0], is.b[1], is.b[2], __uint_as_float(war_pos_index(p.meshID, is, 0)));
+                            nee_at(ww, 5, i) = make_float4(__uint_as_float(war_pos_index(p.meshID, is, 1)),
+                                                           __uint_as_float(war_pos_index(p.meshID, is, 2)), 0.f, 0.f);
                             nee_at(ww, 6, i) = make_float4(weight.x, weight.y, weight.z, 0.f);
                         }
                     }
@@ -270,11 +271,11 @@ __global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(WarParams p, WavePara
         if (p.gradPos && __float_as_uint(d.w)) {
             const float4 bb = nee_at(ww, 4, i), ll = nee_at(ww, 5, i);
             const float bw[3] = {bb.x, bb.y, bb.z};
-            const uint32_t loc[3] = {__float_as_uint(bb.w), __float_as_uint(ll.x), __float_as_uint(ll.y)};
+            const uint32_t loc[3] = {__float_as_uint(bb.w), __float_as_uint(ll.x), __float_as_uint(ll.y)};  // gradient offsets
             float* gp = p.gradPos + size_t(war_hash(pid, p.posHash)) * p.posDim;
 #pragma unroll
             for (int v = 0; v < 3; v++) {
-                const uint32_t o = loc[v] * 3;
+                const uint32_t o = loc[v];
                 if (o + 3 > p.posDim) continue;
                 atomicAdd(gp + o, bw[v] * d.x);
                 atomicAdd(gp + o + 1, bw[v] * d.y);

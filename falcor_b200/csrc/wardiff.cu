@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                                         const DV3<14> J = eval_jacobian<14, HAS_T>(mi, mp, sd.frontFacing, wiL, woL);
                                         const float3 Gf = ((g * thp) * Li) * mis;
                                         add_material_grads<14>(p, hash, sd.materialID, J, Gf);
-                                        if (p.gradPos && is.inst == p.meshID) {
+                                        if (p.gradPos && war_pos_target(p.meshID, is)) {
                                             // Through wo = (L - P) / |L - P| and the ratio a2s / detach(a2s).
                                             const float3 gL = make_float3(Gf.x * J.x.d[11] + Gf.y * J.y.d[11] + Gf.z * J.z.d[11],
                                                                           Gf.x * J.x.d[12] + Gf.y * J.y.d[12] + Gf.z * J.z.d[12],
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                                             float* gp = p.gradPos + size_t(hashPos) * p.posDim;
 #pragma unroll
                                             for (int i = 0; i < 3; i++) {
-                                                const uint32_t o = is.local[i] * 3;
+                                                const uint32_t o = war_pos_index(p.meshID, is, i);
                                                 if (o + 3 > p.posDim) continue;
                                                 atomicAdd(gp + o, is.b[i] * dP.x);
                                                 atomicAdd(gp + o + 1, is.b[i] * dP.y);
@@ -380,7 +380,8 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
     p.useMIS = pass.num("useMIS") != 0;
     p.useAntithetic = pass.num("useAntitheticSampling") != 0;
     p.lambert = pass.str("diffuseBrdf") == "Lambert";
-    p.meshID = uint32_t(pass.num("meshToOptimize"));
+    const double mesh = pass.num("meshToOptimize");
+    p.meshID = mesh < 0 ? 0xffffffffu : uint32_t(mesh);  // -1: every mesh, scene-global vertex indices
     p.frameSeed = pass.useFixedSeed ? uint32_t(pass.num("fixedSeed")) : pass.frameCount;
     p.counters = static_cast<unsigned long long*>(pass.scratch);
     if (p.width == 0 || p.height == 0) return set_error(FPT_ERR_INVALID_ARG, "WARDiffPathTracer: empty frame");

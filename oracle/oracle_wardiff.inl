@@ -106,12 +106,15 @@ static WarIsect<R> war_intersection(const Scene& s, const WarSeeds& seeds, const
     const float t = war_ray_distance(v, o, d);
     V3<float> p = o + d * t;
     war_barycentrics(v, p, is.b);
-    const bool seeded = h.instanceID == seeds.meshID;
+    // meshID 0xffffffff seeds every mesh by scene-global vertex index.
+    const bool all = seeds.meshID == 0xffffffffu;
+    const bool seeded = all || h.instanceID == seeds.meshID;
     V3<R> vr[3];
     for (int i = 0; i < 3; i++) {
         is.localIdx[i] = idx[i] - vb;
+        const uint32_t gi = all ? idx[i] : is.localIdx[i];
         for (int a = 0; a < 3; a++)
-            vr[i][a] = seeded ? Seed<R>::pos(seeds, is.localIdx[i] * 3 + a, v[i][a]) : R(v[i][a]);
+            vr[i][a] = seeded ? Seed<R>::pos(seeds, gi * 3 + a, v[i][a]) : R(v[i][a]);
     }
     is.posW = vr[0] * R(is.b[0]) + vr[1] * R(is.b[1]) + vr[2] * R(is.b[2]);
     // loadVertexNormalsW / loadVertexTangentsW (identity world matrices).

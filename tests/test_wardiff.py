@@ -214,3 +214,59 @@ def test_autograd_material_params(fpt):
     assert float(img2.sum()) < float(img.detach().sum())
     s.set_material_params(list(range(nm)), params0.cpu().numpy())
     assert np.allclose(s.get_material_params(list(range(nm))), params0.cpu().numpy())
+
+
+def small_sphere():
+    from falcor_b200.scene import HostScene, DISPLACED_SPHERE
+    return HostScene.procedural(DISPLACED_SPHERE, seed=3, material_count=64, sphere_subdiv=48, emissive_count=4, aspect_ratio=1.0)
+
+
+def test_oracle_all_meshes_finite_differences(oracle):
+    """Displaced sphere in patches (one material each), every vertex position
+    (meshToOptimize = -1, scene-global vertex indices), maxBounces 4."""
+    host = small_sphere()
+    osc = H.oracle_scene(host)
+    W = Hh = 40
+    p = war_params(W, Hh, max_bounces=4, mesh=0xFFFFFFFF)
+    rng = np.random.default_rng(9)
+    dLdI = rng.standard_normal((Hh, W, 3)).astype(np.float32)
+    P = rng.standard_normal((1, host.desc.vertex_count * 3)) * 0.1
+    _, g, _, _, _ = osc.wardiff(p, mode=1, dLdI=dLdI, pos_tangents=P)
+    eps = 1e-4
+    _, _, pp, _, _ = osc.wardiff(p, mode=2, pos_tangents=P, eps=eps)
+    _, _, pm, _, _ = osc.wardiff(p, mode=2, pos_tangents=P, eps=-eps)
+    fd = float(np.sum(dLdI.astype(np.float64) * (pp - pm) / (2 * eps)))
+    assert abs(g[0]) > 1e-6
+    assert abs(fd - g[0]) <= 1e-5 * max(1.0, abs(g[0])), (fd, g[0])
+
+
+@pytest.mark.gpu
+def test_adjoint_all_meshes_matches_oracle(fpt, oracle):
+    import torch
+    from falcor_b200.passes import WARDiffPathTracer
+    host = small_sphere()
+    W, Hh = 64, 64
+    osc = H.oracle_scene(host)
+    rng = np.random.default_rng(12)
+    dLdI = rng.standard_normal((Hh, W, 3)).astype(np.float32)
+    nm, nv = host.desc.material_count, host.desc.vertex_count
+    T = rng.standard_normal((2, nm * 20))
+    T[:, np.arange(nm * 20) % 20 >= 6] = 0
+    P = rng.standard_normal((2, nv * 3)) * 0.1
+    _, gm_ref, _, _, _ = osc.wardiff(war_params(W, Hh, max_bounces=4, mesh=0xFFFFFFFF), mode=1, dLdI=dLdI, mat_tangents=T)
+    _, gp_ref, _, _, _ = osc.wardiff(war_params(W, Hh, max_bounces=4, mesh=0xFFFFFFFF), mode=1, dLdI=dLdI, pos_tangents=P)
+    s = gpu_scene(host)
+    pt = WARDiffPathTracer(war_props(max_bounces=4, mesh=-1))
+    pt.set_scene(s)
+    color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
+    gm = torch.zeros(nm * 20, dtype=torch.float32, device="cuda")
+    gp = torch.zeros(nv * 3, dtype=torch.float32, device="cuda")
+    pt.backward({"color": color}, torch.from_numpy(dLdI).cuda(), material_grad=gm, position_grad=gp)
+    torch.cuda.synchronize()
+    gm = gm.cpu().numpy().astype(np.float64)
+    gp = gp.cpu().numpy().astype(np.float64)
+    for k in range(2):
+        a, b = float(T[k] @ gm), float(gm_ref[k])
+        assert abs(a - b) <= 2e-3 * max(1.0, abs(b)), ("material", k, a, b)
+        a, b = float(P[k] @ gp), float(gp_ref[k])
+        assert abs(a - b) <= 2e-3 * max(1.0, abs(b)), ("position", k, a, b)
