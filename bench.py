@@ -306,6 +306,7 @@ def main():
     from falcor_b200.scene import WORKLOADS, Scene, make_host_scene
     from falcor_b200 import _ffi
     from falcor_b200.passes import PathTracer, VBufferRT
+    from falcor_b200.replicas import max_over_ranks
 
     w = WORKLOADS[args.workload]
     host = make_host_scene(w)
@@ -362,10 +363,8 @@ def main():
         total_ms += s0.elapsed_time(s1)
     torch.cuda.synchronize()
     clk = clocks.stop()
+    total_ms = max_over_ranks(total_ms, dev)
     if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
     ms_per_step = total_ms / args.steps
     value = paths_per_step * world / (ms_per_step / 1e3) / 1e6
@@ -401,10 +400,7 @@ def main():
         host_img.copy_(accum, non_blocking=True)
         torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dev)
     e2e_value = paths_per_step * world / e2e_s / 1e6
 
     st = pt.stats()

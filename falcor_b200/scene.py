@@ -33,6 +33,57 @@ class HostScene:
         self.desc = lib().fpt_scene_host_desc(handle).contents
 
     @staticmethod
+    def from_arrays(vertices, indices, instances, materials, camera: dict, envmap=None) -> "HostScene":
+        """A scene from host arrays (the SceneBuilder inputs): vertices [N, 12]
+        float32 (position, normal, tangent xyzw, texcoord), indices [3T] uint32
+        (per-mesh local), instances [I, 5] uint32 (vb_offset, ib_offset,
+        triangle_count, material_id, flags), materials [M, 19] float32 in
+        fpt_material order, camera dict of fpt_camera fields, envmap optional
+        (rgb [H, W, 3] float32, tint, intensity)."""
+        obj = HostScene.__new__(HostScene)
+        obj._h = None
+        obj._keep = []
+
+        def arr(a, dtype, cols=None):
+            a = np.ascontiguousarray(a, dtype=dtype)
+            if cols is not None:
+                a = a.reshape(-1, cols)
+            obj._keep.append(a)
+            return a
+        v = arr(vertices, np.float32, 12)
+        ix = arr(indices, np.uint32)
+        ins = arr(instances, np.uint32, 5)
+        mats = arr(materials, np.float32, 19)
+        d = _ffi.fpt_scene_desc()
+        d.vertices = v.ctypes.data_as(C.POINTER(_ffi.fpt_vertex)) if len(v) else None
+        d.vertex_count = len(v)
+        d.indices = ix.ctypes.data_as(C.POINTER(C.c_uint32)) if len(ix) else None
+        d.index_count = len(ix)
+        d.instances = ins.ctypes.data_as(C.POINTER(_ffi.fpt_geometry_instance)) if len(ins) else None
+        d.instance_count = len(ins)
+        d.materials = mats.ctypes.data_as(C.POINTER(_ffi.fpt_material))
+        d.material_count = len(mats)
+        cam = _ffi.fpt_camera()
+        for k, val in camera.items():
+            f = getattr(cam, k)
+            if isinstance(f, float):
+                setattr(cam, k, float(val))
+            else:
+                for i, x in enumerate(val):
+                    f[i] = float(x)
+        d.camera = cam
+        if envmap is not None:
+            rgb = arr(envmap["rgb"], np.float32)
+            env = _ffi.fpt_envmap_desc(width=rgb.shape[1], height=rgb.shape[0], rgb=rgb.ctypes.data_as(C.POINTER(C.c_float)),
+                                      intensity=float(envmap.get("intensity", 1.0)))
+            for i in range(3):
+                env.tint[i] = float(envmap.get("tint", (1, 1, 1))[i])
+            obj._keep.append(env)
+            d.envmap = C.pointer(env)
+        obj.desc = d
+        return obj
+
+    @staticmethod
     def procedural(kind: int, seed: int = 0, grid_res: int = 0, soup_triangles: int = 0, material_count: int = 0,
                    emissive_count: int = 0, sphere_subdiv: int = 0, envmap: tuple[int, int] | None = None,
                    aspect_ratio: float = 0.0) -> "HostScene":
