@@ -57,7 +57,7 @@ struct fpt_batch {
     std::vector<uint32_t> frameReq;          // frame -> request
     fpt_pass* ptDefaults = nullptr;          // PathTracer pass holding the property defaults
     // tuning
-    uint32_t capacity = 1u << 22;
+    uint32_t capacity = 1u << 24;
     int shadeScale = 1;
     bool tuned = false;
     // device state of the batched launch
@@ -306,7 +306,7 @@ FPT_API fpt_status fpt_batch_get_tuning(const fpt_batch* b, uint32_t* wave_capac
 FPT_API fpt_status fpt_batch_autotune(fpt_batch* b, void* stream) {
     if (!b || b->reqs.empty()) return set_error(FPT_ERR_INVALID_ARG, "fpt_batch_autotune: empty batch");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const uint32_t caps[] = {1u << 20, 1u << 21, 1u << 22, 1u << 23};
+    const uint32_t caps[] = {1u << 21, 1u << 22, 1u << 23, 1u << 24, 1u << 25};
     const int scales[] = {1, 2};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);

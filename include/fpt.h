@@ -415,7 +415,7 @@ FPT_API fpt_status fpt_batch_add(fpt_batch* batch, const fpt_batch_request* req)
  * occupancy-sized shade grid; 0 keeps the current value. */
 FPT_API fpt_status fpt_batch_set_tuning(fpt_batch* batch, uint32_t wave_capacity, uint32_t shade_grid_scale);
 FPT_API fpt_status fpt_batch_get_tuning(const fpt_batch* batch, uint32_t* wave_capacity, uint32_t* shade_grid_scale);
-/* Times the batched launch over wave capacities 2^20..2^23 and shade grid
+/* Times the batched launch over wave capacities 2^21..2^25 and shade grid
  * scales 1, 2 on the current requests and keeps the fastest. */
 FPT_API fpt_status fpt_batch_autotune(fpt_batch* batch, void* stream);
 /* All requests as one CUDA graph (built on first call, relaunched after):
