@@ -116,8 +116,11 @@ FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uin
 
 // handleHit / handleMiss for every path of the shade queue.  The hit flag of
 // a path is PF_HIT (0x2) in its flags.
+#ifndef FPT_SHADE_MIN_BLOCKS
+#define FPT_SHADE_MIN_BLOCKS 6  // 80 registers (some spills) beat 126 registers at 4 blocks by 8 %
+#endif
 template <class SG, bool HAS_T, bool MULTI>
-__global__ void __launch_bounds__(kShadeBlock) wf_shade(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+__global__ void __launch_bounds__(kShadeBlock, FPT_SHADE_MIN_BLOCKS) wf_shade(DevScene s, FrameParams p, WaveParams wp, SoA w) {
     Counters cnt;
     const uint32_t n = wp.counts[0];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k - threadIdx.x < n; k += gridDim.x * blockDim.x) {
