@@ -47,6 +47,8 @@ def parse_args():
     ap.add_argument("--resolution", default=None, help="WxH override of the workload's frame size (small profiling cases)")
     ap.add_argument("--frames-per-step", type=int, default=FRAMES_PER_STEP, help="16-spp frames per step")
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched secondary metrics")
+    ap.add_argument("--only", choices=["adjoint", "batched"], default=None,
+                    help="run one secondary metric alone and print it (profiling entry point)")
     return ap.parse_args()
 
 
@@ -292,6 +294,16 @@ def main():
         return
     import torch
     import torch.distributed as dist
+
+    if args.only:
+        from falcor_b200 import build
+        build.build()
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+        torch.cuda.set_device(dev)
+        res = adjoint_bench(dev) if args.only == "adjoint" else batched_bench(dev)
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({args.only: res}), flush=True)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
