@@ -34,7 +34,8 @@ class PathTracerParams(C.Structure):
 
 class WarDiffParams(C.Structure):
     _fields_ = [("width", u32), ("height", u32), ("maxBounces", u32), ("useBSDFSampling", u32), ("useNEE", u32),
-                ("useMIS", u32), ("useAntithetic", u32), ("seed", u32), ("lambert", u32), ("meshID", u32)]
+                ("useMIS", u32), ("useAntithetic", u32), ("seed", u32), ("lambert", u32), ("meshID", u32),
+                ("useWAR", u32), ("auxSampleCount", u32), ("log10Kappa", C.c_float), ("log10KappaScreen", C.c_float)]
 
 
 class SceneInfo(C.Structure):

@@ -46,7 +46,11 @@ struct WarDiffParams {           // WARDiffPathTracer static + runtime parameter
     uint32_t useAntithetic;      // default 1
     uint32_t seed;               // frame seed (fixedSeed or frame count)
     uint32_t lambert;
-    uint32_t meshID;             // mesh whose vertex positions are differentiated
+    uint32_t meshID;             // mesh whose vertex positions are differentiated (0xffffffff: all)
+    uint32_t useWAR;             // warped-area reparameterisation (pass default 1)
+    uint32_t auxSampleCount;     // auxiliary rays per reparameterisation (default 16)
+    float log10Kappa;            // Log10vMFConcentration (default 5)
+    float log10KappaScreen;      // Log10vMFConcentrationScreen (default 5)
 };
 
 struct WarSeeds {

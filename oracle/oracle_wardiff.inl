@@ -30,10 +30,11 @@
 //  * The Gaussian pixel-filter ratio and the area-to-solid-angle ratio are
 //    x / detach(x) (WARDiffPathTracer.rt.slang:92-93, PTUtils.slang:238):
 //    value 1, derivative dx / x.
-// The warped-area reparameterisation (useWAR) leaves every value unchanged (its
-// weight is det(I + infinitesimal J) = 1 and its direction offset is an
-// infinitesimal, WarpedAreaReparam.slang:226-263) and is not restated here:
-// this oracle covers the primal and the interior (useWAR = false) gradients.
+// The warped-area reparameterisation (useWAR, WarpedAreaReparam.slang:226-332)
+// leaves every value unchanged -- its weight is det(I + infinitesimal J) = 1 and
+// its offsets are infinitesimals -- so it only runs for the derivative types;
+// it adds the boundary term of the gradient through the warped screen sample,
+// the warped NEE direction and the warped scatter direction.
 
 template <class R> struct Seed;
 template <> struct Seed<float> {
@@ -128,6 +129,205 @@ static WarIsect<R> war_intersection(const Scene& s, const WarSeeds& seeds, const
     return is;
 }
 
+// ---------------------------------------------------------------------------
+// Warped-area reparameterisation (WarpedAreaReparam.slang:52-332).
+// Every quantity it adds is infinitesimal (x - detach(x)): the primal is
+// unchanged, and only R = Dual / Shadow carry its derivative.  The inner
+// forward derivative with respect to the ray direction (the Jacobian J) uses
+// the custom derivative of computeHarmonicWeight (:74-98) and is written out
+// explicitly; the outer derivative with respect to the scene comes from R.
+// The harmonic weights themselves carry no outer derivative: their custom
+// forward derivative returns a primal that depends on no differentiable input.
+// ---------------------------------------------------------------------------
+template <class R> static R infinitesimal(const R& x) { return x - detach(x); }
+template <class R> static V3<R> infinitesimal3(const V3<R>& v) { return V3<R>(infinitesimal(v.x), infinitesimal(v.y), infinitesimal(v.z)); }
+// normalizeSafe (Utils/Math/MathHelpers.slang:767-771).
+template <class R> static V3<R> normalize_safe(const V3<R>& v) {
+    R len = length(v);
+    return len > R(0) ? v / len : V3<R>(R(0));
+}
+// Directional derivative of normalizeSafe at v along dv.
+template <class R> static V3<R> d_normalize_safe(const V3<R>& v, const V3<R>& dv) {
+    R len = length(v);
+    if (!(len > R(0))) return V3<R>(R(0));
+    V3<R> n = v / len;
+    return (dv - n * dot(n, dv)) / len;
+}
+template <class R> static R clampR(R x, R lo, R hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+// AttachToGeometry intersection of an auxiliary ray (DiffSceneQuery.slang:160-184):
+// the barycentrics of the traversal hit are fixed; the position comes from the
+// (seeded) vertices, the normal is the interpolated vertex normal.
+template <class R>
+static bool war_aux_hit(const Scene& s, const WarSeeds& seeds, V3<float> o, V3<float> d, V3<R>& posW, V3<float>& normalW) {
+    Hit h = s.traceClosest(o, d, 0.f, std::numeric_limits<float>::max(), nullptr);
+    if (!h.valid) return false;
+    uint32_t idx[3];
+    s.getTriangleVertexIndices(h.instanceID, h.primitiveIndex, idx);
+    const uint32_t vb = s.instances[h.instanceID].vb_offset;
+    const float b[3] = {1.f - h.baryX - h.baryY, h.baryX, h.baryY};
+    const bool all = seeds.meshID == 0xffffffffu;
+    const bool seeded = all || h.instanceID == seeds.meshID;
+    V3<R> vr[3];
+    V3<float> n[3];
+    for (int i = 0; i < 3; i++) {
+        const StaticVertex sv = s.getVertex(idx[i]);
+        const uint32_t gi = all ? idx[i] : idx[i] - vb;
+        for (int a = 0; a < 3; a++) vr[i][a] = seeded ? Seed<R>::pos(seeds, gi * 3 + a, sv.position[a]) : R(sv.position[a]);
+        n[i] = normalize(sv.normal);
+    }
+    posW = vr[0] * R(b[0]) + vr[1] * R(b[1]) + vr[2] * R(b[2]);
+    normalW = n[0] * b[0] + n[1] * b[1] + n[2] * b[2];
+    return true;
+}
+
+// traceAsymptoticWeightedMeanIntersection<J> (WarpedAreaReparam.slang:111-193):
+// the mean direction M (identical for every j) and its derivative dM[j] along
+// the tangent dirD[j] of direction j.
+template <class R, int J>
+static void war_mean(const Scene& s, const WarSeeds& seeds, const WarDiffParams& p, float kappa, const V3<R>& origin,
+                     V3<float> baseDir, const V3<R> dirP[J], const V3<R> dirD[J], UniformSG sg, V3<R>& M, V3<R> dM[J]) {
+    const uint32_t N = p.auxSampleCount;
+    std::vector<float> rnd(N + 1, 0.f);
+    for (uint32_t i = 0; i < N; i++) rnd[i] = next1D<float>(sg);
+    // ShadingFrame(baseDirection, float4(perp_stark(baseDirection), 1)) (Utils/Math/ShadingFrame.slang:47-51, 114-118).
+    const V3<float> t = perp_stark(baseDir);
+    const V3<float> Nn = normalize(baseDir);
+    const V3<float> T = normalize(t - Nn * dot(t, Nn));
+    const V3<float> B = cross(Nn, T) * 1.f;
+    R W(0);
+    V3<R> MW(R(0));
+    R dWs[J];
+    V3<R> dMW[J];
+    for (int j = 0; j < J; j++) { dWs[j] = R(0); dMW[j] = V3<R>(R(0)); }
+    const V3<float> ov = val3(origin);
+    for (uint32_t i = 0; i < N; i++) {
+        V2<float> smp;
+        if (p.useAntithetic) {
+            const uint32_t a = i / 2;
+            smp = V2<float>(rnd[a * 2], rnd[a * 2 + 1]);
+        } else {
+            smp = next2D<float>(sg);
+        }
+        const V3<float> dl = sample_von_mises_fisher(smp, kappa);
+        V3<float> auxDir = normalize(T * dl.x + B * dl.y + Nn * dl.z);
+        if (p.useAntithetic && i % 2 == 1) {
+            const V3<float> ii = -auxDir;
+            auxDir = ii - baseDir * (2.f * dot(baseDir, ii));  // reflect(-auxDirection, baseDirection)
+        }
+        V3<R> dirW = lift3<R>(auxDir);
+        V3<float> isectN(0.f);
+        V3<R> P;
+        if (war_aux_hit<R>(s, seeds, ov, auxDir, P, isectN)) dirW = normalize_safe(P - origin);
+        // computeHarmonicWeight and fwd_computeHarmonicWeight (WarpedAreaReparam.slang:52-98).
+        float bt = dot(isectN, auxDir);
+        bt = bt * bt;
+        const float sy = std::max(1.f - smp.y, 1e-6f);
+        const float invVMF = 1.f / ((1.f - sy) * std::exp(-2.f * kappa) + sy);
+        const float wDenom = invVMF - 1.f + bt;
+        const float wDenomRcp = wDenom > 1e-4f ? 1.f / wDenom : 0.f;
+        const float w = wDenomRcp * wDenomRcp * wDenomRcp * invVMF;
+        const float tmp1 = invVMF * w * wDenomRcp * kappa * 3;
+        W += R(w);
+        MW += dirW * R(w);
+        for (int j = 0; j < J; j++) {
+            const V3<R> tmp2 = -cross(dirP[j], cross(dirP[j], dirD[j]));
+            const R dW = clampR(R(tmp1) * dot(tmp2, lift3<R>(auxDir)), R(-1e10f), R(1e10f));
+            dWs[j] += dW;
+            dMW[j] += dirW * dW;
+        }
+    }
+    // totalWeight = max(totalWeight, 1e-8f); warpedDirection = total / totalWeight.
+    const bool pass = W > R(1e-8f);
+    const R Wc = pass ? W : R(1e-8f);
+    M = MW / Wc;
+    for (int j = 0; j < J; j++) {
+        const R dW = pass ? dWs[j] : R(0);
+        dM[j] = (dMW[j] * Wc - MW * dW) / (Wc * Wc);
+    }
+}
+
+template <class R> static R det3(const V3<R> r[3]) {
+    return r[0].x * (r[1].y * r[2].z - r[1].z * r[2].y) - r[0].y * (r[1].x * r[2].z - r[1].z * r[2].x) +
+           r[0].z * (r[1].x * r[2].y - r[1].y * r[2].x);
+}
+
+// reparameterizeRay (WarpedAreaReparam.slang:226-263): returns det(I + J) and
+// adds the infinitesimal warp to `dir`.  The mean direction is never replaced
+// by the unwarped one: the clamped total weight keeps the success test true.
+template <class R>
+static R war_reparam_ray(const Scene& s, const WarSeeds& seeds, const WarDiffParams& p, const V3<R>& origin, V3<R>& dir,
+                         UniformSG sg) {
+    const float kappa = std::pow(10.f, p.log10Kappa);
+    const V3<R> dirP[3] = {dir, dir, dir};
+    const V3<R> dirD[3] = {V3<R>(R(1), R(0), R(0)), V3<R>(R(0), R(1), R(0)), V3<R>(R(0), R(0), R(1))};
+    V3<R> M, dM[3];
+    war_mean<R, 3>(s, seeds, p, kappa, origin, val3(dir), dirP, dirD, sg, M, dM);
+    const V3<R> n = normalize_safe(M);
+    V3<R> rows[3];
+    for (int j = 0; j < 3; j++) {
+        rows[j] = infinitesimal3(d_normalize_safe(M, dM[j]));
+        rows[j][j] = rows[j][j] + R(1);
+    }
+    dir = dir + infinitesimal3(n);
+    return det3(rows);
+}
+
+// computeCameraRayDirection (DiffSceneQuery.slang:314-323) and its derivative
+// along screen axis j.
+template <class R> static V3<R> war_cam_dir(const fpt_camera_data& c, V2<R> posS, float W, float H) {
+    const V2<R> q(posS.x / R(W), posS.y / R(H));
+    const V2<R> ndc(R(2) * q.x + R(-1), R(-2) * q.y + R(1));
+    return normalize_safe(ndc.x * cam_vec<R>(c.cameraU) + ndc.y * cam_vec<R>(c.cameraV) + cam_vec<R>(c.cameraW));
+}
+template <class R> static V3<R> war_d_cam_dir(const fpt_camera_data& c, V2<R> posS, float W, float H, int j) {
+    const V2<R> q(posS.x / R(W), posS.y / R(H));
+    const V2<R> ndc(R(2) * q.x + R(-1), R(-2) * q.y + R(1));
+    const V3<R> u = ndc.x * cam_vec<R>(c.cameraU) + ndc.y * cam_vec<R>(c.cameraV) + cam_vec<R>(c.cameraW);
+    const V3<R> du = j == 0 ? cam_vec<R>(c.cameraU) * (R(2) / R(W)) : cam_vec<R>(c.cameraV) * (R(-2) / R(H));
+    return d_normalize_safe(u, du);
+}
+// computeCameraRayScreenPos (DiffSceneQuery.slang:292-312) and its derivative along dv.
+template <class R> static void war_screen_pos(const fpt_camera_data& c, V3<R> v, V3<R> dv, float Wd, float Hd, V2<R>& pos, V2<R>& dpos) {
+    const V3<R> U = cam_vec<R>(c.cameraU), Vv = cam_vec<R>(c.cameraV), Wc = cam_vec<R>(c.cameraW);
+    const V3<R> rn = normalize_safe(v);
+    const V3<R> drn = d_normalize_safe(v, dv);
+    const R ww = dot(Wc, Wc), wr = dot(Wc, rn);
+    const V3<R> F = rn * ww / wr;
+    const V3<R> dF = drn * ww / wr - rn * (ww * dot(Wc, drn) / (wr * wr));
+    const V3<R> Nc = F - Wc;
+    const R uu = dot(U, U), vv = dot(Vv, Vv);
+    const V2<R> ndc(dot(Nc, U) / uu, dot(Nc, Vv) / vv);
+    const V2<R> dndc(dot(dF, U) / uu, dot(dF, Vv) / vv);
+    const V2<R> pp((ndc.x + R(1)) / R(2), (ndc.y + R(-1)) / R(-2));
+    pos = V2<R>(pp.x * R(Wd) - R(0.5f), pp.y * R(Hd) - R(0.5f));
+    dpos = V2<R>(dndc.x / R(2) * R(Wd), dndc.y / R(-2) * R(Hd));
+}
+
+// reparameterizeScreenSample (WarpedAreaReparam.slang:270-332): returns
+// det(I + J) and adds the infinitesimal warp to the screen sample.
+template <class R>
+static R war_reparam_screen(const Scene& s, const WarSeeds& seeds, const WarDiffParams& p, V2<R>& posS, UniformSG sg) {
+    const float kappa = std::pow(10.f, p.log10KappaScreen);
+    const fpt_camera_data& c = s.camera;
+    const float Wd = float(p.width), Hd = float(p.height);
+    const V2<R> pv(detach(posS.x), detach(posS.y));
+    const V3<R> base = war_cam_dir<R>(c, pv, Wd, Hd);
+    const V3<R> dirP[2] = {base, base};
+    const V3<R> dirD[2] = {war_d_cam_dir<R>(c, pv, Wd, Hd, 0), war_d_cam_dir<R>(c, pv, Wd, Hd, 1)};
+    const V3<R> origin = cam_vec<R>(c.posW);
+    V3<R> M, dM[2];
+    war_mean<R, 2>(s, seeds, p, kappa, origin, val3(base), dirP, dirD, sg, M, dM);
+    const V3<R> n = normalize_safe(M);
+    V2<R> pos0, d0, pos1, d1;
+    war_screen_pos<R>(c, n, d_normalize_safe(M, dM[0]), Wd, Hd, pos0, d0);
+    war_screen_pos<R>(c, n, d_normalize_safe(M, dM[1]), Wd, Hd, pos1, d1);
+    const R a = R(1) + infinitesimal(d0.x), b = infinitesimal(d0.y);
+    const R cc = infinitesimal(d1.x), d = R(1) + infinitesimal(d1.y);
+    posS = V2<R>(posS.x + infinitesimal(pos0.x), posS.y + infinitesimal(pos0.y));
+    return a * d - b * cc;
+}
+
 // Material instance built through GradientIOWrapper.getFloat
 // (StandardMaterial.slang:135-250); R carries the seeded derivatives.
 template <class R>
@@ -213,8 +413,18 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
     path.radiance = V3<R>(R(0));
     path.thp = V3<R>(R(1));
     path.normal = V3<float>(0.f);
-    // The pixel-filter ratio w / detach(w) has value 1; its derivative only
-    // exists through the warped screen sample (useWAR), not restated here.
+    // The warped-area reparameterisation only changes derivatives (see above).
+    const bool war = p.useWAR && p.auxSampleCount > 0 && !std::is_same<R, float>::value;
+    V2<R> pixR(R(pix.x), R(pix.y));
+    if (war) {
+        // tracePath (WARDiffPathTracer.rt.slang:80-89): warped screen sample, then
+        // the Gaussian pixel-filter ratio w / detach(w) (value 1).
+        path.thp *= war_reparam_screen<R>(s, seeds, p, pixR, sg);
+        const V2<R> xy(pixR.x - R(pixelf.x), pixR.y - R(pixelf.y));
+        const R alpha = R(-1.f / (2.f * sigma * sigma));
+        const R pw = std::exp(alpha * (xy.x * xy.x + xy.y * xy.y)) * R(1.f / (2.f * 3.14159265358979323846f * sigma * sigma));
+        path.thp *= pw / detach(pw);
+    }
 
     // computeCameraRayDirection (DiffSceneQuery.slang:314-323).
     const fpt_camera_data& c = s.camera;
@@ -225,6 +435,8 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
     float len = length(dirU);
     V3<float> rayDir = len > 0.f ? dirU / len : V3<float>(0.f);
     V3<float> rayOrigin(c.posW[0], c.posW[1], c.posW[2]);
+    // Differentiable ray direction: sd.V = -rayDir (PTUtils.slang:112).
+    V3<R> rayDirR = war ? war_cam_dir<R>(c, pixR, float(p.width), float(p.height)) : lift3<R>(rayDir);
 
     if (wc) wc->rays++;
     Hit h = s.traceClosest(rayOrigin, rayDir, 0.f, std::numeric_limits<float>::max(), nullptr);
@@ -267,7 +479,8 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
         }
         const MaterialInstance<float> miV = war_material<float>(s, WarSeeds(), sd, p.lambert != 0);
         const MaterialInstance<R> miR = war_material<R>(s, seeds, sd, p.lambert != 0);
-        const ShadingData<R> sdR = sd_lift<R>(sd);
+        ShadingData<R> sdR = sd_lift<R>(sd);
+        sdR.V = -rayDirR;
 
         const bool isPrimaryHit = path.length == 0;
         const bool computeEmissive = isPrimaryHit || (useEmissive && (!p.useNEE || p.useMIS));
@@ -302,6 +515,12 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
                         R dist = length(wo);
                         wo /= dist;
                         V3<R> thp = path.thp;
+                        if (war) {
+                            // computeRayOrigin passes the position derivative through.
+                            const V3<float> o = compute_ray_origin(posV, sd.frontFacing ? sd.faceN : -sd.faceN);
+                            const V3<R> originR = lift3<R>(o) + infinitesimal3(is.posW);
+                            thp *= war_reparam_ray<R>(s, seeds, p, originR, wo, sg);
+                        }
                         R a2s = (dist * dist) / dot(lift3<R>(tls.normalW), -wo);
                         V3<R> bsdfValue = miR.eval(sdR, wo);
                         V3<R> weight = ((lift3<R>(Li) * bsdfValue) * a2s) / detach(a2s);
@@ -320,7 +539,12 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
         if (!(miV.sample(sd, sg, bs, p.useBSDFSampling != 0) && bs.pdf > 0.f)) { path.terminated = true; break; }
         rayDir = bs.wo;
         rayOrigin = compute_ray_origin(val3(is.posW), sd.frontFacing ? sd.faceN : -sd.faceN);
-        V3<R> bsdfWeight = miR.eval(sdR, lift3<R>(bs.wo)) / R(bs.pdf);
+        rayDirR = lift3<R>(bs.wo);
+        if (war) {
+            const V3<R> originR = lift3<R>(rayOrigin) + infinitesimal3(is.posW);
+            path.thp *= war_reparam_ray<R>(s, seeds, p, originR, rayDirR, sg);
+        }
+        V3<R> bsdfWeight = miR.eval(sdR, rayDirR) / R(bs.pdf);
         path.thp *= bsdfWeight;
         path.normal = sd.orientedFaceN();
         path.pdf = bs.pdf;

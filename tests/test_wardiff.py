@@ -18,10 +18,11 @@ import pytest
 from tests import helpers as H
 
 
-def war_params(w, h, seed=3, max_bounces=2, mesh=0):
+def war_params(w, h, seed=3, max_bounces=2, mesh=0, war=False, aux=16):
     from oracle.ffi import WarDiffParams
     return WarDiffParams(width=w, height=h, maxBounces=max_bounces, useBSDFSampling=1, useNEE=1, useMIS=1, useAntithetic=1,
-                         seed=seed, lambert=0, meshID=mesh)
+                         seed=seed, lambert=0, meshID=mesh, useWAR=int(war), auxSampleCount=aux, log10Kappa=5.0,
+                         log10KappaScreen=5.0)
 
 
 def war_props(max_bounces=2, seed=3, mesh=0, mode="BackwardDiff", scheduler="Wavefront"):
@@ -62,8 +63,12 @@ def tangents(host, rng, mesh, k=2):
 # ---------------------------------------------------------------------------
 # CPU: the oracle's derivatives against finite differences.
 # ---------------------------------------------------------------------------
+@pytest.mark.parametrize("war", [False, True])
 @pytest.mark.parametrize("scene", ["box", "heightfield"])
-def test_oracle_gradients_match_finite_differences(oracle, scene):
+def test_oracle_gradients_match_finite_differences(oracle, scene, war):
+    """With war=True the derivative includes the warped-area boundary terms
+    (screen, NEE and scatter reparameterisations); the finite differences
+    perturb the same program, whose warps are infinitesimal offsets."""
     host = H.box_icosphere(3) if scene == "box" else H.small_heightfield(materials=8, emitters=8)
     osc = H.oracle_scene(host)
     W = Hh = 40
@@ -71,6 +76,7 @@ def test_oracle_gradients_match_finite_differences(oracle, scene):
     rng = np.random.default_rng(7)
     dLdI = rng.standard_normal((Hh, W, 3)).astype(np.float32)
     mesh = pick_mesh(osc, host, p, dLdI)
+    p.useWAR = int(war)
     T, P = tangents(host, rng, mesh, k=1)
     for kind in ("mat", "pos"):
         kw = {"mat_tangents": T} if kind == "mat" else {"pos_tangents": P}
