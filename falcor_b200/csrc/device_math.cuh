@@ -33,6 +33,7 @@ FPT_D float3 operator*(float s, float3 a) { return make_float3(s * a.x, s * a.y,
 FPT_D float3 operator/(float3 a, float s) { return make_float3(a.x / s, a.y / s, a.z / s); }
 FPT_D float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
 FPT_D float3& operator+=(float3& a, float3 b) { a = a + b; return a; }
+FPT_D float3& operator-=(float3& a, float3 b) { a = a - b; return a; }
 FPT_D float3& operator*=(float3& a, float3 b) { a = a * b; return a; }
 FPT_D float3& operator*=(float3& a, float s) { a = a * s; return a; }
 FPT_D float3& operator/=(float3& a, float s) { a = a / s; return a; }
@@ -219,6 +220,14 @@ FPT_D float3 perp_stark(float3 u) {
     uint32_t ym = (1u ^ xm) & uzy;
     uint32_t zm = 1u ^ (xm | ym);
     return normalize(cross(u, make_float3(float(xm), float(ym), float(zm))));
+}
+// sampleVonMisesFisher (Utils/Math/MathHelpers.slang:403-411): direction around +z.
+FPT_D float3 sample_von_mises_fisher(float2 u, float kappa) {
+    const float sy = fmaxf(1.f - u.y, 1e-6f);
+    const float phi = 6.28318530717958647692f * u.x;
+    const float cosTheta = 1.f + logf(expf(-2.f * kappa) * (1.f - sy) + sy) / kappa;
+    const float sinTheta = sqrtf(1.f - cosTheta * cosTheta);
+    return make_float3(cosf(phi) * sinTheta, sinf(phi) * sinTheta, cosTheta);
 }
 // computeRayOrigin (Utils/Geometry/GeometryHelpers.slang:51-68).
 FPT_D float ray_origin_1(float p, float n) {

@@ -48,12 +48,34 @@ FPT_D float war_ray_distance(float3 v0, float3 v1, float3 v2, float3 o, float3 d
     return dot(e2, qvec) / det;
 }
 
+// Completes a WarIsect from the hit triangle and its barycentrics; these come
+// from the ray (AttachToRay) or from a stored path vertex.
+FPT_D WarIsect war_isect_bary(const DevScene& s, uint32_t instID, uint32_t prim, float b0, float b1, float b2);
+
 FPT_D WarIsect war_intersect(const DevScene& s, const HitRec& h, float3 o, float3 d) {
-    WarIsect is;
-    is.inst = h.instanceID;
-    is.prim = h.primIndex;
     const DevInstance inst = s.instances[h.instanceID];
     const uint32_t* ip = s.indices + inst.ibOffset + h.primIndex * 3;
+    float3 v0, v1, v2, n0, n1, n2;
+    unpack_vertex(load_vertex(s.vertices, __ldg(ip) + inst.vbOffset), v0, n0);
+    unpack_vertex(load_vertex(s.vertices, __ldg(ip + 1) + inst.vbOffset), v1, n1);
+    unpack_vertex(load_vertex(s.vertices, __ldg(ip + 2) + inst.vbOffset), v2, n2);
+    // computeBarycentrics of the ray/triangle-plane point (GeometryHelpers.slang:442-482).
+    const float t = war_ray_distance(v0, v1, v2, o, d);
+    const float3 p = o + d * t;
+    const float3 e0 = v0 - p, e1 = v1 - p, e2 = v2 - p;
+    const float a0 = length(cross(e1, e2));
+    const float a1 = length(cross(e2, e0));
+    const float a2 = length(cross(e0, e1));
+    const float area = a0 + a1 + a2;
+    return war_isect_bary(s, h.instanceID, h.primIndex, a0 / area, a1 / area, a2 / area);
+}
+
+FPT_D WarIsect war_isect_bary(const DevScene& s, uint32_t instID, uint32_t prim, float b0, float b1, float b2) {
+    WarIsect is;
+    is.inst = instID;
+    is.prim = prim;
+    const DevInstance inst = s.instances[instID];
+    const uint32_t* ip = s.indices + inst.ibOffset + prim * 3;
     is.local[0] = __ldg(ip);
     is.local[1] = __ldg(ip + 1);
     is.local[2] = __ldg(ip + 2);
@@ -65,17 +87,9 @@ FPT_D WarIsect war_intersect(const DevScene& s, const HitRec& h, float3 o, float
     unpack_vertex(pv0, v0, n0);
     unpack_vertex(pv1, v1, n1);
     unpack_vertex(pv2, v2, n2);
-    // computeBarycentrics of the ray/triangle-plane point (GeometryHelpers.slang:442-482).
-    const float t = war_ray_distance(v0, v1, v2, o, d);
-    const float3 p = o + d * t;
-    const float3 e0 = v0 - p, e1 = v1 - p, e2 = v2 - p;
-    const float a0 = length(cross(e1, e2));
-    const float a1 = length(cross(e2, e0));
-    const float a2 = length(cross(e0, e1));
-    const float area = a0 + a1 + a2;
-    is.b[0] = a0 / area;
-    is.b[1] = a1 / area;
-    is.b[2] = a2 / area;
+    is.b[0] = b0;
+    is.b[1] = b1;
+    is.b[2] = b2;
     is.posW = v0 * is.b[0] + v1 * is.b[1] + v2 * is.b[2];
     // loadVertexNormalsW / loadVertexTangentsW (DiffSceneIO.slang:145-258), identity world matrices.
     n0 = normalize(n0); n1 = normalize(n1); n2 = normalize(n2);
@@ -146,13 +160,14 @@ FPT_D MatParams load_mat_params(const DevScene& s, uint32_t id) {
 }
 
 // Jacobian of one evalAD with respect to the 11 material parameters (slots
-// 0-10) and, for N = 14, the local outgoing direction (slots 11-13).
+// 0-10), for N >= 14 the local outgoing direction (slots 11-13) and, for
+// N = 17, the local incident direction (slots 14-16).
 template <int N, bool HAS_T>
 FPT_D DV3<N> eval_jacobian(const MaterialInstance<HAS_T>& mi, const MatParams& mp, bool frontFacing, float3 wiL, float3 woL) {
     const StandardBSDF<HAS_T> b = mi.bsdf(wiL);
     const DBSDFData<N> d = diff_bsdf_data<N>(mp.baseColor, mp.metallic, mp.roughness, mp.ior, mp.transmission, mp.diffTrans,
                                              mp.specTrans, frontFacing);
-    const DV3<N> wi = dv3c<N>(wiL);
+    const DV3<N> wi = N >= 17 ? dv3(dvar<N>(wiL.x, 14), dvar<N>(wiL.y, 15), dvar<N>(wiL.z, 16)) : dv3c<N>(wiL);
     const DV3<N> wo = dv3(dvar<N>(woL.x, 11), dvar<N>(woL.y, 12), dvar<N>(woL.z, 13));
     return diff_bsdf_eval<N>(d, wi, wo, mi.thin, mi.activeLobes, mi.lambert, b.pDR, HAS_T ? b.pDT : 0.f, b.pSR,
                              HAS_T ? b.pST : 0.f);

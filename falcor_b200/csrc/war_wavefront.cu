@@ -19,11 +19,23 @@
 //     A_k = dLdI * e_k + A_{k+1} * w_k,   dS/df_k(ws) = A_{k+1} * thp_k / pdf_k.
 // The NEE term's adjoint is dLdI itself, so its gradients are formed in the
 // shade kernel and applied when the visibility ray finds the light unoccluded.
+//
+// With the warped-area reparameterisation (WAR) and position gradients, the
+// records also keep what the reparameterised rays need -- the sample
+// generator state at each reparameterisation, the unwarped directions and the
+// hit -- and the adjoints of the warped directions and weights are formed
+// where they become known: the NEE warp in the nee_grad kernel (its adjoint is
+// dLdI), the scatter warps in the sweep (the adjoint of the next vertex's
+// incident direction and throughput is known once that vertex has been swept)
+// and the screen warp after the sweep.  Each one traces its auxiliary rays
+// there (war_reparam.cuh); the primal never traces them, since the warps leave
+// every value unchanged.
 #include <algorithm>
 
 #include "passes.h"
 #include "scene_device.h"
 #include "war_common.cuh"
+#include "war_reparam.cuh"
 #include "war_wavefront.h"
 #include "wavefront_common.cuh"
 
@@ -31,23 +43,37 @@ namespace fpt {
 
 namespace {
 
-// Adjoint scratch layout (float4 arrays of `capacity` entries):
-//   pending NEE gradients: 7 arrays, records: kRecArrays per vertex.
-constexpr int kNeeArrays = 7;
-constexpr int kRecArrays = 5;
+// Adjoint scratch layout (float4 arrays of `capacity` entries): the pending
+// NEE gradients (kNeeArrays, kNeeArraysWar with WAR) and, per path vertex, the
+// record (kRecArrays, kRecArraysWar with WAR).
+//   nee  0-2 material gradients, material ID   rec 0 wiL, pdf
+//        3   dP, position-gradient flag            1 wsL, material ID
+//        4-5 barycentrics, vertex offsets          2 thp, flags
+//        6   NEE weight                            3 BSDF weight
+//   WAR: 7   NEE ray origin, distance              4 emission + NEE weight
+//        8   unwarped direction, gRatio      WAR: 5 incident direction, instance
+//        9   adjoint of the warped direction      6 scatter direction, primitive
+//        10  sample generator                     7 sample generator after the BSDF sample
+//        11  adjoint of V (incident direction)    8 NEE adjoint of V, b0
+//                                                 9 b1, b2
+constexpr int kNeeArrays = 7, kNeeArraysWar = 12;
+constexpr int kRecArrays = 5, kRecArraysWar = 10;
 
 struct WarWave {
     uint32_t waveFirstPixel, wavePixels, capacity;
-    float4* nee;        // kNeeArrays x capacity
-    float4* rec;        // maxVertices x kRecArrays x capacity
+    float4* nee;        // neeArrays x capacity
+    float4* rec;        // maxVertices x recArrays x capacity
     uint32_t* nv;       // records per path
-    uint32_t maxVertices;
+    uint32_t maxVertices, recArrays;
 };
 
 FPT_D float4& nee_at(const WarWave& ww, int j, uint32_t i) { return ww.nee[size_t(j) * ww.capacity + i]; }
 FPT_D float4& rec_at(const WarWave& ww, uint32_t k, int j, uint32_t i) {
-    return ww.rec[(size_t(k) * kRecArrays + j) * ww.capacity + i];
+    return ww.rec[(size_t(k) * ww.recArrays + j) * ww.capacity + i];
 }
+FPT_D uint4& as_u4(float4& v) { return reinterpret_cast<uint4&>(v); }
+FPT_D float3 xyz(const float4& v) { return make_float3(v.x, v.y, v.z); }
+FPT_D bool nonzero(float3 v) { return v.x != 0.f || v.y != 0.f || v.z != 0.f; }
 
 // Seeds the wave: camera ray of pixel waveFirstPixel + i (tracePaths,
 // WARDiffPathTracer.rt.slang:115-143 and tracePath :75-112).
@@ -57,16 +83,8 @@ __global__ void __launch_bounds__(kShadeBlock) ww_generate(DevScene s, WarParams
         const uint32_t pid = wp.waveFirstPixel + i;
         const uint32_t x = pid % p.width, y = pid / p.width;
         UniformSG sg;
-        sg.init(x, y, p.frameSeed / 2);
-        next2D(sg);
-        next2D(sg);
-        next2D(sg);
-        const float2 u = next2D(sg);
-        const float r = sqrtf(-2.f * logf(u.x));
-        const float ang = 6.28318530717958647692f * u.y;
-        float jx = (r * cosf(ang)) * 0.5f, jy = (r * sinf(ang)) * 0.5f;
-        if (p.useAntithetic && p.frameSeed % 2 == 0) { jx = -jx; jy = -jy; }
-        const float px = (float(x) + 0.5f) + jx, py = (float(y) + 0.5f) + jy;
+        const float2 pix = war_camera_sample(p, x, y, sg);
+        const float px = pix.x, py = pix.y;
         const float qx = px / float(p.width), qy = py / float(p.height);
         const float ndcx = 2.f * qx + -1.f, ndcy = -2.f * qy + 1.f;
         const float3 dirU = load3(s.camera.cameraU) * ndcx + load3(s.camera.cameraV) * ndcy + load3(s.camera.cameraW);
@@ -90,8 +108,9 @@ __global__ void __launch_bounds__(kShadeBlock) ww_generate(DevScene s, WarParams
 }
 
 // handleHit for every path of the shade queue whose extension ray hit.
-template <bool HAS_T, bool BWD>
+template <bool HAS_T, bool BWD, bool WAR>
 __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p, WaveParams wp, SoA w, WarWave ww) {
+    constexpr int NJ = WAR ? 17 : 14;  // NEE Jacobian: material, wo and (WAR) wi slots
     Counters cnt;
     const bool useEmissive = s.hasEmissive != 0 && s.activeCount > 0;
     const uint32_t n = wp.counts[0];
@@ -131,6 +150,12 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
             rec_at(ww, vk, 1, i) = make_float4(0.f, 0.f, 0.f, __uint_as_float(sd.materialID));
             rec_at(ww, vk, 2, i) = make_float4(thp.x, thp.y, thp.z, __uint_as_float(sd.frontFacing ? 1u : 0u));
             rec_at(ww, vk, 3, i) = make_float4(0.f, 0.f, 0.f, 0.f);  // bw
+            if (WAR) {
+                rec_at(ww, vk, 5, i) = make_float4(rayDir.x, rayDir.y, rayDir.z, __uint_as_float(is.inst));
+                rec_at(ww, vk, 6, i) = make_float4(0.f, 0.f, 0.f, __uint_as_float(is.prim));
+                rec_at(ww, vk, 8, i) = make_float4(0.f, 0.f, 0.f, is.b[0]);
+                rec_at(ww, vk, 9, i) = make_float4(is.b[1], is.b[2], 0.f, 0.f);
+            }
         }
         const bool isPrimaryHit = pathLen == 0;
         const bool computeEmissive = isPrimaryHit || (useEmissive && (!p.useNEE || p.useMIS));
@@ -180,23 +205,33 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
                             float G[11];
 #pragma unroll
                             for (int q = 0; q < 11; q++) G[q] = 0.f;
-                            float3 dP = f3(0.f);
+                            float3 dP = f3(0.f), gwo = f3(0.f), gwi = f3(0.f);
+                            float gRatio = 0.f;
                             const float3 wiL = mi.toLocal(sd.V), woL = mi.toLocal(wo);
                             if (mi.valid_hemisphere(sd, wiL, woL, wo)) {
                                 const MatParams mp = load_mat_params(s, sd.materialID);
-                                const DV3<14> J = eval_jacobian<14, HAS_T>(mi, mp, sd.frontFacing, wiL, woL);
+                                const DV3<NJ> J = eval_jacobian<NJ, HAS_T>(mi, mp, sd.frontFacing, wiL, woL);
                                 const float3 Gf = ((g * thp) * Li) * mis;
 #pragma unroll
                                 for (int q = 0; q < 11; q++) G[q] = Gf.x * J.x.d[q] + Gf.y * J.y.d[q] + Gf.z * J.z.d[q];
-                                if (p.gradPos && war_pos_target(p.meshID, is)) {
+                                if (p.gradPos) {
                                     const float3 gL = make_float3(Gf.x * J.x.d[11] + Gf.y * J.y.d[11] + Gf.z * J.z.d[11],
                                                                   Gf.x * J.x.d[12] + Gf.y * J.y.d[12] + Gf.z * J.z.d[12],
                                                                   Gf.x * J.x.d[13] + Gf.y * J.y.d[13] + Gf.z * J.z.d[13]);
-                                    const float3 gwo = mi.T * gL.x + mi.B * gL.y + mi.N * gL.z;
-                                    const float gRatio = dot(Gf, make_float3(J.x.v, J.y.v, J.z.v));
-                                    const float nlwo = dot(tls.normalW, wo);
-                                    dP = (gwo - wo * dot(wo, gwo)) * (-1.f / dist);
-                                    dP += (wo * (-3.f / dist) + tls.normalW * (1.f / (dist * nlwo))) * gRatio;
+                                    gwo = mi.T * gL.x + mi.B * gL.y + mi.N * gL.z;
+                                    gRatio = dot(Gf, make_float3(J.x.v, J.y.v, J.z.v));
+                                    if (WAR) {
+                                        const int q0 = NJ - 3;  // wi slots
+                                        const float3 gI = make_float3(Gf.x * J.x.d[q0] + Gf.y * J.y.d[q0] + Gf.z * J.z.d[q0],
+                                                                      Gf.x * J.x.d[q0 + 1] + Gf.y * J.y.d[q0 + 1] + Gf.z * J.z.d[q0 + 1],
+                                                                      Gf.x * J.x.d[q0 + 2] + Gf.y * J.y.d[q0 + 2] + Gf.z * J.z.d[q0 + 2]);
+                                        gwi = mi.T * gI.x + mi.B * gI.y + mi.N * gI.z;
+                                    }
+                                    if (war_pos_target(p.meshID, is)) {
+                                        const float nlwo = dot(tls.normalW, wo);
+                                        dP = (gwo - wo * dot(wo, gwo)) * (-1.f / dist);
+                                        dP += (wo * (-3.f / dist) + tls.normalW * (1.f / (dist * nlwo))) * gRatio;
+                                    }
                                 }
                             }
                             const bool posGrad = p.gradPos && war_pos_target(p.meshID, is);
@@ -208,6 +243,19 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
                             nee_at(ww, 5, i) = make_float4(__uint_as_float(war_pos_index(p.meshID, is, 1)),
                                                            __uint_as_float(war_pos_index(p.meshID, is, 2)), 0.f, 0.f);
                             nee_at(ww, 6, i) = make_float4(weight.x, weight.y, weight.z, 0.f);
+                            if (WAR) {
+                                // computeNEE's reparameterizeRay: origin computeRayOrigin(posW, +-faceN),
+                                // direction wo, sample generator after the light sample.
+                                const float3 no = compute_ray_origin(is.posW, sd.frontFacing ? sd.faceN : -sd.faceN);
+                                // Adjoint of the warped direction: evalAD's wo and the
+                                // area-to-solid-angle ratio, d ln(a2s)/d dir = -nl / (nl . dir).
+                                const float3 gdN = gRatio != 0.f ? gwo - tls.normalW * (gRatio / dot(tls.normalW, wo)) : gwo;
+                                nee_at(ww, 7, i) = make_float4(no.x, no.y, no.z, dist);
+                                nee_at(ww, 8, i) = make_float4(wo.x, wo.y, wo.z, gRatio);
+                                nee_at(ww, 9, i) = make_float4(gdN.x, gdN.y, gdN.z, 0.f);
+                                store_sg(as_u4(nee_at(ww, 10, i)), sg);
+                                nee_at(ww, 11, i) = make_float4(gwi.x, gwi.y, gwi.z, 0.f);
+                            }
                         }
                     }
                 }
@@ -228,6 +276,10 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
                     rec_at(ww, vk, 2, i) = make_float4(thp.x, thp.y, thp.z,
                                                        __uint_as_float((sd.frontFacing ? 1u : 0u) | (valid ? 2u : 0u)));
                     rec_at(ww, vk, 3, i) = make_float4(bsdfWeight.x, bsdfWeight.y, bsdfWeight.z, 0.f);
+                    if (WAR) {
+                        rec_at(ww, vk, 6, i) = make_float4(wo.x, wo.y, wo.z, __uint_as_float(is.prim));
+                        store_sg(as_u4(rec_at(ww, vk, 7, i)), sg);
+                    }
                 }
                 thp *= bsdfWeight;
                 if (any_pos(thp)) {
@@ -251,8 +303,13 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
 
 // Applies the NEE gradients of the samples whose visibility ray found the
 // light unoccluded (sLr.w set by the shadow kernel) and adds the NEE weight to
-// the vertex's radiance increment.
-__global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(WarParams p, WaveParams wp, SoA w, WarWave ww) {
+// the vertex's radiance increment.  With WAR it also forms the gradient of the
+// NEE ray's reparameterisation and hands the adjoint of the incident
+// direction to the vertex record.
+template <bool WAR>
+__global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(DevScene s, WarParams p, WaveParams wp, SoA w, WarWave ww) {
+    __shared__ uint2 stackMem[WAR ? kStackSize * kShadeBlock : 1];
+    uint2* stack = stackMem + threadIdx.x;
     const uint32_t n = wp.counts[2];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t i = wp.shadowQueue[k];
@@ -268,6 +325,28 @@ __global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(WarParams p, WavePara
                 if (G[q] != 0.f) atomicAdd(gm + q, G[q]);
         }
         const float4 d = nee_at(ww, 3, i);
+        float3 dP = xyz(d);
+        const uint32_t vk = ww.nv[i] - 1;
+        if (WAR) {
+            const float4 o7 = nee_at(ww, 7, i), o8 = nee_at(ww, 8, i), o9 = nee_at(ww, 9, i);
+            const float3 gdN = xyz(o9);
+            const float gRatio = o8.w;  // also the adjoint of the reparameterisation weight
+            if (nonzero(gdN) || gRatio != 0.f) {
+                UniformSG sg;
+                load_sg(as_u4(nee_at(ww, 10, i)), sg);
+                const float3 wo = xyz(o8);
+                float3 gO = f3(0.f), gD = f3(0.f);
+                war_ray_grad(s, p, pid, xyz(o7), wo, true, sg, gdN, gRatio, stack, kShadeBlock, gO, gD);
+                // The origin follows posW (computeRayOrigin passes its derivative
+                // through); the unwarped direction is (P_light - posW) / dist.
+                dP += gO - (gD - wo * dot(wo, gD)) * (1.f / o7.w);
+            }
+            const float4 gv = nee_at(ww, 11, i);
+            float4& r8 = rec_at(ww, vk, 8, i);
+            r8.x += gv.x;
+            r8.y += gv.y;
+            r8.z += gv.z;
+        }
         if (p.gradPos && __float_as_uint(d.w)) {
             const float4 bb = nee_at(ww, 4, i), ll = nee_at(ww, 5, i);
             const float bw[3] = {bb.x, bb.y, bb.z};
@@ -277,13 +356,12 @@ __global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(WarParams p, WavePara
             for (int v = 0; v < 3; v++) {
                 const uint32_t o = loc[v];
                 if (o + 3 > p.posDim) continue;
-                atomicAdd(gp + o, bw[v] * d.x);
-                atomicAdd(gp + o + 1, bw[v] * d.y);
-                atomicAdd(gp + o + 2, bw[v] * d.z);
+                atomicAdd(gp + o, bw[v] * dP.x);
+                atomicAdd(gp + o + 1, bw[v] * dP.y);
+                atomicAdd(gp + o + 2, bw[v] * dP.z);
             }
         }
         const float4 wt = nee_at(ww, 6, i);
-        const uint32_t vk = ww.nv[i] - 1;
         float4& e = rec_at(ww, vk, 4, i);
         e.x += wt.x;
         e.y += wt.y;
@@ -291,33 +369,44 @@ __global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(WarParams p, WavePara
     }
 }
 
-// Reverse sweep over each path's scatter records.
-template <bool HAS_T>
+// Reverse sweep over each path's records (war_sweep_vertex), then the
+// screen-sample reparameterisation (WAR).
+template <bool HAS_T, bool WAR>
 __global__ void __launch_bounds__(kShadeBlock) ww_sweep(DevScene s, WarParams p, WaveParams wp, WarWave ww) {
+    __shared__ uint2 stackMem[WAR ? kStackSize * kShadeBlock : 1];
+    uint2* stack = stackMem + threadIdx.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePixels; i += gridDim.x * blockDim.x) {
         const uint32_t pid = wp.waveFirstPixel + i;
         const float3 g = make_float3(p.dLdI[3 * size_t(pid)], p.dLdI[3 * size_t(pid) + 1], p.dLdI[3 * size_t(pid) + 2]);
         const uint32_t hash = war_hash(pid, p.matHash);
-        float3 A = f3(0.f);
-        for (int k = int(ww.nv[i]) - 1; k >= 0; k--) {
+        float3 A = f3(0.f), gV = f3(0.f);
+        const int nv = int(ww.nv[i]);
+        for (int k = nv - 1; k >= 0; k--) {
             const float4 r0 = rec_at(ww, k, 0, i), r1 = rec_at(ww, k, 1, i), r2 = rec_at(ww, k, 2, i);
-            const float4 r3 = rec_at(ww, k, 3, i), r4 = rec_at(ww, k, 4, i);
-            const uint32_t flags = __float_as_uint(r2.w);
-            const float3 thp = make_float3(r2.x, r2.y, r2.z);
-            if ((flags & 2u) && (A.x != 0.f || A.y != 0.f || A.z != 0.f)) {
-                const uint32_t matID = __float_as_uint(r1.w);
-                const MatParams mp = load_mat_params(s, matID);
-                ShadingData sd;
-                sd.frontFacing = (flags & 1u) != 0;
-                sd.materialID = matID;
-                const MaterialInstance<HAS_T> mi = material_instance<HAS_T>(s, sd, p.lambert != 0);
-                const DV3<11> J = eval_jacobian<11, HAS_T>(mi, mp, sd.frontFacing, make_float3(r0.x, r0.y, r0.z),
-                                                          make_float3(r1.x, r1.y, r1.z));
-                const float3 Gs = (A * thp) / r0.w;
-                add_material_grads<11>(p, hash, matID, J, Gs);
+            WarSweepVertex v;
+            v.wiL = xyz(r0);
+            v.pdf = r0.w;
+            v.wsL = xyz(r1);
+            v.matID = __float_as_uint(r1.w);
+            v.thp = xyz(r2);
+            v.flags = __float_as_uint(r2.w);
+            v.bw = xyz(rec_at(ww, k, 3, i));
+            v.e = xyz(rec_at(ww, k, 4, i));
+            if (WAR) {
+                const float4 r5 = rec_at(ww, k, 5, i), r6 = rec_at(ww, k, 6, i), r8 = rec_at(ww, k, 8, i), r9 = rec_at(ww, k, 9, i);
+                v.inDir = xyz(r5);
+                v.inst = __float_as_uint(r5.w);
+                v.outDir = xyz(r6);
+                v.prim = __float_as_uint(r6.w);
+                v.sg = as_u4(rec_at(ww, k, 7, i));
+                v.gV = xyz(r8);
+                v.b[0] = r8.w;
+                v.b[1] = r9.x;
+                v.b[2] = r9.y;
             }
-            A = A * make_float3(r3.x, r3.y, r3.z) + g * make_float3(r4.x, r4.y, r4.z);
+            war_sweep_vertex<HAS_T, WAR>(s, p, pid, hash, v, g, A, gV, stack, kShadeBlock);
         }
+        if (WAR && p.gradPos && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kShadeBlock);
     }
 }
 
@@ -346,7 +435,7 @@ __global__ void __launch_bounds__(kTraceBlock, FPT_TRACE_MIN_BLOCKS) ww_shadow(D
     trace_queue<true, MARK>(s, p, wp, w, stackMem + threadIdx.x);
 }
 
-template <bool HAS_T, bool BWD>
+template <bool HAS_T, bool BWD, bool WAR>
 cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adj, cudaStream_t st,
                               uint32_t& launches) {
     SoA w;
@@ -357,22 +446,24 @@ cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBu
     WarWave ww{};
     ww.capacity = b.capacity;
     ww.maxVertices = p.maxBounces + 2;
+    ww.recArrays = WAR ? kRecArraysWar : kRecArrays;
     if (BWD) {
         char* q = static_cast<char*>(adj);
         ww.nee = reinterpret_cast<float4*>(q);
-        q += size_t(kNeeArrays) * b.capacity * sizeof(float4);
+        q += size_t(WAR ? kNeeArraysWar : kNeeArrays) * b.capacity * sizeof(float4);
         ww.rec = reinterpret_cast<float4*>(q);
-        q += size_t(ww.maxVertices) * kRecArrays * b.capacity * sizeof(float4);
+        q += size_t(ww.maxVertices) * ww.recArrays * b.capacity * sizeof(float4);
         ww.nv = reinterpret_cast<uint32_t*>(q);
     }
     // Trace kernels read the ray counters through FrameParams.
     FrameParams fp{};
     fp.counters = p.counters;
-    static int gShade = 0, gTrace = 0, gSweep = 0;
+    static int gShade = 0, gTrace = 0, gSweep = 0, gNee = 0;
     if (!gShade) {
-        gShade = blocks_for(reinterpret_cast<const void*>(ww_shade<HAS_T, BWD>), kShadeBlock);
+        gShade = blocks_for(reinterpret_cast<const void*>(ww_shade<HAS_T, BWD, WAR>), kShadeBlock);
         gTrace = blocks_for(reinterpret_cast<const void*>(ww_extend), kTraceBlock);
-        gSweep = BWD ? blocks_for(reinterpret_cast<const void*>(ww_sweep<HAS_T>), kShadeBlock) : 1;
+        gSweep = BWD ? blocks_for(reinterpret_cast<const void*>(ww_sweep<HAS_T, WAR>), kShadeBlock) : 1;
+        gNee = BWD ? blocks_for(reinterpret_cast<const void*>(ww_nee_grad<WAR>), kShadeBlock) : 1;
     }
     const uint32_t pixels = p.width * p.height;
     const uint32_t maxIter = p.maxBounces + 2;
@@ -399,15 +490,17 @@ cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBu
             std::swap(qa, qb);
             wp.shadeQueue = qa;
             wp.extQueue = qb;
-            ww_shade<HAS_T, BWD><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w, ww);
+            ww_shade<HAS_T, BWD, WAR><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w, ww);
             ww_shadow<BWD><<<gTrace, kTraceBlock, 0, st>>>(s, fp, wp, w);
             launches += 4;
             if (BWD) {
-                ww_nee_grad<<<gShade, kShadeBlock, 0, st>>>(p, wp, w, ww);
+                ww_nee_grad<WAR><<<gNee, kShadeBlock, 0, st>>>(s, p, wp, w, ww);
                 launches++;
             }
         }
-        if (BWD) ww_sweep<HAS_T><<<std::min<int>(gSweep, int((wp.wavePixels + kShadeBlock - 1) / kShadeBlock)), kShadeBlock, 0, st>>>(s, p, wp, ww);
+        if (BWD)
+            ww_sweep<HAS_T, WAR><<<std::min<int>(gSweep, int((wp.wavePixels + kShadeBlock - 1) / kShadeBlock)), kShadeBlock, 0, st>>>(
+                s, p, wp, ww);
         else ww_resolve<<<(wp.wavePixels + 255) / 256, 256, 0, st>>>(p, wp, w);
         launches++;
         e = cudaGetLastError();
@@ -418,18 +511,23 @@ cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBu
 
 }  // namespace
 
-size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces) {
+size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces, bool war) {
     const size_t maxVertices = size_t(maxBounces) + 2;
-    return (size_t(kNeeArrays) + maxVertices * kRecArrays) * capacity * sizeof(float4) + size_t(capacity) * sizeof(uint32_t);
+    const size_t nee = war ? kNeeArraysWar : kNeeArrays, rec = war ? kRecArraysWar : kRecArrays;
+    return (nee + maxVertices * rec) * capacity * sizeof(float4) + size_t(capacity) * sizeof(uint32_t);
 }
 
 cudaError_t launch_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adjointScratch, bool backward,
                                  cudaStream_t st, uint32_t& launches) {
-    if (s.hasTransmission)
-        return backward ? run_war_wavefront<true, true>(s, p, b, adjointScratch, st, launches)
-                        : run_war_wavefront<true, false>(s, p, b, adjointScratch, st, launches);
-    return backward ? run_war_wavefront<false, true>(s, p, b, adjointScratch, st, launches)
-                    : run_war_wavefront<false, false>(s, p, b, adjointScratch, st, launches);
+    const bool war = backward && p.useWAR && p.gradPos;  // the warps only carry position derivatives
+    if (s.hasTransmission) {
+        if (!backward) return run_war_wavefront<true, false, false>(s, p, b, adjointScratch, st, launches);
+        return war ? run_war_wavefront<true, true, true>(s, p, b, adjointScratch, st, launches)
+                   : run_war_wavefront<true, true, false>(s, p, b, adjointScratch, st, launches);
+    }
+    if (!backward) return run_war_wavefront<false, false, false>(s, p, b, adjointScratch, st, launches);
+    return war ? run_war_wavefront<false, true, true>(s, p, b, adjointScratch, st, launches)
+               : run_war_wavefront<false, true, false>(s, p, b, adjointScratch, st, launches);
 }
 
 }  // namespace fpt

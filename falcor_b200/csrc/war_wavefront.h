@@ -20,11 +20,14 @@ struct WarParams {
     float* gradPos;              // [hash][posDim]
     uint32_t posDim, posHash;
     unsigned long long* counters;  // [0] paths, [1] rays
+    // Warped-area reparameterisation (adjoint with position gradients only).
+    uint32_t useWAR, auxCount;
+    float kappa, kappaScreen;    // 10^Log10vMFConcentration, 10^Log10vMFConcentrationScreen
 };
 
 // Bytes of adjoint scratch (pending NEE gradients + per-vertex records) for a
 // wave of `capacity` paths.
-size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces);
+size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces, bool war);
 // Primal (backward = false) or adjoint of one frame; `launches` counts kernels.
 cudaError_t launch_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adjointScratch, bool backward,
                                  cudaStream_t st, uint32_t& launches);

@@ -25,8 +25,11 @@
 //    direction and the area-to-solid-angle ratio x / detach(x)
 //    (PTUtils.slang:211-249);
 //  * warped-area reparameterisation leaves every value unchanged
-//    (WarpedAreaReparam.slang:226-263); its boundary gradients are not
-//    produced by this adjoint (useWAR is accepted and reported).
+//    (WarpedAreaReparam.slang:226-332) and only adds position derivatives;
+//    with useWAR and position gradients, the NEE warp's gradient is formed at
+//    the NEE sample and the scatter and screen warps' in the sweep
+//    (war_reparam.cuh).
+#include <cmath>
 #include <cstring>
 #include <string>
 
@@ -37,6 +40,7 @@
 #include "scene_device.h"
 #include "wardiff.h"
 #include "war_common.cuh"
+#include "war_reparam.cuh"
 
 namespace fpt {
 
@@ -46,15 +50,9 @@ namespace {
 
 constexpr int kWarBlock = 128;
 
-struct WarVertex {
-    float3 wiL, wsL, thp, bw, e;
-    float pdf;
-    uint32_t matID;
-    uint32_t flags;  // 1 front facing, 2 scattered with a valid evaluation
-};
-
-template <bool HAS_T, bool BWD>
+template <bool HAS_T, bool BWD, bool WAR>
 __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p) {
+    constexpr int NJ = WAR ? 17 : 14;
     __shared__ uint2 stackMem[kStackSize * kWarBlock];
     uint2* stack = stackMem + threadIdx.x;
     Counters cnt;
@@ -64,16 +62,8 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
         const uint32_t x = pid % p.width, y = pid / p.width;
         // tracePaths (WARDiffPathTracer.rt.slang:115-143).
         UniformSG sg;
-        sg.init(x, y, p.frameSeed / 2);
-        next2D(sg);
-        next2D(sg);
-        next2D(sg);
-        const float2 u = next2D(sg);
-        const float r = sqrtf(-2.f * logf(u.x));
-        const float ang = 6.28318530717958647692f * u.y;
-        float jx = (r * cosf(ang)) * 0.5f, jy = (r * sinf(ang)) * 0.5f;
-        if (p.useAntithetic && p.frameSeed % 2 == 0) { jx = -jx; jy = -jy; }
-        const float px = (float(x) + 0.5f) + jx, py = (float(y) + 0.5f) + jy;
+        const float2 pix = war_camera_sample(p, x, y, sg);
+        const float px = pix.x, py = pix.y;
         // computeCameraRayDirection (DiffSceneQuery.slang:314-323).
         const float qx = px / float(p.width), qy = py / float(p.height);
         const float ndcx = 2.f * qx + -1.f, ndcy = -2.f * qy + 1.f;
@@ -92,7 +82,7 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
             hash = war_hash(pid, p.matHash ? p.matHash : 1);
             hashPos = war_hash(pid, p.posHash ? p.posHash : 1);
         }
-        WarVertex rec[BWD ? kMaxWarVertices : 1];
+        WarSweepVertex rec[BWD ? kMaxWarVertices : 1];
         int nv = 0;
 
         cnt.v[0]++;
@@ -121,13 +111,22 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                     radiance += (thp * mi.emission) * misWeight;
                     if (BWD) e += mi.emission * misWeight;
                 }
-                WarVertex* vr = BWD ? &rec[nv] : nullptr;
+                WarSweepVertex* vr = BWD ? &rec[nv] : nullptr;
                 if (BWD) {
                     vr->thp = thp;
                     vr->wiL = vr->wsL = vr->bw = vr->e = f3(0.f);
                     vr->pdf = 1.f;
                     vr->flags = sd.frontFacing ? 1u : 0u;
                     vr->matID = sd.materialID;
+                    if (WAR) {
+                        vr->inDir = rayDir;
+                        vr->outDir = vr->gV = f3(0.f);
+                        vr->inst = is.inst;
+                        vr->prim = is.prim;
+                        vr->b[0] = is.b[0];
+                        vr->b[1] = is.b[1];
+                        vr->b[2] = is.b[2];
+                    }
                     nv++;
                 }
                 if (pathLen >= p.maxBounces + 1) {
@@ -170,10 +169,10 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                                     const float3 wiL = mi.toLocal(sd.V), woL = mi.toLocal(wo);
                                     if (mi.valid_hemisphere(sd, wiL, woL, wo)) {
                                         const MatParams mp = load_mat_params(s, sd.materialID);
-                                        const DV3<14> J = eval_jacobian<14, HAS_T>(mi, mp, sd.frontFacing, wiL, woL);
+                                        const DV3<NJ> J = eval_jacobian<NJ, HAS_T>(mi, mp, sd.frontFacing, wiL, woL);
                                         const float3 Gf = ((g * thp) * Li) * mis;
-                                        add_material_grads<14>(p, hash, sd.materialID, J, Gf);
-                                        if (p.gradPos && war_pos_target(p.meshID, is)) {
+                                        add_material_grads<NJ>(p, hash, sd.materialID, J, Gf);
+                                        if (p.gradPos) {
                                             // Through wo = (L - P) / |L - P| and the ratio a2s / detach(a2s).
                                             const float3 gL = make_float3(Gf.x * J.x.d[11] + Gf.y * J.y.d[11] + Gf.z * J.z.d[11],
                                                                           Gf.x * J.x.d[12] + Gf.y * J.y.d[12] + Gf.z * J.z.d[12],
@@ -183,14 +182,32 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                                             const float nlwo = dot(tls.normalW, wo);
                                             float3 dP = (gwo - wo * dot(wo, gwo)) * (-1.f / dist);
                                             dP += (wo * (-3.f / dist) + tls.normalW * (1.f / (dist * nlwo))) * gRatio;
-                                            float* gp = p.gradPos + size_t(hashPos) * p.posDim;
+                                            if (WAR) {
+                                                // computeNEE's reparameterizeRay, adjoint dLdI: the warped
+                                                // direction feeds evalAD and the area-to-solid-angle ratio.
+                                                constexpr int q0 = NJ - 3;
+                                                const float3 gI = make_float3(Gf.x * J.x.d[q0] + Gf.y * J.y.d[q0] + Gf.z * J.z.d[q0],
+                                                                              Gf.x * J.x.d[q0 + 1] + Gf.y * J.y.d[q0 + 1] + Gf.z * J.z.d[q0 + 1],
+                                                                              Gf.x * J.x.d[q0 + 2] + Gf.y * J.y.d[q0 + 2] + Gf.z * J.z.d[q0 + 2]);
+                                                vr->gV += mi.T * gI.x + mi.B * gI.y + mi.N * gI.z;
+                                                const float3 gdN = gRatio != 0.f ? gwo - tls.normalW * (gRatio / nlwo) : gwo;
+                                                if (gdN.x != 0.f || gdN.y != 0.f || gdN.z != 0.f || gRatio != 0.f) {
+                                                    const float3 no = compute_ray_origin(is.posW, sd.frontFacing ? sd.faceN : -sd.faceN);
+                                                    float3 gO = f3(0.f), gD = f3(0.f);
+                                                    war_ray_grad(s, p, pid, no, wo, true, sg, gdN, gRatio, stack, kWarBlock, gO, gD);
+                                                    dP += gO - (gD - wo * dot(wo, gD)) * (1.f / dist);
+                                                }
+                                            }
+                                            if (war_pos_target(p.meshID, is)) {
+                                                float* gp = p.gradPos + size_t(hashPos) * p.posDim;
 #pragma unroll
-                                            for (int i = 0; i < 3; i++) {
-                                                const uint32_t o = war_pos_index(p.meshID, is, i);
-                                                if (o + 3 > p.posDim) continue;
-                                                atomicAdd(gp + o, is.b[i] * dP.x);
-                                                atomicAdd(gp + o + 1, is.b[i] * dP.y);
-                                                atomicAdd(gp + o + 2, is.b[i] * dP.z);
+                                                for (int i = 0; i < 3; i++) {
+                                                    const uint32_t o = war_pos_index(p.meshID, is, i);
+                                                    if (o + 3 > p.posDim) continue;
+                                                    atomicAdd(gp + o, is.b[i] * dP.x);
+                                                    atomicAdd(gp + o + 1, is.b[i] * dP.y);
+                                                    atomicAdd(gp + o + 2, is.b[i] * dP.z);
+                                                }
                                             }
                                         }
                                     }
@@ -214,6 +231,10 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                     vr->pdf = pdf;
                     vr->bw = bsdfWeight;
                     if (mi.valid_hemisphere(sd, vr->wiL, vr->wsL, wo)) vr->flags |= 2u;
+                    if (WAR) {
+                        vr->outDir = wo;
+                        vr->sg = make_uint4(sg.s0, sg.s1, sg.s2, sg.s3);
+                    }
                 }
                 thp *= bsdfWeight;
                 pathPdf = pdf;
@@ -231,21 +252,9 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
             if (p.color) p.color[pid] = make_float4(radiance.x, radiance.y, radiance.z, 1.f);
         } else {
             // Reverse sweep over the scatter terms: A = adjoint of thp_{k+1}.
-            float3 A = f3(0.f);
-            for (int k = nv - 1; k >= 0; k--) {
-                const WarVertex& v = rec[k];
-                if ((v.flags & 2u) && (A.x != 0.f || A.y != 0.f || A.z != 0.f)) {
-                    const MatParams mp = load_mat_params(s, v.matID);
-                    ShadingData sd;
-                    sd.frontFacing = (v.flags & 1u) != 0;
-                    sd.materialID = v.matID;
-                    const MaterialInstance<HAS_T> mi = material_instance<HAS_T>(s, sd, p.lambert != 0);
-                    const DV3<11> J = eval_jacobian<11, HAS_T>(mi, mp, sd.frontFacing, v.wiL, v.wsL);
-                    const float3 Gs = (A * v.thp) / v.pdf;
-                    add_material_grads<11>(p, hash, v.matID, J, Gs);
-                }
-                A = A * v.bw + g * v.e;
-            }
+            float3 A = f3(0.f), gV = f3(0.f);
+            for (int k = nv - 1; k >= 0; k--) war_sweep_vertex<HAS_T, WAR>(s, p, pid, hash, rec[k], g, A, gV, stack, kWarBlock);
+            if (WAR && p.gradPos && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kWarBlock);
         }
     }
     flush_counters(p.counters, cnt);
@@ -267,13 +276,20 @@ int war_blocks(const void* k) {
     return std::max(1, perSM) * sms;
 }
 
-template <bool HAS_T, bool BWD>
+template <bool HAS_T, bool BWD, bool WAR>
 cudaError_t launch_war(const DevScene& s, const WarParams& p, cudaStream_t st) {
     static int blocks = 0;
-    if (!blocks) blocks = war_blocks(reinterpret_cast<const void*>(war_kernel<HAS_T, BWD>));
+    if (!blocks) blocks = war_blocks(reinterpret_cast<const void*>(war_kernel<HAS_T, BWD, WAR>));
     const int need = int((p.width * p.height + kWarBlock - 1) / kWarBlock);
-    war_kernel<HAS_T, BWD><<<std::min(blocks, std::max(need, 1)), kWarBlock, 0, st>>>(s, p);
+    war_kernel<HAS_T, BWD, WAR><<<std::min(blocks, std::max(need, 1)), kWarBlock, 0, st>>>(s, p);
     return cudaGetLastError();
+}
+
+template <bool BWD>
+cudaError_t launch_war_any(const DevScene& s, const WarParams& p, cudaStream_t st) {
+    const bool war = BWD && p.useWAR && p.gradPos;  // the warps only carry position derivatives
+    if (s.hasTransmission) return war ? launch_war<true, BWD, BWD>(s, p, st) : launch_war<true, BWD, false>(s, p, st);
+    return war ? launch_war<false, BWD, BWD>(s, p, st) : launch_war<false, BWD, false>(s, p, st);
 }
 
 }  // namespace
@@ -383,13 +399,17 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
     const double mesh = pass.num("meshToOptimize");
     p.meshID = mesh < 0 ? 0xffffffffu : uint32_t(mesh);  // -1: every mesh, scene-global vertex indices
     p.frameSeed = pass.useFixedSeed ? uint32_t(pass.num("fixedSeed")) : pass.frameCount;
+    p.useWAR = pass.num("useWAR") != 0;
+    p.auxCount = uint32_t(std::max(0.0, pass.num("auxSampleCount")));
+    // kappa = pow(10, Log10vMFConcentration) (WarpedAreaReparam.slang:241, 318).
+    p.kappa = std::pow(10.f, float(pass.num("Log10vMFConcentration")));
+    p.kappaScreen = std::pow(10.f, float(pass.num("Log10vMFConcentrationScreen")));
     p.counters = static_cast<unsigned long long*>(pass.scratch);
     if (p.width == 0 || p.height == 0) return set_error(FPT_ERR_INVALID_ARG, "WARDiffPathTracer: empty frame");
     if (p.width > 4096 || p.height > 4096)
         return set_error(FPT_ERR_INVALID_ARG, "WARDiffPathTracer: frame dimension exceeds kMaxFrameDimension (4096)");
     cudaError_t e = cudaMemsetAsync(pass.scratch, 0, kNumCounters * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, "WARDiffPathTracer: counter reset failed");
-    const bool hasT = scene->dev.hasTransmission != 0;
     const bool wavefront = pass.str("scheduler") != "Megakernel";
     if (backward || wavefront) {
         if (p.maxBounces + 2 > uint32_t(kMaxWarVertices))
@@ -406,7 +426,7 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
         e = pass.wavefront.ensure(cap);
         if (e != cudaSuccess) return set_error(FPT_ERR_OOM, std::string("WARDiffPathTracer: wavefront buffers: ") + cudaGetErrorString(e));
         if (backward) {
-            const size_t need = war_adjoint_bytes(pass.wavefront.capacity, p.maxBounces);
+            const size_t need = war_adjoint_bytes(pass.wavefront.capacity, p.maxBounces, p.useWAR != 0);
             if (pass.adjointScratchBytes < need) {
                 if (pass.adjointScratch) cudaFree(pass.adjointScratch);
                 pass.adjointScratch = nullptr;
@@ -419,7 +439,7 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
     }
     if (!backward) {
         if (wavefront) e = launch_war_wavefront(scene->dev, p, pass.wavefront, nullptr, false, st, pass.launches);
-        else e = hasT ? launch_war<true, false>(scene->dev, p, st) : launch_war<false, false>(scene->dev, p, st);
+        else e = launch_war_any<false>(scene->dev, p, st);
     } else {
         if (direct) {
             p.dLdI = dLdI;
@@ -441,8 +461,16 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
         }
         p.matHash = std::max(p.matHash, 1u);
         p.posHash = std::max(p.posHash, 1u);
+        if (p.useWAR && p.gradPos) {
+            if (p.auxCount == 0 || p.auxCount > uint32_t(kMaxAux))
+                return set_error(FPT_ERR_UNSUPPORTED, "WARDiffPathTracer: auxSampleCount must be in [1, 32]");
+            if (p.useAntithetic && (p.auxCount & 1u))
+                return set_error(FPT_ERR_UNSUPPORTED, "WARDiffPathTracer: antithetic sampling needs an even auxSampleCount");
+            if (!(p.kappa > 0.f) || !(p.kappaScreen > 0.f) || std::isinf(p.kappa) || std::isinf(p.kappaScreen))
+                return set_error(FPT_ERR_INVALID_ARG, "WARDiffPathTracer: vMF concentrations must be finite");
+        }
         if (wavefront) e = launch_war_wavefront(scene->dev, p, pass.wavefront, pass.adjointScratch, true, st, pass.launches);
-        else e = hasT ? launch_war<true, true>(scene->dev, p, st) : launch_war<false, true>(scene->dev, p, st);
+        else e = launch_war_any<true>(scene->dev, p, st);
     }
     if (!wavefront) pass.launches = 1;
     pass.frameCount++;

@@ -25,8 +25,8 @@ def war_params(w, h, seed=3, max_bounces=2, mesh=0, war=False, aux=16):
                          log10KappaScreen=5.0)
 
 
-def war_props(max_bounces=2, seed=3, mesh=0, mode="BackwardDiff", scheduler="Wavefront"):
-    return {"diffMode": mode, "maxBounces": max_bounces, "fixedSeed": seed, "useWAR": False, "meshToOptimize": mesh,
+def war_props(max_bounces=2, seed=3, mesh=0, mode="BackwardDiff", scheduler="Wavefront", war=False):
+    return {"diffMode": mode, "maxBounces": max_bounces, "fixedSeed": seed, "useWAR": war, "meshToOptimize": mesh,
             "scheduler": scheduler}
 
 
@@ -276,3 +276,165 @@ def test_adjoint_all_meshes_matches_oracle(fpt, oracle):
         assert abs(a - b) <= 2e-3 * max(1.0, abs(b)), ("material", k, a, b)
         a, b = float(P[k] @ gp), float(gp_ref[k])
         assert abs(a - b) <= 2e-3 * max(1.0, abs(b)), ("position", k, a, b)
+
+
+# ---------------------------------------------------------------------------
+# Warped-area reparameterisation: the CUDA reverse sweep against the oracle's
+# forward-mode derivatives of the same reparameterised program.
+# ---------------------------------------------------------------------------
+def _gpu_gradients(host, W, Hh, dLdI, nm_dim, nv_dim, props):
+    import torch
+    from falcor_b200.passes import WARDiffPathTracer
+    s = gpu_scene(host)
+    pt = WARDiffPathTracer(props)
+    pt.set_scene(s)
+    color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
+    gm = torch.zeros(nm_dim, dtype=torch.float32, device="cuda")
+    gp = torch.zeros(nv_dim, dtype=torch.float32, device="cuda")
+    pt.backward({"color": color}, torch.from_numpy(dLdI).cuda(), material_grad=gm, position_grad=gp)
+    torch.cuda.synchronize()
+    return gm.cpu().numpy().astype(np.float64), gp.cpu().numpy().astype(np.float64)
+
+
+# The warp gradients sum harmonic weights up to ~1e18 in FP32 (the oracle sums
+# them in FP64), so the position check allows 1e-2 relative.  The material
+# check allows the same: at these sizes and seeds a glossy path over materials
+# of roughness < 0.1 (GGX alpha^2 ~ 2e-5) carries the FP32 cancellation of
+# 1 + (alpha^2 - 1) cos^2 theta in the normal distribution (~0.6 % on one pixel's
+# derivatives; the FP32 primal agrees with the oracle's FP32 primal on every pixel).
+WAR_RTOL = 1e-2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scheduler", ["Wavefront", "Megakernel"])
+@pytest.mark.parametrize("scene", ["box", "heightfield"])
+def test_adjoint_war_matches_oracle(fpt, oracle, scene, scheduler):
+    host = H.box_icosphere(3) if scene == "box" else H.small_heightfield(materials=16, emitters=16)
+    W, Hh = 64, 48
+    osc = H.oracle_scene(host)
+    rng = np.random.default_rng(21)
+    dLdI = rng.standard_normal((Hh, W, 3)).astype(np.float32)
+    mesh = pick_mesh(osc, host, war_params(W, Hh), dLdI)
+    T, P = tangents(host, rng, mesh, k=2)
+    _, gm_ref, _, _, _ = osc.wardiff(war_params(W, Hh, mesh=mesh, war=True), mode=1, dLdI=dLdI, mat_tangents=T)
+    _, gp_ref, _, _, _ = osc.wardiff(war_params(W, Hh, mesh=mesh, war=True), mode=1, dLdI=dLdI, pos_tangents=P)
+    _, gp_int, _, _, _ = osc.wardiff(war_params(W, Hh, mesh=mesh, war=False), mode=1, dLdI=dLdI, pos_tangents=P)
+    gm, gp = _gpu_gradients(host, W, Hh, dLdI, T.shape[1], P.shape[1], war_props(mesh=mesh, scheduler=scheduler, war=True))
+    for k in range(2):
+        a, b = float(T[k] @ gm), float(gm_ref[k])
+        assert abs(a - b) <= WAR_RTOL * max(1.0, abs(b)), ("material", k, a, b)
+        a, b = float(P[k] @ gp), float(gp_ref[k])
+        assert abs(a - b) <= WAR_RTOL * max(1.0, abs(b)), ("position", k, a, b)
+    # The boundary terms are present: the interior-only derivative differs.
+    assert max(abs(float(gp_ref[k]) - float(gp_int[k])) for k in range(2)) > 1e-3 * max(1.0, abs(float(gp_ref[0])))
+
+
+@pytest.mark.gpu
+def test_adjoint_war_all_meshes_matches_oracle(fpt, oracle):
+    host = small_sphere()
+    W, Hh = 48, 48
+    osc = H.oracle_scene(host)
+    rng = np.random.default_rng(22)
+    dLdI = rng.standard_normal((Hh, W, 3)).astype(np.float32)
+    nm, nv = host.desc.material_count, host.desc.vertex_count
+    P = rng.standard_normal((2, nv * 3)) * 0.1
+    _, gp_ref, _, _, _ = osc.wardiff(war_params(W, Hh, max_bounces=3, mesh=0xFFFFFFFF, war=True), mode=1, dLdI=dLdI,
+                                     pos_tangents=P)
+    for scheduler in ("Wavefront", "Megakernel"):
+        _, gp = _gpu_gradients(host, W, Hh, dLdI, nm * 20, nv * 3,
+                               war_props(max_bounces=3, mesh=-1, scheduler=scheduler, war=True))
+        for k in range(2):
+            a, b = float(P[k] @ gp), float(gp_ref[k])
+            assert abs(a - b) <= WAR_RTOL * max(1.0, abs(b)), (scheduler, k, a, b)
+
+
+@pytest.mark.gpu
+def test_war_primal_unchanged_and_limits(fpt):
+    """useWAR changes no value of the primal; out-of-range auxiliary counts are refused."""
+    import torch
+    from falcor_b200 import _ffi
+    from falcor_b200.passes import WARDiffPathTracer
+    host = H.box_icosphere(3)
+    W, Hh = 32, 24
+    s = gpu_scene(host)
+    outs = []
+    for war in (False, True):
+        pt = WARDiffPathTracer(war_props(mode="Primal", war=war))
+        pt.set_scene(s)
+        c = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
+        pt.execute({"color": c})
+        outs.append(c.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+    dLdI = torch.ones((Hh, W, 3), dtype=torch.float32, device="cuda")
+    gp = torch.zeros(mesh_vertex_count(host, 0) * 3, dtype=torch.float32, device="cuda")
+    for aux in (0, 33, 15):  # 15: antithetic pairs need an even count
+        props = war_props(war=True)
+        props["auxSampleCount"] = aux
+        pt = WARDiffPathTracer(props)
+        pt.set_scene(s)
+        with pytest.raises(_ffi.FptError):
+            pt.backward({"color": torch.zeros((Hh, W, 4), device="cuda")}, dLdI, position_grad=gp)
+
+
+def _camera_dict(host):
+    c = host.desc.camera
+    return {n: (list(getattr(c, n)) if hasattr(getattr(c, n), "__len__") else getattr(c, n)) for n, _ in c._fields_}
+
+
+def _box_emissive_sphere(delta=(0.0, 0.0, 0.0)):
+    """The box scene with its sphere (mesh 13) made emissive and translated by delta."""
+    from falcor_b200.scene import HostScene
+    base = H.box_icosphere(3)
+    v, m = base.vertices.copy(), base.materials.copy()
+    vb, n = int(base.instances[13, 0]), mesh_vertex_count(base, 13)
+    v[vb:vb + n, 0:3] += np.asarray(delta, np.float32)
+    m[int(base.instances[13, 3]), 8:11] = 2.0
+    return HostScene.from_arrays(v, base.indices.copy(), base.instances.copy(), m, _camera_dict(base))
+
+
+@pytest.mark.gpu
+def test_war_matches_finite_differences_of_moved_geometry(fpt):
+    """The warped-area gradient estimates the derivative of the rendered image
+    itself, boundaries included: translating the emissive sphere of the closed
+    box, the mean WAR gradient over many frames agrees with central differences
+    of frames re-rendered (BVH rebuilt) with the sphere moved, while the
+    interior-only gradient (useWAR off) misses the silhouette term.  Seeds are
+    fixed, so the outcome is deterministic."""
+    import torch
+    from falcor_b200.passes import WARDiffPathTracer
+    W = Hh = 64
+    F = 4096
+    eps = 1e-2
+    host = _box_emissive_sphere()
+    nv = mesh_vertex_count(host, 13)
+    xs = (np.arange(W) + 0.5) / W
+    dLdI = torch.from_numpy(np.repeat(np.repeat(xs[None, :, None], Hh, 0), 3, 2).astype(np.float32)).cuda()
+    props = {"maxBounces": 0, "useNEE": False, "useMIS": False, "meshToOptimize": 13, "diffMode": "BackwardDiff"}
+
+    def gradients(war):
+        pt = WARDiffPathTracer(dict(props, useWAR=war))
+        pt.set_scene(gpu_scene(host))
+        color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
+        gp = torch.zeros((F, nv * 3), dtype=torch.float32, device="cuda")
+        for f in range(F):
+            pt.set_properties({"fixedSeed": f})
+            pt.backward({"color": color}, dLdI, position_grad=gp[f])
+        torch.cuda.synchronize()
+        return gp.view(F, nv, 3)[:, :, 0].sum(1).double().cpu().numpy()  # x translation
+
+    def frames(scene):
+        pt = WARDiffPathTracer(dict(props, diffMode="Primal"))
+        pt.set_scene(scene)
+        out = torch.zeros((F, Hh, W, 4), dtype=torch.float32, device="cuda")
+        for f in range(F):
+            pt.set_properties({"fixedSeed": f})
+            pt.execute({"color": out[f]})
+        torch.cuda.synchronize()
+        return (out[..., :3] * dLdI).double().sum((1, 2, 3)).cpu().numpy()
+
+    gw, gi = gradients(True), gradients(False)
+    fd = (frames(gpu_scene(_box_emissive_sphere((eps, 0, 0)))) - frames(gpu_scene(_box_emissive_sphere((-eps, 0, 0))))) / (2 * eps)
+    se = np.sqrt(gw.var() / F + fd.var() / F)
+    assert abs(fd.mean()) > 10 * fd.std() / np.sqrt(F), (fd.mean(), fd.std())
+    assert abs(gw.mean() - fd.mean()) <= 4 * se, (gw.mean(), fd.mean(), se)
+    assert abs(gi.mean() - fd.mean()) > 4 * np.sqrt(gi.var() / F + fd.var() / F), (gi.mean(), fd.mean())
