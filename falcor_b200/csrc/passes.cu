@@ -419,6 +419,22 @@ FPT_API fpt_status fpt_pass_set_scene_gradients(fpt_pass* pass, fpt_scene_gradie
     return FPT_OK;
 }
 
+FPT_API fpt_status fpt_pass_set_diff_debug_params(fpt_pass* pass, uint32_t var_type, uint32_t id_x, uint32_t id_y,
+                                                  uint32_t offset, const float grad[4]) {
+    if (!pass || !grad) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_diff_debug_params: null argument");
+    if (var_type > FPT_DIFF_VAR_GEOMETRY_TRANSLATION)
+        return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_diff_debug_params: invalid variable type");
+    if (var_type == FPT_DIFF_VAR_MATERIAL && offset >= 20)
+        return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_diff_debug_params: material offset must be < 20");
+    pass->diffDebugExplicit = true;
+    pass->diffDebugType = var_type;
+    pass->diffDebugId[0] = id_x;
+    pass->diffDebugId[1] = id_y;
+    pass->diffDebugOffset = offset;
+    for (int i = 0; i < 4; i++) pass->diffDebugGrad[i] = grad[i];
+    return FPT_OK;
+}
+
 FPT_API fpt_status fpt_pass_set_dLdI(fpt_pass* pass, const float* dLdI) {
     if (!pass) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_dLdI: null pass");
     if (pass->type != "WARDiffPathTracer") return set_error(FPT_ERR_UNSUPPORTED, "dL_dI: only WARDiffPathTracer takes dL_dI");

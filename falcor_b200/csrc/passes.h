@@ -36,6 +36,10 @@ struct fpt_pass {
     fpt::KernelTimer timer;           // per-category kernel timing ("profileKernels")
     fpt_scene_gradients* sceneGradients = nullptr;  // WARDiffPathTracer::scene_gradients (not owned)
     const float* dLdI = nullptr;                    // WARDiffPathTracer::dL_dI (device, float3 per pixel)
+    // WARDiffPathTracer::setDiffDebugParams (explicit) or the diffVarName presets.
+    bool diffDebugExplicit = false;
+    uint32_t diffDebugType = 0, diffDebugId[2] = {0, 0}, diffDebugOffset = 0;
+    float diffDebugGrad[4] = {0.f, 0.f, 0.f, 0.f};
 
     double num(const std::string& k) const;
     std::string str(const std::string& k) const;

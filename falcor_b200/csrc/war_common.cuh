@@ -175,18 +175,82 @@ FPT_D DV3<N> eval_jacobian(const MaterialInstance<HAS_T>& mi, const MatParams& m
 
 FPT_D uint32_t war_hash(uint32_t pixelID, uint32_t hashSize) { return jenkins_hash(pixelID) % hashSize; }
 
-// Adds sum_c G_c * J_c[i] for the 11 material parameters.
-template <int N>
-FPT_D void add_material_grads(const WarParams& p, uint32_t hash, uint32_t matID, const DV3<N>& J, float3 G) {
+// Debug gradient image (ForwardDiffDebug / BackwardDiffDebug): one scene
+// variable -- the floats one material read returns (GradientIOWrapper.slang:87-94)
+// or the translation of one mesh (DiffSceneIO.slang:85-93, 122-131) -- whose
+// derivative d(color.r)/d(variable) goes to dbgColor[pixel].x.  DiffVariableType
+// values (DiffRendering/SharedTypes.slang:90-96).
+constexpr uint32_t kDbgNone = 0, kDbgMaterial = 1, kDbgTranslation = 2;
+
+// The adjoint of a pixel's radiance: dLdI, or (1, 0, 0) for the debug image.
+FPT_D float3 war_dLdI(const WarParams& p, uint32_t pid) {
+    if (!p.dLdI) return make_float3(1.f, 0.f, 0.f);
+    return make_float3(p.dLdI[3 * size_t(pid)], p.dLdI[3 * size_t(pid) + 1], p.dLdI[3 * size_t(pid) + 2]);
+}
+// Whether vertex-position derivatives are wanted (gradients or the translation image).
+FPT_D bool war_wants_pos(const WarParams& p) { return p.gradPos != nullptr || (p.dbgColor && p.dbgType == kDbgTranslation); }
+
+// Tangent of material parameter `slot` under the debug variable: the floats of
+// the getFloat read at dbgOffset (3 for the colours at 0, 6 and 11, else 1).
+FPT_D float war_dbg_tangent(const WarParams& p, uint32_t slot) {
+    const uint32_t o = p.dbgOffset;
+    const uint32_t width = (o == 0 || o == 6 || o == 11) ? 3u : 1u;
+    if (slot < o || slot - o >= width) return 0.f;
+    const uint32_t i = slot - o;
+    return i == 0 ? p.dbgGrad.x : (i == 1 ? p.dbgGrad.y : p.dbgGrad.z);
+}
+
+// Material-parameter gradients G[0..10] of material matID from pixel pid.
+FPT_D void add_material_grad_values(const WarParams& p, uint32_t pid, uint32_t hash, uint32_t matID, const float (&G)[11]) {
+    if (p.dbgColor && p.dbgType == kDbgMaterial) {
+        if (matID != p.dbgId) return;
+        float acc = 0.f;
+#pragma unroll
+        for (int i = 0; i < 11; i++) acc += G[i] * war_dbg_tangent(p, uint32_t(i));
+        if (acc != 0.f) atomicAdd(&p.dbgColor[pid].x, acc);
+        return;
+    }
     if (!p.gradMat) return;
     const uint32_t base = matID * kMatParams;
     if (base + 11 > p.matDim) return;
     float* g = p.gradMat + size_t(hash) * p.matDim + base;
 #pragma unroll
-    for (int i = 0; i < 11; i++) {
-        const float v = G.x * J.x.d[i] + G.y * J.y.d[i] + G.z * J.z.d[i];
-        if (v != 0.f) atomicAdd(g + i, v);
+    for (int i = 0; i < 11; i++)
+        if (G[i] != 0.f) atomicAdd(g + i, G[i]);
+}
+
+// Adds sum_c G_c * J_c[i] for the 11 material parameters.
+template <int N>
+FPT_D void add_material_grads(const WarParams& p, uint32_t pid, uint32_t hash, uint32_t matID, const DV3<N>& J, float3 G) {
+    float v[11];
+#pragma unroll
+    for (int i = 0; i < 11; i++) v[i] = G.x * J.x.d[i] + G.y * J.y.d[i] + G.z * J.z.d[i];
+    add_material_grad_values(p, pid, hash, matID, v);
+}
+
+// Position gradient g of a point sum_v b_v x_v of a target mesh's triangle whose
+// vertices sit at gradient offsets off[v] (the caller checks the target mesh).
+FPT_D void add_position_grad(const WarParams& p, uint32_t pid, const uint32_t (&off)[3], const float (&b)[3], float3 g) {
+    if (p.dbgColor && p.dbgType == kDbgTranslation) {
+        // sum_v dot(velocity, dPos_v) (DiffSceneIO.slang:127-129).
+        const float v = dot(make_float3(p.dbgGrad.x, p.dbgGrad.y, p.dbgGrad.z), g) * (b[0] + b[1] + b[2]);
+        if (v != 0.f) atomicAdd(&p.dbgColor[pid].x, v);
+        return;
     }
+    if (!p.gradPos) return;
+    float* gp = p.gradPos + size_t(war_hash(pid, p.posHash)) * p.posDim;
+#pragma unroll
+    for (int v = 0; v < 3; v++) {
+        const uint32_t o = off[v];
+        if (o + 3 > p.posDim) continue;
+        atomicAdd(gp + o, b[v] * g.x);
+        atomicAdd(gp + o + 1, b[v] * g.y);
+        atomicAdd(gp + o + 2, b[v] * g.z);
+    }
+}
+FPT_D void add_position_grad(const WarParams& p, uint32_t pid, const WarIsect& is, float3 g) {
+    const uint32_t off[3] = {war_pos_index(p.meshID, is, 0), war_pos_index(p.meshID, is, 1), war_pos_index(p.meshID, is, 2)};
+    add_position_grad(p, pid, off, is.b, g);
 }
 
 }  // namespace

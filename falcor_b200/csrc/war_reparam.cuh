@@ -181,7 +181,6 @@ FPT_D void war_aux_backprop(const DevScene& s, const WarParams& p, uint32_t pixe
     const float inv = 1.f / m.Wc;
     const float inv2 = inv * inv;
     const float3 Mp = m.pass ? m.M : f3(0.f);
-    float* gp = p.gradPos ? p.gradPos + size_t(war_hash(pixelID, p.posHash)) * p.posDim : nullptr;
     for (uint32_t i = 0; i < n; i++) {
         const WarAux& a = aux[i];
         float3 gu = gM * (a.w * inv);
@@ -191,19 +190,17 @@ FPT_D void war_aux_backprop(const DevScene& s, const WarParams& p, uint32_t pixe
             // u = normalizeSafe(P - O).
             const float3 g = (gu - a.u * dot(a.u, gu)) / a.len;
             gO -= g;
-            if (gp && (p.meshID == kAllMeshes || a.inst == p.meshID)) {
+            if (p.meshID == kAllMeshes || a.inst == p.meshID) {
                 const DevInstance inst = s.instances[a.inst];
                 const uint32_t* ip = s.indices + inst.ibOffset + a.prim * 3;
                 const float bw[3] = {1.f - a.bx - a.by, a.bx, a.by};
+                uint32_t off[3];
 #pragma unroll
                 for (int v = 0; v < 3; v++) {
                     const uint32_t local = __ldg(ip + v);
-                    const uint32_t o = (p.meshID == kAllMeshes ? inst.vbOffset + local : local) * 3u;
-                    if (o + 3 > p.posDim) continue;
-                    atomicAdd(gp + o, bw[v] * g.x);
-                    atomicAdd(gp + o + 1, bw[v] * g.y);
-                    atomicAdd(gp + o + 2, bw[v] * g.z);
+                    off[v] = (p.meshID == kAllMeshes ? inst.vbOffset + local : local) * 3u;
                 }
+                add_position_grad(p, pixelID, off, bw, g);
             }
         }
         if (needD) {
@@ -378,16 +375,7 @@ struct WarSweepVertex {
 // Adds g * b_v to the position gradients of the vertices of a path vertex's
 // hit triangle (posW = sum v_i b_i).
 FPT_D void add_vertex_position_grad(const WarParams& p, uint32_t pid, const WarIsect& is, float3 g) {
-    if (!p.gradPos || !war_pos_target(p.meshID, is)) return;
-    float* gp = p.gradPos + size_t(war_hash(pid, p.posHash)) * p.posDim;
-#pragma unroll
-    for (int v = 0; v < 3; v++) {
-        const uint32_t o = war_pos_index(p.meshID, is, v);
-        if (o + 3 > p.posDim) continue;
-        atomicAdd(gp + o, is.b[v] * g.x);
-        atomicAdd(gp + o + 1, is.b[v] * g.y);
-        atomicAdd(gp + o + 2, is.b[v] * g.z);
-    }
+    if (war_wants_pos(p) && war_pos_target(p.meshID, is)) add_position_grad(p, pid, is, g);
 }
 
 // One step of the reverse sweep over a path's vertices, last to first:
@@ -402,7 +390,7 @@ FPT_D void war_sweep_vertex(const DevScene& s, const WarParams& p, uint32_t pid,
     constexpr int NJ = WAR ? 17 : 11;
     const bool scattered = (v.flags & 2u) != 0;
     const bool evalGrad = scattered && (A.x != 0.f || A.y != 0.f || A.z != 0.f);
-    const bool needWar = WAR && p.gradPos && scattered;
+    const bool needWar = WAR && war_wants_pos(p) && scattered;
     float3 gV = WAR ? v.gV : f3(0.f), gdS = f3(0.f);
     WarIsect is;
     ShadingData sd;
@@ -419,7 +407,7 @@ FPT_D void war_sweep_vertex(const DevScene& s, const WarParams& p, uint32_t pid,
         const MaterialInstance<HAS_T> mi = material_instance<HAS_T>(s, sd, p.lambert != 0);
         const DV3<NJ> J = eval_jacobian<NJ, HAS_T>(mi, mp, (v.flags & 1u) != 0, v.wiL, v.wsL);
         const float3 Gs = (A * v.thp) / v.pdf;
-        add_material_grads<NJ>(p, hash, v.matID, J, Gs);
+        add_material_grads<NJ>(p, pid, hash, v.matID, J, Gs);
         if (needWar) {
             const float3 gO = make_float3(Gs.x * J.x.d[11] + Gs.y * J.y.d[11] + Gs.z * J.z.d[11],
                                           Gs.x * J.x.d[12] + Gs.y * J.y.d[12] + Gs.z * J.z.d[12],

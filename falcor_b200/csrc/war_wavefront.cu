@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
         float3 g = f3(0.f), e = f3(0.f);
         uint32_t vk = 0;
         if (BWD) {
-            g = make_float3(p.dLdI[3 * size_t(pid)], p.dLdI[3 * size_t(pid) + 1], p.dLdI[3 * size_t(pid) + 2]);
+            g = war_dLdI(p, pid);
             vk = ww.nv[i];
             ww.nv[i] = vk + 1;
             rec_at(ww, vk, 0, i) = make_float4(0.f, 0.f, 0.f, 1.f);  // wiL, pdf
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
                                 const float3 Gf = ((g * thp) * Li) * mis;
 #pragma unroll
                                 for (int q = 0; q < 11; q++) G[q] = Gf.x * J.x.d[q] + Gf.y * J.y.d[q] + Gf.z * J.z.d[q];
-                                if (p.gradPos) {
+                                if (war_wants_pos(p)) {
                                     const float3 gL = make_float3(Gf.x * J.x.d[11] + Gf.y * J.y.d[11] + Gf.z * J.z.d[11],
                                                                   Gf.x * J.x.d[12] + Gf.y * J.y.d[12] + Gf.z * J.z.d[12],
                                                                   Gf.x * J.x.d[13] + Gf.y * J.y.d[13] + Gf.z * J.z.d[13]);
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
                                     }
                                 }
                             }
-                            const bool posGrad = p.gradPos && war_pos_target(p.meshID, is);
+                            const bool posGrad = war_wants_pos(p) && war_pos_target(p.meshID, is);
                             nee_at(ww, 0, i) = make_float4(G[0], G[1], G[2], G[3]);
                             nee_at(ww, 1, i) = make_float4(G[4], G[5], G[6], G[7]);
                             nee_at(ww, 2, i) = make_float4(G[8], G[9], G[10], __uint_as_float(sd.materialID));
@@ -318,12 +318,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(DevScene s, WarParams
         const float4 a = nee_at(ww, 0, i), b = nee_at(ww, 1, i), c = nee_at(ww, 2, i);
         const float G[11] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z};
         const uint32_t matID = __float_as_uint(c.w);
-        if (p.gradMat && matID * kMatParams + 11 <= p.matDim) {
-            float* gm = p.gradMat + size_t(war_hash(pid, p.matHash)) * p.matDim + matID * kMatParams;
-#pragma unroll
-            for (int q = 0; q < 11; q++)
-                if (G[q] != 0.f) atomicAdd(gm + q, G[q]);
-        }
+        add_material_grad_values(p, pid, war_hash(pid, p.matHash), matID, G);
         const float4 d = nee_at(ww, 3, i);
         float3 dP = xyz(d);
         const uint32_t vk = ww.nv[i] - 1;
@@ -347,19 +342,11 @@ __global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(DevScene s, WarParams
             r8.y += gv.y;
             r8.z += gv.z;
         }
-        if (p.gradPos && __float_as_uint(d.w)) {
+        if (__float_as_uint(d.w)) {
             const float4 bb = nee_at(ww, 4, i), ll = nee_at(ww, 5, i);
             const float bw[3] = {bb.x, bb.y, bb.z};
             const uint32_t loc[3] = {__float_as_uint(bb.w), __float_as_uint(ll.x), __float_as_uint(ll.y)};  // gradient offsets
-            float* gp = p.gradPos + size_t(war_hash(pid, p.posHash)) * p.posDim;
-#pragma unroll
-            for (int v = 0; v < 3; v++) {
-                const uint32_t o = loc[v];
-                if (o + 3 > p.posDim) continue;
-                atomicAdd(gp + o, bw[v] * dP.x);
-                atomicAdd(gp + o + 1, bw[v] * dP.y);
-                atomicAdd(gp + o + 2, bw[v] * dP.z);
-            }
+            add_position_grad(p, pid, loc, bw, dP);
         }
         const float4 wt = nee_at(ww, 6, i);
         float4& e = rec_at(ww, vk, 4, i);
@@ -377,7 +364,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_sweep(DevScene s, WarParams p,
     uint2* stack = stackMem + threadIdx.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePixels; i += gridDim.x * blockDim.x) {
         const uint32_t pid = wp.waveFirstPixel + i;
-        const float3 g = make_float3(p.dLdI[3 * size_t(pid)], p.dLdI[3 * size_t(pid) + 1], p.dLdI[3 * size_t(pid) + 2]);
+        const float3 g = war_dLdI(p, pid);
         const uint32_t hash = war_hash(pid, p.matHash);
         float3 A = f3(0.f), gV = f3(0.f);
         const int nv = int(ww.nv[i]);
@@ -406,7 +393,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_sweep(DevScene s, WarParams p,
             }
             war_sweep_vertex<HAS_T, WAR>(s, p, pid, hash, v, g, A, gV, stack, kShadeBlock);
         }
-        if (WAR && p.gradPos && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kShadeBlock);
+        if (WAR && war_wants_pos(p) && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kShadeBlock);
     }
 }
 
@@ -519,7 +506,7 @@ size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces, bool war) {
 
 cudaError_t launch_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adjointScratch, bool backward,
                                  cudaStream_t st, uint32_t& launches) {
-    const bool war = backward && p.useWAR && p.gradPos;  // the warps only carry position derivatives
+    const bool war = backward && p.useWAR && (p.gradPos || (p.dbgColor && p.dbgType == kDbgTranslation));  // position derivatives only
     if (s.hasTransmission) {
         if (!backward) return run_war_wavefront<true, false, false>(s, p, b, adjointScratch, st, launches);
         return war ? run_war_wavefront<true, true, true>(s, p, b, adjointScratch, st, launches)

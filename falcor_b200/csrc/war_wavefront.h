@@ -23,6 +23,11 @@ struct WarParams {
     // Warped-area reparameterisation (adjoint with position gradients only).
     uint32_t useWAR, auxCount;
     float kappa, kappaScreen;    // 10^Log10vMFConcentration, 10^Log10vMFConcentrationScreen
+    // Debug gradient image (ForwardDiffDebug / BackwardDiffDebug): d(color.r)/d(variable)
+    // accumulated into dbgColor[pixel].x; dLdI is then null (adjoint (1, 0, 0) per pixel).
+    float4* dbgColor;
+    uint32_t dbgType, dbgId, dbgOffset;  // kDbg*, material or mesh, material read offset
+    float4 dbgGrad;                      // tangent of the read floats / translation velocity
 };
 
 // Bytes of adjoint scratch (pending NEE gradients + per-vertex records) for a

@@ -76,11 +76,10 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
         float pathPdf = 0.f;
         uint32_t pathLen = 0;
         float3 g = f3(0.f);
-        uint32_t hash = 0, hashPos = 0;
+        uint32_t hash = 0;
         if (BWD) {
-            g = make_float3(p.dLdI[3 * size_t(pid)], p.dLdI[3 * size_t(pid) + 1], p.dLdI[3 * size_t(pid) + 2]);
+            g = war_dLdI(p, pid);
             hash = war_hash(pid, p.matHash ? p.matHash : 1);
-            hashPos = war_hash(pid, p.posHash ? p.posHash : 1);
         }
         WarSweepVertex rec[BWD ? kMaxWarVertices : 1];
         int nv = 0;
@@ -171,8 +170,8 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                                         const MatParams mp = load_mat_params(s, sd.materialID);
                                         const DV3<NJ> J = eval_jacobian<NJ, HAS_T>(mi, mp, sd.frontFacing, wiL, woL);
                                         const float3 Gf = ((g * thp) * Li) * mis;
-                                        add_material_grads<NJ>(p, hash, sd.materialID, J, Gf);
-                                        if (p.gradPos) {
+                                        add_material_grads<NJ>(p, pid, hash, sd.materialID, J, Gf);
+                                        if (war_wants_pos(p)) {
                                             // Through wo = (L - P) / |L - P| and the ratio a2s / detach(a2s).
                                             const float3 gL = make_float3(Gf.x * J.x.d[11] + Gf.y * J.y.d[11] + Gf.z * J.z.d[11],
                                                                           Gf.x * J.x.d[12] + Gf.y * J.y.d[12] + Gf.z * J.z.d[12],
@@ -198,17 +197,7 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                                                     dP += gO - (gD - wo * dot(wo, gD)) * (1.f / dist);
                                                 }
                                             }
-                                            if (war_pos_target(p.meshID, is)) {
-                                                float* gp = p.gradPos + size_t(hashPos) * p.posDim;
-#pragma unroll
-                                                for (int i = 0; i < 3; i++) {
-                                                    const uint32_t o = war_pos_index(p.meshID, is, i);
-                                                    if (o + 3 > p.posDim) continue;
-                                                    atomicAdd(gp + o, is.b[i] * dP.x);
-                                                    atomicAdd(gp + o + 1, is.b[i] * dP.y);
-                                                    atomicAdd(gp + o + 2, is.b[i] * dP.z);
-                                                }
-                                            }
+                                            if (war_pos_target(p.meshID, is)) add_position_grad(p, pid, is, dP);
                                         }
                                     }
                                 }
@@ -254,10 +243,17 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
             // Reverse sweep over the scatter terms: A = adjoint of thp_{k+1}.
             float3 A = f3(0.f), gV = f3(0.f);
             for (int k = nv - 1; k >= 0; k--) war_sweep_vertex<HAS_T, WAR>(s, p, pid, hash, rec[k], g, A, gV, stack, kWarBlock);
-            if (WAR && p.gradPos && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kWarBlock);
+            if (WAR && war_wants_pos(p) && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kWarBlock);
         }
     }
     flush_counters(p.counters, cnt);
+}
+
+__global__ void war_debug_finalize(float4* dColor, uint32_t n, float maxValue) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float d = dColor[i].x;
+        dColor[i] = (d >= -maxValue && d <= maxValue) ? make_float4(d, 0.f, 0.f, 1.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
 }
 
 __global__ void war_aggregate(const float* tmp, float* out, uint32_t dim, uint32_t hash) {
@@ -287,7 +283,7 @@ cudaError_t launch_war(const DevScene& s, const WarParams& p, cudaStream_t st) {
 
 template <bool BWD>
 cudaError_t launch_war_any(const DevScene& s, const WarParams& p, cudaStream_t st) {
-    const bool war = BWD && p.useWAR && p.gradPos;  // the warps only carry position derivatives
+    const bool war = BWD && p.useWAR && (p.gradPos || (p.dbgColor && p.dbgType == kDbgTranslation));  // position derivatives only
     if (s.hasTransmission) return war ? launch_war<true, BWD, BWD>(s, p, st) : launch_war<true, BWD, false>(s, p, st);
     return war ? launch_war<false, BWD, BWD>(s, p, st) : launch_war<false, BWD, false>(s, p, st);
 }
@@ -415,31 +411,99 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
         if (p.maxBounces + 2 > uint32_t(kMaxWarVertices))
             return set_error(FPT_ERR_UNSUPPORTED, "WARDiffPathTracer: the adjoint supports maxBounces <= 14");
     }
+    const bool debug = !backward && (mode == 2 || mode == 3) && io->d_color != nullptr;
     if (!backward) {
         if (!io->color) return set_error(FPT_ERR_INVALID_ARG, "WARDiffPathTracer: 'color' is required");
         p.color = reinterpret_cast<float4*>(io->color);
+        // Outputs are cleared every frame except in BackwardDiff with runBackward
+        // (WARDiffPathTracer.cpp:518-529).
         if (io->d_color) cudaMemsetAsync(io->d_color, 0, size_t(p.width) * p.height * 16, st);
+        if (mode == 3) cudaMemsetAsync(io->color, 0, size_t(p.width) * p.height * 16, st);
     }
+    auto adjointScratch = [&](bool war) -> fpt_status {
+        const size_t need = war_adjoint_bytes(pass.wavefront.capacity, p.maxBounces, war);
+        if (pass.adjointScratchBytes < need) {
+            if (pass.adjointScratch) cudaFree(pass.adjointScratch);
+            pass.adjointScratch = nullptr;
+            pass.adjointScratchBytes = 0;
+            if (cudaMalloc(&pass.adjointScratch, need) != cudaSuccess)
+                return set_error(FPT_ERR_OOM, "WARDiffPathTracer: adjoint scratch allocation failed");
+            pass.adjointScratchBytes = need;
+        }
+        return FPT_OK;
+    };
+    auto checkWar = [&](const WarParams& q) -> fpt_status {
+        const bool pos = q.gradPos || (q.dbgColor && q.dbgType == kDbgTranslation);
+        if (!q.useWAR || !pos) return FPT_OK;
+        if (q.auxCount == 0 || q.auxCount > uint32_t(kMaxAux))
+            return set_error(FPT_ERR_UNSUPPORTED, "WARDiffPathTracer: auxSampleCount must be in [1, 32]");
+        if (q.useAntithetic && (q.auxCount & 1u))
+            return set_error(FPT_ERR_UNSUPPORTED, "WARDiffPathTracer: antithetic sampling needs an even auxSampleCount");
+        if (!(q.kappa > 0.f) || !(q.kappaScreen > 0.f) || std::isinf(q.kappa) || std::isinf(q.kappaScreen))
+            return set_error(FPT_ERR_INVALID_ARG, "WARDiffPathTracer: vMF concentrations must be finite");
+        return FPT_OK;
+    };
     if (wavefront) {
         const uint32_t pixels = p.width * p.height;
         const uint32_t cap = std::min<uint32_t>(pixels, uint32_t(std::max(1.0, pass.num("wavefrontCapacity"))));
         e = pass.wavefront.ensure(cap);
         if (e != cudaSuccess) return set_error(FPT_ERR_OOM, std::string("WARDiffPathTracer: wavefront buffers: ") + cudaGetErrorString(e));
-        if (backward) {
-            const size_t need = war_adjoint_bytes(pass.wavefront.capacity, p.maxBounces, p.useWAR != 0);
-            if (pass.adjointScratchBytes < need) {
-                if (pass.adjointScratch) cudaFree(pass.adjointScratch);
-                pass.adjointScratch = nullptr;
-                pass.adjointScratchBytes = 0;
-                if (cudaMalloc(&pass.adjointScratch, need) != cudaSuccess)
-                    return set_error(FPT_ERR_OOM, "WARDiffPathTracer: adjoint scratch allocation failed");
-                pass.adjointScratchBytes = need;
-            }
+        if (backward || debug) {
+            const fpt_status s = adjointScratch(p.useWAR != 0);
+            if (s != FPT_OK) return s;
         }
     }
     if (!backward) {
-        if (wavefront) e = launch_war_wavefront(scene->dev, p, pass.wavefront, nullptr, false, st, pass.launches);
-        else e = launch_war_any<false>(scene->dev, p, st);
+        if (mode != 3) {
+            if (wavefront) e = launch_war_wavefront(scene->dev, p, pass.wavefront, nullptr, false, st, pass.launches);
+            else e = launch_war_any<false>(scene->dev, p, st);
+        }
+        if (debug && e == cudaSuccess) {
+            // ForwardDiffDebug / BackwardDiffDebug (WARDiffPathTracer.rt.slang:182-210): the
+            // reverse sweep with adjoint (1, 0, 0) per pixel gives d(color.r)/d(variable)
+            // pixel by pixel, each path belonging to one pixel.
+            WarParams q = p;
+            q.color = nullptr;
+            q.dLdI = nullptr;
+            q.dbgColor = reinterpret_cast<float4*>(io->d_color);
+            uint32_t type = pass.diffDebugType, id = pass.diffDebugId[0], offset = pass.diffDebugOffset;
+            float4 grad = make_float4(pass.diffDebugGrad[0], pass.diffDebugGrad[1], pass.diffDebugGrad[2], pass.diffDebugGrad[3]);
+            if (!pass.diffDebugExplicit) {
+                // The diffVarName presets of the WARDiffPathTracer constructor (WARDiffPathTracer.cpp:83-93).
+                const std::string var = pass.str("diffVarName");
+                type = kDbgNone;
+                if (var == "CBOX_BUNNY_MATERIAL") { type = kDbgMaterial; id = 0; offset = 0; grad = make_float4(1.f, 1.f, 1.f, 0.f); }
+                else if (var == "CBOX_BUNNY_TRANSLATION") { type = kDbgTranslation; id = 0; offset = 0; grad = make_float4(0.f, 1.f, 0.f, 0.f); }
+            }
+            // Reverse mode routes material derivatives to the scene gradients, not to
+            // the image (GradientIOWrapper.slang:97-104 has no debug branch).
+            if (mode == 3 && type == kDbgMaterial) type = kDbgNone;
+            q.dbgType = type;
+            q.dbgId = id;
+            q.dbgOffset = offset;
+            q.dbgGrad = grad;
+            if (type == kDbgTranslation) q.meshID = id;
+            if (mode == 3 && pass.sceneGradients && pass.sceneGradients->e[FPT_GRAD_MATERIAL].active) {
+                const auto& gm = pass.sceneGradients->e[FPT_GRAD_MATERIAL];
+                q.gradMat = gm.tmp;
+                q.matDim = gm.dim;
+                q.matHash = gm.hash;
+            }
+            q.matHash = std::max(q.matHash, 1u);
+            q.posHash = std::max(q.posHash, 1u);
+            const fpt_status cs = checkWar(q);
+            if (cs != FPT_OK) return cs;
+            uint32_t launches = 0;
+            if (wavefront) e = launch_war_wavefront(scene->dev, q, pass.wavefront, pass.adjointScratch, true, st, launches);
+            else e = launch_war_any<true>(scene->dev, q, st);
+            pass.launches += launches;
+            if (e == cudaSuccess && mode == 2) {
+                // gOutputDColor = (d.r, 0, 0, 1) when |d| <= assertThreshold (Params.slang:61), else cleared.
+                const uint32_t n = p.width * p.height;
+                war_debug_finalize<<<(n + 255) / 256, 256, 0, st>>>(q.dbgColor, n, 1e9f);
+                e = cudaGetLastError();
+            }
+        }
     } else {
         if (direct) {
             p.dLdI = dLdI;
@@ -461,14 +525,8 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
         }
         p.matHash = std::max(p.matHash, 1u);
         p.posHash = std::max(p.posHash, 1u);
-        if (p.useWAR && p.gradPos) {
-            if (p.auxCount == 0 || p.auxCount > uint32_t(kMaxAux))
-                return set_error(FPT_ERR_UNSUPPORTED, "WARDiffPathTracer: auxSampleCount must be in [1, 32]");
-            if (p.useAntithetic && (p.auxCount & 1u))
-                return set_error(FPT_ERR_UNSUPPORTED, "WARDiffPathTracer: antithetic sampling needs an even auxSampleCount");
-            if (!(p.kappa > 0.f) || !(p.kappaScreen > 0.f) || std::isinf(p.kappa) || std::isinf(p.kappaScreen))
-                return set_error(FPT_ERR_INVALID_ARG, "WARDiffPathTracer: vMF concentrations must be finite");
-        }
+        const fpt_status cs = checkWar(p);
+        if (cs != FPT_OK) return cs;
         if (wavefront) e = launch_war_wavefront(scene->dev, p, pass.wavefront, pass.adjointScratch, true, st, pass.launches);
         else e = launch_war_any<true>(scene->dev, p, st);
     }

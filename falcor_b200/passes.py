@@ -222,6 +222,15 @@ class WARDiffPathTracer(RenderPass):
     def set_mesh_to_optimize(self, mesh_id: int) -> None:
         self.set_properties({"meshToOptimize": int(mesh_id)})
 
+    def set_diff_debug_params(self, var_type, id=(0, 0), offset: int = 0, grad=(0.0, 0.0, 0.0, 0.0)) -> None:
+        """setDiffDebugParams (WARDiffPathTracer.cpp:689-695): the variable of the
+        ForwardDiffDebug / BackwardDiffDebug gradient image.  var_type: "None",
+        "Material" or "GeometryTranslation" (or 0, 1, 2); id: (material or mesh, unused)."""
+        types = {"None": 0, "Material": 1, "GeometryTranslation": 2}
+        t = types[var_type] if isinstance(var_type, str) else int(getattr(var_type, "value", var_type))
+        g = (C.c_float * 4)(*[float(x) for x in grad])
+        check(lib().fpt_pass_set_diff_debug_params(self._h, t, int(id[0]), int(id[1]), int(offset), g))
+
     def backward(self, render_data: Mapping[str, Any], dLdI, material_grad=None, position_grad=None, frame: int = 0) -> None:
         """Adjoint of one frame into flat gradient tensors (fpt_pass_backward)."""
         some = next((t for t in render_data.values() if t is not None), dLdI)

@@ -369,6 +369,22 @@ FPT_API fpt_status fpt_scene_gradients_get(const fpt_scene_gradients* grads, uin
 FPT_API fpt_status fpt_pass_set_scene_gradients(fpt_pass* pass, fpt_scene_gradients* grads);
 FPT_API fpt_status fpt_pass_set_dLdI(fpt_pass* pass, const float* dLdI);
 
+/* DiffVariableType (DiffRendering/SharedTypes.slang:86-96). */
+typedef enum fpt_diff_variable_type {
+    FPT_DIFF_VAR_NONE = 0,
+    FPT_DIFF_VAR_MATERIAL = 1,              /* the floats of material id_x read at offset */
+    FPT_DIFF_VAR_GEOMETRY_TRANSLATION = 2   /* translation of mesh id_x by grad.xyz       */
+} fpt_diff_variable_type;
+/* WARDiffPathTracer::setDiffDebugParams (WARDiffPathTracer.cpp:689-695): the
+ * variable of the debug gradient image.  With diffMode "ForwardDiffDebug" the
+ * 'dColor' output holds (d color.r / d variable, 0, 0, 1) per pixel; with
+ * "BackwardDiffDebug" a translation variable's derivative is accumulated into
+ * dColor.r and material derivatives go to the scene gradients.  Overrides the
+ * presets of the diffVarName property ("CBOX_BUNNY_MATERIAL": material 0
+ * baseColor, grad (1, 1, 1); "CBOX_BUNNY_TRANSLATION": mesh 0, (0, 1, 0)). */
+FPT_API fpt_status fpt_pass_set_diff_debug_params(fpt_pass* pass, uint32_t var_type, uint32_t id_x, uint32_t id_y,
+                                                  uint32_t offset, const float grad[4]);
+
 /* Device counters of the last execute (rays traced, paths, error word). */
 typedef struct fpt_pass_stats {
     uint64_t paths;

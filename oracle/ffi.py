@@ -159,7 +159,8 @@ class OracleScene:
         """WARDiffPathTracer restatement.  mode 0: FP32 primal; 1: forward-mode
         derivatives along the rows of mat_tangents / pos_tangents (K <= 4) ->
         sum over pixels of dLdI . dL/dv_k; 2: radiance with the parameters offset
-        by eps * (row 0) (FP64), for finite differences.
+        by eps * (row 0) (FP64), for finite differences; 3: per-pixel derivative
+        dL/dv_0 (FP64) in place of the perturbed radiance.
         Returns (color RGBA32F, grads[K] or None, perturbed radiance or None, rays, seconds)."""
         w, h = params.width, params.height
         color = np.zeros((h, w, 4), dtype=np.float32)
@@ -172,7 +173,7 @@ class OracleScene:
             pt = np.ascontiguousarray(np.atleast_2d(pos_tangents), dtype=np.float64)
             K = max(K, pt.shape[0])
         grads = np.zeros(4, dtype=np.float64)
-        pert = np.zeros((h, w, 3), dtype=np.float64) if mode == 2 else None
+        pert = np.zeros((h, w, 3), dtype=np.float64) if mode in (2, 3) else None
         g = np.ascontiguousarray(dLdI, dtype=np.float32) if dLdI is not None else None
         x0, y0, x1, y1 = rect if rect else (0, 0, w, h)
         rays = C.c_uint64()

@@ -67,7 +67,8 @@ struct WarCounters { uint64_t rays = 0, hits = 0; };
 
 // mode 0: FP32 primal into colorOut (RGBA); 1: forward-mode derivatives along
 // the K <= 4 seeded directions, gradAcc[k] += dLdI . dL/dv_k; 2: the path with
-// the seeded parameters offset by eps * v_0, perturbed radiance into pertOut (FP64).
+// the seeded parameters offset by eps * v_0, perturbed radiance into pertOut (FP64);
+// 3: the per-pixel derivative dL/dv_0 into pertOut (FP64).
 void wardiff_pixel(const Scene& s, const WarDiffParams& p, const WarSeeds& seeds, int mode, uint32_t x, uint32_t y,
                    const float* dLdI, float* colorOut, double* gradAcc, double* pertOut, WarCounters* wc);
 

@@ -570,6 +570,11 @@ void wardiff_pixel(const Scene& s, const WarDiffParams& p, const WarSeeds& seeds
         if (gradAcc && dLdI)
             for (int k = 0; k < 4 && k < seeds.K; k++)
                 gradAcc[k] += double(dLdI[0]) * L.x.d[k] + double(dLdI[1]) * L.y.d[k] + double(dLdI[2]) * L.z.d[k];
+    } else if (mode == 3) {
+        // Per-pixel forward-mode derivative along tangent 0 (the ForwardDiffDebug image).
+        V3<Dual<4>> L = war_trace_path<Dual<4>>(s, p, seeds, x, y, wc);
+        if (colorOut) { colorOut[0] = float(L.x.v); colorOut[1] = float(L.y.v); colorOut[2] = float(L.z.v); colorOut[3] = 1.f; }
+        if (pertOut) { pertOut[0] = L.x.d[0]; pertOut[1] = L.y.d[0]; pertOut[2] = L.z.d[0]; }
     } else {
         V3<Shadow> L = war_trace_path<Shadow>(s, p, seeds, x, y, wc);
         if (pertOut) { pertOut[0] = L.x.p; pertOut[1] = L.y.p; pertOut[2] = L.z.p; }
