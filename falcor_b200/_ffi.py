@@ -80,7 +80,8 @@ class fpt_frame_io(C.Structure):
 
 
 class fpt_grad_buffers(C.Structure):
-    _fields_ = [("material", C.c_void_p), ("mesh_position", C.c_void_p), ("material_dim", u32), ("position_dim", u32)]
+    _fields_ = [("material", C.c_void_p), ("mesh_position", C.c_void_p), ("material_dim", u32), ("position_dim", u32),
+                ("mesh_normal", C.c_void_p), ("mesh_tangent", C.c_void_p), ("normal_dim", u32), ("tangent_dim", u32)]
 
 
 class fpt_grad_config(C.Structure):

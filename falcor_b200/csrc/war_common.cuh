@@ -253,5 +253,67 @@ FPT_D void add_position_grad(const WarParams& p, uint32_t pid, const WarIsect& i
     add_position_grad(p, pid, off, is.b, g);
 }
 
+// Whether vertex normal / tangent gradients are wanted.
+FPT_D bool war_wants_frame(const WarParams& p) { return p.gradNrm != nullptr || p.gradTan != nullptr; }
+
+// Adjoint of the interpolated (unnormalised) vertex normal and tangent of a
+// path vertex from the adjoints gwiL, gwoL of one evalAD's local directions
+// wiL = frame(V), woL = frame(wo).  The frame is loadShadingData's
+// ShadingFrame::createSafe(normalW, float4(tangentW, w)) (ShadingFrame.slang:76-153)
+// with flipShadingNormal (ShadingUtils.slang:111-117); perp_stark is no_diff.
+FPT_D void war_frame_adjoint(const WarIsect& is, bool flip, float3 V, float3 wo, float3 gwiL, float3 gwoL, float3& gn, float3& gt) {
+    const float ln = length(is.normalW);
+    const float3 N0 = is.normalW / ln;
+    const float3 t = is.tangentW;
+    const float tn = dot(t, N0);
+    const bool valid = fabsf(is.tw) == 1.f && dot(t, t) > 0.f && fabsf(tn) < 0.9999f;
+    float3 u = f3(0.f), T;
+    float lu = 1.f, sw = 1.f;
+    if (valid) {
+        u = t - N0 * tn;
+        lu = length(u);
+        T = u / lu;
+        sw = is.tw;
+    } else {
+        T = perp_stark(N0);
+    }
+    float3 gT = V * gwiL.x + wo * gwoL.x;
+    const float3 gB = V * gwiL.y + wo * gwoL.y;
+    float3 gN0 = (V * gwiL.z + wo * gwoL.z) * (flip ? -1.f : 1.f);
+    // B = cross(N0, T) * w.
+    gN0 += cross(T, gB) * sw;
+    gT += cross(gB, N0) * sw;
+    gt = f3(0.f);
+    if (valid) {
+        // T = normalize(t - N0 (t . N0)).
+        const float3 gu = (gT - T * dot(T, gT)) / lu;
+        gt = gu - N0 * dot(N0, gu);
+        gN0 -= gu * tn + t * dot(N0, gu);
+    }
+    // N0 = normalize(normalW).
+    gn = (gN0 - N0 * dot(N0, gN0)) / ln;
+}
+
+// Normal / tangent gradients gn, gt of the interpolation sum_v b_v n_v of a
+// target mesh's triangle (vertex gradient offsets off[v]).
+FPT_D void add_frame_grad(const WarParams& p, uint32_t pid, const uint32_t (&off)[3], const float (&b)[3], float3 gn, float3 gt) {
+    float* an = p.gradNrm ? p.gradNrm + size_t(war_hash(pid, p.nrmHash)) * p.nrmDim : nullptr;
+    float* at = p.gradTan ? p.gradTan + size_t(war_hash(pid, p.tanHash)) * p.tanDim : nullptr;
+#pragma unroll
+    for (int v = 0; v < 3; v++) {
+        const uint32_t o = off[v];
+        if (an && o + 3 <= p.nrmDim) {
+            atomicAdd(an + o, b[v] * gn.x);
+            atomicAdd(an + o + 1, b[v] * gn.y);
+            atomicAdd(an + o + 2, b[v] * gn.z);
+        }
+        if (at && o + 3 <= p.tanDim && (gt.x != 0.f || gt.y != 0.f || gt.z != 0.f)) {
+            atomicAdd(at + o, b[v] * gt.x);
+            atomicAdd(at + o + 1, b[v] * gt.y);
+            atomicAdd(at + o + 2, b[v] * gt.z);
+        }
+    }
+}
+
 }  // namespace
 }  // namespace fpt

@@ -390,11 +390,12 @@ FPT_D void war_sweep_vertex(const DevScene& s, const WarParams& p, uint32_t pid,
     constexpr int NJ = WAR ? 17 : 11;
     const bool scattered = (v.flags & 2u) != 0;
     const bool evalGrad = scattered && (A.x != 0.f || A.y != 0.f || A.z != 0.f);
-    const bool needWar = WAR && war_wants_pos(p) && scattered;
+    const bool needWar = WAR && p.useWAR && war_wants_pos(p) && scattered;
+    const bool needFrame = WAR && war_wants_frame(p) && evalGrad;
     float3 gV = WAR ? v.gV : f3(0.f), gdS = f3(0.f);
     WarIsect is;
     ShadingData sd;
-    if (needWar) {
+    if (needWar || needFrame) {
         // Re-derive the vertex (hit, shading frame) from the record.
         is = war_isect_bary(s, v.inst, v.prim, v.b[0], v.b[1], v.b[2]);
         sd = war_shading_data(s, is, v.inDir);
@@ -408,7 +409,7 @@ FPT_D void war_sweep_vertex(const DevScene& s, const WarParams& p, uint32_t pid,
         const DV3<NJ> J = eval_jacobian<NJ, HAS_T>(mi, mp, (v.flags & 1u) != 0, v.wiL, v.wsL);
         const float3 Gs = (A * v.thp) / v.pdf;
         add_material_grads<NJ>(p, pid, hash, v.matID, J, Gs);
-        if (needWar) {
+        if (needWar || needFrame) {
             const float3 gO = make_float3(Gs.x * J.x.d[11] + Gs.y * J.y.d[11] + Gs.z * J.z.d[11],
                                           Gs.x * J.x.d[12] + Gs.y * J.y.d[12] + Gs.z * J.z.d[12],
                                           Gs.x * J.x.d[13] + Gs.y * J.y.d[13] + Gs.z * J.z.d[13]);
@@ -418,6 +419,13 @@ FPT_D void war_sweep_vertex(const DevScene& s, const WarParams& p, uint32_t pid,
                                           Gs.x * J.x.d[q0 + 2] + Gs.y * J.y.d[q0 + 2] + Gs.z * J.z.d[q0 + 2]);
             gdS = mi.T * gO.x + mi.B * gO.y + mi.N * gO.z;
             gV += mi.T * gI.x + mi.B * gI.y + mi.N * gI.z;
+            if (needFrame && war_pos_target(p.meshID, is)) {
+                // generateScatterRay's evalAD through the shading frame.
+                float3 gn, gt;
+                war_frame_adjoint(is, dot(mi.N, sd.N) < 0.f, sd.V, v.outDir, gI, gO, gn, gt);
+                const uint32_t off[3] = {war_pos_index(p.meshID, is, 0), war_pos_index(p.meshID, is, 1), war_pos_index(p.meshID, is, 2)};
+                add_frame_grad(p, pid, off, is.b, gn, gt);
+            }
         }
     }
     if (needWar) {

@@ -55,8 +55,10 @@ namespace {
 //        9   adjoint of the warped direction      6 scatter direction, primitive
 //        10  sample generator                     7 sample generator after the BSDF sample
 //        11  adjoint of V (incident direction)    8 NEE adjoint of V, b0
-//                                                 9 b1, b2
-constexpr int kNeeArrays = 7, kNeeArraysWar = 12;
+//        12  normal adjoint, flag                 9 b1, b2
+//        13  tangent adjoint
+// ("WAR" = the extended layout, used for the warps and for normal / tangent gradients.)
+constexpr int kNeeArrays = 7, kNeeArraysWar = 14;
 constexpr int kRecArrays = 5, kRecArraysWar = 10;
 
 struct WarWave {
@@ -205,8 +207,9 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
                             float G[11];
 #pragma unroll
                             for (int q = 0; q < 11; q++) G[q] = 0.f;
-                            float3 dP = f3(0.f), gwo = f3(0.f), gwi = f3(0.f);
+                            float3 dP = f3(0.f), gwo = f3(0.f), gwi = f3(0.f), gn = f3(0.f), gt = f3(0.f);
                             float gRatio = 0.f;
+                            bool frameGrad = false;
                             const float3 wiL = mi.toLocal(sd.V), woL = mi.toLocal(wo);
                             if (mi.valid_hemisphere(sd, wiL, woL, wo)) {
                                 const MatParams mp = load_mat_params(s, sd.materialID);
@@ -214,7 +217,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
                                 const float3 Gf = ((g * thp) * Li) * mis;
 #pragma unroll
                                 for (int q = 0; q < 11; q++) G[q] = Gf.x * J.x.d[q] + Gf.y * J.y.d[q] + Gf.z * J.z.d[q];
-                                if (war_wants_pos(p)) {
+                                if (war_wants_pos(p) || (WAR && war_wants_frame(p))) {
                                     const float3 gL = make_float3(Gf.x * J.x.d[11] + Gf.y * J.y.d[11] + Gf.z * J.z.d[11],
                                                                   Gf.x * J.x.d[12] + Gf.y * J.y.d[12] + Gf.z * J.z.d[12],
                                                                   Gf.x * J.x.d[13] + Gf.y * J.y.d[13] + Gf.z * J.z.d[13]);
@@ -226,8 +229,12 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
                                                                       Gf.x * J.x.d[q0 + 1] + Gf.y * J.y.d[q0 + 1] + Gf.z * J.z.d[q0 + 1],
                                                                       Gf.x * J.x.d[q0 + 2] + Gf.y * J.y.d[q0 + 2] + Gf.z * J.z.d[q0 + 2]);
                                         gwi = mi.T * gI.x + mi.B * gI.y + mi.N * gI.z;
+                                        if (war_wants_frame(p) && war_pos_target(p.meshID, is)) {
+                                            frameGrad = true;
+                                            war_frame_adjoint(is, dot(mi.N, sd.N) < 0.f, sd.V, wo, gI, gL, gn, gt);
+                                        }
                                     }
-                                    if (war_pos_target(p.meshID, is)) {
+                                    if (war_wants_pos(p) && war_pos_target(p.meshID, is)) {
                                         const float nlwo = dot(tls.normalW, wo);
                                         dP = (gwo - wo * dot(wo, gwo)) * (-1.f / dist);
                                         dP += (wo * (-3.f / dist) + tls.normalW * (1.f / (dist * nlwo))) * gRatio;
@@ -255,6 +262,8 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
                                 nee_at(ww, 9, i) = make_float4(gdN.x, gdN.y, gdN.z, 0.f);
                                 store_sg(as_u4(nee_at(ww, 10, i)), sg);
                                 nee_at(ww, 11, i) = make_float4(gwi.x, gwi.y, gwi.z, 0.f);
+                                nee_at(ww, 12, i) = make_float4(gn.x, gn.y, gn.z, __uint_as_float(frameGrad ? 1u : 0u));
+                                nee_at(ww, 13, i) = make_float4(gt.x, gt.y, gt.z, 0.f);
                             }
                         }
                     }
@@ -322,11 +331,16 @@ __global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(DevScene s, WarParams
         const float4 d = nee_at(ww, 3, i);
         float3 dP = xyz(d);
         const uint32_t vk = ww.nv[i] - 1;
+        const float4 bb = nee_at(ww, 4, i), ll = nee_at(ww, 5, i);
+        const float bw[3] = {bb.x, bb.y, bb.z};
+        const uint32_t loc[3] = {__float_as_uint(bb.w), __float_as_uint(ll.x), __float_as_uint(ll.y)};  // gradient offsets
         if (WAR) {
             const float4 o7 = nee_at(ww, 7, i), o8 = nee_at(ww, 8, i), o9 = nee_at(ww, 9, i);
             const float3 gdN = xyz(o9);
             const float gRatio = o8.w;  // also the adjoint of the reparameterisation weight
-            if (nonzero(gdN) || gRatio != 0.f) {
+            const float4 fn = nee_at(ww, 12, i);
+            if (__float_as_uint(fn.w)) add_frame_grad(p, pid, loc, bw, xyz(fn), xyz(nee_at(ww, 13, i)));
+            if (p.useWAR && war_wants_pos(p) && (nonzero(gdN) || gRatio != 0.f)) {
                 UniformSG sg;
                 load_sg(as_u4(nee_at(ww, 10, i)), sg);
                 const float3 wo = xyz(o8);
@@ -342,12 +356,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(DevScene s, WarParams
             r8.y += gv.y;
             r8.z += gv.z;
         }
-        if (__float_as_uint(d.w)) {
-            const float4 bb = nee_at(ww, 4, i), ll = nee_at(ww, 5, i);
-            const float bw[3] = {bb.x, bb.y, bb.z};
-            const uint32_t loc[3] = {__float_as_uint(bb.w), __float_as_uint(ll.x), __float_as_uint(ll.y)};  // gradient offsets
-            add_position_grad(p, pid, loc, bw, dP);
-        }
+        if (__float_as_uint(d.w)) add_position_grad(p, pid, loc, bw, dP);
         const float4 wt = nee_at(ww, 6, i);
         float4& e = rec_at(ww, vk, 4, i);
         e.x += wt.x;
@@ -393,7 +402,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_sweep(DevScene s, WarParams p,
             }
             war_sweep_vertex<HAS_T, WAR>(s, p, pid, hash, v, g, A, gV, stack, kShadeBlock);
         }
-        if (WAR && war_wants_pos(p) && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kShadeBlock);
+        if (WAR && p.useWAR && war_wants_pos(p) && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kShadeBlock);
     }
 }
 
@@ -506,7 +515,9 @@ size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces, bool war) {
 
 cudaError_t launch_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adjointScratch, bool backward,
                                  cudaStream_t st, uint32_t& launches) {
-    const bool war = backward && p.useWAR && (p.gradPos || (p.dbgColor && p.dbgType == kDbgTranslation));  // position derivatives only
+    // Extended records: the warps (position derivatives only) and normal / tangent gradients.
+    const bool war = backward && ((p.useWAR && (p.gradPos || (p.dbgColor && p.dbgType == kDbgTranslation))) ||
+                                  p.gradNrm || p.gradTan);
     if (s.hasTransmission) {
         if (!backward) return run_war_wavefront<true, false, false>(s, p, b, adjointScratch, st, launches);
         return war ? run_war_wavefront<true, true, true>(s, p, b, adjointScratch, st, launches)

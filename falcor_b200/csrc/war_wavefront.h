@@ -19,6 +19,10 @@ struct WarParams {
     uint32_t matDim, matHash;
     float* gradPos;              // [hash][posDim]
     uint32_t posDim, posHash;
+    float* gradNrm;              // [hash][nrmDim] vertex normals of the mesh (MeshNormal)
+    uint32_t nrmDim, nrmHash;
+    float* gradTan;              // [hash][tanDim] vertex tangents of the mesh (MeshTangent)
+    uint32_t tanDim, tanHash;
     unsigned long long* counters;  // [0] paths, [1] rays
     // Warped-area reparameterisation (adjoint with position gradients only).
     uint32_t useWAR, auxCount;

@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                                         const DV3<NJ> J = eval_jacobian<NJ, HAS_T>(mi, mp, sd.frontFacing, wiL, woL);
                                         const float3 Gf = ((g * thp) * Li) * mis;
                                         add_material_grads<NJ>(p, pid, hash, sd.materialID, J, Gf);
-                                        if (war_wants_pos(p)) {
+                                        if (war_wants_pos(p) || (WAR && war_wants_frame(p))) {
                                             // Through wo = (L - P) / |L - P| and the ratio a2s / detach(a2s).
                                             const float3 gL = make_float3(Gf.x * J.x.d[11] + Gf.y * J.y.d[11] + Gf.z * J.z.d[11],
                                                                           Gf.x * J.x.d[12] + Gf.y * J.y.d[12] + Gf.z * J.z.d[12],
@@ -189,15 +189,22 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                                                                               Gf.x * J.x.d[q0 + 1] + Gf.y * J.y.d[q0 + 1] + Gf.z * J.z.d[q0 + 1],
                                                                               Gf.x * J.x.d[q0 + 2] + Gf.y * J.y.d[q0 + 2] + Gf.z * J.z.d[q0 + 2]);
                                                 vr->gV += mi.T * gI.x + mi.B * gI.y + mi.N * gI.z;
+                                                if (war_wants_frame(p) && war_pos_target(p.meshID, is)) {
+                                                    float3 gn, gt;
+                                                    war_frame_adjoint(is, dot(mi.N, sd.N) < 0.f, sd.V, wo, gI, gL, gn, gt);
+                                                    const uint32_t off[3] = {war_pos_index(p.meshID, is, 0), war_pos_index(p.meshID, is, 1),
+                                                                             war_pos_index(p.meshID, is, 2)};
+                                                    add_frame_grad(p, pid, off, is.b, gn, gt);
+                                                }
                                                 const float3 gdN = gRatio != 0.f ? gwo - tls.normalW * (gRatio / nlwo) : gwo;
-                                                if (gdN.x != 0.f || gdN.y != 0.f || gdN.z != 0.f || gRatio != 0.f) {
+                                                if (p.useWAR && war_wants_pos(p) && (gdN.x != 0.f || gdN.y != 0.f || gdN.z != 0.f || gRatio != 0.f)) {
                                                     const float3 no = compute_ray_origin(is.posW, sd.frontFacing ? sd.faceN : -sd.faceN);
                                                     float3 gO = f3(0.f), gD = f3(0.f);
                                                     war_ray_grad(s, p, pid, no, wo, true, sg, gdN, gRatio, stack, kWarBlock, gO, gD);
                                                     dP += gO - (gD - wo * dot(wo, gD)) * (1.f / dist);
                                                 }
                                             }
-                                            if (war_pos_target(p.meshID, is)) add_position_grad(p, pid, is, dP);
+                                            if (war_wants_pos(p) && war_pos_target(p.meshID, is)) add_position_grad(p, pid, is, dP);
                                         }
                                     }
                                 }
@@ -243,7 +250,7 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
             // Reverse sweep over the scatter terms: A = adjoint of thp_{k+1}.
             float3 A = f3(0.f), gV = f3(0.f);
             for (int k = nv - 1; k >= 0; k--) war_sweep_vertex<HAS_T, WAR>(s, p, pid, hash, rec[k], g, A, gV, stack, kWarBlock);
-            if (WAR && war_wants_pos(p) && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kWarBlock);
+            if (WAR && p.useWAR && war_wants_pos(p) && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kWarBlock);
         }
     }
     flush_counters(p.counters, cnt);
@@ -283,7 +290,8 @@ cudaError_t launch_war(const DevScene& s, const WarParams& p, cudaStream_t st) {
 
 template <bool BWD>
 cudaError_t launch_war_any(const DevScene& s, const WarParams& p, cudaStream_t st) {
-    const bool war = BWD && p.useWAR && (p.gradPos || (p.dbgColor && p.dbgType == kDbgTranslation));  // position derivatives only
+    // Extended records: the warps (position derivatives only) and normal / tangent gradients.
+    const bool war = BWD && ((p.useWAR && (p.gradPos || (p.dbgColor && p.dbgType == kDbgTranslation))) || p.gradNrm || p.gradTan);
     if (s.hasTransmission) return war ? launch_war<true, BWD, BWD>(s, p, st) : launch_war<true, BWD, false>(s, p, st);
     return war ? launch_war<false, BWD, BWD>(s, p, st) : launch_war<false, BWD, false>(s, p, st);
 }
@@ -449,7 +457,8 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
         e = pass.wavefront.ensure(cap);
         if (e != cudaSuccess) return set_error(FPT_ERR_OOM, std::string("WARDiffPathTracer: wavefront buffers: ") + cudaGetErrorString(e));
         if (backward || debug) {
-            const fpt_status s = adjointScratch(p.useWAR != 0);
+            // The extended record layout (warps, normal / tangent gradients) covers every adjoint.
+            const fpt_status s = adjointScratch(true);
             if (s != FPT_OK) return s;
         }
     }
@@ -513,6 +522,10 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
             p.gradPos = grads->mesh_position;
             p.posDim = grads->mesh_position ? grads->position_dim : 0;
             p.posHash = 1;
+            p.gradNrm = grads->mesh_normal;
+            p.nrmDim = grads->mesh_normal ? grads->normal_dim : 0;
+            p.gradTan = grads->mesh_tangent;
+            p.tanDim = grads->mesh_tangent ? grads->tangent_dim : 0;
         } else {
             if (!pass.dLdI) return set_error(FPT_ERR_INVALID_ARG, "WARDiffPathTracer: dL_dI is not set (fpt_pass_set_dLdI)");
             if (!pass.sceneGradients)
@@ -522,9 +535,15 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
             const auto& gp = pass.sceneGradients->e[FPT_GRAD_MESH_POSITION];
             if (gm.active) { p.gradMat = gm.tmp; p.matDim = gm.dim; p.matHash = gm.hash; }
             if (gp.active) { p.gradPos = gp.tmp; p.posDim = gp.dim; p.posHash = gp.hash; }
+            const auto& gn = pass.sceneGradients->e[FPT_GRAD_MESH_NORMAL];
+            const auto& gt = pass.sceneGradients->e[FPT_GRAD_MESH_TANGENT];
+            if (gn.active) { p.gradNrm = gn.tmp; p.nrmDim = gn.dim; p.nrmHash = gn.hash; }
+            if (gt.active) { p.gradTan = gt.tmp; p.tanDim = gt.dim; p.tanHash = gt.hash; }
         }
         p.matHash = std::max(p.matHash, 1u);
         p.posHash = std::max(p.posHash, 1u);
+        p.nrmHash = std::max(p.nrmHash, 1u);
+        p.tanHash = std::max(p.tanHash, 1u);
         const fpt_status cs = checkWar(p);
         if (cs != FPT_OK) return cs;
         if (wavefront) e = launch_war_wavefront(scene->dev, p, pass.wavefront, pass.adjointScratch, true, st, pass.launches);

@@ -231,8 +231,11 @@ class WARDiffPathTracer(RenderPass):
         g = (C.c_float * 4)(*[float(x) for x in grad])
         check(lib().fpt_pass_set_diff_debug_params(self._h, t, int(id[0]), int(id[1]), int(offset), g))
 
-    def backward(self, render_data: Mapping[str, Any], dLdI, material_grad=None, position_grad=None, frame: int = 0) -> None:
-        """Adjoint of one frame into flat gradient tensors (fpt_pass_backward)."""
+    def backward(self, render_data: Mapping[str, Any], dLdI, material_grad=None, position_grad=None, frame: int = 0,
+                 normal_grad=None, tangent_grad=None) -> None:
+        """Adjoint of one frame into flat gradient tensors (fpt_pass_backward):
+        material parameters, and the positions, normals and tangents of the
+        vertices of meshToOptimize."""
         some = next((t for t in render_data.values() if t is not None), dLdI)
         height, width = int(some.shape[0]), int(some.shape[1])
         io = self._io(render_data, width, height, frame)
@@ -241,4 +244,8 @@ class WARDiffPathTracer(RenderPass):
         g.mesh_position = _ptr(position_grad)
         g.material_dim = material_grad.numel() if material_grad is not None else 0
         g.position_dim = position_grad.numel() if position_grad is not None else 0
+        g.mesh_normal = _ptr(normal_grad)
+        g.mesh_tangent = _ptr(tangent_grad)
+        g.normal_dim = normal_grad.numel() if normal_grad is not None else 0
+        g.tangent_dim = tangent_grad.numel() if tangent_grad is not None else 0
         check(lib().fpt_pass_backward(self._h, C.byref(io), C.c_void_p(_ptr(dLdI)), C.byref(g), C.c_void_p(_stream())))

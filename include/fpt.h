@@ -319,6 +319,10 @@ typedef struct fpt_grad_buffers {
     float* mesh_position;        /* vertex_count * 3 floats, or NULL          */
     uint32_t material_dim;       /* number of floats in `material`            */
     uint32_t position_dim;       /* number of floats in `mesh_position`       */
+    float* mesh_normal;          /* vertex normals (MeshNormal), or NULL      */
+    float* mesh_tangent;         /* vertex tangents (MeshTangent), or NULL    */
+    uint32_t normal_dim;         /* number of floats in `mesh_normal`         */
+    uint32_t tangent_dim;        /* number of floats in `mesh_tangent`        */
 } fpt_grad_buffers;
 
 /* bwd_diff(tracePaths) of WARDiffPathTracer.rt.slang:167-180 into caller-owned

@@ -79,7 +79,8 @@ def lib() -> C.CDLL:
         l.orc_path_tracer.argtypes = [_P, C.POINTER(PathTracerParams), _P, _P, _P, C.c_int, u32, u32, u32, u32, u32,
                                       C.POINTER(Counters)]
         l.orc_wardiff.restype = C.c_double
-        l.orc_wardiff.argtypes = [_P, C.POINTER(WarDiffParams), C.c_int, C.c_int, _P, u32, _P, u32, C.c_double, _P, _P, _P,
+        l.orc_wardiff.argtypes = [_P, C.POINTER(WarDiffParams), C.c_int, C.c_int, _P, u32, _P, u32, _P, u32, _P, u32, C.c_double,
+                                  _P, _P, _P,
                                   _P, u32, u32, u32, u32, u32, C.POINTER(C.c_uint64)]
         for n in ("orc_xoshiro", "orc_lcg"):
             getattr(l, n).argtypes = [_P, u32, u32, _P]
@@ -155,7 +156,7 @@ class OracleScene:
         return out, smp, cnt, dt
 
     def wardiff(self, params: WarDiffParams, mode: int = 0, dLdI=None, mat_tangents=None, pos_tangents=None, eps: float = 0.0,
-                threads: int = 0, rect=None):
+                threads: int = 0, rect=None, nrm_tangents=None, tan_tangents=None):
         """WARDiffPathTracer restatement.  mode 0: FP32 primal; 1: forward-mode
         derivatives along the rows of mat_tangents / pos_tangents (K <= 4) ->
         sum over pixels of dLdI . dL/dv_k; 2: radiance with the parameters offset
@@ -172,6 +173,13 @@ class OracleScene:
         if pos_tangents is not None:
             pt = np.ascontiguousarray(np.atleast_2d(pos_tangents), dtype=np.float64)
             K = max(K, pt.shape[0])
+        nt = tt = None
+        if nrm_tangents is not None:
+            nt = np.ascontiguousarray(np.atleast_2d(nrm_tangents), dtype=np.float64)
+            K = max(K, nt.shape[0])
+        if tan_tangents is not None:
+            tt = np.ascontiguousarray(np.atleast_2d(tan_tangents), dtype=np.float64)
+            K = max(K, tt.shape[0])
         grads = np.zeros(4, dtype=np.float64)
         pert = np.zeros((h, w, 3), dtype=np.float64) if mode in (2, 3) else None
         g = np.ascontiguousarray(dLdI, dtype=np.float32) if dLdI is not None else None
@@ -179,7 +187,9 @@ class OracleScene:
         rays = C.c_uint64()
         dt = lib().orc_wardiff(self._h, C.byref(params), mode, K, ptr(mt) if mt is not None else None,
                                mt.shape[1] if mt is not None else 0, ptr(pt) if pt is not None else None,
-                               pt.shape[1] if pt is not None else 0, eps, ptr(g) if g is not None else None, ptr(color),
+                               pt.shape[1] if pt is not None else 0, ptr(nt) if nt is not None else None,
+                               nt.shape[1] if nt is not None else 0, ptr(tt) if tt is not None else None,
+                               tt.shape[1] if tt is not None else 0, eps, ptr(g) if g is not None else None, ptr(color),
                                ptr(grads), ptr(pert) if pert is not None else None, threads, x0, y0, x1, y1, C.byref(rays))
         return color, (grads[:K] if mode == 1 else None), pert, int(rays.value), dt
 

@@ -259,7 +259,8 @@ void orc_bsdf_sample(const float* data, int lambert, uint32_t n, const float* wi
 // doubles, sum over the rectangle of dLdI . dL/dv_k (mode 1); pert: 3 doubles
 // per pixel of the perturbed radiance (mode 2).
 double orc_wardiff(const void* sp, const WarDiffParams* p, int mode, int K, const double* matTangents, uint32_t matDim,
-                   const double* posTangents, uint32_t posDim, double eps, const float* dLdI, float* color, double* grads,
+                   const double* posTangents, uint32_t posDim, const double* nrmTangents, uint32_t nrmDim,
+                   const double* tanTangents, uint32_t tanDim, double eps, const float* dLdI, float* color, double* grads,
                    double* pert, uint32_t threads, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, uint64_t* rays) {
     const Scene& s = *static_cast<const Scene*>(sp);
     WarSeeds seeds;
@@ -269,6 +270,10 @@ double orc_wardiff(const void* sp, const WarDiffParams* p, int mode, int K, cons
     seeds.pos = posTangents;
     seeds.posDim = posDim;
     seeds.meshID = p->meshID;
+    seeds.nrm = nrmTangents;
+    seeds.nrmDim = nrmDim;
+    seeds.tan = tanTangents;
+    seeds.tanDim = tanDim;
     seeds.eps = eps;
     uint32_t nthreads = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
     std::vector<std::vector<double>> acc(nthreads, std::vector<double>(4, 0.0));

@@ -60,6 +60,10 @@ struct WarSeeds {
     const double* pos = nullptr;     // K x posDim tangents of the positions of mesh `meshID` (localVertex * 3 + axis)
     uint32_t posDim = 0;
     uint32_t meshID = 0xffffffffu;
+    const double* nrm = nullptr;     // K x nrmDim tangents of the (normalised) vertex normals of mesh `meshID`
+    uint32_t nrmDim = 0;
+    const double* tan = nullptr;     // K x tanDim tangents of the (normalised) vertex tangents of mesh `meshID`
+    uint32_t tanDim = 0;
     double eps = 0;                  // Shadow: perturbation scale
 };
 

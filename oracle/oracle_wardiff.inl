@@ -40,6 +40,8 @@ template <class R> struct Seed;
 template <> struct Seed<float> {
     static float mat(const WarSeeds&, uint32_t, float v) { return v; }
     static float pos(const WarSeeds&, uint32_t, float v) { return v; }
+    static float nrm(const WarSeeds&, uint32_t, float v) { return v; }
+    static float tan(const WarSeeds&, uint32_t, float v) { return v; }
 };
 template <int N> struct Seed<Dual<N>> {
     static Dual<N> get(const double* t, uint32_t dim, int K, uint32_t idx, float v) {
@@ -50,6 +52,8 @@ template <int N> struct Seed<Dual<N>> {
     }
     static Dual<N> mat(const WarSeeds& s, uint32_t idx, float v) { return get(s.mat, s.matDim, s.K, idx, v); }
     static Dual<N> pos(const WarSeeds& s, uint32_t idx, float v) { return get(s.pos, s.posDim, s.K, idx, v); }
+    static Dual<N> nrm(const WarSeeds& s, uint32_t idx, float v) { return get(s.nrm, s.nrmDim, s.K, idx, v); }
+    static Dual<N> tan(const WarSeeds& s, uint32_t idx, float v) { return get(s.tan, s.tanDim, s.K, idx, v); }
 };
 template <> struct Seed<Shadow> {
     static Shadow get(const double* t, uint32_t dim, double eps, uint32_t idx, float v) {
@@ -59,6 +63,8 @@ template <> struct Seed<Shadow> {
     }
     static Shadow mat(const WarSeeds& s, uint32_t idx, float v) { return get(s.mat, s.matDim, s.eps, idx, v); }
     static Shadow pos(const WarSeeds& s, uint32_t idx, float v) { return get(s.pos, s.posDim, s.eps, idx, v); }
+    static Shadow nrm(const WarSeeds& s, uint32_t idx, float v) { return get(s.nrm, s.nrmDim, s.eps, idx, v); }
+    static Shadow tan(const WarSeeds& s, uint32_t idx, float v) { return get(s.tan, s.tanDim, s.eps, idx, v); }
 };
 
 template <class R> static V3<R> lift3(const V3<float>& a) { return V3<R>(R(a.x), R(a.y), R(a.z)); }
@@ -70,6 +76,7 @@ template <class R> struct WarIsect {
     float b[3];                  // computeBarycentrics of the ray/plane point
     V3<R> posW;                  // sum(v_i * b_i)
     V3<float> normalW, tangentW; // interpolated vertex normal / tangent (unnormalised)
+    V3<R> normalR, tangentR;     // the same with the seeded normal / tangent derivatives
     uint32_t localIdx[3];        // vertex indices within the mesh
 };
 
@@ -126,6 +133,18 @@ static WarIsect<R> war_intersection(const Scene& s, const WarSeeds& seeds, const
     }
     is.normalW = n[0] * is.b[0] + n[1] * is.b[1] + n[2] * is.b[2];
     is.tangentW = tg[0] * is.b[0] + tg[1] * is.b[1] + tg[2] * is.b[2];
+    // Vertex normals and tangents carry their own derivatives (bwd_loadVertexNormalsW /
+    // bwd_loadVertexTangentsW, DiffSceneIO.slang:151-250), indexed like the positions.
+    V3<R> nr[3], tr[3];
+    for (int i = 0; i < 3; i++) {
+        const uint32_t gi = all ? idx[i] : is.localIdx[i];
+        for (int a = 0; a < 3; a++) {
+            nr[i][a] = seeded ? Seed<R>::nrm(seeds, gi * 3 + a, n[i][a]) : R(n[i][a]);
+            tr[i][a] = seeded ? Seed<R>::tan(seeds, gi * 3 + a, tg[i][a]) : R(tg[i][a]);
+        }
+    }
+    is.normalR = nr[0] * R(is.b[0]) + nr[1] * R(is.b[1]) + nr[2] * R(is.b[2]);
+    is.tangentR = tr[0] * R(is.b[0]) + tr[1] * R(is.b[1]) + tr[2] * R(is.b[2]);
     return is;
 }
 
@@ -331,7 +350,8 @@ static R war_reparam_screen(const Scene& s, const WarSeeds& seeds, const WarDiff
 // Material instance built through GradientIOWrapper.getFloat
 // (StandardMaterial.slang:135-250); R carries the seeded derivatives.
 template <class R>
-static MaterialInstance<R> war_material(const Scene& s, const WarSeeds& seeds, const ShadingData<float>& sd, bool lambert) {
+static MaterialInstance<R> war_material(const Scene& s, const WarSeeds& seeds, const ShadingData<float>& sd, bool lambert,
+                                        const V3<R>* frame = nullptr) {
     const Material& m = s.materials[sd.materialID];
     const uint32_t base = sd.materialID * 20u;
     MaterialInstance<R> mi;
@@ -358,6 +378,7 @@ static MaterialInstance<R> war_material(const Scene& s, const WarSeeds& seeds, c
     d.roughness = roughness;
     d.metallic = metallic;
     mi.T = lift3<R>(sd.T); mi.B = lift3<R>(sd.B); mi.N = lift3<R>(sd.N);
+    if (frame) { mi.T = frame[0]; mi.B = frame[1]; mi.N = frame[2]; }
     if (!sd.frontFacing && m.doubleSided) mi.N = -mi.N;  // flipShadingNormal
     mi.emission = V3<R>(R(0));
     if (sd.frontFacing) mi.emission = V3<R>(R(m.emissive[0]), R(m.emissive[1]), R(m.emissive[2])) * R(m.emissiveFactor);
@@ -454,6 +475,8 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
         th.baryX = is.b[1];
         th.baryY = is.b[2];
         ShadingData<float> sd = load_shading_data<float>(s, th, rayDir);
+        float frameTw = 1.f;
+        bool frameValid = false;
         {
             // loadShadingData: sd.frame = createSafe(isect.normalW, float4(isect.tangentW, v.tangentW.w)).
             uint32_t vi[3];
@@ -469,6 +492,8 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
             const bool nonParallel = std::fabs(NdotT) < 0.9999f;
             const bool nonZero = dot(tg, tg) > 0.f;
             const bool valid = std::fabs(tw) == 1.f && nonZero && nonParallel;
+            frameTw = tw;
+            frameValid = valid;
             if (valid) {
                 sd.T = normalize(tg - sd.N * NdotT);
                 sd.B = cross(sd.N, sd.T) * tw;
@@ -478,7 +503,22 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
             }
         }
         const MaterialInstance<float> miV = war_material<float>(s, WarSeeds(), sd, p.lambert != 0);
-        const MaterialInstance<R> miR = war_material<R>(s, seeds, sd, p.lambert != 0);
+        // The differentiable frame: createSafe on the seeded normal and tangent, with the
+        // decisions (validity, perp_stark) taken on the FP32 values above.
+        V3<R> frameR[3];
+        {
+            const V3<R> NR = normalize(is.normalR);
+            const V3<R> tg = is.tangentR;
+            if (frameValid) {
+                frameR[0] = normalize(tg - NR * dot(tg, NR));
+                frameR[1] = cross(NR, frameR[0]) * R(frameTw);
+            } else {
+                frameR[0] = lift3<R>(sd.T);  // no_diff perp_stark
+                frameR[1] = cross(NR, frameR[0]);
+            }
+            frameR[2] = NR;
+        }
+        const MaterialInstance<R> miR = war_material<R>(s, seeds, sd, p.lambert != 0, frameR);
         ShadingData<R> sdR = sd_lift<R>(sd);
         sdR.V = -rayDirR;
 

@@ -514,3 +514,82 @@ def test_backward_diff_debug_translation_image(fpt):
     assert np.all(bc == 0) and np.all(bd[..., 1:] == 0)
     assert np.allclose(bd[..., 0], fd[..., 0], rtol=1e-5, atol=1e-5 * max(1.0, np.abs(fd[..., 0]).max()))
     assert np.abs(fd[..., 0]).max() > 0 and fc[..., :3].mean() > 0
+
+
+def _with_tangents(host):
+    """The scene with a valid tangent frame at every vertex (tangent = a fixed
+    direction made perpendicular to the normal, w = +1)."""
+    from falcor_b200.scene import HostScene
+    v = host.vertices.copy()
+    n = v[:, 3:6] / np.linalg.norm(v[:, 3:6], axis=1, keepdims=True)
+    t = np.cross(n, np.array([0.3, 0.5, 0.81], np.float32))
+    t /= np.linalg.norm(t, axis=1, keepdims=True)
+    v[:, 6:9] = t
+    v[:, 9] = 1.0
+    return HostScene.from_arrays(v, host.indices.copy(), host.instances.copy(), host.materials.copy(), _camera_dict(host))
+
+
+@pytest.mark.parametrize("kind", ["normal", "tangent"])
+def test_oracle_normal_tangent_gradients_match_finite_differences(oracle, kind):
+    """Derivatives with respect to the (normalised) vertex normals and tangents
+    of one mesh (bwd_loadVertexNormalsW / bwd_loadVertexTangentsW,
+    DiffSceneIO.slang:151-250) through the createSafe shading frame.  For an
+    isotropic BSDF a tangent change only rotates the frame about the normal, so
+    its derivative vanishes up to rounding."""
+    host = _with_tangents(H.box_icosphere(3))
+    osc = H.oracle_scene(host)
+    W = Hh = 40
+    mesh = 13
+    nv = mesh_vertex_count(host, mesh)
+    rng = np.random.default_rng(4)
+    dLdI = rng.standard_normal((Hh, W, 3)).astype(np.float32)
+    p = war_params(W, Hh, mesh=mesh)
+    Tg = rng.standard_normal((1, nv * 3)) * 0.1
+    key = "nrm_tangents" if kind == "normal" else "tan_tangents"
+    _, g, _, _, _ = osc.wardiff(p, mode=1, dLdI=dLdI, **{key: Tg})
+    eps = 1e-5
+    _, _, pp, _, _ = osc.wardiff(p, mode=2, eps=eps, **{key: Tg})
+    _, _, pm, _, _ = osc.wardiff(p, mode=2, eps=-eps, **{key: Tg})
+    fd = float(np.sum(dLdI.astype(np.float64) * (pp - pm) / (2 * eps)))
+    if kind == "normal":
+        assert abs(g[0]) > 1e-3
+        assert abs(fd - g[0]) <= 1e-4 * max(1.0, abs(g[0])), (fd, g[0])
+    else:
+        assert abs(g[0]) < 1e-6 and abs(fd) < 1e-4, (fd, g[0])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scheduler", ["Wavefront", "Megakernel"])
+def test_adjoint_normal_tangent_gradients_match_oracle(fpt, oracle, scheduler):
+    """MeshNormal / MeshTangent gradients through the shading frame, requested
+    together with position gradients (warped-area terms on)."""
+    import torch
+    from falcor_b200.passes import WARDiffPathTracer
+    host = _with_tangents(H.box_icosphere(3))
+    W, Hh = 64, 48
+    osc = H.oracle_scene(host)
+    mesh = 13
+    nv = mesh_vertex_count(host, mesh)
+    rng = np.random.default_rng(31)
+    dLdI = rng.standard_normal((Hh, W, 3)).astype(np.float32)
+    N = rng.standard_normal((2, nv * 3))
+    P = rng.standard_normal((2, nv * 3)) * 0.1
+    p = war_params(W, Hh, mesh=mesh, war=True)
+    _, gn_ref, _, _, _ = osc.wardiff(p, mode=1, dLdI=dLdI, nrm_tangents=N)
+    _, gt_ref, _, _, _ = osc.wardiff(p, mode=1, dLdI=dLdI, tan_tangents=N)
+    _, gp_ref, _, _, _ = osc.wardiff(p, mode=1, dLdI=dLdI, pos_tangents=P)
+    s = gpu_scene(host)
+    pt = WARDiffPathTracer(war_props(mesh=mesh, scheduler=scheduler, war=True))
+    pt.set_scene(s)
+    color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
+    gp, gn, gt = (torch.zeros(nv * 3, dtype=torch.float32, device="cuda") for _ in range(3))
+    pt.backward({"color": color}, torch.from_numpy(dLdI).cuda(), position_grad=gp, normal_grad=gn, tangent_grad=gt)
+    torch.cuda.synchronize()
+    gp, gn, gt = (t.cpu().numpy().astype(np.float64) for t in (gp, gn, gt))
+    for k in range(2):
+        a, b = float(N[k] @ gn), float(gn_ref[k])
+        assert abs(b) > 1e-2 and abs(a - b) <= WAR_RTOL * max(1.0, abs(b)), ("normal", k, a, b)
+        a, b = float(P[k] @ gp), float(gp_ref[k])
+        assert abs(a - b) <= WAR_RTOL * max(1.0, abs(b)), ("position", k, a, b)
+        # Isotropic BSDF: the tangent derivative vanishes up to FP32 rounding.
+        assert abs(float(N[k] @ gt)) <= 1e-3 * abs(float(gn_ref[k])) + 1e-4 and abs(float(gt_ref[k])) < 1e-6
