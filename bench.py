@@ -240,19 +240,42 @@ def adjoint_bench(dev) -> dict:
             pw.set_properties({"fixedSeed": f})
             pw.backward({"color": color}, dLdI, material_grad=gm, position_grad=gp)
 
+    # Checkpointed vertices: each frame's forward stores its hits and visibility,
+    # its adjoint reads them instead of re-tracing (frames interleaved).
+    pc = WARDiffPathTracer({"diffMode": "BackwardDiff", "maxBounces": w.max_bounces, "useWAR": False, "runBackward": 0,
+                            "meshToOptimize": -1, "adjointMode": "Checkpoint"})
+    pc.set_scene(scene)
+
+    def pair(q):
+        def run():
+            for f in range(frames):
+                q.set_properties({"fixedSeed": f})
+                q.execute({"color": color})
+                q.backward({"color": color}, dLdI, material_grad=gm, position_grad=gp)
+        return run
+
     for _ in range(2):
         fwd()
         bwd()
     bwd_war()
+    pair(pt)()
+    pair(pc)()
     t_fwd = _time_ms(fwd, 3)
     t_bwd = _time_ms(bwd, 3)
     t_war = _time_ms(bwd_war, 2)
+    t_pair_replay = _time_ms(pair(pt), 3)
+    t_pair_ckpt = _time_ms(pair(pc), 3)
+    ck_stats = pc.stats()
     paths = W * Hh * frames
     return {"workload": "displaced_sphere 512x512, 16 frames x 1 spp, maxBounces 4, material + position gradients",
             "unit": "Mpaths/s", "forward": round(paths / t_fwd / 1e3, 2), "adjoint": round(paths / t_bwd / 1e3, 2),
             "fwd_plus_adjoint": round(paths / (t_fwd + t_bwd) / 1e3, 2), "ms_forward": round(t_fwd, 3),
             "ms_adjoint": round(t_bwd, 3), "adjoint_war": round(paths / t_war / 1e3, 2),
             "fwd_plus_adjoint_war": round(paths / (t_fwd + t_war) / 1e3, 2), "ms_adjoint_war": round(t_war, 3),
+            "fwd_plus_adjoint_replay_interleaved": round(paths / t_pair_replay / 1e3, 2),
+            "fwd_plus_adjoint_checkpointed": round(paths / t_pair_ckpt / 1e3, 2),
+            "checkpoint_mb_per_frame": round(ck_stats.checkpoint_bytes / 2**20, 1),
+            "checkpoint_used": int(ck_stats.adjoint_checkpointed),
             "triangles": scene.info.triangle_count, "gradient_dims": [gm.numel(), gp.numel()]}
 
 

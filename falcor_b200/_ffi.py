@@ -89,7 +89,8 @@ class fpt_grad_config(C.Structure):
 
 
 class fpt_pass_stats(C.Structure):
-    _fields_ = [("paths", C.c_uint64), ("rays", C.c_uint64), ("device_error", u32), ("kernel_launches", u32)]
+    _fields_ = [("paths", C.c_uint64), ("rays", C.c_uint64), ("device_error", u32), ("kernel_launches", u32),
+                ("adjoint_checkpointed", u32), ("reserved", u32), ("checkpoint_bytes", C.c_uint64)]
 
 
 class fpt_batch_request(C.Structure):

@@ -123,6 +123,9 @@ void set_defaults(fpt_pass& p) {
         // "Wavefront" (default) or "Megakernel" (one thread per pixel); paths per wave.
         d["scheduler"] = PropValue::str("Wavefront");
         d["wavefrontCapacity"] = PropValue::num(1 << 22);
+        // "Replay" (re-trace the frame in the adjoint) or "Checkpoint" (the forward
+        // render stores the path vertices; the adjoint of the same frame reads them).
+        d["adjointMode"] = PropValue::str("Replay");
     }
 }
 
@@ -227,6 +230,7 @@ FPT_API void fpt_pass_destroy(fpt_pass* pass) {
     if (!pass) return;
     if (pass->scratch) cudaFree(pass->scratch);
     if (pass->adjointScratch) cudaFree(pass->adjointScratch);
+    if (pass->checkpoint) cudaFree(pass->checkpoint);
     delete pass;
 }
 
@@ -278,6 +282,8 @@ FPT_API fpt_status fpt_pass_set_property_string(fpt_pass* pass, const char* key,
         return set_error(FPT_ERR_INVALID_ARG, "diffuseBrdf must be 'Frostbite' or 'Lambert'");
     if (k == "scheduler" && v != "Wavefront" && v != "Megakernel")
         return set_error(FPT_ERR_INVALID_ARG, "scheduler must be 'Wavefront' or 'Megakernel'");
+    if (k == "adjointMode" && v != "Replay" && v != "Checkpoint")
+        return set_error(FPT_ERR_INVALID_ARG, "adjointMode must be 'Replay' or 'Checkpoint'");
     it->second.s = v;
     return FPT_OK;
 }
@@ -457,6 +463,8 @@ FPT_API fpt_status fpt_pass_get_stats(fpt_pass* pass, fpt_pass_stats* out, void*
     out->rays = c[1];
     out->device_error = err;
     out->kernel_launches = pass->launches;
+    out->adjoint_checkpointed = pass->lastAdjointCheckpointed ? 1u : 0u;
+    out->checkpoint_bytes = pass->checkpointBytes;
     return err ? set_error(FPT_ERR_DEVICE, "device error word 0x" + std::to_string(err)) : FPT_OK;
 }
 

@@ -40,6 +40,12 @@ struct fpt_pass {
     bool diffDebugExplicit = false;
     uint32_t diffDebugType = 0, diffDebugId[2] = {0, 0}, diffDebugOffset = 0;
     float diffDebugGrad[4] = {0.f, 0.f, 0.f, 0.f};
+    // WARDiffPathTracer adjointMode "Checkpoint": the path vertices of the last
+    // forward frame and the state they belong to.
+    void* checkpoint = nullptr;
+    size_t checkpointBytes = 0;
+    bool checkpointValid = false, lastAdjointCheckpointed = false;
+    uint64_t checkpointKey[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
     double num(const std::string& k) const;
     std::string str(const std::string& k) const;

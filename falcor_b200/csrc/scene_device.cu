@@ -395,6 +395,7 @@ FPT_API fpt_status fpt_scene_set_camera(fpt_scene* scene, const fpt_camera* came
     if (!scene || !camera) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_camera: null argument");
     compute_camera(*camera, scene->info.camera);
     scene->dev.camera = scene->info.camera;
+    scene->version++;
     return FPT_OK;
 }
 
@@ -449,6 +450,7 @@ FPT_API fpt_status fpt_scene_set_material_params(fpt_scene* scene, const uint32_
             hasTransmission = true;
     scene->materials.swap(next);
     scene->dev.hasTransmission = hasTransmission ? 1u : 0u;
+    scene->version++;
     return FPT_OK;
 }
 

@@ -30,4 +30,5 @@ struct fpt_scene {
     std::vector<fpt_material> materials;  // host copy of the material parameters
     float aliasWeightSum = 0.f;
     fpt_scene_info info{};
+    uint64_t version = 0;             // bumped by every change that can change a path (camera, materials)
 };

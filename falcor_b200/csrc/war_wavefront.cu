@@ -406,6 +406,58 @@ __global__ void __launch_bounds__(kShadeBlock) ww_sweep(DevScene s, WarParams p,
     }
 }
 
+// Checkpoint record (forward): the hits of the extension rays just traced.
+__global__ void ww_ck_record_hits(WaveParams wp, SoA w, WarCheckpoint ck, uint32_t it) {
+    const uint32_t n = wp.counts[1];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = wp.extQueue[k];
+        const uint32_t f = __float_as_uint(w.dirV[i].w);
+        ck.hits[size_t(it) * ck.pixels + wp.waveFirstPixel + i] = (f & 0x2u) ? w.hit[i] : make_uint4(kCkMiss, 0, 0, 0);
+    }
+}
+// Checkpoint record (forward): the visibility rays that found the light.
+__global__ void ww_ck_record_visible(WaveParams wp, SoA w, WarCheckpoint ck, uint32_t it) {
+    const uint32_t n = wp.counts[2];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = wp.shadowQueue[k];
+        if (w.sLr[i].w == 1.f) ck.visible[wp.waveFirstPixel + i] |= 1u << it;
+    }
+}
+// Checkpoint read (adjoint): the extension kernel's effect on the path state
+// (trace_queue, closest hit) from the stored hit.
+__global__ void ww_ck_extend(WaveParams wp, SoA w, WarCheckpoint ck, uint32_t it) {
+    const uint32_t n = wp.counts[1];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = wp.extQueue[k];
+        const uint4 h = ck.hits[size_t(it) * ck.pixels + wp.waveFirstPixel + i];
+        float4 d = w.dirV[i];
+        uint32_t f = __float_as_uint(d.w) + (1u << 16);  // vertexIndex++
+        if (h.x != kCkMiss) {
+            f |= 0x2u;
+            w.hit[i] = h;
+        } else {
+            f &= ~0x2u;
+        }
+        d.w = __uint_as_float(f);
+        w.dirV[i] = d;
+    }
+}
+// Checkpoint read (adjoint): the visibility kernel's effect (trace_queue, any hit).
+__global__ void ww_ck_shadow(WaveParams wp, SoA w, WarCheckpoint ck, uint32_t it) {
+    const uint32_t n = wp.counts[2];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = wp.shadowQueue[k];
+        if (!((ck.visible[wp.waveFirstPixel + i] >> it) & 1u)) continue;
+        const float4 lr = w.sLr[i];
+        float4 L = w.L[i];
+        L.x += lr.x;
+        L.y += lr.y;
+        L.z += lr.z;
+        w.L[i] = L;
+        w.sLr[i].w = 1.f;
+    }
+}
+
 __global__ void ww_resolve(WarParams p, WaveParams wp, SoA w) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePixels; i += gridDim.x * blockDim.x) {
         const float4 L = w.L[i];
@@ -433,7 +485,8 @@ __global__ void __launch_bounds__(kTraceBlock, FPT_TRACE_MIN_BLOCKS) ww_shadow(D
 
 template <bool HAS_T, bool BWD, bool WAR>
 cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adj, cudaStream_t st,
-                              uint32_t& launches) {
+                              uint32_t& launches, const WarCheckpoint* ck) {
+    const int ckMode = ck ? ck->mode : 0;
     SoA w;
     w.originPdf = b.f4(0); w.dirV = b.f4(1); w.thpB = b.f4(2); w.L = b.f4(3);
     w.sg = reinterpret_cast<uint4*>(b.f4(4)); w.hit = reinterpret_cast<uint4*>(b.f4(5));
@@ -480,14 +533,31 @@ cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBu
         const int genBlocks = std::min<int>(gShade, int((wp.wavePixels + kShadeBlock - 1) / kShadeBlock));
         ww_generate<BWD><<<genBlocks, kShadeBlock, 0, st>>>(s, p, wp, w, ww);
         launches++;
+        const int ckBlocks = std::min<int>(gShade, int((wp.wavePixels + kShadeBlock - 1) / kShadeBlock));
         for (uint32_t it = 0; it < maxIter; it++) {
-            ww_extend<<<gTrace, kTraceBlock, 0, st>>>(s, fp, wp, w);
+            if (ckMode == 2) {
+                ww_ck_extend<<<ckBlocks, kShadeBlock, 0, st>>>(wp, w, *ck, it);
+            } else {
+                ww_extend<<<gTrace, kTraceBlock, 0, st>>>(s, fp, wp, w);
+                if (ckMode == 1) {
+                    ww_ck_record_hits<<<ckBlocks, kShadeBlock, 0, st>>>(wp, w, *ck, it);
+                    launches++;
+                }
+            }
             ww_advance<<<1, 1, 0, st>>>(wp);
             std::swap(qa, qb);
             wp.shadeQueue = qa;
             wp.extQueue = qb;
             ww_shade<HAS_T, BWD, WAR><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w, ww);
-            ww_shadow<BWD><<<gTrace, kTraceBlock, 0, st>>>(s, fp, wp, w);
+            if (ckMode == 2) {
+                ww_ck_shadow<<<ckBlocks, kShadeBlock, 0, st>>>(wp, w, *ck, it);
+            } else if (ckMode == 1) {
+                ww_shadow<true><<<gTrace, kTraceBlock, 0, st>>>(s, fp, wp, w);
+                ww_ck_record_visible<<<ckBlocks, kShadeBlock, 0, st>>>(wp, w, *ck, it);
+                launches++;
+            } else {
+                ww_shadow<BWD><<<gTrace, kTraceBlock, 0, st>>>(s, fp, wp, w);
+            }
             launches += 4;
             if (BWD) {
                 ww_nee_grad<WAR><<<gNee, kShadeBlock, 0, st>>>(s, p, wp, w, ww);
@@ -507,6 +577,10 @@ cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBu
 
 }  // namespace
 
+size_t war_checkpoint_bytes(uint32_t pixels, uint32_t maxBounces) {
+    return (size_t(maxBounces) + 2) * pixels * sizeof(uint4) + size_t(pixels) * sizeof(uint32_t);
+}
+
 size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces, bool war) {
     const size_t maxVertices = size_t(maxBounces) + 2;
     const size_t nee = war ? kNeeArraysWar : kNeeArrays, rec = war ? kRecArraysWar : kRecArrays;
@@ -514,18 +588,18 @@ size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces, bool war) {
 }
 
 cudaError_t launch_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adjointScratch, bool backward,
-                                 cudaStream_t st, uint32_t& launches) {
+                                 cudaStream_t st, uint32_t& launches, const WarCheckpoint* ck) {
     // Extended records: the warps (position derivatives only) and normal / tangent gradients.
     const bool war = backward && ((p.useWAR && (p.gradPos || (p.dbgColor && p.dbgType == kDbgTranslation))) ||
                                   p.gradNrm || p.gradTan);
     if (s.hasTransmission) {
-        if (!backward) return run_war_wavefront<true, false, false>(s, p, b, adjointScratch, st, launches);
-        return war ? run_war_wavefront<true, true, true>(s, p, b, adjointScratch, st, launches)
-                   : run_war_wavefront<true, true, false>(s, p, b, adjointScratch, st, launches);
+        if (!backward) return run_war_wavefront<true, false, false>(s, p, b, adjointScratch, st, launches, ck);
+        return war ? run_war_wavefront<true, true, true>(s, p, b, adjointScratch, st, launches, ck)
+                   : run_war_wavefront<true, true, false>(s, p, b, adjointScratch, st, launches, ck);
     }
-    if (!backward) return run_war_wavefront<false, false, false>(s, p, b, adjointScratch, st, launches);
-    return war ? run_war_wavefront<false, true, true>(s, p, b, adjointScratch, st, launches)
-               : run_war_wavefront<false, true, false>(s, p, b, adjointScratch, st, launches);
+    if (!backward) return run_war_wavefront<false, false, false>(s, p, b, adjointScratch, st, launches, ck);
+    return war ? run_war_wavefront<false, true, true>(s, p, b, adjointScratch, st, launches, ck)
+               : run_war_wavefront<false, true, false>(s, p, b, adjointScratch, st, launches, ck);
 }
 
 }  // namespace fpt

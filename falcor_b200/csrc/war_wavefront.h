@@ -37,8 +37,22 @@ struct WarParams {
 // Bytes of adjoint scratch (pending NEE gradients + per-vertex records) for a
 // wave of `capacity` paths.
 size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces, bool war);
+
+// Checkpointed path vertices (adjointMode "Checkpoint"): the forward render
+// stores the hit of every extension ray and the outcome of every visibility
+// ray; the adjoint of the same frame reads them instead of tracing, and
+// recomputes the shading.
+struct WarCheckpoint {
+    uint4* hits;        // [bounce][pixel]: instance, primitive, baryX, baryY (instance kCkMiss: missed)
+    uint32_t* visible;  // [pixel]: bit b set when bounce b's visibility ray found the light
+    uint32_t pixels;
+    int mode;           // 0 off, 1 record (forward), 2 read (adjoint)
+};
+constexpr uint32_t kCkMiss = 0xffffffffu;
+size_t war_checkpoint_bytes(uint32_t pixels, uint32_t maxBounces);
+
 // Primal (backward = false) or adjoint of one frame; `launches` counts kernels.
 cudaError_t launch_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adjointScratch, bool backward,
-                                 cudaStream_t st, uint32_t& launches);
+                                 cudaStream_t st, uint32_t& launches, const WarCheckpoint* ck = nullptr);
 
 }  // namespace fpt

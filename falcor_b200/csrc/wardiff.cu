@@ -462,10 +462,47 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
             if (s != FPT_OK) return s;
         }
     }
+    // Checkpointed vertices belong to one frame: seed, size and the settings and
+    // scene state that decide the paths.
+    const bool checkpointMode = wavefront && pass.str("adjointMode") == "Checkpoint";
+    const uint64_t key[8] = {p.frameSeed, (uint64_t(p.width) << 32) | p.height, p.maxBounces,
+                             (uint64_t(p.useBSDFSampling) << 3) | (p.useNEE << 2) | (p.useMIS << 1) | p.useAntithetic,
+                             p.lambert, reinterpret_cast<uint64_t>(scene), scene->version, 0};
+    pass.lastAdjointCheckpointed = false;
     if (!backward) {
         if (mode != 3) {
-            if (wavefront) e = launch_war_wavefront(scene->dev, p, pass.wavefront, nullptr, false, st, pass.launches);
+            WarCheckpoint ck{};
+            bool record = false;
+            if (checkpointMode && wavefront) {
+                // Where memory allows: at most half of the free device memory.
+                const uint32_t pixels = p.width * p.height;
+                const size_t need = war_checkpoint_bytes(pixels, p.maxBounces);
+                if (pass.checkpointBytes < need) {
+                    if (pass.checkpoint) cudaFree(pass.checkpoint);
+                    pass.checkpoint = nullptr;
+                    pass.checkpointBytes = 0;
+                    size_t freeB = 0, totalB = 0;
+                    if (cudaMemGetInfo(&freeB, &totalB) == cudaSuccess && need <= freeB / 2 &&
+                        cudaMalloc(&pass.checkpoint, need) == cudaSuccess)
+                        pass.checkpointBytes = need;
+                    else
+                        log_warning("WARDiffPathTracer: not enough device memory for checkpointed vertices; the adjoint replays");
+                }
+                if (pass.checkpoint) {
+                    ck.hits = static_cast<uint4*>(pass.checkpoint);
+                    ck.visible = reinterpret_cast<uint32_t*>(ck.hits + size_t(p.maxBounces + 2) * pixels);
+                    ck.pixels = pixels;
+                    ck.mode = 1;
+                    record = cudaMemsetAsync(ck.visible, 0, size_t(pixels) * 4, st) == cudaSuccess;
+                }
+            }
+            pass.checkpointValid = false;
+            if (wavefront) e = launch_war_wavefront(scene->dev, p, pass.wavefront, nullptr, false, st, pass.launches, record ? &ck : nullptr);
             else e = launch_war_any<false>(scene->dev, p, st);
+            if (record && e == cudaSuccess) {
+                std::memcpy(pass.checkpointKey, key, sizeof(key));
+                pass.checkpointValid = true;
+            }
         }
         if (debug && e == cudaSuccess) {
             // ForwardDiffDebug / BackwardDiffDebug (WARDiffPathTracer.rt.slang:182-210): the
@@ -546,7 +583,17 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
         p.tanHash = std::max(p.tanHash, 1u);
         const fpt_status cs = checkWar(p);
         if (cs != FPT_OK) return cs;
-        if (wavefront) e = launch_war_wavefront(scene->dev, p, pass.wavefront, pass.adjointScratch, true, st, pass.launches);
+        WarCheckpoint ck{};
+        if (checkpointMode && pass.checkpointValid && std::memcmp(pass.checkpointKey, key, sizeof(key)) == 0) {
+            const uint32_t pixels = p.width * p.height;
+            ck.hits = static_cast<uint4*>(pass.checkpoint);
+            ck.visible = reinterpret_cast<uint32_t*>(ck.hits + size_t(p.maxBounces + 2) * pixels);
+            ck.pixels = pixels;
+            ck.mode = 2;
+            pass.lastAdjointCheckpointed = true;
+        }
+        if (wavefront)
+            e = launch_war_wavefront(scene->dev, p, pass.wavefront, pass.adjointScratch, true, st, pass.launches, ck.mode ? &ck : nullptr);
         else e = launch_war_any<true>(scene->dev, p, st);
     }
     if (!wavefront) pass.launches = 1;

@@ -395,6 +395,9 @@ typedef struct fpt_pass_stats {
     uint64_t rays;
     uint32_t device_error;
     uint32_t kernel_launches;
+    uint32_t adjoint_checkpointed;  /* WARDiff: the last adjoint read checkpointed vertices */
+    uint32_t reserved;
+    uint64_t checkpoint_bytes;      /* WARDiff: device bytes held for checkpointed vertices */
 } fpt_pass_stats;
 FPT_API fpt_status fpt_pass_get_stats(fpt_pass* pass, fpt_pass_stats* out, void* stream);
 

@@ -593,3 +593,44 @@ def test_adjoint_normal_tangent_gradients_match_oracle(fpt, oracle, scheduler):
         assert abs(a - b) <= WAR_RTOL * max(1.0, abs(b)), ("position", k, a, b)
         # Isotropic BSDF: the tangent derivative vanishes up to FP32 rounding.
         assert abs(float(N[k] @ gt)) <= 1e-3 * abs(float(gn_ref[k])) + 1e-4 and abs(float(gt_ref[k])) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("war", [False, True])
+def test_checkpointed_adjoint_matches_replay(fpt, war):
+    """adjointMode "Checkpoint": the forward frame stores its path vertices (hits
+    and visibility) and the adjoint of the same frame reads them instead of
+    tracing; the gradients equal the replay adjoint's.  A frame the checkpoint
+    does not belong to (another seed) falls back to replay."""
+    import torch
+    from falcor_b200.passes import WARDiffPathTracer
+    host = small_sphere()
+    W, Hh = 64, 64
+    s = gpu_scene(host)
+    nm, nv = host.desc.material_count, host.desc.vertex_count
+    dLdI = torch.randn((Hh, W, 3), dtype=torch.float32, device="cuda", generator=torch.Generator(device="cuda").manual_seed(3))
+    res = {}
+    for mode in ("Replay", "Checkpoint"):
+        props = dict(war_props(max_bounces=3, mesh=-1, war=war), adjointMode=mode)
+        pt = WARDiffPathTracer(props)
+        pt.set_scene(s)
+        color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
+        gm = torch.zeros(nm * 20, dtype=torch.float32, device="cuda")
+        gp = torch.zeros(nv * 3, dtype=torch.float32, device="cuda")
+        pt.set_properties({"diffMode": "Primal"})
+        pt.execute({"color": color})
+        pt.set_properties({"diffMode": "BackwardDiff"})
+        pt.backward({"color": color}, dLdI, material_grad=gm, position_grad=gp)
+        st = pt.stats()
+        res[mode] = (gm.cpu().numpy(), gp.cpu().numpy(), st.adjoint_checkpointed, st.rays, st.checkpoint_bytes)
+        if mode == "Checkpoint":
+            pt.set_properties({"fixedSeed": 4})
+            pt.backward({"color": color}, dLdI, material_grad=torch.zeros_like(gm), position_grad=torch.zeros_like(gp))
+            assert pt.stats().adjoint_checkpointed == 0
+    (rm, rp, rc, rr, _), (cm, cp, cc, cr, cb) = res["Replay"], res["Checkpoint"]
+    assert rc == 0 and cc == 1 and cb == (3 + 2) * W * Hh * 16 + W * Hh * 4
+    if not war:
+        assert rr > 0 and cr == 0  # the checkpointed adjoint traced no ray
+    assert np.abs(rm).max() > 0 and np.abs(rp).max() > 0
+    assert np.allclose(cm, rm, rtol=1e-4, atol=1e-5 * np.abs(rm).max())
+    assert np.allclose(cp, rp, rtol=1e-4, atol=1e-5 * np.abs(rp).max())
