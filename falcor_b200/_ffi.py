@@ -143,6 +143,9 @@ SIGNATURES = {
     "fpt_pass_set_scene_gradients": (C.c_int, [_P, _P]),
     "fpt_pass_set_dLdI": (C.c_int, [_P, _P]),
     "fpt_pass_set_diff_debug_params": (C.c_int, [_P, u32, u32, u32, u32, C.POINTER(C.c_float)]),
+    "fpt_scene_get_mesh_info": (C.c_int, [_P, u32, C.POINTER(u32), C.POINTER(u32)]),
+    "fpt_scene_get_mesh_vertices_and_indices": (C.c_int, [_P, u32, _P, _P, _P, _P]),
+    "fpt_scene_set_mesh_vertices": (C.c_int, [_P, u32, _P, _P, _P, _P, _P]),
     "fpt_pass_get_stats": (C.c_int, [_P, C.POINTER(fpt_pass_stats), _P]),
     "fpt_pass_get_counters": (C.c_int, [_P, C.POINTER(C.c_uint64), u32, _P]),
     "fpt_pass_get_kernel_times": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_uint64), u32, C.c_int]),

@@ -272,6 +272,17 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
         }
     }
     build_alias_table(flux, s.aliasTable, s.aliasWeightSum);
+    s.meshVertexCount.assign(d.instance_count, 0);
+    s.meshTriCount.assign(d.instance_count, 0);
+    s.meshEmissive.assign(d.instance_count, 0);
+    for (uint32_t i = 0; i < d.instance_count; i++) {
+        const fpt_geometry_instance& in = d.instances[i];
+        uint32_t nv = 0;
+        for (uint32_t k = 0; k < in.triangle_count * 3; k++) nv = std::max(nv, d.indices[in.ib_offset + k] + 1);
+        s.meshVertexCount[i] = nv;
+        s.meshTriCount[i] = in.triangle_count;
+        s.meshEmissive[i] = instOff[i] != 0xffffffffu ? 1 : 0;
+    }
     std::vector<uint2> alias(em.size());
     for (size_t i = 0; i < em.size(); i++) alias[i] = make_uint2(s.aliasTable[2 * i], s.aliasTable[2 * i + 1]);
 

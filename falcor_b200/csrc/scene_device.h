@@ -30,5 +30,13 @@ struct fpt_scene {
     std::vector<fpt_material> materials;  // host copy of the material parameters
     float aliasWeightSum = 0.f;
     fpt_scene_info info{};
-    uint64_t version = 0;             // bumped by every change that can change a path (camera, materials)
+    uint64_t version = 0;             // bumped by every change that can change a path (camera, materials, vertices)
+    // Per mesh (= geometry instance): vertex and triangle counts, emissive flag.
+    std::vector<uint32_t> meshVertexCount, meshTriCount;
+    std::vector<uint8_t> meshEmissive;
+    // BVH refit after vertex updates: node index range of each tree level
+    // (breadth-first order), a node-box buffer and a device status word.
+    std::vector<uint32_t> levelStart;
+    float* nodeBoxes = nullptr;
+    uint32_t* refitStatus = nullptr;
 };

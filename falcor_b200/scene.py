@@ -182,6 +182,46 @@ class Scene:
         check(lib().fpt_scene_set_material_params(self._h, ids.ctypes.data_as(C.POINTER(C.c_uint32)), len(ids),
                                                   params.ctypes.data_as(C.POINTER(C.c_float))))
 
+    def get_mesh(self, mesh_id: int) -> dict:
+        """Scene::getMesh: vertex and triangle counts of a mesh (geometry instance)."""
+        nv, nt = C.c_uint32(), C.c_uint32()
+        check(lib().fpt_scene_get_mesh_info(self._h, int(mesh_id), C.byref(nv), C.byref(nt)))
+        return {"vertex_count": int(nv.value), "triangle_count": int(nt.value)}
+
+    def get_mesh_vertices_and_indices(self, mesh_id: int, buffers: dict) -> None:
+        """Scene::getMeshVerticesAndIndices into CUDA tensors: buffers["positions"]
+        and ["texcrds"] float32 [vertex_count, 3], ["triangleIndices"] int32/uint32
+        [triangle_count, 3]."""
+        import torch
+        req = ("positions", "texcrds", "triangleIndices")
+        for k in req:
+            if k not in buffers:
+                raise KeyError(f"Mesh data buffer '{k}' is missing.")
+        info = self.get_mesh(mesh_id)
+        for k, n in (("positions", info["vertex_count"]), ("texcrds", info["vertex_count"]), ("triangleIndices", info["triangle_count"])):
+            t = buffers[k]
+            if not (t.is_cuda and t.is_contiguous() and t.numel() >= 3 * n and t.element_size() == 4):
+                raise ValueError(f"buffer '{k}' must be a contiguous CUDA tensor of >= {3 * n} 4-byte elements")
+        check(lib().fpt_scene_get_mesh_vertices_and_indices(self._h, int(mesh_id), buffers["positions"].data_ptr(),
+                                                             buffers["texcrds"].data_ptr(), buffers["triangleIndices"].data_ptr(),
+                                                             torch.cuda.current_stream().cuda_stream))
+
+    def set_mesh_vertices(self, mesh_id: int, buffers: dict) -> None:
+        """Scene::setMeshVertices from CUDA float32 tensors [vertex_count, 3]:
+        buffers["positions"], ["normals"], ["tangents"], ["texcrds"]; refits the BVH."""
+        import torch
+        info = self.get_mesh(mesh_id)
+        ptrs = []
+        for k in ("positions", "normals", "tangents", "texcrds"):
+            if k not in buffers:
+                raise KeyError(f"Mesh data buffer '{k}' is missing.")
+            t = buffers[k]
+            if not (t.is_cuda and t.is_contiguous() and t.dtype == torch.float32 and t.numel() >= 3 * info["vertex_count"]):
+                raise ValueError(f"buffer '{k}' must be a contiguous CUDA float32 tensor of [{info['vertex_count']}, 3]")
+            ptrs.append(t.data_ptr())
+        check(lib().fpt_scene_set_mesh_vertices(self._h, int(mesh_id), *ptrs, torch.cuda.current_stream().cuda_stream))
+        check(lib().fpt_scene_get_info(self._h, C.byref(self.info)))
+
     def bvh(self) -> tuple[np.ndarray, np.ndarray]:
         """Host copies of the 8-wide BVH nodes (80 B each) and triangle records (48 B each)."""
         v = _ffi.fpt_bvh_view()

@@ -245,6 +245,24 @@ FPT_API fpt_status fpt_scene_get_material_params(const fpt_scene* scene, const u
 FPT_API fpt_status fpt_scene_set_material_params(fpt_scene* scene, const uint32_t* ids, uint32_t count, const float* params);
 /* Host view of the scene's BVH (valid until the scene is destroyed). */
 FPT_API fpt_status fpt_scene_get_bvh(const fpt_scene* scene, fpt_bvh_view* out);
+/* Scene::getMesh(meshID).vertexCount / getTriangleCount() (Scene.h): mesh =
+ * geometry instance of the scene description. */
+FPT_API fpt_status fpt_scene_get_mesh_info(const fpt_scene* scene, uint32_t mesh_id, uint32_t* vertex_count,
+                                           uint32_t* triangle_count);
+/* Scene::getMeshVerticesAndIndices (Scene.cpp:4291-4312, MeshIO.cs.slang:36-63):
+ * device arrays positions[vertex_count * 3], texcrds[vertex_count * 3]
+ * (u, v, 0) and triangle_indices[triangle_count * 3] (mesh-local), all
+ * required, written on `stream`. */
+FPT_API fpt_status fpt_scene_get_mesh_vertices_and_indices(fpt_scene* scene, uint32_t mesh_id, float* positions, float* texcrds,
+                                                           uint32_t* triangle_indices, void* stream);
+/* Scene::setMeshVertices (Scene.cpp:4314-4330, MeshIO.cs.slang:65-92): device
+ * arrays positions, normals, tangents, texcrds of vertex_count * 3 floats
+ * (tangent w is set to +1).  Refits the BVH on the device (the BLAS/TLAS
+ * update of updateForInverseRendering) and synchronises `stream`.  Emissive
+ * meshes are fixed (FPT_ERR_UNSUPPORTED); positions beyond |x| = 1e15 are
+ * reported with FPT_ERR_INVALID_ARG after the update. */
+FPT_API fpt_status fpt_scene_set_mesh_vertices(fpt_scene* scene, uint32_t mesh_id, const float* positions, const float* normals,
+                                               const float* tangents, const float* texcrds, void* stream);
 /* Host copy of the emissive alias table (uint2 per emissive triangle) and
  * the reciprocal weight sum (EmissivePowerSampler::bindShaderData). */
 FPT_API fpt_status fpt_scene_get_alias_table(const fpt_scene* scene, uint32_t* out_pairs,
