@@ -88,6 +88,11 @@ class fpt_grad_config(C.Structure):
     _fields_ = [("grad_type", u32), ("dim", u32), ("hash_size", u32)]
 
 
+class fpt_light_bvh_view(C.Structure):
+    _fields_ = [("nodes", C.POINTER(u32)), ("node_count", u32), ("triangle_indices", C.POINTER(u32)),
+                ("triangle_index_count", u32), ("bitmasks", C.POINTER(C.c_uint64)), ("bitmask_count", u32)]
+
+
 class fpt_pass_stats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("rays", C.c_uint64), ("device_error", u32), ("kernel_launches", u32),
                 ("adjoint_checkpointed", u32), ("reserved", u32), ("checkpoint_bytes", C.c_uint64)]
@@ -144,6 +149,7 @@ SIGNATURES = {
     "fpt_pass_set_dLdI": (C.c_int, [_P, _P]),
     "fpt_pass_set_diff_debug_params": (C.c_int, [_P, u32, u32, u32, u32, C.POINTER(C.c_float)]),
     "fpt_scene_get_mesh_info": (C.c_int, [_P, u32, C.POINTER(u32), C.POINTER(u32)]),
+    "fpt_scene_get_light_bvh": (C.c_int, [_P, _P]),
     "fpt_scene_get_mesh_vertices_and_indices": (C.c_int, [_P, u32, _P, _P, _P, _P]),
     "fpt_scene_set_mesh_vertices": (C.c_int, [_P, u32, _P, _P, _P, _P, _P]),
     "fpt_pass_get_stats": (C.c_int, [_P, C.POINTER(fpt_pass_stats), _P]),

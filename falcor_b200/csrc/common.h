@@ -25,6 +25,7 @@ fpt_hitinfo_bits compute_hit_bits(const fpt_scene_desc& d);
 uint16_t f32_to_f16_host(float v);
 float f16_to_f32_host(uint16_t h);
 uint32_t encode_normal_2x16_host(const float n[3]);
+void decode_normal_2x16_host(uint32_t p, float n[3]);
 
 // ---------------------------------------------------------------------------
 // Device data layouts (all 16-byte aligned).
@@ -119,6 +120,23 @@ struct BVH8 {
 // slot ordering and quantises the child boxes conservatively.
 void build_bvh8(const std::vector<float>& triVerts,  // 9 floats per global triangle
                 const std::vector<uint32_t>& triInstance, const std::vector<uint32_t>& triPrim, BVH8& out);
+
+// Light BVH (Rendering/Lights/LightBVH*.{cpp,slang}): 32-byte compressed
+// PackedNode (LightBVHTypes.slang:102-200), the emissive-triangle index list of
+// the leaves, and per emissive triangle the bit path to its leaf (all ones:
+// culled, zero flux).
+struct LightBVHNode {
+    uint32_t w[8];
+};
+struct LightBVH {
+    std::vector<LightBVHNode> nodes;
+    std::vector<uint32_t> triIndices;
+    std::vector<uint64_t> bitmasks;
+};
+// triVerts: 9 floats, triNormals: 3 floats (unit face normal), flux: 1 float per
+// emissive triangle of the light collection.
+void build_light_bvh(const std::vector<float>& triVerts, const std::vector<float>& triNormals, const std::vector<float>& flux,
+                     LightBVH& out);
 
 // Decodes a quantised child box exactly as the device does (fmaf(q, scale, p)).
 void decode_child_box(const BVH8Node& n, int slot, float lo[3], float hi[3]);

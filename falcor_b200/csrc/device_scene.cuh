@@ -21,6 +21,10 @@ struct DevScene {
     const uint2* alias;
     const uint32_t* instEmissiveOffset;
     const uint32_t* activeTris;
+    const uint4* lbvhNodes;           // light BVH: PackedNode, 2 x uint4 each
+    const uint32_t* lbvhTriIndices;   // emissive triangle indices of the leaves
+    const uint2* lbvhBitmasks;        // per emissive triangle: bit path to its leaf (lo, hi)
+    uint32_t lbvhNodeCount;
     const float4* env;                // envW x envH texels (rgb, 0)
     const float* impMips;             // importance mips, concatenated
     uint32_t emissiveCount, activeCount;
@@ -734,8 +738,155 @@ FPT_D float eval_triangle_pdf(const DevScene& s, float3 posW, uint32_t tri, floa
     const float denom = hmax(kFltMin, cosTheta * area);
     return distSqr / denom;
 }
+// ---------------------------------------------------------------------------
+// LightBVHSampler (Rendering/Lights/LightBVHSampler.slang:55-534) with its
+// default options: bounding cone, lighting cone, node flux, uniform triangle
+// selection in a leaf, SolidAngleBoundMethod::Sphere.
+// ---------------------------------------------------------------------------
+struct LbvhNode {
+    uint32_t w0;  // leaf: 1 << 31 | count << 27 | offset; internal: right child
+    float3 origin, extent, coneDir;
+    float cosCone, flux;
+};
+FPT_D LbvhNode lbvh_node(const DevScene& s, uint32_t i) {
+    const uint4 a = __ldg(s.lbvhNodes + 2 * i), b = __ldg(s.lbvhNodes + 2 * i + 1);
+    LbvhNode n;
+    n.w0 = a.x;
+    n.origin = make_float3(__uint_as_float(a.y), __uint_as_float(a.z), __uint_as_float(a.w));
+    n.extent = make_float3(f16(b.x & 0xffffu), f16(b.x >> 16), f16(b.y & 0xffffu));
+    n.cosCone = float(b.y >> 16) * (1.f / 32767.f) - 1.f;
+    n.coneDir = decode_normal2x16(b.z);
+    n.flux = __uint_as_float(b.w);
+    return n;
+}
+FPT_D bool lbvh_is_leaf(uint32_t w0) { return (w0 >> 31) != 0; }
+FPT_D float cos_sub_clamped(float sinA, float cosA, float sinB, float cosB) {
+    if (cosA > cosB) return 1.f;
+    return cosA * cosB + sinA * sinB;
+}
+FPT_D float sin_sub_clamped(float sinA, float cosA, float sinB, float cosB) {
+    if (cosA > cosB) return 0.f;
+    return sinA * cosB - cosA * sinB;
+}
+// boundCosineTerm with boundSphereSubtendedConeAngle (GeometryHelpers.slang:222-240).
+FPT_D float lbvh_bound_cosine(float3 posW, float3 normalW, float3 center, float3 extent, float& cosThetaCone) {
+    const float sqrRadius = dot(extent, extent);
+    const float3 c = center - posW;
+    const float d2 = dot(c, c);
+    float sinThetaCone;
+    if (d2 < sqrRadius) {
+        sinThetaCone = 0.f;
+        cosThetaCone = -1.f;
+    } else {
+        const float sin2 = sqrRadius / d2;
+        cosThetaCone = sqrtf(1.f - sin2);
+        sinThetaCone = sqrtf(sin2);
+    }
+    const float3 L = normalize(center - posW);
+    const float cosThetaL = fminf(fmaxf(dot(normalW, L), -1.f), 1.f);
+    const float sinThetaL = sqrtf(1.f - cosThetaL * cosThetaL);
+    return saturate(cos_sub_clamped(sinThetaL, cosThetaL, sinThetaCone, cosThetaCone));
+}
+// computeImportance (LightBVHSampler.slang:206-259).
+FPT_D float lbvh_importance(const DevScene& s, float3 posW, float3 normalW, bool upper, uint32_t i) {
+    const LbvhNode n = lbvh_node(s, i);
+    float distance = length(n.origin - posW);
+    float cosThetaBoundingCone = 0.f;
+    float NdotL = lbvh_bound_cosine(posW, normalW, n.origin, n.extent, cosThetaBoundingCone);
+    if (!upper) NdotL = 1.f;  // the NdotL bound only for the upper hemisphere
+    float orientationWeight = 1.f;
+    const float3 dirToAabb = (n.origin - posW) / distance;
+    if (n.cosCone != -1.f && n.cosCone > 0.f) {
+        const float sinConeAngle = sqrtf(fmaxf(0.f, 1.f - n.cosCone * n.cosCone));
+        const float cosTheta = dot(n.coneDir, -dirToAabb);
+        const float sinTheta = sqrtf(fmaxf(0.f, 1.f - cosTheta * cosTheta));
+        const float sinThetaBoundingCone = sqrtf(fmaxf(0.f, 1.f - cosThetaBoundingCone * cosThetaBoundingCone));
+        const float cosTheta0 = cos_sub_clamped(sinTheta, cosTheta, sinConeAngle, n.cosCone);
+        const float sinTheta0 = sin_sub_clamped(sinTheta, cosTheta, sinConeAngle, n.cosCone);
+        const float cosThetaPrime = cos_sub_clamped(sinTheta0, cosTheta0, sinThetaBoundingCone, cosThetaBoundingCone);
+        orientationWeight = fmaxf(0.f, cosThetaPrime);
+    }
+    const float halfRadius = fmaxf(n.extent.x, fmaxf(n.extent.y, n.extent.z));
+    distance = fmaxf(halfRadius, distance);
+    return (n.flux * NdotL) * orientationWeight / (distance * distance);
+}
+// sampleLightViaBVH (traverseTree + pickTriangle, uniform in the leaf).
+FPT_D bool lbvh_select(const DevScene& s, float3 posW, float3 normalW, bool upper, float u, float& pdf, uint32_t& tri) {
+    pdf = 1.f;
+    uint32_t node = 0;
+    uint32_t w0 = __ldg(&s.lbvhNodes[0].x);
+    for (int depth = 0; !lbvh_is_leaf(w0) && depth < 64; depth++) {
+        const uint32_t left = node + 1, right = w0;
+        const float il = lbvh_importance(s, posW, normalW, upper, left);
+        const float ir = lbvh_importance(s, posW, normalW, upper, right);
+        const float total = il + ir;
+        if (total == 0.f) return false;
+        const float pLeft = il / total;
+        const float pRight = 1.f - pLeft;
+        if (u < pLeft) {
+            u = u / pLeft;
+            pdf *= pLeft;
+            node = left;
+        } else {
+            u = (u - pLeft) / pRight;
+            pdf *= pRight;
+            node = right;
+        }
+        w0 = __ldg(&s.lbvhNodes[2 * node].x);
+    }
+    if (!lbvh_is_leaf(w0)) return false;
+    const uint32_t count = (w0 >> 27) & 15u, offset = w0 & ((1u << 27) - 1u);
+    const uint32_t idx = min(uint32_t(u * float(count)), count - 1);
+    tri = __ldg(s.lbvhTriIndices + offset + idx);
+    pdf *= 1.f / float(count);
+    return true;
+}
+// evalTriangleSelectionPdf (LightBVHSampler.slang:95-125): the traversal pdf along
+// the triangle's bit path times the uniform leaf selection.
+FPT_D float lbvh_selection_pdf(const DevScene& s, float3 posW, float3 normalW, bool upper, uint32_t tri) {
+    const uint2 m = __ldg(s.lbvhBitmasks + tri);
+    uint64_t bitmask = (uint64_t(m.y) << 32) | m.x;
+    float pdf = 1.f;
+    uint32_t node = 0;
+    uint32_t w0 = __ldg(&s.lbvhNodes[0].x);
+    for (int depth = 0; !lbvh_is_leaf(w0) && depth < 64; depth++) {
+        const uint32_t left = node + 1, right = w0;
+        const float il = lbvh_importance(s, posW, normalW, upper, left);
+        const float ir = lbvh_importance(s, posW, normalW, upper, right);
+        const float total = il + ir;
+        if (total == 0.f) return 0.f;
+        const float pLeft = il / total;
+        const float pRight = 1.f - pLeft;
+        if ((bitmask & 1ull) == 0) {
+            pdf *= pLeft;
+            node = left;
+        } else {
+            pdf *= pRight;
+            node = right;
+        }
+        bitmask >>= 1;
+        w0 = __ldg(&s.lbvhNodes[2 * node].x);
+    }
+    if (!lbvh_is_leaf(w0)) return 0.f;
+    const uint32_t count = (w0 >> 27) & 15u;
+    return pdf * (1.f / float(count));
+}
+
 template <class SG>
-FPT_D bool emissive_sample(const DevScene& s, uint32_t samplerType, float3 posW, SG& sg, TriLightSample& ls) {
+FPT_D bool emissive_sample(const DevScene& s, uint32_t samplerType, float3 posW, SG& sg, TriLightSample& ls,
+                           float3 normalW = make_float3(0.f, 0.f, 0.f), bool upperHemisphere = false) {
+    if (samplerType == 1) {
+        // LightBVHSampler::sampleLight (LightBVHSampler.slang:70-90).
+        if (s.emissiveCount == 0 || s.lbvhNodeCount == 0) return false;
+        const float uLight = next1D(sg);
+        float selPdf;
+        uint32_t tri;
+        if (!lbvh_select(s, posW, normalW, upperHemisphere, uLight, selPdf, tri)) return false;
+        const float2 u = next2D(sg);
+        if (!sample_triangle_light(s, posW, tri, u, ls)) return false;
+        ls.pdf *= selPdf;
+        return true;
+    }
     if (samplerType == 0) {
         if (s.activeCount == 0) return false;
         const float uLight = next1D(sg);
@@ -763,10 +914,15 @@ FPT_D bool emissive_sample(const DevScene& s, uint32_t samplerType, float3 posW,
     ls.pdf *= selPdf;
     return true;
 }
-FPT_D float emissive_eval_pdf(const DevScene& s, uint32_t samplerType, float3 posW, uint32_t tri, float3 hitPos, float3 hitN) {
+FPT_D float emissive_eval_pdf(const DevScene& s, uint32_t samplerType, float3 posW, uint32_t tri, float3 hitPos, float3 hitN,
+                              float3 normalW = make_float3(0.f, 0.f, 0.f), bool upperHemisphere = false) {
     if (tri == 0xffffffffu) return 0.f;
     float sel;
-    if (samplerType == 0) sel = s.activeCount > 0 ? 1.f / float(s.activeCount) : 0.f;
+    if (samplerType == 1) {
+        if (s.lbvhNodeCount == 0) return 0.f;
+        sel = lbvh_selection_pdf(s, posW, normalW, upperHemisphere, tri);
+        if (sel == 0.f) return 0.f;
+    } else if (samplerType == 0) sel = s.activeCount > 0 ? 1.f / float(s.activeCount) : 0.f;
     else sel = __ldg(s.flux + tri) * s.invWeightSum;
     return sel * eval_triangle_pdf(s, posW, tri, hitPos, hitN);
 }

@@ -135,6 +135,22 @@ uint32_t encode_normal_2x16_host(const float n[3]) {
     return (uint32_t(float_to_snorm16(px)) & 0xffffu) | (uint32_t(float_to_snorm16(py)) << 16);
 }
 
+void decode_normal_2x16_host(uint32_t p, float n[3]) {
+    // decodeNormal2x16 (Utils/Math/PackedFormats.h:87-91): snorm 2x16, octahedral map,
+    // normalize as v * rsqrt(dot(v, v)).
+    const float x = std::max(float(int32_t(p << 16) >> 16) / 32767.f, -1.f);
+    const float y = std::max(float(int32_t(p) >> 16) / 32767.f, -1.f);
+    float v[3] = {x, y, 1.f - std::fabs(x) - std::fabs(y)};
+    if (v[2] < 0.f) {
+        const float wx = (1.f - std::fabs(v[1])) * (v[0] >= 0.f ? 1.f : -1.f);
+        const float wy = (1.f - std::fabs(v[0])) * (v[1] >= 0.f ? 1.f : -1.f);
+        v[0] = wx;
+        v[1] = wy;
+    }
+    const float r = 1.f / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    for (int a = 0; a < 3; a++) n[a] = v[a] * r;
+}
+
 }  // namespace fpt
 
 extern "C" {

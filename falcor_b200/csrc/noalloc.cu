@@ -27,7 +27,7 @@ constexpr uint32_t kNoAllocPaths = 16384;
 constexpr size_t kHeaderBytes = 256;  // event counters, work counter
 constexpr size_t kNoAllocBytes =
     kHeaderBytes + WavefrontBuffers::kFloat4Arrays * size_t(kNoAllocPaths) * 16 + size_t(kNoAllocPaths) * 12 +
-    3 * size_t(kNoAllocPaths) * 4 + 256;  // = WavefrontBuffers::bytes_for(kNoAllocPaths) + header (2.63 MiB)
+    3 * size_t(kNoAllocPaths) * 4 + 256;  // = WavefrontBuffers::bytes_for(kNoAllocPaths) + header (2.88 MiB)
 constexpr uint32_t kNoAllocMaxDim = 4096;  // PathTracer kMaxFrameDimension (Params.slang:68)
 
 __device__ __align__(256) unsigned char g_noallocScratch[kNoAllocBytes];

@@ -192,14 +192,7 @@ void path_tracer_params(fpt_pass& p, FrameParams& fp) {
     fp.misHeuristic = mh == kMISHeuristics.end() ? 0u : uint32_t(mh->second);
     fp.misPowerExponent = float(p.num("misPowerExponent"));
     auto es = kEmissiveSamplers.find(p.str("emissiveSampler"));
-    int sampler = es == kEmissiveSamplers.end() ? 1 : es->second;
-    if (sampler == 1) {
-        if (!p.warnedLightBVH) {
-            log_warning("PathTracer: emissiveSampler 'LightBVH' is not implemented; using 'Power'");
-            p.warnedLightBVH = true;
-        }
-        sampler = 2;
-    }
+    const int sampler = es == kEmissiveSamplers.end() ? 1 : es->second;
     fp.emissiveSampler = uint32_t(sampler);
     fp.specularRoughnessThreshold = float(std::clamp(p.num("specularRoughnessThreshold"), 0.0, 1.0));
     auto cf = kColorFormats.find(p.str("colorFormat"));

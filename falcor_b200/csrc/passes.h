@@ -30,7 +30,6 @@ struct fpt_pass {
     size_t adjointScratchBytes = 0;
     uint32_t frameCount = 0;
     bool useFixedSeed = false;
-    bool warnedLightBVH = false;
     uint32_t launches = 0;
     fpt::WavefrontBuffers wavefront;  // path state of the wavefront scheduler
     fpt::KernelTimer timer;           // per-category kernel timing ("profileKernels")

@@ -109,7 +109,8 @@ FPT_D bool generate_light_sample(const DevScene& s, const FrameParams& p, const 
     if (useEm && lightType == 1) {
         TriLightSample tls;
         cnt.v[7]++;
-        if (emissive_sample(s, p.emissiveSampler, sd.posW, sg, tls)) {
+        // generateEmissiveSample: upperHemisphere = upper && !lower (PathTracer.slang:705-720).
+        if (emissive_sample(s, p.emissiveSampler, sd.posW, sg, tls, sd_oriented_face_n(sd), upper && !lower)) {
             Li = tls.pdf > 0.f ? tls.Le / tls.pdf : f3(0.f);
             lpdf = tls.pdf;
             const float3 lightPos = compute_ray_origin(tls.posW, tls.normalW);
@@ -147,7 +148,10 @@ FPT_D void pt_handle_hit(const DevScene& s, const FrameParams& p, PathState<SG>&
             const uint32_t off = __ldg(s.instEmissiveOffset + path.hit.instanceID);
             const uint32_t triIdx = off == 0xffffffffu ? 0xffffffffu : off + path.hit.primIndex;
             const float emissiveSel = (useEnv && useEm) ? 0.5f : 1.f;
-            const float lightPdf = emissiveSel * emissive_eval_pdf(s, p.emissiveSampler, path.origin, triIdx, sd.posW, sd_oriented_face_n(sd));
+            // upperHemisphere = isLightSampledUpper && !isLightSampledLower (PathTracer.slang:909).
+            const bool upperOnly = path.has(PF_LIGHT_UPPER) && !path.has(PF_LIGHT_LOWER);
+            const float lightPdf = emissiveSel * emissive_eval_pdf(s, p.emissiveSampler, path.origin, triIdx, sd.posW,
+                                                                   sd_oriented_face_n(sd), path.normal, upperOnly);
             misWeight = eval_mis(p, path.pdf, lightPdf);
         }
         path.L += path.thp * (misWeight * mi.emission);

@@ -234,6 +234,7 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
     std::vector<DevEmissiveTri> em;
     std::vector<float> flux;
     std::vector<uint32_t> instOff(d.instance_count, 0xffffffffu), active;
+    std::vector<float> emVerts, emNormals;  // light BVH input
     for (uint32_t i = 0; i < d.instance_count; i++) {
         const fpt_geometry_instance& in = d.instances[i];
         if (!emissiveMat[in.material_id]) continue;
@@ -261,6 +262,13 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
             if (in.flags & FPT_INSTANCE_FRONT_FACE_CW) { N[0] = -N[0]; N[1] = -N[1]; N[2] = -N[2]; }
             const float nn[3] = {N[0] / len, N[1] / len, N[2] / len};
             e.normal = encode_normal_2x16_host(nn);
+            for (int k = 0; k < 3; k++)
+                for (int a = 0; a < 3; a++) emVerts.push_back(P[k][a]);
+            // The builder sees the light collection's unpacked (decoded) normal
+            // (LightCollection::syncCPUData, LightCollection.cpp:680-689).
+            float dn[3];
+            decode_normal_2x16_host(e.normal, dn);
+            for (int a = 0; a < 3; a++) emNormals.push_back(dn[a]);
             e.materialID = in.material_id;
             e.lightIdx = i;
             // FinalizeIntegration.cs.slang:103-111.
@@ -272,6 +280,11 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
         }
     }
     build_alias_table(flux, s.aliasTable, s.aliasWeightSum);
+    try {
+        build_light_bvh(emVerts, emNormals, flux, s.lightBvh);
+    } catch (const std::exception& ex) {
+        return set_error(FPT_ERR_UNSUPPORTED, std::string("light BVH build failed: ") + ex.what());
+    }
     s.meshVertexCount.assign(d.instance_count, 0);
     s.meshTriCount.assign(d.instance_count, 0);
     s.meshEmissive.assign(d.instance_count, 0);
@@ -306,6 +319,17 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
     if ((st = upload(B, alias, ds.alias)) != FPT_OK) return st;
     if ((st = upload(B, instOff, ds.instEmissiveOffset)) != FPT_OK) return st;
     if ((st = upload(B, active, ds.activeTris)) != FPT_OK) return st;
+    {
+        const LightBVHNode* ln;
+        if ((st = upload(B, s.lightBvh.nodes, ln)) != FPT_OK) return st;
+        ds.lbvhNodes = reinterpret_cast<const uint4*>(ln);
+        if ((st = upload(B, s.lightBvh.triIndices, ds.lbvhTriIndices)) != FPT_OK) return st;
+        std::vector<uint2> masks(s.lightBvh.bitmasks.size());
+        for (size_t i = 0; i < masks.size(); i++)
+            masks[i] = make_uint2(uint32_t(s.lightBvh.bitmasks[i]), uint32_t(s.lightBvh.bitmasks[i] >> 32));
+        if ((st = upload(B, masks, ds.lbvhBitmasks)) != FPT_OK) return st;
+        ds.lbvhNodeCount = uint32_t(s.lightBvh.nodes.size());
+    }
     ds.emissiveCount = uint32_t(em.size());
     ds.activeCount = uint32_t(active.size());
     ds.invWeightSum = s.aliasWeightSum > 0.f ? 1.0f / s.aliasWeightSum : 0.f;
@@ -472,6 +496,18 @@ FPT_API fpt_status fpt_scene_get_bvh(const fpt_scene* scene, fpt_bvh_view* out) 
     out->tris = scene->bvh.tris.data();
     out->tri_count = uint32_t(scene->bvh.tris.size());
     for (int a = 0; a < 3; a++) { out->scene_lo[a] = scene->bvh.lo[a]; out->scene_hi[a] = scene->bvh.hi[a]; }
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_scene_get_light_bvh(const fpt_scene* scene, fpt_light_bvh_view* out) {
+    if (!scene || !out) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_get_light_bvh: null argument");
+    const LightBVH& b = scene->lightBvh;
+    out->nodes = b.nodes.empty() ? nullptr : b.nodes[0].w;
+    out->node_count = uint32_t(b.nodes.size());
+    out->triangle_indices = b.triIndices.data();
+    out->triangle_index_count = uint32_t(b.triIndices.size());
+    out->bitmasks = b.bitmasks.data();
+    out->bitmask_count = uint32_t(b.bitmasks.size());
     return FPT_OK;
 }
 

@@ -28,6 +28,7 @@ struct fpt_scene {
     fpt::BVH8 bvh;                    // host copy of the acceleration structure
     std::vector<uint32_t> aliasTable; // host copy of the alias table
     std::vector<fpt_material> materials;  // host copy of the material parameters
+    fpt::LightBVH lightBvh;               // host copy of the light BVH
     float aliasWeightSum = 0.f;
     fpt_scene_info info{};
     uint64_t version = 0;             // bumped by every change that can change a path (camera, materials, vertices)

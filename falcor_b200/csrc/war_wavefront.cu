@@ -491,6 +491,7 @@ cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBu
     w.originPdf = b.f4(0); w.dirV = b.f4(1); w.thpB = b.f4(2); w.L = b.f4(3);
     w.sg = reinterpret_cast<uint4*>(b.f4(4)); w.hit = reinterpret_cast<uint4*>(b.f4(5));
     w.sOrigin = b.f4(6); w.sDir = b.f4(7); w.sLr = b.f4(8);
+    w.nrm = nullptr;
     w.sampleL = b.sampleL;
     WarWave ww{};
     ww.capacity = b.capacity;

@@ -230,6 +230,7 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
     w.originPdf = b.f4(0); w.dirV = b.f4(1); w.thpB = b.f4(2); w.L = b.f4(3);
     w.sg = reinterpret_cast<uint4*>(b.f4(4)); w.hit = reinterpret_cast<uint4*>(b.f4(5));
     w.sOrigin = b.f4(6); w.sDir = b.f4(7); w.sLr = b.f4(8);
+    w.nrm = p.emissiveSampler == 1 ? b.f4(9) : nullptr;  // the LightBVH pdf needs the previous vertex's normal
     w.sampleL = b.sampleL;
     const uint32_t pixels = p.width * p.height;
     const uint32_t wavePixels = std::max<uint32_t>(1, std::min<uint32_t>(pixels, b.capacity / p.spp));
@@ -291,6 +292,7 @@ cudaError_t run_batch(const BatchDevice& bd, const std::vector<BatchWave>& waves
     w.originPdf = b.f4(0); w.dirV = b.f4(1); w.thpB = b.f4(2); w.L = b.f4(3);
     w.sg = reinterpret_cast<uint4*>(b.f4(4)); w.hit = reinterpret_cast<uint4*>(b.f4(5));
     w.sOrigin = b.f4(6); w.sDir = b.f4(7); w.sLr = b.f4(8);
+    w.nrm = nullptr;  // batched requests use the Power sampler
     w.sampleL = b.sampleL;
     DevScene none;
     std::memset(&none, 0, sizeof(none));

@@ -12,7 +12,7 @@ namespace fpt {
 // Structure-of-arrays path state for `capacity` paths in flight, allocated
 // once per pass and reused by every frame (scratch owned by the pass).
 struct WavefrontBuffers {
-    static constexpr int kFloat4Arrays = 9;
+    static constexpr int kFloat4Arrays = 10;
     void* base = nullptr;
     uint32_t capacity = 0;
     size_t bytesAllocated = 0;

@@ -48,6 +48,7 @@ struct SoA {
     float4* sOrigin;      // shadow origin, distance
     float4* sDir;         // shadow direction, -
     float4* sLr;          // shadow contribution thp * Lr
+    float4* nrm;          // oriented face normal of the last scatter vertex (LightBVH MIS), or null
     float* sampleL;       // per-path radiance (3 floats), wave slot order
 };
 
@@ -78,6 +79,10 @@ FPT_D void load_path(const SoA& w, uint32_t i, PathState<SG>& path) {
     path.hit.baryY = __uint_as_float(h.w);
     path.hit.valid = true;
     path.normal = f3(0.f);
+    if (w.nrm) {
+        const float4 n = w.nrm[i];
+        path.normal = make_float3(n.x, n.y, n.z);
+    }
     path.shadowPending = false;
 }
 
@@ -88,6 +93,7 @@ FPT_D void store_path(const SoA& w, uint32_t i, const PathState<SG>& path) {
     w.thpB[i] = make_float4(path.thp.x, path.thp.y, path.thp.z, __uint_as_float(path.bounces));
     w.L[i] = make_float4(path.L.x, path.L.y, path.L.z, 0.f);
     store_sg(w.sg[i], path.sg);
+    if (w.nrm) w.nrm[i] = make_float4(path.normal.x, path.normal.y, path.normal.z, 0.f);
 }
 
 // Warp-aggregated push of `item` onto queue q (count at *cnt).

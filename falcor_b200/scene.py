@@ -230,6 +230,16 @@ class Scene:
         tris = np.ctypeslib.as_array(C.cast(v.tris, C.POINTER(C.c_uint8)), shape=(v.tri_count * 48,)).copy()
         return nodes.reshape(-1, 80), tris.reshape(-1, 48)
 
+    def light_bvh(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Host copies of the light BVH: nodes [n, 8] uint32 (compressed PackedNode),
+        leaf triangle indices, per emissive triangle bit paths (uint64)."""
+        v = _ffi.fpt_light_bvh_view()
+        check(lib().fpt_scene_get_light_bvh(self._h, C.byref(v)))
+        nodes = np.ctypeslib.as_array(v.nodes, shape=(v.node_count * 8,)).copy() if v.node_count else np.zeros(0, np.uint32)
+        idx = np.ctypeslib.as_array(v.triangle_indices, shape=(v.triangle_index_count,)).copy() if v.triangle_index_count else np.zeros(0, np.uint32)
+        masks = np.ctypeslib.as_array(v.bitmasks, shape=(v.bitmask_count,)).copy() if v.bitmask_count else np.zeros(0, np.uint64)
+        return nodes.reshape(-1, 8), idx, masks
+
     def alias_table(self) -> tuple[np.ndarray, float]:
         n = self.info.emissive_triangle_count
         out = np.zeros(2 * max(n, 1), dtype=np.uint32)

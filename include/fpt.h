@@ -245,6 +245,20 @@ FPT_API fpt_status fpt_scene_get_material_params(const fpt_scene* scene, const u
 FPT_API fpt_status fpt_scene_set_material_params(fpt_scene* scene, const uint32_t* ids, uint32_t count, const float* params);
 /* Host view of the scene's BVH (valid until the scene is destroyed). */
 FPT_API fpt_status fpt_scene_get_bvh(const fpt_scene* scene, fpt_bvh_view* out);
+/* Host view of the light BVH built for the LightBVH emissive sampler
+ * (LightBVHBuilder::build, LightBVHBuilder.cpp:228-309): node_count
+ * compressed 32-byte PackedNodes (8 uint32 each), the leaves' emissive triangle
+ * indices, and per emissive triangle the 64-bit path to its leaf (all ones:
+ * left out for zero flux).  Valid until the scene is destroyed. */
+typedef struct fpt_light_bvh_view {
+    const uint32_t* nodes;
+    uint32_t node_count;
+    const uint32_t* triangle_indices;
+    uint32_t triangle_index_count;
+    const uint64_t* bitmasks;
+    uint32_t bitmask_count;
+} fpt_light_bvh_view;
+FPT_API fpt_status fpt_scene_get_light_bvh(const fpt_scene* scene, fpt_light_bvh_view* out);
 /* Scene::getMesh(meshID).vertexCount / getTriangleCount() (Scene.h): mesh =
  * geometry instance of the scene description. */
 FPT_API fpt_status fpt_scene_get_mesh_info(const fpt_scene* scene, uint32_t mesh_id, uint32_t* vertex_count,
@@ -319,7 +333,7 @@ FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void
  * memory is reserved for its own pool, or a frame loop that must not take the
  * device-wide synchronisation of cudaMalloc/cudaFree -- it renders the same
  * frame as fpt_pass_execute on a PathTracer pass, with all scratch (path
- * state, queues, counters; 2.63 MiB, 16384 paths in flight per wave) in one
+ * state, queues, counters; 2.88 MiB, 16384 paths in flight per wave) in one
  * static device array that every GPU loading this library holds until exit.
  * Limits: PathTracer passes only, frames up to 4096 x 4096 (larger sizes are
  * rejected with FPT_ERR_INVALID_ARG).  The first call on a device looks up the

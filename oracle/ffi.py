@@ -69,6 +69,12 @@ def lib() -> C.CDLL:
         l.orc_scene_destroy.argtypes = [_P]
         l.orc_scene_get_info.argtypes = [_P, C.POINTER(SceneInfo)]
         l.orc_scene_get_lights.argtypes = [_P, _P, _P, _P]
+        l.orc_scene_light_bvh_sizes.argtypes = [_P, _P, _P, _P]
+        l.orc_scene_get_light_bvh.argtypes = [_P, _P, _P, _P]
+        l.orc_lbvh_selection_pdf.restype = C.c_float
+        l.orc_lbvh_selection_pdf.argtypes = [_P, _P, _P, C.c_int, u32]
+        l.orc_lbvh_select.restype = C.c_int
+        l.orc_lbvh_select.argtypes = [_P, _P, _P, C.c_int, C.c_float, _P, _P]
         l.orc_scene_get_importance.argtypes = [_P, u32, _P]
         l.orc_vbuffer.argtypes = [_P, u32, u32, _P, u32]
         l.orc_trace_closest.argtypes = [_P, u32, _P, _P, _P, _P, _P, _P, C.c_int]
@@ -192,6 +198,28 @@ class OracleScene:
                                tt.shape[1] if tt is not None else 0, eps, ptr(g) if g is not None else None, ptr(color),
                                ptr(grads), ptr(pert) if pert is not None else None, threads, x0, y0, x1, y1, C.byref(rays))
         return color, (grads[:K] if mode == 1 else None), pert, int(rays.value), dt
+
+    def light_bvh(self):
+        """(nodes [n, 8] uint32, leaf triangle indices, per-triangle bit paths uint64)."""
+        a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        lib().orc_scene_light_bvh_sizes(self._h, C.byref(a), C.byref(b), C.byref(c))
+        nodes = np.zeros(8 * a.value, dtype=np.uint32)
+        tris = np.zeros(b.value, dtype=np.uint32)
+        masks = np.zeros(c.value, dtype=np.uint64)
+        lib().orc_scene_get_light_bvh(self._h, ptr(nodes), ptr(tris), ptr(masks))
+        return nodes.reshape(-1, 8), tris, masks
+
+    def lbvh_selection_pdf(self, pos, normal, upper, tri) -> float:
+        p = np.ascontiguousarray(pos, np.float32)
+        n = np.ascontiguousarray(normal, np.float32)
+        return float(lib().orc_lbvh_selection_pdf(self._h, ptr(p), ptr(n), int(upper), int(tri)))
+
+    def lbvh_select(self, pos, normal, upper, u):
+        p = np.ascontiguousarray(pos, np.float32)
+        n = np.ascontiguousarray(normal, np.float32)
+        t, pdf = C.c_uint32(), C.c_float()
+        ok = lib().orc_lbvh_select(self._h, ptr(p), ptr(n), int(upper), float(u), C.byref(t), C.byref(pdf))
+        return (int(t.value), float(pdf.value)) if ok else None
 
     def lights(self):
         n = self.info.emissive_count

@@ -54,6 +54,26 @@ void orc_scene_get_info(const void* sp, orc_scene_info* out) {
     out->imp_base_mip = s.impBaseMip;
 }
 // Alias table (2 uints per emissive triangle) and per-triangle flux.
+// Light BVH of the oracle scene: sizes, then copies into caller arrays.
+void orc_scene_light_bvh_sizes(const void* sp, uint32_t* nodes, uint32_t* tris, uint32_t* masks) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    *nodes = uint32_t(s.lightBvh.nodes.size() / 8);
+    *tris = uint32_t(s.lightBvh.triIndices.size());
+    *masks = uint32_t(s.lightBvh.bitmasks.size());
+}
+void orc_scene_get_light_bvh(const void* sp, uint32_t* nodes, uint32_t* tris, uint64_t* masks) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    std::copy(s.lightBvh.nodes.begin(), s.lightBvh.nodes.end(), nodes);
+    std::copy(s.lightBvh.triIndices.begin(), s.lightBvh.triIndices.end(), tris);
+    std::copy(s.lightBvh.bitmasks.begin(), s.lightBvh.bitmasks.end(), masks);
+}
+float orc_lbvh_selection_pdf(const void* sp, const float* posW, const float* n, int upper, uint32_t tri) {
+    return lbvh_selection_pdf_f(*static_cast<const Scene*>(sp), posW, n, upper != 0, tri);
+}
+int orc_lbvh_select(const void* sp, const float* posW, const float* n, int upper, float u, uint32_t* tri, float* pdf) {
+    return lbvh_select_f(*static_cast<const Scene*>(sp), posW, n, upper != 0, u, tri, pdf) ? 1 : 0;
+}
+
 void orc_scene_get_lights(const void* sp, uint32_t* alias, float* flux, float* area) {
     const Scene& s = *static_cast<const Scene*>(sp);
     for (size_t i = 0; i < s.emissive.size(); i++) {

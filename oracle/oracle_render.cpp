@@ -303,10 +303,119 @@ static R eval_triangle_pdf(const Scene& s, V3<R> posW, uint32_t tri, V3<R> hitPo
     return distSqr / denom;
 }
 
-// EmissiveUniformSampler.sampleLight (EmissiveUniformSampler.slang:55-76) and
+// LightBVHSampler (Rendering/Lights/LightBVHSampler.slang:70-534), default
+// options: bounding cone, lighting cone, node flux, uniform leaf selection,
+// SolidAngleBoundMethod::Sphere (GeometryHelpers.slang:222-240).
+template <class R> struct LbvhNodeR { uint32_t w0; V3<R> origin, extent, coneDir; R cosCone, flux; };
+template <class R> static LbvhNodeR<R> lbvh_node(const Scene& s, uint32_t i) {
+    const uint32_t* w = &s.lightBvh.nodes[8 * size_t(i)];
+    LbvhNodeR<R> n;
+    n.w0 = w[0];
+    float o[3], fl;
+    std::memcpy(o, &w[1], 12);
+    std::memcpy(&fl, &w[7], 4);
+    n.origin = V3<R>(R(o[0]), R(o[1]), R(o[2]));
+    n.extent = V3<R>(R(f16tof32(w[4] & 0xffffu)), R(f16tof32(w[4] >> 16)), R(f16tof32(w[5] & 0xffffu)));
+    n.cosCone = R(float(w[5] >> 16) * (1.f / 32767.f) - 1.f);
+    const V3<float> cd = decode_normal2x16(w[6]);
+    n.coneDir = V3<R>(R(cd.x), R(cd.y), R(cd.z));
+    n.flux = R(fl);
+    return n;
+}
+template <class R> static R cos_sub_clamped(R sinA, R cosA, R sinB, R cosB) { return cosA > cosB ? R(1) : cosA * cosB + sinA * sinB; }
+template <class R> static R sin_sub_clamped(R sinA, R cosA, R sinB, R cosB) { return cosA > cosB ? R(0) : sinA * cosB - cosA * sinB; }
+// computeImportance (LightBVHSampler.slang:206-259).
+template <class R> static R lbvh_importance(const Scene& s, V3<R> posW, V3<R> normalW, bool upper, uint32_t i) {
+    const LbvhNodeR<R> n = lbvh_node<R>(s, i);
+    R distance = length(n.origin - posW);
+    // boundCosineTerm with the bounding sphere of the box.
+    const R sqrRadius = dot(n.extent, n.extent);
+    const V3<R> c = n.origin - posW;
+    const R d2 = dot(c, c);
+    R sinCone, cosCone;
+    if (d2 < sqrRadius) { sinCone = R(0); cosCone = R(-1); }
+    else { R s2 = sqrRadius / d2; cosCone = std::sqrt(R(1) - s2); sinCone = std::sqrt(s2); }
+    const V3<R> L = normalize(n.origin - posW);
+    R cosL = dot(normalW, L);
+    cosL = cosL < R(-1) ? R(-1) : (cosL > R(1) ? R(1) : cosL);
+    const R sinL = std::sqrt(R(1) - cosL * cosL);
+    R NdotL = cos_sub_clamped(sinL, cosL, sinCone, cosCone);
+    NdotL = NdotL < R(0) ? R(0) : (NdotL > R(1) ? R(1) : NdotL);
+    if (!upper) NdotL = R(1);
+    R orient = R(1);
+    const V3<R> toBox = (n.origin - posW) / distance;
+    if (n.cosCone != R(-1) && n.cosCone > R(0)) {
+        const R sinConeAngle = std::sqrt(vmax(R(0), R(1) - n.cosCone * n.cosCone));
+        const R cosT = dot(n.coneDir, -toBox);
+        const R sinT = std::sqrt(vmax(R(0), R(1) - cosT * cosT));
+        const R sinB = std::sqrt(vmax(R(0), R(1) - cosCone * cosCone));
+        const R c0 = cos_sub_clamped(sinT, cosT, sinConeAngle, n.cosCone);
+        const R s0 = sin_sub_clamped(sinT, cosT, sinConeAngle, n.cosCone);
+        orient = vmax(R(0), cos_sub_clamped(s0, c0, sinB, cosCone));
+    }
+    const R half = vmax(n.extent.x, vmax(n.extent.y, n.extent.z));
+    distance = vmax(half, distance);
+    return (n.flux * NdotL) * orient / (distance * distance);
+}
+// traverseTree + pickTriangle (uniform) (LightBVHSampler.slang:262-392).
+template <class R> static bool lbvh_select(const Scene& s, V3<R> posW, V3<R> normalW, bool upper, R u, R& pdf, uint32_t& tri) {
+    pdf = R(1);
+    uint32_t node = 0;
+    uint32_t w0 = s.lightBvh.nodes[0];
+    while (!(w0 >> 31)) {
+        const uint32_t left = node + 1, right = w0;
+        const R il = lbvh_importance<R>(s, posW, normalW, upper, left), ir = lbvh_importance<R>(s, posW, normalW, upper, right);
+        const R total = il + ir;
+        if (total == R(0)) return false;
+        const R pLeft = il / total, pRight = R(1) - pLeft;
+        if (u < pLeft) { u = u / pLeft; pdf *= pLeft; node = left; }
+        else { u = (u - pLeft) / pRight; pdf *= pRight; node = right; }
+        w0 = s.lightBvh.nodes[8 * size_t(node)];
+    }
+    const uint32_t count = (w0 >> 27) & 15u, offset = w0 & ((1u << 27) - 1u);
+    const uint32_t idx = std::min(uint32_t(u * R(float(count))), count - 1);
+    tri = s.lightBvh.triIndices[offset + idx];
+    pdf *= R(1) / R(float(count));
+    return true;
+}
+// evalTriangleSelectionPdf (LightBVHSampler.slang:95-125, 418-458).
+template <class R> static R lbvh_selection_pdf(const Scene& s, V3<R> posW, V3<R> normalW, bool upper, uint32_t tri) {
+    uint64_t mask = s.lightBvh.bitmasks[tri];
+    R pdf = R(1);
+    uint32_t node = 0;
+    uint32_t w0 = s.lightBvh.nodes[0];
+    while (!(w0 >> 31)) {
+        const uint32_t left = node + 1, right = w0;
+        const R il = lbvh_importance<R>(s, posW, normalW, upper, left), ir = lbvh_importance<R>(s, posW, normalW, upper, right);
+        const R total = il + ir;
+        if (total == R(0)) return R(0);
+        const R pLeft = il / total, pRight = R(1) - pLeft;
+        if ((mask & 1ull) == 0) { pdf *= pLeft; node = left; }
+        else { pdf *= pRight; node = right; }
+        mask >>= 1;
+        w0 = s.lightBvh.nodes[8 * size_t(node)];
+    }
+    const uint32_t count = (w0 >> 27) & 15u;
+    return pdf * (R(1) / R(float(count)));
+}
+
+// EmissiveUniformSampler.sampleLight (EmissiveUniformSampler.slang:55-76),
+// LightBVHSampler.sampleLight (LightBVHSampler.slang:70-90) and
 // EmissivePowerSampler.sampleLight (EmissivePowerSampler.slang:61-91).
 template <class R, class SG>
-static bool emissive_sample_light(const Scene& s, int samplerType, V3<R> posW, SG& sg, TriLightSample<R>& ls) {
+static bool emissive_sample_light(const Scene& s, int samplerType, V3<R> posW, SG& sg, TriLightSample<R>& ls,
+                                  V3<R> normalW = V3<R>(R(0)), bool upperHemisphere = false) {
+    if (samplerType == 1) {
+        if (s.emissive.empty() || s.lightBvh.nodes.empty()) return false;
+        R uLight = next1D<R>(sg);
+        R selPdf;
+        uint32_t tri;
+        if (!lbvh_select<R>(s, posW, normalW, upperHemisphere, uLight, selPdf, tri)) return false;
+        V2<R> u = next2D<R>(sg);
+        if (!sample_triangle_light(s, posW, tri, u, ls)) return false;
+        ls.pdf *= selPdf;
+        return true;
+    }
     if (samplerType == 0) {
         if (s.activeTriangles.empty()) return false;
         R uLight = next1D<R>(sg);
@@ -335,10 +444,15 @@ static bool emissive_sample_light(const Scene& s, int samplerType, V3<R> posW, S
     return true;
 }
 template <class R>
-static R emissive_eval_pdf(const Scene& s, int samplerType, V3<R> posW, uint32_t tri, V3<R> hitPos, V3<R> hitN) {
+static R emissive_eval_pdf(const Scene& s, int samplerType, V3<R> posW, uint32_t tri, V3<R> hitPos, V3<R> hitN,
+                           V3<R> normalW = V3<R>(R(0)), bool upperHemisphere = false) {
     if (tri == 0xffffffffu) return R(0);
     R sel;
-    if (samplerType == 0) {
+    if (samplerType == 1) {
+        if (s.lightBvh.nodes.empty()) return R(0);
+        sel = lbvh_selection_pdf<R>(s, posW, normalW, upperHemisphere, tri);
+        if (sel == R(0)) return R(0);
+    } else if (samplerType == 0) {
         uint32_t n = uint32_t(s.activeTriangles.size());
         sel = n > 0 ? R(1) / R(float(n)) : R(0);
     } else {
@@ -564,7 +678,7 @@ static bool generate_light_sample(const Scene& s, const PathTracerParams& p, V3<
     }
     if (useEmissive && lightType == 1) {
         TriLightSample<R> tls;
-        if (emissive_sample_light<R>(s, p.emissiveSampler, vpos, sg, tls)) {
+        if (emissive_sample_light<R>(s, p.emissiveSampler, vpos, sg, tls, orientedN, upper && !lower)) {
             ls.Li = tls.pdf > R(0) ? tls.Le / tls.pdf : V3<R>(R(0));
             ls.pdf = tls.pdf;
             V3<R> lightPos = compute_ray_origin(tls.posW, tls.normalW);
@@ -599,9 +713,9 @@ static void pt_handle_hit(const Scene& s, const PathTracerParams& p, PTPath<R, S
         if (useEmissive && p.useNEE && p.useMIS && !isPrimaryHit && path.isLightSampled() && isLightSamplable) {
             uint32_t triIdx = s.emissiveIndex(path.hit.instanceID, path.hit.primitiveIndex);
             bool upperHemisphere = path.has(PF_LIGHT_UPPER) && !path.has(PF_LIGHT_LOWER);
-            (void)upperHemisphere;
             R emissiveSel = (useEnv && useEmissive) ? R(0.5f) : R(1);
-            R lightPdf = emissiveSel * emissive_eval_pdf<R>(s, p.emissiveSampler, path.origin, triIdx, sd.posW, sd.orientedFaceN());
+            R lightPdf = emissiveSel * emissive_eval_pdf<R>(s, p.emissiveSampler, path.origin, triIdx, sd.posW, sd.orientedFaceN(),
+                                                            path.normal, upperHemisphere);
             misWeight = eval_mis<R>(p, R(1), path.pdf, R(1), lightPdf);
         }
         path.L += path.thp * (misWeight * emission);
@@ -752,6 +866,15 @@ void path_tracer_pixel(const Scene& s, const PathTracerParams& p, uint32_t x, ui
     if (spp == 1) invSpp = R(1);
     V3<R> out = spp == 1 ? color : color * invSpp;
     colorOut[0] = float(out.x); colorOut[1] = float(out.y); colorOut[2] = float(out.z); colorOut[3] = 1.f;
+}
+
+float lbvh_selection_pdf_f(const Scene& s, const float posW[3], const float n[3], bool upper, uint32_t tri) {
+    if (s.lightBvh.nodes.empty() || tri >= s.lightBvh.bitmasks.size()) return 0.f;
+    return lbvh_selection_pdf<float>(s, V3<float>(posW[0], posW[1], posW[2]), V3<float>(n[0], n[1], n[2]), upper, tri);
+}
+bool lbvh_select_f(const Scene& s, const float posW[3], const float n[3], bool upper, float u, uint32_t* tri, float* pdf) {
+    if (s.lightBvh.nodes.empty()) return false;
+    return lbvh_select<float>(s, V3<float>(posW[0], posW[1], posW[2]), V3<float>(n[0], n[1], n[2]), upper, u, *pdf, *tri);
 }
 
 #include "oracle_wardiff.inl"

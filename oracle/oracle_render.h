@@ -76,6 +76,11 @@ struct WarCounters { uint64_t rays = 0, hits = 0; };
 void wardiff_pixel(const Scene& s, const WarDiffParams& p, const WarSeeds& seeds, int mode, uint32_t x, uint32_t y,
                    const float* dLdI, float* colorOut, double* gradAcc, double* pertOut, WarCounters* wc);
 
+// LightBVHSampler selection pdf of emissive triangle `tri` and one traversal
+// sample (tri, pdf) from shading point posW with normal n (FP32).
+float lbvh_selection_pdf_f(const Scene& s, const float posW[3], const float n[3], bool upper, uint32_t tri);
+bool lbvh_select_f(const Scene& s, const float posW[3], const float n[3], bool upper, float u, uint32_t* tri, float* pdf);
+
 void pack_hit(const fpt_hitinfo_bits& b, const Hit& h, uint32_t out[4]);
 Hit unpack_hit(const fpt_hitinfo_bits& b, const uint32_t in[4]);
 

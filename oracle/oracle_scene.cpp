@@ -180,7 +180,8 @@ void Scene::buildLights(uint32_t) {
             V3<float> N = cross(e0, e1);
             t.area = 0.5f * length(N);
             if (instances[i].flags & FPT_INSTANCE_FRONT_FACE_CW) N = -N;
-            t.normal = decode_normal2x16(encode_normal2x16(normalize(N)));
+            t.normalEnc = encode_normal2x16(normalize(N));
+            t.normal = decode_normal2x16(t.normalEnc);
             t.materialID = instances[i].material_id;
             V3<float> avg(m.emissive[0], m.emissive[1], m.emissive[2]);
             t.averageRadiance = avg * m.emissiveFactor;
@@ -195,6 +196,20 @@ void Scene::buildLights(uint32_t) {
         w[k] = emissive[k].flux;
     }
     generate_alias_table(w, aliasTable, aliasWeightSum);
+    // LightBVHBuilder::build on the light collection's CPU copy, whose normals are
+    // the unpacked octahedral ones decoded by the host code (normalize = v * rsqrt).
+    std::vector<float> lv, ln, lf;
+    for (const EmissiveTri& t : emissive) {
+        for (int k = 0; k < 3; k++) { lv.push_back(t.posW[k].x); lv.push_back(t.posW[k].y); lv.push_back(t.posW[k].z); }
+        const V2<float> o = unpack_snorm2x16(t.normalEnc);
+        V3<float> n(o.x, o.y, 1.f - std::fabs(o.x) - std::fabs(o.y));
+        if (n.z < 0.f) { V2<float> wv = oct_wrap(V2<float>(n.x, n.y)); n.x = wv.x; n.y = wv.y; }
+        n = n * (1.f / std::sqrt(dot(n, n)));
+        ln.push_back(n.x); ln.push_back(n.y); ln.push_back(n.z);
+        lf.push_back(t.flux);
+    }
+    build_light_bvh_oracle(lv, ln, lf, [](float v) { return f32tof16_host(v); },
+                           [](const float* d) { return encode_normal2x16(V3<float>(d[0], d[1], d[2])); }, lightBvh);
 }
 
 void Scene::buildEnv(const fpt_envmap_desc* env) {

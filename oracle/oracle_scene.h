@@ -9,6 +9,7 @@
 #include <vector>
 #include <cstdint>
 #include "oracle_math.h"
+#include "oracle_lightbvh.h"
 #include "../include/fpt.h"
 
 namespace orc {
@@ -47,6 +48,7 @@ struct EmissiveTri {
     V3<float> posW[3];
     V2<float> uv[3];     // fp16-quantised
     V3<float> normal;    // decoded from the 2x16 octahedral encoding
+    uint32_t normalEnc;  // the 2x16 octahedral encoding
     float area;
     uint32_t materialID;
     float flux;          // FinalizeIntegration.cs.slang:103-111
@@ -84,6 +86,7 @@ public:
     std::vector<uint32_t> instanceEmissiveOffset;   // perMeshInstanceOffset, 0xffffffff if none
     std::vector<uint32_t> activeTriangles;
     std::vector<uint32_t> aliasTable;               // 2 uints per emissive triangle
+    LightBvhOracle lightBvh;                        // LightBVH sampler data
     float aliasWeightSum = 0.f;
 
     // environment
