@@ -38,6 +38,39 @@ __global__ void __launch_bounds__(kVBufferBlock) vbuffer_kernel(DevScene s, Fram
     HitRec h;
     trace_bvh<false>(s, load3(s.camera.posW), dir, tMin, tMax, h, stack, kVBufferBlock);
     p.vbufferOut[idx] = pack_hit(s.bits, h);
+    if (p.viewWOut) p.viewWOut[idx] = make_float4(-dir.x, -dir.y, -dir.z, 0.f);  // writeAux
+    if (!p.depthOut && !p.mvecOut && !p.maskOut) return;
+    float depth = 1.f, mask = 0.f;
+    float2 mvec = make_float2(0.f, 0.f);
+    if (h.valid) {
+        // writeHit: NDC depth of the perspective projection without jitter
+        // (right-handed, depth 0 at nearZ and 1 at farZ), and the motion vector
+        // from the previous camera's projection of the hit (static geometry),
+        // with the jitter added back.
+        const DevInstance inst = s.instances[h.instanceID];
+        const uint32_t* ip = s.indices + inst.ibOffset + h.primIndex * 3;
+        float3 p0, p1, p2, n;
+        unpack_vertex(load_vertex(s.vertices, __ldg(ip) + inst.vbOffset), p0, n);
+        unpack_vertex(load_vertex(s.vertices, __ldg(ip + 1) + inst.vbOffset), p1, n);
+        unpack_vertex(load_vertex(s.vertices, __ldg(ip + 2) + inst.vbOffset), p2, n);
+        float3 posW = p0 * (1.f - h.baryX - h.baryY);
+        posW += p1 * h.baryX;
+        posW += p2 * h.baryY;
+        const fpt_camera_data& c = s.camera;
+        const float d = dot(posW - load3(c.posW), normalize(load3(c.cameraW)));
+        depth = (c.farZ * (d - c.nearZ)) / (d * (c.farZ - c.nearZ));
+        const fpt_camera_data& q = p.prevCamera;
+        const float3 r = posW - load3(q.posW), U = load3(q.cameraU), V = load3(q.cameraV), Wq = load3(q.cameraW);
+        const float t = dot(r, Wq) / dot(Wq, Wq);
+        const float nx = dot(r, U) / (dot(U, U) * t), ny = dot(r, V) / (dot(V, V) * t);
+        const float2 prevCrd = make_float2(nx * 0.5f + 0.5f, ny * -0.5f + 0.5f);
+        mvec = make_float2(prevCrd.x - (float(x) + 0.5f) / float(p.width) + c.jitterX,
+                           prevCrd.y - (float(y) + 0.5f) / float(p.height) - c.jitterY);
+        mask = 1.f;
+    }
+    if (p.depthOut) p.depthOut[idx] = depth;
+    if (p.mvecOut) p.mvecOut[idx] = mvec;
+    if (p.maskOut) p.maskOut[idx] = mask;
 }
 
 // ---------------------------------------------------------------------------

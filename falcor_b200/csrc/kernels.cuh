@@ -22,6 +22,13 @@ struct FrameParams {
     uint32_t* pathLength;      // optional per-pixel path length
     float* sampleColor;        // optional per-sample radiance (3 floats)
     uint4* vbufferOut;         // VBufferRT output
+    // VBufferRT optional outputs (VBufferRT.slang:69-143) and the camera of the
+    // previous frame for the motion vectors.
+    float* depthOut;
+    float2* mvecOut;
+    float4* viewWOut;
+    float* maskOut;
+    fpt_camera_data prevCamera;
     // MinimalPathTracer
     uint32_t maxBounces, computeDirect, useImportanceSampling;
     // PathTracer

@@ -331,6 +331,7 @@ FPT_API fpt_status fpt_scene_set_mesh_vertices(fpt_scene* scene, uint32_t mesh_i
             scene->bvh.hi[a] = box[3 + a];
         }
     scene->version++;
+    scene->resetVersion++;
     if (dummy & kRefitBadPosition)
         return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_mesh_vertices: a non-finite or out-of-range (|x| > 1e15) position");
     if (dummy & kRefitQuantisation) return set_error(FPT_ERR_DEVICE, "fpt_scene_set_mesh_vertices: BVH quantisation failed");

@@ -5,6 +5,7 @@
 //   PathTracer         RenderPasses/PathTracer/PathTracer.cpp:155-415,1329-1598
 //   VBufferRT          RenderPasses/GBuffer/VBuffer/VBufferRT.cpp
 //   WARDiffPathTracer  RenderPasses/WARDiffPathTracer/WARDiffPathTracer.cpp:53-144 (adjoint.cu)
+//   AccumulatePass, ToneMapper, ColorMapPass, RenderToViewportPass (image_passes.cu)
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -13,6 +14,7 @@
 #include <sstream>
 #include <string>
 
+#include "image_passes.h"
 #include "kernels.cuh"
 #include "passes.h"
 #include "scene_device.h"
@@ -45,7 +47,31 @@ const ChannelSpec kPathTracerChannels[] = {
 };
 const ChannelSpec kVBufferChannels[] = {
     {"vbuffer", "Visibility buffer in packed format", false, false, "PackedHitInfo"},
+    {"depth", "Depth buffer (NDC)", false, true, "R32Float"},
+    {"mvec", "Motion vector", false, true, "RG32Float"},
+    {"viewW", "View direction in world space", false, true, "RGBA32Float"},
+    {"mask", "Mask", false, true, "R32Float"},
 };
+const ChannelSpec kAccumulateChannels[] = {
+    {"input", "Input data to be temporally accumulated", true, false, "RGBA32Float"},
+    {"output", "Output data that is temporally accumulated", false, false, "RGBA32Float"},
+};
+const ChannelSpec kToneMapperChannels[] = {
+    {"src", "Source texture", true, false, "RGBA32Float"},
+    {"dst", "Tone-mapped output texture", false, false, "RGBA32Float"},
+};
+const ChannelSpec kColorMapChannels[] = {
+    {"input", "Input image", true, false, "RGBA32Float"},
+    {"output", "Output image", false, false, "RGBA32Float"},
+};
+const ChannelSpec kViewportChannels[] = {
+    {"input", "input", true, false, "RGBA32Float"},
+    {"output", "output", false, false, "RGBA32Float"},
+};
+
+bool is_image_pass(const std::string& t) {
+    return t == "AccumulatePass" || t == "ToneMapper" || t == "ColorMapPass" || t == "RenderToViewportPass";
+}
 const ChannelSpec kWARDiffChannels[] = {
     {"color", "Output color (linear)", false, false, "RGBA32Float"},
     {"dColor", "Output gradient of color w.r.t. the debug variable", false, true, "RGBA32Float"},
@@ -97,8 +123,52 @@ void set_defaults(fpt_pass& p) {
         // CUDA-event timing of each wavefront kernel category (fpt_pass_get_kernel_times).
         d["profileKernels"] = PropValue::num(0);
     } else if (p.type == "VBufferRT") {
+        // GBufferBase.h:96-98.
         d["samplePattern"] = PropValue::str("Center");
+        d["sampleCount"] = PropValue::num(16);
         d["useAlphaTest"] = PropValue::num(1);
+        // Accepted for graph-script compatibility; the traversal is always the
+        // build's own, never culls and has no depth of field.
+        d["outputSize"] = PropValue::str("Default");
+        d["useTraceRayInline"] = PropValue::num(0);
+        d["useDOF"] = PropValue::num(1);
+        d["adjustShadingNormals"] = PropValue::num(0);
+        d["forceCullMode"] = PropValue::num(0);
+        d["cull"] = PropValue::str("Back");
+    } else if (p.type == "AccumulatePass") {
+        // AccumulatePass.h:135-150.
+        d["enabled"] = PropValue::num(1);
+        d["autoReset"] = PropValue::num(1);
+        d["precisionMode"] = PropValue::str("Single");
+        d["maxFrameCount"] = PropValue::num(0);
+        d["overflowMode"] = PropValue::str("Stop");
+        d["outputSize"] = PropValue::str("Default");
+        d["outputFormat"] = PropValue::str("Unknown");
+    } else if (p.type == "ToneMapper") {
+        // ToneMapper.h:121-169.
+        d["outputSize"] = PropValue::str("Default");
+        d["outputFormat"] = PropValue::str("Unknown");
+        d["useSceneMetadata"] = PropValue::num(1);
+        d["exposureCompensation"] = PropValue::num(0);
+        d["autoExposure"] = PropValue::num(0);
+        d["exposureValue"] = PropValue::num(0);
+        d["filmSpeed"] = PropValue::num(100);
+        d["whiteBalance"] = PropValue::num(0);
+        d["whitePoint"] = PropValue::num(6500);
+        d["operator"] = PropValue::str("Aces");
+        d["clamp"] = PropValue::num(1);
+        d["whiteMaxLuminance"] = PropValue::num(1);
+        d["whiteScale"] = PropValue::num(11.199999809265137);
+        d["fNumber"] = PropValue::num(1);
+        d["shutter"] = PropValue::num(1);
+        d["exposureMode"] = PropValue::str("AperturePriority");
+    } else if (p.type == "ColorMapPass") {
+        // ColorMapPass.h:52-56.
+        d["colorMap"] = PropValue::str("Jet");
+        d["channel"] = PropValue::num(0);
+        d["autoRange"] = PropValue::num(1);
+        d["minValue"] = PropValue::num(0);
+        d["maxValue"] = PropValue::num(1);
     } else if (p.type == "WARDiffPathTracer") {
         d["samplesPerPixel"] = PropValue::num(1);
         d["maxBounces"] = PropValue::num(0);
@@ -133,6 +203,52 @@ const std::map<std::string, int> kMISHeuristics = {{"Balance", 0}, {"PowerTwo", 
 const std::map<std::string, int> kEmissiveSamplers = {{"Uniform", 0}, {"LightBVH", 1}, {"Power", 2}};
 const std::map<std::string, int> kColorFormats = {{"RGBA32F", 0}, {"LogLuvHDR", 1}};
 const std::map<std::string, int> kDiffModes = {{"Primal", 0}, {"BackwardDiff", 1}, {"ForwardDiffDebug", 2}, {"BackwardDiffDebug", 3}};
+const std::map<std::string, int> kSamplePatterns = {{"Center", 0}, {"DirectX", 1}, {"Halton", 2}, {"Stratified", 3}};
+
+// Enum-valued string properties: the accepted names (and integer values).
+const std::map<std::string, int>* enum_map(const std::string& k) {
+    if (k == "misHeuristic") return &kMISHeuristics;
+    if (k == "emissiveSampler") return &kEmissiveSamplers;
+    if (k == "colorFormat") return &kColorFormats;
+    if (k == "diffMode") return &kDiffModes;
+    if (k == "samplePattern") return &kSamplePatterns;
+    if (k == "operator") return &kToneMapOperators;
+    if (k == "exposureMode") return &kToneMapExposureModes;
+    if (k == "colorMap") return &kColorMaps;
+    if (k == "precisionMode") return &kPrecisionModes;
+    if (k == "overflowMode") return &kOverflowModes;
+    return nullptr;
+}
+
+// ToneMapper setters (ToneMapper.cpp:405-510): clamping and the exposure
+// value tied to the shutter and f-number.  Float arithmetic as in the reference.
+void tone_mapper_set(fpt_pass& p, const std::string& k, double value) {
+    const float kShutterMin = 0.1f, kShutterMax = 10000.f, kFNumberMin = 0.1f, kFNumberMax = 100.f;
+    const float kEVMin = std::log2(kShutterMin * kFNumberMin * kFNumberMin), kEVMax = std::log2(kShutterMax * kFNumberMax * kFNumberMax);
+    auto& d = p.props;
+    float v = float(value);
+    auto updateEV = [&]() {
+        const float sh = float(d["shutter"].n), fN = float(d["fNumber"].n);
+        d["exposureValue"].n = std::log2(sh * fN * fN);
+    };
+    if (k == "exposureCompensation") d[k].n = std::clamp(v, -12.f, 12.f);
+    else if (k == "filmSpeed") d[k].n = std::clamp(v, 1.f, 6400.f);
+    else if (k == "whitePoint") d[k].n = std::clamp(v, 1905.f, 25000.f);
+    else if (k == "whiteScale") d[k].n = std::max(0.001f, v);
+    else if (k == "fNumber") { d[k].n = std::clamp(v, kFNumberMin, kFNumberMax); updateEV(); }
+    else if (k == "shutter") { d[k].n = std::clamp(v, kShutterMin, kShutterMax); updateEV(); }
+    else if (k == "exposureValue") {
+        const float ev = std::clamp(v, kEVMin, kEVMax);
+        if (d["exposureMode"].s == "ShutterPriority") {
+            const float sh = float(d["shutter"].n);
+            d["fNumber"].n = std::clamp(std::sqrt(std::pow(2.f, ev) / sh), kFNumberMin, kFNumberMax);
+        } else {
+            const float fN = float(d["fNumber"].n);
+            d["shutter"].n = std::clamp(std::pow(2.f, ev) / (fN * fN), kShutterMin, kShutterMax);
+        }
+        updateEV();
+    } else d[k].n = value;
+}
 
 std::string json_escape(const std::string& s) {
     std::string o;
@@ -170,9 +286,87 @@ fpt_status ensure_scratch(fpt_pass& p) {
     return FPT_OK;
 }
 
-fpt_status check_device_error(fpt_pass& p, cudaStream_t st) {
-    (void)st;
-    return FPT_OK;
+// The camera jitter of VBufferRT's sample pattern (GBufferBase.cpp:202-229,
+// Camera.cpp:50-58): the next pattern sample x (1/width, 1/height) becomes the
+// scene camera's jitter for this frame; "Center" leaves the camera unjittered.
+//   DirectX     Utils/SampleGenerators/DxSamplePattern.cpp (8 positions)
+//   Halton      HaltonSamplePattern.cpp: bases 2 and 3, frac(v + 0.5) - 0.5
+//   Stratified  StratifiedSamplePattern.cpp: binsX x binsY strata, a fresh
+//               std::shuffle of the strata per round, std::mt19937 (default
+//               seed) and std::uniform_real_distribution<float> for the offsets
+void vbuffer_apply_jitter(fpt_pass& p, uint32_t width, uint32_t height) {
+    auto it = kSamplePatterns.find(p.str("samplePattern"));
+    const int pattern = it == kSamplePatterns.end() ? 0 : it->second;
+    fpt_scene* sc = p.scene;
+    if (p.patternBinsX == 0) {
+        // (Re)create the generator (GBufferBase::updateSamplePattern).
+        p.patternIndex = 0;
+        p.patternRng = std::mt19937();
+        p.patternBinsX = p.patternBinsY = 1;
+        p.patternPermutation.clear();
+        uint32_t count = uint32_t(std::max(0.0, p.num("sampleCount")));
+        if (pattern == 1) {
+            if (count != 8) log_warning("DxSamplePattern() currently requires sampleCount = 8. Using that number.");
+            p.props["sampleCount"].n = 8;
+        } else if (pattern == 3) {
+            count = std::clamp(count, 1u, 1024u);
+            uint32_t bx = uint32_t(std::sqrt(double(count))), by = count / bx;
+            while (bx * by != count) {
+                bx++;
+                by = count / bx;
+            }
+            p.patternBinsX = bx;
+            p.patternBinsY = by;
+            p.patternPermutation.resize(count);
+            for (uint32_t i = 0; i < count; i++) p.patternPermutation[i] = i;
+            p.props["sampleCount"].n = count;
+        }
+        if (pattern == 0 && (sc->dev.camera.jitterX != 0.f || sc->dev.camera.jitterY != 0.f)) {
+            sc->info.camera.jitterX = sc->info.camera.jitterY = 0.f;
+            sc->dev.camera = sc->info.camera;
+            sc->version++;
+        }
+    }
+    if (pattern == 0) return;
+    float jx = 0.f, jy = 0.f;
+    if (pattern == 1) {
+        static const float kDx[8][2] = {{1.f / 16.f, -3.f / 16.f}, {-1.f / 16.f, 3.f / 16.f}, {5.f / 16.f, 1.f / 16.f},
+                                        {-3.f / 16.f, -5.f / 16.f}, {-5.f / 16.f, 5.f / 16.f}, {-7.f / 16.f, -1.f / 16.f},
+                                        {3.f / 16.f, 7.f / 16.f}, {7.f / 16.f, -7.f / 16.f}};
+        jx = kDx[p.patternIndex % 8][0];
+        jy = kDx[p.patternIndex % 8][1];
+        p.patternIndex++;
+    } else if (pattern == 2) {
+        auto radical = [](uint32_t index, uint32_t base) {
+            float result = 0.f, factor = 1.f;
+            for (; index > 0; index /= base) {
+                factor /= float(base);
+                result += factor * float(index % base);
+            }
+            return result;
+        };
+        const float hx = radical(p.patternIndex, 2), hy = radical(p.patternIndex, 3);
+        const uint32_t count = uint32_t(std::max(0.0, p.num("sampleCount")));
+        p.patternIndex++;
+        if (count != 0) p.patternIndex %= count;
+        auto frac = [](float v) { return v - std::floor(v); };
+        jx = frac(hx + 0.5f) - 0.5f;
+        jy = frac(hy + 0.5f) - 0.5f;
+    } else {
+        std::uniform_real_distribution<float> dist;
+        if (p.patternIndex == 0) std::shuffle(p.patternPermutation.begin(), p.patternPermutation.end(), p.patternRng);
+        const uint32_t bin = p.patternPermutation[p.patternIndex];
+        const uint32_t i = bin % p.patternBinsX, j = bin / p.patternBinsX;
+        p.patternIndex = (p.patternIndex + 1) % uint32_t(p.patternPermutation.size());
+        const float x = (float(i) + dist(p.patternRng)) / float(p.patternBinsX);
+        const float y = (float(j) + dist(p.patternRng)) / float(p.patternBinsY);
+        jx = x - 0.5f;
+        jy = y - 0.5f;
+    }
+    sc->info.camera.jitterX = jx * (1.f / float(width));
+    sc->info.camera.jitterY = jy * (1.f / float(height));
+    sc->dev.camera = sc->info.camera;
+    sc->version++;
 }
 
 // Fills the PathTracer parameters after PathTracer::validateOptions (PathTracer.cpp:370-415).
@@ -210,7 +404,7 @@ extern "C" {
 FPT_API fpt_status fpt_pass_create(const char* type_name, fpt_pass** out) {
     if (!type_name || !out) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_create: null argument");
     std::string t(type_name);
-    if (t != "MinimalPathTracer" && t != "PathTracer" && t != "VBufferRT" && t != "WARDiffPathTracer")
+    if (t != "MinimalPathTracer" && t != "PathTracer" && t != "VBufferRT" && t != "WARDiffPathTracer" && !is_image_pass(t))
         return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_create: unknown render pass type '" + t + "'");
     auto* p = new fpt_pass();
     p->type = t;
@@ -224,6 +418,9 @@ FPT_API void fpt_pass_destroy(fpt_pass* pass) {
     if (pass->scratch) cudaFree(pass->scratch);
     if (pass->adjointScratch) cudaFree(pass->adjointScratch);
     if (pass->checkpoint) cudaFree(pass->checkpoint);
+    if (pass->accumSum) cudaFree(pass->accumSum);
+    if (pass->accumCorr) cudaFree(pass->accumCorr);
+    if (pass->imageScratch) cudaFree(pass->imageScratch);
     delete pass;
 }
 
@@ -233,25 +430,32 @@ FPT_API fpt_status fpt_pass_set_property_int(fpt_pass* pass, const char* key, in
 
 FPT_API fpt_status fpt_pass_set_property_float(fpt_pass* pass, const char* key, double value) {
     if (!pass || !key) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_property: null argument");
-    auto it = pass->props.find(key);
+    std::string k(key);
+    if (pass->type == "AccumulatePass" && k == "enableAccumulation") {
+        // AccumulatePass.cpp:87-92.
+        log_warning("'enableAccumulation' is deprecated. Use 'enabled' instead.");
+        k = "enabled";
+    }
+    auto it = pass->props.find(k);
     if (it == pass->props.end()) {
-        log_warning("Unknown property '" + std::string(key) + "' in " + pass->type + " properties.");
+        log_warning("Unknown property '" + k + "' in " + pass->type + " properties.");
         return FPT_OK;
     }
     if (it->second.isString) {
         // Enum-valued properties also accept their integer value.
-        const std::map<std::string, int>* m = nullptr;
-        std::string k(key);
-        if (k == "misHeuristic") m = &kMISHeuristics;
-        else if (k == "emissiveSampler") m = &kEmissiveSamplers;
-        else if (k == "colorFormat") m = &kColorFormats;
-        else if (k == "diffMode") m = &kDiffModes;
+        const std::map<std::string, int>* m = enum_map(k);
         if (!m) return set_error(FPT_ERR_INVALID_ARG, "property '" + k + "' expects a string");
         for (auto& kv : *m)
-            if (kv.second == int(value)) { it->second.s = kv.first; return FPT_OK; }
+            if (kv.second == int(value)) return fpt_pass_set_property_string(pass, k.c_str(), kv.first.c_str());
         return set_error(FPT_ERR_INVALID_ARG, "invalid value for property '" + k + "'");
     }
-    if (std::string(key) == "fixedSeed") pass->useFixedSeed = true;
+    if (k == "fixedSeed") pass->useFixedSeed = true;
+    if (pass->type == "ToneMapper") {
+        tone_mapper_set(*pass, k, value);
+        return FPT_OK;
+    }
+    if (pass->type == "AccumulatePass" && k == "enabled" && (value != 0) != (it->second.n != 0)) pass->frameCount = 0;
+    if (pass->type == "VBufferRT" && k == "sampleCount") pass->patternBinsX = 0;  // re-create the pattern
     it->second.n = value;
     return FPT_OK;
 }
@@ -265,12 +469,9 @@ FPT_API fpt_status fpt_pass_set_property_string(fpt_pass* pass, const char* key,
     }
     if (!it->second.isString) return set_error(FPT_ERR_INVALID_ARG, "property '" + std::string(key) + "' expects a number");
     std::string k(key), v(value);
-    const std::map<std::string, int>* m = nullptr;
-    if (k == "misHeuristic") m = &kMISHeuristics;
-    else if (k == "emissiveSampler") m = &kEmissiveSamplers;
-    else if (k == "colorFormat") m = &kColorFormats;
-    else if (k == "diffMode") m = &kDiffModes;
+    const std::map<std::string, int>* m = enum_map(k);
     if (m && m->find(v) == m->end()) return set_error(FPT_ERR_INVALID_ARG, "invalid value '" + v + "' for property '" + k + "'");
+    if (k == "samplePattern") pass->patternBinsX = 0;  // re-create the pattern
     if (k == "diffuseBrdf" && v != "Frostbite" && v != "Lambert")
         return set_error(FPT_ERR_INVALID_ARG, "diffuseBrdf must be 'Frostbite' or 'Lambert'");
     if (k == "scheduler" && v != "Wavefront" && v != "Megakernel")
@@ -308,6 +509,10 @@ FPT_API fpt_status fpt_pass_reflect_json(const fpt_pass* pass, char* buf, size_t
     if (pass->type == "MinimalPathTracer") { ch = kMinimalChannels; n = sizeof(kMinimalChannels) / sizeof(ChannelSpec); }
     else if (pass->type == "PathTracer") { ch = kPathTracerChannels; n = sizeof(kPathTracerChannels) / sizeof(ChannelSpec); }
     else if (pass->type == "VBufferRT") { ch = kVBufferChannels; n = sizeof(kVBufferChannels) / sizeof(ChannelSpec); }
+    else if (pass->type == "AccumulatePass") { ch = kAccumulateChannels; n = 2; }
+    else if (pass->type == "ToneMapper") { ch = kToneMapperChannels; n = 2; }
+    else if (pass->type == "ColorMapPass") { ch = kColorMapChannels; n = 2; }
+    else if (pass->type == "RenderToViewportPass") { ch = kViewportChannels; n = 2; }
     else { ch = kWARDiffChannels; n = sizeof(kWARDiffChannels) / sizeof(ChannelSpec); }
     std::ostringstream os;
     os << "{\"inputs\": [";
@@ -334,14 +539,23 @@ FPT_API fpt_status fpt_pass_set_scene(fpt_pass* pass, fpt_scene* scene) {
     if (!pass) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_scene: null pass");
     pass->scene = scene;
     pass->frameCount = 0;
+    pass->havePrevCamera = false;
+    if (scene) pass->accumSceneVersion = scene->resetVersion;
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_pass_reset(fpt_pass* pass) {
+    if (!pass) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_reset: null pass");
+    pass->frameCount = 0;
     return FPT_OK;
 }
 
 FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void* stream) {
     if (!pass || !io) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_execute: null argument");
-    if (!pass->scene) return set_error(FPT_ERR_NO_SCENE, pass->type + ": no scene set");
     if (io->width == 0 || io->height == 0 || io->width > 16384 || io->height > 16384)
         return set_error(FPT_ERR_INVALID_ARG, pass->type + ": invalid frame size");
+    if (is_image_pass(pass->type)) return image_pass_execute(*pass, io, static_cast<cudaStream_t>(stream));
+    if (!pass->scene) return set_error(FPT_ERR_NO_SCENE, pass->type + ": no scene set");
     if (pass->type == "PathTracer" && (io->width > 4096 || io->height > 4096))
         return set_error(FPT_ERR_INVALID_ARG, "PathTracer: frame dimension exceeds kMaxFrameDimension (4096)");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -368,7 +582,15 @@ FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void
     pass->launches = 1;
     if (pass->type == "VBufferRT") {
         if (!io->vbuffer_out) return set_error(FPT_ERR_INVALID_ARG, "VBufferRT: output 'vbuffer' not connected");
-        e = launch_vbuffer(ds, fp, st);
+        vbuffer_apply_jitter(*pass, io->width, io->height);
+        fp.depthOut = io->depth;
+        fp.mvecOut = reinterpret_cast<float2*>(io->mvec);
+        fp.viewWOut = reinterpret_cast<float4*>(io->view_w);
+        fp.maskOut = io->mask;
+        fp.prevCamera = pass->havePrevCamera ? pass->prevCamera : pass->scene->dev.camera;
+        pass->prevCamera = pass->scene->dev.camera;
+        pass->havePrevCamera = true;
+        e = launch_vbuffer(pass->scene->dev, fp, st);
     } else if (pass->type == "MinimalPathTracer") {
         if (!io->vbuffer || !io->color) return set_error(FPT_ERR_INVALID_ARG, "MinimalPathTracer: 'vbuffer' and 'color' are required");
         fp.maxBounces = uint32_t(std::max(0.0, pass->num("maxBounces")));

@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <random>
 #include <string>
+#include <vector>
 
 #include "common.h"
 #include "wavefront.h"
@@ -45,6 +47,27 @@ struct fpt_pass {
     size_t checkpointBytes = 0;
     bool checkpointValid = false, lastAdjointCheckpointed = false;
     uint64_t checkpointKey[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // AccumulatePass: running sums (double4 or float4 per pixel), the Kahan
+    // correction, the frame size they belong to and the scene state seen last.
+    void* accumSum = nullptr;
+    float4* accumCorr = nullptr;
+    size_t accumSumBytes = 0, accumCorrBytes = 0;
+    int accumPrecision = -1;
+    uint32_t accumW = 0, accumH = 0;
+    uint64_t accumSceneVersion = 0;
+    // ToneMapper / ColorMapPass reduction scratch; ColorMapPass auto range.
+    void* imageScratch = nullptr;
+    size_t imageScratchBytes = 0;
+    double autoMin = 0.0, autoMax = 0.0;
+    bool reductionAvailable = false;
+    // VBufferRT camera-jitter pattern (GBufferBase.cpp:202-229) and the camera
+    // of the previous frame (motion vectors).
+    uint32_t patternIndex = 0;
+    uint32_t patternBinsX = 1, patternBinsY = 1;
+    std::vector<uint32_t> patternPermutation;
+    std::mt19937 patternRng;
+    bool havePrevCamera = false;
+    fpt_camera_data prevCamera{};
 
     double num(const std::string& k) const;
     std::string str(const std::string& k) const;

@@ -428,8 +428,14 @@ FPT_API fpt_status fpt_scene_get_info(const fpt_scene* scene, fpt_scene_info* ou
 
 FPT_API fpt_status fpt_scene_set_camera(fpt_scene* scene, const fpt_camera* camera) {
     if (!scene || !camera) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_camera: null argument");
-    compute_camera(*camera, scene->info.camera);
-    scene->dev.camera = scene->info.camera;
+    fpt_camera_data cd;
+    compute_camera(*camera, cd);
+    // A change of the jitter alone does not restart accumulation (Camera::Changes::Jitter).
+    fpt_camera_data a = scene->info.camera, b = cd;
+    a.jitterX = a.jitterY = b.jitterX = b.jitterY = 0.f;
+    if (std::memcmp(&a, &b, sizeof(a)) != 0) scene->resetVersion++;
+    scene->info.camera = cd;
+    scene->dev.camera = cd;
     scene->version++;
     return FPT_OK;
 }
@@ -486,6 +492,7 @@ FPT_API fpt_status fpt_scene_set_material_params(fpt_scene* scene, const uint32_
     scene->materials.swap(next);
     scene->dev.hasTransmission = hasTransmission ? 1u : 0u;
     scene->version++;
+    scene->resetVersion++;
     return FPT_OK;
 }
 

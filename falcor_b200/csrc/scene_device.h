@@ -32,6 +32,9 @@ struct fpt_scene {
     float aliasWeightSum = 0.f;
     fpt_scene_info info{};
     uint64_t version = 0;             // bumped by every change that can change a path (camera, materials, vertices)
+    // Bumped by the changes that restart progressive accumulation: all of the
+    // above except camera jitter (AccumulatePass.cpp:150-168).
+    uint64_t resetVersion = 0;
     // Per mesh (= geometry instance): vertex and triangle counts, emissive flag.
     std::vector<uint32_t> meshVertexCount, meshTriCount;
     std::vector<uint8_t> meshEmissive;

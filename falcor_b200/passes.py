@@ -3,7 +3,9 @@
 ``RenderPass.create(type, props)`` mirrors ``RenderPass::create`` by name
 (RenderGraph/RenderPass.cpp:53-60) for the passes of the hot path:
 ``MinimalPathTracer``, ``PathTracer``, ``WARDiffPathTracer`` and the
-``VBufferRT`` that feeds them.  Properties use the reference names and
+``VBufferRT`` that feeds them, and the image passes of the same graphs
+(``AccumulatePass``, ``ToneMapper``, ``ColorMapPass``,
+``RenderToViewportPass``).  Properties use the reference names and
 defaults; unknown keys are warned about and ignored.  ``execute`` takes a
 ``RenderData``-like mapping from channel names to CUDA tensors and runs on the
 current torch stream.  All work goes through libfpt.so; there is no fallback.
@@ -30,6 +32,11 @@ def _ptr(t) -> int | None:
     return t.data_ptr()
 
 
+def _torch():
+    import torch
+    return torch
+
+
 def _stream() -> int:
     import torch
     return torch.cuda.current_stream().cuda_stream
@@ -38,7 +45,11 @@ def _stream() -> int:
 class RenderPass:
     """A render pass object backed by an fpt_pass handle."""
 
-    TYPES = ("MinimalPathTracer", "PathTracer", "VBufferRT", "WARDiffPathTracer")
+    TYPES = ("MinimalPathTracer", "PathTracer", "VBufferRT", "WARDiffPathTracer", "AccumulatePass", "ToneMapper",
+             "ColorMapPass", "RenderToViewportPass")
+    # Image passes: (input channel, output channel).
+    IMAGE_IO = {"AccumulatePass": ("input", "output"), "ToneMapper": ("src", "dst"), "ColorMapPass": ("input", "output"),
+                "RenderToViewportPass": ("input", "output")}
 
     def __init__(self, type_name: str, props: Mapping[str, Any] | None = None):
         h = C.c_void_p()
@@ -46,13 +57,16 @@ class RenderPass:
         self._h = h
         self.type = type_name
         self.scene: Scene | None = None
+        self.options_changed = False
         if props:
             self.set_properties(props)
+        self.options_changed = False
 
     @classmethod
     def create(cls, type_name: str, props: Mapping[str, Any] | None = None) -> "RenderPass":
         cls_map = {"MinimalPathTracer": MinimalPathTracer, "PathTracer": PathTracer, "VBufferRT": VBufferRT,
-                   "WARDiffPathTracer": WARDiffPathTracer}
+                   "WARDiffPathTracer": WARDiffPathTracer, "AccumulatePass": AccumulatePass, "ToneMapper": ToneMapper,
+                   "ColorMapPass": ColorMapPass, "RenderToViewportPass": RenderToViewportPass}
         if type_name not in cls_map:
             raise ValueError(f"unknown render pass type '{type_name}'")
         return cls_map[type_name](props)
@@ -85,6 +99,9 @@ class RenderPass:
                 check(lib().fpt_pass_set_property_string(self._h, key, str(v.name).encode()))
             else:
                 raise TypeError(f"unsupported property type for '{k}': {type(v)}")
+        # The path tracers flag RenderPassRefreshFlags::RenderOptionsChanged on
+        # the next frame after a property change (PathTracer.cpp:1340-1346).
+        self.options_changed = True
 
     setProperties = set_properties
 
@@ -108,11 +125,23 @@ class RenderPass:
     setScene = set_scene
 
     def _io(self, rd: Mapping[str, Any], width: int, height: int, frame: int, prng_dim: int = 0,
-            sample_color=None) -> _ffi.fpt_frame_io:
+            sample_color=None, refresh: bool = False) -> _ffi.fpt_frame_io:
         io = _ffi.fpt_frame_io()
         io.width, io.height = width, height
         io.frame_index = frame
         io.prng_dimension = prng_dim
+        io.refresh = int(bool(refresh))
+        if self.type in self.IMAGE_IO:
+            cin, cout = self.IMAGE_IO[self.type]
+            src, dst = rd.get(cin), rd.get(cout)
+            for name, t in ((cin, src), (cout, dst)):
+                if t is not None and (t.dtype != _torch().float32 or t.dim() != 3 or t.shape[2] != 4):
+                    raise TypeError(f"{self.type}: channel '{name}' must be an H x W x 4 float32 (RGBA32Float) tensor")
+            io.src = _ptr(src)
+            io.dst = _ptr(dst)
+            if src is not None:
+                io.src_height, io.src_width = int(src.shape[0]), int(src.shape[1])
+            return io
         io.vbuffer = _ptr(rd.get("vbuffer")) if self.type != "VBufferRT" else None
         io.color = _ptr(rd.get("color"))
         io.ray_count = _ptr(rd.get("rayCount"))
@@ -120,16 +149,31 @@ class RenderPass:
         io.d_color = _ptr(rd.get("dColor"))
         io.vbuffer_out = _ptr(rd.get("vbuffer")) if self.type == "VBufferRT" else None
         io.sample_color = _ptr(sample_color)
+        if self.type == "VBufferRT":
+            io.depth = _ptr(rd.get("depth"))
+            io.mvec = _ptr(rd.get("mvec"))
+            io.view_w = _ptr(rd.get("viewW"))
+            io.mask = _ptr(rd.get("mask"))
         return io
 
-    def execute(self, render_data: Mapping[str, Any], frame: int = 0, prng_dimension: int = 0, sample_color=None) -> None:
-        """RenderPass::execute: render into the output channels of `render_data`."""
-        some = next((t for t in render_data.values() if t is not None), None)
+    def execute(self, render_data: Mapping[str, Any], frame: int = 0, prng_dimension: int = 0, sample_color=None,
+                refresh: bool = False) -> None:
+        """RenderPass::execute: render into the output channels of `render_data`.
+        The frame size is that of the output channel (image passes) or of the
+        first channel given; `refresh` carries RenderPassRefreshFlags != None."""
+        if self.type in self.IMAGE_IO:
+            some = render_data.get(self.IMAGE_IO[self.type][1])
+        else:
+            some = next((t for t in render_data.values() if t is not None), None)
         if some is None:
-            raise ValueError("render_data has no channels")
+            raise ValueError(f"{self.type}: render_data has no output channel")
         height, width = int(some.shape[0]), int(some.shape[1])
-        io = self._io(render_data, width, height, frame, prng_dimension, sample_color)
+        io = self._io(render_data, width, height, frame, prng_dimension, sample_color, refresh)
         check(lib().fpt_pass_execute(self._h, C.byref(io), C.c_void_p(_stream())))
+
+    def reset(self) -> None:
+        """Restart the pass's frame count (AccumulatePass::reset, PathTracer::reset)."""
+        check(lib().fpt_pass_reset(self._h))
 
     def stats(self) -> _ffi.fpt_pass_stats:
         s = _ffi.fpt_pass_stats()
@@ -171,8 +215,7 @@ class PathTracer(RenderPass):
 
     def reset(self) -> None:
         """PathTracer::reset (PathTracer.cpp:198-214): restart the frame counter."""
-        if self.scene is not None:
-            self.set_scene(self.scene)
+        check(lib().fpt_pass_reset(self._h))
 
     @property
     def fixedSeed(self) -> int:
@@ -249,3 +292,61 @@ class WARDiffPathTracer(RenderPass):
         g.normal_dim = normal_grad.numel() if normal_grad is not None else 0
         g.tangent_dim = tangent_grad.numel() if tangent_grad is not None else 0
         check(lib().fpt_pass_backward(self._h, C.byref(io), C.c_void_p(_ptr(dLdI)), C.byref(g), C.c_void_p(_stream())))
+
+
+class AccumulatePass(RenderPass):
+    """AccumulatePass (RenderPasses/AccumulatePass/AccumulatePass.cpp): progressive
+    accumulation of "input" into "output" in Single, SingleCompensated or Double
+    precision; moving average when maxFrameCount > 0 (overflowMode Stop, Reset
+    or EMA).  ``reset()`` restarts it."""
+
+    def __init__(self, props=None):
+        super().__init__("AccumulatePass", props)
+
+    @property
+    def enabled(self) -> bool:
+        return bool(self.properties["enabled"])
+
+    @enabled.setter
+    def enabled(self, v: bool) -> None:
+        self.set_properties({"enabled": bool(v)})
+
+
+class ToneMapper(RenderPass):
+    """ToneMapper (RenderPasses/ToneMapper/ToneMapper.cpp): exposure (manual from
+    film speed, shutter and f-number, or automatic), white balance, operator
+    (Linear, Reinhard, ReinhardModified, HejiHableAlu, HableUc2, Aces) and clamp."""
+
+    _PROPS = ("exposureCompensation", "autoExposure", "exposureValue", "filmSpeed", "whiteBalance", "whitePoint",
+              "operator", "clamp", "whiteMaxLuminance", "whiteScale", "fNumber", "shutter", "exposureMode")
+
+    def __init__(self, props=None):
+        super().__init__("ToneMapper", props)
+
+    def __getattr__(self, k):
+        if k in ToneMapper._PROPS:
+            return self.properties[k]
+        raise AttributeError(k)
+
+    def __setattr__(self, k, v):
+        if k in ToneMapper._PROPS:
+            self.set_properties({k: v})
+        else:
+            super().__setattr__(k, v)
+
+
+class ColorMapPass(RenderPass):
+    """ColorMapPass (RenderPasses/DebugPasses/ColorMapPass/ColorMapPass.cpp): one
+    channel mapped through Grey, Jet, Viridis, Plasma, Magma or Inferno over
+    [minValue, maxValue], optionally auto-ranged from the previous frame."""
+
+    def __init__(self, props=None):
+        super().__init__("ColorMapPass", props)
+
+
+class RenderToViewportPass(RenderPass):
+    """RenderToViewportPass (RenderPasses/Viewport/RenderToViewportPass.cpp):
+    headless, a blit of "input" to "output"."""
+
+    def __init__(self, props=None):
+        super().__init__("RenderToViewportPass", props)

@@ -162,6 +162,12 @@ class Scene:
                 pass
             self._h = None
 
+    def camera_data(self) -> _ffi.fpt_camera_data:
+        """The camera of the next frame, including the jitter a VBufferRT
+        sample pattern set (fpt_scene_get_info)."""
+        check(lib().fpt_scene_get_info(self._h, C.byref(self.info)))
+        return self.info.camera
+
     def set_camera(self, camera: _ffi.fpt_camera) -> None:
         """Replaces the camera for the next frames (fpt_scene_set_camera)."""
         check(lib().fpt_scene_set_camera(self._h, C.byref(camera)))

@@ -288,6 +288,11 @@ FPT_API fpt_status fpt_scene_get_alias_table(const fpt_scene* scene, uint32_t* o
 /*   PathTracer        (RenderPasses/PathTracer/PathTracer.cpp)               */
 /*   WARDiffPathTracer (RenderPasses/WARDiffPathTracer/WARDiffPathTracer.cpp) */
 /*   VBufferRT         (RenderPasses/GBuffer/VBuffer/VBufferRT.cpp)          */
+/* and the image passes of the same graphs                                    */
+/*   AccumulatePass    (RenderPasses/AccumulatePass/AccumulatePass.cpp)       */
+/*   ToneMapper        (RenderPasses/ToneMapper/ToneMapper.cpp)               */
+/*   ColorMapPass      (RenderPasses/DebugPasses/ColorMapPass/ColorMapPass.cpp) */
+/*   RenderToViewportPass (RenderPasses/Viewport/RenderToViewportPass.cpp)    */
 /* created by name as RenderPass::create (RenderGraph/RenderPass.cpp:53-60). */
 /* ------------------------------------------------------------------------ */
 FPT_API fpt_status fpt_pass_create(const char* type_name, fpt_pass** out);
@@ -323,10 +328,27 @@ typedef struct fpt_frame_io {
     float* sample_color;         /* out, optional: per-sample RGB radiance
                                     (3 floats, pixel-major, spp per pixel),
                                     before the per-sample colour format      */
+    /* Image passes: AccumulatePass "input"/"output", ToneMapper "src"/"dst",
+     * ColorMapPass and RenderToViewportPass "input"/"output".  RGBA32F, 16 B
+     * per pixel, row-major; dst is width x height, src is src_width x
+     * src_height (0: the same as dst). */
+    const float* src;
+    float* dst;
+    uint32_t src_width, src_height;
+    uint32_t refresh;            /* RenderPassRefreshFlags != None this frame
+                                    (AccumulatePass autoReset restarts)       */
+    /* VBufferRT optional outputs (GBuffer/VBuffer/VBufferRT.cpp:51-59): */
+    float* depth;                /* "depth": R32Float NDC depth, 1 on a miss  */
+    float* mvec;                 /* "mvec": RG32Float motion vector (UV)      */
+    float* view_w;               /* "viewW": RGBA32Float, -ray dir, w = 0     */
+    float* mask;                 /* "mask": R32Float, 1 on a hit, 0 on a miss */
 } fpt_frame_io;
 
 /* RenderPass::execute (RenderGraph/RenderPass.h:184). */
 FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void* stream);
+/* AccumulatePass::reset (AccumulatePass.cpp:375-378) / PathTracer::reset
+ * (PathTracer.cpp:198-214): restart the frame count. */
+FPT_API fpt_status fpt_pass_reset(fpt_pass* pass);
 
 /* PathTracer execute that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot call cudaMalloc -- a host whose device

@@ -100,6 +100,7 @@ def lib() -> C.CDLL:
         l.orc_logluv.argtypes = [_P, u32, _P, _P]
         l.orc_intersect_triangle.restype = u32
         l.orc_intersect_triangle.argtypes = [_P, _P, _P, _P, _P]
+        l.orc_sample_pattern.argtypes = [C.c_int, u32, u32, _P]
         l.orc_bsdf_sample.argtypes = [_P, C.c_int, u32, _P, _P, u32, _P, _P, _P, _P, _P, _P, _P]
         _lib = l
     return _lib
@@ -234,3 +235,12 @@ class OracleScene:
         out = np.zeros((d, d), dtype=np.float32)
         lib().orc_scene_get_importance(self._h, mip, ptr(out))
         return out
+
+
+def sample_pattern(kind: str, sample_count: int, n: int) -> np.ndarray:
+    """The first n camera-jitter samples of a VBufferRT sample pattern
+    ("DirectX", "Halton" or "Stratified"), in [-0.5, 0.5)^2."""
+    kinds = {"DirectX": 1, "Halton": 2, "Stratified": 3}
+    out = np.zeros((n, 2), np.float32)
+    lib().orc_sample_pattern(kinds[kind], sample_count, n, ptr(out))
+    return out

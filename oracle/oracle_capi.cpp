@@ -9,6 +9,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <random>
 #include <vector>
 
 #include "oracle_render.h"
@@ -315,6 +316,58 @@ double orc_wardiff(const void* sp, const WarDiffParams* p, int mode, int K, cons
         for (auto& c : wcs) *rays += c.rays;
     }
     return dt;
+}
+
+// Camera-jitter sample patterns of VBufferRT (Utils/SampleGenerators):
+// kind 1 DirectX (DxSamplePattern.cpp:33-45), 2 Halton (HaltonSamplePattern.cpp:
+// 33-64), 3 Stratified (StratifiedSamplePattern.cpp:35-95, std::mt19937 with its
+// default seed, std::shuffle once per round, uniform_real_distribution<float>).
+// Writes n (x, y) pairs in [-0.5, 0.5).
+void orc_sample_pattern(int kind, uint32_t sampleCount, uint32_t n, float* out) {
+    if (kind == 1) {
+        static const float t[8][2] = {{1, -3}, {-1, 3}, {5, 1}, {-3, -5}, {-5, 5}, {-7, -1}, {3, 7}, {7, -7}};
+        for (uint32_t i = 0; i < n; i++) {
+            out[2 * i] = t[i % 8][0] / 16.f;
+            out[2 * i + 1] = t[i % 8][1] / 16.f;
+        }
+        return;
+    }
+    if (kind == 2) {
+        uint32_t cur = 0;
+        auto halton = [](uint32_t index, uint32_t base) {
+            float r = 0.f, f = 1.f;
+            while (index > 0) {
+                f /= float(base);
+                r += f * float(index % base);
+                index /= base;
+            }
+            return r;
+        };
+        for (uint32_t i = 0; i < n; i++) {
+            float v[2] = {halton(cur, 2), halton(cur, 3)};
+            cur++;
+            if (sampleCount) cur %= sampleCount;
+            for (int k = 0; k < 2; k++) out[2 * i + k] = (v[k] + 0.5f - std::floor(v[k] + 0.5f)) - 0.5f;
+        }
+        return;
+    }
+    const uint32_t count = std::min(std::max(sampleCount, 1u), 1024u);
+    uint32_t bx = uint32_t(std::sqrt(double(count))), by = count / bx;
+    while (bx * by != count) by = count / ++bx;
+    std::vector<uint32_t> perm(count);
+    for (uint32_t i = 0; i < count; i++) perm[i] = i;
+    std::mt19937 rng;
+    uint32_t cur = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        std::uniform_real_distribution<float> u;
+        if (cur == 0) std::shuffle(perm.begin(), perm.end(), rng);
+        const uint32_t bin = perm[cur];
+        cur = (cur + 1) % count;
+        const float fx = (float(bin % bx) + u(rng)) / float(bx);
+        const float fy = (float(bin / bx) + u(rng)) / float(by);
+        out[2 * i] = fx - 0.5f;
+        out[2 * i + 1] = fy - 0.5f;
+    }
 }
 
 }  // extern "C"
