@@ -254,6 +254,7 @@ FPT_API fpt_status fpt_batch_add(fpt_batch* b, const fpt_batch_request* req) {
         pt.props["maxSurfaceBounces"] = PropValue::num(req->max_bounces);
         pt.props["maxDiffuseBounces"] = PropValue::num(req->max_bounces);
         pt.props["maxSpecularBounces"] = PropValue::num(req->max_bounces);
+        pt.explicitKeys.insert({"maxSurfaceBounces", "maxDiffuseBounces", "maxSpecularBounces"});
         pt.props["emissiveSampler"] = PropValue::str("Power");
         pt.props["fixedSeed"] = PropValue::num(double(req->seed) * 64.0 + f);
         pt.useFixedSeed = true;

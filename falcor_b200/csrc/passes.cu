@@ -373,11 +373,21 @@ void vbuffer_apply_jitter(fpt_pass& p, uint32_t width, uint32_t height) {
 void path_tracer_params(fpt_pass& p, FrameParams& fp) {
     fp.spp = uint32_t(std::clamp(p.num("samplesPerPixel"), 1.0, 16.0));
     auto clampB = [](double v) { return uint32_t(std::clamp(v, 0.0, 254.0)); };
+    uint32_t surface = clampB(p.num("maxSurfaceBounces"));
     fp.maxDiffuseBounces = clampB(p.num("maxDiffuseBounces"));
     fp.maxSpecularBounces = clampB(p.num("maxSpecularBounces"));
     fp.maxTransmissionBounces = clampB(p.num("maxTransmissionBounces"));
-    fp.maxSurfaceBounces = std::max(clampB(p.num("maxSurfaceBounces")),
-                                    std::max(fp.maxDiffuseBounces, std::max(fp.maxSpecularBounces, fp.maxTransmissionBounces)));
+    // PathTracer::parseProperties (PathTracer.cpp:336-350): an explicit
+    // maxSurfaceBounces initialises the per-type counts that were not set;
+    // otherwise it is the largest of them.  validateOptions (:398-401) then
+    // raises it to at least each per-type count.
+    if (p.explicitKeys.count("maxSurfaceBounces")) {
+        if (!p.explicitKeys.count("maxDiffuseBounces")) fp.maxDiffuseBounces = surface;
+        if (!p.explicitKeys.count("maxSpecularBounces")) fp.maxSpecularBounces = surface;
+        if (!p.explicitKeys.count("maxTransmissionBounces")) fp.maxTransmissionBounces = surface;
+    }
+    const uint32_t typeMax = std::max(fp.maxDiffuseBounces, std::max(fp.maxSpecularBounces, fp.maxTransmissionBounces));
+    fp.maxSurfaceBounces = p.explicitKeys.count("maxSurfaceBounces") ? std::max(surface, typeMax) : typeMax;
     fp.sampleGenerator = uint32_t(p.num("sampleGenerator")) == 1 ? 1u : 0u;
     fp.useBSDFSampling = p.num("useBSDFSampling") != 0;
     fp.useNEE = p.num("useNEE") != 0;
@@ -450,6 +460,7 @@ FPT_API fpt_status fpt_pass_set_property_float(fpt_pass* pass, const char* key, 
         return set_error(FPT_ERR_INVALID_ARG, "invalid value for property '" + k + "'");
     }
     if (k == "fixedSeed") pass->useFixedSeed = true;
+    pass->explicitKeys.insert(k);
     if (pass->type == "ToneMapper") {
         tone_mapper_set(*pass, k, value);
         return FPT_OK;
@@ -472,6 +483,7 @@ FPT_API fpt_status fpt_pass_set_property_string(fpt_pass* pass, const char* key,
     const std::map<std::string, int>* m = enum_map(k);
     if (m && m->find(v) == m->end()) return set_error(FPT_ERR_INVALID_ARG, "invalid value '" + v + "' for property '" + k + "'");
     if (k == "samplePattern") pass->patternBinsX = 0;  // re-create the pattern
+    pass->explicitKeys.insert(k);
     if (k == "diffuseBrdf" && v != "Frostbite" && v != "Lambert")
         return set_error(FPT_ERR_INVALID_ARG, "diffuseBrdf must be 'Frostbite' or 'Lambert'");
     if (k == "scheduler" && v != "Wavefront" && v != "Megakernel")
@@ -484,10 +496,24 @@ FPT_API fpt_status fpt_pass_set_property_string(fpt_pass* pass, const char* key,
 
 FPT_API fpt_status fpt_pass_get_properties_json(const fpt_pass* pass, char* buf, size_t cap) {
     if (!pass) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_get_properties_json: null pass");
+    std::map<std::string, PropValue> props = pass->props;
+    if (pass->type == "PathTracer") {
+        // PathTracer::getProperties reports the bounce counts after parsing and validation.
+        FrameParams fp;
+        std::memset(&fp, 0, sizeof(fp));
+        fpt_pass tmp;
+        tmp.props = pass->props;
+        tmp.explicitKeys = pass->explicitKeys;
+        path_tracer_params(tmp, fp);
+        props["maxSurfaceBounces"].n = fp.maxSurfaceBounces;
+        props["maxDiffuseBounces"].n = fp.maxDiffuseBounces;
+        props["maxSpecularBounces"].n = fp.maxSpecularBounces;
+        props["maxTransmissionBounces"].n = fp.maxTransmissionBounces;
+    }
     std::ostringstream os;
     os << "{";
     bool first = true;
-    for (auto& kv : pass->props) {
+    for (auto& kv : props) {
         if (!first) os << ", ";
         first = false;
         os << "\"" << json_escape(kv.first) << "\": ";

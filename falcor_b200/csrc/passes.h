@@ -5,6 +5,7 @@
 
 #include <map>
 #include <random>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -26,6 +27,7 @@ struct PropValue {
 struct fpt_pass {
     std::string type;
     std::map<std::string, fpt::PropValue> props;
+    std::set<std::string> explicitKeys;  // properties set by the caller (Properties::has)
     fpt_scene* scene = nullptr;
     void* scratch = nullptr;          // counters (16 B) + work counter (4 B)
     void* adjointScratch = nullptr;   // checkpointed path vertices (adjoint)

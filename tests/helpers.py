@@ -49,8 +49,10 @@ def minimal_params(w, h, frame=0, max_bounces=3, lambert=0):
 
 def pt_params(w, h, spp, seed, max_bounces=3, sampler=2, color_format=1, mis=0, lambert=0):
     from oracle.ffi import PathTracerParams
+    # The PathTracer properties of pt_props set maxSurfaceBounces, so the
+    # transmission count follows it (PathTracer.cpp:336-345).
     return PathTracerParams(width=w, height=h, samplesPerPixel=spp, maxSurfaceBounces=max_bounces,
-                            maxDiffuseBounces=max_bounces, maxSpecularBounces=max_bounces, maxTransmissionBounces=10,
+                            maxDiffuseBounces=max_bounces, maxSpecularBounces=max_bounces, maxTransmissionBounces=max_bounces,
                             sampleGenerator=0, useBSDFSampling=1, useNEE=1, useMIS=1, misHeuristic=mis,
                             misPowerExponent=2.0, emissiveSampler=sampler, specularRoughnessThreshold=0.25,
                             colorFormat=color_format, seed=seed, lambert=lambert)

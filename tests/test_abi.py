@@ -84,3 +84,21 @@ def test_procedural_scenes_and_camera(fpt):
                              emissive_count=8, envmap=(64, 32), aspect_ratio=16 / 9)
     assert h.triangle_count == 2 * 63 * 63 + 1000 + 8
     assert h.desc.envmap and h.desc.envmap.contents.width == 64
+
+
+def test_path_tracer_bounce_count_rules(fpt):
+    """PathTracer::parseProperties / validateOptions (PathTracer.cpp:336-401): an
+    explicit maxSurfaceBounces initialises the per-type counts left unset; without
+    it the surface count is the largest per-type count; it is never below any."""
+    from falcor_b200.passes import PathTracer
+    keys = ("maxSurfaceBounces", "maxDiffuseBounces", "maxSpecularBounces", "maxTransmissionBounces")
+    p = PathTracer().properties
+    assert [p[k] for k in keys] == [10, 3, 3, 10]
+    p = PathTracer({"maxSurfaceBounces": 5}).properties
+    assert [p[k] for k in keys] == [5, 5, 5, 5]
+    p = PathTracer({"maxSurfaceBounces": 2, "maxDiffuseBounces": 4}).properties
+    assert [p[k] for k in keys] == [4, 4, 2, 2]
+    p = PathTracer({"maxSurfaceBounces": 8, "maxDiffuseBounces": 8, "maxSpecularBounces": 8}).properties
+    assert [p[k] for k in keys] == [8, 8, 8, 8]
+    p = PathTracer({"maxDiffuseBounces": 6}).properties
+    assert [p[k] for k in keys] == [10, 6, 3, 10]
