@@ -38,6 +38,7 @@ struct DevScene {
     uint32_t hasEnv, hasEmissive, hasTransmission;
     uint32_t nodeCount, triCount;
     uint32_t bvhDepth;                // levels of the 8-wide tree (root = 1)
+    uint32_t materialCount;
     uint32_t* errorWord;              // device error word (FPT_DEVERR_*)
 };
 
@@ -270,7 +271,8 @@ FPT_D void visit_node(const DevScene& s, const TraceRay& r, float tBest, uint32_
 #endif
 constexpr int kPostponeLanes = FPT_POSTPONE_LANES;
 
-template <bool ANY>
+// STACK: entries of this thread's stack (at least the tree depth).
+template <bool ANY, int STACK = kStackSize>
 FPT_D void trace_step(const DevScene& s, const TraceRay& r, TraceState& t, uint2* stack, uint32_t stride, int postponeLimit) {
     if (t.gHits) {
         const uint32_t i = uint32_t(__ffs(t.gHits) - 1);
@@ -288,7 +290,7 @@ FPT_D void trace_step(const DevScene& s, const TraceRay& r, TraceState& t, uint2
         uint32_t innerHits, childBase, imask, triBase, triHits;
         visit_node(s, r, t.tBest, nodeIdx, innerHits, childBase, imask, triBase, triHits);
         if (t.gHits) {
-            if (t.sp >= kStackSize) {
+            if (t.sp >= STACK) {
                 atomicOr(s.errorWord, FPT_DEVERR_STACK_OVERFLOW);
                 t.status = kTraceError;
                 return;

@@ -40,6 +40,7 @@ struct FrameParams {
     uint32_t colorFormat;
     uint32_t seed;
     uint32_t lambert;          // DiffuseBrdf = Lambert (instead of Frostbite)
+    uint32_t sortMaterials;    // wavefront: sort each secondary shade queue by material
     // bookkeeping
     unsigned long long* counters;  // [0] paths, [1] rays
     uint32_t* workCounter;         // persistent scheduling counter (zeroed by the launcher)

@@ -338,6 +338,7 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
     ds.nodeCount = uint32_t(s.bvh.nodes.size());
     ds.triCount = total;
     ds.bvhDepth = s.bvh.maxDepth;
+    ds.materialCount = d.material_count;
     ds.camera = s.info.camera;
     ds.bits = s.info.hit_bits;
 

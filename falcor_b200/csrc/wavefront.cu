@@ -142,15 +142,25 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_SHADE_MIN_BLOCKS) wf_shade(De
 }
 
 // Visibility rays of the NEE samples: any hit; adds thp * Lr when unoccluded.
-__global__ void __launch_bounds__(kTraceBlock, FPT_TRACE_MIN_BLOCKS) wf_shadow(DevScene s, FrameParams p, WaveParams wp, SoA w) {
-    __shared__ uint2 stackMem[kStackSize * kTraceBlock];
-    trace_queue<true>(s, p, wp, w, stackMem + threadIdx.x);
+// Scenes whose tree is at most kShortStack levels deep trace with a stack of
+// that many entries (half the shared memory per block).
+#ifndef FPT_TRACE_MIN_BLOCKS_SHORT
+#define FPT_TRACE_MIN_BLOCKS_SHORT 6
+#endif
+constexpr int kShortStack = 16;
+template <int STACK>
+__global__ void __launch_bounds__(kTraceBlock, STACK <= kShortStack ? FPT_TRACE_MIN_BLOCKS_SHORT : FPT_TRACE_MIN_BLOCKS)
+    wf_shadow(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    __shared__ uint2 stackMem[STACK * kTraceBlock];
+    trace_queue<true, false, false, STACK>(s, p, wp, w, stackMem + threadIdx.x);
 }
 
 // Extension rays: closest hit; the path re-enters the shade queue.
-__global__ void __launch_bounds__(kTraceBlock, FPT_TRACE_MIN_BLOCKS) wf_extend(DevScene s, FrameParams p, WaveParams wp, SoA w) {
-    __shared__ uint2 stackMem[kStackSize * kTraceBlock];
-    trace_queue<false>(s, p, wp, w, stackMem + threadIdx.x);
+template <int STACK>
+__global__ void __launch_bounds__(kTraceBlock, STACK <= kShortStack ? FPT_TRACE_MIN_BLOCKS_SHORT : FPT_TRACE_MIN_BLOCKS)
+    wf_extend(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    __shared__ uint2 stackMem[STACK * kTraceBlock];
+    trace_queue<false, false, false, STACK>(s, p, wp, w, stackMem + threadIdx.x);
 }
 
 // Batched waves: each ray traced in its own request's scene.
@@ -213,6 +223,57 @@ __global__ void wf_resolve(DevScene s, FrameParams p, WaveParams wp, SoA w) {
     }
 }
 
+// Counting sort of the shade queue by material (misses in the last bin), so
+// that the warps of the shade kernel see one material -- and hits apart from
+// misses -- instead of a random mix.  The keys were written by the extension
+// kernel at the queue positions; sorting moves 12 B per path.
+__global__ void wf_sort_count(WaveParams wp, uint32_t* bins) {
+    __shared__ uint32_t h[WavefrontBuffers::kMaxSortBins];
+    for (uint32_t b = threadIdx.x; b < wp.sortBins; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    const uint32_t n = wp.counts[0];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        atomicAdd(&h[min(wp.sortKeys[k], wp.sortBins - 1u)], 1u);
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < wp.sortBins; b += blockDim.x)
+        if (h[b]) atomicAdd(&bins[b], h[b]);
+}
+
+// Exclusive prefix sum of the bin counts into the cursors (one block of
+// kMaxSortBins threads).
+__global__ void wf_sort_scan(WaveParams wp, uint32_t* bins) {
+    __shared__ uint32_t v[WavefrontBuffers::kMaxSortBins];
+    const uint32_t t = threadIdx.x;
+    const uint32_t own = t < wp.sortBins ? bins[t] : 0u;
+    v[t] = own;
+    __syncthreads();
+    for (uint32_t off = 1; off < blockDim.x; off <<= 1) {
+        const uint32_t add = t >= off ? v[t - off] : 0u;
+        __syncthreads();
+        v[t] += add;
+        __syncthreads();
+    }
+    if (t < wp.sortBins) bins[WavefrontBuffers::kMaxSortBins + t] = v[t] - own;
+}
+
+// Scatters queue entries to their bins (warp-aggregated per key).
+__global__ void wf_sort_scatter(WaveParams wp, uint32_t* bins, uint32_t* out) {
+    const uint32_t n = wp.counts[0];
+    uint32_t* cursor = bins + WavefrontBuffers::kMaxSortBins;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k - lane < n; k += gridDim.x * blockDim.x) {
+        const bool valid = k < n;
+        const uint32_t key = valid ? min(wp.sortKeys[k], wp.sortBins - 1u) : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        if (!valid) continue;
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (int(lane) == leader) base = atomicAdd(&cursor[key], uint32_t(__popc(peers)));
+        base = __shfl_sync(peers, base, leader);
+        out[base + uint32_t(__popc(peers & ((1u << lane) - 1u)))] = wp.shadeQueue[k];
+    }
+}
+
 // Moves the extension queue into the shade queue for the next bounce.
 __global__ void wf_advance(WaveParams wp) {
     wp.counts[0] = wp.counts[1];
@@ -234,12 +295,18 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
     w.sampleL = b.sampleL;
     const uint32_t pixels = p.width * p.height;
     const uint32_t wavePixels = std::max<uint32_t>(1, std::min<uint32_t>(pixels, b.capacity / p.spp));
-    static int gShade = 0, gTrace = 0, gGen = 0;
+    static int gShade = 0, gTrace = 0, gTraceShort = 0, gGen = 0;
     if (!gShade) {
         gShade = blocks_for(reinterpret_cast<const void*>(wf_shade<SG, HAS_T, false>), kShadeBlock);
-        gTrace = blocks_for(reinterpret_cast<const void*>(wf_extend), kTraceBlock);
+        gTrace = blocks_for(reinterpret_cast<const void*>(wf_extend<kStackSize>), kTraceBlock);
+        gTraceShort = blocks_for(reinterpret_cast<const void*>(wf_extend<kShortStack>), kTraceBlock);
         gGen = blocks_for(reinterpret_cast<const void*>(wf_generate<SG, false>), kShadeBlock);
     }
+    const bool shortStack = s.bvhDepth <= uint32_t(kShortStack);
+    // Material sort of the secondary shade queues (primary hits come in pixel
+    // order, already coherent).
+    const bool sortQueue = p.sortMaterials && b.owning && b.ensure_sort() == cudaSuccess;
+    const uint32_t sortBins = std::min<uint32_t>(std::max<uint32_t>(s.materialCount, 1u), WavefrontBuffers::kMaxSortBins - 1u) + 1u;
     const uint32_t maxIter = p.maxSurfaceBounces + 2;
     for (uint32_t first = 0; first < pixels; first += wavePixels) {
         WaveParams wp{};
@@ -254,19 +321,33 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
         wp.shadeQueue = qa;
         wp.extQueue = qb;
         wp.shadowQueue = b.shadowQueue;
+        wp.sortKeys = sortQueue ? b.sortKeys : nullptr;
+        wp.sortBins = sortBins;
         const int genBlocks = std::min<int>(gGen, int((wp.wavePaths + kShadeBlock - 1) / kShadeBlock));
         T0(KC_GENERATE);
         wf_generate<SG, false><<<genBlocks, kShadeBlock, 0, st>>>(s, p, wp, w);
         T1();
         for (uint32_t it = 0; it < maxIter; it++) {
+            if (sortQueue && it > 0) {
+                T0(KC_SORT);
+                e = cudaMemsetAsync(b.sortBins, 0, WavefrontBuffers::kMaxSortBins * sizeof(uint32_t), st);
+                if (e != cudaSuccess) return e;
+                wf_sort_count<<<gGen, kShadeBlock, 0, st>>>(wp, b.sortBins);
+                wf_sort_scan<<<1, WavefrontBuffers::kMaxSortBins, 0, st>>>(wp, b.sortBins);
+                wf_sort_scatter<<<gGen, kShadeBlock, 0, st>>>(wp, b.sortBins, b.sortQueue);
+                T1();
+                wp.shadeQueue = b.sortQueue;
+            }
             T0(KC_SHADE);
             wf_shade<SG, HAS_T, false><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
             T1();
             T0(KC_SHADOW);
-            wf_shadow<<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
+            if (shortStack) wf_shadow<kShortStack><<<gTraceShort, kTraceBlock, 0, st>>>(s, p, wp, w);
+            else wf_shadow<kStackSize><<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
             T1();
             T0(KC_EXTEND);
-            wf_extend<<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
+            if (shortStack) wf_extend<kShortStack><<<gTraceShort, kTraceBlock, 0, st>>>(s, p, wp, w);
+            else wf_extend<kStackSize><<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
             T1();
             wf_advance<<<1, 1, 0, st>>>(wp);
             std::swap(qa, qb);
@@ -383,9 +464,29 @@ cudaError_t WavefrontBuffers::ensure(uint32_t cap) {
 }
 
 void WavefrontBuffers::release() {
-    if (base) cudaFree(base);
+    if (base && owning) cudaFree(base);
+    if (sortBase) cudaFree(sortBase);
     base = nullptr;
     capacity = 0;
+    sortBase = nullptr;
+    sortCapacity = 0;
+    sortKeys = sortQueue = sortBins = nullptr;
+}
+
+cudaError_t WavefrontBuffers::ensure_sort() {
+    if (!owning) return cudaErrorNotSupported;
+    if (sortBase && sortCapacity >= capacity) return cudaSuccess;
+    if (sortBase) cudaFree(sortBase);
+    sortBase = nullptr;
+    sortCapacity = 0;
+    const size_t bytes = 2 * size_t(capacity) * sizeof(uint32_t) + 2 * kMaxSortBins * sizeof(uint32_t);
+    cudaError_t e = cudaMalloc(&sortBase, bytes);
+    if (e != cudaSuccess) { sortBase = nullptr; return e; }
+    sortCapacity = capacity;
+    sortKeys = static_cast<uint32_t*>(sortBase);
+    sortQueue = sortKeys + capacity;
+    sortBins = sortQueue + capacity;
+    return cudaSuccess;
 }
 
 size_t WavefrontBuffers::bytes_for(uint32_t cap) {

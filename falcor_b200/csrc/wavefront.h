@@ -23,8 +23,17 @@ struct WavefrontBuffers {
     uint32_t* queueB = nullptr;
     uint32_t* shadowQueue = nullptr;
     uint32_t* counts = nullptr;    // [0] shade, [1] extension, [2] shadow
+    // Material sort of the shade queue (allocated on first use, owning mode
+    // only): per-position keys, the sorted queue, bin counts and cursors.
+    void* sortBase = nullptr;
+    uint32_t sortCapacity = 0;
+    uint32_t* sortKeys = nullptr;
+    uint32_t* sortQueue = nullptr;
+    uint32_t* sortBins = nullptr;  // kMaxSortBins counts + kMaxSortBins cursors
+    static constexpr uint32_t kMaxSortBins = 1024;
     float4* f4(int k) const { return arrays + size_t(k) * capacity; }
     cudaError_t ensure(uint32_t capacity);
+    cudaError_t ensure_sort();
     void release();
     ~WavefrontBuffers() { release(); }
 
@@ -36,7 +45,7 @@ struct WavefrontBuffers {
 };
 
 // Kernel categories timed by KernelTimer.
-enum KernelCategory { KC_GENERATE = 0, KC_SHADE = 1, KC_SHADOW = 2, KC_EXTEND = 3, KC_RESOLVE = 4, KC_COUNT = 5 };
+enum KernelCategory { KC_GENERATE = 0, KC_SHADE = 1, KC_SHADOW = 2, KC_EXTEND = 3, KC_RESOLVE = 4, KC_SORT = 5, KC_COUNT = 6 };
 
 // Optional CUDA-event timing of each kernel launch, by category (the
 // equivalent of Falcor's FALCOR_PROFILE scopes, Utils/Timing/Profiler.h).

@@ -27,6 +27,10 @@ struct WaveParams {
     const uint32_t* shadeQueue;
     uint32_t* extQueue;
     uint32_t* shadowQueue;
+    // Material sort of the next shade queue: the extension kernel writes the
+    // sort key of queue position k to sortKeys[k] (null: no sort).
+    uint32_t* sortKeys;
+    uint32_t sortBins;         // material bins + 1 miss bin
     // Batched waves only: per-request scenes/frames, this wave's tiles, slot -> tile.
     const DevScene* scenes;
     const FrameParams* frames;
@@ -125,18 +129,19 @@ constexpr uint32_t kFetchChunk = 128;
 constexpr int kRefillBelow = FPT_REFILL_BELOW;
 
 // MULTI: rays of a batched wave, each traced in its own request's scene.
-template <bool SHADOW, bool MARK_VISIBLE = false, bool MULTI = false>
+// STACK: traversal-stack entries per thread (>= the tree depth).
+template <bool SHADOW, bool MARK_VISIBLE = false, bool MULTI = false, int STACK = kStackSize>
 FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams& wp, const SoA& w, uint2* stack) {
     const uint32_t lane = threadIdx.x & 31u;
     Counters cnt;
     const uint32_t n = wp.counts[SHADOW ? 2 : 1];
     uint32_t* fetch = wp.counts + (SHADOW ? kFetchShadow : kFetchExtend);
     const uint32_t* queue = SHADOW ? wp.shadowQueue : wp.extQueue;
-    const int postponeLimit = MULTI ? 0 : kStackSize - int(s.bvhDepth);
+    const int postponeLimit = MULTI ? 0 : STACK - int(s.bvhDepth);
     uint32_t chunkNext = 0, chunkEnd = 0;  // warp-uniform
     bool drained = n == 0 || (!MULTI && s.nodeCount == 0);
     bool active = false;
-    uint32_t path = 0, fv = 0;
+    uint32_t path = 0, fv = 0, qpos = 0;
     const DevScene* S = nullptr;  // MULTI: this lane's scene
     TraceRay r;
     TraceState t;
@@ -154,7 +159,8 @@ FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams
                 const uint32_t avail = chunkEnd - chunkNext;
                 const uint32_t rank = __popc(idle & ((1u << lane) - 1u));
                 if (!active && rank < avail) {
-                    path = queue[chunkNext + rank];
+                    qpos = chunkNext + rank;
+                    path = queue[qpos];
                     float4 o, d;
                     if (SHADOW) { o = w.sOrigin[path]; d = w.sDir[path]; }
                     else { o = w.originPdf[path]; d = w.dirV[path]; }
@@ -174,9 +180,9 @@ FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams
         for (;;) {
             if (active) {
                 if (MULTI) {
-                    if (t.status == kTraceRunning) trace_step<SHADOW>(*S, r, t, stack, kTraceBlock, 0);
+                    if (t.status == kTraceRunning) trace_step<SHADOW, STACK>(*S, r, t, stack, kTraceBlock, 0);
                 } else {
-                    trace_step<SHADOW>(s, r, t, stack, kTraceBlock, postponeLimit);
+                    trace_step<SHADOW, STACK>(s, r, t, stack, kTraceBlock, postponeLimit);
                 }
                 if (t.status != kTraceRunning) {
                     active = false;
@@ -202,6 +208,11 @@ FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams
                             w.hit[path] = make_uint4(h.instanceID, h.primIndex, __float_as_uint(h.baryX), __float_as_uint(h.baryY));
                         } else {
                             f &= ~0x2u;
+                        }
+                        if (!MULTI && wp.sortKeys) {
+                            // Material bin of the hit (misses in the last bin).
+                            const uint32_t last = wp.sortBins - 1u;
+                            wp.sortKeys[qpos] = h.valid ? min(__ldg(&s.instances[h.instanceID].materialID), last - 1u) : last;
                         }
                         float4 d = w.dirV[path];
                         d.w = __uint_as_float(f);
