@@ -270,11 +270,15 @@ FPT_D void visit_node(const DevScene& s, const TraceRay& r, float tBest, uint32_
 #define FPT_POSTPONE_LANES 0
 #endif
 constexpr int kPostponeLanes = FPT_POSTPONE_LANES;
+// TRIS: triangle tests per traversal step (0: all of the visited node's
+// leaves in one step).  A bounded count keeps the lanes of a warp in step when
+// one lane has a long leaf list; the next node is visited only once the list
+// is empty, so the visiting order -- and the result -- are unchanged.
 
 // STACK: entries of this thread's stack (at least the tree depth).
-template <bool ANY, int STACK = kStackSize>
+template <bool ANY, int STACK = kStackSize, int TRIS = 0>
 FPT_D void trace_step(const DevScene& s, const TraceRay& r, TraceState& t, uint2* stack, uint32_t stride, int postponeLimit) {
-    if (t.gHits) {
+    if (t.gHits && (TRIS == 0 || t.tHits == 0)) {
         const uint32_t i = uint32_t(__ffs(t.gHits) - 1);
         t.gHits &= t.gHits - 1u;
         const uint32_t slot = i ^ r.octinv;
@@ -304,7 +308,7 @@ FPT_D void trace_step(const DevScene& s, const TraceRay& r, TraceState& t, uint2
         t.tBase = triBase;
         t.tHits = triHits;
     }
-    while (t.tHits) {
+    for (int tested = 0; t.tHits && (TRIS == 0 || tested < TRIS); tested++) {
         if (postponeLimit > 0 && t.gHits && t.sp < postponeLimit && __popc(__activemask()) < kPostponeLanes) {
             stack[size_t(t.sp) * stride] = make_uint2(t.tBase | kTriGroupFlag, t.tHits);
             t.sp++;

@@ -125,6 +125,15 @@ FPT_D void push(bool pred, uint32_t item, uint32_t* q, uint32_t* cnt) {
 #ifndef FPT_TRACE_MIN_BLOCKS
 #define FPT_TRACE_MIN_BLOCKS 6
 #endif
+// Triangle tests per traversal step of the queue kernels (measured on the
+// 1080p heightfield frame: extension rays 8 % faster with 1, visibility rays
+// 6 % faster with 2, than testing a whole leaf list per step).
+#ifndef FPT_EXTEND_TRIS_PER_STEP
+#define FPT_EXTEND_TRIS_PER_STEP 1
+#endif
+#ifndef FPT_SHADOW_TRIS_PER_STEP
+#define FPT_SHADOW_TRIS_PER_STEP 2
+#endif
 constexpr uint32_t kFetchChunk = 128;
 constexpr int kRefillBelow = FPT_REFILL_BELOW;
 
@@ -180,9 +189,11 @@ FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams
         for (;;) {
             if (active) {
                 if (MULTI) {
-                    if (t.status == kTraceRunning) trace_step<SHADOW, STACK>(*S, r, t, stack, kTraceBlock, 0);
+                    if (t.status == kTraceRunning)
+                        trace_step<SHADOW, STACK, SHADOW ? FPT_SHADOW_TRIS_PER_STEP : FPT_EXTEND_TRIS_PER_STEP>(*S, r, t, stack, kTraceBlock, 0);
                 } else {
-                    trace_step<SHADOW, STACK>(s, r, t, stack, kTraceBlock, postponeLimit);
+                    trace_step<SHADOW, STACK, SHADOW ? FPT_SHADOW_TRIS_PER_STEP : FPT_EXTEND_TRIS_PER_STEP>(s, r, t, stack, kTraceBlock,
+                                                                                                         postponeLimit);
                 }
                 if (t.status != kTraceRunning) {
                     active = false;
