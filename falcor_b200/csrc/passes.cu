@@ -127,6 +127,11 @@ void set_defaults(fpt_pass& p) {
         // the 1080p heightfield frame it made shading 3.7 % faster but cost
         // 3.2 ms per frame and slowed the extension rays that follow (net -6 %).
         d["sortShadeQueue"] = PropValue::num(0);
+        // Wavefront: the extension kernel queues hits and misses apart; misses
+        // (environment emission) are shaded by their own small kernel.  Off by
+        // default: on the 1080p heightfield frame shading got 5 % faster but the
+        // queue pushes made the extension kernel 10 % slower (net -2 %).
+        d["splitMisses"] = PropValue::num(0);
     } else if (p.type == "VBufferRT") {
         // GBufferBase.h:96-98.
         d["samplePattern"] = PropValue::str("Center");
@@ -409,6 +414,7 @@ void path_tracer_params(fpt_pass& p, FrameParams& fp) {
     fp.seed = p.useFixedSeed ? uint32_t(p.num("fixedSeed")) : p.frameCount;
     fp.lambert = p.str("diffuseBrdf") == "Lambert";
     fp.sortMaterials = p.num("sortShadeQueue") != 0 ? 1u : 0u;
+    fp.splitMisses = p.num("splitMisses") != 0 ? 1u : 0u;
 }
 
 }  // namespace fpt
@@ -645,7 +651,8 @@ FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void
             e = launch_path_tracer_wavefront(ds, fp, pass->wavefront, st, &pass->timer);
             const uint32_t wavePixels = std::max<uint32_t>(1, std::min<uint32_t>(fp.width * fp.height, pass->wavefront.capacity / fp.spp));
             const uint32_t waves = (fp.width * fp.height + wavePixels - 1) / wavePixels;
-            pass->launches = waves * (4 * (fp.maxSurfaceBounces + 2) + 3 + (fp.sortMaterials ? 3 * (fp.maxSurfaceBounces + 1) : 0));
+            pass->launches = waves * (4 * (fp.maxSurfaceBounces + 2) + 3 + (fp.sortMaterials ? 3 * (fp.maxSurfaceBounces + 1) : 0) +
+                                      (fp.splitMisses ? fp.maxSurfaceBounces + 1 : 0));
         }
         pass->frameCount++;
     } else {

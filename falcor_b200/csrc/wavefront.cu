@@ -274,9 +274,35 @@ __global__ void wf_sort_scatter(WaveParams wp, uint32_t* bins, uint32_t* out) {
     }
 }
 
-// Moves the extension queue into the shade queue for the next bounce.
+// handleMiss for the paths of the miss queue (hit/miss split): the short
+// environment-light branch of the shade stage, run apart so that the shade
+// kernel's warps hold hits only.
+template <class SG>
+__global__ void __launch_bounds__(kShadeBlock) wf_miss(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+    Counters cnt;
+    const uint32_t n = wp.counts[kMissCount];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = wp.missQueue[k];
+        PathState<SG> path;
+        load_path(w, i, path);
+        pt_handle_miss<SG>(s, p, path, cnt);
+        store_path(w, i, path);
+        if (!path.has(PF_ACTIVE)) cnt.v[0]++;
+    }
+    flush_counters(p.counters, cnt);
+}
+
+// Moves the extension queue (or, with the hit/miss split, the next-bounce hit
+// and miss queues) into the shade (and miss) queue for the next bounce.
 __global__ void wf_advance(WaveParams wp) {
-    wp.counts[0] = wp.counts[1];
+    if (wp.nextHitQueue) {
+        wp.counts[0] = wp.counts[kNextHitCount];
+        wp.counts[kMissCount] = wp.counts[kNextMissCount];
+        wp.counts[kNextHitCount] = 0;
+        wp.counts[kNextMissCount] = 0;
+    } else {
+        wp.counts[0] = wp.counts[1];
+    }
     wp.counts[1] = 0;
     wp.counts[2] = 0;
     wp.counts[kFetchExtend] = 0;
@@ -307,6 +333,8 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
     // order, already coherent).
     const bool sortQueue = p.sortMaterials && b.owning && b.ensure_sort() == cudaSuccess;
     const uint32_t sortBins = std::min<uint32_t>(std::max<uint32_t>(s.materialCount, 1u), WavefrontBuffers::kMaxSortBins - 1u) + 1u;
+    // Hit/miss split of the shade stage.
+    const bool split = p.splitMisses && b.owning && b.ensure_split() == cudaSuccess;
     const uint32_t maxIter = p.maxSurfaceBounces + 2;
     for (uint32_t first = 0; first < pixels; first += wavePixels) {
         WaveParams wp{};
@@ -323,6 +351,13 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
         wp.shadowQueue = b.shadowQueue;
         wp.sortKeys = sortQueue ? b.sortKeys : nullptr;
         wp.sortBins = sortBins;
+        uint32_t* qHit = qa;
+        uint32_t* qMiss = b.missQueue;
+        uint32_t* qNextHit = b.nextHitQueue;
+        uint32_t* qNextMiss = b.nextMissQueue;
+        wp.missQueue = split ? qMiss : nullptr;
+        wp.nextHitQueue = split ? qNextHit : nullptr;
+        wp.nextMissQueue = split ? qNextMiss : nullptr;
         const int genBlocks = std::min<int>(gGen, int((wp.wavePaths + kShadeBlock - 1) / kShadeBlock));
         T0(KC_GENERATE);
         wf_generate<SG, false><<<genBlocks, kShadeBlock, 0, st>>>(s, p, wp, w);
@@ -340,6 +375,7 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
             }
             T0(KC_SHADE);
             wf_shade<SG, HAS_T, false><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
+            if (split && it > 0) wf_miss<SG><<<gGen, kShadeBlock, 0, st>>>(s, p, wp, w);
             T1();
             T0(KC_SHADOW);
             if (shortStack) wf_shadow<kShortStack><<<gTraceShort, kTraceBlock, 0, st>>>(s, p, wp, w);
@@ -350,9 +386,20 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
             else wf_extend<kStackSize><<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
             T1();
             wf_advance<<<1, 1, 0, st>>>(wp);
-            std::swap(qa, qb);
-            wp.shadeQueue = qa;
-            wp.extQueue = qb;
+            if (split) {
+                // Hits of this bounce are the next shade queue; the extension
+                // queue buffer is reused as is.
+                std::swap(qHit, qNextHit);
+                std::swap(qMiss, qNextMiss);
+                wp.shadeQueue = qHit;
+                wp.missQueue = qMiss;
+                wp.nextHitQueue = qNextHit;
+                wp.nextMissQueue = qNextMiss;
+            } else {
+                std::swap(qa, qb);
+                wp.shadeQueue = qa;
+                wp.extQueue = qb;
+            }
         }
         T0(KC_RESOLVE);
         wf_collect<false><<<gGen, 256, 0, st>>>(p, wp, w);
@@ -466,11 +513,30 @@ cudaError_t WavefrontBuffers::ensure(uint32_t cap) {
 void WavefrontBuffers::release() {
     if (base && owning) cudaFree(base);
     if (sortBase) cudaFree(sortBase);
+    if (splitBase) cudaFree(splitBase);
     base = nullptr;
     capacity = 0;
     sortBase = nullptr;
     sortCapacity = 0;
     sortKeys = sortQueue = sortBins = nullptr;
+    splitBase = nullptr;
+    splitCapacity = 0;
+    missQueue = nextHitQueue = nextMissQueue = nullptr;
+}
+
+cudaError_t WavefrontBuffers::ensure_split() {
+    if (!owning) return cudaErrorNotSupported;
+    if (splitBase && splitCapacity >= capacity) return cudaSuccess;
+    if (splitBase) cudaFree(splitBase);
+    splitBase = nullptr;
+    splitCapacity = 0;
+    cudaError_t e = cudaMalloc(&splitBase, 3 * size_t(capacity) * sizeof(uint32_t));
+    if (e != cudaSuccess) { splitBase = nullptr; return e; }
+    splitCapacity = capacity;
+    missQueue = static_cast<uint32_t*>(splitBase);
+    nextHitQueue = missQueue + capacity;
+    nextMissQueue = nextHitQueue + capacity;
+    return cudaSuccess;
 }
 
 cudaError_t WavefrontBuffers::ensure_sort() {

@@ -31,9 +31,17 @@ struct WavefrontBuffers {
     uint32_t* sortQueue = nullptr;
     uint32_t* sortBins = nullptr;  // kMaxSortBins counts + kMaxSortBins cursors
     static constexpr uint32_t kMaxSortBins = 1024;
+    // Hit/miss split of the shade stage (owning mode only): the extension
+    // kernel pushes hits and misses into separate next-bounce queues.
+    void* splitBase = nullptr;
+    uint32_t splitCapacity = 0;
+    uint32_t* missQueue = nullptr;
+    uint32_t* nextHitQueue = nullptr;
+    uint32_t* nextMissQueue = nullptr;
     float4* f4(int k) const { return arrays + size_t(k) * capacity; }
     cudaError_t ensure(uint32_t capacity);
     cudaError_t ensure_sort();
+    cudaError_t ensure_split();
     void release();
     ~WavefrontBuffers() { release(); }
 

@@ -18,7 +18,10 @@ constexpr int kShadeBlock = 128;
 
 // Counts: [0] shade queue, [1] extension queue, [2] shadow queue, [4] and [5]
 // the fetch counters of the extension and visibility ray kernels.
+// Wave counters: [0] shade (hit) queue, [1] extension, [2] shadow, [3] miss
+// queue, [4]/[5] fetch cursors, [6]/[7] next-bounce hit / miss queues.
 constexpr int kFetchExtend = 4, kFetchShadow = 5, kNumWaveCounts = 8;
+constexpr int kMissCount = 3, kNextHitCount = 6, kNextMissCount = 7;
 struct WaveParams {
     uint32_t waveFirstPixel;   // first pixel of the wave
     uint32_t wavePixels;       // pixels in the wave
@@ -31,6 +34,11 @@ struct WaveParams {
     // sort key of queue position k to sortKeys[k] (null: no sort).
     uint32_t* sortKeys;
     uint32_t sortBins;         // material bins + 1 miss bin
+    // Hit/miss split (null: the extension queue itself becomes the next
+    // shade queue, hits and misses mixed).
+    const uint32_t* missQueue;
+    uint32_t* nextHitQueue;
+    uint32_t* nextMissQueue;
     // Batched waves only: per-request scenes/frames, this wave's tiles, slot -> tile.
     const DevScene* scenes;
     const FrameParams* frames;
@@ -101,15 +109,23 @@ FPT_D void store_path(const SoA& w, uint32_t i, const PathState<SG>& path) {
 }
 
 // Warp-aggregated push of `item` onto queue q (count at *cnt).
-FPT_D void push(bool pred, uint32_t item, uint32_t* q, uint32_t* cnt) {
-    const uint32_t mask = __ballot_sync(__activemask(), pred);
-    if (mask == 0) return;
+// Returns the queue position of the pushed item (or 0xffffffff).  The lanes
+// taking part are those converged at the call, read once: the ballot and the
+// shuffle run over the same set even where the caller's control flow has
+// split the warp.
+FPT_D uint32_t push(bool pred, uint32_t item, uint32_t* q, uint32_t* cnt) {
+    const uint32_t group = __activemask();
+    const uint32_t mask = __ballot_sync(group, pred);
+    if (mask == 0) return 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u;
     const int leader = __ffs(mask) - 1;
     uint32_t base = 0;
     if (int(lane) == leader) base = atomicAdd(cnt, uint32_t(__popc(mask)));
-    base = __shfl_sync(__activemask(), base, leader);
-    if (pred) q[base + uint32_t(__popc(mask & ((1u << lane) - 1u)))] = item;
+    base = __shfl_sync(group, base, leader);
+    if (!pred) return 0xffffffffu;
+    const uint32_t pos = base + uint32_t(__popc(mask & ((1u << lane) - 1u)));
+    q[pos] = item;
+    return pos;
 }
 
 // Ray tracing kernels (visibility and extension rays) with per-lane dynamic
@@ -120,7 +136,7 @@ FPT_D void push(bool pred, uint32_t item, uint32_t* q, uint32_t* cnt) {
 // rays of very different lengths share a warp without leaving most of its
 // lanes idle until the longest ray is done.
 #ifndef FPT_REFILL_BELOW
-#define FPT_REFILL_BELOW 24
+#define FPT_REFILL_BELOW 28
 #endif
 #ifndef FPT_TRACE_MIN_BLOCKS
 #define FPT_TRACE_MIN_BLOCKS 6
@@ -220,10 +236,17 @@ FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams
                         } else {
                             f &= ~0x2u;
                         }
-                        if (!MULTI && wp.sortKeys) {
+                        if (!MULTI) {
                             // Material bin of the hit (misses in the last bin).
                             const uint32_t last = wp.sortBins - 1u;
-                            wp.sortKeys[qpos] = h.valid ? min(__ldg(&s.instances[h.instanceID].materialID), last - 1u) : last;
+                            const uint32_t key = h.valid ? min(__ldg(&s.instances[h.instanceID].materialID), last - 1u) : last;
+                            if (wp.nextHitQueue) {
+                                const uint32_t pos = push(h.valid, path, wp.nextHitQueue, wp.counts + kNextHitCount);
+                                push(!h.valid, path, wp.nextMissQueue, wp.counts + kNextMissCount);
+                                if (wp.sortKeys && h.valid) wp.sortKeys[pos] = key;
+                            } else if (wp.sortKeys) {
+                                wp.sortKeys[qpos] = key;
+                            }
                         }
                         float4 d = w.dirV[path];
                         d.w = __uint_as_float(f);
