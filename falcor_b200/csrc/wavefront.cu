@@ -119,8 +119,17 @@ FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uin
 #ifndef FPT_SHADE_MIN_BLOCKS
 #define FPT_SHADE_MIN_BLOCKS 6  // 80 registers (some spills) beat 126 registers at 4 blocks by 8 %
 #endif
-template <class SG, bool HAS_T, bool MULTI>
-__global__ void __launch_bounds__(kShadeBlock, FPT_SHADE_MIN_BLOCKS) wf_shade(DevScene s, FrameParams p, WaveParams wp, SoA w) {
+// ES >= 0: the emissive sampler (0 Uniform, 1 LightBVH, 2 Power) fixed at
+// compile time, so that the code of the other two samplers is not in the
+// kernel (a smaller kernel stalls less on instruction fetch); -1: read from
+// the frame parameters.
+#ifndef FPT_SPECIALIZE_SAMPLER
+#define FPT_SPECIALIZE_SAMPLER 1
+#endif
+template <class SG, bool HAS_T, bool MULTI, int ES = -1>
+__global__ void __launch_bounds__(kShadeBlock, FPT_SHADE_MIN_BLOCKS) wf_shade(DevScene s, FrameParams pk, WaveParams wp, SoA w) {
+    FrameParams p = pk;
+    if (ES >= 0) p.emissiveSampler = uint32_t(ES);
     Counters cnt;
     const uint32_t n = wp.counts[0];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k - threadIdx.x < n; k += gridDim.x * blockDim.x) {
@@ -324,6 +333,7 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
     static int gShade = 0, gTrace = 0, gTraceShort = 0, gGen = 0;
     if (!gShade) {
         gShade = blocks_for(reinterpret_cast<const void*>(wf_shade<SG, HAS_T, false>), kShadeBlock);
+        // The specialised variants have the same launch bounds.
         gTrace = blocks_for(reinterpret_cast<const void*>(wf_extend<kStackSize>), kTraceBlock);
         gTraceShort = blocks_for(reinterpret_cast<const void*>(wf_extend<kShortStack>), kTraceBlock);
         gGen = blocks_for(reinterpret_cast<const void*>(wf_generate<SG, false>), kShadeBlock);
@@ -374,7 +384,10 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
                 wp.shadeQueue = b.sortQueue;
             }
             T0(KC_SHADE);
-            wf_shade<SG, HAS_T, false><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
+            if (FPT_SPECIALIZE_SAMPLER && p.emissiveSampler == 2) wf_shade<SG, HAS_T, false, 2><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
+            else if (FPT_SPECIALIZE_SAMPLER && p.emissiveSampler == 1) wf_shade<SG, HAS_T, false, 1><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
+            else if (FPT_SPECIALIZE_SAMPLER && p.emissiveSampler == 0) wf_shade<SG, HAS_T, false, 0><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
+            else wf_shade<SG, HAS_T, false><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
             if (split && it > 0) wf_miss<SG><<<gGen, kShadeBlock, 0, st>>>(s, p, wp, w);
             T1();
             T0(KC_SHADOW);
