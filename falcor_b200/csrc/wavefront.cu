@@ -117,7 +117,10 @@ FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uin
 // handleHit / handleMiss for every path of the shade queue.  The hit flag of
 // a path is PF_HIT (0x2) in its flags.
 #ifndef FPT_SHADE_MIN_BLOCKS
-#define FPT_SHADE_MIN_BLOCKS 6  // 80 registers (some spills) beat 126 registers at 4 blocks by 8 %
+// 8 resident blocks (64 registers, spills to L1) measured best on the 1080p
+// heightfield frame with the sampler-specialised kernel: shading 18.77 ms per
+// frame at 6 blocks (80 registers), 17.88 at 7, 17.68 at 8, 19.51 at 5.
+#define FPT_SHADE_MIN_BLOCKS 8
 #endif
 // ES >= 0: the emissive sampler (0 Uniform, 1 LightBVH, 2 Power) fixed at
 // compile time, so that the code of the other two samplers is not in the
