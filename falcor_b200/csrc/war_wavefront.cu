@@ -79,6 +79,14 @@ FPT_D bool nonzero(float3 v) { return v.x != 0.f || v.y != 0.f || v.z != 0.f; }
 
 // Seeds the wave: camera ray of pixel waveFirstPixel + i (tracePaths,
 // WARDiffPathTracer.rt.slang:115-143 and tracePath :75-112).
+// Resident blocks per SM of the adjoint's shading kernels (registers are
+// capped accordingly).  Uncapped they took up to 255 registers (2 blocks per
+// SM); on the displaced-sphere adjoint 4 blocks measured best: replay adjoint
+// 168.5 -> 176 Mpaths/s, with the boundary term 16.8 -> 19.1, checkpointed
+// forward + adjoint 142.8 -> 149.
+#ifndef FPT_WW_MIN_BLOCKS
+#define FPT_WW_MIN_BLOCKS 4
+#endif
 template <bool BWD>
 __global__ void __launch_bounds__(kShadeBlock) ww_generate(DevScene s, WarParams p, WaveParams wp, SoA w, WarWave ww) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePixels; i += gridDim.x * blockDim.x) {
@@ -111,7 +119,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_generate(DevScene s, WarParams
 
 // handleHit for every path of the shade queue whose extension ray hit.
 template <bool HAS_T, bool BWD, bool WAR>
-__global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p, WaveParams wp, SoA w, WarWave ww) {
+__global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_shade(DevScene s, WarParams p, WaveParams wp, SoA w, WarWave ww) {
     constexpr int NJ = WAR ? 17 : 14;  // NEE Jacobian: material, wo and (WAR) wi slots
     Counters cnt;
     const bool useEmissive = s.hasEmissive != 0 && s.activeCount > 0;
@@ -316,7 +324,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_shade(DevScene s, WarParams p,
 // NEE ray's reparameterisation and hands the adjoint of the incident
 // direction to the vertex record.
 template <bool WAR>
-__global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(DevScene s, WarParams p, WaveParams wp, SoA w, WarWave ww) {
+__global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_nee_grad(DevScene s, WarParams p, WaveParams wp, SoA w, WarWave ww) {
     __shared__ uint2 stackMem[WAR ? kStackSize * kShadeBlock : 1];
     uint2* stack = stackMem + threadIdx.x;
     const uint32_t n = wp.counts[2];
@@ -368,7 +376,7 @@ __global__ void __launch_bounds__(kShadeBlock) ww_nee_grad(DevScene s, WarParams
 // Reverse sweep over each path's records (war_sweep_vertex), then the
 // screen-sample reparameterisation (WAR).
 template <bool HAS_T, bool WAR>
-__global__ void __launch_bounds__(kShadeBlock) ww_sweep(DevScene s, WarParams p, WaveParams wp, WarWave ww) {
+__global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_sweep(DevScene s, WarParams p, WaveParams wp, WarWave ww) {
     __shared__ uint2 stackMem[WAR ? kStackSize * kShadeBlock : 1];
     uint2* stack = stackMem + threadIdx.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePixels; i += gridDim.x * blockDim.x) {
