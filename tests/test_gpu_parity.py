@@ -105,8 +105,10 @@ def test_path_tracer_per_sample_parity(torch_cuda, oracle):
     assert st.device_error == 0
 
 
-def test_path_tracer_material_sort_same_samples(torch_cuda):
-    """sortShadeQueue reorders the shade queue only: every sample is unchanged."""
+@pytest.mark.parametrize("option", ["sortShadeQueue", "splitMisses"])
+def test_path_tracer_queue_options_same_samples(torch_cuda, option):
+    """sortShadeQueue (material sort of the shade queue) and splitMisses (misses
+    shaded by their own kernel) reorder work only: every sample is unchanged."""
     torch = torch_cuda
     from falcor_b200.scene import Scene
     from falcor_b200.passes import PathTracer
@@ -115,12 +117,12 @@ def test_path_tracer_material_sort_same_samples(torch_cuda):
     W, Hh, spp = 64, 48, 4
     vb = H.gpu_vbuffer(scene, W, Hh)
     out = []
-    for sort in (0, 1):
-        pt = PathTracer(dict(H.pt_props(spp, max_bounces=4, seed=3), sortShadeQueue=sort))
+    for on in (0, 1):
+        pt = PathTracer(dict(H.pt_props(spp, max_bounces=4, seed=3), **{option: on}))
         pt.set_scene(scene)
         color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
         samples = torch.zeros((Hh, W, spp, 3), dtype=torch.float32, device="cuda")
         pt.execute({"vbuffer": vb, "color": color}, sample_color=samples)
         torch.cuda.synchronize()
-        out.append((samples.cpu().numpy(), pt.stats().launches if hasattr(pt.stats(), "launches") else 0))
-    np.testing.assert_array_equal(out[0][0], out[1][0])
+        out.append(samples.cpu().numpy())
+    np.testing.assert_array_equal(out[0], out[1])
