@@ -47,7 +47,7 @@ def parse_args():
     ap.add_argument("--resolution", default=None, help="WxH override of the workload's frame size (small profiling cases)")
     ap.add_argument("--frames-per-step", type=int, default=FRAMES_PER_STEP, help="16-spp frames per step")
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched secondary metrics")
-    ap.add_argument("--only", choices=["adjoint", "batched"], default=None,
+    ap.add_argument("--only", choices=["adjoint", "batched", "inverse"], default=None,
                     help="run one secondary metric alone and print it (profiling entry point)")
     return ap.parse_args()
 
@@ -196,6 +196,59 @@ def _time_ms(fn, reps: int) -> float:
     return e0.elapsed_time(e1) / reps
 
 
+def inverse_bench(dev, iterations: int = 50) -> dict:
+    """Inverse-rendering loop: Adam (lr 1e-2) over the 50 625 per-vertex normal
+    displacements and the base colour of a 100 352-triangle grid, 8 views per
+    iteration at 256 x 256, 8 spp, 4 bounces, forward + adjoint per view with
+    the warped-area boundary term (the displacements move silhouettes); the
+    same loop with path replay and with checkpointed path vertices.  Targets are
+    rendered once at 64 spp; every iteration draws fresh sample seeds.  Reports the
+    time per iteration, the forward + adjoint path rate, the loss reduction, the
+    device memory the mode holds at the end of its loop (scene, pass buffers,
+    torch tensors; measured from an emptied allocator cache) and the bytes of
+    stored path vertices."""
+    import gc
+    import torch
+    from falcor_b200.inverse import InverseLoop, displaced_grid_scene, orbit_cameras
+    from falcor_b200.scene import Scene
+    out = {"workload": "displaced grid 100k tris, 8 views 256x256, 8 spp, 4 bounces, WAR adjoint, Adam lr 1e-2, "
+                       f"{iterations} iterations", "unit": "ms per iteration"}
+    for mode in ("Replay", "Checkpoint"):
+        gc.collect()
+        torch.cuda.empty_cache()
+        torch.cuda.synchronize()
+        free0, total = torch.cuda.mem_get_info(dev)
+        scene = Scene(displaced_grid_scene(res=224))
+        loop = InverseLoop(scene, 0, orbit_cameras(8), 256, 256, spp=8, max_bounces=4, adjoint_mode=mode, lr=1e-2)
+        p0 = loop.p0
+        loop.render_targets(0.03 * torch.sin(4.0 * p0[:, 0]) * torch.cos(4.0 * p0[:, 2]),
+                            (loop.color.detach() * 0.8 + 0.1).clamp(0, 1), spp=64)
+        loop.step()  # warm-up: allocations, checkpoint buffers
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        losses = []
+        a.record()
+        for _ in range(iterations):
+            losses.append(loop.step())
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / iterations
+        free1, _ = torch.cuda.mem_get_info(dev)
+        paths = 8 * 256 * 256 * 8
+        key = mode.lower()
+        out[key] = {"ms_per_iteration": round(ms, 3), "fwd_plus_adjoint_Mpaths_s": round(paths / (ms / 1e3) / 1e6, 2),
+                    "loss_first": losses[0], "loss_last": losses[-1],
+                    "device_mb_in_use": round((free0 - free1) / 2**20, 1)}
+        st = loop.renderer.pt.stats()
+        out[key]["checkpoint_mb"] = round(st.checkpoint_bytes / 2**20, 1)
+        if mode == "Checkpoint":
+            out[key]["checkpoint_used"] = int(st.adjoint_checkpointed)
+        del loop, scene
+        gc.collect()
+        torch.cuda.synchronize()
+    return out
+
+
 def adjoint_bench(dev) -> dict:
     """WARDiffPathTracer forward + adjoint on the displaced-sphere workload:
     512 x 512, one path per pixel per frame, 16 frames per step, maxBounces 4,
@@ -338,7 +391,7 @@ def main():
         build.build()
         dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
         torch.cuda.set_device(dev)
-        res = adjoint_bench(dev) if args.only == "adjoint" else batched_bench(dev)
+        res = {"adjoint": adjoint_bench, "batched": batched_bench, "inverse": inverse_bench}[args.only](dev)
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps({args.only: res}), flush=True)
         return
@@ -481,6 +534,7 @@ def main():
         # Secondary metrics of the same run (every rank does its own replica).
         line["adjoint"] = adjoint_bench(dev)
         line["batched"] = batched_bench(dev)
+        line["inverse"] = inverse_bench(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, desc = cpu_baseline(w.name, args.cpu_seconds)
         line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpaths/s", "cores": cores, "kind": "port", "sample": desc}

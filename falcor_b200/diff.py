@@ -162,12 +162,17 @@ class DiffRenderer:
         self.pt.execute({"color": self.color})
         return self.color[..., :3].clone()
 
-    def gradients(self, grad_img, frame_seed: int, position_dim: int = 0):
+    def gradients(self, grad_img, frame_seed: int, position_dim: int = 0, normal_dim: int = 0):
+        """Material gradients and, with position_dim / normal_dim > 0, the
+        gradients of the optimised mesh's vertex positions / normals (3 floats
+        per vertex; the normal gradients are kept in ``normal_grad``)."""
         import torch
         self.pt.set_properties({"fixedSeed": int(frame_seed)})
         gm = torch.zeros(self.material_count * 20, dtype=torch.float32, device="cuda")
         gp = torch.zeros(max(position_dim, 1), dtype=torch.float32, device="cuda") if position_dim else None
+        gn = torch.zeros(normal_dim, dtype=torch.float32, device="cuda") if normal_dim else None
         dLdI = grad_img[..., :3].contiguous().float()
-        self.pt.backward({"color": self.color}, dLdI, material_grad=gm, position_grad=gp)
+        self.pt.backward({"color": self.color}, dLdI, material_grad=gm, position_grad=gp, normal_grad=gn)
         self.position_grad = gp
+        self.normal_grad = gn
         return gm, gp
