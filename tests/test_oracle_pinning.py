@@ -5,7 +5,7 @@ oracle/_ref/kat_runner is built (by __graft_entry__.build() or
 (Tests/Sampling/PseudorandomTests.cpp, Tests/Utils/HashUtilsTests.cpp,
 Tests/Utils/BitTricksTests.cpp, Tests/Utils/GeometryHelpersTests.cpp) and the
 reference's Utils/Math/Float16.cpp; the tests' Slang programs are replaced by
-the oracle, so the reference's own EXPECT_EQ checks judge the oracle.
+the oracle, so the reference's own EXPECT_EQ checks decide whether the oracle passes.
 """
 import subprocess
 from pathlib import Path
