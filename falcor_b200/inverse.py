@@ -32,7 +32,6 @@ does not differentiate them either), so the colour parameters are per material.
 """
 from __future__ import annotations
 
-import ctypes as C
 import math
 
 import numpy as np
