@@ -76,3 +76,63 @@ def test_inverse_displacement_gradient_points_to_target(fpt):
     g = loop._solve(gd, torch.zeros_like(gd))
     corr = float(torch.nn.functional.cosine_similarity(-g, d_target, dim=0))
     assert corr > 0.1, corr
+
+
+def _grid_loop(res):
+    """An InverseLoop shell over a flat grid on the CPU (no scene, no renderer):
+    enough for the Laplacian solve and the normal recomputation."""
+    import torch
+    from falcor_b200.inverse import InverseLoop
+    loop = InverseLoop.__new__(InverseLoop)
+    n = res + 1
+    i = np.arange(res)
+    a = (i[None, :] + n * i[:, None]).ravel()
+    loop.tri = torch.from_numpy(np.stack([a, a + n, a + 1, a + 1, a + n, a + n + 1], 1).reshape(-1, 3)).long()
+    loop.nv = n * n
+    e = torch.cat([loop.tri[:, [0, 1]], loop.tri[:, [1, 2]], loop.tri[:, [2, 0]]])
+    loop.edges = torch.unique(torch.sort(e, dim=1).values, dim=0)
+    loop.degree = torch.zeros(loop.nv)
+    loop.degree.index_add_(0, loop.edges[:, 0], torch.ones(len(loop.edges)))
+    loop.degree.index_add_(0, loop.edges[:, 1], torch.ones(len(loop.edges)))
+    loop.smoothing = 20.0
+    xs = torch.linspace(-1, 1, n)
+    X, Z = torch.meshgrid(xs, xs, indexing="xy")
+    loop.p0 = torch.stack([X.ravel(), torch.zeros(n * n), Z.ravel()], 1)
+    return loop
+
+
+def test_large_steps_solve():
+    """(I + lambda L) x = b by conjugate gradients; the solution is smoother than b."""
+    import torch
+    loop = _grid_loop(30)
+    b = torch.randn(loop.nv, generator=torch.Generator().manual_seed(0))
+    x = loop._solve(b, torch.zeros(loop.nv))
+    assert float((loop._system(x) - b).norm() / b.norm()) < 1e-4
+    rough = lambda v: float((v[1:] - v[:-1]).abs().mean())
+    assert rough(x) < 0.05 * rough(b)
+    # Warm start from the solution returns it.
+    x2 = loop._solve(b, x)
+    assert torch.allclose(x, x2)
+
+
+def test_displacement_chain_rule_matches_finite_differences():
+    """d/dd of sum(g_p . p(d)) + sum(g_n . n(p(d))) for p = p0 + d n0, n = the
+    area-weighted vertex normals, against central differences."""
+    import torch
+    loop = _grid_loop(6)
+    n0 = loop._normals(loop.p0)
+    gen = torch.Generator().manual_seed(1)
+    gp, gn = torch.randn(loop.nv, 3, generator=gen), torch.randn(loop.nv, 3, generator=gen)
+    d0 = 0.05 * torch.randn(loop.nv, generator=gen)
+
+    def f(d):
+        p = loop.p0 + d[:, None] * n0
+        return (gp * p).sum() + (gn * loop._normals(p)).sum()
+
+    d = d0.clone().requires_grad_(True)
+    g, = torch.autograd.grad(f(d), d)
+    for k in (3, 17, 30):
+        e = torch.zeros(loop.nv)
+        e[k] = 1e-3
+        fd = (f(d0 + e) - f(d0 - e)) / 2e-3
+        assert abs(float(g[k]) - float(fd)) < 1e-3 * max(1.0, abs(float(fd)))
