@@ -9,7 +9,6 @@
 // file-scope device array.  The array is part of the library image: every GPU
 // that loads the library holds it until the process exits.
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "kernels.cuh"
@@ -25,34 +24,25 @@ namespace {
 // kNoAllocPaths / spp pixels.
 constexpr uint32_t kNoAllocPaths = 16384;
 constexpr size_t kHeaderBytes = 256;  // event counters, work counter
-constexpr size_t kNoAllocBytes =
-    kHeaderBytes + WavefrontBuffers::kFloat4Arrays * size_t(kNoAllocPaths) * 16 + size_t(kNoAllocPaths) * 12 +
-    3 * size_t(kNoAllocPaths) * 4 + 256;  // = WavefrontBuffers::bytes_for(kNoAllocPaths) + header (2.88 MiB)
+constexpr size_t kNoAllocBytes = kHeaderBytes + WavefrontBuffers::bytes_for(kNoAllocPaths);  // 2.88 MiB
 constexpr uint32_t kNoAllocMaxDim = 4096;  // PathTracer kMaxFrameDimension (Params.slang:68)
+constexpr uint32_t kMaxSpp = 16;           // PathTracer kMaxSamplesPerPixel (Params.slang:67)
+static_assert(kMaxSpp <= kNoAllocPaths, "one pixel's samples must fit one wave");
+static_assert(kWorkCounterOffset + sizeof(uint32_t) <= kHeaderBytes, "work counter inside the header");
 
 __device__ __align__(256) unsigned char g_noallocScratch[kNoAllocBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-void* g_devPtr[kMaxDevices] = {nullptr};
-
 // Device address of the scratch array on the current device.  The array's
-// name in host code is only a host-side stand-in, so the address must come
-// from cudaGetSymbolAddress, once per device, with that device current.
+// name in host code is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress with the calling device current.  It is looked up on
+// every call (a host-side query, no stream work), so it stays valid after a
+// cudaDeviceReset reloads the module.  The first call on a device loads the
+// library's module there; make it before any stream capture.
 fpt_status scratch_address(void** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) return set_error(FPT_ERR_UNSUPPORTED, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_devPtr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noallocScratch);
-        if (e != cudaSuccess || !p)
-            return set_error(FPT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_devPtr[dev] = p;
-    }
-    *out = g_devPtr[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
+    if (e != cudaSuccess || !p) return set_error(FPT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    *out = p;
     return FPT_OK;
 }
 
@@ -75,6 +65,8 @@ FPT_API fpt_status fpt_pass_execute_noalloc(fpt_pass* pass, const fpt_frame_io* 
         return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_execute_noalloc: frame " + std::to_string(io->width) + "x" +
                                                   std::to_string(io->height) + " exceeds the maximum of " +
                                                   std::to_string(kNoAllocMaxDim) + "x" + std::to_string(kNoAllocMaxDim));
+    if (pass->str("scheduler") == "Megakernel")
+        return set_error(FPT_ERR_UNSUPPORTED, "fpt_pass_execute_noalloc: the Megakernel scheduler is not available without allocation");
     void* scratch = nullptr;
     fpt_status s = scratch_address(&scratch);
     if (s != FPT_OK) return s;
@@ -94,12 +86,13 @@ FPT_API fpt_status fpt_pass_execute_noalloc(fpt_pass* pass, const fpt_frame_io* 
     fp.workCounter = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + kWorkCounterOffset);
     fp.workItems = io->width * io->height;
     path_tracer_params(*pass, fp);
-    if (fp.spp > kNoAllocPaths) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_execute_noalloc: too many samples per pixel");
+    // sortShadeQueue and splitMisses need pass-owned queues; they only reorder
+    // work (the samples are the same), so the static layout runs without them.
+    fp.sortMaterials = false;
+    fp.splitMisses = false;
     // The event counters start at zero; the queue counts are cleared per wave.
     cudaError_t e = cudaMemsetAsync(scratch, 0, kHeaderBytes, st);
     if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, cudaGetErrorString(e));
-    if (WavefrontBuffers::bytes_for(kNoAllocPaths) + kHeaderBytes > kNoAllocBytes)
-        return set_error(FPT_ERR_UNSUPPORTED, "fpt_pass_execute_noalloc: scratch layout larger than the static array");
     WavefrontBuffers view;
     view.view(static_cast<char*>(scratch) + kHeaderBytes, kNoAllocPaths);
     e = launch_path_tracer_wavefront(pass->scene->dev, fp, view, st);

@@ -114,10 +114,11 @@ void set_defaults(fpt_pass& p) {
         d["colorFormat"] = PropValue::str("LogLuvHDR");
         d["diffuseBrdf"] = PropValue::str("Frostbite");
         // Scheduling of this implementation (no reference counterpart):
-        // "Wavefront" (default) or "Megakernel"; paths in flight per wave.  A
-        // 1920x1080 16-spp frame (33.2 M paths) fits one wave of 2^25 paths
-        // (5.6 GB of path state): every bounce then runs once per frame, which
-        // on that frame is 1.5x faster than four waves of 2^23.
+        // "Wavefront" (default) or "Megakernel"; the most paths in flight per
+        // wave.  A 1920x1080 16-spp frame (33.2 M paths) fits one wave of 2^25
+        // paths (6.2 GB of path state at 184 B per path): every bounce then
+        // runs once per frame, which on that frame is 1.5x faster than four
+        // waves of 2^23.  Smaller frames allocate only what they use.
         d["scheduler"] = PropValue::str("Wavefront");
         d["wavefrontCapacity"] = PropValue::num(1 << 25);
         // CUDA-event timing of each wavefront kernel category (fpt_pass_get_kernel_times).
@@ -644,8 +645,12 @@ FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void
             pass->launches = 2;
             e = launch_path_tracer(ds, fp, st);
         } else {
+            // Path state grows to the largest wave this pass has rendered, up to
+            // wavefrontCapacity (184 B per path): a small frame holds little memory.
             const uint32_t cap = uint32_t(std::max(1.0, pass->num("wavefrontCapacity")));
-            e = pass->wavefront.ensure(std::max<uint32_t>(cap, fp.spp));
+            const uint64_t framePaths = uint64_t(fp.width) * fp.height * fp.spp;
+            const uint32_t need = uint32_t(std::min<uint64_t>(cap, std::max<uint64_t>(framePaths, fp.spp)));
+            e = pass->wavefront.ensure(std::max<uint32_t>(need, fp.spp));
             if (e != cudaSuccess) return set_error(FPT_ERR_OOM, std::string("PathTracer: wavefront buffers: ") + cudaGetErrorString(e));
             pass->timer.enabled = pass->num("profileKernels") != 0;
             e = launch_path_tracer_wavefront(ds, fp, pass->wavefront, st, &pass->timer);

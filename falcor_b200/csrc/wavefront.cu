@@ -506,7 +506,7 @@ cudaError_t WavefrontBuffers::ensure(uint32_t cap) {
     if (capacity >= cap && base) return cudaSuccess;
     release();
     const size_t f4Bytes = size_t(cap) * sizeof(float4);
-    const size_t bytes = kFloat4Arrays * f4Bytes + size_t(cap) * 3 * sizeof(float) + 3 * size_t(cap) * sizeof(uint32_t) + 256;
+    const size_t bytes = bytes_for(cap);
     cudaError_t e = cudaMalloc(&base, bytes);
     if (e != cudaSuccess) { base = nullptr; return e; }
     capacity = cap;
@@ -569,10 +569,6 @@ cudaError_t WavefrontBuffers::ensure_sort() {
     sortQueue = sortKeys + capacity;
     sortBins = sortQueue + capacity;
     return cudaSuccess;
-}
-
-size_t WavefrontBuffers::bytes_for(uint32_t cap) {
-    return kFloat4Arrays * size_t(cap) * sizeof(float4) + size_t(cap) * 3 * sizeof(float) + 3 * size_t(cap) * sizeof(uint32_t) + 256;
 }
 
 void WavefrontBuffers::view(void* mem, uint32_t cap) {

@@ -46,7 +46,9 @@ struct WavefrontBuffers {
     ~WavefrontBuffers() { release(); }
 
     // Bytes needed for `capacity` paths in flight.
-    static size_t bytes_for(uint32_t capacity);
+    static constexpr size_t bytes_for(uint32_t cap) {
+        return kFloat4Arrays * size_t(cap) * 16 + size_t(cap) * 3 * sizeof(float) + 3 * size_t(cap) * sizeof(uint32_t) + 256;
+    }
     // Lays the buffers out over `mem` (at least bytes_for(capacity) bytes,
     // 256-byte aligned) without allocating; the view never frees `mem`.
     void view(void* mem, uint32_t capacity);

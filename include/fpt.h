@@ -357,12 +357,17 @@ FPT_API fpt_status fpt_pass_reset(fpt_pass* pass);
  * frame as fpt_pass_execute on a PathTracer pass, with all scratch (path
  * state, queues, counters; 2.88 MiB, 16384 paths in flight per wave) in one
  * static device array that every GPU loading this library holds until exit.
- * Limits: PathTracer passes only, frames up to 4096 x 4096 (larger sizes are
- * rejected with FPT_ERR_INVALID_ARG).  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture.  Calls share the array: calls that overlap on the GPU (other
- * streams, other threads) race and must be serialised by the caller.  The
- * event counters of fpt_pass_get_counters are not updated by this call. */
+ * Limits: PathTracer passes with the Wavefront scheduler only (Megakernel is
+ * rejected with FPT_ERR_UNSUPPORTED), frames up to 4096 x 4096 (larger sizes
+ * are rejected with FPT_ERR_INVALID_ARG).  wavefrontCapacity is replaced by
+ * the fixed 16384 paths; sortShadeQueue and splitMisses are not applied (they
+ * only reorder work, the samples are the same).  Every call looks up the
+ * array's device address (cudaGetSymbolAddress, no stream work) with the
+ * calling device current; the first call on a device loads the library's
+ * module there and should come before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU (other streams, other threads) race
+ * and must be serialised by the caller.  The event counters of
+ * fpt_pass_get_counters are not updated by this call. */
 FPT_API fpt_status fpt_pass_execute_noalloc(fpt_pass* pass, const fpt_frame_io* io, void* stream);
 
 /* Gradient buffers (DiffRendering/SceneGradients.cpp:42-206): caller-owned

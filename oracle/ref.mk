@@ -4,8 +4,9 @@
 # test framework and the oracle standing in for the Slang test programs; plus
 # the reference's Utils/Math/Float16.cpp.  Test infrastructure only; the
 # outputs go to oracle/_ref/ (git-ignored).  Run from oracle/:
-#   make -f ref.mk
-REF ?= /root/reference/Source
+#   make -f ref.mk            (FALCOR_REF names the reference checkout)
+FALCOR_REF ?= /root/reference
+REF ?= $(FALCOR_REF)/Source
 TESTS := $(REF)/Tools/FalcorTest/Tests
 CXX ?= g++
 CXXFLAGS ?= -O2 -std=gnu++17 -ffp-contract=off -Wno-unused-function -Wno-unused-variable

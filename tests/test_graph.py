@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 from falcor_b200.graph import RenderGraph, SceneBuilderFlags, createPass, run_graph_script
+from oracle import ref_tree
 
 MINIMAL_SCRIPT = """
 from falcor import *
@@ -147,10 +148,10 @@ def test_accumulate_properties(fpt):
     assert a.properties["precisionMode"] == "Double"
 
 
-@pytest.mark.skipif(not Path("/root/reference/scripts").exists(), reason="reference tree not present")
+@pytest.mark.skipif(not (ref_tree.root() / "scripts").exists(), reason="reference tree not present")
 def test_reference_graph_scripts_compile(fpt):
     """The reference's own path-tracer graph scripts, unmodified, build and compile."""
-    root = Path("/root/reference")
+    root = ref_tree.root()
     names = ["scripts/MinimalPathTracer.py", "scripts/PathTracer.py", "scripts/WARDiffPathTracer.py"]
     gdir = root / "tests/image_tests/renderpasses/graphs"
     names += [f"tests/image_tests/renderpasses/graphs/{n}" for n in

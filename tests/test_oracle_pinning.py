@@ -15,7 +15,9 @@ import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
 RUNNER = ROOT / "oracle" / "_ref" / "kat_runner"
-REF = Path("/root/reference/Source")
+from oracle import ref_tree
+
+REF = ref_tree.source()
 
 
 def _runner():

@@ -12,6 +12,7 @@ import pytest
 
 from falcor_b200.graph import SceneBuilderFlags
 from falcor_b200.pyscene import (Transform, TriangleMesh, float3, load_pyscene, read_radiance_hdr)
+from oracle import ref_tree
 from tests import helpers as H
 
 ROOM = """
@@ -177,12 +178,12 @@ def test_radiance_hdr_reader(tmp_path):
     np.testing.assert_allclose(img, expect, rtol=1e-7)
 
 
-@pytest.mark.skipif(not Path("/root/reference/Scene/Box/CornellBox.pyscene").exists(), reason="reference tree not present")
+@pytest.mark.skipif(not (ref_tree.root() / "Scene/Box/CornellBox.pyscene").exists(), reason="reference tree not present")
 def test_reference_cornell_box_loads(fpt):
-    hs, b = _load(Path("/root/reference/Scene/Box/CornellBox.pyscene"), aspect=1.0)
+    hs, b = _load(ref_tree.root() / "Scene/Box/CornellBox.pyscene", aspect=1.0)
     assert hs.triangle_count == 36 and hs.desc.instance_count == 8
     assert hs.desc.material_count == 4  # five identical white materials merge
-    hs, b = _load(Path("/root/reference/Scene/Box/CornellBox.pyscene"), flags=SceneBuilderFlags.DontMergeMaterials)
+    hs, b = _load(ref_tree.root() / "Scene/Box/CornellBox.pyscene", flags=SceneBuilderFlags.DontMergeMaterials)
     assert hs.desc.material_count == 8
 
 
