@@ -78,7 +78,8 @@ class fpt_frame_io(C.Structure):
                 ("vbuffer", C.c_void_p), ("color", C.c_void_p), ("ray_count", C.c_void_p), ("path_length", C.c_void_p),
                 ("d_color", C.c_void_p), ("vbuffer_out", C.c_void_p), ("sample_color", C.c_void_p),
                 ("src", C.c_void_p), ("dst", C.c_void_p), ("src_width", u32), ("src_height", u32), ("refresh", u32),
-                ("depth", C.c_void_p), ("mvec", C.c_void_p), ("view_w", C.c_void_p), ("mask", C.c_void_p)]
+                ("depth", C.c_void_p), ("mvec", C.c_void_p), ("view_w", C.c_void_p), ("mask", C.c_void_p),
+                ("hit_trace", C.c_void_p)]
 
 
 class fpt_grad_buffers(C.Structure):
@@ -142,6 +143,7 @@ SIGNATURES = {
     "fpt_pass_execute": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P]),
     "fpt_pass_reset": (C.c_int, [_P]),
     "fpt_pass_execute_noalloc": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P]),
+    "fpt_fmath_eval": (C.c_int, [u32, u32, u32, _P, _P, _P, _P]),
     "fpt_pass_backward": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P, C.POINTER(fpt_grad_buffers), _P]),
     "fpt_scene_gradients_create": (C.c_int, [C.POINTER(fpt_grad_config), u32, C.POINTER(_P)]),
     "fpt_scene_gradients_destroy": (None, [_P]),

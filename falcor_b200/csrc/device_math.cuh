@@ -9,6 +9,7 @@
 // from a CPU libm in the last ulp.
 #pragma once
 
+#include "fmath.h"
 #include <cstdint>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -169,7 +170,9 @@ FPT_D float2 sample_disk_concentric(float2 u) {
     float phi, r;
     if (fabsf(u.x) > fabsf(u.y)) { r = u.x; phi = (u.y / u.x) * kPi_4; }
     else { r = u.y; phi = kPi_2 - (u.x / u.y) * kPi_4; }
-    return make_float2(r * cosf(phi), r * sinf(phi));
+    float sp, cp;
+    fm::sincos(phi, sp, cp);
+    return make_float2(r * cp, r * sp);
 }
 FPT_D float3 sample_cosine_hemisphere_concentric(float2 u, float& pdf) {
     float2 d = sample_disk_concentric(u);
@@ -185,13 +188,13 @@ FPT_D float3 sample_triangle_bary(float2 u) {
 FPT_D float2 world_to_latlong_map(float3 dir) {
     float3 p = normalize(dir);
     float2 uv;
-    uv.x = atan2f(p.x, -p.z) * kInv2Pi + 0.5f;
-    uv.y = acosf(p.y) * kInvPi;
+    uv.x = fm::atan2(p.x, -p.z) * kInv2Pi + 0.5f;
+    uv.y = fm::acos(p.y) * kInvPi;
     return uv;
 }
 FPT_D float2 ndir_to_oct_equal_area_unorm(float3 n) {
     float r = sqrtf(1.f - fabsf(n.z));
-    float phi = atan2f(fabsf(n.y), fabsf(n.x));
+    float phi = fm::atan2(fabsf(n.y), fabsf(n.x));
     float2 p;
     p.y = r * phi * k2OverPi;
     p.x = r - p.y;
@@ -206,8 +209,10 @@ FPT_D float3 oct_to_ndir_equal_area_unorm(float2 p) {
     float r = 1.f - fabsf(d);
     float phi = (r > 0.f) ? ((fabsf(p.y) - fabsf(p.x)) / r + 1.f) * kPi_4 : 0.f;
     float f = r * sqrtf(2.f - r * r);
-    float x = f * sgn(p.x) * cosf(phi);
-    float y = f * sgn(p.y) * sinf(phi);
+    float sp, cp;
+    fm::sincos(phi, sp, cp);
+    float x = f * sgn(p.x) * cp;
+    float y = f * sgn(p.y) * sp;
     float z = sgn(d) * (1.f - r * r);
     return make_float3(x, y, z);
 }
@@ -225,9 +230,11 @@ FPT_D float3 perp_stark(float3 u) {
 FPT_D float3 sample_von_mises_fisher(float2 u, float kappa) {
     const float sy = fmaxf(1.f - u.y, 1e-6f);
     const float phi = 6.28318530717958647692f * u.x;
-    const float cosTheta = 1.f + logf(expf(-2.f * kappa) * (1.f - sy) + sy) / kappa;
+    const float cosTheta = 1.f + fm::log(fm::exp(-2.f * kappa) * (1.f - sy) + sy) / kappa;
     const float sinTheta = sqrtf(1.f - cosTheta * cosTheta);
-    return make_float3(cosf(phi) * sinTheta, sinf(phi) * sinTheta, cosTheta);
+    float sp, cp;
+    fm::sincos(phi, sp, cp);
+    return make_float3(cp * sinTheta, sp * sinTheta, cosTheta);
 }
 // computeRayOrigin (Utils/Geometry/GeometryHelpers.slang:51-68).
 FPT_D float ray_origin_1(float p, float n) {
@@ -247,7 +254,7 @@ FPT_D uint32_t encode_logluv_hdr(float3 c) {
     const float X = 0.4123907992659595f * c.x + 0.3575843393838780f * c.y + 0.1804807884018343f * c.z;
     const float Y = 0.2126390058715104f * c.x + 0.7151686787677559f * c.y + 0.0721923153607337f * c.z;
     const float Z = 0.0193308187155918f * c.x + 0.1191947797946259f * c.y + 0.9505321522496608f * c.z;
-    float logY = 409.6f * (log2f(Y) + 20.f);
+    float logY = 409.6f * (fm::log2(Y) + 20.f);
     float cl = fminf(fmaxf(logY, 0.f), 16383.f);
     uint32_t Le = uint32_t(cl);
     if (Le == 0) return 0;
@@ -261,7 +268,7 @@ FPT_D float3 decode_logluv_hdr(uint32_t p) {
     uint32_t Le = p >> 18;
     if (Le == 0) return f3(0.f);
     float logY = (float(Le) + 0.5f) / 409.6f - 20.f;
-    float Y = powf(2.f, logY);
+    float Y = fm::pow(2.f, logY);
     float u = (float((p >> 9) & 0x1ffu) + 0.5f) / 820.f, v = (float(p & 0x1ffu) + 0.5f) / 820.f;
     float invDenom = 1.f / (6.f * u - 16.f * v + 12.f);
     float x = 9.f * u * invDenom, y = 4.f * v * invDenom;
@@ -307,14 +314,16 @@ FPT_D float3 sample_ggx_vndf(float alpha, float3 wi, float2 u, float& pdf) {
     float phi = 2.f * kPi * u.x;
     float z = fmaf((1.f - u.y), (1.f + Vh.z), -Vh.z);
     float sinTheta = sqrtf(saturate(1.f - z * z));
-    float3 Nh = make_float3(sinTheta * cosf(phi), sinTheta * sinf(phi), z) + Vh;
+    float sp, cp;
+    fm::sincos(phi, sp, cp);
+    float3 Nh = make_float3(sinTheta * cp, sinTheta * sp, z) + Vh;
     float3 h = normalize(make_float3(alpha * Nh.x, alpha * Nh.y, Nh.z));
     pdf = eval_pdf_ggx_vndf(alpha, wi, h);
     return h;
 }
-FPT_D float fresnel_schlick(float f0, float f90, float c) { return f0 + (f90 - f0) * powf(hmax(1.f - c, 0.f), 5.f); }
+FPT_D float fresnel_schlick(float f0, float f90, float c) { return f0 + (f90 - f0) * fm::pow(hmax(1.f - c, 0.f), 5.f); }
 FPT_D float3 fresnel_schlick(float3 f0, float c) {
-    float p = powf(hmax(1.f - c, 0.f), 5.f);
+    float p = fm::pow(hmax(1.f - c, 0.f), 5.f);
     return f0 + (f3(1.f) - f0) * p;
 }
 FPT_D float fresnel_dielectric(float eta, float ci, float& ct) {

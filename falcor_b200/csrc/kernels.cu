@@ -91,7 +91,9 @@ __global__ void __launch_bounds__(kMinimalBlock) minimal_pt_kernel(DevScene s, F
         uint32_t rays = 0;
         const bool useEmissive = s.hasEmissive != 0, useEnv = s.hasEnv != 0;
         const bool lambert = p.lambert != 0, useIS = p.useImportanceSampling != 0;
+        const uint32_t traceLen = p.maxBounces + 2;
         if (unpack_hit(s.bits, __ldg(p.vbuffer + idx), hit)) {
+            if (p.hitTrace) record_vertex(p, 1, traceLen, idx, 0, 1, true, hit);
             ShadingData sd = load_shading_data(s, hit, primaryDir);
             MaterialInstance<HAS_T> mi = material_instance<HAS_T>(s, sd, lambert);
             UniformSG sg;
@@ -122,6 +124,7 @@ __global__ void __launch_bounds__(kMinimalBlock) minimal_pt_kernel(DevScene s, F
                 TraceStats ts;
                 trace_bvh<false>(s, origin, direction, 0.f, 3.402823466e+38f, h, stack, kMinimalBlock, &ts);
                 cnt.trace(false, ts);
+                if (p.hitTrace) record_vertex(p, 1, traceLen, idx, 0, depth + 2, h.valid, h);
                 if (!h.valid) {
                     terminated = true;
                     if (useEnv && (p.computeDirect || pathLength > 0)) radiance += thp * env_eval(s, direction);
@@ -258,6 +261,8 @@ __global__ void __launch_bounds__(kPathBlock) path_tracer_kernel(DevScene s, Fra
         }
 
         // (3) Shading: handleHit / handleMiss.
+        if (p.hitTrace && (state == LS_SHADE || state == LS_MISS))
+            record_vertex(p, spp, p.maxSurfaceBounces + 2, idx, sampleIdx, path.vertexIndex, state == LS_SHADE, path.hit);
         if (state == LS_SHADE) pt_handle_hit<SG, HAS_T>(s, p, path, cnt);
         else if (state == LS_MISS) pt_handle_miss<SG>(s, p, path, cnt);
         if (state == LS_SHADE || state == LS_MISS || state == LS_TRACE) {

@@ -21,6 +21,7 @@ struct FrameParams {
     uint32_t* rayCount;        // optional per-pixel ray count
     uint32_t* pathLength;      // optional per-pixel path length
     float* sampleColor;        // optional per-sample radiance (3 floats)
+    uint4* hitTrace;           // optional per-sample hit of every path vertex (fpt_frame_io::hit_trace)
     uint4* vbufferOut;         // VBufferRT output
     // VBufferRT optional outputs (VBufferRT.slang:69-143) and the camera of the
     // previous frame for the motion vectors.

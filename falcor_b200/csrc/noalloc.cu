@@ -82,6 +82,7 @@ FPT_API fpt_status fpt_pass_execute_noalloc(fpt_pass* pass, const fpt_frame_io* 
     fp.rayCount = io->ray_count;
     fp.pathLength = io->path_length;
     fp.sampleColor = io->sample_color;
+    fp.hitTrace = reinterpret_cast<uint4*>(io->hit_trace);
     fp.counters = static_cast<unsigned long long*>(scratch);
     fp.workCounter = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + kWorkCounterOffset);
     fp.workItems = io->width * io->height;

@@ -612,6 +612,7 @@ FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void
     fp.rayCount = io->ray_count;
     fp.pathLength = io->path_length;
     fp.sampleColor = io->sample_color;
+    fp.hitTrace = reinterpret_cast<uint4*>(io->hit_trace);
     fp.vbufferOut = reinterpret_cast<uint4*>(io->vbuffer_out);
     fp.counters = reinterpret_cast<unsigned long long*>(pass->scratch);
     fp.workCounter = reinterpret_cast<uint32_t*>(static_cast<char*>(pass->scratch) + kWorkCounterOffset);

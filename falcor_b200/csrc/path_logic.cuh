@@ -48,7 +48,7 @@ constexpr uint32_t PF_LIGHT_UPPER = 0x40, PF_LIGHT_LOWER = 0x80;
 FPT_D float eval_mis(const FrameParams& p, float p0, float p1) {
     if (p.misHeuristic == 0) { const float q0 = p0, q1 = p1; return q0 / (q0 + q1); }
     if (p.misHeuristic == 1) { const float q0 = p0 * p0, q1 = p1 * p1; return q0 / (q0 + q1); }
-    const float q0 = powf(p0, p.misPowerExponent), q1 = powf(p1, p.misPowerExponent);
+    const float q0 = fm::pow(p0, p.misPowerExponent), q1 = fm::pow(p1, p.misPowerExponent);
     return q0 / (q0 + q1);
 }
 
@@ -69,6 +69,18 @@ struct PathState {
     FPT_D bool isLightSampled() const { return (flags & (PF_LIGHT_UPPER | PF_LIGHT_LOWER)) != 0; }
     FPT_D bool isLightSamplable() const { return !has(PF_DELTA); }
 };
+
+// Optional record of the hit of path vertex `vertexIndex` (1 = the primary
+// hit) of one sample: (instanceID + 1, primitiveIndex, bary.x, bary.y bits), or
+// zeros for a miss.  `perSample` entries per sample, `spp` samples per pixel
+// (fpt_frame_io::hit_trace).
+FPT_D void record_vertex(const FrameParams& p, uint32_t spp, uint32_t perSample, uint32_t pix, uint32_t sample,
+                         uint32_t vertexIndex, bool valid, const HitRec& h) {
+    if (vertexIndex == 0 || vertexIndex > perSample) return;
+    const uint4 v = valid ? make_uint4(h.instanceID + 1u, h.primIndex, __float_as_uint(h.baryX), __float_as_uint(h.baryY))
+                          : make_uint4(0u, 0u, 0u, 0u);
+    p.hitTrace[(size_t(pix) * spp + sample) * perSample + (vertexIndex - 1)] = v;
+}
 
 FPT_D bool finished_surface_bounces(const FrameParams& p, uint32_t bounces) {
     const uint32_t d = bounces & 0xffu, sp = (bounces >> 8) & 0xffu, tr = (bounces >> 16) & 0xffu;

@@ -137,7 +137,7 @@ FPT_D void war_aux_pass(const DevScene& s, uint32_t n, bool antithetic, float ka
         float bt = dot(nrm, c);
         bt = bt * bt;
         const float sy = fmaxf(1.f - smp.y, 1e-6f);
-        const float invVMF = 1.f / ((1.f - sy) * expf(-2.f * kappa) + sy);
+        const float invVMF = 1.f / ((1.f - sy) * fm::exp(-2.f * kappa) + sy);
         const float wDenom = invVMF - 1.f + bt;
         const float wDenomRcp = wDenom > 1e-4f ? 1.f / wDenom : 0.f;
         a.w = wDenomRcp * wDenomRcp * wDenomRcp * invVMF;
@@ -350,9 +350,11 @@ FPT_D float2 war_camera_sample(const WarParams& p, uint32_t x, uint32_t y, Unifo
     next2D(sg);
     next2D(sg);
     const float2 u = next2D(sg);
-    const float r = sqrtf(-2.f * logf(u.x));
+    const float r = sqrtf(-2.f * fm::log(u.x));
     const float ang = 6.28318530717958647692f * u.y;
-    float jx = (r * cosf(ang)) * 0.5f, jy = (r * sinf(ang)) * 0.5f;
+    float sa, ca;
+    fm::sincos(ang, sa, ca);
+    float jx = (r * ca) * 0.5f, jy = (r * sa) * 0.5f;
     if (p.useAntithetic && p.frameSeed % 2 == 0) {
         jx = -jx;
         jy = -jy;

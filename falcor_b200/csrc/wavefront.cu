@@ -98,9 +98,13 @@ __global__ void __launch_bounds__(kShadeBlock) wf_generate(DevScene s, FramePara
 }
 
 template <class SG, bool HAS_T>
-FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uint32_t i, bool& ext, bool& shadow, Counters& cnt) {
+FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uint32_t i, bool& ext, bool& shadow, Counters& cnt,
+                      const WaveParams* wp = nullptr) {
     PathState<SG> path;
     load_path(w, i, path);
+    if (wp && p.hitTrace)
+        record_vertex(p, p.spp, p.maxSurfaceBounces + 2, wp->waveFirstPixel + i % wp->wavePixels, i / wp->wavePixels, path.vertexIndex,
+                      (path.flags & 0x2u) != 0, path.hit);
     if (path.flags & 0x2u) pt_handle_hit<SG, HAS_T>(s, p, path, cnt);
     else pt_handle_miss<SG>(s, p, path, cnt);
     shadow = path.shadowPending;
@@ -144,7 +148,7 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_SHADE_MIN_BLOCKS) wf_shade(De
                 const uint32_t r = slot_request(wp, i);
                 shade_slot<SG, HAS_T>(wp.scenes[r], wp.frames[r], w, i, ext, shadow, cnt);
             } else {
-                shade_slot<SG, HAS_T>(s, p, w, i, ext, shadow, cnt);
+                shade_slot<SG, HAS_T>(s, p, w, i, ext, shadow, cnt, &wp);
             }
         }
         push(shadow, i, wp.shadowQueue, wp.counts + 2);

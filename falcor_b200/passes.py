@@ -125,7 +125,7 @@ class RenderPass:
     setScene = set_scene
 
     def _io(self, rd: Mapping[str, Any], width: int, height: int, frame: int, prng_dim: int = 0,
-            sample_color=None, refresh: bool = False) -> _ffi.fpt_frame_io:
+            sample_color=None, refresh: bool = False, hit_trace=None) -> _ffi.fpt_frame_io:
         io = _ffi.fpt_frame_io()
         io.width, io.height = width, height
         io.frame_index = frame
@@ -149,6 +149,7 @@ class RenderPass:
         io.d_color = _ptr(rd.get("dColor"))
         io.vbuffer_out = _ptr(rd.get("vbuffer")) if self.type == "VBufferRT" else None
         io.sample_color = _ptr(sample_color)
+        io.hit_trace = _ptr(hit_trace)
         if self.type == "VBufferRT":
             io.depth = _ptr(rd.get("depth"))
             io.mvec = _ptr(rd.get("mvec"))
@@ -157,10 +158,12 @@ class RenderPass:
         return io
 
     def execute(self, render_data: Mapping[str, Any], frame: int = 0, prng_dimension: int = 0, sample_color=None,
-                refresh: bool = False) -> None:
+                refresh: bool = False, hit_trace=None) -> None:
         """RenderPass::execute: render into the output channels of `render_data`.
         The frame size is that of the output channel (image passes) or of the
-        first channel given; `refresh` carries RenderPassRefreshFlags != None."""
+        first channel given; `refresh` carries RenderPassRefreshFlags != None.
+        `sample_color` (H x W x spp x 3 float32) and `hit_trace` (H x W x spp x
+        T x 4 int32, T = bounce limit + 2) are optional per-sample outputs."""
         if self.type in self.IMAGE_IO:
             some = render_data.get(self.IMAGE_IO[self.type][1])
         else:
@@ -168,7 +171,7 @@ class RenderPass:
         if some is None:
             raise ValueError(f"{self.type}: render_data has no output channel")
         height, width = int(some.shape[0]), int(some.shape[1])
-        io = self._io(render_data, width, height, frame, prng_dimension, sample_color, refresh)
+        io = self._io(render_data, width, height, frame, prng_dimension, sample_color, refresh, hit_trace)
         check(lib().fpt_pass_execute(self._h, C.byref(io), C.c_void_p(_stream())))
 
     def reset(self) -> None:

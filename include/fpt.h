@@ -342,6 +342,15 @@ typedef struct fpt_frame_io {
     float* mvec;                 /* "mvec": RG32Float motion vector (UV)      */
     float* view_w;               /* "viewW": RGBA32Float, -ray dir, w = 0     */
     float* mask;                 /* "mask": R32Float, 1 on a hit, 0 on a miss */
+    /* Optional (MinimalPathTracer, PathTracer): the hit of every path vertex
+     * of every sample, for checking traversal per bounce.  T = maxBounces + 2
+     * (MinimalPathTracer) or maxSurfaceBounces + 2 (PathTracer) uint4 entries
+     * per sample, pixel-major, spp samples per pixel; entry k is vertex k + 1
+     * (entry 0 is the V-buffer's primary hit): (instanceID + 1,
+     * primitiveIndex, barycentric x bits, barycentric y bits), zeros for a
+     * miss.  Entries after a path's end are left as the caller set them.
+     * No counterpart in the reference (a debugging output). */
+    uint32_t* hit_trace;
 } fpt_frame_io;
 
 /* RenderPass::execute (RenderGraph/RenderPass.h:184). */
@@ -349,6 +358,19 @@ FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void
 /* AccumulatePass::reset (AccumulatePass.cpp:375-378) / PathTracer::reset
  * (PathTracer.cpp:198-214): restart the frame count. */
 FPT_API fpt_status fpt_pass_reset(fpt_pass* pass);
+
+/* Elementary functions of the path (sin, cos, atan2(x, y), acos, exp, log,
+ * log2, exp2, pow(x, y)) evaluated on device arrays of n floats: the
+ * deterministic single-precision implementations every kernel uses
+ * (cuda_libm = 0) or CUDA's own functions (cuda_libm = 1).  No counterpart
+ * in the reference (HLSL leaves these functions' last bits to the platform);
+ * a test hook for checking that host and device evaluate them identically. */
+typedef enum fpt_fmath_fn {
+    FPT_FMATH_SIN = 0, FPT_FMATH_COS = 1, FPT_FMATH_ATAN2 = 2, FPT_FMATH_ACOS = 3, FPT_FMATH_EXP = 4,
+    FPT_FMATH_LOG = 5, FPT_FMATH_LOG2 = 6, FPT_FMATH_EXP2 = 7, FPT_FMATH_POW = 8
+} fpt_fmath_fn;
+FPT_API fpt_status fpt_fmath_eval(uint32_t fn, uint32_t cuda_libm, uint32_t n, const float* x, const float* y, float* out,
+                                  void* stream);
 
 /* PathTracer execute that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot call cudaMalloc -- a host whose device

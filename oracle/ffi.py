@@ -67,6 +67,7 @@ def lib() -> C.CDLL:
         l.orc_scene_create.restype = _P
         l.orc_scene_create.argtypes = [_P, _P]
         l.orc_scene_destroy.argtypes = [_P]
+        l.orc_camera_compute.argtypes = [_P, _P]
         l.orc_scene_get_info.argtypes = [_P, C.POINTER(SceneInfo)]
         l.orc_scene_get_lights.argtypes = [_P, _P, _P, _P]
         l.orc_scene_light_bvh_sizes.argtypes = [_P, _P, _P, _P]
@@ -77,13 +78,14 @@ def lib() -> C.CDLL:
         l.orc_lbvh_select.argtypes = [_P, _P, _P, C.c_int, C.c_float, _P, _P]
         l.orc_scene_get_importance.argtypes = [_P, u32, _P]
         l.orc_vbuffer.argtypes = [_P, u32, u32, _P, u32]
+        l.orc_fmath.argtypes = [u32, u32, _P, _P, _P]
         l.orc_trace_closest.argtypes = [_P, u32, _P, _P, _P, _P, _P, _P, C.c_int]
         l.orc_trace_visibility.argtypes = [_P, u32, _P, _P, _P, _P]
         l.orc_minimal_pt.restype = C.c_double
-        l.orc_minimal_pt.argtypes = [_P, C.POINTER(MinimalPTParams), _P, _P, _P, C.c_int, u32, u32, u32, u32, u32]
+        l.orc_minimal_pt.argtypes = [_P, C.POINTER(MinimalPTParams), _P, _P, _P, C.c_int, u32, u32, u32, u32, u32, _P]
         l.orc_path_tracer.restype = C.c_double
         l.orc_path_tracer.argtypes = [_P, C.POINTER(PathTracerParams), _P, _P, _P, C.c_int, u32, u32, u32, u32, u32,
-                                      C.POINTER(Counters)]
+                                      C.POINTER(Counters), _P]
         l.orc_wardiff.restype = C.c_double
         l.orc_wardiff.argtypes = [_P, C.POINTER(WarDiffParams), C.c_int, C.c_int, _P, u32, _P, u32, _P, u32, _P, u32, C.c_double,
                                   _P, _P, _P,
@@ -114,8 +116,11 @@ def ptr(a: np.ndarray) -> C.c_void_p:
 class OracleScene:
     """The oracle's copy of a scene, built from the same host description."""
 
-    def __init__(self, desc_ptr, camera_data):
-        self._h = lib().orc_scene_create(C.cast(desc_ptr, _P), C.cast(C.pointer(camera_data), _P))
+    def __init__(self, desc_ptr, camera_data=None):
+        """camera_data None: the oracle computes the camera vectors from the
+        description's camera itself (Camera.cpp:112-195)."""
+        cam = C.cast(C.pointer(camera_data), _P) if camera_data is not None else None
+        self._h = lib().orc_scene_create(C.cast(desc_ptr, _P), cam)
         if not self._h:
             raise RuntimeError("oracle scene creation failed")
         self.info = SceneInfo()
@@ -142,25 +147,32 @@ class OracleScene:
         lib().orc_trace_closest(self._h, n, ptr(o), ptr(d), ptr(tmin), ptr(tmax), ptr(out), ptr(t), int(brute))
         return out, t
 
-    def minimal_pt(self, vbuffer: np.ndarray, params: MinimalPTParams, fp64: bool = False, threads: int = 0, rect=None):
+    def minimal_pt(self, vbuffer: np.ndarray, params: MinimalPTParams, fp64: bool = False, threads: int = 0, rect=None,
+                   trace: bool = False):
+        """(colour, rays per pixel, seconds[, hit trace [H, W, maxBounces + 2, 4]])."""
         h, w = vbuffer.shape[:2]
         out = np.zeros((h, w, 4), dtype=np.float32)
         rays = np.zeros((h, w), dtype=np.uint32)
+        tr = np.zeros((h, w, params.maxBounces + 2, 4), dtype=np.uint32) if trace else None
         x0, y0, x1, y1 = rect if rect else (0, 0, w, h)
         dt = lib().orc_minimal_pt(self._h, C.byref(params), ptr(np.ascontiguousarray(vbuffer)), ptr(out), ptr(rays),
-                                  int(fp64), threads, x0, y0, x1, y1)
-        return out, rays, dt
+                                  int(fp64), threads, x0, y0, x1, y1, ptr(tr) if tr is not None else None)
+        return (out, rays, dt, tr) if trace else (out, rays, dt)
 
     def path_tracer(self, vbuffer: np.ndarray, params: PathTracerParams, fp64: bool = False, threads: int = 0, rect=None,
-                    samples: bool = False):
+                    samples: bool = False, trace: bool = False):
+        """(colour, per-sample radiance or None, counters, seconds[, hit trace
+        [H, W, spp, maxSurfaceBounces + 2, 4]])."""
         h, w = vbuffer.shape[:2]
         out = np.zeros((h, w, 4), dtype=np.float32)
         smp = np.zeros((h, w, params.samplesPerPixel, 3), dtype=np.float32) if samples else None
         cnt = Counters()
+        tr = np.zeros((h, w, params.samplesPerPixel, params.maxSurfaceBounces + 2, 4), dtype=np.uint32) if trace else None
         x0, y0, x1, y1 = rect if rect else (0, 0, w, h)
         dt = lib().orc_path_tracer(self._h, C.byref(params), ptr(np.ascontiguousarray(vbuffer)), ptr(out),
-                                   ptr(smp) if smp is not None else None, int(fp64), threads, x0, y0, x1, y1, C.byref(cnt))
-        return out, smp, cnt, dt
+                                   ptr(smp) if smp is not None else None, int(fp64), threads, x0, y0, x1, y1, C.byref(cnt),
+                                   ptr(tr) if tr is not None else None)
+        return (out, smp, cnt, dt, tr) if trace else (out, smp, cnt, dt)
 
     def wardiff(self, params: WarDiffParams, mode: int = 0, dLdI=None, mat_tangents=None, pos_tangents=None, eps: float = 0.0,
                 threads: int = 0, rect=None, nrm_tangents=None, tan_tangents=None):
@@ -235,6 +247,26 @@ class OracleScene:
         out = np.zeros((d, d), dtype=np.float32)
         lib().orc_scene_get_importance(self._h, mip, ptr(out))
         return out
+
+
+def camera_data(camera, out_type):
+    """The oracle's camera vectors for an fpt_camera (ctypes structure); the
+    result is an instance of out_type (the fpt_camera_data layout)."""
+    out = out_type()
+    lib().orc_camera_compute(C.cast(C.pointer(camera), _P), C.cast(C.pointer(out), _P))
+    return out
+
+
+FMATH = {"sin": 0, "cos": 1, "atan2": 2, "acos": 3, "exp": 4, "log": 5, "log2": 6, "exp2": 7, "pow": 8}
+
+
+def fmath(fn: str, x: np.ndarray, y: np.ndarray | None = None) -> np.ndarray:
+    """The deterministic elementary functions the kernels use, on the host."""
+    x = np.ascontiguousarray(x, np.float32)
+    yy = np.ascontiguousarray(y, np.float32) if y is not None else None
+    out = np.zeros_like(x)
+    lib().orc_fmath(FMATH[fn], x.size, ptr(x), ptr(yy) if yy is not None else None, ptr(out))
+    return out
 
 
 def sample_pattern(kind: str, sample_count: int, n: int) -> np.ndarray:

@@ -33,6 +33,7 @@ void* orc_scene_create(const fpt_scene_desc* d, const fpt_camera_data* cam) {
     }
 }
 void orc_scene_destroy(void* s) { delete static_cast<Scene*>(s); }
+void orc_camera_compute(const fpt_camera* c, fpt_camera_data* out) { camera_data_from(*c, *out); }
 
 struct orc_scene_info {
     uint32_t triangle_count, instance_count, emissive_count, active_emissive_count;
@@ -90,6 +91,27 @@ void orc_scene_get_importance(const void* sp, uint32_t mip, float* out) {
     std::copy(s.impMips[mip].begin(), s.impMips[mip].end(), out);
 }
 
+// The deterministic elementary functions (falcor_b200/csrc/fmath.h) on host
+// arrays, numbered as fpt_fmath_fn.
+void orc_fmath(uint32_t fn, uint32_t n, const float* x, const float* y, float* out) {
+    for (uint32_t i = 0; i < n; i++) {
+        const float a = x[i], b = y ? y[i] : 0.f;
+        float r;
+        switch (fn) {
+            case 0: r = fm::sin(a); break;
+            case 1: r = fm::cos(a); break;
+            case 2: r = fm::atan2(a, b); break;
+            case 3: r = fm::acos(a); break;
+            case 4: r = fm::exp(a); break;
+            case 5: r = fm::log(a); break;
+            case 6: r = fm::log2(a); break;
+            case 7: r = fm::exp2(a); break;
+            default: r = fm::pow(a, b); break;
+        }
+        out[i] = r;
+    }
+}
+
 void orc_vbuffer(const void* sp, uint32_t W, uint32_t H, uint32_t* out, uint32_t threads) {
     const Scene& s = *static_cast<const Scene*>(sp);
     parallel_tiles(0, 0, W, H, threads, [&](uint32_t x, uint32_t y, uint32_t) { render_vbuffer_pixel(s, W, H, x, y, out); });
@@ -117,8 +139,9 @@ void orc_trace_visibility(const void* sp, uint32_t n, const float* o, const floa
 
 // MinimalPathTracer over the rectangle [x0,x1)x[y0,y1) of a W x H frame.
 // out: RGBA32F for the full frame (only the rectangle is written).
+// trace (optional): per pixel (maxBounces + 2) x 4 uints of per-vertex hits.
 double orc_minimal_pt(const void* sp, const MinimalPTParams* p, const uint32_t* vbuffer, float* out, uint32_t* rays,
-                      int fp64, uint32_t threads, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1) {
+                      int fp64, uint32_t threads, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, uint32_t* trace) {
     const Scene& s = *static_cast<const Scene*>(sp);
     auto t0 = std::chrono::steady_clock::now();
     parallel_tiles(x0, y0, x1, y1, threads, [&](uint32_t x, uint32_t y, uint32_t) {
@@ -129,7 +152,8 @@ double orc_minimal_pt(const void* sp, const MinimalPTParams* p, const uint32_t* 
             V3<double> c = minimal_pt_pixel<double>(s, *p, x, y, vbuffer + 4 * i, &r);
             o[0] = float(c.x); o[1] = float(c.y); o[2] = float(c.z);
         } else {
-            V3<float> c = minimal_pt_pixel<float>(s, *p, x, y, vbuffer + 4 * i, &r);
+            uint32_t* tr = trace ? trace + i * size_t(p->maxBounces + 2) * 4 : nullptr;
+            V3<float> c = minimal_pt_pixel<float>(s, *p, x, y, vbuffer + 4 * i, &r, tr);
             o[0] = c.x; o[1] = c.y; o[2] = c.z;
         }
         o[3] = 1.f;
@@ -142,8 +166,10 @@ struct orc_counters { uint64_t paths, rays, closest, shadow, node_visits, tri_te
 
 // PathTracer over a rectangle.  color: RGBA32F full frame; samples (optional):
 // per pixel spp*3 floats, pixel-major over the full frame.
+// trace (optional): per pixel spp x (maxSurfaceBounces + 2) x 4 uints of per-vertex hits.
 double orc_path_tracer(const void* sp, const PathTracerParams* p, const uint32_t* vbuffer, float* color, float* samples,
-                       int fp64, uint32_t threads, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, orc_counters* cnt) {
+                       int fp64, uint32_t threads, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, orc_counters* cnt,
+                       uint32_t* trace) {
     const Scene& s = *static_cast<const Scene*>(sp);
     uint32_t nthreads = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
     std::vector<PathCounters> pcs(nthreads);
@@ -152,7 +178,8 @@ double orc_path_tracer(const void* sp, const PathTracerParams* p, const uint32_t
         size_t i = size_t(y) * p->width + x;
         float* so = samples ? samples + i * size_t(p->samplesPerPixel) * 3 : nullptr;
         if (fp64) path_tracer_pixel<double>(s, *p, x, y, vbuffer + 4 * i, so, color + 4 * i, &pcs[tid]);
-        else path_tracer_pixel<float>(s, *p, x, y, vbuffer + 4 * i, so, color + 4 * i, &pcs[tid]);
+        else path_tracer_pixel<float>(s, *p, x, y, vbuffer + 4 * i, so, color + 4 * i, &pcs[tid],
+                                      trace ? trace + i * size_t(p->samplesPerPixel) * (p->maxSurfaceBounces + 2) * 4 : nullptr);
     });
     double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (cnt) {

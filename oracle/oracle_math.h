@@ -20,6 +20,30 @@
 #include <limits>
 
 #include "oracle_dual.h"
+#include "../falcor_b200/csrc/fmath.h"
+
+namespace orc {
+// Elementary functions of the restatement.  Single precision goes through the
+// deterministic functions the kernels use (falcor_b200/csrc/fmath.h: HLSL
+// leaves their last bits to the platform, so both sides fix one definition);
+// double and the derivative types use the C library.
+template <class R> inline R el_sin(const R& x) { return std::sin(x); }
+template <class R> inline R el_cos(const R& x) { return std::cos(x); }
+template <class R> inline R el_exp(const R& x) { return std::exp(x); }
+template <class R> inline R el_log(const R& x) { return std::log(x); }
+template <class R> inline R el_log2(const R& x) { return std::log2(x); }
+template <class R> inline R el_atan2(const R& y, const R& x) { return std::atan2(y, x); }
+template <class R> inline R el_acos(const R& x) { return std::acos(x); }
+template <class R> inline R el_pow(const R& x, const R& y) { return std::pow(x, y); }
+inline float el_sin(float x) { return fm::sin(x); }
+inline float el_cos(float x) { return fm::cos(x); }
+inline float el_exp(float x) { return fm::exp(x); }
+inline float el_log(float x) { return fm::log(x); }
+inline float el_log2(float x) { return fm::log2(x); }
+inline float el_atan2(float y, float x) { return fm::atan2(y, x); }
+inline float el_acos(float x) { return fm::acos(x); }
+inline float el_pow(float x, float y) { return fm::pow(x, y); }
+}  // namespace orc
 
 namespace orc {
 
@@ -343,7 +367,7 @@ inline uint32_t encode_logluv_hdr(V3<float> c) {
     const float X = 0.4123907992659595f * c.x + 0.3575843393838780f * c.y + 0.1804807884018343f * c.z;
     const float Y = 0.2126390058715104f * c.x + 0.7151686787677559f * c.y + 0.0721923153607337f * c.z;
     const float Z = 0.0193308187155918f * c.x + 0.1191947797946259f * c.y + 0.9505321522496608f * c.z;
-    float logY = 409.6f * (std::log2(Y) + 20.f);
+    float logY = 409.6f * (el_log2(Y) + 20.f);
     float cl = std::min(std::max(logY, 0.f), 16383.f);
     if (std::isnan(logY)) cl = 0.f;
     uint32_t Le = uint32_t(cl);
@@ -359,7 +383,7 @@ inline V3<float> decode_logluv_hdr(uint32_t p) {
     uint32_t Le = p >> 18;
     if (Le == 0) return V3<float>(0.f);
     float logY = (float(Le) + 0.5f) / 409.6f - 20.f;
-    float Y = std::pow(2.f, logY);
+    float Y = el_pow(2.f, logY);
     float u = (float((p >> 9) & 0x1ffu) + 0.5f) / 820.f;
     float v = (float(p & 0x1ffu) + 0.5f) / 820.f;
     float invDenom = 1.f / (6.f * u - 16.f * v + 12.f);
@@ -387,7 +411,7 @@ template <class R> inline V2<R> sample_disk_concentric(V2<R> u) {
         r = u.y;
         phi = K<R>::pi_2 - (u.x / u.y) * K<R>::pi_4;
     }
-    return V2<R>(r * std::cos(phi), r * std::sin(phi));
+    return V2<R>(r * el_cos(phi), r * el_sin(phi));
 }
 template <class R> inline V3<R> sample_cosine_hemisphere_concentric(V2<R> u, R& pdf) {
     V2<R> d = sample_disk_concentric(u);
@@ -403,20 +427,20 @@ template <class R> inline V3<R> sample_triangle(V2<R> u) {
 template <class R> inline V3<R> sample_von_mises_fisher(V2<R> u, R kappa) {
     R sy = vmax(R(1) - u.y, R(1e-6f));
     R phi = K<R>::two_pi * u.x;
-    R cosTheta = R(1) + std::log(std::exp(R(-2) * kappa) * (R(1) - sy) + sy) / kappa;
+    R cosTheta = R(1) + el_log(el_exp(R(-2) * kappa) * (R(1) - sy) + sy) / kappa;
     R sinTheta = std::sqrt(R(1) - cosTheta * cosTheta);
-    return V3<R>(std::cos(phi) * sinTheta, std::sin(phi) * sinTheta, cosTheta);
+    return V3<R>(el_cos(phi) * sinTheta, el_sin(phi) * sinTheta, cosTheta);
 }
 template <class R> inline V2<R> world_to_latlong_map(V3<R> dir) {
     V3<R> p = normalize(dir);
     V2<R> uv;
-    uv.x = std::atan2(p.x, -p.z) * K<R>::inv_2pi + R(0.5f);
-    uv.y = std::acos(p.y) * K<R>::inv_pi;
+    uv.x = el_atan2(p.x, -p.z) * K<R>::inv_2pi + R(0.5f);
+    uv.y = el_acos(p.y) * K<R>::inv_pi;
     return uv;
 }
 template <class R> inline V2<R> ndir_to_oct_equal_area_unorm(V3<R> n) {
     R r = std::sqrt(R(1) - std::fabs(n.z));
-    R phi = std::atan2(std::fabs(n.y), std::fabs(n.x));
+    R phi = el_atan2(R(std::fabs(n.y)), R(std::fabs(n.x)));
     V2<R> p;
     p.y = r * phi * K<R>::two_over_pi;
     p.x = r - p.y;
@@ -431,8 +455,8 @@ template <class R> inline V3<R> oct_to_ndir_equal_area_unorm(V2<R> p) {
     R r = R(1) - std::fabs(d);
     R phi = (r > R(0)) ? ((std::fabs(p.y) - std::fabs(p.x)) / r + R(1)) * K<R>::pi_4 : R(0);
     R f = r * std::sqrt(R(2) - r * r);
-    R x = f * sgn(p.x) * std::cos(phi);
-    R y = f * sgn(p.y) * std::sin(phi);
+    R x = f * sgn(p.x) * el_cos(phi);
+    R y = f * sgn(p.y) * el_sin(phi);
     R z = sgn(d) * (R(1) - r * r);
     return V3<R>(x, y, z);
 }
@@ -519,7 +543,7 @@ inline bool intersect_ray_triangle(const V3<R>& ro, const V3<R>& rd, const V3<R>
 // GGX microfacet model (Rendering/Materials/IsotropicGGX.slang:46-206) and
 // Fresnel (Rendering/Materials/Fresnel.slang:42-51).
 // ---------------------------------------------------------------------------
-template <class R> inline R pw(R a, R b) { return std::pow(a, b); }
+template <class R> inline R pw(R a, R b) { return el_pow(a, b); }
 
 template <class R> inline R eval_ndf_ggx(R alpha, R cosTheta) {
     R a2 = alpha * alpha;
@@ -553,8 +577,8 @@ template <class R> inline V3<R> sample_vndf_hemisphere(V2<R> u, V3<R> Vh) {
     R phi = R(2) * K<R>::pi * u.x;
     R z = std::fma((R(1) - u.y), (R(1) + Vh.z), -Vh.z);
     R sinTheta = std::sqrt(saturate(R(1) - z * z));
-    R x = sinTheta * std::cos(phi);
-    R y = sinTheta * std::sin(phi);
+    R x = sinTheta * el_cos(phi);
+    R y = sinTheta * el_sin(phi);
     return V3<R>(x, y, z) + Vh;
 }
 template <class R> inline V3<R> sample_ggx_vndf(R alpha, V3<R> wi, V2<R> u, R& pdf) {

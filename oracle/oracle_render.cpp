@@ -561,9 +561,21 @@ static bool mpt_generate_scatter_ray(const ShadingData<R>& sd, const MaterialIns
     return false;
 }
 
+// One entry of a per-vertex hit record (see oracle_render.h).
+static void record_hit(uint32_t* trace, uint32_t perSample, uint32_t vertexIndex, const Hit& h) {
+    if (!trace || vertexIndex == 0 || vertexIndex > perSample) return;
+    uint32_t* e = trace + 4 * size_t(vertexIndex - 1);
+    if (!h.valid) { e[0] = e[1] = e[2] = e[3] = 0; return; }
+    e[0] = h.instanceID + 1;
+    e[1] = h.primitiveIndex;
+    std::memcpy(&e[2], &h.baryX, 4);
+    std::memcpy(&e[3], &h.baryY, 4);
+}
+
 template <class R>
 V3<R> minimal_pt_pixel(const Scene& s, const MinimalPTParams& p, uint32_t x, uint32_t y, const uint32_t* vbufferPixel,
-                       uint32_t* rays) {
+                       uint32_t* rays, uint32_t* trace) {
+    const uint32_t traceLen = p.maxBounces + 2;
     const bool useEmissive = !s.emissive.empty();
     const bool useEnvLight = s.hasEnv, useEnvBg = s.hasEnv;
     V3<R> outColor(R(0));
@@ -572,6 +584,7 @@ V3<R> minimal_pt_pixel(const Scene& s, const MinimalPTParams& p, uint32_t x, uin
     Hit hit = unpack_hit(s.hitBits, vbufferPixel);
     uint32_t nrays = 0;
     if (hit.valid) {
+        record_hit(trace, traceLen, 1, hit);
         ShadingData<R> sd = load_shading_data<R>(s, hit, primaryDir);
         MaterialInstance<R> mi = material_instance<R>(s, sd, p.lambert != 0);
         UniformSG sg(x, y, p.frameCount);
@@ -584,6 +597,7 @@ V3<R> minimal_pt_pixel(const Scene& s, const MinimalPTParams& p, uint32_t x, uin
             // traceScatterRay (.rt.slang:233-243): TMin 0, TMax FLT_MAX.
             nrays++;
             Hit h = trace_closest<R>(s, rd.origin, rd.direction, R(0), R(std::numeric_limits<float>::max()), nullptr);
+            record_hit(trace, traceLen, depth + 2, h);
             if (!h.valid) {
                 // scatterMiss (.rt.slang:475-486)
                 rd.terminated = true;
@@ -635,7 +649,7 @@ template <class R, class SG> struct PTPath {
 template <class R> static R eval_mis(const PathTracerParams& p, R n0, R p0, R n1, R p1) {
     if (p.misHeuristic == 0) { R q0 = n0 * p0, q1 = n1 * p1; return q0 / (q0 + q1); }
     if (p.misHeuristic == 1) { R q0 = (n0 * p0) * (n0 * p0), q1 = (n1 * p1) * (n1 * p1); return q0 / (q0 + q1); }
-    R q0 = std::pow(n0 * p0, R(p.misPowerExponent)), q1 = std::pow(n1 * p1, R(p.misPowerExponent));
+    R q0 = el_pow(R(n0 * p0), R(p.misPowerExponent)), q1 = el_pow(R(n1 * p1), R(p.misPowerExponent));
     return q0 / (q0 + q1);
 }
 
@@ -800,7 +814,8 @@ static void pt_handle_miss(const Scene& s, const PathTracerParams& p, PTPath<R, 
 
 template <class R, class SG>
 static V3<R> pt_trace_path(const Scene& s, const PathTracerParams& p, uint32_t x, uint32_t y, uint32_t sampleIdx,
-                           const uint32_t* vbufferPixel, PathCounters* pc) {
+                           const uint32_t* vbufferPixel, PathCounters* pc, uint32_t* trace) {
+    const uint32_t traceLen = p.maxSurfaceBounces + 2;
     // generatePath (PathTracer.slang:273-301)
     const uint32_t maxSpp = p.samplesPerPixel;
     SG sg(x, y, p.seed * maxSpp + sampleIdx);
@@ -818,11 +833,13 @@ static V3<R> pt_trace_path(const Scene& s, const PathTracerParams& p, uint32_t x
         path.set(PF_HIT);
         path.vertexIndex = 1;
     }
+    record_hit(trace, traceLen, 1, hit);
     pt_handle_hit<R, SG>(s, p, path, pc);
     while (path.has(PF_ACTIVE)) {
         path.vertexIndex++;
         if (pc) pc->rays++;
         Hit h = trace_closest<R>(s, path.origin, path.dir, R(0), R(1e30f), pc ? &pc->tc : nullptr);
+        record_hit(trace, traceLen, path.vertexIndex, h);
         if (h.valid) {
             path.hit = h;
             path.set(PF_HIT);
@@ -838,7 +855,7 @@ static V3<R> pt_trace_path(const Scene& s, const PathTracerParams& p, uint32_t x
 
 template <class R>
 void path_tracer_pixel(const Scene& s, const PathTracerParams& p, uint32_t x, uint32_t y, const uint32_t* vbufferPixel,
-                       float* sampleOut, float* colorOut, PathCounters* pc) {
+                       float* sampleOut, float* colorOut, PathCounters* pc, uint32_t* trace) {
     Hit hit = unpack_hit(s.hitBits, vbufferPixel);
     const uint32_t spp = p.samplesPerPixel;
     V3<R> color(R(0));
@@ -854,8 +871,9 @@ void path_tracer_pixel(const Scene& s, const PathTracerParams& p, uint32_t x, ui
         }
     } else {
         for (uint32_t i = 0; i < spp; i++) {
-            V3<R> L = (p.sampleGenerator == 0) ? pt_trace_path<R, TinyUniformSG>(s, p, x, y, i, vbufferPixel, pc)
-                                               : pt_trace_path<R, UniformSG>(s, p, x, y, i, vbufferPixel, pc);
+            uint32_t* tr = trace ? trace + size_t(i) * (p.maxSurfaceBounces + 2) * 4 : nullptr;
+            V3<R> L = (p.sampleGenerator == 0) ? pt_trace_path<R, TinyUniformSG>(s, p, x, y, i, vbufferPixel, pc, tr)
+                                               : pt_trace_path<R, UniformSG>(s, p, x, y, i, vbufferPixel, pc, tr);
             if (sampleOut) { float* o = sampleOut + size_t(i) * 3; o[0] = float(L.x); o[1] = float(L.y); o[2] = float(L.z); }
             V3<R> stored = L;
             if (spp != 1 && p.colorFormat == 1) stored = cvt3<R>(decode_logluv_hdr(encode_logluv_hdr(tof(L))));
@@ -879,10 +897,14 @@ bool lbvh_select_f(const Scene& s, const float posW[3], const float n[3], bool u
 
 #include "oracle_wardiff.inl"
 
-template V3<float> minimal_pt_pixel<float>(const Scene&, const MinimalPTParams&, uint32_t, uint32_t, const uint32_t*, uint32_t*);
-template V3<double> minimal_pt_pixel<double>(const Scene&, const MinimalPTParams&, uint32_t, uint32_t, const uint32_t*, uint32_t*);
-template void path_tracer_pixel<float>(const Scene&, const PathTracerParams&, uint32_t, uint32_t, const uint32_t*, float*, float*, PathCounters*);
-template void path_tracer_pixel<double>(const Scene&, const PathTracerParams&, uint32_t, uint32_t, const uint32_t*, float*, float*, PathCounters*);
+template V3<float> minimal_pt_pixel<float>(const Scene&, const MinimalPTParams&, uint32_t, uint32_t, const uint32_t*, uint32_t*,
+                                           uint32_t*);
+template V3<double> minimal_pt_pixel<double>(const Scene&, const MinimalPTParams&, uint32_t, uint32_t, const uint32_t*, uint32_t*,
+                                             uint32_t*);
+template void path_tracer_pixel<float>(const Scene&, const PathTracerParams&, uint32_t, uint32_t, const uint32_t*, float*, float*,
+                                       PathCounters*, uint32_t*);
+template void path_tracer_pixel<double>(const Scene&, const PathTracerParams&, uint32_t, uint32_t, const uint32_t*, float*, float*,
+                                        PathCounters*, uint32_t*);
 
 // Runs fn(x, y) over the pixels of [x0,x1)x[y0,y1) in 16x16 tiles on `threads` threads.
 void parallel_tiles(uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, uint32_t threads,

@@ -87,13 +87,17 @@ Hit unpack_hit(const fpt_hitinfo_bits& b, const uint32_t in[4]);
 void render_vbuffer_pixel(const Scene& s, uint32_t W, uint32_t H, uint32_t x, uint32_t y, uint32_t* out);
 void render_vbuffer(const Scene& s, uint32_t W, uint32_t H, uint32_t* out, uint32_t y0, uint32_t y1, TraceCounters* c);
 
+// trace (optional): the hit of every path vertex, 4 uints per entry
+// (instanceID + 1, primitiveIndex, bary.x bits, bary.y bits; zeros for a miss),
+// maxBounces + 2 (MinimalPathTracer) or maxSurfaceBounces + 2 (PathTracer)
+// entries per sample, samples of the pixel one after the other.
 template <class R>
 V3<R> minimal_pt_pixel(const Scene& s, const MinimalPTParams& p, uint32_t x, uint32_t y, const uint32_t* vbufferPixel,
-                       uint32_t* rays);
+                       uint32_t* rays, uint32_t* trace = nullptr);
 
 template <class R>
 void path_tracer_pixel(const Scene& s, const PathTracerParams& p, uint32_t x, uint32_t y, const uint32_t* vbufferPixel,
-                       float* sampleOut, float* colorOut, PathCounters* pc);
+                       float* sampleOut, float* colorOut, PathCounters* pc, uint32_t* trace = nullptr);
 
 void parallel_tiles(uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, uint32_t threads,
                     const std::function<void(uint32_t, uint32_t, uint32_t)>& fn);

@@ -81,9 +81,34 @@ void generate_alias_table(std::vector<float> weights, std::vector<uint32_t>& tab
     weightSum = float(sum);
 }
 
+// Camera::calculateCameraParameters (Scene/Camera/Camera.cpp:112-195), the
+// ray-tracing vectors only: frame height preserved, fovY from
+// focalLengthToFovY (Utils/Math/FalcorMath.h:123-126), 0 focal length = 0 FOV.
+void camera_data_from(const fpt_camera& c, fpt_camera_data& o) {
+    const float fovY = c.focal_length == 0.0f ? 0.0f : 2.0f * std::atan(0.5f * c.frame_height / c.focal_length);
+    const V3<float> posW(c.position[0], c.position[1], c.position[2]);
+    const V3<float> target(c.target[0], c.target[1], c.target[2]);
+    const V3<float> up(c.up[0], c.up[1], c.up[2]);
+    const V3<float> camW = normalize(target - posW) * c.focal_distance;
+    V3<float> camU = normalize(cross(camW, up));
+    V3<float> camV = normalize(cross(camU, camW));
+    const float ulen = c.focal_distance * std::tan(fovY * 0.5f) * c.aspect_ratio;
+    camU = camU * ulen;
+    const float vlen = c.focal_distance * std::tan(fovY * 0.5f);
+    camV = camV * vlen;
+    const V3<float>* vs[4] = {&posW, &camU, &camV, &camW};
+    float* outs[4] = {o.posW, o.cameraU, o.cameraV, o.cameraW};
+    for (int k = 0; k < 4; k++) { outs[k][0] = vs[k]->x; outs[k][1] = vs[k]->y; outs[k][2] = vs[k]->z; }
+    o.nearZ = c.near_z;
+    o.farZ = c.far_z;
+    o.jitterX = c.jitter_x;
+    o.jitterY = c.jitter_y;
+}
+
 Scene::Scene(const fpt_scene_desc* d, const fpt_camera_data* cam, uint32_t aliasSeed) {
-    if (!d || !cam) throw std::runtime_error("null scene");
-    camera = *cam;
+    if (!d) throw std::runtime_error("null scene");
+    if (cam) camera = *cam;
+    else camera_data_from(d->camera, camera);
     vertices.resize(d->vertex_count);
     for (uint32_t i = 0; i < d->vertex_count; i++) vertices[i] = pack_vertex(d->vertices[i]);
     indices.assign(d->indices, d->indices + d->index_count);

@@ -66,8 +66,12 @@ struct TraceCounters {
     uint64_t closest = 0, shadow = 0, nodeVisits = 0, triTests = 0;
 };
 
+// Camera::calculateCameraParameters ray-tracing vectors (Scene/Camera/Camera.cpp:112-195).
+void camera_data_from(const fpt_camera& c, fpt_camera_data& o);
+
 class Scene {
 public:
+    // cam == nullptr: the camera vectors are computed from d->camera here.
     Scene(const fpt_scene_desc* d, const fpt_camera_data* cam, uint32_t aliasSeedDefault = 1);
 
     // geometry

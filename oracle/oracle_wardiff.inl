@@ -242,7 +242,7 @@ static void war_mean(const Scene& s, const WarSeeds& seeds, const WarDiffParams&
         float bt = dot(isectN, auxDir);
         bt = bt * bt;
         const float sy = std::max(1.f - smp.y, 1e-6f);
-        const float invVMF = 1.f / ((1.f - sy) * std::exp(-2.f * kappa) + sy);
+        const float invVMF = 1.f / ((1.f - sy) * el_exp(-2.f * kappa) + sy);
         const float wDenom = invVMF - 1.f + bt;
         const float wDenomRcp = wDenom > 1e-4f ? 1.f / wDenom : 0.f;
         const float w = wDenomRcp * wDenomRcp * wDenomRcp * invVMF;
@@ -424,9 +424,9 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
     V2<float> u = next2D<float>(sg);
     // sampleGaussian (WARDiffPathTracer.rt.slang:59-62), sigma 0.5.
     const float sigma = 0.5f;
-    const float r = std::sqrt(-2.f * std::log(u.x));
+    const float r = std::sqrt(-2.f * el_log(u.x));
     const float ang = 6.28318530717958647692f * u.y;
-    V2<float> jitter((r * std::cos(ang)) * sigma, (r * std::sin(ang)) * sigma);
+    V2<float> jitter((r * el_cos(ang)) * sigma, (r * el_sin(ang)) * sigma);
     if (p.useAntithetic && frameSeed % 2 == 0) jitter = V2<float>(-jitter.x, -jitter.y);
     V2<float> pix = pixelf + jitter;
 

@@ -102,3 +102,31 @@ def test_path_tracer_bounce_count_rules(fpt):
     assert [p[k] for k in keys] == [8, 8, 8, 8]
     p = PathTracer({"maxDiffuseBounces": 6}).properties
     assert [p[k] for k in keys] == [10, 6, 3, 10]
+
+
+def test_oracle_camera_matches_library_camera(fpt, oracle):
+    """The oracle derives the camera vectors itself (Camera.cpp:112-195); they
+    equal the library's fpt_camera_compute bit for bit on the procedural
+    cameras and on random look-at cameras."""
+    from falcor_b200 import _ffi
+    from falcor_b200.scene import HostScene, BOX_ICOSPHERE, HEIGHTFIELD_SOUP, DISPLACED_SPHERE
+    cams = [HostScene.procedural(BOX_ICOSPHERE, seed=0, sphere_subdiv=2, aspect_ratio=1.0).desc.camera,
+            HostScene.procedural(HEIGHTFIELD_SOUP, seed=1, grid_res=16, soup_triangles=10, material_count=2,
+                                 emissive_count=2, aspect_ratio=16 / 9).desc.camera,
+            HostScene.procedural(DISPLACED_SPHERE, seed=2, sphere_subdiv=16, aspect_ratio=1.0).desc.camera]
+    rng = np.random.default_rng(5)
+    for _ in range(50):
+        c = _ffi.fpt_camera()
+        for k in range(3):
+            c.position[k], c.target[k] = rng.uniform(-10, 10, 2)
+        c.up[1] = 1.0
+        c.focal_length = float(rng.uniform(5, 100))
+        c.frame_height = 24.0
+        c.aspect_ratio = float(rng.uniform(0.5, 2.5))
+        c.near_z, c.far_z, c.focal_distance = 0.1, 1000.0, float(rng.uniform(0.5, 1e4))
+        cams.append(c)
+    for c in cams:
+        lib_cd = _ffi.fpt_camera_data()
+        _ffi.check(fpt.fpt_camera_compute(C.byref(c), C.byref(lib_cd)))
+        orc_cd = oracle.camera_data(c, _ffi.fpt_camera_data)
+        assert bytes(lib_cd) == bytes(orc_cd)
