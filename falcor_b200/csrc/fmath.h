@@ -296,18 +296,8 @@ FM_HD float ipow(float x, int n) {
     for (int i = 1; i < n; i++) r = r * x;
     return r;
 }
-FM_HD float pow(float x, float y) {
-    if (y == 0.f) return 1.f;
-    if (isnan_(x) || isnan_(y)) return qnan();
-    const bool yInt = rint_(y) == y;
-    if (yInt && y >= 1.f && y <= 8.f) return ipow(x, int(y));
-    if (x == 0.f) return y > 0.f ? 0.f : inf();
-    if (x < 0.f) {
-        if (!yInt) return qnan();
-        const float a = pow(-x, y);
-        const bool odd = fabs_(y) < 16777216.f && (int64_t(y) & 1) != 0;
-        return odd ? -a : a;
-    }
+// x^y for finite x > 0 and y not handled by the integer path.
+FM_HD float pow_pos(float x, float y) {
     if (x == 1.f) return 1.f;
     if (x == inf()) return y > 0.f ? inf() : 0.f;
     // y log2 x carried as hi + lo so that the exponent keeps its low bits.
@@ -319,6 +309,20 @@ FM_HD float pow(float x, float y) {
     if (zh < -150.f) return 0.f;
     const float k = rint_(zh);
     return exp2_kf(k, (zh - k) + zl);
+}
+FM_HD float pow(float x, float y) {
+    if (y == 0.f) return 1.f;
+    if (isnan_(x) || isnan_(y)) return qnan();
+    const bool yInt = rint_(y) == y;
+    if (yInt && y >= 1.f && y <= 8.f) return ipow(x, int(y));
+    if (x == 0.f) return y > 0.f ? 0.f : inf();
+    if (x < 0.f) {
+        if (!yInt) return qnan();
+        const float a = pow_pos(-x, y);
+        const bool odd = fabs_(y) < 16777216.f && (int64_t(y) & 1) != 0;
+        return odd ? -a : a;
+    }
+    return pow_pos(x, y);
 }
 
 }  // namespace fm

@@ -49,6 +49,19 @@ class Counters(C.Structure):
                 ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64)]
 
 
+class ProceduralParams(C.Structure):
+    """fpt_procedural_params (include/fpt.h)."""
+    _fields_ = [("kind", u32), ("seed", u32), ("grid_res", u32), ("soup_triangles", u32), ("material_count", u32),
+                ("emissive_count", u32), ("sphere_subdiv", u32), ("envmap_width", u32), ("envmap_height", u32),
+                ("lambert", u32), ("aspect_ratio", C.c_float)]
+
+
+class SceneDescHead(C.Structure):
+    """Leading fields of fpt_scene_desc (include/fpt.h): array pointers and counts."""
+    _fields_ = [("vertices", _P), ("vertex_count", u32), ("indices", _P), ("index_count", u32),
+                ("instances", _P), ("instance_count", u32), ("materials", _P), ("material_count", u32)]
+
+
 _lib = None
 
 
@@ -68,6 +81,12 @@ def lib() -> C.CDLL:
         l.orc_scene_create.argtypes = [_P, _P]
         l.orc_scene_destroy.argtypes = [_P]
         l.orc_camera_compute.argtypes = [_P, _P]
+        l.orc_procedural_scene.restype = _P
+        l.orc_procedural_scene.argtypes = [C.POINTER(ProceduralParams)]
+        l.orc_procedural_desc.restype = _P
+        l.orc_procedural_desc.argtypes = [_P]
+        l.orc_procedural_free.argtypes = [_P]
+        l.orc_last_error.restype = C.c_char_p
         l.orc_scene_get_info.argtypes = [_P, C.POINTER(SceneInfo)]
         l.orc_scene_get_lights.argtypes = [_P, _P, _P, _P]
         l.orc_scene_light_bvh_sizes.argtypes = [_P, _P, _P, _P]
@@ -111,6 +130,45 @@ def lib() -> C.CDLL:
 def ptr(a: np.ndarray) -> C.c_void_p:
     assert a.flags["C_CONTIGUOUS"]
     return C.c_void_p(a.ctypes.data)
+
+
+class ProceduralScene:
+    """A synthetic workload scene built by the oracle library itself (the same
+    generator the CUDA library compiles), without loading the CUDA library."""
+
+    def __init__(self, kind: int, seed: int = 0, grid_res: int = 0, soup_triangles: int = 0, material_count: int = 0,
+                 emissive_count: int = 0, sphere_subdiv: int = 0, envmap=None, aspect_ratio: float = 0.0):
+        p = ProceduralParams(kind=kind, seed=seed, grid_res=grid_res, soup_triangles=soup_triangles,
+                             material_count=material_count, emissive_count=emissive_count, sphere_subdiv=sphere_subdiv,
+                             envmap_width=envmap[0] if envmap else 0, envmap_height=envmap[1] if envmap else 0, lambert=0,
+                             aspect_ratio=aspect_ratio)
+        self._h = lib().orc_procedural_scene(C.byref(p))
+        if not self._h:
+            raise RuntimeError("oracle procedural scene: " + lib().orc_last_error().decode())
+        self.desc_ptr = C.c_void_p(lib().orc_procedural_desc(self._h))
+        self.head = SceneDescHead.from_address(self.desc_ptr.value)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_procedural_free(self._h)
+            self._h = None
+
+    @property
+    def triangle_count(self) -> int:
+        inst = np.ctypeslib.as_array(C.cast(self.head.instances, C.POINTER(u32)), shape=(self.head.instance_count, 5))
+        return int(inst[:, 2].sum())
+
+    def arrays(self):
+        """(vertices [N, 12] float32, indices, instances [I, 5], materials [M, 19] float32 view) copies."""
+        h = self.head
+        v = np.ctypeslib.as_array(C.cast(h.vertices, C.POINTER(C.c_float)), shape=(h.vertex_count * 12,)).copy()
+        i = np.ctypeslib.as_array(C.cast(h.indices, C.POINTER(u32)), shape=(h.index_count,)).copy()
+        n = np.ctypeslib.as_array(C.cast(h.instances, C.POINTER(u32)), shape=(h.instance_count * 5,)).copy()
+        m = np.ctypeslib.as_array(C.cast(h.materials, C.POINTER(u32)), shape=(h.material_count * 19,)).copy()
+        return v.reshape(-1, 12), i, n.reshape(-1, 5), m.reshape(-1, 19)
+
+    def oracle_scene(self) -> "OracleScene":
+        return OracleScene(self.desc_ptr)
 
 
 class OracleScene:

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "oracle_render.h"
+#include "../falcor_b200/csrc/procedural.h"
 
 using namespace orc;
 
@@ -33,6 +34,19 @@ void* orc_scene_create(const fpt_scene_desc* d, const fpt_camera_data* cam) {
     }
 }
 void orc_scene_destroy(void* s) { delete static_cast<Scene*>(s); }
+
+// The synthetic workloads (falcor_b200/csrc/procedural.h, compiled into this
+// library too), so that the oracle renders them without the CUDA library.
+void* orc_procedural_scene(const fpt_procedural_params* p) {
+    try {
+        return build_procedural_scene(*p);
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+const fpt_scene_desc* orc_procedural_desc(const void* h) { return &static_cast<const fpt_scene_host*>(h)->desc; }
+void orc_procedural_free(void* h) { delete static_cast<fpt_scene_host*>(h); }
 void orc_camera_compute(const fpt_camera* c, fpt_camera_data* out) { camera_data_from(*c, *out); }
 
 struct orc_scene_info {

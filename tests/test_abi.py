@@ -5,6 +5,7 @@ import re
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
 
@@ -130,3 +131,35 @@ def test_oracle_camera_matches_library_camera(fpt, oracle):
         _ffi.check(fpt.fpt_camera_compute(C.byref(c), C.byref(lib_cd)))
         orc_cd = oracle.camera_data(c, _ffi.fpt_camera_data)
         assert bytes(lib_cd) == bytes(orc_cd)
+
+
+@pytest.mark.parametrize("kind,params", [
+    (0, dict(seed=0, sphere_subdiv=4, aspect_ratio=1.0)),
+    (1, dict(seed=1, grid_res=96, soup_triangles=3000, material_count=16, emissive_count=16, envmap=(64, 32),
+             aspect_ratio=16 / 9)),
+    (2, dict(seed=3, material_count=256, sphere_subdiv=142, emissive_count=8, envmap=(32, 16), aspect_ratio=1.0)),
+    (3, dict(seed=100, soup_triangles=10000, material_count=256, emissive_count=64, aspect_ratio=1.0)),
+    (4, dict(seed=101, grid_res=71, material_count=256, emissive_count=64, aspect_ratio=1.0)),
+])
+def test_oracle_builds_the_same_workload_scenes(fpt, oracle, kind, params):
+    """The oracle library builds the synthetic workloads itself (so the CPU
+    reference arm never loads the CUDA library); its arrays equal the
+    library's fpt_procedural_scene bit for bit."""
+    from falcor_b200.scene import HostScene
+    h = HostScene.procedural(kind, **params)
+    o = oracle.ProceduralScene(kind, **params)
+    ov, oi, on, om = o.arrays()
+    np.testing.assert_array_equal(h.vertices.view(np.uint32), ov.view(np.uint32))
+    np.testing.assert_array_equal(h.indices, oi)
+    np.testing.assert_array_equal(h.instances, on)
+    np.testing.assert_array_equal(h.materials.view(np.uint32), om)
+    assert o.triangle_count == h.triangle_count
+    from falcor_b200 import _ffi
+    od = _ffi.fpt_scene_desc.from_address(o.desc_ptr.value)
+    assert bytes(h.desc.camera) == bytes(od.camera)
+    assert bool(h.desc.envmap) == bool(od.envmap)
+    if h.desc.envmap:
+        he, oe = h.desc.envmap.contents, od.envmap.contents
+        n = he.width * he.height * 3
+        assert (he.width, he.height) == (oe.width, oe.height)
+        assert C.string_at(C.cast(he.rgb, C.c_void_p).value, 4 * n) == C.string_at(C.cast(oe.rgb, C.c_void_p).value, 4 * n)
