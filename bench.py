@@ -11,7 +11,9 @@ colour.  One step = one 64-spp frame = 132.7 M paths.
 
 Prints one JSON line (rank 0).  `--impl reference` times the CPU restatement
 of the same path (the reference's GPU path needs DXR/Vulkan, unavailable on
-this box) on a bounded crop of the same workload using all host cores.
+this box) on a bounded crop of the same workload using all host cores; that
+arm is built by the oracle alone and does not load the CUDA library.  Both
+arms carry an `rmse` block against the committed FP64 references.
 """
 from __future__ import annotations
 
@@ -147,41 +149,107 @@ def load_traffic(workload: str, kernel: str):
     return None
 
 
-def cpu_baseline(workload_name: str, seconds: float):
-    """Times the CPU oracle (FP32 PathTracer restatement) on a crop of the workload
-    on all host cores: a square crop at the frame centre (side <= 1024) rendered
-    at 16 spp for as many frames (seeds 0, 1, ...) as fill about `seconds`.
-    Returns (Mpaths/s, cores, sample description)."""
-    import numpy as np
-    from falcor_b200.scene import WORKLOADS, make_host_scene
+# The synthetic workloads as the CPU reference arm builds them, through the
+# oracle's own copy of the scene generator (the CUDA library is not loaded on
+# that arm).  Same kinds and parameters as falcor_b200.scene.WORKLOADS.
+REFERENCE_WORKLOADS = {
+    "heightfield_soup_1080p": dict(kind=1, width=1920, height=1080, max_bounces=8,
+                                   params=dict(seed=1, grid_res=1024, soup_triangles=200000, material_count=256,
+                                               emissive_count=64, envmap=(1024, 512), aspect_ratio=1920 / 1080)),
+}
+GOLDEN = ROOT / "tests" / "golden"
+
+
+def workload_config(name: str, width: int, height: int, frames: int, max_bounces: int, triangles: int, world: int) -> dict:
+    """The `config` of both arms' JSON lines (identical for the same workload)."""
+    return {"workload": name, "resolution": [width, height], "spp": SPP_PER_FRAME * frames, "frames_per_step": frames,
+            "max_bounces": max_bounces, "triangles": triangles, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (BVH, triangle records and vertices of 2.29 M triangles, ~270 MB); "
+                  "the GPU arm also writes a 256 MB buffer before every timed step"}
+
+
+def rmse(a, b) -> float:
+    return float(np.sqrt(np.mean((np.asarray(a, np.float64)[..., :3] - np.asarray(b, np.float64)[..., :3]) ** 2)))
+
+
+def golden(name: str):
+    p = GOLDEN / name
+    if not p.exists():
+        return None
+    d = np.load(p)
+    return {k: d[k] for k in d.files}
+
+
+def cpu_reference(workload_name: str, seconds: float, steps: int = 1, variant: str = "native"):
+    """Times the CPU oracle (the FP32 PathTracer restatement) on the workload
+    with all host cores, built by the oracle alone (its own scene generator,
+    camera and V-buffer; the CUDA library is not loaded): a square crop at the
+    frame centre at 16 spp, sized to about `seconds` of work per step, `steps`
+    times.  variant "native" is the -O3 -march=native -ffp-contract=fast
+    timing build compiled on this machine, "parity" the -ffp-contract=off
+    checker build.  Returns (Mpaths/s median over steps, cores, sample
+    description, the oracle scene objects)."""
     from oracle import ffi as orc
     from tests import helpers as H
-    w = WORKLOADS[workload_name]
-    host = make_host_scene(w)
-    osc = H.oracle_scene(host)
+    w = REFERENCE_WORKLOADS[workload_name]
+    ps = orc.ProceduralScene(w["kind"], variant=variant, **w["params"])
+    osc = ps.oracle_scene()
+    W, Hh = w["width"], w["height"]
     cores = os.cpu_count() or 1
-    vb = osc.vbuffer(w.width, w.height, threads=cores)
+    vb = osc.vbuffer(W, Hh, threads=cores)
     # Calibrate on a small crop, then size the sample to ~`seconds` of work.
-    cx, cy = w.width // 2 - 64, w.height // 2 - 64
-    params = H.pt_params(w.width, w.height, SPP_PER_FRAME, seed=0, max_bounces=w.max_bounces, sampler=2, color_format=1)
+    cx, cy = W // 2 - 64, Hh // 2 - 64
+    params = H.pt_params(W, Hh, SPP_PER_FRAME, seed=0, max_bounces=w["max_bounces"], sampler=2, color_format=1)
     _, _, cnt, dt = osc.path_tracer(vb, params, threads=cores, rect=(cx, cy, cx + 128, cy + 128))
     rate = max(cnt.paths, 1) / max(dt, 1e-6)
     target = rate * seconds
-    side = int(min(max(32, (target / SPP_PER_FRAME) ** 0.5), 1024, w.width, w.height))
+    side = int(min(max(32, (target / SPP_PER_FRAME) ** 0.5), 1024, W, Hh))
     side -= side % 16
-    frames = max(1, int(round(target / (side * side * SPP_PER_FRAME))))
-    x0, y0 = max(0, w.width // 2 - side // 2), max(0, w.height // 2 - side // 2)
+    x0, y0 = max(0, W // 2 - side // 2), max(0, Hh // 2 - side // 2)
     # Background pixels also count as paths in the workload's unit (they are written per sample).
     bg = int(np.sum(vb[y0:y0 + side, x0:x0 + side, 0] == 0)) * SPP_PER_FRAME
-    paths, total = 0, 0.0
-    for f in range(frames):
-        params.seed = f
+    rates = []
+    for k in range(max(1, steps)):
+        params.seed = k
         _, _, cnt, dt = osc.path_tracer(vb, params, threads=cores, rect=(x0, y0, x0 + side, y0 + side))
-        paths += cnt.paths + bg
-        total += dt
-    desc = (f"{side}x{side} crop at the frame centre, {frames} frame(s) of {SPP_PER_FRAME} spp, {w.max_bounces} bounces, "
-            f"FP32 CPU oracle (-O3 -ffp-contract=off), {paths} paths in {total:.2f} s")
-    return paths / total / 1e6, cores, desc
+        rates.append((cnt.paths + bg) / dt / 1e6)
+    flags = "-O3 -march=native -ffp-contract=fast" if variant == "native" else "-O3 -ffp-contract=off"
+    desc = (f"{side}x{side} crop at the frame centre of the {W}x{Hh} frame, {SPP_PER_FRAME} spp per step "
+            f"(seeds 0..{max(1, steps) - 1}), {w['max_bounces']} bounces, FP32 CPU oracle ({flags}), "
+            f"{cores} threads; Mpaths/s is per path, so the crop stands for the full frame")
+    return statistics.median(rates), cores, desc, (ps, osc, vb)
+
+
+def reference_rmse(workload_name: str, osc, vb) -> dict:
+    """RMSE of the FP32 oracle's images against the committed FP64 references
+    (tests/golden/fp64_*.npz): C1 (MinimalPathTracer frame 0, 1 spp) and the
+    256 x 256 centre crop of the C2 frame at the benchmark's 64 spp (4 frames
+    of 16 spp, seeds 0..3, LogLuv per sample)."""
+    from oracle import ffi as orc
+    from tests import helpers as H
+    out = {}
+    cores = os.cpu_count() or 1
+    g1 = golden("fp64_c1_box_icosphere_256.npz")
+    if g1 is not None:
+        ps1 = orc.ProceduralScene(0, seed=0, sphere_subdiv=4, aspect_ratio=1.0, variant="parity")
+        o1 = ps1.oracle_scene()
+        vb1 = o1.vbuffer(256, 256, threads=cores)
+        img, _, _ = o1.minimal_pt(vb1, H.minimal_params(256, 256, frame=0), threads=cores)
+        out["c1_1spp"] = round(rmse(img, g1["rgb"]), 5)
+        out["c1_reference_spp"] = int(g1["spp"])
+    g2 = golden("fp64_c2_crop256.npz")
+    if g2 is not None and workload_name == "heightfield_soup_1080p":
+        w = REFERENCE_WORKLOADS[workload_name]
+        x0, y0, x1, y1 = (int(v) for v in g2["rect"])
+        acc = np.zeros((y1 - y0, x1 - x0, 4), np.float64)
+        for f in range(FRAMES_PER_STEP):
+            img, _, _, _ = osc.path_tracer(vb, H.pt_params(w["width"], w["height"], SPP_PER_FRAME, seed=f,
+                                                           max_bounces=w["max_bounces"], sampler=2, color_format=1),
+                                           threads=cores, rect=(x0, y0, x1, y1))
+            acc += img[y0:y1, x0:x1]
+        out["c2_crop_64spp"] = round(rmse(acc / FRAMES_PER_STEP, g2["rgb"]), 4)
+        out["c2_reference_spp"] = int(g2["spp"])
+    return out
 
 
 def _time_ms(fn, reps: int) -> float:
@@ -366,22 +434,60 @@ def batched_bench(dev) -> dict:
             "graph_kernel_launches": int(st.kernel_launches), "device_error": int(st.device_error)}
 
 
+def gpu_rmse(accum, dev) -> dict:
+    """RMSE of the GPU images against the committed FP64 references: the C2 crop
+    of the benchmark's last 64-spp image (accum), and C1 (MinimalPathTracer,
+    box + icosphere, 256 x 256) at frame 0 (1 spp) and over frames 0..63."""
+    import torch
+    from falcor_b200.passes import MinimalPathTracer
+    from falcor_b200.scene import WORKLOADS, Scene, make_host_scene
+    from tests import helpers as H
+    out = {}
+    g2 = golden("fp64_c2_crop256.npz")
+    if g2 is not None:
+        x0, y0, x1, y1 = (int(v) for v in g2["rect"])
+        out["c2_crop_64spp"] = round(rmse(accum[y0:y1, x0:x1].cpu().numpy(), g2["rgb"]), 4)
+        out["c2_reference_spp"] = int(g2["spp"])
+    g1 = golden("fp64_c1_box_icosphere_256.npz")
+    if g1 is not None:
+        scene = Scene(make_host_scene(WORKLOADS["box_icosphere_256"]))
+        vb = H.gpu_vbuffer(scene, 256, 256)
+        mpt = MinimalPathTracer({"maxBounces": 3})
+        mpt.set_scene(scene)
+        col = torch.zeros((256, 256, 4), dtype=torch.float32, device=dev)
+        acc = torch.zeros_like(col)
+        for f in range(64):
+            mpt.execute({"vbuffer": vb, "color": col}, frame=f)
+            if f == 0:
+                out["c1_1spp"] = round(rmse(col.cpu().numpy(), g1["rgb"]), 5)
+            acc += col
+        out["c1_64spp"] = round(rmse((acc / 64).cpu().numpy(), g1["rgb"]), 5)
+        out["c1_reference_spp"] = int(g1["spp"])
+    return out
+
+
 def run_reference(args):
+    """The reference arm: the CPU restatement of the path (the reference's own
+    path needs DXR / Vulkan ray tracing, unavailable on this box), built and run
+    by the oracle alone, timed on all host cores on a bounded sample of the
+    same workload."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    value, cores, desc = cpu_baseline(args.workload, args.cpu_seconds / max(args.steps, 1))
-    vals = [value]
-    for _ in range(max(args.steps - 1, 0)):
-        v, _, _ = cpu_baseline(args.workload, args.cpu_seconds / max(args.steps, 1))
-        vals.append(v)
-    v = statistics.median(vals)
-    line = {"impl": "reference", "metric": "Mpaths/s (PathTracer forward, NEE+MIS)", "value": round(v, 4), "unit": "Mpaths/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic procedural scene",
-            "config": {"workload": args.workload},
-            "cpu_baseline": {"value": round(v, 4), "unit": "Mpaths/s", "cores": cores, "kind": "port", "sample": desc},
-            "e2e": {"value": round(v, 4), "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    w = REFERENCE_WORKLOADS[args.workload]
+    per_step = args.cpu_seconds / max(args.steps, 1)
+    value, cores, desc, (ps, osc, vb) = cpu_reference(args.workload, per_step, args.steps, "native")
+    parity, _, _, _ = cpu_reference(args.workload, per_step, 1, "parity")
+    config = workload_config(args.workload, w["width"], w["height"], FRAMES_PER_STEP, w["max_bounces"], ps.triangle_count,
+                             args.gpus)
+    line = {"impl": "reference", "metric": "Mpaths/s (PathTracer forward, NEE+MIS)", "value": round(value, 4),
+            "unit": "Mpaths/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic procedural scene (seeded), no dataset",
+            "config": config,
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mpaths/s", "cores": cores, "kind": "port", "sample": desc,
+                             "parity_build_value": round(parity, 4)},
+            "e2e": {"value": round(value, 4), "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "rmse": reference_rmse(args.workload, osc, vb),
             "note": "reference GPU path (Slang on DXR/Vulkan RT) unavailable on this box; CPU restatement timed instead"}
     print(json.dumps(line), flush=True)
 
@@ -520,11 +626,9 @@ def main():
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic procedural scene (seeded), no dataset",
-        "config": {"workload": w.name, "resolution": [W, Hh], "spp": SPP_PER_FRAME * frames,
-                   "frames_per_step": frames, "max_bounces": w.max_bounces,
-                   "triangles": scene.info.triangle_count, "emissive_triangles": scene.info.emissive_triangle_count,
-                   "bvh_nodes": scene.info.bvh_node_count, "bvh_build_s": round(scene.info.bvh_build_seconds, 3),
-                   "parallelism": f"replicas x{world}", "l2_flush": "256 MB buffer written before every timed step"},
+        "config": workload_config(w.name, W, Hh, frames, w.max_bounces, scene.info.triangle_count, world),
+        "scene": {"emissive_triangles": scene.info.emissive_triangle_count, "bvh_nodes": scene.info.bvh_node_count,
+                  "bvh_build_s": round(scene.info.bvh_build_seconds, 3)},
         "mrays_per_s": round(rays_per_step * world / (ms_per_step / 1e3) / 1e6, 3),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "traffic": None if args.resolution else load_traffic(w.name, dominant), "peak_kind": peak_kind,
@@ -543,8 +647,10 @@ def main():
         line["adjoint"] = adjoint_bench(dev)
         line["batched"] = batched_bench(dev)
         line["inverse"] = inverse_bench(dev)
+    if not args.resolution and w.name == "heightfield_soup_1080p":
+        line["rmse"] = gpu_rmse(accum, dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, desc = cpu_baseline(w.name, args.cpu_seconds)
+        v, cores, desc, _ = cpu_reference(w.name, args.cpu_seconds, 1, "native")
         line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpaths/s", "cores": cores, "kind": "port", "sample": desc}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -62,21 +62,37 @@ class SceneDescHead(C.Structure):
                 ("instances", _P), ("instance_count", u32), ("materials", _P), ("material_count", u32)]
 
 
-_lib = None
+_libs: dict = {}
+NATIVE_DIR = ORACLE_DIR / "_build" / "native"
 
 
 def build() -> Path:
-    """Builds liboracle.so with the committed Makefile."""
+    """Builds liboracle.so (the parity build) with the committed Makefile."""
     subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True)
     return LIB_PATH
 
 
-def lib() -> C.CDLL:
-    global _lib
-    if _lib is None:
-        if not LIB_PATH.exists():
-            build()
-        l = C.CDLL(str(LIB_PATH))
+def native_path() -> Path:
+    """The timing build of this machine: -O3 -march=native -ffp-contract=fast,
+    compiled on the machine that runs it (the instruction set is the host's)."""
+    import platform
+    return NATIVE_DIR / platform.node() / "liboracle.so"
+
+
+def build_native() -> Path:
+    out = native_path()
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "native", f"NATIVE_OUT={out}"], check=True)
+    return out
+
+
+def lib(variant: str = "parity") -> C.CDLL:
+    """The oracle library: "parity" (-ffp-contract=off, the checker) or
+    "native" (the contracting, host-tuned timing build; CPU baseline only)."""
+    if variant not in _libs:
+        path = LIB_PATH if variant == "parity" else native_path()
+        if not path.exists():
+            build() if variant == "parity" else build_native()
+        l = C.CDLL(str(path))
         l.orc_scene_create.restype = _P
         l.orc_scene_create.argtypes = [_P, _P]
         l.orc_scene_destroy.argtypes = [_P]
@@ -123,8 +139,8 @@ def lib() -> C.CDLL:
         l.orc_intersect_triangle.argtypes = [_P, _P, _P, _P, _P]
         l.orc_sample_pattern.argtypes = [C.c_int, u32, u32, _P]
         l.orc_bsdf_sample.argtypes = [_P, C.c_int, u32, _P, _P, u32, _P, _P, _P, _P, _P, _P, _P]
-        _lib = l
-    return _lib
+        _libs[variant] = l
+    return _libs[variant]
 
 
 def ptr(a: np.ndarray) -> C.c_void_p:
@@ -137,20 +153,23 @@ class ProceduralScene:
     generator the CUDA library compiles), without loading the CUDA library."""
 
     def __init__(self, kind: int, seed: int = 0, grid_res: int = 0, soup_triangles: int = 0, material_count: int = 0,
-                 emissive_count: int = 0, sphere_subdiv: int = 0, envmap=None, aspect_ratio: float = 0.0):
+                 emissive_count: int = 0, sphere_subdiv: int = 0, envmap=None, aspect_ratio: float = 0.0,
+                 variant: str = "parity"):
+        self._l = lib(variant)
+        self.variant = variant
         p = ProceduralParams(kind=kind, seed=seed, grid_res=grid_res, soup_triangles=soup_triangles,
                              material_count=material_count, emissive_count=emissive_count, sphere_subdiv=sphere_subdiv,
                              envmap_width=envmap[0] if envmap else 0, envmap_height=envmap[1] if envmap else 0, lambert=0,
                              aspect_ratio=aspect_ratio)
-        self._h = lib().orc_procedural_scene(C.byref(p))
+        self._h = self._l.orc_procedural_scene(C.byref(p))
         if not self._h:
-            raise RuntimeError("oracle procedural scene: " + lib().orc_last_error().decode())
-        self.desc_ptr = C.c_void_p(lib().orc_procedural_desc(self._h))
+            raise RuntimeError("oracle procedural scene: " + self._l.orc_last_error().decode())
+        self.desc_ptr = C.c_void_p(self._l.orc_procedural_desc(self._h))
         self.head = SceneDescHead.from_address(self.desc_ptr.value)
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().orc_procedural_free(self._h)
+            self._l.orc_procedural_free(self._h)
             self._h = None
 
     @property
@@ -168,30 +187,31 @@ class ProceduralScene:
         return v.reshape(-1, 12), i, n.reshape(-1, 5), m.reshape(-1, 19)
 
     def oracle_scene(self) -> "OracleScene":
-        return OracleScene(self.desc_ptr)
+        return OracleScene(self.desc_ptr, variant=self.variant)
 
 
 class OracleScene:
     """The oracle's copy of a scene, built from the same host description."""
 
-    def __init__(self, desc_ptr, camera_data=None):
+    def __init__(self, desc_ptr, camera_data=None, variant: str = "parity"):
         """camera_data None: the oracle computes the camera vectors from the
         description's camera itself (Camera.cpp:112-195)."""
+        self._l = lib(variant)
         cam = C.cast(C.pointer(camera_data), _P) if camera_data is not None else None
-        self._h = lib().orc_scene_create(C.cast(desc_ptr, _P), cam)
+        self._h = self._l.orc_scene_create(C.cast(desc_ptr, _P), cam)
         if not self._h:
             raise RuntimeError("oracle scene creation failed")
         self.info = SceneInfo()
-        lib().orc_scene_get_info(self._h, C.byref(self.info))
+        self._l.orc_scene_get_info(self._h, C.byref(self.info))
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().orc_scene_destroy(self._h)
+            self._l.orc_scene_destroy(self._h)
             self._h = None
 
     def vbuffer(self, w: int, h: int, threads: int = 0) -> np.ndarray:
         out = np.zeros((h, w, 4), dtype=np.uint32)
-        lib().orc_vbuffer(self._h, w, h, ptr(out), threads)
+        self._l.orc_vbuffer(self._h, w, h, ptr(out), threads)
         return out
 
     def trace_closest(self, o: np.ndarray, d: np.ndarray, tmin: np.ndarray, tmax: np.ndarray, brute: bool = False):
@@ -202,7 +222,7 @@ class OracleScene:
         tmax = np.ascontiguousarray(tmax, dtype=np.float32)
         out = np.zeros((n, 4), dtype=np.uint32)
         t = np.zeros(n, dtype=np.float32)
-        lib().orc_trace_closest(self._h, n, ptr(o), ptr(d), ptr(tmin), ptr(tmax), ptr(out), ptr(t), int(brute))
+        self._l.orc_trace_closest(self._h, n, ptr(o), ptr(d), ptr(tmin), ptr(tmax), ptr(out), ptr(t), int(brute))
         return out, t
 
     def minimal_pt(self, vbuffer: np.ndarray, params: MinimalPTParams, fp64: bool = False, threads: int = 0, rect=None,
@@ -213,7 +233,7 @@ class OracleScene:
         rays = np.zeros((h, w), dtype=np.uint32)
         tr = np.zeros((h, w, params.maxBounces + 2, 4), dtype=np.uint32) if trace else None
         x0, y0, x1, y1 = rect if rect else (0, 0, w, h)
-        dt = lib().orc_minimal_pt(self._h, C.byref(params), ptr(np.ascontiguousarray(vbuffer)), ptr(out), ptr(rays),
+        dt = self._l.orc_minimal_pt(self._h, C.byref(params), ptr(np.ascontiguousarray(vbuffer)), ptr(out), ptr(rays),
                                   int(fp64), threads, x0, y0, x1, y1, ptr(tr) if tr is not None else None)
         return (out, rays, dt, tr) if trace else (out, rays, dt)
 
@@ -227,7 +247,7 @@ class OracleScene:
         cnt = Counters()
         tr = np.zeros((h, w, params.samplesPerPixel, params.maxSurfaceBounces + 2, 4), dtype=np.uint32) if trace else None
         x0, y0, x1, y1 = rect if rect else (0, 0, w, h)
-        dt = lib().orc_path_tracer(self._h, C.byref(params), ptr(np.ascontiguousarray(vbuffer)), ptr(out),
+        dt = self._l.orc_path_tracer(self._h, C.byref(params), ptr(np.ascontiguousarray(vbuffer)), ptr(out),
                                    ptr(smp) if smp is not None else None, int(fp64), threads, x0, y0, x1, y1, C.byref(cnt),
                                    ptr(tr) if tr is not None else None)
         return (out, smp, cnt, dt, tr) if trace else (out, smp, cnt, dt)
@@ -262,7 +282,7 @@ class OracleScene:
         g = np.ascontiguousarray(dLdI, dtype=np.float32) if dLdI is not None else None
         x0, y0, x1, y1 = rect if rect else (0, 0, w, h)
         rays = C.c_uint64()
-        dt = lib().orc_wardiff(self._h, C.byref(params), mode, K, ptr(mt) if mt is not None else None,
+        dt = self._l.orc_wardiff(self._h, C.byref(params), mode, K, ptr(mt) if mt is not None else None,
                                mt.shape[1] if mt is not None else 0, ptr(pt) if pt is not None else None,
                                pt.shape[1] if pt is not None else 0, ptr(nt) if nt is not None else None,
                                nt.shape[1] if nt is not None else 0, ptr(tt) if tt is not None else None,
@@ -273,23 +293,23 @@ class OracleScene:
     def light_bvh(self):
         """(nodes [n, 8] uint32, leaf triangle indices, per-triangle bit paths uint64)."""
         a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
-        lib().orc_scene_light_bvh_sizes(self._h, C.byref(a), C.byref(b), C.byref(c))
+        self._l.orc_scene_light_bvh_sizes(self._h, C.byref(a), C.byref(b), C.byref(c))
         nodes = np.zeros(8 * a.value, dtype=np.uint32)
         tris = np.zeros(b.value, dtype=np.uint32)
         masks = np.zeros(c.value, dtype=np.uint64)
-        lib().orc_scene_get_light_bvh(self._h, ptr(nodes), ptr(tris), ptr(masks))
+        self._l.orc_scene_get_light_bvh(self._h, ptr(nodes), ptr(tris), ptr(masks))
         return nodes.reshape(-1, 8), tris, masks
 
     def lbvh_selection_pdf(self, pos, normal, upper, tri) -> float:
         p = np.ascontiguousarray(pos, np.float32)
         n = np.ascontiguousarray(normal, np.float32)
-        return float(lib().orc_lbvh_selection_pdf(self._h, ptr(p), ptr(n), int(upper), int(tri)))
+        return float(self._l.orc_lbvh_selection_pdf(self._h, ptr(p), ptr(n), int(upper), int(tri)))
 
     def lbvh_select(self, pos, normal, upper, u):
         p = np.ascontiguousarray(pos, np.float32)
         n = np.ascontiguousarray(normal, np.float32)
         t, pdf = C.c_uint32(), C.c_float()
-        ok = lib().orc_lbvh_select(self._h, ptr(p), ptr(n), int(upper), float(u), C.byref(t), C.byref(pdf))
+        ok = self._l.orc_lbvh_select(self._h, ptr(p), ptr(n), int(upper), float(u), C.byref(t), C.byref(pdf))
         return (int(t.value), float(pdf.value)) if ok else None
 
     def lights(self):
@@ -297,13 +317,13 @@ class OracleScene:
         alias = np.zeros(2 * max(n, 1), dtype=np.uint32)
         flux = np.zeros(max(n, 1), dtype=np.float32)
         area = np.zeros(max(n, 1), dtype=np.float32)
-        lib().orc_scene_get_lights(self._h, ptr(alias), ptr(flux), ptr(area))
+        self._l.orc_scene_get_lights(self._h, ptr(alias), ptr(flux), ptr(area))
         return alias[: 2 * n], flux[:n], area[:n]
 
     def importance(self, mip: int = 0) -> np.ndarray:
         d = self.info.imp_dim >> mip
         out = np.zeros((d, d), dtype=np.float32)
-        lib().orc_scene_get_importance(self._h, mip, ptr(out))
+        self._l.orc_scene_get_importance(self._h, mip, ptr(out))
         return out
 
 
