@@ -116,7 +116,7 @@ Program find_program(const std::string& entry) {
                 out->setElement<Falcor::float3>(i, Falcor::float3(r.x, r.y, r.z));
             }
         };
-    return nullptr;
+    return find_program_bsdf(entry);
 }
 
 }  // namespace kat
@@ -153,9 +153,18 @@ static void check_float16() {
     for (int i = 0; i < (1 << 22); i++) check(rng());
 }
 
-int main() {
+// Usage: kat_runner [substring ...] -- runs the tests whose names contain one
+// of the substrings (all tests and the fp16 check without arguments).
+int main(int argc, char** argv) {
     int failedTests = 0, passed = 0, skipped = 0;
+    auto selected = [&](const std::string& name) {
+        if (argc < 2) return true;
+        for (int i = 1; i < argc; i++)
+            if (name.find(argv[i]) != std::string::npos) return true;
+        return false;
+    };
     for (auto& t : kat::tests()) {
+        if (!selected(t.name)) continue;
         if (t.opt.disabled) {
             std::printf("SKIP %-36s (disabled in the reference)\n", t.name.c_str());
             skipped++;
@@ -173,7 +182,7 @@ int main() {
                 t.cpu(ctx);
             }
         } catch (const std::exception& e) {
-            if (kat::g_missingProgram) {
+            if (kat::g_missingProgram || std::string(e.what()).find("no oracle restatement") != std::string::npos) {
                 std::printf("SKIP %-36s (%s)\n", t.name.c_str(), e.what());
                 skipped++;
                 continue;
@@ -186,6 +195,10 @@ int main() {
         std::printf("%s %-36s %llu checks, %llu failed\n", nf ? "FAIL" : "PASS", t.name.c_str(), (unsigned long long)nc,
                     (unsigned long long)nf);
         if (nf) failedTests++; else passed++;
+    }
+    if (!selected("Float16Conversions")) {
+        std::printf("SUMMARY passed=%d failed=%d skipped=%d\n", passed, failedTests, skipped);
+        return failedTests ? 1 : 0;
     }
     const uint64_t f0 = kat::g_fail, c0 = kat::g_checks;
     check_float16();

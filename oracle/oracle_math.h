@@ -657,6 +657,7 @@ template <class R> struct StandardBSDF {
     R diffTrans, specTrans;
     R pDiffuseReflection, pDiffuseTransmission, pSpecularReflection, pSpecularTransmission;
 
+    StandardBSDF() = default;  // lobes set field by field (single-lobe unit tests)
     StandardBSDF(const V3<R>& wi, const BSDFData<R>& d, bool thinSurface, uint32_t lobes, bool lambertDiffuse) {
         lambert = lambertDiffuse;
         V3<R> transmissionAlbedo = thinSurface ? d.transmission

@@ -8,10 +8,13 @@
 // CPU implementations.
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <filesystem>
 #include <functional>
+#include <iterator>
 #include <map>
 #include <memory>
 #include <sstream>
@@ -60,6 +63,11 @@ struct int3 {
     int3() = default;
     int3(int a, int b, int c) : x(a), y(b), z(c) {}
 };
+struct uint2 {
+    uint32_t x = 0, y = 0;
+    uint2() = default;
+    uint2(uint32_t a, uint32_t b) : x(a), y(b) {}
+};
 struct uint4 {
     uint32_t x = 0, y = 0, z = 0, w = 0;
     uint4() = default;
@@ -81,7 +89,17 @@ enum class ResourceBindFlags { None = 0, ShaderResource = 1, UnorderedAccess = 2
 inline ResourceBindFlags operator|(ResourceBindFlags a, ResourceBindFlags b) { return ResourceBindFlags(int(a) | int(b)); }
 enum class MemoryType { DeviceLocal };
 enum class SlangCompilerFlags { None = 0, FloatingPointModePrecise = 1 };
-struct DefineList {};
+struct DefineList {
+    std::map<std::string, std::string> values;
+    DefineList& add(const std::string& name, const std::string& value = "") { values[name] = value; return *this; }
+};
+enum class ResourceFormat { RGB32Float };
+// Image output of a test (histogram dumps); not used by the shimmed runs.
+struct Bitmap {
+    enum class FileFormat { ExrFile };
+    enum class ExportFlags { None };
+    static void saveImage(const std::filesystem::path&, uint32_t, uint32_t, FileFormat, ExportFlags, ResourceFormat, bool, void*) {}
+};
 
 class Buffer {
 public:
@@ -108,9 +126,28 @@ public:
     void clearUAV(Buffer* b, uint4 v) { std::fill(b->data.begin(), b->data.end(), uint8_t(v.x)); }
 };
 
+class GPUUnitTestContext;
+// A named shader variable of the fake program ("CB.sz", "gSamplingTest.testWi").
+struct ShaderVar {
+    GPUUnitTestContext* ctx;
+    std::string name;
+    ShaderVar operator[](const char* sub) const { return ShaderVar{ctx, name + "." + sub}; }
+    const ShaderVar& operator=(const ref<Buffer>& b) const;
+    const ShaderVar& operator=(uint32_t v) const;
+    const ShaderVar& operator=(uint2 v) const;
+    std::string leaf() const { const size_t p = name.rfind('.'); return p == std::string::npos ? name : name.substr(p + 1); }
+};
+
 class Device {
 public:
     enum class Type { Default, D3D12, Vulkan };
+    RenderContext renderContext;
+    RenderContext* getRenderContext() { return &renderContext; }
+    // Structured buffer typed by the shader variable it is created for; the
+    // element size comes from the oracle's restatement of that program.
+    ref<Buffer> createStructuredBuffer(const ShaderVar& var, uint32_t n,
+                                       ResourceBindFlags = ResourceBindFlags::ShaderResource, MemoryType = MemoryType::DeviceLocal,
+                                       const void* init = nullptr);
     ref<Buffer> createBuffer(size_t size, ResourceBindFlags, MemoryType, const void* init) {
         auto b = std::make_shared<Buffer>();
         b->data.resize(size);
@@ -136,14 +173,16 @@ public:
     }
 };
 
-class GPUUnitTestContext;
-
 }  // namespace Falcor
 
 namespace kat {
+// Element size of a structured-buffer variable of a shimmed program (by leaf name).
+size_t element_size(const std::string& leaf);
 // The oracle-side implementation of a Slang test program (kat_main.cpp).
 using Program = std::function<void(Falcor::GPUUnitTestContext&, uint32_t, uint32_t, uint32_t)>;
 Program find_program(const std::string& entry);
+// Programs of the BSDF sampling and scene-gradient tests (kat_bsdf.cpp).
+Program find_program_bsdf(const std::string& entry);
 struct Failure { std::string test, expr, file; int line; };
 void record(bool ok, const char* expr, const char* file, int line);
 struct Expect {
@@ -168,22 +207,20 @@ namespace Falcor {
 
 class GPUUnitTestContext {
 public:
-    struct Var {
-        GPUUnitTestContext* ctx;
-        std::string name;
-        Var operator[](const char* sub) { return Var{ctx, name + "." + sub}; }
-        Var& operator=(const ref<Buffer>& b) { ctx->buffers[name] = b; return *this; }
-        Var& operator=(uint32_t v) { ctx->constants[name] = v; return *this; }
-    };
+    using Var = ShaderVar;
     std::map<std::string, ref<Buffer>> buffers;
     std::map<std::string, uint32_t> constants;
+    std::map<std::string, std::string> defines;
+    std::map<std::string, const void*> blocks;  // parameter blocks bound by host objects (SceneGradients)
     std::string entry;
     Device device;
-    RenderContext renderContext;
 
     ref<Device> getDevice() { return ref<Device>(&device, [](Device*) {}); }
-    RenderContext* getRenderContext() { return &renderContext; }
-    void createProgram(const std::string&, const std::string& e, DefineList = {}, SlangCompilerFlags = SlangCompilerFlags::None) { entry = e; }
+    RenderContext* getRenderContext() { return device.getRenderContext(); }
+    void createProgram(const std::string&, const std::string& e, DefineList d = {}, SlangCompilerFlags = SlangCompilerFlags::None) {
+        entry = e;
+        defines = d.values;
+    }
     void allocateStructuredBuffer(const std::string& name, uint32_t n, const void* init = nullptr, size_t size = 0) {
         auto b = std::make_shared<Buffer>();
         b->elementCount = n;
@@ -194,6 +231,23 @@ public:
     void runProgram(uint32_t x, uint32_t y = 1, uint32_t z = 1);
     template <class T> std::vector<T> readBuffer(const std::string& name) { return buffers.at(name)->getElements<T>(); }
 };
+
+inline const ShaderVar& ShaderVar::operator=(const ref<Buffer>& b) const { ctx->buffers[name] = b; return *this; }
+inline const ShaderVar& ShaderVar::operator=(uint32_t v) const { ctx->constants[name] = v; return *this; }
+inline const ShaderVar& ShaderVar::operator=(uint2 v) const {
+    ctx->constants[name + ".x"] = v.x;
+    ctx->constants[name + ".y"] = v.y;
+    return *this;
+}
+inline ref<Buffer> Device::createStructuredBuffer(const ShaderVar& var, uint32_t n, ResourceBindFlags, MemoryType, const void* init) {
+    const size_t es = kat::element_size(var.leaf());
+    auto b = std::make_shared<Buffer>();
+    b->data.assign(es * n, 0);
+    if (init) std::memcpy(b->data.data(), init, es * n);
+    b->elementSize = es;
+    b->elementCount = n;
+    return b;
+}
 
 }  // namespace Falcor
 

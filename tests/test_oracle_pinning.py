@@ -3,9 +3,11 @@
 oracle/_ref/kat_runner is built (by __graft_entry__.build() or
 `make -f ref.mk` in oracle/) from the reference's unit-test sources
 (Tests/Sampling/PseudorandomTests.cpp, Tests/Utils/HashUtilsTests.cpp,
-Tests/Utils/BitTricksTests.cpp, Tests/Utils/GeometryHelpersTests.cpp) and the
-reference's Utils/Math/Float16.cpp; the tests' Slang programs are replaced by
-the oracle, so the reference's own EXPECT_EQ checks decide whether the oracle passes.
+Tests/Utils/BitTricksTests.cpp, Tests/Utils/GeometryHelpersTests.cpp,
+Tests/Scene/Material/BSDFTests.cpp, Tests/DiffRendering/SceneGradientsTest.cpp)
+and the reference's Utils/Math/Float16.cpp; the tests' Slang programs are
+replaced by the oracle, so the reference's own EXPECT checks decide whether the
+oracle passes.
 """
 import subprocess
 from pathlib import Path
@@ -29,11 +31,28 @@ def _runner():
 
 
 def test_reference_known_answer_tests_pass_against_oracle():
-    out = subprocess.run([str(_runner())], capture_output=True, text=True, timeout=300)
+    names = ("XoshiroPRNG", "SplitMixPRNG", "LCGPRNG", "JenkinsHash_CompareToCPU", "BitInterleave", "ComputeRayOrigin",
+             "Float16Conversions")
+    out = subprocess.run([str(_runner()), *names], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     lines = {l.split()[1]: l.split()[0] for l in out.stdout.splitlines() if l[:4] in ("PASS", "FAIL", "SKIP")}
-    for name in ("XoshiroPRNG", "SplitMixPRNG", "LCGPRNG", "JenkinsHash_CompareToCPU", "BitInterleave",
-                 "ComputeRayOrigin", "Float16Conversions"):
+    for name in names:
+        assert lines.get(name) == "PASS", (name, out.stdout)
+
+
+def test_reference_bsdf_sampling_and_gradient_tests_pass_against_oracle():
+    """The reference's Tests/Scene/Material/BSDFTests.cpp (chi^2 over 130 x 65
+    bins of 64 M samples per configuration, hypothesis::chi2_test at
+    significance 0.01, and sampled weight / pdf within 1e-3 of eval / evalPdf)
+    and Tests/DiffRendering/SceneGradientsTest.cpp (AggregateGradients: 1024
+    atomic adds of 10^i per element, hashed, then aggregated, within 1e-6),
+    compiled unmodified, judge the oracle's lobes of StandardBSDF and its
+    gradient accumulation.  BSDFs off the hot path are reported as skipped."""
+    out = subprocess.run([str(_runner()), "TestBsdf", "AggregateGradients"], capture_output=True, text=True, timeout=900)
+    assert out.returncode == 0, out.stdout + out.stderr
+    lines = {l.split()[1]: l.split()[0] for l in out.stdout.splitlines() if l[:4] in ("PASS", "FAIL", "SKIP")}
+    for name in ("TestBsdf_FrostbiteDiffuseBRDF", "TestBsdf_LambertDiffuseBRDF", "TestBsdf_LambertDiffuseBTDF",
+                 "TestBsdf_SpecularMicrofacetBRDF", "AggregateGradients"):
         assert lines.get(name) == "PASS", (name, out.stdout)
 
 
