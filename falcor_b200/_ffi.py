@@ -58,6 +58,11 @@ class fpt_procedural_params(C.Structure):
                 ("lambert", u32), ("aspect_ratio", f32)]
 
 
+class fpt_bsdf_probe(C.Structure):
+    _fields_ = [("lobe", u32), ("wi", f32 * 3), ("params", f32 * 4), ("sample_count", u32), ("thread_sample_count", u32),
+                ("phi_bins", u32), ("cos_bins", u32), ("bin_sample_count", u32)]
+
+
 class fpt_hitinfo_bits(C.Structure):
     _fields_ = [("type_bits", u32), ("instance_id_bits", u32), ("primitive_index_bits", u32)]
 
@@ -144,6 +149,7 @@ SIGNATURES = {
     "fpt_pass_reset": (C.c_int, [_P]),
     "fpt_pass_execute_noalloc": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P]),
     "fpt_fmath_eval": (C.c_int, [u32, u32, u32, _P, _P, _P, _P]),
+    "fpt_bsdf_probe_run": (C.c_int, [C.POINTER(fpt_bsdf_probe), _P, _P, _P, _P, _P]),
     "fpt_pass_backward": (C.c_int, [_P, C.POINTER(fpt_frame_io), _P, C.POINTER(fpt_grad_buffers), _P]),
     "fpt_scene_gradients_create": (C.c_int, [C.POINTER(fpt_grad_config), u32, C.POINTER(_P)]),
     "fpt_scene_gradients_destroy": (None, [_P]),

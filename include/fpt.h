@@ -372,6 +372,32 @@ typedef enum fpt_fmath_fn {
 FPT_API fpt_status fpt_fmath_eval(uint32_t fn, uint32_t cuda_libm, uint32_t n, const float* x, const float* y, float* out,
                                   void* stream);
 
+/* The three programs of the reference's BSDF unit test
+ * (Tools/FalcorTest/Tests/Scene/Material/BSDFTests.cpp:242-300 with
+ * BSDFTests.cs.slang) run on the kernels' StandardBSDF with one lobe active:
+ * `histogram` (phi_bins * cos_bins uint32, caller-zeroed) counts sampled
+ * directions; `weight_error` / `pdf_error` (same size, caller-zeroed, float
+ * bits) keep each bin's largest relative error of the sampled weight and pdf
+ * against eval / evalPdf; `pdf_integral` (double per bin) is the midpoint
+ * integral of evalPdf over the bin times sample_count.  Null outputs are
+ * skipped.  sample_count / thread_sample_count threads each draw
+ * thread_sample_count samples.  A test hook for the sampling statistics. */
+typedef enum fpt_bsdf_probe_lobe {
+    FPT_PROBE_FROSTBITE_BRDF = 0,   /* params[0] = roughness                  */
+    FPT_PROBE_LAMBERT_BRDF = 1,
+    FPT_PROBE_LAMBERT_BTDF = 2,
+    FPT_PROBE_MICROFACET_BRDF = 3   /* params[0] = GGX alpha                   */
+} fpt_bsdf_probe_lobe;
+typedef struct fpt_bsdf_probe {
+    uint32_t lobe;
+    float wi[3];
+    float params[4];
+    uint32_t sample_count, thread_sample_count;
+    uint32_t phi_bins, cos_bins, bin_sample_count;
+} fpt_bsdf_probe;
+FPT_API fpt_status fpt_bsdf_probe_run(const fpt_bsdf_probe* probe, uint32_t* histogram, uint32_t* weight_error,
+                                      uint32_t* pdf_error, double* pdf_integral, void* stream);
+
 /* PathTracer execute that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot call cudaMalloc -- a host whose device
  * memory is reserved for its own pool, or a frame loop that must not take the
