@@ -155,6 +155,7 @@ SIGNATURES = {
     "fpt_scene_gradients_destroy": (None, [_P]),
     "fpt_scene_gradients_clear": (C.c_int, [_P, u32, _P]),
     "fpt_scene_gradients_aggregate": (C.c_int, [_P, u32, _P]),
+    "fpt_scene_gradients_atomic_add": (C.c_int, [_P, u32, u32, _P, _P, _P, _P]),
     "fpt_scene_gradients_get": (C.c_int, [_P, u32, C.POINTER(C.POINTER(C.c_float)), C.POINTER(u32), C.POINTER(u32)]),
     "fpt_pass_set_scene_gradients": (C.c_int, [_P, _P]),
     "fpt_pass_set_dLdI": (C.c_int, [_P, _P]),

@@ -200,6 +200,39 @@ FPT_D float war_dbg_tangent(const WarParams& p, uint32_t slot) {
     return i == 0 ? p.dbgGrad.x : (i == 1 ? p.dbgGrad.y : p.dbgGrad.z);
 }
 
+// Warp-aggregated gradient atomics (SceneGradients::atomicAddGrad,
+// DiffRendering/SceneGradients.slang:50-57, InterlockedAddF32): the lanes of a
+// warp that add to the same N-float row find one another with match.any, sum
+// their values with shuffles, and the lowest lane of each group issues one
+// atomic per non-zero float.  Lanes adding to distinct rows pay one match, one
+// max-reduction and one shuffle per value.
+template <int N>
+FPT_D void atomic_add_row(float* row, const float (&v)[N]) {
+    const uint32_t active = __activemask();
+    const uint32_t peers = __match_any_sync(active, reinterpret_cast<unsigned long long>(row));
+    uint32_t lane;
+    asm("mov.u32 %0, %%laneid;" : "=r"(lane));
+    const uint32_t rounds = __reduce_max_sync(active, uint32_t(__popc(peers)));
+    float sum[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) sum[i] = 0.f;
+    uint32_t rem = peers;
+    for (uint32_t k = 0; k < rounds; k++) {
+        const int src = rem ? __ffs(rem) - 1 : int(lane);
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            const float x = __shfl_sync(active, v[i], src);
+            if (rem) sum[i] += x;
+        }
+        if (rem) rem &= rem - 1u;
+    }
+    if (int(lane) == __ffs(peers) - 1) {
+#pragma unroll
+        for (int i = 0; i < N; i++)
+            if (sum[i] != 0.f) atomicAdd(row + i, sum[i]);
+    }
+}
+
 // Material-parameter gradients G[0..10] of material matID from pixel pid.
 FPT_D void add_material_grad_values(const WarParams& p, uint32_t pid, uint32_t hash, uint32_t matID, const float (&G)[11]) {
     if (p.dbgColor && p.dbgType == kDbgMaterial) {
@@ -213,10 +246,7 @@ FPT_D void add_material_grad_values(const WarParams& p, uint32_t pid, uint32_t h
     if (!p.gradMat) return;
     const uint32_t base = matID * kMatParams;
     if (base + 11 > p.matDim) return;
-    float* g = p.gradMat + size_t(hash) * p.matDim + base;
-#pragma unroll
-    for (int i = 0; i < 11; i++)
-        if (G[i] != 0.f) atomicAdd(g + i, G[i]);
+    atomic_add_row<11>(p.gradMat + size_t(hash) * p.matDim + base, G);
 }
 
 // Adds sum_c G_c * J_c[i] for the 11 material parameters.
@@ -243,9 +273,8 @@ FPT_D void add_position_grad(const WarParams& p, uint32_t pid, const uint32_t (&
     for (int v = 0; v < 3; v++) {
         const uint32_t o = off[v];
         if (o + 3 > p.posDim) continue;
-        atomicAdd(gp + o, b[v] * g.x);
-        atomicAdd(gp + o + 1, b[v] * g.y);
-        atomicAdd(gp + o + 2, b[v] * g.z);
+        const float row[3] = {b[v] * g.x, b[v] * g.y, b[v] * g.z};
+        atomic_add_row<3>(gp + o, row);
     }
 }
 FPT_D void add_position_grad(const WarParams& p, uint32_t pid, const WarIsect& is, float3 g) {
@@ -303,14 +332,12 @@ FPT_D void add_frame_grad(const WarParams& p, uint32_t pid, const uint32_t (&off
     for (int v = 0; v < 3; v++) {
         const uint32_t o = off[v];
         if (an && o + 3 <= p.nrmDim) {
-            atomicAdd(an + o, b[v] * gn.x);
-            atomicAdd(an + o + 1, b[v] * gn.y);
-            atomicAdd(an + o + 2, b[v] * gn.z);
+            const float row[3] = {b[v] * gn.x, b[v] * gn.y, b[v] * gn.z};
+            atomic_add_row<3>(an + o, row);
         }
         if (at && o + 3 <= p.tanDim && (gt.x != 0.f || gt.y != 0.f || gt.z != 0.f)) {
-            atomicAdd(at + o, b[v] * gt.x);
-            atomicAdd(at + o + 1, b[v] * gt.y);
-            atomicAdd(at + o + 2, b[v] * gt.z);
+            const float row[3] = {b[v] * gt.x, b[v] * gt.y, b[v] * gt.z};
+            atomic_add_row<3>(at + o, row);
         }
     }
 }

@@ -271,6 +271,18 @@ __global__ void war_aggregate(const float* tmp, float* out, uint32_t dim, uint32
     }
 }
 
+// SceneGradients::atomicAddGrad over arrays of contributions: value i goes to
+// scratch row hashIndex[i], element gradIndex[i] (ignored beyond the dimension).
+__global__ void war_atomic_add_grads(float* tmp, uint32_t dim, uint32_t hash, uint32_t n, const uint32_t* gradIndex,
+                                     const uint32_t* hashIndex, const float* values) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t g = gradIndex[i], h = hashIndex[i];
+        if (g >= dim || h >= hash) continue;
+        const float v[1] = {values[i]};
+        atomic_add_row<1>(tmp + size_t(h) * dim + g, v);
+    }
+}
+
 int war_blocks(const void* k) {
     int perSM = 0, dev = 0, sms = 148;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k, kWarBlock, 0);
@@ -357,6 +369,21 @@ FPT_API fpt_status fpt_scene_gradients_aggregate(fpt_scene_gradients* g, uint32_
     fpt::war_aggregate<<<std::max(blocks, 1), 256, 0, static_cast<cudaStream_t>(stream)>>>(e.tmp, e.grads, e.dim, e.hash);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return set_error(FPT_ERR_CUDA, std::string("fpt_scene_gradients_aggregate: ") + cudaGetErrorString(err));
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_scene_gradients_atomic_add(fpt_scene_gradients* g, uint32_t type, uint32_t count,
+                                                  const uint32_t* grad_index, const uint32_t* hash_index, const float* values,
+                                                  void* stream) {
+    if (!g || type >= FPT_GRAD_TYPE_COUNT) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_gradients_atomic_add: invalid argument");
+    auto& e = g->e[type];
+    if (!e.active || count == 0) return FPT_OK;
+    if (!grad_index || !hash_index || !values) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_gradients_atomic_add: null array");
+    const int blocks = int(std::min<uint32_t>((count + 255) / 256, 148u * 8u));
+    fpt::war_atomic_add_grads<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(e.tmp, e.dim, e.hash, count, grad_index,
+                                                                                       hash_index, values);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return set_error(FPT_ERR_CUDA, std::string("fpt_scene_gradients_atomic_add: ") + cudaGetErrorString(err));
     return FPT_OK;
 }
 

@@ -78,6 +78,18 @@ class SceneGradients:
     def aggregate_grads(self, render_context=None, grad_type: GradientType = GradientType.Material) -> None:
         check(lib().fpt_scene_gradients_aggregate(self._h, int(grad_type), C.c_void_p(_stream())))
 
+    def atomic_add_grad(self, grad_type: GradientType, grad_index, hash_index, values) -> None:
+        """atomicAddGrad (SceneGradients.slang:50-57) for CUDA tensors of
+        element indices, hash rows (int32) and values (float32)."""
+        import torch
+        gi = grad_index.to(device="cuda", dtype=torch.int32).contiguous()
+        hi = hash_index.to(device="cuda", dtype=torch.int32).contiguous()
+        v = values.to(device="cuda", dtype=torch.float32).contiguous()
+        if not (gi.numel() == hi.numel() == v.numel()):
+            raise ValueError("atomic_add_grad: index and value arrays differ in length")
+        check(lib().fpt_scene_gradients_atomic_add(self._h, int(grad_type), v.numel(), gi.data_ptr(), hi.data_ptr(),
+                                                   v.data_ptr(), C.c_void_p(_stream())))
+
     def clear_all_grads(self, render_context=None) -> None:
         for t in self._types:
             self.clear_grads(render_context, t)

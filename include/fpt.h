@@ -470,6 +470,13 @@ FPT_API fpt_status fpt_scene_gradients_clear(fpt_scene_gradients* grads, uint32_
 /* aggregateGrads (SceneGradients.cpp:120-135, AggregateGradients.cs.slang:50-73):
  * result[i] += sum over hash rows of scratch[row][i]. */
 FPT_API fpt_status fpt_scene_gradients_aggregate(fpt_scene_gradients* grads, uint32_t grad_type, void* stream);
+/* SceneGradients::atomicAddGrad (DiffRendering/SceneGradients.slang:50-57)
+ * over device arrays: values[i] is added to scratch row hash_index[i],
+ * element grad_index[i] (contributions beyond the dimension or the hash size
+ * are ignored), with the warp-aggregated atomics the adjoint kernels use. */
+FPT_API fpt_status fpt_scene_gradients_atomic_add(fpt_scene_gradients* grads, uint32_t grad_type, uint32_t count,
+                                                  const uint32_t* grad_index, const uint32_t* hash_index, const float* values,
+                                                  void* stream);
 /* getGradsBuffer: device pointer of the result (valid until destroy). */
 FPT_API fpt_status fpt_scene_gradients_get(const fpt_scene_gradients* grads, uint32_t grad_type, float** out,
                                            uint32_t* dim, uint32_t* hash_size);
