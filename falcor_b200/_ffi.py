@@ -135,6 +135,7 @@ SIGNATURES = {
     "fpt_scene_set_camera": (C.c_int, [_P, C.POINTER(fpt_camera)]),
     "fpt_scene_get_material_params": (C.c_int, [_P, C.POINTER(u32), u32, C.POINTER(C.c_float)]),
     "fpt_scene_set_material_params": (C.c_int, [_P, C.POINTER(u32), u32, C.POINTER(C.c_float)]),
+    "fpt_scene_set_material_params_device": (C.c_int, [_P, C.POINTER(u32), u32, _P, _P]),
     "fpt_scene_get_bvh": (C.c_int, [_P, C.POINTER(fpt_bvh_view)]),
     "fpt_scene_get_alias_table": (C.c_int, [_P, C.POINTER(u32), u32, C.POINTER(f32)]),
     "fpt_pass_create": (C.c_int, [C.c_char_p, C.POINTER(_P)]),

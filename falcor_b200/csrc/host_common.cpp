@@ -7,6 +7,7 @@
 #include <cstring>
 
 #include "common.h"
+#include "f16.h"
 
 namespace fpt {
 
@@ -72,32 +73,7 @@ fpt_hitinfo_bits compute_hit_bits(const fpt_scene_desc& d) {
     return b;
 }
 
-uint16_t f32_to_f16_host(float value) {
-    // Round to nearest with ties away from zero on the magnitude bits, as the
-    // reference's host conversion does (Utils/Math/Float16.cpp:56-169).
-    uint32_t bits;
-    std::memcpy(&bits, &value, 4);
-    const int32_t sign = int32_t((bits >> 16) & 0x8000u);
-    int32_t exp = int32_t((bits >> 23) & 0xffu) - (127 - 15);
-    int32_t man = int32_t(bits & 0x007fffffu);
-    if (exp <= 0) {
-        if (exp < -10) return uint16_t(sign);
-        man = (man | 0x00800000) >> (1 - exp);
-        if (man & 0x00001000) man += 0x00002000;
-        return uint16_t(sign | (man >> 13));
-    }
-    if (exp == 0xff - (127 - 15)) {
-        if (man == 0) return uint16_t(sign | 0x7c00);
-        man >>= 13;
-        return uint16_t(sign | 0x7c00 | man | (man == 0));
-    }
-    if (man & 0x00001000) {
-        man += 0x00002000;
-        if (man & 0x00800000) { man = 0; exp += 1; }
-    }
-    if (exp > 30) return uint16_t(sign | 0x7c00);
-    return uint16_t(sign | (exp << 10) | (man >> 13));
-}
+uint16_t f32_to_f16_host(float value) { return f32_to_f16_bits(value); }
 
 float f16_to_f32_host(uint16_t h) {
     const uint32_t sign = (uint32_t(h) & 0x8000u) << 16;

@@ -14,6 +14,7 @@
 #include <random>
 #include <string>
 
+#include "f16.h"
 #include "scene_device.h"
 
 namespace fpt {
@@ -392,6 +393,49 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
     return FPT_OK;
 }
 
+// Refreshes the host copy of the materials from the device after device-side
+// updates (the device holds the fp16 values of the updated fields).
+fpt_status sync_materials_from_device(fpt_scene& scene) {
+    if (!scene.materialsOnDevice) return FPT_OK;
+    std::vector<DevMaterial> dm(scene.materials.size());
+    if (cudaMemcpy(dm.data(), scene.dev.materials, dm.size() * sizeof(DevMaterial), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return set_error(FPT_ERR_CUDA, "material parameters: download failed");
+    for (size_t i = 0; i < dm.size(); i++) {
+        fpt_material& m = scene.materials[i];
+        for (int k = 0; k < 3; k++) {
+            m.base_color[k] = f16_to_f32_host(dm[i].baseColor[k]);
+            m.transmission[k] = f16_to_f32_host(dm[i].transmission[k]);
+        }
+        m.specular[1] = f16_to_f32_host(dm[i].specular[1]);
+        m.specular[2] = f16_to_f32_host(dm[i].specular[2]);
+        m.ior = f16_to_f32_host(dm[i].ior);
+        m.specular_transmission = f16_to_f32_host(dm[i].specTrans);
+        m.diffuse_transmission = f16_to_f32_host(dm[i].diffTrans);
+    }
+    scene.materialsOnDevice = false;
+    return FPT_OK;
+}
+
+// setMaterialParams on the device: the differentiable fields of material
+// ids[i] (i when ids is null) from params[i * 20 ...], packed like the host
+// packer; emissive entries are ignored (the light collection is fixed).
+__global__ void set_material_params_kernel(DevMaterial* mats, const uint32_t* ids, uint32_t count, const float* params) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t id = ids ? ids[i] : i;
+        const float* v = params + size_t(i) * 20;
+        DevMaterial& m = mats[id];
+        for (int k = 0; k < 3; k++) {
+            m.baseColor[k] = f32_to_f16_bits(v[k]);
+            m.transmission[k] = f32_to_f16_bits(v[6 + k]);
+        }
+        m.specular[2] = f32_to_f16_bits(v[3]);
+        m.specular[1] = f32_to_f16_bits(v[4]);
+        m.ior = f32_to_f16_bits(v[5]);
+        m.diffTrans = f32_to_f16_bits(v[9]);
+        m.specTrans = f32_to_f16_bits(v[10]);
+    }
+}
+
 }  // namespace fpt
 
 using namespace fpt;
@@ -445,8 +489,50 @@ FPT_API fpt_status fpt_scene_set_camera(fpt_scene* scene, const fpt_camera* came
 // Material::serializeParams / deserializeParams): baseColor 0-2, metallic 3,
 // roughness 4, ior 5, transmissionColor 6-8, diffuseTransmission 9,
 // specularTransmission 10, emissiveColor 11-13, emissiveFactor 14, 15-19 unused.
-FPT_API fpt_status fpt_scene_get_material_params(const fpt_scene* scene, const uint32_t* ids, uint32_t count, float* params) {
+FPT_API fpt_status fpt_scene_set_material_params_device(fpt_scene* scene, const uint32_t* ids, uint32_t count, const float* params,
+                                                        void* stream) {
+    if (!scene || (count && !params)) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_material_params_device: null argument");
+    if (count == 0) return FPT_OK;
+    const uint32_t nm = uint32_t(scene->materials.size());
+    if (!ids && count > nm)
+        return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_material_params_device: more parameter rows than materials");
+    for (uint32_t i = 0; ids && i < count; i++)
+        if (ids[i] >= nm) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_material_params_device: material ID out of range");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const uint32_t* dIds = nullptr;
+    if (ids) {
+        if (scene->materialIdCapacity < count) {
+            void* p = nullptr;
+            if (cudaMalloc(&p, size_t(count) * 4) != cudaSuccess)
+                return set_error(FPT_ERR_OOM, "fpt_scene_set_material_params_device: allocation failed");
+            scene->buffers.ptrs.push_back(p);
+            scene->materialIds = static_cast<uint32_t*>(p);
+            scene->materialIdCapacity = count;
+        }
+        if (cudaMemcpyAsync(scene->materialIds, ids, size_t(count) * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            return set_error(FPT_ERR_CUDA, "fpt_scene_set_material_params_device: ID upload failed");
+        dIds = scene->materialIds;
+    }
+    const uint32_t grid = std::min<uint32_t>((count + 127) / 128, 1024);
+    set_material_params_kernel<<<grid, 128, 0, st>>>(const_cast<DevMaterial*>(scene->dev.materials), dIds, count, params);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, std::string("fpt_scene_set_material_params_device: ") + cudaGetErrorString(e));
+    // Transmission values are not read back: the transmission-capable kernels
+    // (which render materials without transmission identically) are used from now on.
+    scene->dev.hasTransmission = 1u;
+    scene->materialsOnDevice = true;
+    scene->version++;
+    scene->resetVersion++;
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_scene_get_material_params(const fpt_scene* cscene, const uint32_t* ids, uint32_t count, float* params) {
+    const fpt_scene* scene = cscene;
     if (!scene || (count && (!ids || !params))) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_get_material_params: null argument");
+    if (scene->materialsOnDevice) {
+        const fpt_status s = sync_materials_from_device(*const_cast<fpt_scene*>(scene));
+        if (s != FPT_OK) return s;
+    }
     for (uint32_t i = 0; i < count; i++) {
         if (ids[i] >= scene->materials.size()) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_get_material_params: material ID out of range");
         const fpt_material& m = scene->materials[ids[i]];
@@ -465,6 +551,10 @@ FPT_API fpt_status fpt_scene_get_material_params(const fpt_scene* scene, const u
 
 FPT_API fpt_status fpt_scene_set_material_params(fpt_scene* scene, const uint32_t* ids, uint32_t count, const float* params) {
     if (!scene || (count && (!ids || !params))) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_material_params: null argument");
+    if (scene->materialsOnDevice) {
+        const fpt_status st = sync_materials_from_device(*scene);
+        if (st != FPT_OK) return st;
+    }
     for (uint32_t i = 0; i < count; i++)
         if (ids[i] >= scene->materials.size()) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_material_params: material ID out of range");
     std::vector<fpt_material> next = scene->materials;

@@ -43,4 +43,9 @@ struct fpt_scene {
     std::vector<uint32_t> levelStart;
     float* nodeBoxes = nullptr;
     uint32_t* refitStatus = nullptr;
+    // Material parameters last written on the device (fpt_scene_set_material_params_device):
+    // the host copy is refreshed from the device before it is read.
+    bool materialsOnDevice = false;
+    uint32_t* materialIds = nullptr;     // device copy of the IDs of a device-side update
+    uint32_t materialIdCapacity = 0;
 };

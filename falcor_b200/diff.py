@@ -15,6 +15,8 @@ import ctypes as C
 import enum
 from dataclasses import dataclass
 
+import numpy as np
+
 from . import _ffi
 from ._ffi import check, lib
 
@@ -140,6 +142,42 @@ def _autograd():
     return WARDiffRender
 
 
+def _mesh_autograd():
+    import torch
+
+    class MeshDiffRender(torch.autograd.Function):
+        """image = render(mesh positions, normals, tangents) of the renderer's
+        mesh (the reference's shape-optimisation DiffRenderFunction,
+        scripts/inv-rendering/shape_optimization/diff_render_module.py:11-63):
+        forward writes the vertex data to the scene (setMeshVertices) and
+        renders the primal; backward runs the adjoint of the same frame and
+        returns the MeshPosition, MeshNormal and MeshTangent gradients."""
+
+        @staticmethod
+        def forward(ctx, positions, normals, tangents, renderer, frame_seed):
+            renderer.set_mesh(positions, normals, tangents)
+            img = renderer.render(frame_seed)
+            ctx.renderer = renderer
+            ctx.frame_seed = frame_seed
+            ctx.shape = positions.shape
+            return img
+
+        @staticmethod
+        def backward(ctx, grad_img):
+            n = int(np.prod(ctx.shape))
+            _, gp = ctx.renderer.gradients(grad_img, ctx.frame_seed, position_dim=n, normal_dim=n, tangent_dim=n)
+            return (gp.view(ctx.shape), ctx.renderer.normal_grad.view(ctx.shape), ctx.renderer.tangent_grad.view(ctx.shape),
+                    None, None)
+
+    return MeshDiffRender
+
+
+def mesh_diff_render(positions, normals, tangents, renderer, frame_seed: int):
+    """Differentiable render with the optimised mesh's vertex data as inputs
+    (see ``MeshDiffRender``)."""
+    return _mesh_autograd().apply(positions, normals, tangents, renderer, frame_seed)
+
+
 def war_diff_render(material_params, renderer, frame_seed: int):
     """Differentiable WARDiffPathTracer render (see ``WARDiffRender``)."""
     return _autograd().apply(material_params, renderer, frame_seed)
@@ -164,27 +202,50 @@ class DiffRenderer:
         self.mesh_id = mesh_id
         self.material_count = scene.info.material_count
         self.position_grad = None
+        self._texcrds = None
         self.color = torch.zeros((height, width, 4), dtype=torch.float32, device="cuda")
 
     def set_material_params(self, params) -> None:
-        self.scene.set_material_params(list(range(params.shape[0])), params.detach().reshape(-1, 20).cpu().numpy())
+        """Material parameters [M, 20] on the device (no host round trip)."""
+        self.scene.set_material_params_device(params.detach().reshape(-1, 20))
+
+    def set_mesh(self, positions, normals, tangents) -> None:
+        """The optimised mesh's vertex data [V, 3] (CUDA tensors), texture
+        coordinates kept; the BVH is refitted (Scene::setMeshVertices)."""
+        import torch
+        if self.mesh_id is None:
+            raise ValueError("DiffRenderer: no mesh to optimise (mesh_id)")
+        if self._texcrds is None:
+            info = self.scene.get_mesh(self.mesh_id)
+            nv, nt = info["vertex_count"], info["triangle_count"]
+            pos = torch.zeros((nv, 3), dtype=torch.float32, device="cuda")
+            self._texcrds = torch.zeros((nv, 3), dtype=torch.float32, device="cuda")
+            idx = torch.zeros((nt, 3), dtype=torch.int32, device="cuda")
+            self.scene.get_mesh_vertices_and_indices(self.mesh_id, {"positions": pos, "texcrds": self._texcrds,
+                                                                    "triangleIndices": idx})
+        f = lambda t: t.detach().to(device="cuda", dtype=torch.float32).reshape(-1, 3).contiguous()  # noqa: E731
+        self.scene.set_mesh_vertices(self.mesh_id, {"positions": f(positions), "normals": f(normals),
+                                                    "tangents": f(tangents), "texcrds": self._texcrds})
 
     def render(self, frame_seed: int):
         self.pt.set_properties({"fixedSeed": int(frame_seed), "runBackward": 0})
         self.pt.execute({"color": self.color})
         return self.color[..., :3].clone()
 
-    def gradients(self, grad_img, frame_seed: int, position_dim: int = 0, normal_dim: int = 0):
-        """Material gradients and, with position_dim / normal_dim > 0, the
-        gradients of the optimised mesh's vertex positions / normals (3 floats
-        per vertex; the normal gradients are kept in ``normal_grad``)."""
+    def gradients(self, grad_img, frame_seed: int, position_dim: int = 0, normal_dim: int = 0, tangent_dim: int = 0):
+        """Material gradients and, with position_dim / normal_dim / tangent_dim
+        > 0, the gradients of the optimised mesh's vertex positions / normals /
+        tangents (3 floats per vertex; normals and tangents are kept in
+        ``normal_grad`` / ``tangent_grad``)."""
         import torch
         self.pt.set_properties({"fixedSeed": int(frame_seed)})
         gm = torch.zeros(self.material_count * 20, dtype=torch.float32, device="cuda")
         gp = torch.zeros(max(position_dim, 1), dtype=torch.float32, device="cuda") if position_dim else None
         gn = torch.zeros(normal_dim, dtype=torch.float32, device="cuda") if normal_dim else None
+        gt = torch.zeros(tangent_dim, dtype=torch.float32, device="cuda") if tangent_dim else None
         dLdI = grad_img[..., :3].contiguous().float()
-        self.pt.backward({"color": self.color}, dLdI, material_grad=gm, position_grad=gp, normal_grad=gn)
+        self.pt.backward({"color": self.color}, dLdI, material_grad=gm, position_grad=gp, normal_grad=gn, tangent_grad=gt)
         self.position_grad = gp
         self.normal_grad = gn
+        self.tangent_grad = gt
         return gm, gp

@@ -188,6 +188,25 @@ class Scene:
         check(lib().fpt_scene_set_material_params(self._h, ids.ctypes.data_as(C.POINTER(C.c_uint32)), len(ids),
                                                   params.ctypes.data_as(C.POINTER(C.c_float))))
 
+    def set_material_params_device(self, params, ids=None) -> None:
+        """setMaterialParams from a CUDA float32 tensor [count, 20] without a
+        host round trip (ids: host list, or None for materials 0..count-1);
+        emissive entries are ignored (fpt_scene_set_material_params_device)."""
+        import torch
+        p = params.detach()
+        if not (p.is_cuda and p.dtype == torch.float32):
+            raise ValueError("params must be a CUDA float32 tensor of [count, 20]")
+        p = p.reshape(-1, 20).contiguous()
+        n = p.shape[0]
+        idp = None
+        if ids is not None:
+            ida = np.ascontiguousarray(ids, dtype=np.uint32)
+            if len(ida) != n:
+                raise ValueError("one material ID per parameter row")
+            idp = ida.ctypes.data_as(C.POINTER(C.c_uint32))
+        check(lib().fpt_scene_set_material_params_device(self._h, idp, n, p.data_ptr(),
+                                                         torch.cuda.current_stream().cuda_stream))
+
     def get_mesh(self, mesh_id: int) -> dict:
         """Scene::getMesh: vertex and triangle counts of a mesh (geometry instance)."""
         nv, nt = C.c_uint32(), C.c_uint32()

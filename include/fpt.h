@@ -243,6 +243,17 @@ FPT_API fpt_status fpt_scene_set_camera(fpt_scene* scene, const fpt_camera* came
  * (FPT_ERR_UNSUPPORTED): the light collection is built once per scene. */
 FPT_API fpt_status fpt_scene_get_material_params(const fpt_scene* scene, const uint32_t* ids, uint32_t count, float* params);
 FPT_API fpt_status fpt_scene_set_material_params(fpt_scene* scene, const uint32_t* ids, uint32_t count, const float* params);
+/* setMaterialParams with the parameters in device memory (params: count * 20
+ * floats on the device, read on `stream`; ids: host array, or NULL for
+ * materials 0..count-1), so that an optimisation loop updates materials
+ * without a host round trip.  The differentiable fields are packed on the
+ * device exactly as the host packer does; the emissive entries are ignored.
+ * Afterwards the scene renders with the transmission-capable kernels (which
+ * give the same images for materials without transmission) and the host
+ * copy read by fpt_scene_get_material_params is refreshed from the device.
+ * Extension of the reference's Scene::setMaterialParams. */
+FPT_API fpt_status fpt_scene_set_material_params_device(fpt_scene* scene, const uint32_t* ids, uint32_t count, const float* params,
+                                                        void* stream);
 /* Host view of the scene's BVH (valid until the scene is destroyed). */
 FPT_API fpt_status fpt_scene_get_bvh(const fpt_scene* scene, fpt_bvh_view* out);
 /* Host view of the light BVH built for the LightBVH emissive sampler

@@ -698,3 +698,79 @@ def test_c3_displaced_sphere_adjoint_matches_oracle(fpt, oracle, war):
     ep = check_projections("position", P, gp.cpu().numpy().astype(np.float64), gp_ref, rtol)
     print(f"C3 sphere adjoint (useWAR={war}): primal exact {np.mean(np.all(got[..., :3] == ref_color[..., :3], axis=-1)):.4f}, "
           f"max relative error material {em:.2e}, position {ep:.2e}")
+
+
+@pytest.mark.gpu
+def test_device_material_update_matches_host_update(fpt):
+    """fpt_scene_set_material_params_device packs the parameters on the device
+    exactly as the host path does: the same images, and the parameters read
+    back are the fp16 values the host path stores."""
+    import torch
+    from falcor_b200.passes import WARDiffPathTracer
+    host = H.small_heightfield(materials=16, emitters=16)
+    nm = host.desc.material_count
+    rng = np.random.default_rng(2)
+    imgs, reads = [], []
+    for device_path in (False, True):
+        s = gpu_scene(host)
+        p = s.get_material_params(list(range(nm)))
+        p[:, :3] = rng.uniform(0.1, 0.9, (nm, 3)) if not imgs else p_set[:, :3]
+        p[:, 4] = rng.uniform(0.2, 0.9, nm) if not imgs else p_set[:, 4]
+        p_set = p.copy()
+        if device_path:
+            s.set_material_params_device(torch.from_numpy(p_set).cuda())
+        else:
+            s.set_material_params(list(range(nm)), p_set)
+        pt = WARDiffPathTracer(war_props(mode="Primal", max_bounces=3, seed=4))
+        pt.set_scene(s)
+        c = torch.zeros((48, 64, 4), dtype=torch.float32, device="cuda")
+        pt.execute({"color": c})
+        torch.cuda.synchronize()
+        imgs.append(c.cpu().numpy())
+        reads.append(s.get_material_params(list(range(nm))))
+    np.testing.assert_array_equal(imgs[0], imgs[1])
+    q = lambda a: a.astype(np.float16).astype(np.float32)  # noqa: E731
+    np.testing.assert_array_equal(q(reads[0][:, :6]), reads[1][:, :6])
+
+
+@pytest.mark.gpu
+def test_autograd_mesh_vertices(fpt):
+    """mesh_diff_render takes the optimised mesh's positions, normals and
+    tangents as autograd inputs (the reference's shape-optimisation
+    DiffRenderFunction); its gradients equal the adjoint's direct output for
+    the same frame, and moving the vertices changes the image."""
+    import torch
+    from falcor_b200.diff import DiffRenderer, mesh_diff_render
+    from falcor_b200.passes import WARDiffPathTracer
+    host = _with_tangents(H.box_icosphere(3))
+    mesh = 13
+    s = gpu_scene(host)
+    r = DiffRenderer(s, 64, 48, props={"maxBounces": 2, "useWAR": True}, mesh_id=mesh)
+    info = s.get_mesh(mesh)
+    nv, nt = info["vertex_count"], info["triangle_count"]
+    pos = torch.zeros((nv, 3), dtype=torch.float32, device="cuda")
+    tex = torch.zeros((nv, 3), dtype=torch.float32, device="cuda")
+    idx = torch.zeros((nt, 3), dtype=torch.int32, device="cuda")
+    s.get_mesh_vertices_and_indices(mesh, {"positions": pos, "texcrds": tex, "triangleIndices": idx})
+    v = torch.from_numpy(host.vertices[int(host.instances[mesh, 0]):int(host.instances[mesh, 0]) + nv].copy()).cuda()
+    nrm0, tan0 = v[:, 3:6].contiguous(), v[:, 6:9].contiguous()
+    p = pos.clone().requires_grad_(True)
+    n = nrm0.clone().requires_grad_(True)
+    t = tan0.clone().requires_grad_(True)
+    img = mesh_diff_render(p, n, t, r, 7)
+    target = torch.zeros_like(img)
+    loss = ((img - target) ** 2).sum()
+    loss.backward()
+    # The direct adjoint of the same frame with dL/dI = 2 img.
+    pt = WARDiffPathTracer(war_props(max_bounces=2, seed=7, mesh=mesh, war=True))
+    pt.set_scene(s)
+    color = torch.zeros((48, 64, 4), dtype=torch.float32, device="cuda")
+    gp, gn, gt = (torch.zeros(nv * 3, dtype=torch.float32, device="cuda") for _ in range(3))
+    pt.backward({"color": color}, (2 * img.detach()).contiguous(), position_grad=gp, normal_grad=gn, tangent_grad=gt)
+    torch.cuda.synchronize()
+    for a, b in ((p.grad, gp), (n.grad, gn)):
+        a, b = a.reshape(-1).cpu().numpy(), b.cpu().numpy()
+        assert np.abs(b).max() > 0
+        assert np.allclose(a, b, rtol=1e-4, atol=1e-4 * np.abs(b).max())
+    moved = mesh_diff_render(p.detach() + 0.05, n.detach(), t.detach(), r, 7)
+    assert float((moved - img.detach()).abs().sum()) > 0
