@@ -143,6 +143,7 @@ SIGNATURES = {
     "fpt_pass_set_property_int": (C.c_int, [_P, C.c_char_p, C.c_int64]),
     "fpt_pass_set_property_float": (C.c_int, [_P, C.c_char_p, C.c_double]),
     "fpt_pass_set_property_string": (C.c_int, [_P, C.c_char_p, C.c_char_p]),
+    "fpt_pass_set_properties_json": (C.c_int, [_P, C.c_char_p]),
     "fpt_pass_get_properties_json": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
     "fpt_pass_reflect_json": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
     "fpt_pass_set_scene": (C.c_int, [_P, _P]),

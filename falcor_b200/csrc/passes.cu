@@ -9,6 +9,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cctype>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <sstream>
@@ -504,6 +506,119 @@ FPT_API fpt_status fpt_pass_set_property_string(fpt_pass* pass, const char* key,
     if (k == "adjointMode" && v != "Replay" && v != "Checkpoint")
         return set_error(FPT_ERR_INVALID_ARG, "adjointMode must be 'Replay' or 'Checkpoint'");
     it->second.s = v;
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_pass_set_properties_json(fpt_pass* pass, const char* json) {
+    if (!pass || !json) return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_properties_json: null argument");
+    // A flat JSON object (Properties::dump): strings, numbers and booleans are
+    // applied like the typed setters; nested objects, arrays and null are
+    // skipped with a warning (sub-option blocks such as lightBVHOptions).
+    const char* c = json;
+    auto ws = [&] { while (*c == ' ' || *c == '\t' || *c == '\n' || *c == '\r') c++; };
+    auto fail = [&](const std::string& what) {
+        return set_error(FPT_ERR_INVALID_ARG, "fpt_pass_set_properties_json: " + what + " at offset " + std::to_string(c - json));
+    };
+    auto parse_string = [&](std::string& out) -> bool {
+        if (*c != '"') return false;
+        c++;
+        out.clear();
+        while (*c && *c != '"') {
+            if (*c == '\\') {
+                c++;
+                switch (*c) {
+                    case '"': out += '"'; break;
+                    case '\\': out += '\\'; break;
+                    case '/': out += '/'; break;
+                    case 'b': out += '\b'; break;
+                    case 'f': out += '\f'; break;
+                    case 'n': out += '\n'; break;
+                    case 'r': out += '\r'; break;
+                    case 't': out += '\t'; break;
+                    case 'u': {
+                        unsigned v = 0;
+                        for (int k = 1; k <= 4; k++) {
+                            const char h = c[k];
+                            if (!std::isxdigit(static_cast<unsigned char>(h))) return false;
+                            v = v * 16 + unsigned(std::isdigit(static_cast<unsigned char>(h)) ? h - '0' : (std::tolower(h) - 'a' + 10));
+                        }
+                        c += 4;
+                        if (v < 0x80) out += char(v);
+                        else if (v < 0x800) { out += char(0xc0 | (v >> 6)); out += char(0x80 | (v & 0x3f)); }
+                        else { out += char(0xe0 | (v >> 12)); out += char(0x80 | ((v >> 6) & 0x3f)); out += char(0x80 | (v & 0x3f)); }
+                        break;
+                    }
+                    default: return false;
+                }
+                c++;
+            } else {
+                out += *c++;
+            }
+        }
+        if (*c != '"') return false;
+        c++;
+        return true;
+    };
+    // Skips a nested value (object or array), honouring strings.
+    auto skip_nested = [&]() -> bool {
+        int depth = 0;
+        std::string tmp;
+        do {
+            if (*c == '"') {
+                if (!parse_string(tmp)) return false;
+                continue;
+            }
+            if (*c == '{' || *c == '[') depth++;
+            else if (*c == '}' || *c == ']') depth--;
+            else if (!*c) return false;
+            c++;
+        } while (depth > 0);
+        return true;
+    };
+    ws();
+    if (*c != '{') return fail("expected '{'");
+    c++;
+    ws();
+    if (*c == '}') return FPT_OK;
+    for (;;) {
+        ws();
+        std::string key;
+        if (!parse_string(key)) return fail("expected a key");
+        ws();
+        if (*c != ':') return fail("expected ':'");
+        c++;
+        ws();
+        fpt_status st = FPT_OK;
+        if (*c == '"') {
+            std::string v;
+            if (!parse_string(v)) return fail("bad string");
+            st = fpt_pass_set_property_string(pass, key.c_str(), v.c_str());
+        } else if (!std::strncmp(c, "true", 4) || !std::strncmp(c, "false", 5)) {
+            const bool b = *c == 't';
+            c += b ? 4 : 5;
+            st = fpt_pass_set_property_int(pass, key.c_str(), b ? 1 : 0);
+        } else if (!std::strncmp(c, "null", 4)) {
+            c += 4;
+            log_warning("Property '" + key + "' is null; ignored.");
+        } else if (*c == '{' || *c == '[') {
+            if (!skip_nested()) return fail("bad nested value");
+            log_warning("Property '" + key + "' (a nested object or array) is not supported by " + pass->type + "; ignored.");
+        } else {
+            char* end = nullptr;
+            const double v = std::strtod(c, &end);
+            if (end == c) return fail("bad value");
+            c = end;
+            st = fpt_pass_set_property_float(pass, key.c_str(), v);
+        }
+        if (st != FPT_OK) return st;
+        ws();
+        if (*c == ',') {
+            c++;
+            continue;
+        }
+        if (*c == '}') break;
+        return fail("expected ',' or '}'");
+    }
     return FPT_OK;
 }
 

@@ -315,6 +315,11 @@ FPT_API void fpt_pass_destroy(fpt_pass* pass);
 FPT_API fpt_status fpt_pass_set_property_int(fpt_pass* pass, const char* key, int64_t value);
 FPT_API fpt_status fpt_pass_set_property_float(fpt_pass* pass, const char* key, double value);
 FPT_API fpt_status fpt_pass_set_property_string(fpt_pass* pass, const char* key, const char* value);
+/* RenderPass::setProperties from a Properties object's JSON dump
+ * (Properties::dump, Utils/Properties.h): a flat JSON object whose strings,
+ * numbers and booleans go through the typed setters above; nested objects
+ * and arrays are logged and ignored like unknown keys. */
+FPT_API fpt_status fpt_pass_set_properties_json(fpt_pass* pass, const char* json);
 /* Serialises the current properties as a JSON object into buf (NUL-terminated).
  * Returns FPT_ERR_INVALID_ARG if capacity is too small. */
 FPT_API fpt_status fpt_pass_get_properties_json(const fpt_pass* pass, char* buf, size_t capacity);

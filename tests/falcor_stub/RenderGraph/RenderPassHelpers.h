@@ -1,0 +1,3 @@
+// Stand-in (see tests/falcor_stub/Falcor.h).
+#pragma once
+#include "../Falcor.h"

@@ -163,3 +163,25 @@ def test_oracle_builds_the_same_workload_scenes(fpt, oracle, kind, params):
         n = he.width * he.height * 3
         assert (he.width, he.height) == (oe.width, oe.height)
         assert C.string_at(C.cast(he.rgb, C.c_void_p).value, 4 * n) == C.string_at(C.cast(oe.rgb, C.c_void_p).value, 4 * n)
+
+
+def test_set_properties_from_json_dump(fpt):
+    """fpt_pass_set_properties_json takes a Properties object's JSON dump (how a
+    Falcor RenderPass plugin forwards setProperties): strings, numbers and
+    booleans as the typed setters, nested objects skipped, errors reported."""
+    import json
+    from falcor_b200 import _ffi
+    from falcor_b200.passes import PathTracer
+    pt = PathTracer()
+    props = {"samplesPerPixel": 4, "maxSurfaceBounces": 5, "useNEE": False, "misPowerExponent": 3.5,
+             "emissiveSampler": "Power", "colorFormat": "RGBA32F", "lightBVHOptions": {"maxTriangleCountPerLeaf": 10},
+             "unknownKey": "ignored", "diffuseBrdf": "Lam\\u0062ert"}
+    text = json.dumps(props).replace("Lam\\\\u0062ert", "Lam\\u0062ert")
+    _ffi.check(fpt.fpt_pass_set_properties_json(pt.handle, text.encode()))
+    p = pt.properties
+    assert p["samplesPerPixel"] == 4 and p["maxSurfaceBounces"] == 5 and p["useNEE"] == 0
+    assert p["misPowerExponent"] == 3.5 and p["emissiveSampler"] == "Power" and p["colorFormat"] == "RGBA32F"
+    assert p["diffuseBrdf"] == "Lambert"
+    assert fpt.fpt_pass_set_properties_json(pt.handle, b'{"samplesPerPixel": }') == 1
+    assert fpt.fpt_pass_set_properties_json(pt.handle, b'{"emissiveSampler": "Nope"}') == 1
+    assert fpt.fpt_pass_set_properties_json(pt.handle, b"{}") == 0

@@ -1,0 +1,88 @@
+"""The Falcor render-pass plugin (falcor_b200/plugin/FalcorB200Passes.cpp):
+the drop-in boundary of the C-ABI as Falcor sees it.
+
+The plugin is compiled against a stand-in of the slice of Falcor's C++ API it
+uses (tests/falcor_stub/, names and signatures of the reference headers) and
+driven by tests/falcor_stub/plugin_host.cpp the way a render graph drives a
+pass: registerPlugin, RenderPass::create by type name with Properties,
+reflect, setScene with a Falcor Scene (meshes read back through
+getMeshVerticesAndIndices), execute with the channels in textures.  The CPU
+test compiles it; the GPU test runs VBufferRT -> PathTracer and
+MinimalPathTracer through it and requires the same pixels as the library's
+Python passes on the same scene and properties.
+"""
+import os
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from tests import helpers as H
+
+ROOT = Path(__file__).resolve().parent.parent
+STUB = ROOT / "tests" / "falcor_stub"
+
+
+def _cuda_home() -> Path:
+    nvcc = shutil.which("nvcc")
+    return Path(nvcc).resolve().parent.parent if nvcc else Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+
+
+def _build(out_dir: Path) -> Path:
+    from falcor_b200 import build
+    lib = build.build()
+    cuda = _cuda_home()
+    exe = out_dir / "plugin_host"
+    cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O1", "-Wall", "-Werror", "-I", str(STUB), "-I", str(ROOT / "include"),
+           "-I", str(cuda / "include"), str(STUB / "plugin_host.cpp"), str(ROOT / "falcor_b200/plugin/FalcorB200Passes.cpp"),
+           "-L", str(lib.parent), "-lfpt", "-L", str(cuda / "lib64"), "-lcudart", f"-Wl,-rpath,{lib.parent}", "-o", str(exe)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    assert res.returncode == 0, res.stdout + res.stderr
+    return exe
+
+
+def test_plugin_compiles_against_falcor_api(fpt, tmp_path):
+    exe = _build(tmp_path)
+    assert exe.exists()
+
+
+@pytest.mark.gpu
+def test_plugin_passes_render_like_the_library(fpt, tmp_path):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from falcor_b200.passes import MinimalPathTracer, PathTracer
+    from falcor_b200.scene import Scene
+    W, Hh = 64, 48
+    exe = _build(tmp_path)
+    out = tmp_path / "out.bin"
+    res = subprocess.run([str(exe), str(out), str(W), str(Hh)], capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
+    log = res.stdout
+    assert "reflect PathTracer: in:vbuffer in:viewW? out:color out:rayCount? out:pathLength?" in log, log
+    assert "reflect VBufferRT: out:vbuffer out:depth? out:mvec? out:viewW? out:mask?" in log, log
+    assert '"samplesPerPixel": 4' in log and '"emissiveSampler": "Power"' in log, log
+    data = np.fromfile(out, dtype=np.uint32)
+    n = W * Hh * 4
+    vb_plugin = data[:n].reshape(Hh, W, 4)
+    pt_plugin = data[n:2 * n].view(np.float32).reshape(Hh, W, 4)
+    mpt_plugin = data[2 * n:3 * n].view(np.float32).reshape(Hh, W, 4)
+
+    host = H.small_heightfield()  # the scene plugin_host builds (heightfield + soup, env map, 4:3)
+    scene = Scene(host)
+    vb = H.gpu_vbuffer(scene, W, Hh)
+    np.testing.assert_array_equal(vb.cpu().numpy().view(np.uint32), vb_plugin)
+    pt = PathTracer(H.pt_props(4, max_bounces=4, seed=3))
+    pt.set_scene(scene)
+    c = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
+    pt.execute({"vbuffer": vb, "color": c})
+    mpt = MinimalPathTracer({"maxBounces": 3})
+    mpt.set_scene(scene)
+    c2 = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
+    mpt.execute({"vbuffer": vb, "color": c2})
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(c.cpu().numpy(), pt_plugin)
+    np.testing.assert_array_equal(c2.cpu().numpy(), mpt_plugin)
+    assert pt_plugin[..., :3].mean() > 0
