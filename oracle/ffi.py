@@ -46,7 +46,9 @@ class SceneInfo(C.Structure):
 
 class Counters(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("rays", C.c_uint64), ("closest", C.c_uint64), ("shadow", C.c_uint64),
-                ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64)]
+                ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64),
+                ("b8_nodes_closest", C.c_uint64), ("b8_tris_closest", C.c_uint64), ("b8_nodes_shadow", C.c_uint64),
+                ("b8_tris_shadow", C.c_uint64), ("b8_mismatch", C.c_uint64)]
 
 
 class ProceduralParams(C.Structure):
@@ -118,6 +120,9 @@ def lib(variant: str = "parity") -> C.CDLL:
         l.orc_trace_visibility.argtypes = [_P, u32, _P, _P, _P, _P]
         l.orc_minimal_pt.restype = C.c_double
         l.orc_minimal_pt.argtypes = [_P, C.POINTER(MinimalPTParams), _P, _P, _P, C.c_int, u32, u32, u32, u32, u32, _P]
+        l.orc_scene_attach_bvh8.argtypes = [_P, _P, u32, _P, u32]
+        l.orc_path_tracer_counts.restype = C.c_double
+        l.orc_path_tracer_counts.argtypes = [_P, C.POINTER(PathTracerParams), _P, u32, u32, C.POINTER(Counters)]
         l.orc_path_tracer.restype = C.c_double
         l.orc_path_tracer.argtypes = [_P, C.POINTER(PathTracerParams), _P, _P, _P, C.c_int, u32, u32, u32, u32, u32,
                                       C.POINTER(Counters), _P]
@@ -251,6 +256,22 @@ class OracleScene:
                                    ptr(smp) if smp is not None else None, int(fp64), threads, x0, y0, x1, y1, C.byref(cnt),
                                    ptr(tr) if tr is not None else None)
         return (out, smp, cnt, dt, tr) if trace else (out, smp, cnt, dt)
+
+    def attach_bvh8(self, nodes: np.ndarray, tris: np.ndarray) -> None:
+        """A copy of the library's 8-wide BVH (80-byte nodes, 48-byte triangle
+        records, as raw bytes) for the algorithmic traversal counts."""
+        nodes = np.ascontiguousarray(nodes)
+        tris = np.ascontiguousarray(tris)
+        self._l.orc_scene_attach_bvh8(self._h, ptr(nodes), nodes.nbytes // 80, ptr(tris), tris.nbytes // 48)
+
+    def path_tracer_counts(self, vbuffer: np.ndarray, params: PathTracerParams, stride: int = 4, threads: int = 0):
+        """(Counters, seconds) of the FP32 PathTracer over every stride-th pixel
+        in x and y (no image): events, and with attach_bvh8 the exact traversal
+        counts on the library's tree."""
+        cnt = Counters()
+        dt = self._l.orc_path_tracer_counts(self._h, C.byref(params), ptr(np.ascontiguousarray(vbuffer)), stride, threads,
+                                            C.byref(cnt))
+        return cnt, dt
 
     def wardiff(self, params: WarDiffParams, mode: int = 0, dLdI=None, mat_tangents=None, pos_tangents=None, eps: float = 0.0,
                 threads: int = 0, rect=None, nrm_tangents=None, tan_tangents=None):

@@ -176,7 +176,26 @@ double orc_minimal_pt(const void* sp, const MinimalPTParams* p, const uint32_t* 
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
-struct orc_counters { uint64_t paths, rays, closest, shadow, node_visits, tri_tests; };
+struct orc_counters {
+    uint64_t paths, rays, closest, shadow, node_visits, tri_tests;
+    uint64_t b8_nodes_closest, b8_tris_closest, b8_nodes_shadow, b8_tris_shadow, b8_mismatch;
+};
+
+static void sum_counters(const std::vector<PathCounters>& pcs, orc_counters* cnt) {
+    *cnt = orc_counters{};
+    for (auto& c : pcs) {
+        cnt->paths += c.paths; cnt->rays += c.rays; cnt->closest += c.tc.closest; cnt->shadow += c.tc.shadow;
+        cnt->node_visits += c.tc.nodeVisits; cnt->tri_tests += c.tc.triTests;
+        cnt->b8_nodes_closest += c.tc.b8NodesClosest; cnt->b8_tris_closest += c.tc.b8TrisClosest;
+        cnt->b8_nodes_shadow += c.tc.b8NodesShadow; cnt->b8_tris_shadow += c.tc.b8TrisShadow;
+        cnt->b8_mismatch += c.tc.b8Mismatch;
+    }
+}
+
+// A copy of the library's 8-wide BVH for the algorithmic traversal counts.
+void orc_scene_attach_bvh8(void* sp, const void* nodes, uint32_t nodeCount, const void* tris, uint32_t triCount) {
+    static_cast<Scene*>(sp)->attachBvh8(nodes, nodeCount, tris, triCount);
+}
 
 // PathTracer over a rectangle.  color: RGBA32F full frame; samples (optional):
 // per pixel spp*3 floats, pixel-major over the full frame.
@@ -196,13 +215,27 @@ double orc_path_tracer(const void* sp, const PathTracerParams* p, const uint32_t
                                       trace ? trace + i * size_t(p->samplesPerPixel) * (p->maxSurfaceBounces + 2) * 4 : nullptr);
     });
     double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    if (cnt) {
-        *cnt = orc_counters{0, 0, 0, 0, 0, 0};
-        for (auto& c : pcs) {
-            cnt->paths += c.paths; cnt->rays += c.rays; cnt->closest += c.tc.closest; cnt->shadow += c.tc.shadow;
-            cnt->node_visits += c.tc.nodeVisits; cnt->tri_tests += c.tc.triTests;
-        }
-    }
+    if (cnt) sum_counters(pcs, cnt);
+    return dt;
+}
+
+// PathTracer (FP32) over the pixels with x % stride == 0 and y % stride == 0
+// of the frame, images discarded: event and traversal counts only.
+double orc_path_tracer_counts(const void* sp, const PathTracerParams* p, const uint32_t* vbuffer, uint32_t stride,
+                              uint32_t threads, orc_counters* cnt) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    uint32_t nthreads = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
+    std::vector<PathCounters> pcs(nthreads);
+    const uint32_t sw = (p->width + stride - 1) / stride, sh = (p->height + stride - 1) / stride;
+    auto t0 = std::chrono::steady_clock::now();
+    parallel_tiles(0, 0, sw, sh, nthreads, [&](uint32_t sx, uint32_t sy, uint32_t tid) {
+        const uint32_t x = sx * stride, y = sy * stride;
+        const size_t i = size_t(y) * p->width + x;
+        float color[4];
+        path_tracer_pixel<float>(s, *p, x, y, vbuffer + 4 * i, nullptr, color, &pcs[tid]);
+    });
+    double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (cnt) sum_counters(pcs, cnt);
     return dt;
 }
 

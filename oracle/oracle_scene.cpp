@@ -5,6 +5,8 @@
 #include "oracle_scene.h"
 
 #include <algorithm>
+#include <cmath>
+#include <cstring>
 #include <numeric>
 #include <random>
 #include <stdexcept>
@@ -448,11 +450,111 @@ Hit Scene::traceImpl(V3<R> o, V3<R> d, R tMin, R tMax, bool anyHit, TraceCounter
     return best;
 }
 
+void Scene::attachBvh8(const void* nodes, uint32_t nodeCount, const void* tris, uint32_t triCount) {
+    b8nodes.resize(nodeCount);
+    b8tris.resize(triCount);
+    if (nodeCount) std::memcpy(b8nodes.data(), nodes, size_t(nodeCount) * sizeof(Bvh8NodeO));
+    if (triCount) std::memcpy(b8tris.data(), tris, size_t(triCount) * sizeof(Bvh8TriO));
+}
+
+// Exact traversal of the attached 8-wide BVH: child boxes decoded in double,
+// exact slab tests against [tMin, best t], hit children visited nearest entry
+// first (a child whose entry lies beyond the best hit found meanwhile is
+// skipped when popped).  Counts every node visited and every triangle tested:
+// the algorithmic work of a closest-hit (any-hit) query on this tree.
+Hit Scene::traceBvh8(V3<float> o, V3<float> d, float tMin, float tMax, bool anyHit, uint64_t& nodes, uint64_t& tris) const {
+    Hit best;
+    float bestT = tMax;
+    uint32_t bestTri = 0xffffffffu;
+    float bestU = 0.f, bestV = 0.f;
+    if (b8nodes.empty()) return best;
+    const double inv[3] = {1.0 / double(d.x), 1.0 / double(d.y), 1.0 / double(d.z)};
+    const double org[3] = {o.x, o.y, o.z};
+    struct Entry { uint32_t node; double t; };
+    std::vector<Entry> stack;
+    stack.reserve(128);
+    stack.push_back({0u, double(tMin)});
+    while (!stack.empty()) {
+        const Entry e = stack.back();
+        stack.pop_back();
+        if (e.t > double(bestT)) continue;
+        const Bvh8NodeO& n = b8nodes[e.node];
+        nodes++;
+        Entry kids[8];
+        int nk = 0;
+        uint32_t rank = 0;
+        for (int k = 0; k < 8; k++) {
+            const bool internal = (n.imask >> k) & 1u;
+            const uint32_t childRank = internal ? rank++ : 0u;
+            const uint32_t meta = n.meta[k];
+            if (!internal && meta == 0) continue;  // empty slot
+            double t0 = double(tMin), t1 = double(bestT);
+            for (int a = 0; a < 3 && t0 <= t1; a++) {
+                const double s = std::ldexp(1.0, int(n.e[a]) - 127);
+                const double lo = double(n.p[a]) + double(n.qlo[a][k]) * s, hi = double(n.p[a]) + double(n.qhi[a][k]) * s;
+                double ta = (lo - org[a]) * inv[a], tb = (hi - org[a]) * inv[a];
+                if (std::isnan(ta) || std::isnan(tb)) { ta = -INFINITY; tb = INFINITY; }
+                if (ta > tb) std::swap(ta, tb);
+                t0 = std::max(t0, ta);
+                t1 = std::min(t1, tb);
+            }
+            if (t0 > t1) continue;
+            if (internal) {
+                kids[nk++] = {n.childBase + childRank, t0};
+                continue;
+            }
+            // Leaf slot: its triangles are tested now (nearest-first order
+            // matters only across internal children).
+            const uint32_t first = n.triBase + (meta & 31u), count = meta >> 5;
+            for (uint32_t i = 0; i < count; i++) {
+                const Bvh8TriO& tr = b8tris[first + i];
+                V3<float> v[3] = {V3<float>(tr.v0[0], tr.v0[1], tr.v0[2]), V3<float>(tr.v1[0], tr.v1[1], tr.v1[2]),
+                                  V3<float>(tr.v2[0], tr.v2[1], tr.v2[2])};
+                V3<float> bary;
+                float t;
+                tris++;
+                if (!intersect_ray_triangle(o, d, v, bary, t)) continue;
+                if (!(t >= tMin && t <= bestT)) continue;
+                if (t == bestT && tr.globalTri > bestTri) continue;
+                bestT = t;
+                bestTri = tr.globalTri;
+                bestU = bary.y;
+                bestV = bary.z;
+                if (anyHit) {
+                    best.valid = true;
+                    return best;
+                }
+            }
+        }
+        // Push far to near so that the nearest child is popped first.
+        std::sort(kids, kids + nk, [](const Entry& a, const Entry& b) { return a.t > b.t; });
+        for (int i = 0; i < nk; i++) stack.push_back(kids[i]);
+    }
+    if (bestTri != 0xffffffffu) {
+        best.valid = true;
+        best.globalTri = bestTri;
+        best.baryX = bestU;
+        best.baryY = bestV;
+        best.t = bestT;
+    }
+    return best;
+}
+
 Hit Scene::traceClosest(V3<float> o, V3<float> d, float tMin, float tMax, TraceCounters* c) const {
-    return traceImpl<float>(o, d, tMin, tMax, false, c);
+    Hit h = traceImpl<float>(o, d, tMin, tMax, false, c);
+    if (c && !b8nodes.empty()) {
+        const Hit g = traceBvh8(o, d, tMin, tMax, false, c->b8NodesClosest, c->b8TrisClosest);
+        if (g.valid != h.valid || (h.valid && (g.globalTri != h.globalTri || g.t != h.t))) c->b8Mismatch++;
+    }
+    return h;
 }
 bool Scene::traceVisibility(V3<float> o, V3<float> d, float tMin, float tMax, TraceCounters* c) const {
-    return !traceImpl<float>(o, d, tMin, tMax, true, c).valid;
+    const bool vis = !traceImpl<float>(o, d, tMin, tMax, true, c).valid;
+    if (c && !b8nodes.empty()) {
+        const Hit g = traceBvh8(o, d, tMin, tMax, true, c->b8NodesShadow, c->b8TrisShadow);
+        if (g.valid == vis) c->b8Mismatch++;
+    }
+    return vis;
 }
 Hit Scene::traceClosestD(V3<double> o, V3<double> d, double tMin, double tMax) const {
     return traceImpl<double>(o, d, tMin, tMax, false, nullptr);

@@ -64,7 +64,31 @@ struct Hit {
 
 struct TraceCounters {
     uint64_t closest = 0, shadow = 0, nodeVisits = 0, triTests = 0;
+    // Exact nearest-first traversal of the library's 8-wide BVH (attachBvh8):
+    // node visits and triangle tests of closest-hit and visibility rays, and
+    // rays whose result differs from the oracle's own tree.
+    uint64_t b8NodesClosest = 0, b8TrisClosest = 0, b8NodesShadow = 0, b8TrisShadow = 0, b8Mismatch = 0;
 };
+
+// The library's compressed 8-wide BVH node and triangle record, as
+// falcor_b200/csrc/common.h lays them out (80 and 48 bytes): box slot k
+// spans p + q{lo,hi}[k] 2^(e - 127) per axis; meta[k] = (count << 5) | offset
+// of a leaf slot; internal children are contiguous from childBase in slot order.
+struct Bvh8NodeO {
+    float p[3];
+    uint8_t e[3];
+    uint8_t imask;
+    uint32_t childBase, triBase;
+    uint8_t meta[8];
+    uint8_t qlo[3][8], qhi[3][8];
+};
+static_assert(sizeof(Bvh8NodeO) == 80, "Bvh8NodeO must be 80 bytes");
+struct Bvh8TriO {
+    float v0[3]; uint32_t globalTri;
+    float v1[3]; uint32_t instanceID;
+    float v2[3]; uint32_t primIndex;
+};
+static_assert(sizeof(Bvh8TriO) == 48, "Bvh8TriO must be 48 bytes");
 
 // Camera::calculateCameraParameters ray-tracing vectors (Scene/Camera/Camera.cpp:112-195).
 void camera_data_from(const fpt_camera& c, fpt_camera_data& o);
@@ -119,6 +143,12 @@ public:
 
     // brute-force closest hit over all triangles (for traversal tests)
     Hit traceClosestBrute(V3<float> o, V3<float> d, float tMin, float tMax) const;
+    // Attaches a copy of the library's 8-wide BVH: the FP32 traces then also
+    // traverse it (exactly, nearest child first) to count the algorithmic node
+    // visits and triangle tests into TraceCounters::b8*.
+    void attachBvh8(const void* nodes, uint32_t nodeCount, const void* tris, uint32_t triCount);
+    std::vector<Bvh8NodeO> b8nodes;
+    std::vector<Bvh8TriO> b8tris;
 
 private:
     struct Node { float lo[3], hi[3]; uint32_t left, right, first, count; };
@@ -128,6 +158,7 @@ private:
     void buildLights(uint32_t aliasSeed);
     void buildEnv(const fpt_envmap_desc* env);
     template <class R> Hit traceImpl(V3<R> o, V3<R> d, R tMin, R tMax, bool anyHit, TraceCounters* c) const;
+    Hit traceBvh8(V3<float> o, V3<float> d, float tMin, float tMax, bool anyHit, uint64_t& nodes, uint64_t& tris) const;
 };
 
 // Packs one vertex like PackedStaticVertexData::pack on the host.

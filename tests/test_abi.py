@@ -185,3 +185,37 @@ def test_set_properties_from_json_dump(fpt):
     assert fpt.fpt_pass_set_properties_json(pt.handle, b'{"samplesPerPixel": }') == 1
     assert fpt.fpt_pass_set_properties_json(pt.handle, b'{"emissiveSampler": "Nope"}') == 1
     assert fpt.fpt_pass_set_properties_json(pt.handle, b"{}") == 0
+
+
+def _host_bvh8(fpt, host):
+    from falcor_b200 import _ffi
+    h = C.c_void_p()
+    _ffi.check(fpt.fpt_bvh_build(C.byref(host.desc), C.byref(h)))
+    v = _ffi.fpt_bvh_view()
+    depth, secs = C.c_uint32(), C.c_double()
+    _ffi.check(fpt.fpt_bvh_get_view(h, C.byref(v), C.byref(depth), C.byref(secs)))
+    nodes = np.ctypeslib.as_array(C.cast(v.nodes, C.POINTER(C.c_uint8)), shape=(v.node_count * 80,)).copy()
+    tris = np.ctypeslib.as_array(C.cast(v.tris, C.POINTER(C.c_uint8)), shape=(v.tri_count * 48,)).copy()
+    fpt.fpt_bvh_free(h)
+    return nodes, tris
+
+
+def test_oracle_traverses_library_bvh8_with_identical_hits(fpt, oracle):
+    """The oracle's exact nearest-first traversal of the library's 8-wide BVH
+    (the counter behind the benchmark's algorithmic bytes) finds the same
+    closest hits and visibility as the oracle's own tree on every ray of a
+    path-traced frame, and counts node visits and triangle tests."""
+    from tests import helpers as H
+    host = H.small_heightfield(grid_res=64, soup=2000, emitters=16)
+    nodes, tris = _host_bvh8(fpt, host)
+    osc = H.oracle_scene(host)
+    osc.attach_bvh8(nodes, tris)
+    W, Hh = 64, 48
+    vb = osc.vbuffer(W, Hh)
+    cnt, _ = osc.path_tracer_counts(vb, H.pt_params(W, Hh, 4, seed=3, max_bounces=4), stride=1)
+    assert cnt.closest > 0 and cnt.shadow > 0
+    assert cnt.b8_mismatch == 0, cnt.b8_mismatch
+    assert cnt.b8_nodes_closest >= cnt.closest and cnt.b8_tris_closest > 0 and cnt.b8_nodes_shadow > 0
+    # A strided sample covers every stride^2-th pixel.
+    c2, _ = osc.path_tracer_counts(vb, H.pt_params(W, Hh, 4, seed=3, max_bounces=4), stride=4)
+    assert 0 < c2.paths <= cnt.paths // 8
