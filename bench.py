@@ -305,6 +305,7 @@ def inverse_bench(dev, iterations: int = 50) -> dict:
     import gc
     import torch
     from falcor_b200.inverse import InverseLoop, displaced_grid_scene, orbit_cameras
+    from falcor_b200.replicas import max_over_ranks
     from falcor_b200.scene import Scene
     out = {"workload": "displaced grid 100k tris, 8 views 256x256, 8 spp, 4 bounces, WAR adjoint, Adam lr 1e-2, "
                        f"{iterations} iterations", "unit": "ms per iteration"}
@@ -335,7 +336,7 @@ def inverse_bench(dev, iterations: int = 50) -> dict:
             losses.append(loop.step())
         b.record()
         torch.cuda.synchronize()
-        ms = a.elapsed_time(b) / iterations
+        ms = max_over_ranks(a.elapsed_time(b) / iterations, dev)  # views split across ranks
         free1, _ = torch.cuda.mem_get_info(dev)
         paths = 8 * 256 * 256 * 8
         key = mode.lower()
@@ -443,15 +444,18 @@ def batched_bench(dev) -> dict:
     from falcor_b200.scene import HostScene, Scene, batch_requests, batch_scene_params
     hosts = [HostScene.procedural(batch_scene_params(i)[0], **batch_scene_params(i)[1]) for i in range(8)]
     scenes = [Scene(h) for h in hosts]
+    from falcor_b200.replicas import max_over_ranks, shard
     b = Batch()
-    for i, (si, wdt, hgt, spp, mb) in enumerate(batch_requests()):
+    # With several ranks each renders its share of the 64 requests (strong
+    # scaling of a fixed request set); times are the maximum over ranks.
+    for i, (si, wdt, hgt, spp, mb) in shard(batch_requests()):
         b.add(scenes[si], wdt, hgt, spp, mb, seed=i)
-    paths = b.total_paths
+    paths = sum(w * h * spp for (_, w, h, spp, _) in batch_requests())  # all ranks together
     b.launch_sequential()
-    t_seq = _time_ms(b.launch_sequential, 2)
+    t_seq = max_over_ranks(_time_ms(b.launch_sequential, 2), dev)
     tuning = b.autotune()
     b.launch()
-    t_bat = _time_ms(b.launch, 3)
+    t_bat = max_over_ranks(_time_ms(b.launch, 3), dev)
     st = b.stats()
     return {"workload": "64 requests, 8 scenes of 10k-1M triangles, res {128..1024}^2, spp {1,4,16,32}, bounces 2-8",
             "unit": "Mpaths/s", "paths_per_launch": paths, "batched": round(paths / t_bat / 1e3, 2),

@@ -38,6 +38,7 @@ import numpy as np
 
 from . import _ffi
 from .diff import DiffRenderer
+from .replicas import shard, sharded_sum
 from .scene import HostScene, Scene
 
 
@@ -214,15 +215,16 @@ class InverseLoop:
     def render_targets(self, disp_target, color_target, spp: int | None = None) -> list:
         """Renders the target views with the given parameters (then restores the
         current ones), at `spp` samples per pixel if given.  With fresh seeds the
-        targets use seeds of their own; otherwise view v uses seed v."""
+        targets use seeds of their own; otherwise view v uses seed v.  Returns
+        {view index: image} for the views of this rank (all views on one GPU)."""
         self.apply(disp_target, color_target)
         if spp:
             self.renderer.pt.set_properties({"samplesPerPixel": int(spp)})
-        out = []
+        out = {}
         base = (1 << 20) if self.fresh_seeds else 0
-        for v, cam in enumerate(self.views):
+        for v, cam in shard(self.views):
             self.scene.set_camera(cam)
-            out.append(self.renderer.render(base + v))
+            out[v] = self.renderer.render(base + v)
         if spp:
             self.renderer.pt.set_properties({"samplesPerPixel": int(self.spp)})
         self.targets = out
@@ -230,23 +232,27 @@ class InverseLoop:
         return out
 
     def gradients(self):
-        """Loss and the gradients of the current parameters, summed over the views."""
+        """Loss and the gradients of the current parameters, summed over the views.
+        Under torch.distributed the views are split across the ranks (``shard``)
+        and the per-rank sums are all-reduced, so every rank returns the same
+        totals and takes the same optimizer step."""
         import torch
-        gp = torch.zeros((self.nv, 3), dtype=torch.float32, device="cuda")
-        gn = torch.zeros((self.nv, 3), dtype=torch.float32, device="cuda")
-        gc = torch.zeros_like(self.color)
-        loss = 0.0
-        for v, cam in enumerate(self.views):
+
+        def view(v, cam):
             seed = self.iteration * len(self.views) + v if self.fresh_seeds else v
             self.scene.set_camera(cam)
             img = self.renderer.render(seed)
             diff = img - self.targets[v]
-            loss += float((diff * diff).mean())
+            loss = (diff * diff).mean().reshape(1)
             dLdI = (2.0 / diff.numel()) * diff
             gm, gpv = self.renderer.gradients(dLdI, seed, position_dim=3 * self.nv, normal_dim=3 * self.nv)
-            gp += gpv.view(self.nv, 3)
-            gn += self.renderer.normal_grad.view(self.nv, 3)
-            gc += gm.view(-1, 20)[:, 0:3]
+            return (loss, gpv.view(self.nv, 3).clone(), self.renderer.normal_grad.view(self.nv, 3).clone(),
+                    gm.view(-1, 20)[:, 0:3].clone())
+
+        zeros = (torch.zeros(1, device="cuda"), torch.zeros((self.nv, 3), device="cuda"),
+                 torch.zeros((self.nv, 3), device="cuda"), torch.zeros_like(self.color))
+        loss_t, gp, gn, gc = sharded_sum(self.views, view, like=zeros)
+        loss = float(loss_t.item())
         # Chain rule through p = p0 + d n0 and n(p).
         with torch.enable_grad():
             d = self.disp.detach().clone().requires_grad_(True)
