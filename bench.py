@@ -291,13 +291,15 @@ def _time_ms(fn, reps: int) -> float:
     return e0.elapsed_time(e1) / reps
 
 
-def inverse_bench(dev, iterations: int = 50) -> dict:
+def inverse_bench(dev, iterations: int = 200) -> dict:
     """Inverse-rendering loop: Adam (lr 1e-2) over the 50 625 per-vertex normal
-    displacements and the base colour of a 100 352-triangle grid, 8 views per
-    iteration at 256 x 256, 8 spp, 4 bounces, forward + adjoint per view with
-    the warped-area boundary term (the displacements move silhouettes); the
-    same loop with path replay and with checkpointed path vertices.  Targets are
-    rendered once at 64 spp; every iteration draws fresh sample seeds.  Reports the
+    displacements of a 100 352-triangle grid and its 512 x 512 RGBA8 (sRGB)
+    albedo texture, 8 views per iteration at 256 x 256, 8 spp, 4 bounces,
+    forward + adjoint per view with the warped-area boundary term (the
+    displacements move silhouettes); the same loop with path replay and with
+    checkpointed path vertices.  Targets are rendered once at 64 spp from a
+    target displacement field and a target texture; every iteration draws
+    fresh sample seeds.  Reports the
     time per iteration, the forward + adjoint path rate, the loss reduction, the
     device memory the mode holds at the end of its loop (scene, pass buffers,
     torch tensors; measured from an emptied allocator cache) and the bytes of
@@ -307,13 +309,13 @@ def inverse_bench(dev, iterations: int = 50) -> dict:
     from falcor_b200.inverse import InverseLoop, displaced_grid_scene, orbit_cameras
     from falcor_b200.replicas import max_over_ranks
     from falcor_b200.scene import Scene
-    out = {"workload": "displaced grid 100k tris, 8 views 256x256, 8 spp, 4 bounces, WAR adjoint, Adam lr 1e-2, "
-                       f"{iterations} iterations", "unit": "ms per iteration"}
+    out = {"workload": "displaced grid 100k tris + 512x512 RGBA8 albedo texture, 8 views 256x256, 8 spp, 4 bounces, "
+                       f"WAR adjoint, Adam lr 1e-2, {iterations} iterations", "unit": "ms per iteration"}
     # One small iteration of each mode first, so that lazily loaded kernels and
     # library workspaces are not counted in the first mode's memory.
     for mode in ("Replay", "Checkpoint"):
-        small = InverseLoop(Scene(displaced_grid_scene(res=8)), 0, orbit_cameras(1), 32, 32, spp=1, max_bounces=1,
-                            adjoint_mode=mode)
+        small = InverseLoop(Scene(displaced_grid_scene(res=8, texture=(16, 16))), 0, orbit_cameras(1), 32, 32, spp=1,
+                            max_bounces=1, adjoint_mode=mode, texture_index=0, optimize=("displacement", "color", "texture"))
         small.render_targets(small.disp, small.color.detach())
         small.step()
         del small
@@ -322,11 +324,16 @@ def inverse_bench(dev, iterations: int = 50) -> dict:
         torch.cuda.empty_cache()
         torch.cuda.synchronize()
         free0, total = torch.cuda.mem_get_info(dev)
-        scene = Scene(displaced_grid_scene(res=224))
-        loop = InverseLoop(scene, 0, orbit_cameras(8), 256, 256, spp=8, max_bounces=4, adjoint_mode=mode, lr=1e-2)
+        scene = Scene(displaced_grid_scene(res=224, texture=(512, 512)))
+        loop = InverseLoop(scene, 0, orbit_cameras(8), 256, 256, spp=8, max_bounces=4, adjoint_mode=mode, lr=1e-2,
+                           texture_index=0, optimize=("displacement", "color", "texture"))
         p0 = loop.p0
+        ty, tx = torch.meshgrid(torch.linspace(0, 1, 512, device=dev), torch.linspace(0, 1, 512, device=dev), indexing="ij")
+        tex_target = torch.stack([0.45 + 0.3 * torch.sin(9.0 * tx), 0.4 + 0.3 * torch.cos(7.0 * ty),
+                                  0.35 + 0.25 * torch.sin(5.0 * (tx + ty))], 2)
         loop.render_targets(0.03 * torch.sin(4.0 * p0[:, 0]) * torch.cos(4.0 * p0[:, 2]),
-                            (loop.color.detach() * 0.8 + 0.1).clamp(0, 1), spp=64)
+                            (loop.color.detach() * 0.8 + 0.1).clamp(0, 1), spp=64, texture_target=tex_target)
+        tex_err0 = float((loop.texture.detach() - tex_target).abs().mean())
         loop.step()  # warm-up: allocations, checkpoint buffers
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -342,6 +349,8 @@ def inverse_bench(dev, iterations: int = 50) -> dict:
         key = mode.lower()
         out[key] = {"ms_per_iteration": round(ms, 3), "fwd_plus_adjoint_Mpaths_s": round(paths / (ms / 1e3) / 1e6, 2),
                     "loss_first": losses[0], "loss_last": losses[-1],
+                    "texture_mean_abs_error_first": round(tex_err0, 5),
+                    "texture_mean_abs_error_last": round(float((loop.texture.detach() - tex_target).abs().mean()), 5),
                     "device_mb_in_use": round((free0 - free1) / 2**20, 1)}
         st = loop.renderer.pt.stats()
         out[key]["checkpoint_mb"] = round(st.checkpoint_bytes / 2**20, 1)
@@ -424,6 +433,7 @@ def adjoint_bench(dev) -> dict:
     t_pair_ckpt = _time_ms(pair(pc), 3)
     ck_stats = pc.stats()
     paths = W * Hh * frames
+    roof = adjoint_roofline(host, scene, W, Hh, w.max_bounces, {"adjoint": t_bwd / frames, "adjoint_war": t_war / frames})
     return {"workload": "displaced_sphere 512x512, 16 frames x 1 spp, maxBounces 4, material + position gradients",
             "unit": "Mpaths/s", "forward": round(paths / t_fwd / 1e3, 2), "adjoint": round(paths / t_bwd / 1e3, 2),
             "fwd_plus_adjoint": round(paths / (t_fwd + t_bwd) / 1e3, 2), "ms_forward": round(t_fwd, 3),
@@ -433,7 +443,38 @@ def adjoint_bench(dev) -> dict:
             "fwd_plus_adjoint_checkpointed": round(paths / t_pair_ckpt / 1e3, 2),
             "checkpoint_mb_per_frame": round(ck_stats.checkpoint_bytes / 2**20, 1),
             "checkpoint_used": int(ck_stats.adjoint_checkpointed),
-            "triangles": scene.info.triangle_count, "gradient_dims": [gm.numel(), gp.numel()]}
+            "triangles": scene.info.triangle_count, "gradient_dims": [gm.numel(), gp.numel()], "roofline": roof}
+
+
+def adjoint_roofline(host, scene, W: int, Hh: int, max_bounces: int, ms_per_frame: dict) -> dict:
+    """HBM roofline of the adjoint: the algorithmic bytes of one frame's
+    traversals (80 B per BVH8 node visit, 48 B per triangle test) from the CPU
+    oracle's exact traversal of the same tree for the rays the adjoint traces
+    -- the replayed path, its visibility rays and, with WAR, the 16 auxiliary
+    rays of every reparameterisation -- over every 2nd pixel in x and y,
+    scaled to the frame; divided by the measured adjoint time per frame."""
+    from tests import helpers as H
+    from oracle.ffi import WarDiffParams
+    peak, peak_kind = peaks()
+    osc = H.oracle_scene(host)
+    nodes, tris = scene.bvh()
+    osc.attach_bvh8(nodes, tris)
+    out = {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_kind": peak_kind}
+    for key, war in (("adjoint", 0), ("adjoint_war", 1)):
+        prm = WarDiffParams(width=W, height=Hh, maxBounces=max_bounces, useBSDFSampling=1, useNEE=1, useMIS=1, useAntithetic=1,
+                            seed=0, lambert=0, meshID=0xffffffff, useWAR=war, auxSampleCount=16, log10Kappa=5.0,
+                            log10KappaScreen=5.0)
+        c = osc.wardiff_traversal(prm, stride=2, threads=os.cpu_count() or 1)
+        scale = (W * Hh) / c["sampled_pixels"]
+        b = (80 * (c["nodes_closest"] + c["nodes_shadow"]) + 48 * (c["tris_closest"] + c["tris_shadow"])) * scale
+        ach = b / (ms_per_frame[key] / 1e3) / 1e9
+        out[key] = {"algorithmic_bytes_per_frame": int(b), "ms_per_frame": round(ms_per_frame[key], 3),
+                    "achieved": round(ach, 2), "frac": round(ach / peak, 4),
+                    "node_visits_per_frame": int((c["nodes_closest"] + c["nodes_shadow"]) * scale),
+                    "oracle_mismatches": c["mismatches"]}
+    out["source"] = ("CPU oracle forward-mode pass (the adjoint's rays) with exact nearest-first traversal of the same BVH8, "
+                     "every 2nd pixel in x and y, frame seed 0")
+    return out
 
 
 def batched_bench(dev) -> dict:

@@ -45,11 +45,19 @@ class fpt_envmap_desc(C.Structure):
     _fields_ = [("width", u32), ("height", u32), ("rgb", C.POINTER(f32)), ("tint", f32 * 3), ("intensity", f32)]
 
 
+class fpt_texture_desc(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("format", u32), ("texels", C.c_void_p)]
+
+
+TEXTURE_RGBA8_UNORM_SRGB, TEXTURE_RGBA8_UNORM, TEXTURE_RGBA32_FLOAT = 0, 1, 2
+
+
 class fpt_scene_desc(C.Structure):
     _fields_ = [("vertices", C.POINTER(fpt_vertex)), ("vertex_count", u32), ("indices", C.POINTER(u32)), ("index_count", u32),
                 ("instances", C.POINTER(fpt_geometry_instance)), ("instance_count", u32),
                 ("materials", C.POINTER(fpt_material)), ("material_count", u32), ("camera", fpt_camera),
-                ("envmap", C.POINTER(fpt_envmap_desc))]
+                ("envmap", C.POINTER(fpt_envmap_desc)), ("textures", C.POINTER(fpt_texture_desc)), ("texture_count", u32),
+                ("base_color_textures", C.POINTER(u32))]
 
 
 class fpt_procedural_params(C.Structure):
@@ -89,7 +97,8 @@ class fpt_frame_io(C.Structure):
 
 class fpt_grad_buffers(C.Structure):
     _fields_ = [("material", C.c_void_p), ("mesh_position", C.c_void_p), ("material_dim", u32), ("position_dim", u32),
-                ("mesh_normal", C.c_void_p), ("mesh_tangent", C.c_void_p), ("normal_dim", u32), ("tangent_dim", u32)]
+                ("mesh_normal", C.c_void_p), ("mesh_tangent", C.c_void_p), ("normal_dim", u32), ("tangent_dim", u32),
+                ("base_color_texture", C.c_void_p), ("texture_dim", u32)]
 
 
 class fpt_grad_config(C.Structure):
@@ -136,6 +145,7 @@ SIGNATURES = {
     "fpt_scene_get_material_params": (C.c_int, [_P, C.POINTER(u32), u32, C.POINTER(C.c_float)]),
     "fpt_scene_set_material_params": (C.c_int, [_P, C.POINTER(u32), u32, C.POINTER(C.c_float)]),
     "fpt_scene_set_material_params_device": (C.c_int, [_P, C.POINTER(u32), u32, _P, _P]),
+    "fpt_scene_set_texture_device": (C.c_int, [_P, u32, _P, _P]),
     "fpt_scene_get_bvh": (C.c_int, [_P, C.POINTER(fpt_bvh_view)]),
     "fpt_scene_get_alias_table": (C.c_int, [_P, C.POINTER(u32), u32, C.POINTER(f32)]),
     "fpt_pass_create": (C.c_int, [C.c_char_p, C.POINTER(_P)]),

@@ -89,11 +89,24 @@ struct alignas(16) DevMaterial {
     uint16_t specTrans;       // fp16
     uint16_t diffTrans;       // fp16
     uint16_t transmission[3]; // fp16
-    uint16_t flags;           // bit0 double-sided, bit1 thin surface
+    uint16_t flags;           // bit0 double-sided, bit1 thin surface, bit2 base-colour texture
     uint16_t activeLobes;
-    uint32_t pad[4];
+    uint32_t baseColorTexture; // texture index when flags bit2 is set (the fourth 16-byte load)
+    uint32_t pad[3];
 };
 static_assert(sizeof(DevMaterial) == 64, "DevMaterial must be 64 bytes");
+
+constexpr uint16_t kMatFlagBaseColorTexture = 4;
+
+// A material texture in the scene's texel buffer, 32 bytes.
+struct alignas(16) DevTexture {
+    uint64_t offset;     // byte offset of texel (0, 0) in the texel buffer
+    uint32_t width, height;
+    uint32_t format;     // fpt_texture_format
+    uint32_t texelBase;  // texels of the textures before this one (gradient index base)
+    uint32_t pad[2];
+};
+static_assert(sizeof(DevTexture) == 32, "DevTexture must be 32 bytes");
 
 // PackedEmissiveTriangle (Scene/Lights/LightCollectionShared.slang:77-135), 64 bytes.
 struct alignas(16) DevEmissiveTri {

@@ -5,6 +5,7 @@
 #pragma once
 
 #include "device_math.cuh"
+#include "texture.h"
 
 namespace fpt {
 
@@ -40,6 +41,10 @@ struct DevScene {
     uint32_t bvhDepth;                // levels of the 8-wide tree (root = 1)
     uint32_t materialCount;
     uint32_t* errorWord;              // device error word (FPT_DEVERR_*)
+    const uint8_t* texData;           // texels of all material textures
+    const DevTexture* textures;
+    const float* srgbDecode;          // 256-entry sRGB decode table
+    uint32_t textureCount;
 };
 
 namespace dev {
@@ -454,6 +459,7 @@ FPT_D float3 camera_ray_dir(const fpt_camera_data& c, uint32_t px, uint32_t py, 
 // ---------------------------------------------------------------------------
 struct ShadingData {
     float3 posW, V, T, B, N, faceN;
+    float2 uv;
     bool frontFacing;
     uint32_t materialID;
 };
@@ -501,6 +507,9 @@ FPT_D ShadingData load_shading_data(const DevScene& s, const HitRec& hit, float3
     tw += w1 * b1;
     tw += w2 * b2;
     tw = sgn(tw);
+    float2 uv = make_float2(pv0.uv[0] * b0, pv0.uv[1] * b0);
+    uv.x += pv1.uv[0] * b1; uv.y += pv1.uv[1] * b1;
+    uv.x += pv2.uv[0] * b2; uv.y += pv2.uv[1] * b2;
     float3 faceN = normalize(cross(p1 - p0, p2 - p0));
     if (inst.flags & FPT_INSTANCE_FRONT_FACE_CW) faceN = -faceN;
     normalW = normalize(normalW);
@@ -523,9 +532,67 @@ FPT_D ShadingData load_shading_data(const DevScene& s, const HitRec& hit, float3
         sd.B = cross(sd.N, sd.T);
     }
     sd.faceN = faceN;
+    sd.uv = uv;
     sd.frontFacing = dot(sd.V, sd.faceN) >= 0.f;
     sd.materialID = inst.materialID;
     return sd;
+}
+
+// Interpolated texture coordinate of a triangle hit (getVertexData's texC,
+// Scene.slang) for code that has the hit but not its ShadingData.
+FPT_D float2 hit_uv(const DevScene& s, uint32_t instanceID, uint32_t primIndex, float bx, float by) {
+    const DevInstance inst = s.instances[instanceID];
+    const uint32_t* ip = s.indices + inst.ibOffset + primIndex * 3;
+    const float b0 = 1.f - bx - by;
+    const PackedVertex v0 = load_vertex(s.vertices, __ldg(ip) + inst.vbOffset);
+    const PackedVertex v1 = load_vertex(s.vertices, __ldg(ip + 1) + inst.vbOffset);
+    const PackedVertex v2 = load_vertex(s.vertices, __ldg(ip + 2) + inst.vbOffset);
+    float2 uv = make_float2(v0.uv[0] * b0, v0.uv[1] * b0);
+    uv.x += v1.uv[0] * bx; uv.y += v1.uv[1] * bx;
+    uv.x += v2.uv[0] * by; uv.y += v2.uv[1] * by;
+    return uv;
+}
+
+// ---------------------------------------------------------------------------
+// Base-colour textures: MaterialSystem::sampleTexture with
+// ExplicitLodTextureSampler(0) (MaterialSystem.slang:308-320), bilinear at mip 0
+// with wrap addressing (texture.h), texels decoded per format.
+// ---------------------------------------------------------------------------
+FPT_D float3 tex_texel(const DevScene& s, const DevTexture& t, uint32_t x, uint32_t y) {
+    const size_t i = size_t(y) * t.width + x;
+    if (t.format == fpt_tex::kRGBA32Float) {
+        const float4 c = __ldg(reinterpret_cast<const float4*>(s.texData + t.offset) + i);
+        return make_float3(c.x, c.y, c.z);
+    }
+    const uint32_t c = __ldg(reinterpret_cast<const uint32_t*>(s.texData + t.offset) + i);
+    if (t.format == fpt_tex::kRGBA8Srgb)
+        return make_float3(__ldg(s.srgbDecode + (c & 0xffu)), __ldg(s.srgbDecode + ((c >> 8) & 0xffu)),
+                           __ldg(s.srgbDecode + ((c >> 16) & 0xffu)));
+    return make_float3(fpt_tex::unorm8(c & 0xffu), fpt_tex::unorm8((c >> 8) & 0xffu), fpt_tex::unorm8((c >> 16) & 0xffu));
+}
+FPT_D DevTexture load_texture(const DevScene& s, uint32_t id) {
+    const uint4* p = reinterpret_cast<const uint4*>(s.textures + id);
+    const uint4 a = __ldg(p), b = __ldg(p + 1);
+    DevTexture t;
+    t.offset = uint64_t(a.x) | (uint64_t(a.y) << 32);
+    t.width = a.z; t.height = a.w; t.format = b.x; t.texelBase = b.y;
+    return t;
+}
+FPT_D float3 tex_sample(const DevScene& s, uint32_t id, float2 uv) {
+    const DevTexture t = load_texture(s, id);
+    const fpt_tex::Bilinear b = fpt_tex::bilinear(uv.x, uv.y, t.width, t.height);
+    float3 c = tex_texel(s, t, b.x0, b.y0) * b.w[0];
+    c += tex_texel(s, t, b.x1, b.y0) * b.w[1];
+    c += tex_texel(s, t, b.x0, b.y1) * b.w[2];
+    c += tex_texel(s, t, b.x1, b.y1) * b.w[3];
+    return c;
+}
+// Texture index of material `id` if its base colour is textured, else ~0u.
+FPT_D uint32_t material_base_texture(const DevScene& s, uint32_t id) {
+    const uint4* mp = reinterpret_cast<const uint4*>(s.materials + id);
+    const uint4 m2 = __ldg(mp + 2);
+    if (!(m2.w & kMatFlagBaseColorTexture)) return ~0u;
+    return __ldg(reinterpret_cast<const uint32_t*>(mp + 3));
 }
 
 FPT_D float3 sd_ray_origin(const ShadingData& sd, bool viewside = true) {
@@ -627,7 +694,8 @@ FPT_D MaterialInstance<HAS_TRANSMISSION> material_instance(const DevScene& s, co
     if (d.diffTrans > 0.f || d.specTrans > 0.f) d.transmission = make_float3(f16(m2.y >> 16), f16(m2.z & 0xffffu), f16(m2.z >> 16));
     const float f = (IoR - 1.f) / (IoR + 1.f);
     const float F0 = f * f;
-    const float3 baseColor = make_float3(f16(m0.x & 0xffffu), f16(m0.x >> 16), f16(m0.y & 0xffffu));
+    float3 baseColor = make_float3(f16(m0.x & 0xffffu), f16(m0.x >> 16), f16(m0.y & 0xffffu));
+    if (flags & kMatFlagBaseColorTexture) baseColor = tex_sample(s, __ldg(reinterpret_cast<const uint32_t*>(mp + 3)), sd.uv);
     const float specG = f16(m0.z >> 16), specB = f16(m0.w & 0xffffu);
     d.diffuse = lerp(baseColor, f3(0.f), specB);
     d.specular = lerp(f3(F0), baseColor, specB);

@@ -129,7 +129,7 @@ DeviceBuffers::~DeviceBuffers() {
 
 // BasicMaterialData packing of a StandardMaterial (fp16 fields quantised on
 // the host like Falcor's float16_t, Utils/Math/Float16.cpp:56-169).
-DevMaterial pack_material(const fpt_material& s0) {
+DevMaterial pack_material(const fpt_material& s0, uint32_t baseColorTexture) {
     DevMaterial o;
     std::memset(&o, 0, sizeof(o));
     for (int k = 0; k < 4; k++) { o.baseColor[k] = f32_to_f16_host(s0.base_color[k]); o.specular[k] = f32_to_f16_host(s0.specular[k]); }
@@ -140,6 +140,10 @@ DevMaterial pack_material(const fpt_material& s0) {
     o.diffTrans = f32_to_f16_host(s0.diffuse_transmission);
     o.flags = uint16_t((s0.flags & FPT_MATERIAL_DOUBLE_SIDED ? 1u : 0u) | (s0.flags & FPT_MATERIAL_THIN_SURFACE ? 2u : 0u));
     o.activeLobes = 0xff;
+    if (baseColorTexture) {
+        o.flags |= kMatFlagBaseColorTexture;
+        o.baseColorTexture = baseColorTexture - 1;
+    }
     return o;
 }
 
@@ -151,6 +155,17 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
     if (d.index_count && !d.indices) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: indices is NULL");
     if (d.instance_count && !d.instances) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: instances is NULL");
     if (d.material_count == 0 || !d.materials) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: no materials");
+    if (d.texture_count && !d.textures) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: textures is NULL");
+    for (uint32_t t = 0; t < d.texture_count; t++) {
+        const fpt_texture_desc& td = d.textures[t];
+        if (!td.texels || td.width == 0 || td.height == 0 || td.width > 65536 || td.height > 65536 || td.format > FPT_TEXTURE_RGBA32_FLOAT)
+            return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: texture " + std::to_string(t) +
+                                                      " needs texels, a size in [1, 65536]^2 and a known format");
+    }
+    if (d.base_color_textures)
+        for (uint32_t m = 0; m < d.material_count; m++)
+            if (d.base_color_textures[m] > d.texture_count)
+                return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: material " + std::to_string(m) + " names a missing texture");
     // The traversal's conservative box test needs |coordinate| * |1/d| to
     // stay finite (|1/d| <= 1e20): positions are limited to |x| <= 1e15.
     for (uint32_t i = 0; i < d.vertex_count; i++)
@@ -222,10 +237,12 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
     std::vector<DevMaterial> mats(d.material_count);
     std::vector<bool> emissiveMat(d.material_count, false);
     s.materials.assign(d.materials, d.materials + d.material_count);
+    s.baseColorTex.assign(d.material_count, 0u);
+    if (d.base_color_textures) s.baseColorTex.assign(d.base_color_textures, d.base_color_textures + d.material_count);
     for (uint32_t m = 0; m < d.material_count; m++) {
         const fpt_material& s0 = d.materials[m];
         DevMaterial& o = mats[m];
-        o = pack_material(s0);
+        o = pack_material(s0, s.baseColorTex[m]);
         if (f16_to_f32_host(o.specTrans) > 0.f || f16_to_f32_host(o.diffTrans) > 0.f) hasTransmission = true;
         emissiveMat[m] = (s0.emissive[0] * s0.emissive_factor > 0.f) || (s0.emissive[1] * s0.emissive_factor > 0.f) ||
                          (s0.emissive[2] * s0.emissive_factor > 0.f);
@@ -374,6 +391,39 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
         }
         if (cudaDeviceSynchronize() != cudaSuccess) return set_error(FPT_ERR_CUDA, std::string("importance map: ") + cudaGetErrorString(cudaGetLastError()));
         ds.impMips = impf;
+    }
+    // Material textures: one texel buffer (each texture 16-byte aligned), the
+    // texture table and the sRGB decode table.
+    if (d.texture_count) {
+        std::vector<DevTexture> tex(d.texture_count);
+        uint64_t bytes = 0;
+        uint32_t texels = 0;
+        for (uint32_t t = 0; t < d.texture_count; t++) {
+            const fpt_texture_desc& td = d.textures[t];
+            DevTexture& o = tex[t];
+            std::memset(&o, 0, sizeof(o));
+            o.offset = bytes;
+            o.width = td.width;
+            o.height = td.height;
+            o.format = td.format;
+            o.texelBase = texels;
+            const uint64_t n = uint64_t(td.width) * td.height;
+            if (uint64_t(texels) + n > 0x7fffffffull) return set_error(FPT_ERR_UNSUPPORTED, "fpt_scene_create: more than 2^31 texels");
+            texels += uint32_t(n);
+            bytes += (n * fpt_tex::texel_bytes(td.format) + 15u) & ~uint64_t(15);
+        }
+        std::vector<uint8_t> data(bytes, 0);
+        for (uint32_t t = 0; t < d.texture_count; t++)
+            std::memcpy(data.data() + tex[t].offset, d.textures[t].texels,
+                        size_t(tex[t].width) * tex[t].height * fpt_tex::texel_bytes(tex[t].format));
+        if ((st = upload(B, data, ds.texData)) != FPT_OK) return st;
+        if ((st = upload(B, tex, ds.textures)) != FPT_OK) return st;
+        float lut[256];
+        fpt_tex::srgb_decode_table(lut);
+        std::vector<float> lutv(lut, lut + 256);
+        if ((st = upload(B, lutv, ds.srgbDecode)) != FPT_OK) return st;
+        ds.textureCount = d.texture_count;
+        s.textures = tex;
     }
     void* err = nullptr;
     if (cudaMalloc(&err, sizeof(uint32_t)) != cudaSuccess) return set_error(FPT_ERR_OOM, "cudaMalloc error word");
@@ -573,7 +623,7 @@ FPT_API fpt_status fpt_scene_set_material_params(fpt_scene* scene, const uint32_
     }
     bool hasTransmission = false;
     for (uint32_t i = 0; i < count; i++) {
-        const DevMaterial dm = pack_material(next[ids[i]]);
+        const DevMaterial dm = pack_material(next[ids[i]], scene->baseColorTex[ids[i]]);
         if (cudaMemcpy(const_cast<DevMaterial*>(scene->dev.materials) + ids[i], &dm, sizeof(dm), cudaMemcpyHostToDevice) != cudaSuccess)
             return set_error(FPT_ERR_CUDA, "fpt_scene_set_material_params: upload failed");
     }
@@ -582,6 +632,19 @@ FPT_API fpt_status fpt_scene_set_material_params(fpt_scene* scene, const uint32_
             hasTransmission = true;
     scene->materials.swap(next);
     scene->dev.hasTransmission = hasTransmission ? 1u : 0u;
+    scene->version++;
+    scene->resetVersion++;
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_scene_set_texture_device(fpt_scene* scene, uint32_t index, const void* texels, void* stream) {
+    if (!scene || !texels) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_texture_device: null argument");
+    if (index >= scene->textures.size()) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_set_texture_device: texture index out of range");
+    const DevTexture& t = scene->textures[index];
+    const size_t bytes = size_t(t.width) * t.height * fpt_tex::texel_bytes(t.format);
+    const cudaError_t e = cudaMemcpyAsync(const_cast<uint8_t*>(scene->dev.texData) + t.offset, texels, bytes, cudaMemcpyDeviceToDevice,
+                                          static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, std::string("fpt_scene_set_texture_device: ") + cudaGetErrorString(e));
     scene->version++;
     scene->resetVersion++;
     return FPT_OK;

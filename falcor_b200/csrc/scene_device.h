@@ -18,7 +18,8 @@ struct DeviceBuffers {
 };
 
 fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out);
-DevMaterial pack_material(const fpt_material& m);
+// baseColorTexture: 1 + texture index, or 0 for the uniform base colour.
+DevMaterial pack_material(const fpt_material& m, uint32_t baseColorTexture = 0);
 
 }  // namespace fpt
 
@@ -28,6 +29,8 @@ struct fpt_scene {
     fpt::BVH8 bvh;                    // host copy of the acceleration structure
     std::vector<uint32_t> aliasTable; // host copy of the alias table
     std::vector<fpt_material> materials;  // host copy of the material parameters
+    std::vector<uint32_t> baseColorTex;   // per material: 1 + base-colour texture index, or 0
+    std::vector<fpt::DevTexture> textures; // host copy of the texture table
     fpt::LightBVH lightBvh;               // host copy of the light BVH
     float aliasWeightSum = 0.f;
     fpt_scene_info info{};

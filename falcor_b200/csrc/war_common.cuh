@@ -145,11 +145,13 @@ struct MatParams {
     float3 baseColor, transmission;
     float metallic, roughness, ior, diffTrans, specTrans;
 };
-FPT_D MatParams load_mat_params(const DevScene& s, uint32_t id) {
+// A textured material's base colour is its texture's value at uv.
+FPT_D MatParams load_mat_params(const DevScene& s, uint32_t id, float2 uv) {
     const uint4* mp = reinterpret_cast<const uint4*>(s.materials + id);
     const uint4 m0 = __ldg(mp), m2 = __ldg(mp + 2);
     MatParams m;
     m.baseColor = make_float3(f16(m0.x & 0xffffu), f16(m0.x >> 16), f16(m0.y & 0xffffu));
+    if (m2.w & kMatFlagBaseColorTexture) m.baseColor = tex_sample(s, __ldg(reinterpret_cast<const uint32_t*>(mp + 3)), uv);
     m.roughness = f16(m0.z >> 16);
     m.metallic = f16(m0.w & 0xffffu);
     m.ior = f16(m2.x & 0xffffu);
@@ -233,8 +235,36 @@ FPT_D void atomic_add_row(float* row, const float (&v)[N]) {
     }
 }
 
-// Material-parameter gradients G[0..10] of material matID from pixel pid.
-FPT_D void add_material_grad_values(const WarParams& p, uint32_t pid, uint32_t hash, uint32_t matID, const float (&G)[11]) {
+// Gradient of a textured base colour.  The reference samples textures no_diff
+// (StandardMaterial.slang:164); here dL/d(texel rgb) += w_k dL/d(baseColor)
+// for the four texels k of the bilinear lookup at uv, into a flat buffer of 3
+// floats per texel of every texture (DevTexture::texelBase order).
+FPT_D void add_texture_grad(const DevScene& s, const WarParams& p, uint32_t tex, float2 uv, float g0, float g1, float g2) {
+    if (!p.gradTex || (g0 == 0.f && g1 == 0.f && g2 == 0.f)) return;
+    const DevTexture t = load_texture(s, tex);
+    const fpt_tex::Bilinear b = fpt_tex::bilinear(uv.x, uv.y, t.width, t.height);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const uint32_t x = (k & 1) ? b.x1 : b.x0, y = (k & 2) ? b.y1 : b.y0;
+        const uint64_t idx = (uint64_t(t.texelBase) + uint64_t(y) * t.width + x) * 3u;
+        if (idx + 3u > p.texDim) continue;
+        const float row[3] = {g0 * b.w[k], g1 * b.w[k], g2 * b.w[k]};
+        atomic_add_row<3>(p.gradTex + idx, row);
+    }
+}
+
+// Material-parameter gradients G[0..10] of material matID from pixel pid; the
+// base-colour entries of a textured material go to its texture at uv.
+FPT_D void add_material_grad_values(const DevScene& s, const WarParams& p, uint32_t pid, uint32_t hash, uint32_t matID, float2 uv,
+                                    const float (&G0)[11]) {
+    float G[11];
+#pragma unroll
+    for (int i = 0; i < 11; i++) G[i] = G0[i];
+    const uint32_t tex = material_base_texture(s, matID);
+    if (tex != ~0u) {
+        add_texture_grad(s, p, tex, uv, G[0], G[1], G[2]);
+        G[0] = G[1] = G[2] = 0.f;
+    }
     if (p.dbgColor && p.dbgType == kDbgMaterial) {
         if (matID != p.dbgId) return;
         float acc = 0.f;
@@ -251,11 +281,12 @@ FPT_D void add_material_grad_values(const WarParams& p, uint32_t pid, uint32_t h
 
 // Adds sum_c G_c * J_c[i] for the 11 material parameters.
 template <int N>
-FPT_D void add_material_grads(const WarParams& p, uint32_t pid, uint32_t hash, uint32_t matID, const DV3<N>& J, float3 G) {
+FPT_D void add_material_grads(const DevScene& s, const WarParams& p, uint32_t pid, uint32_t hash, uint32_t matID, float2 uv,
+                              const DV3<N>& J, float3 G) {
     float v[11];
 #pragma unroll
     for (int i = 0; i < 11; i++) v[i] = G.x * J.x.d[i] + G.y * J.y.d[i] + G.z * J.z.d[i];
-    add_material_grad_values(p, pid, hash, matID, v);
+    add_material_grad_values(s, p, pid, hash, matID, uv, v);
 }
 
 // Position gradient g of a point sum_v b_v x_v of a target mesh's triangle whose

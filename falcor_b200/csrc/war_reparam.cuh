@@ -341,6 +341,228 @@ FPT_D void war_screen_grad(const DevScene& s, const WarParams& p, uint32_t pixel
     war_aux_backprop<2>(s, p, pixelID, p.auxCount, aux, m, gM, gdM, false, base, gO, gD);
 }
 
+// ---------------------------------------------------------------------------
+// Warp-cooperative reparameterisation (wavefront adjoint).  The auxiliary rays
+// of one reparameterisation leave one origin in directions within about
+// 1/sqrt(kappa) of each other, so they visit nearly the same BVH nodes.  A
+// group of G lanes (the power of two >= auxSampleCount) works on one request:
+// lane k samples, traces and weighs auxiliary ray k, the pass-1 sums and the
+// pass-2 origin / direction adjoints are reduced with shuffles inside the
+// group, and 32 / G requests are served side by side.  Compared with one
+// thread tracing all auxiliary rays of its request in turn (war_ray_grad), the
+// traversal is coherent across the group and no per-thread array of samples is
+// kept.  The sums run in a different order than the sequential pass, so the
+// results agree with it to rounding.
+// ---------------------------------------------------------------------------
+struct WarCoopReq {
+    bool active;
+    float3 origin, dir;  // J = 3: ray origin and unwarped direction
+    float2 posS;         // J = 2: jittered screen sample
+    uint4 sg;            // sample generator at the reparameterisation
+    float3 gDir;         // J = 3: adjoint of the warped direction
+    float2 gPix;         // J = 2: adjoint of the warped screen sample
+    float gJ;            // adjoint of the warp's Jacobian determinant
+    bool needD;          // J = 3: the direction's adjoint is wanted (NEE)
+};
+
+FPT_D float3 shfl3(float3 v, int src) {
+    return make_float3(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src), __shfl_sync(0xffffffffu, v.z, src));
+}
+FPT_D float group_sum(float x, uint32_t G) {
+    for (uint32_t off = G >> 1; off; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+    return x;
+}
+FPT_D float3 group_sum3(float3 v, uint32_t G) { return make_float3(group_sum(v.x, G), group_sum(v.y, G), group_sum(v.z, G)); }
+
+// Called by all 32 lanes of a converged warp; J = 3 reparameterizeRay
+// (WarpedAreaReparam.slang:226-263), J = 2 reparameterizeScreenSample
+// (:270-332).  Adds each requesting lane's origin / direction adjoints to gO / gD
+// and the auxiliary hits' position gradients to the scene gradients.
+template <int J>
+FPT_D void war_coop(const DevScene& s, const WarParams& p, uint32_t pid, const WarCoopReq& rq, uint2* stack, uint32_t stride,
+                    float3& gO, float3& gD) {
+    uint32_t lane;
+    asm("mov.u32 %0, %%laneid;" : "=r"(lane));
+    const uint32_t n = p.auxCount;  // 1..kMaxAux, checked by the host
+    uint32_t G = 1;
+    while (G < n) G <<= 1;
+    const uint32_t groups = 32u / G, grp = lane / G, k = lane % G;
+    const float kappa = J == 3 ? p.kappa : p.kappaScreen;
+    const bool anti = p.useAntithetic != 0;
+    const float Wd = float(p.width), Hd = float(p.height);
+    uint32_t pending = __ballot_sync(0xffffffffu, rq.active);
+    while (pending) {
+        // This round's requests: the lowest pending lanes, one per group.
+        int src = -1, myGroup = -1;
+        for (uint32_t gi = 0; gi < groups; gi++) {
+            const int r = pending ? __ffs(pending) - 1 : -1;
+            if (gi == grp) src = r;
+            if (r == int(lane)) myGroup = int(gi);
+            if (pending) pending &= pending - 1u;
+        }
+        const int sl = src >= 0 ? src : int(lane);
+        const bool act = src >= 0 && k < n;
+        const uint32_t rpid = __shfl_sync(0xffffffffu, pid, sl);
+        UniformSG sg;
+        sg.s0 = __shfl_sync(0xffffffffu, rq.sg.x, sl);
+        sg.s1 = __shfl_sync(0xffffffffu, rq.sg.y, sl);
+        sg.s2 = __shfl_sync(0xffffffffu, rq.sg.z, sl);
+        sg.s3 = __shfl_sync(0xffffffffu, rq.sg.w, sl);
+        const float gJ = __shfl_sync(0xffffffffu, rq.gJ, sl);
+        const bool needD = J == 3 && __shfl_sync(0xffffffffu, int(rq.needD), sl) != 0;
+        float3 origin, base, dirD[J];
+        float2 posS = make_float2(0.f, 0.f), gPix = make_float2(0.f, 0.f);
+        float3 gDir = f3(0.f);
+        if constexpr (J == 3) {
+            origin = shfl3(rq.origin, sl);
+            base = shfl3(rq.dir, sl);
+            gDir = shfl3(rq.gDir, sl);
+#pragma unroll
+            for (int j = 0; j < J; j++) dirD[j] = make_float3(j == 0 ? 1.f : 0.f, j == 1 ? 1.f : 0.f, j == 2 ? 1.f : 0.f);
+        } else {
+            posS = make_float2(__shfl_sync(0xffffffffu, rq.posS.x, sl), __shfl_sync(0xffffffffu, rq.posS.y, sl));
+            gPix = make_float2(__shfl_sync(0xffffffffu, rq.gPix.x, sl), __shfl_sync(0xffffffffu, rq.gPix.y, sl));
+            origin = load3(s.camera.posW);
+            base = war_cam_dir(s.camera, posS, Wd, Hd);
+#pragma unroll
+            for (int j = 0; j < J; j++) dirD[j] = war_d_cam_dir(s.camera, posS, Wd, Hd, j);
+        }
+        // Pass 1 (traceAsymptoticWeightedMeanIntersection, WarpedAreaReparam.slang:111-193)
+        // for auxiliary sample k: its sample pair as the sequential pass draws it.
+        if (!anti)
+            for (uint32_t i = 0; i < n; i++) next1D(sg);
+        float2 smp = make_float2(0.f, 0.f);
+        for (uint32_t i = 0; i <= k && i < n; i++) {
+            if (!anti || (i & 1u) == 0) smp = next2D(sg);
+        }
+        WarAux a;
+        a.u = a.c = f3(0.f);
+        a.w = a.tmp1 = a.len = 0.f;
+        a.dW[0] = a.dW[1] = a.dW[2] = 0.f;
+        a.inst = kAuxMiss;
+        a.prim = 0;
+        a.bx = a.by = 0.f;
+        a.clamped = 0;
+        if (act) {
+            const float3 t = perp_stark(base);
+            const float3 Nn = normalize(base);
+            const float3 T = normalize(t - Nn * dot(t, Nn));
+            const float3 B = cross(Nn, T) * 1.f;
+            const float3 dl = sample_von_mises_fisher(smp, kappa);
+            float3 c = normalize(T * dl.x + B * dl.y + Nn * dl.z);
+            if (anti && (k & 1u)) {
+                const float3 ii = -c;
+                c = ii - base * (2.f * dot(base, ii));
+            }
+            a.c = c;
+            a.u = c;
+            float3 nrm = f3(0.f);
+            HitRec h;
+            trace_bvh<false>(s, origin, c, 0.f, FLT_MAX, h, stack, stride);
+            if (h.valid) {
+                const DevInstance inst = s.instances[h.instanceID];
+                const uint32_t* ip = s.indices + inst.ibOffset + h.primIndex * 3;
+                float3 v0, v1, v2, n0, n1, n2;
+                unpack_vertex(load_vertex(s.vertices, __ldg(ip) + inst.vbOffset), v0, n0);
+                unpack_vertex(load_vertex(s.vertices, __ldg(ip + 1) + inst.vbOffset), v1, n1);
+                unpack_vertex(load_vertex(s.vertices, __ldg(ip + 2) + inst.vbOffset), v2, n2);
+                const float b0 = 1.f - h.baryX - h.baryY;
+                const float3 P = v0 * b0 + v1 * h.baryX + v2 * h.baryY;
+                nrm = normalize(n0) * b0 + normalize(n1) * h.baryX + normalize(n2) * h.baryY;
+                const float3 d = P - origin;
+                const float L = length(d);
+                a.u = L > 0.f ? d / L : f3(0.f);
+                a.len = L;
+                a.inst = h.instanceID;
+                a.prim = h.primIndex;
+                a.bx = h.baryX;
+                a.by = h.baryY;
+            }
+            float bt = dot(nrm, c);
+            bt = bt * bt;
+            const float sy = fmaxf(1.f - smp.y, 1e-6f);
+            const float invVMF = 1.f / ((1.f - sy) * fm::exp(-2.f * kappa) + sy);
+            const float wDenom = invVMF - 1.f + bt;
+            const float wDenomRcp = wDenom > 1e-4f ? 1.f / wDenom : 0.f;
+            a.w = wDenomRcp * wDenomRcp * wDenomRcp * invVMF;
+            a.tmp1 = invVMF * a.w * wDenomRcp * kappa * 3.f;
+#pragma unroll
+            for (int j = 0; j < J; j++) {
+                const float3 tmp2 = -cross(base, cross(base, dirD[j]));
+                const float raw = a.tmp1 * dot(tmp2, c);
+                a.dW[j] = fminf(fmaxf(raw, -1e10f), 1e10f);
+                if (!(raw >= -1e10f && raw <= 1e10f)) a.clamped |= 1u << j;
+            }
+        }
+        const float W = group_sum(a.w, G);
+        const float3 MW = group_sum3(a.u * a.w, G);
+        WarMean<J> m;
+        m.pass = W > 1e-8f;
+        m.Wc = m.pass ? W : 1e-8f;
+        m.MW = MW;
+        m.M = MW / m.Wc;
+#pragma unroll
+        for (int j = 0; j < J; j++) {
+            const float Dj = group_sum(a.dW[j], G);
+            const float3 dMWj = group_sum3(a.u * a.dW[j], G);
+            m.D[j] = m.pass ? Dj : 0.f;
+            m.dM[j] = (dMWj * m.Wc - MW * m.D[j]) / (m.Wc * m.Wc);
+        }
+        float3 gM, gdM[J];
+        if constexpr (J == 3) war_ray_phi(m, gDir, gJ, gM, gdM);
+        else war_screen_phi(s.camera, Wd, Hd, m, gPix, gJ, gM, gdM);
+        // Pass 2 (war_aux_backprop) for sample k.
+        float3 lO = f3(0.f), lD = f3(0.f);
+        if (act) {
+            const float inv = 1.f / m.Wc;
+            const float inv2 = inv * inv;
+            const float3 Mp = m.pass ? m.M : f3(0.f);
+            float3 gu = gM * (a.w * inv);
+#pragma unroll
+            for (int j = 0; j < J; j++) gu += gdM[j] * (a.dW[j] * inv - a.w * m.D[j] * inv2);
+            if (a.len > 0.f) {
+                const float3 g = (gu - a.u * dot(a.u, gu)) / a.len;
+                lO -= g;
+                if (p.meshID == kAllMeshes || a.inst == p.meshID) {
+                    const DevInstance inst = s.instances[a.inst];
+                    const uint32_t* ip = s.indices + inst.ibOffset + a.prim * 3;
+                    const float bw[3] = {1.f - a.bx - a.by, a.bx, a.by};
+                    uint32_t off[3];
+#pragma unroll
+                    for (int v = 0; v < 3; v++) {
+                        const uint32_t local = __ldg(ip + v);
+                        off[v] = (p.meshID == kAllMeshes ? inst.vbOffset + local : local) * 3u;
+                    }
+                    add_position_grad(p, rpid, off, bw, g);
+                }
+            }
+            if (needD) {
+                const float dc = dot(base, a.c);
+#pragma unroll
+                for (int j = 0; j < J; j++) {
+                    if (a.clamped & (1u << j)) continue;
+                    const float gdw = dot(gdM[j], (a.u - Mp) * inv) * a.tmp1;
+                    const float cj = j == 0 ? a.c.x : (j == 1 ? a.c.y : a.c.z);
+                    const float dj = j == 0 ? base.x : (j == 1 ? base.y : base.z);
+                    float3 gj = base * (2.f * cj) - a.c * dj;
+                    if (j == 0) gj.x -= dc;
+                    if (j == 1) gj.y -= dc;
+                    if (j == 2) gj.z -= dc;
+                    lD += gj * gdw;
+                }
+            }
+        }
+        lO = group_sum3(lO, G);
+        lD = group_sum3(lD, G);
+        const int from = myGroup >= 0 ? myGroup * int(G) : int(lane);
+        const float3 tO = shfl3(lO, from), tD = shfl3(lD, from);
+        if (myGroup >= 0) {
+            gO += tO;
+            gD += tD;
+        }
+    }
+}
+
 // The camera sample of a WARDiffPathTracer path (tracePaths,
 // WARDiffPathTracer.rt.slang:115-143): the sample generator after the jitter
 // draw and the jittered screen position.
@@ -386,9 +608,13 @@ FPT_D void add_vertex_position_grad(const WarParams& p, uint32_t pid, const WarI
 // adjoint of the next vertex's incident direction V on entry and this
 // vertex's on return; the warped scatter direction is the next vertex's -V
 // and its weight scales thp_{k+1} = thp_k * w_k.
+// With `req`, the scatter reparameterisation is not evaluated here: it is
+// returned as a request for war_coop<3>, with the target of the origin's
+// adjoint in `req_off` / `req_b` (req_pos false: no position gradient wanted).
 template <bool HAS_T, bool WAR>
 FPT_D void war_sweep_vertex(const DevScene& s, const WarParams& p, uint32_t pid, uint32_t hash, const WarSweepVertex& v, float3 g,
-                            float3& A, float3& gVnext, uint2* stack, uint32_t stride) {
+                            float3& A, float3& gVnext, uint2* stack, uint32_t stride, WarCoopReq* req = nullptr,
+                            uint32_t (*req_off)[3] = nullptr, float (*req_b)[3] = nullptr, bool* req_pos = nullptr) {
     constexpr int NJ = WAR ? 17 : 11;
     const bool scattered = (v.flags & 2u) != 0;
     const bool evalGrad = scattered && (A.x != 0.f || A.y != 0.f || A.z != 0.f);
@@ -404,13 +630,15 @@ FPT_D void war_sweep_vertex(const DevScene& s, const WarParams& p, uint32_t pid,
     } else {
         sd.frontFacing = (v.flags & 1u) != 0;
         sd.materialID = v.matID;
+        sd.uv = make_float2(0.f, 0.f);
+        if (evalGrad && material_base_texture(s, v.matID) != ~0u) sd.uv = hit_uv(s, v.inst, v.prim, v.b[1], v.b[2]);
     }
     if (evalGrad) {
-        const MatParams mp = load_mat_params(s, v.matID);
+        const MatParams mp = load_mat_params(s, v.matID, sd.uv);
         const MaterialInstance<HAS_T> mi = material_instance<HAS_T>(s, sd, p.lambert != 0);
         const DV3<NJ> J = eval_jacobian<NJ, HAS_T>(mi, mp, (v.flags & 1u) != 0, v.wiL, v.wsL);
         const float3 Gs = (A * v.thp) / v.pdf;
-        add_material_grads<NJ>(p, pid, hash, v.matID, J, Gs);
+        add_material_grads<NJ>(s, p, pid, hash, v.matID, sd.uv, J, Gs);
         if (needWar || needFrame) {
             const float3 gO = make_float3(Gs.x * J.x.d[11] + Gs.y * J.y.d[11] + Gs.z * J.z.d[11],
                                           Gs.x * J.x.d[12] + Gs.y * J.y.d[12] + Gs.z * J.z.d[12],
@@ -441,9 +669,25 @@ FPT_D void war_sweep_vertex(const DevScene& s, const WarParams& p, uint32_t pid,
             sg.s2 = v.sg.z;
             sg.s3 = v.sg.w;
             const float3 origin = compute_ray_origin(is.posW, sd.frontFacing ? sd.faceN : -sd.faceN);
-            float3 gO = f3(0.f), gD = f3(0.f);
-            war_ray_grad(s, p, pid, origin, v.outDir, false, sg, gdS, gJ, stack, stride, gO, gD);
-            add_vertex_position_grad(p, pid, is, gO);
+            if (req) {
+                req->active = true;
+                req->origin = origin;
+                req->dir = v.outDir;
+                req->sg = v.sg;
+                req->gDir = gdS;
+                req->gJ = gJ;
+                req->needD = false;
+                *req_pos = war_wants_pos(p) && war_pos_target(p.meshID, is);
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    (*req_off)[q] = war_pos_index(p.meshID, is, q);
+                    (*req_b)[q] = is.b[q];
+                }
+            } else {
+                float3 gO = f3(0.f), gD = f3(0.f);
+                war_ray_grad(s, p, pid, origin, v.outDir, false, sg, gdS, gJ, stack, stride, gO, gD);
+                add_vertex_position_grad(p, pid, is, gO);
+            }
         }
     }
     gVnext = gV;
@@ -455,7 +699,8 @@ FPT_D void war_sweep_vertex(const DevScene& s, const WarParams& p, uint32_t pid,
 // V0 = -direction, and the throughput starts at detJ * w / detach(w) for the
 // Gaussian pixel filter w.  A is the adjoint of the primary throughput, gV0
 // the adjoint of V0.
-FPT_D void war_sweep_screen(const DevScene& s, const WarParams& p, uint32_t pid, float3 A, float3 gV0, uint2* stack, uint32_t stride) {
+FPT_D void war_sweep_screen(const DevScene& s, const WarParams& p, uint32_t pid, float3 A, float3 gV0, uint2* stack, uint32_t stride,
+                             WarCoopReq* req = nullptr) {
     const uint32_t x = pid % p.width, y = pid / p.width;
     UniformSG sg;
     const float2 pix = war_camera_sample(p, x, y, sg);
@@ -465,7 +710,18 @@ FPT_D void war_sweep_screen(const DevScene& s, const WarParams& p, uint32_t pid,
     // d ln w / d sample = -(sample - centre) / sigma^2 with sigma = 0.5.
     const float2 gPix = make_float2(dot(gRay, war_d_cam_dir(s.camera, pix, Wd, Hd, 0)) - 4.f * gs * (pix.x - (float(x) + 0.5f)),
                                     dot(gRay, war_d_cam_dir(s.camera, pix, Wd, Hd, 1)) - 4.f * gs * (pix.y - (float(y) + 0.5f)));
-    if (gPix.x != 0.f || gPix.y != 0.f || gs != 0.f) war_screen_grad(s, p, pid, pix, sg, gPix, gs, stack, stride);
+    if (gPix.x != 0.f || gPix.y != 0.f || gs != 0.f) {
+        if (req) {
+            req->active = true;
+            req->posS = pix;
+            req->sg = make_uint4(sg.s0, sg.s1, sg.s2, sg.s3);
+            req->gPix = gPix;
+            req->gJ = gs;
+            req->needD = false;
+        } else {
+            war_screen_grad(s, p, pid, pix, sg, gPix, gs, stack, stride);
+        }
+    }
 }
 
 }  // namespace

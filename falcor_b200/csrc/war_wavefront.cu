@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_shade(DevSc
                             bool frameGrad = false;
                             const float3 wiL = mi.toLocal(sd.V), woL = mi.toLocal(wo);
                             if (mi.valid_hemisphere(sd, wiL, woL, wo)) {
-                                const MatParams mp = load_mat_params(s, sd.materialID);
+                                const MatParams mp = load_mat_params(s, sd.materialID, sd.uv);
                                 const DV3<NJ> J = eval_jacobian<NJ, HAS_T>(mi, mp, sd.frontFacing, wiL, woL);
                                 const float3 Gf = ((g * thp) * Li) * mis;
 #pragma unroll
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_shade(DevSc
                             nee_at(ww, 3, i) = make_float4(dP.x, dP.y, dP.z, __uint_as_float(posGrad ? 1u : 0u));
                             nee_at(ww, 4, i) = make_float4(is.b[0], is.b[1], is.b[2], __uint_as_float(war_pos_index(p.meshID, is, 0)));
                             nee_at(ww, 5, i) = make_float4(__uint_as_float(war_pos_index(p.meshID, is, 1)),
-                                                           __uint_as_float(war_pos_index(p.meshID, is, 2)), 0.f, 0.f);
+                                                           __uint_as_float(war_pos_index(p.meshID, is, 2)), sd.uv.x, sd.uv.y);
                             nee_at(ww, 6, i) = make_float4(weight.x, weight.y, weight.z, 0.f);
                             if (WAR) {
                                 // computeNEE's reparameterizeRay: origin computeRayOrigin(posW, +-faceN),
@@ -328,48 +328,74 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_nee_grad(De
     __shared__ uint2 stackMem[WAR ? kStackSize * kShadeBlock : 1];
     uint2* stack = stackMem + threadIdx.x;
     const uint32_t n = wp.counts[2];
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t i = wp.shadowQueue[k];
-        if (w.sLr[i].w != 1.f) continue;
-        const uint32_t pid = wp.waveFirstPixel + i;
-        const float4 a = nee_at(ww, 0, i), b = nee_at(ww, 1, i), c = nee_at(ww, 2, i);
-        const float G[11] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z};
-        const uint32_t matID = __float_as_uint(c.w);
-        add_material_grad_values(p, pid, war_hash(pid, p.matHash), matID, G);
-        const float4 d = nee_at(ww, 3, i);
-        float3 dP = xyz(d);
-        const uint32_t vk = ww.nv[i] - 1;
-        const float4 bb = nee_at(ww, 4, i), ll = nee_at(ww, 5, i);
-        const float bw[3] = {bb.x, bb.y, bb.z};
-        const uint32_t loc[3] = {__float_as_uint(bb.w), __float_as_uint(ll.x), __float_as_uint(ll.y)};  // gradient offsets
-        if (WAR) {
-            const float4 o7 = nee_at(ww, 7, i), o8 = nee_at(ww, 8, i), o9 = nee_at(ww, 9, i);
-            const float3 gdN = xyz(o9);
-            const float gRatio = o8.w;  // also the adjoint of the reparameterisation weight
-            const float4 fn = nee_at(ww, 12, i);
-            if (__float_as_uint(fn.w)) add_frame_grad(p, pid, loc, bw, xyz(fn), xyz(nee_at(ww, 13, i)));
-            if (p.useWAR && war_wants_pos(p) && (nonzero(gdN) || gRatio != 0.f)) {
-                UniformSG sg;
-                load_sg(as_u4(nee_at(ww, 10, i)), sg);
-                const float3 wo = xyz(o8);
-                float3 gO = f3(0.f), gD = f3(0.f);
-                war_ray_grad(s, p, pid, xyz(o7), wo, true, sg, gdN, gRatio, stack, kShadeBlock, gO, gD);
-                // The origin follows posW (computeRayOrigin passes its derivative
-                // through); the unwarped direction is (P_light - posW) / dist.
-                dP += gO - (gD - wo * dot(wo, gD)) * (1.f / o7.w);
-            }
-            const float4 gv = nee_at(ww, 11, i);
-            float4& r8 = rec_at(ww, vk, 8, i);
-            r8.x += gv.x;
-            r8.y += gv.y;
-            r8.z += gv.z;
+    // Warp-uniform trip count: with WAR the reparameterisations of the warp's
+    // samples are served together (war_coop), which needs converged warps.
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x - lane; k0 < n; k0 += gridDim.x * blockDim.x) {
+        const uint32_t k = k0 + lane;
+        uint32_t i = 0, pid = 0;
+        bool live = false;
+        if (k < n) {
+            i = wp.shadowQueue[k];
+            live = w.sLr[i].w == 1.f;
+            pid = wp.waveFirstPixel + i;
         }
-        if (__float_as_uint(d.w)) add_position_grad(p, pid, loc, bw, dP);
-        const float4 wt = nee_at(ww, 6, i);
-        float4& e = rec_at(ww, vk, 4, i);
-        e.x += wt.x;
-        e.y += wt.y;
-        e.z += wt.z;
+        WarCoopReq rq;
+        rq.active = false;
+        float3 dP = f3(0.f), wo = f3(0.f);
+        float invDist = 0.f;
+        bool posGrad = false;
+        uint32_t loc[3] = {0, 0, 0};
+        float bw[3] = {0.f, 0.f, 0.f};
+        if (live) {
+            const float4 a = nee_at(ww, 0, i), b = nee_at(ww, 1, i), c = nee_at(ww, 2, i);
+            const float G[11] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z};
+            const uint32_t matID = __float_as_uint(c.w);
+            const float4 bb = nee_at(ww, 4, i), ll = nee_at(ww, 5, i);
+            add_material_grad_values(s, p, pid, war_hash(pid, p.matHash), matID, make_float2(ll.z, ll.w), G);
+            const float4 d = nee_at(ww, 3, i);
+            dP = xyz(d);
+            posGrad = __float_as_uint(d.w) != 0;
+            const uint32_t vk = ww.nv[i] - 1;
+            bw[0] = bb.x; bw[1] = bb.y; bw[2] = bb.z;
+            loc[0] = __float_as_uint(bb.w); loc[1] = __float_as_uint(ll.x); loc[2] = __float_as_uint(ll.y);  // gradient offsets
+            if (WAR) {
+                const float4 o7 = nee_at(ww, 7, i), o8 = nee_at(ww, 8, i), o9 = nee_at(ww, 9, i);
+                const float3 gdN = xyz(o9);
+                const float gRatio = o8.w;  // also the adjoint of the reparameterisation weight
+                const float4 fn = nee_at(ww, 12, i);
+                if (__float_as_uint(fn.w)) add_frame_grad(p, pid, loc, bw, xyz(fn), xyz(nee_at(ww, 13, i)));
+                if (p.useWAR && war_wants_pos(p) && (nonzero(gdN) || gRatio != 0.f)) {
+                    wo = xyz(o8);
+                    invDist = 1.f / o7.w;
+                    rq.active = true;
+                    rq.origin = xyz(o7);
+                    rq.dir = wo;
+                    rq.sg = as_u4(nee_at(ww, 10, i));
+                    rq.gDir = gdN;
+                    rq.gJ = gRatio;
+                    rq.needD = true;
+                }
+                const float4 gv = nee_at(ww, 11, i);
+                float4& r8 = rec_at(ww, vk, 8, i);
+                r8.x += gv.x;
+                r8.y += gv.y;
+                r8.z += gv.z;
+            }
+            const float4 wt = nee_at(ww, 6, i);
+            float4& e = rec_at(ww, vk, 4, i);
+            e.x += wt.x;
+            e.y += wt.y;
+            e.z += wt.z;
+        }
+        if (WAR) {
+            float3 gO = f3(0.f), gD = f3(0.f);
+            war_coop<3>(s, p, pid, rq, stack, kShadeBlock, gO, gD);
+            // The origin follows posW (computeRayOrigin passes its derivative
+            // through); the unwarped direction is (P_light - posW) / dist.
+            if (rq.active) dP += gO - (gD - wo * dot(wo, gD)) * invDist;
+        }
+        if (live && posGrad) add_position_grad(p, pid, loc, bw, dP);
     }
 }
 
@@ -379,38 +405,63 @@ template <bool HAS_T, bool WAR>
 __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_sweep(DevScene s, WarParams p, WaveParams wp, WarWave ww) {
     __shared__ uint2 stackMem[WAR ? kStackSize * kShadeBlock : 1];
     uint2* stack = stackMem + threadIdx.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePixels; i += gridDim.x * blockDim.x) {
-        const uint32_t pid = wp.waveFirstPixel + i;
-        const float3 g = war_dLdI(p, pid);
+    // Warp-uniform trip counts (paths and vertices): the scatter and screen
+    // reparameterisations of the warp's paths are served together (war_coop).
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x - lane; i0 < wp.wavePixels; i0 += gridDim.x * blockDim.x) {
+        const uint32_t i = i0 + lane;
+        const bool valid = i < wp.wavePixels;
+        const uint32_t pid = wp.waveFirstPixel + (valid ? i : 0u);
+        const float3 g = valid ? war_dLdI(p, pid) : f3(0.f);
         const uint32_t hash = war_hash(pid, p.matHash);
         float3 A = f3(0.f), gV = f3(0.f);
-        const int nv = int(ww.nv[i]);
-        for (int k = nv - 1; k >= 0; k--) {
-            const float4 r0 = rec_at(ww, k, 0, i), r1 = rec_at(ww, k, 1, i), r2 = rec_at(ww, k, 2, i);
-            WarSweepVertex v;
-            v.wiL = xyz(r0);
-            v.pdf = r0.w;
-            v.wsL = xyz(r1);
-            v.matID = __float_as_uint(r1.w);
-            v.thp = xyz(r2);
-            v.flags = __float_as_uint(r2.w);
-            v.bw = xyz(rec_at(ww, k, 3, i));
-            v.e = xyz(rec_at(ww, k, 4, i));
-            if (WAR) {
-                const float4 r5 = rec_at(ww, k, 5, i), r6 = rec_at(ww, k, 6, i), r8 = rec_at(ww, k, 8, i), r9 = rec_at(ww, k, 9, i);
-                v.inDir = xyz(r5);
-                v.inst = __float_as_uint(r5.w);
-                v.outDir = xyz(r6);
-                v.prim = __float_as_uint(r6.w);
-                v.sg = as_u4(rec_at(ww, k, 7, i));
-                v.gV = xyz(r8);
-                v.b[0] = r8.w;
-                v.b[1] = r9.x;
-                v.b[2] = r9.y;
+        const int nv = valid ? int(ww.nv[i]) : 0;
+        const int maxNv = WAR ? __reduce_max_sync(0xffffffffu, uint32_t(nv)) : nv;
+        for (int k = maxNv - 1; k >= 0; k--) {
+            WarCoopReq rq;
+            rq.active = false;
+            uint32_t off[3] = {0, 0, 0};
+            float bwt[3] = {0.f, 0.f, 0.f};
+            bool posT = false;
+            if (k < nv) {
+                const float4 r0 = rec_at(ww, k, 0, i), r1 = rec_at(ww, k, 1, i), r2 = rec_at(ww, k, 2, i);
+                WarSweepVertex v;
+                v.wiL = xyz(r0);
+                v.pdf = r0.w;
+                v.wsL = xyz(r1);
+                v.matID = __float_as_uint(r1.w);
+                v.thp = xyz(r2);
+                v.flags = __float_as_uint(r2.w);
+                v.bw = xyz(rec_at(ww, k, 3, i));
+                v.e = xyz(rec_at(ww, k, 4, i));
+                if (WAR) {
+                    const float4 r5 = rec_at(ww, k, 5, i), r6 = rec_at(ww, k, 6, i), r8 = rec_at(ww, k, 8, i), r9 = rec_at(ww, k, 9, i);
+                    v.inDir = xyz(r5);
+                    v.inst = __float_as_uint(r5.w);
+                    v.outDir = xyz(r6);
+                    v.prim = __float_as_uint(r6.w);
+                    v.sg = as_u4(rec_at(ww, k, 7, i));
+                    v.gV = xyz(r8);
+                    v.b[0] = r8.w;
+                    v.b[1] = r9.x;
+                    v.b[2] = r9.y;
+                }
+                war_sweep_vertex<HAS_T, WAR>(s, p, pid, hash, v, g, A, gV, stack, kShadeBlock, WAR ? &rq : nullptr, &off, &bwt,
+                                             &posT);
             }
-            war_sweep_vertex<HAS_T, WAR>(s, p, pid, hash, v, g, A, gV, stack, kShadeBlock);
+            if (WAR) {
+                float3 gO = f3(0.f), gD = f3(0.f);
+                war_coop<3>(s, p, pid, rq, stack, kShadeBlock, gO, gD);
+                if (rq.active && posT) add_position_grad(p, pid, off, bwt, gO);
+            }
         }
-        if (WAR && p.useWAR && war_wants_pos(p) && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kShadeBlock);
+        if (WAR) {
+            WarCoopReq rq;
+            rq.active = false;
+            if (valid && p.useWAR && war_wants_pos(p) && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kShadeBlock, &rq);
+            float3 gO = f3(0.f), gD = f3(0.f);
+            war_coop<2>(s, p, pid, rq, stack, kShadeBlock, gO, gD);
+        }
     }
 }
 

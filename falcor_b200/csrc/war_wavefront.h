@@ -23,6 +23,8 @@ struct WarParams {
     uint32_t nrmDim, nrmHash;
     float* gradTan;              // [hash][tanDim] vertex tangents of the mesh (MeshTangent)
     uint32_t tanDim, tanHash;
+    float* gradTex;              // [texDim] base-colour texels, 3 floats each (no hashing)
+    uint32_t texDim;
     unsigned long long* counters;  // [0] paths, [1] rays
     // Warped-area reparameterisation (adjoint with position gradients only).
     uint32_t useWAR, auxCount;

@@ -167,10 +167,10 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                                     e += weight;
                                     const float3 wiL = mi.toLocal(sd.V), woL = mi.toLocal(wo);
                                     if (mi.valid_hemisphere(sd, wiL, woL, wo)) {
-                                        const MatParams mp = load_mat_params(s, sd.materialID);
+                                        const MatParams mp = load_mat_params(s, sd.materialID, sd.uv);
                                         const DV3<NJ> J = eval_jacobian<NJ, HAS_T>(mi, mp, sd.frontFacing, wiL, woL);
                                         const float3 Gf = ((g * thp) * Li) * mis;
-                                        add_material_grads<NJ>(p, pid, hash, sd.materialID, J, Gf);
+                                        add_material_grads<NJ>(s, p, pid, hash, sd.materialID, sd.uv, J, Gf);
                                         if (war_wants_pos(p) || (WAR && war_wants_frame(p))) {
                                             // Through wo = (L - P) / |L - P| and the ratio a2s / detach(a2s).
                                             const float3 gL = make_float3(Gf.x * J.x.d[11] + Gf.y * J.y.d[11] + Gf.z * J.z.d[11],
@@ -590,6 +590,8 @@ fpt_status wardiff_execute(fpt_pass& pass, const fpt_frame_io* io, const float* 
             p.nrmDim = grads->mesh_normal ? grads->normal_dim : 0;
             p.gradTan = grads->mesh_tangent;
             p.tanDim = grads->mesh_tangent ? grads->tangent_dim : 0;
+            p.gradTex = grads->base_color_texture;
+            p.texDim = grads->base_color_texture ? grads->texture_dim : 0;
         } else {
             if (!pass.dLdI) return set_error(FPT_ERR_INVALID_ARG, "WARDiffPathTracer: dL_dI is not set (fpt_pass_set_dLdI)");
             if (!pass.sceneGradients)

@@ -232,20 +232,91 @@ class DiffRenderer:
         self.pt.execute({"color": self.color})
         return self.color[..., :3].clone()
 
-    def gradients(self, grad_img, frame_seed: int, position_dim: int = 0, normal_dim: int = 0, tangent_dim: int = 0):
+    def set_texture(self, index: int, rgb) -> None:
+        """Writes linear rgb values [H, W, 3] (CUDA float tensor) into texture
+        `index` in its own format: RGBA32Float as is, RGBA8 UNORM rounded,
+        RGBA8 sRGB encoded (IEC 61966-2-1) and rounded, values clamped to
+        [0, 1] for the 8-bit formats; alpha 1."""
+        self.scene.set_texture_device(index, encode_texture(rgb, self.scene.host.desc.textures[index].format))
+
+    def gradients(self, grad_img, frame_seed: int, position_dim: int = 0, normal_dim: int = 0, tangent_dim: int = 0,
+                  texture: bool = False):
         """Material gradients and, with position_dim / normal_dim / tangent_dim
         > 0, the gradients of the optimised mesh's vertex positions / normals /
         tangents (3 floats per vertex; normals and tangents are kept in
-        ``normal_grad`` / ``tangent_grad``)."""
+        ``normal_grad`` / ``tangent_grad``); with texture=True the gradients of
+        the base-colour texels' linear rgb (3 floats per texel of every texture,
+        kept in ``texture_grad``)."""
         import torch
         self.pt.set_properties({"fixedSeed": int(frame_seed)})
         gm = torch.zeros(self.material_count * 20, dtype=torch.float32, device="cuda")
         gp = torch.zeros(max(position_dim, 1), dtype=torch.float32, device="cuda") if position_dim else None
         gn = torch.zeros(normal_dim, dtype=torch.float32, device="cuda") if normal_dim else None
         gt = torch.zeros(tangent_dim, dtype=torch.float32, device="cuda") if tangent_dim else None
+        gx = torch.zeros(3 * self.scene.texel_count, dtype=torch.float32, device="cuda") if texture else None
         dLdI = grad_img[..., :3].contiguous().float()
-        self.pt.backward({"color": self.color}, dLdI, material_grad=gm, position_grad=gp, normal_grad=gn, tangent_grad=gt)
+        self.pt.backward({"color": self.color}, dLdI, material_grad=gm, position_grad=gp, normal_grad=gn, tangent_grad=gt,
+                         texture_grad=gx)
         self.position_grad = gp
         self.normal_grad = gn
         self.tangent_grad = gt
+        self.texture_grad = gx
         return gm, gp
+
+    def texture_slice(self, flat, index: int):
+        """The [H, W, 3] part of a flat texel-gradient buffer that belongs to texture `index`."""
+        d = self.scene.host.desc
+        base = sum(d.textures[i].width * d.textures[i].height for i in range(index))
+        w, h = d.textures[index].width, d.textures[index].height
+        return flat[3 * base:3 * (base + w * h)].view(h, w, 3)
+
+
+def encode_texture(rgb, fmt: int):
+    """Linear rgb [H, W, 3] (CUDA float) to the texels of a texture format
+    (fpt_texture_format): float32 RGBA for RGBA32Float, uint8 RGBA otherwise."""
+    import torch
+    x = rgb.detach().float()
+    h, w = x.shape[0], x.shape[1]
+    one = torch.ones((h, w, 1), dtype=torch.float32, device=x.device)
+    if fmt == _ffi.TEXTURE_RGBA32_FLOAT:
+        return torch.cat([x, one], dim=2).contiguous()
+    x = x.clamp(0.0, 1.0)
+    if fmt == _ffi.TEXTURE_RGBA8_UNORM_SRGB:
+        x = torch.where(x <= 0.0031308, 12.92 * x, 1.055 * x.clamp_min(1e-12) ** (1.0 / 2.4) - 0.055)
+    q = torch.round(torch.cat([x, one], dim=2) * 255.0).clamp(0, 255).to(torch.uint8)
+    return q.contiguous()
+
+
+def _texture_autograd():
+    import torch
+
+    class TextureDiffRender(torch.autograd.Function):
+        """image = render(texture) for the linear rgb [H, W, 3] of base-colour
+        texture `index`: forward writes it into the texture (encoded in the
+        texture's format, so that an 8-bit texture's gradient passes straight
+        through its quantisation) and renders the primal; backward runs the
+        adjoint of the same frame and returns the texels' gradients.  The
+        reference samples textures no_diff (StandardMaterial.slang:164), so
+        this has no reference counterpart."""
+
+        @staticmethod
+        def forward(ctx, rgb, renderer, frame_seed, index):
+            renderer.set_texture(index, rgb)
+            img = renderer.render(frame_seed)
+            ctx.renderer = renderer
+            ctx.frame_seed = frame_seed
+            ctx.index = index
+            return img
+
+        @staticmethod
+        def backward(ctx, grad_img):
+            ctx.renderer.gradients(grad_img, ctx.frame_seed, texture=True)
+            return ctx.renderer.texture_slice(ctx.renderer.texture_grad, ctx.index), None, None, None
+
+    return TextureDiffRender
+
+
+def texture_diff_render(rgb, renderer, frame_seed: int, index: int = 0):
+    """Differentiable render with base-colour texture `index` as the input (see
+    ``TextureDiffRender``)."""
+    return _texture_autograd().apply(rgb, renderer, frame_seed, index)

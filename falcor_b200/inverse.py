@@ -27,11 +27,16 @@ Displacements change visibility (self-occlusion, shadows), so their gradient
 needs the warped-area boundary term (``use_war``, the pass's default): on a
 test grid the interior term alone gave a directional derivative of -0.007
 towards the target displacement where finite differences gave -0.25.
-Textures are not part of the material model (the reference's StandardMaterial
-does not differentiate them either), so the colour parameters are per material.
+The colour parameters are per material, and optionally (``texture_index``) an
+albedo texture of the grid: its texels' linear rgb are optimised and written
+back into the scene's texture (an RGBA8 sRGB texture is re-encoded after every
+step, its gradient passing straight through the quantisation).  The reference
+samples textures no_diff (StandardMaterial.slang:164), so texture gradients are
+this library's extension.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 
 import numpy as np
@@ -42,10 +47,27 @@ from .replicas import shard, sharded_sum
 from .scene import HostScene, Scene
 
 
-def displaced_grid_scene(res: int = 224, extent: float = 2.0, aspect: float = 1.0, base_color=(0.6, 0.55, 0.5)) -> HostScene:
+def srgb_encode8(rgb: np.ndarray) -> np.ndarray:
+    """Linear rgb in [0, 1] to 8-bit sRGB codes (IEC 61966-2-1)."""
+    x = np.clip(np.asarray(rgb, dtype=np.float64), 0.0, 1.0)
+    e = np.where(x <= 0.0031308, 12.92 * x, 1.055 * np.power(x, 1.0 / 2.4) - 0.055)
+    return np.clip(np.rint(e * 255.0), 0, 255).astype(np.uint8)
+
+
+def srgb_decode8(codes: np.ndarray) -> np.ndarray:
+    """8-bit sRGB codes to linear rgb (float32)."""
+    c = np.asarray(codes, dtype=np.float64) / 255.0
+    return np.where(c <= 0.04045, c / 12.92, np.power((c + 0.055) / 1.055, 2.4)).astype(np.float32)
+
+
+def displaced_grid_scene(res: int = 224, extent: float = 2.0, aspect: float = 1.0, base_color=(0.6, 0.55, 0.5),
+                         texture: tuple[int, int] | None = None) -> HostScene:
     """One flat res x res grid mesh in the xz plane ((res+1)^2 vertices, 2 res^2
     triangles; res = 224 gives 100 352 triangles), an emissive quad above it and
-    a small constant sky.  Material 0 is the grid's, material 1 the light's."""
+    a small constant sky.  Material 0 is the grid's, material 1 the light's.
+    texture=(width, height): the grid's base colour comes from an RGBA8 sRGB
+    albedo texture of that size (texture 0) holding base_color, mapped once
+    over the grid."""
     n = res + 1
     xs = (np.arange(n, dtype=np.float64) / res - 0.5) * extent
     X, Z = np.meshgrid(xs, xs, indexing="xy")
@@ -85,7 +107,14 @@ def displaced_grid_scene(res: int = 224, extent: float = 2.0, aspect: float = 1.
     sky = np.full((8, 16, 3), 0.3, np.float32)
     cam = {"position": [0.0, 1.2, 2.2], "target": [0.0, 0.0, 0.0], "up": [0.0, 1.0, 0.0], "focal_length": 35.0,
            "frame_height": 24.0, "aspect_ratio": float(aspect), "near_z": 0.01, "far_z": 100.0, "focal_distance": 10000.0}
-    return HostScene.from_arrays(verts, indices, instances, mats, cam, {"rgb": sky, "intensity": 1.0})
+    if texture is None:
+        return HostScene.from_arrays(verts, indices, instances, mats, cam, {"rgb": sky, "intensity": 1.0})
+    tw, th = texture
+    tex = np.zeros((th, tw, 4), np.uint8)
+    tex[..., 0:3] = srgb_encode8(base_color)
+    tex[..., 3] = 255
+    return HostScene.from_arrays(verts, indices, instances, mats, cam, {"rgb": sky, "intensity": 1.0}, textures=[tex],
+                                 base_color_textures=[0, -1])
 
 
 def orbit_cameras(count: int, radius: float = 2.3, height: float = 1.3, aspect: float = 1.0) -> list[dict]:
@@ -116,7 +145,8 @@ class InverseLoop:
 
     def __init__(self, scene: Scene, mesh_id: int, views: list[dict], width: int, height: int, spp: int = 8,
                  max_bounces: int = 4, adjoint_mode: str = "Replay", lr: float = 1e-2, use_war: bool = True,
-                 smoothing: float = 20.0, fresh_seeds: bool = True, optimize=("displacement", "color")):
+                 smoothing: float = 20.0, fresh_seeds: bool = True, optimize=("displacement", "color"),
+                 texture_index: int | None = None):
         import torch
         self.scene = scene
         self.mesh_id = mesh_id
@@ -150,7 +180,23 @@ class InverseLoop:
         self.u = torch.zeros(self.nv, dtype=torch.float32, device="cuda", requires_grad=True)
         self.gu = torch.zeros(self.nv, dtype=torch.float32, device="cuda")
         self.color = self.params[:, 0:3].clone().requires_grad_(True)
-        self.opt = torch.optim.Adam([self.u, self.color], lr=lr)
+        # An albedo texture as linear rgb [H, W, 3], written into the scene's
+        # texture in its own format after every step.
+        self.texture_index = texture_index
+        self.texture = None
+        opt_params = [self.u, self.color]
+        if texture_index is not None:
+            td = scene.host.desc.textures[texture_index]
+            host_texels = np.ctypeslib.as_array(C.cast(td.texels, C.POINTER(C.c_uint8)), shape=(td.height, td.width, 4))
+            if td.format == _ffi.TEXTURE_RGBA32_FLOAT:
+                lin = np.ctypeslib.as_array(C.cast(td.texels, C.POINTER(C.c_float)), shape=(td.height, td.width, 4))[..., :3]
+            elif td.format == _ffi.TEXTURE_RGBA8_UNORM_SRGB:
+                lin = srgb_decode8(host_texels[..., :3])
+            else:
+                lin = host_texels[..., :3].astype(np.float32) / 255.0
+            self.texture = torch.from_numpy(np.ascontiguousarray(lin, dtype=np.float32)).cuda().requires_grad_(True)
+            opt_params.append(self.texture)
+        self.opt = torch.optim.Adam(opt_params, lr=lr)
         self.targets = None
         self.iteration = 0
         # fresh_seeds: new sample seeds every iteration (unbiased over the loop);
@@ -197,10 +243,12 @@ class InverseLoop:
             n.index_add_(0, self.tri[:, k], fn)
         return n / n.norm(dim=1, keepdim=True).clamp_min(1e-20)
 
-    def apply(self, disp, color) -> None:
-        """Writes displaced positions (with recomputed normals and tangents) and
-        base colours into the scene."""
+    def apply(self, disp, color, texture=None) -> None:
+        """Writes displaced positions (with recomputed normals and tangents),
+        base colours and, if given, the albedo texture into the scene."""
         import torch
+        if texture is not None and self.texture_index is not None:
+            self.renderer.set_texture(self.texture_index, texture.detach().clamp(0.0, 1.0))
         with torch.no_grad():
             p = (self.p0 + disp[:, None] * self.n0).contiguous()
             n = self._normals(p)
@@ -212,12 +260,12 @@ class InverseLoop:
             prm[~self.emissive, 0:3] = color[~self.emissive].clamp(0.0, 1.0)
             self.renderer.set_material_params(prm)
 
-    def render_targets(self, disp_target, color_target, spp: int | None = None) -> list:
+    def render_targets(self, disp_target, color_target, spp: int | None = None, texture_target=None) -> dict:
         """Renders the target views with the given parameters (then restores the
         current ones), at `spp` samples per pixel if given.  With fresh seeds the
         targets use seeds of their own; otherwise view v uses seed v.  Returns
         {view index: image} for the views of this rank (all views on one GPU)."""
-        self.apply(disp_target, color_target)
+        self.apply(disp_target, color_target, texture_target)
         if spp:
             self.renderer.pt.set_properties({"samplesPerPixel": int(spp)})
         out = {}
@@ -228,7 +276,7 @@ class InverseLoop:
         if spp:
             self.renderer.pt.set_properties({"samplesPerPixel": int(self.spp)})
         self.targets = out
-        self.apply(self.disp.detach(), self.color.detach())
+        self.apply(self.disp.detach(), self.color.detach(), self.texture)
         return out
 
     def gradients(self):
@@ -245,13 +293,21 @@ class InverseLoop:
             diff = img - self.targets[v]
             loss = (diff * diff).mean().reshape(1)
             dLdI = (2.0 / diff.numel()) * diff
-            gm, gpv = self.renderer.gradients(dLdI, seed, position_dim=3 * self.nv, normal_dim=3 * self.nv)
-            return (loss, gpv.view(self.nv, 3).clone(), self.renderer.normal_grad.view(self.nv, 3).clone(),
-                    gm.view(-1, 20)[:, 0:3].clone())
+            tex = self.texture is not None
+            gm, gpv = self.renderer.gradients(dLdI, seed, position_dim=3 * self.nv, normal_dim=3 * self.nv, texture=tex)
+            out = (loss, gpv.view(self.nv, 3).clone(), self.renderer.normal_grad.view(self.nv, 3).clone(),
+                   gm.view(-1, 20)[:, 0:3].clone())
+            if tex:
+                out += (self.renderer.texture_slice(self.renderer.texture_grad, self.texture_index).clone(),)
+            return out
 
         zeros = (torch.zeros(1, device="cuda"), torch.zeros((self.nv, 3), device="cuda"),
                  torch.zeros((self.nv, 3), device="cuda"), torch.zeros_like(self.color))
-        loss_t, gp, gn, gc = sharded_sum(self.views, view, like=zeros)
+        if self.texture is not None:
+            zeros += (torch.zeros_like(self.texture),)
+        sums = sharded_sum(self.views, view, like=zeros)
+        loss_t, gp, gn, gc = sums[:4]
+        self.texture_grad = sums[4] if self.texture is not None else None
         loss = float(loss_t.item())
         # Chain rule through p = p0 + d n0 and n(p).
         with torch.enable_grad():
@@ -270,9 +326,13 @@ class InverseLoop:
         self.opt.zero_grad(set_to_none=False)
         self.u.grad = self.gu.clone() if "displacement" in self.optimize else torch.zeros_like(self.gu)
         self.color.grad = gc if "color" in self.optimize else torch.zeros_like(gc)
+        if self.texture is not None:
+            self.texture.grad = self.texture_grad if "texture" in self.optimize else torch.zeros_like(self.texture)
         self.opt.step()
         with torch.no_grad():
             self.disp = self._solve(self.u.detach(), self.disp)
-        self.apply(self.disp, self.color.detach())
+            if self.texture is not None:
+                self.texture.clamp_(0.0, 1.0)
+        self.apply(self.disp, self.color.detach(), self.texture)
         self.iteration += 1
         return loss

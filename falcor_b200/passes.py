@@ -278,10 +278,11 @@ class WARDiffPathTracer(RenderPass):
         check(lib().fpt_pass_set_diff_debug_params(self._h, t, int(id[0]), int(id[1]), int(offset), g))
 
     def backward(self, render_data: Mapping[str, Any], dLdI, material_grad=None, position_grad=None, frame: int = 0,
-                 normal_grad=None, tangent_grad=None) -> None:
+                 normal_grad=None, tangent_grad=None, texture_grad=None) -> None:
         """Adjoint of one frame into flat gradient tensors (fpt_pass_backward):
-        material parameters, and the positions, normals and tangents of the
-        vertices of meshToOptimize."""
+        material parameters, the positions, normals and tangents of the
+        vertices of meshToOptimize, and the texels of the base-colour textures
+        (3 floats per texel, textures in scene order)."""
         some = next((t for t in render_data.values() if t is not None), dLdI)
         height, width = int(some.shape[0]), int(some.shape[1])
         io = self._io(render_data, width, height, frame)
@@ -294,6 +295,8 @@ class WARDiffPathTracer(RenderPass):
         g.mesh_tangent = _ptr(tangent_grad)
         g.normal_dim = normal_grad.numel() if normal_grad is not None else 0
         g.tangent_dim = tangent_grad.numel() if tangent_grad is not None else 0
+        g.base_color_texture = _ptr(texture_grad)
+        g.texture_dim = texture_grad.numel() if texture_grad is not None else 0
         check(lib().fpt_pass_backward(self._h, C.byref(io), C.c_void_p(_ptr(dLdI)), C.byref(g), C.c_void_p(_stream())))
 
 

@@ -250,7 +250,9 @@ void makeDescFromScene(RenderContext* pRenderContext, const ref<Device>& pDevice
 class FptRenderPass : public RenderPass {
 public:
     FptRenderPass(ref<Device> pDevice, const Properties& props, const char* type, ChannelList inputs, ChannelList outputs)
-        : RenderPass(pDevice), mInputs(std::move(inputs)), mOutputs(std::move(outputs)) {
+        : RenderPass(pDevice), mType(type), mInputs(std::move(inputs)), mOutputs(std::move(outputs)) {
+        // The type name is kept here: the constructor runs before the derived
+        // class exists, so it must not reach mType (a virtual call).
         check(fpt_pass_create(type, &mpPass), std::string("fpt_pass_create(") + type + ")");
         if (cudaStreamCreateWithFlags(&mStream, cudaStreamNonBlocking) != cudaSuccess) FALCOR_THROW("cudaStreamCreate failed");
         setProperties(props);
@@ -264,11 +266,11 @@ public:
     }
 
     void setProperties(const Properties& props) override {
-        check(fpt_pass_set_properties_json(mpPass, props.dump().c_str()), getType() + "::setProperties");
+        check(fpt_pass_set_properties_json(mpPass, props.dump().c_str()), mType + "::setProperties");
     }
     Properties getProperties() const override {
         std::vector<char> buf(1 << 16);
-        check(fpt_pass_get_properties_json(mpPass, buf.data(), buf.size()), getType() + "::getProperties");
+        check(fpt_pass_get_properties_json(mpPass, buf.data(), buf.size()), mType + "::getProperties");
         return Properties(Properties::json::parse(buf.data()));
     }
     RenderPassReflection reflect(const CompileData& compileData) override {
@@ -287,7 +289,7 @@ public:
         SceneArrays arrays;
         makeDescFromScene(pRenderContext, mpDevice, pScene, arrays);
         check(fpt_scene_create(&arrays.desc, &mpScene), "fpt_scene_create");
-        check(fpt_pass_set_scene(mpPass, mpScene), getType() + "::setScene");
+        check(fpt_pass_set_scene(mpPass, mpScene), mType + "::setScene");
     }
     void execute(RenderContext* pRenderContext, const RenderData& renderData) override {
         const uint2 dims = renderData.getDefaultTextureDims();
@@ -310,7 +312,7 @@ public:
             bindChannel(io, ch.name, b.cuda);
         }
         pRenderContext->waitForFalcor(mStream);
-        check(fpt_pass_execute(mpPass, &io, mStream), getType() + "::execute");
+        check(fpt_pass_execute(mpPass, &io, mStream), mType + "::execute");
         pRenderContext->waitForCuda(mStream);
         // Outputs: shared buffer -> texture.
         for (const ChannelDesc& ch : mOutputs) {
@@ -356,7 +358,7 @@ private:
     // fpt_frame_io channel of a Falcor channel name.
     void bindChannel(fpt_frame_io& io, const std::string& name, void* p) {
         if (name == "vbuffer") {
-            if (getType() == "VBufferRT") io.vbuffer_out = static_cast<uint32_t*>(p);
+            if (mType == "VBufferRT") io.vbuffer_out = static_cast<uint32_t*>(p);
             else io.vbuffer = static_cast<const uint32_t*>(p);
         } else if (name == "color") io.color = static_cast<float*>(p);
         else if (name == "dColor") io.d_color = static_cast<float*>(p);
@@ -368,6 +370,7 @@ private:
         else if (name == "mask") io.mask = static_cast<float*>(p);
     }
 
+    std::string mType;
     fpt_pass* mpPass = nullptr;
     fpt_scene* mpScene = nullptr;
     cudaStream_t mStream = nullptr;

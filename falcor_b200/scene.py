@@ -33,13 +33,18 @@ class HostScene:
         self.desc = lib().fpt_scene_host_desc(handle).contents
 
     @staticmethod
-    def from_arrays(vertices, indices, instances, materials, camera: dict, envmap=None) -> "HostScene":
+    def from_arrays(vertices, indices, instances, materials, camera: dict, envmap=None, textures=None,
+                    base_color_textures=None) -> "HostScene":
         """A scene from host arrays (the SceneBuilder inputs): vertices [N, 12]
         float32 (position, normal, tangent xyzw, texcoord), indices [3T] uint32
         (per-mesh local), instances [I, 5] uint32 (vb_offset, ib_offset,
         triangle_count, material_id, flags), materials [M, 19] float32 in
         fpt_material order, camera dict of fpt_camera fields, envmap optional
-        (rgb [H, W, 3] float32, tint, intensity)."""
+        (rgb [H, W, 3] float32, tint, intensity).  textures: list of texel
+        arrays, [H, W, 4] uint8 (RGBA8, sRGB-encoded unless given as
+        (array, "RGBA8Unorm")) or [H, W, 4] float32 (RGBA32Float);
+        base_color_textures: per material, the index of its base-colour
+        texture or -1 (StandardMaterial::setBaseColorTexture)."""
         obj = HostScene.__new__(HostScene)
         obj._h = None
         obj._keep = []
@@ -80,6 +85,31 @@ class HostScene:
                 env.tint[i] = float(envmap.get("tint", (1, 1, 1))[i])
             obj._keep.append(env)
             d.envmap = C.pointer(env)
+        if textures:
+            descs = (_ffi.fpt_texture_desc * len(textures))()
+            for i, t in enumerate(textures):
+                fmt = None
+                if isinstance(t, tuple):
+                    t, fmt = t
+                t = np.asarray(t)
+                if t.ndim != 3 or t.shape[2] != 4:
+                    raise ValueError("textures must be [H, W, 4] arrays")
+                if t.dtype == np.uint8:
+                    code = _ffi.TEXTURE_RGBA8_UNORM if fmt == "RGBA8Unorm" else _ffi.TEXTURE_RGBA8_UNORM_SRGB
+                    a = arr(t, np.uint8)
+                else:
+                    code = _ffi.TEXTURE_RGBA32_FLOAT
+                    a = arr(t, np.float32)
+                descs[i].width, descs[i].height, descs[i].format = t.shape[1], t.shape[0], code
+                descs[i].texels = a.ctypes.data
+            obj._keep.append(descs)
+            d.textures = C.cast(descs, C.POINTER(_ffi.fpt_texture_desc))
+            d.texture_count = len(textures)
+        if base_color_textures is not None:
+            bt = arr(np.asarray(base_color_textures, dtype=np.int64) + 1, np.uint32)
+            if len(bt) != len(mats):
+                raise ValueError("base_color_textures needs one entry per material")
+            d.base_color_textures = bt.ctypes.data_as(C.POINTER(C.c_uint32))
         obj.desc = d
         return obj
 
@@ -187,6 +217,28 @@ class Scene:
         params = np.ascontiguousarray(params, dtype=np.float32).reshape(len(ids), 20)
         check(lib().fpt_scene_set_material_params(self._h, ids.ctypes.data_as(C.POINTER(C.c_uint32)), len(ids),
                                                   params.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def set_texture_device(self, index: int, texels) -> None:
+        """Replaces the texels of texture `index` from a CUDA tensor of the same
+        size and format: [H, W, 4] uint8 (RGBA8) or float32 (RGBA32Float)
+        (fpt_scene_set_texture_device, ordered on the current stream)."""
+        import torch
+        t = texels.detach().contiguous()
+        if not t.is_cuda or t.dtype not in (torch.uint8, torch.float32):
+            raise ValueError("texels must be a CUDA uint8 or float32 tensor")
+        desc = self.host.desc.textures[index] if index < self.host.desc.texture_count else None
+        if desc is None or tuple(t.shape) != (desc.height, desc.width, 4) or \
+                (t.dtype == torch.float32) != (desc.format == _ffi.TEXTURE_RGBA32_FLOAT):
+            raise ValueError("texels must match the texture's size and format")
+        check(lib().fpt_scene_set_texture_device(self._h, index, C.c_void_p(t.data_ptr()),
+                                                 C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        self._texture_keep = t  # the copy is stream-ordered
+
+    @property
+    def texel_count(self) -> int:
+        """Texels of all textures (the length / 3 of a texture gradient buffer)."""
+        d = self.host.desc
+        return sum(d.textures[i].width * d.textures[i].height for i in range(d.texture_count))
 
     def set_material_params_device(self, params, ids=None) -> None:
         """setMaterialParams from a CUDA float32 tensor [count, 20] without a

@@ -116,6 +116,27 @@ typedef struct fpt_envmap_desc {  /* EnvMap (Scene/Lights/EnvMap.slang)      */
     float intensity;
 } fpt_envmap_desc;
 
+/* Material textures (Scene/Material/MaterialTextureLoader, TextureHandle in
+ * Scene/Material/TextureHandle.slang).  Only the base-colour slot
+ * (StandardMaterial::setBaseColorTexture, StandardMaterial.h:58) is
+ * supported: a textured material takes its base colour from a bilinear
+ * lookup at mip level 0 with wrap addressing, as the PathTracer's default
+ * texture LOD mode (TexLODMode::Mip0: ExplicitLodTextureSampler(0),
+ * PathTracer.slang:799-814; MaterialSystem.slang:308-320) does, with the
+ * filtering done in FP32 in the kernels. */
+typedef enum fpt_texture_format {
+    FPT_TEXTURE_RGBA8_UNORM_SRGB = 0, /* ResourceFormat::RGBA8UnormSrgb: rgb decoded from sRGB */
+    FPT_TEXTURE_RGBA8_UNORM = 1,      /* ResourceFormat::RGBA8Unorm                          */
+    FPT_TEXTURE_RGBA32_FLOAT = 2      /* ResourceFormat::RGBA32Float                         */
+} fpt_texture_format;
+
+typedef struct fpt_texture_desc {
+    uint32_t width, height;
+    uint32_t format;              /* fpt_texture_format                        */
+    const void* texels;           /* width*height texels, row-major, top row
+                                     first; 4 bytes (RGBA8) or 16 bytes each  */
+} fpt_texture_desc;
+
 typedef struct fpt_scene_desc {
     const fpt_vertex* vertices;
     uint32_t vertex_count;
@@ -127,6 +148,11 @@ typedef struct fpt_scene_desc {
     uint32_t material_count;
     fpt_camera camera;
     const fpt_envmap_desc* envmap; /* NULL: no environment light              */
+    const fpt_texture_desc* textures; /* material textures (NULL: none)        */
+    uint32_t texture_count;
+    /* Per material: 1 + the index of its base-colour texture, or 0 for the
+     * uniform base_color.  NULL: no material is textured. */
+    const uint32_t* base_color_textures;
 } fpt_scene_desc;
 
 /* Procedural synthetic scenes (the benchmark workloads). */
@@ -254,6 +280,11 @@ FPT_API fpt_status fpt_scene_set_material_params(fpt_scene* scene, const uint32_
  * Extension of the reference's Scene::setMaterialParams. */
 FPT_API fpt_status fpt_scene_set_material_params_device(fpt_scene* scene, const uint32_t* ids, uint32_t count, const float* params,
                                                         void* stream);
+/* Replaces the texels of texture `index` (same size and format as created)
+ * from device memory, read on `stream`: the update an optimisation loop
+ * makes to a base-colour texture (Texture::setSubresourceBlob,
+ * Core/API/Texture.h).  RGBA8 texels are 4 bytes, RGBA32Float 16. */
+FPT_API fpt_status fpt_scene_set_texture_device(fpt_scene* scene, uint32_t index, const void* texels, void* stream);
 /* Host view of the scene's BVH (valid until the scene is destroyed). */
 FPT_API fpt_status fpt_scene_get_bvh(const fpt_scene* scene, fpt_bvh_view* out);
 /* Host view of the light BVH built for the LightBVH emissive sampler
@@ -446,6 +477,12 @@ typedef struct fpt_grad_buffers {
     float* mesh_tangent;         /* vertex tangents (MeshTangent), or NULL    */
     uint32_t normal_dim;         /* number of floats in `mesh_normal`         */
     uint32_t tangent_dim;        /* number of floats in `mesh_tangent`        */
+    /* Base-colour texture gradients, or NULL: 3 floats (linear rgb) per texel
+     * of every scene texture, textures in order, texels row-major.  The
+     * reference samples textures no_diff (StandardMaterial.slang:164); this is
+     * an extension (for RGBA8 textures, the gradient of the decoded value). */
+    float* base_color_texture;
+    uint32_t texture_dim;        /* number of floats in `base_color_texture`  */
 } fpt_grad_buffers;
 
 /* bwd_diff(tracePaths) of WARDiffPathTracer.rt.slang:167-180 into caller-owned

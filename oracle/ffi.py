@@ -126,10 +126,12 @@ def lib(variant: str = "parity") -> C.CDLL:
         l.orc_path_tracer.restype = C.c_double
         l.orc_path_tracer.argtypes = [_P, C.POINTER(PathTracerParams), _P, _P, _P, C.c_int, u32, u32, u32, u32, u32,
                                       C.POINTER(Counters), _P]
+        l.orc_wardiff_traversal.restype = C.c_double
+        l.orc_wardiff_traversal.argtypes = [_P, C.POINTER(WarDiffParams), u32, u32, C.POINTER(C.c_uint64)]
         l.orc_wardiff.restype = C.c_double
         l.orc_wardiff.argtypes = [_P, C.POINTER(WarDiffParams), C.c_int, C.c_int, _P, u32, _P, u32, _P, u32, _P, u32, C.c_double,
                                   _P, _P, _P,
-                                  _P, u32, u32, u32, u32, u32, C.POINTER(C.c_uint64)]
+                                  _P, u32, u32, u32, u32, u32, C.POINTER(C.c_uint64), _P, u32]
         for n in ("orc_xoshiro", "orc_lcg"):
             getattr(l, n).argtypes = [_P, u32, u32, _P]
         l.orc_splitmix.argtypes = [_P, u32, u32, _P]
@@ -274,7 +276,7 @@ class OracleScene:
         return cnt, dt
 
     def wardiff(self, params: WarDiffParams, mode: int = 0, dLdI=None, mat_tangents=None, pos_tangents=None, eps: float = 0.0,
-                threads: int = 0, rect=None, nrm_tangents=None, tan_tangents=None):
+                threads: int = 0, rect=None, nrm_tangents=None, tan_tangents=None, tex_tangents=None):
         """WARDiffPathTracer restatement.  mode 0: FP32 primal; 1: forward-mode
         derivatives along the rows of mat_tangents / pos_tangents (K <= 4) ->
         sum over pixels of dLdI . dL/dv_k; 2: radiance with the parameters offset
@@ -298,6 +300,10 @@ class OracleScene:
         if tan_tangents is not None:
             tt = np.ascontiguousarray(np.atleast_2d(tan_tangents), dtype=np.float64)
             K = max(K, tt.shape[0])
+        xt = None
+        if tex_tangents is not None:  # rows of 3 floats per texel of every texture
+            xt = np.ascontiguousarray(np.atleast_2d(tex_tangents), dtype=np.float64)
+            K = max(K, xt.shape[0])
         grads = np.zeros(4, dtype=np.float64)
         pert = np.zeros((h, w, 3), dtype=np.float64) if mode in (2, 3) else None
         g = np.ascontiguousarray(dLdI, dtype=np.float32) if dLdI is not None else None
@@ -308,8 +314,20 @@ class OracleScene:
                                pt.shape[1] if pt is not None else 0, ptr(nt) if nt is not None else None,
                                nt.shape[1] if nt is not None else 0, ptr(tt) if tt is not None else None,
                                tt.shape[1] if tt is not None else 0, eps, ptr(g) if g is not None else None, ptr(color),
-                               ptr(grads), ptr(pert) if pert is not None else None, threads, x0, y0, x1, y1, C.byref(rays))
+                               ptr(grads), ptr(pert) if pert is not None else None, threads, x0, y0, x1, y1, C.byref(rays),
+                               ptr(xt) if xt is not None else None, xt.shape[1] if xt is not None else 0)
         return color, (grads[:K] if mode == 1 else None), pert, int(rays.value), dt
+
+    def wardiff_traversal(self, params: WarDiffParams, stride: int = 4, threads: int = 0) -> dict:
+        """Exact traversal counts of the library's attached 8-wide BVH for the
+        rays the WARDiffPathTracer adjoint traces (path, visibility and, with
+        useWAR, auxiliary rays) over every stride-th pixel in x and y."""
+        out = (C.c_uint64 * 7)()
+        dt = self._l.orc_wardiff_traversal(self._h, C.byref(params), stride, threads, out)
+        keys = ("nodes_closest", "tris_closest", "nodes_shadow", "tris_shadow", "mismatches", "rays", "sampled_pixels")
+        d = {k: int(v) for k, v in zip(keys, out)}
+        d["seconds"] = dt
+        return d
 
     def light_bvh(self):
         """(nodes [n, 8] uint32, leaf triangle indices, per-triangle bit paths uint64)."""

@@ -356,7 +356,8 @@ void orc_bsdf_sample(const float* data, int lambert, uint32_t n, const float* wi
 double orc_wardiff(const void* sp, const WarDiffParams* p, int mode, int K, const double* matTangents, uint32_t matDim,
                    const double* posTangents, uint32_t posDim, const double* nrmTangents, uint32_t nrmDim,
                    const double* tanTangents, uint32_t tanDim, double eps, const float* dLdI, float* color, double* grads,
-                   double* pert, uint32_t threads, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, uint64_t* rays) {
+                   double* pert, uint32_t threads, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, uint64_t* rays,
+                   const double* texTangents, uint32_t texDim) {
     const Scene& s = *static_cast<const Scene*>(sp);
     WarSeeds seeds;
     seeds.K = K;
@@ -369,6 +370,8 @@ double orc_wardiff(const void* sp, const WarDiffParams* p, int mode, int K, cons
     seeds.nrmDim = nrmDim;
     seeds.tan = tanTangents;
     seeds.tanDim = tanDim;
+    seeds.tex = texTangents;
+    seeds.texDim = texDim;
     seeds.eps = eps;
     uint32_t nthreads = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
     std::vector<std::vector<double>> acc(nthreads, std::vector<double>(4, 0.0));
@@ -389,6 +392,40 @@ double orc_wardiff(const void* sp, const WarDiffParams* p, int mode, int K, cons
         *rays = 0;
         for (auto& c : wcs) *rays += c.rays;
     }
+    return dt;
+}
+
+// Traversal counts of the WARDiffPathTracer adjoint's rays: forward-mode
+// derivatives (mode 1, K = 1, no seeded tangents) of every stride-th pixel in
+// x and y, which trace the same rays as the adjoint (the path, its visibility
+// rays and, with useWAR, every auxiliary ray), with the library's 8-wide BVH
+// attached.  out: b8 nodes / triangles of closest-hit rays, of visibility
+// rays, mismatches, rays, sampled pixels.  Returns seconds.
+double orc_wardiff_traversal(const void* sp, const WarDiffParams* p, uint32_t stride, uint32_t threads, uint64_t* out) {
+    const Scene& s = *static_cast<const Scene*>(sp);
+    const uint32_t nthreads = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
+    std::vector<TraceCounters> tcs(nthreads);
+    std::vector<WarCounters> wcs(nthreads);
+    const uint32_t sw = (p->width + stride - 1) / stride, sh = (p->height + stride - 1) / stride;
+    auto t0 = std::chrono::steady_clock::now();
+    parallel_tiles(0, 0, sw, sh, nthreads, [&](uint32_t xs, uint32_t ys, uint32_t tid) {
+        WarSeeds seeds;
+        seeds.K = 1;
+        seeds.meshID = p->meshID;
+        seeds.tc = &tcs[tid];
+        double acc[4] = {0, 0, 0, 0};
+        const uint32_t x = xs * stride, y = ys * stride;
+        const float g[3] = {1.f, 1.f, 1.f};
+        wardiff_pixel(s, *p, seeds, 1, x, y, g, nullptr, acc, nullptr, &wcs[tid]);
+    });
+    const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    for (int i = 0; i < 7; i++) out[i] = 0;
+    for (const TraceCounters& c : tcs) {
+        out[0] += c.b8NodesClosest; out[1] += c.b8TrisClosest; out[2] += c.b8NodesShadow; out[3] += c.b8TrisShadow;
+        out[4] += c.b8Mismatch;
+    }
+    for (const WarCounters& c : wcs) out[5] += c.rays;
+    out[6] = uint64_t(sw) * sh;
     return dt;
 }
 

@@ -247,6 +247,7 @@ static MaterialInstance<R> material_instance(const Scene& s, const ShadingData<R
     R f = (IoR - R(1)) / (IoR + R(1));
     R F0 = f * f;
     V3<R> baseColor(R(m.baseColor[0]), R(m.baseColor[1]), R(m.baseColor[2]));
+    if (m.baseColorTexture >= 0) baseColor = tex_sample<R>(s, uint32_t(m.baseColorTexture), float(sd.uv.x), float(sd.uv.y));
     R specG = R(m.specular[1]), specB = R(m.specular[2]);
     d.diffuse = lerp(baseColor, V3<R>(R(0)), specB);
     d.specular = lerp(V3<R>(F0), baseColor, specB);

@@ -64,6 +64,9 @@ struct WarSeeds {
     uint32_t nrmDim = 0;
     const double* tan = nullptr;     // K x tanDim tangents of the (normalised) vertex tangents of mesh `meshID`
     uint32_t tanDim = 0;
+    const double* tex = nullptr;     // K x texDim tangents of the texels' linear rgb ((texelBase + texel) * 3 + channel)
+    uint32_t texDim = 0;
+    TraceCounters* tc = nullptr;     // traversal counters of every ray traced (per thread)
     double eps = 0;                  // Shadow: perturbation scale
 };
 

@@ -130,6 +130,30 @@ Scene::Scene(const fpt_scene_desc* d, const fpt_camera_data* cam, uint32_t alias
         o.activeLobes = LOBE_ALL;
         V3<float> e = V3<float>(o.emissive[0], o.emissive[1], o.emissive[2]) * o.emissiveFactor;
         o.emissiveNonZero = any_pos(e);
+        if (d->base_color_textures && d->base_color_textures[m]) o.baseColorTexture = int32_t(d->base_color_textures[m]) - 1;
+    }
+    // Material textures (StandardMaterial base colour), texels decoded once.
+    float srgb[256];
+    fpt_tex::srgb_decode_table(srgb);
+    textures.resize(d->texture_count);
+    for (uint32_t t = 0; t < d->texture_count; t++) {
+        const fpt_texture_desc& td = d->textures[t];
+        TextureO& o = textures[t];
+        o.width = td.width;
+        o.height = td.height;
+        o.format = td.format;
+        o.texelBase = texelCount;
+        const size_t n = size_t(td.width) * td.height;
+        texelCount += uint32_t(n);
+        o.rgb.resize(n * 3);
+        for (size_t i = 0; i < n; i++)
+            for (int c = 0; c < 3; c++) {
+                if (td.format == FPT_TEXTURE_RGBA32_FLOAT) o.rgb[3 * i + c] = static_cast<const float*>(td.texels)[4 * i + c];
+                else {
+                    const uint8_t b = static_cast<const uint8_t*>(td.texels)[4 * i + c];
+                    o.rgb[3 * i + c] = td.format == FPT_TEXTURE_RGBA8_UNORM_SRGB ? srgb[b] : fpt_tex::unorm8(b);
+                }
+            }
     }
     // Global triangle numbering: instance-major, primitive-minor.
     uint32_t total = 0, maxTris = 0;
@@ -527,7 +551,8 @@ Hit Scene::traceBvh8(V3<float> o, V3<float> d, float tMin, float tMax, bool anyH
             }
         }
         // Push far to near so that the nearest child is popped first.
-        std::sort(kids, kids + nk, [](const Entry& a, const Entry& b) { return a.t > b.t; });
+        for (int i = 1; i < nk; i++)  // insertion sort, descending t (at most 8 entries)
+            for (int j = i; j > 0 && kids[j - 1].t < kids[j].t; j--) std::swap(kids[j - 1], kids[j]);
         for (int i = 0; i < nk; i++) stack.push_back(kids[i]);
     }
     if (bestTri != 0xffffffffu) {

@@ -11,6 +11,7 @@
 #include "oracle_math.h"
 #include "oracle_lightbvh.h"
 #include "../include/fpt.h"
+#include "../falcor_b200/csrc/texture.h"
 
 namespace orc {
 
@@ -41,6 +42,14 @@ struct Material {
     bool doubleSided, thinSurface;
     uint32_t activeLobes;
     bool emissiveNonZero;
+    int32_t baseColorTexture = -1;  // texture index, or -1 for the uniform baseColor
+};
+
+// A material texture with its texels decoded to linear rgb as the kernels
+// decode them (sRGB table, c / 255, or the float value).
+struct TextureO {
+    uint32_t width = 0, height = 0, format = 0, texelBase = 0;
+    std::vector<float> rgb;  // 3 floats per texel, row-major
 };
 
 // EmissiveTriangle after PackedEmissiveTriangle::unpack (LightCollectionShared.slang:41-135).
@@ -125,6 +134,10 @@ public:
     uint32_t impDim = 0, impBaseMip = 0;
     std::vector<std::vector<float>> impMips;        // mip 0 = impDim^2
 
+    // material textures
+    std::vector<TextureO> textures;
+    uint32_t texelCount = 0;
+
     // helpers
     StaticVertex getVertex(uint32_t globalIndex) const;
     void getTriangleVertexIndices(uint32_t instanceID, uint32_t prim, uint32_t idx[3]) const;
@@ -160,6 +173,23 @@ private:
     template <class R> Hit traceImpl(V3<R> o, V3<R> d, R tMin, R tMax, bool anyHit, TraceCounters* c) const;
     Hit traceBvh8(V3<float> o, V3<float> d, float tMin, float tMax, bool anyHit, uint64_t& nodes, uint64_t& tris) const;
 };
+
+// MaterialSystem::sampleTexture with ExplicitLodTextureSampler(0)
+// (MaterialSystem.slang:308-320): bilinear at mip 0 with wrap addressing
+// (texture.h), accumulated in R in the kernels' order.
+template <class R> V3<R> tex_sample(const Scene& s, uint32_t tex, float u, float v) {
+    const TextureO& t = s.textures[tex];
+    const fpt_tex::Bilinear b = fpt_tex::bilinear(u, v, t.width, t.height);
+    auto texel = [&](uint32_t x, uint32_t y) {
+        const float* c = &t.rgb[(size_t(y) * t.width + x) * 3];
+        return V3<R>(R(c[0]), R(c[1]), R(c[2]));
+    };
+    V3<R> c = texel(b.x0, b.y0) * R(b.w[0]);
+    c += texel(b.x1, b.y0) * R(b.w[1]);
+    c += texel(b.x0, b.y1) * R(b.w[2]);
+    c += texel(b.x1, b.y1) * R(b.w[3]);
+    return c;
+}
 
 // Packs one vertex like PackedStaticVertexData::pack on the host.
 PackedVertex pack_vertex(const fpt_vertex& v);

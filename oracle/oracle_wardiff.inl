@@ -42,6 +42,7 @@ template <> struct Seed<float> {
     static float pos(const WarSeeds&, uint32_t, float v) { return v; }
     static float nrm(const WarSeeds&, uint32_t, float v) { return v; }
     static float tan(const WarSeeds&, uint32_t, float v) { return v; }
+    static float tex(const WarSeeds&, uint32_t, float v) { return v; }
 };
 template <int N> struct Seed<Dual<N>> {
     static Dual<N> get(const double* t, uint32_t dim, int K, uint32_t idx, float v) {
@@ -54,6 +55,7 @@ template <int N> struct Seed<Dual<N>> {
     static Dual<N> pos(const WarSeeds& s, uint32_t idx, float v) { return get(s.pos, s.posDim, s.K, idx, v); }
     static Dual<N> nrm(const WarSeeds& s, uint32_t idx, float v) { return get(s.nrm, s.nrmDim, s.K, idx, v); }
     static Dual<N> tan(const WarSeeds& s, uint32_t idx, float v) { return get(s.tan, s.tanDim, s.K, idx, v); }
+    static Dual<N> tex(const WarSeeds& s, uint32_t idx, float v) { return get(s.tex, s.texDim, s.K, idx, v); }
 };
 template <> struct Seed<Shadow> {
     static Shadow get(const double* t, uint32_t dim, double eps, uint32_t idx, float v) {
@@ -65,6 +67,7 @@ template <> struct Seed<Shadow> {
     static Shadow pos(const WarSeeds& s, uint32_t idx, float v) { return get(s.pos, s.posDim, s.eps, idx, v); }
     static Shadow nrm(const WarSeeds& s, uint32_t idx, float v) { return get(s.nrm, s.nrmDim, s.eps, idx, v); }
     static Shadow tan(const WarSeeds& s, uint32_t idx, float v) { return get(s.tan, s.tanDim, s.eps, idx, v); }
+    static Shadow tex(const WarSeeds& s, uint32_t idx, float v) { return get(s.tex, s.texDim, s.eps, idx, v); }
 };
 
 template <class R> static V3<R> lift3(const V3<float>& a) { return V3<R>(R(a.x), R(a.y), R(a.z)); }
@@ -179,7 +182,7 @@ template <class R> static R clampR(R x, R lo, R hi) { return x < lo ? lo : (x > 
 // (seeded) vertices, the normal is the interpolated vertex normal.
 template <class R>
 static bool war_aux_hit(const Scene& s, const WarSeeds& seeds, V3<float> o, V3<float> d, V3<R>& posW, V3<float>& normalW) {
-    Hit h = s.traceClosest(o, d, 0.f, std::numeric_limits<float>::max(), nullptr);
+    Hit h = s.traceClosest(o, d, 0.f, std::numeric_limits<float>::max(), seeds.tc);
     if (!h.valid) return false;
     uint32_t idx[3];
     s.getTriangleVertexIndices(h.instanceID, h.primitiveIndex, idx);
@@ -371,6 +374,22 @@ static MaterialInstance<R> war_material(const Scene& s, const WarSeeds& seeds, c
     R F0 = f * f;
     V3<R> baseColor(Seed<R>::mat(seeds, base + 0, m.baseColor[0]), Seed<R>::mat(seeds, base + 1, m.baseColor[1]),
                     Seed<R>::mat(seeds, base + 2, m.baseColor[2]));
+    if (m.baseColorTexture >= 0) {
+        // Textured base colour: the bilinear lookup of tex_sample with the
+        // texels' seeded derivatives (an extension: the reference samples
+        // textures no_diff, StandardMaterial.slang:164).
+        const TextureO& t = s.textures[uint32_t(m.baseColorTexture)];
+        const fpt_tex::Bilinear b = fpt_tex::bilinear(sd.uv.x, sd.uv.y, t.width, t.height);
+        for (int k = 0; k < 4; k++) {
+            const uint32_t x = (k & 1) ? b.x1 : b.x0, y = (k & 2) ? b.y1 : b.y0;
+            const size_t texel = size_t(y) * t.width + x;
+            const uint32_t g = (t.texelBase + uint32_t(texel)) * 3u;
+            const V3<R> c(Seed<R>::tex(seeds, g, t.rgb[3 * texel]), Seed<R>::tex(seeds, g + 1, t.rgb[3 * texel + 1]),
+                          Seed<R>::tex(seeds, g + 2, t.rgb[3 * texel + 2]));
+            if (k == 0) baseColor = c * R(b.w[0]);
+            else baseColor += c * R(b.w[k]);
+        }
+    }
     R roughness = Seed<R>::mat(seeds, base + 4, m.specular[1]);
     R metallic = Seed<R>::mat(seeds, base + 3, m.specular[2]);
     d.diffuse = lerp(baseColor, V3<R>(R(0)), metallic);
@@ -460,7 +479,7 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
     V3<R> rayDirR = war ? war_cam_dir<R>(c, pixR, float(p.width), float(p.height)) : lift3<R>(rayDir);
 
     if (wc) wc->rays++;
-    Hit h = s.traceClosest(rayOrigin, rayDir, 0.f, std::numeric_limits<float>::max(), nullptr);
+    Hit h = s.traceClosest(rayOrigin, rayDir, 0.f, std::numeric_limits<float>::max(), seeds.tc);
     if (!h.valid) return path.radiance;
     WarIsect<R> is = war_intersection<R>(s, seeds, h, rayOrigin, rayDir);
 
@@ -548,7 +567,7 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
                 V3<float> ldir = normalize(toLight);
                 if (any_pos(Li)) {
                     if (wc) wc->rays++;
-                    const bool visible = s.traceVisibility(origin, ldir, 0.f, distance, nullptr);
+                    const bool visible = s.traceVisibility(origin, ldir, 0.f, distance, seeds.tc);
                     if (visible) {
                         // computeNEE (PTUtils.slang:211-249).
                         V3<R> wo = lift3<R>(tls.posW) - is.posW;
@@ -592,7 +611,7 @@ static V3<R> war_trace_path(const Scene& s, const WarDiffParams& p, const WarSee
         path.length++;
 
         if (wc) wc->rays++;
-        h = s.traceClosest(rayOrigin, rayDir, 0.f, std::numeric_limits<float>::max(), nullptr);
+        h = s.traceClosest(rayOrigin, rayDir, 0.f, std::numeric_limits<float>::max(), seeds.tc);
         if (!h.valid) break;
         is = war_intersection<R>(s, seeds, h, rayOrigin, rayDir);
     }

@@ -120,3 +120,35 @@ def check_per_sample(gs, os_, listed, what, rtol=1e-4, atol=1e-6, max_listed=1e-
     assert listed.sum() <= max(1, max_listed * ok.size), f"{what}: {int(listed.sum())} edge-ray samples listed"
     exact = np.all(gs.view(np.uint32) == os_.view(np.uint32), axis=-1)
     return float(exact.mean()), int(listed.sum())
+
+
+def textured(host, seed=5, every=4):
+    """A copy of a host scene whose non-emissive materials (except every
+    `every`-th) take their base colour from one of three textures -- a 64x48
+    RGBA8 sRGB, a 16x16 RGBA8 UNORM and a 24x32 RGBA32Float texture of random
+    texels -- with texture coordinates spread over several periods (negative
+    ones included) so that the lookups wrap."""
+    from falcor_b200.scene import HostScene
+    rng = np.random.default_rng(seed)
+    v = host.vertices.copy()
+    p = v[:, 0:3]
+    v[:, 10] = p[:, 0] * 1.7 + p[:, 2] * 0.6 + 0.13
+    v[:, 11] = p[:, 1] * 1.3 - p[:, 2] * 0.45 - 0.21
+    mats = host.materials.copy()
+    emissive = (mats[:, 8:11] * mats[:, 11:12]).sum(1) > 0
+    textures = [rng.integers(0, 256, (48, 64, 4), dtype=np.uint8),
+                (rng.integers(0, 256, (16, 16, 4), dtype=np.uint8), "RGBA8Unorm"),
+                rng.random((32, 24, 4)).astype(np.float32)]
+    bct = [-1 if (emissive[m] or m % every == every - 1) else m % 3 for m in range(len(mats))]
+    d = host.desc
+    cam = {}
+    for name, _ in d.camera._fields_:
+        val = getattr(d.camera, name)
+        cam[name] = list(val) if not isinstance(val, float) else val
+    env = None
+    if d.envmap:
+        e = d.envmap.contents
+        rgb = np.ctypeslib.as_array(e.rgb, shape=(e.height * e.width * 3,)).reshape(e.height, e.width, 3).copy()
+        env = {"rgb": rgb, "tint": list(e.tint), "intensity": e.intensity}
+    return HostScene.from_arrays(v, host.indices.copy(), host.instances.copy(), mats, cam, env, textures=textures,
+                                 base_color_textures=bct)

@@ -136,3 +136,37 @@ def test_displacement_chain_rule_matches_finite_differences():
         e[k] = 1e-3
         fd = (f(d0 + e) - f(d0 - e)) / 2e-3
         assert abs(float(g[k]) - float(fd)) < 1e-3 * max(1.0, abs(float(fd)))
+
+
+def test_srgb_encode_decode_round_trip():
+    from falcor_b200.inverse import srgb_decode8, srgb_encode8
+    codes = np.arange(256, dtype=np.uint8)
+    assert np.array_equal(srgb_encode8(srgb_decode8(codes)), codes)
+    hs = displaced_grid_scene(res=4, texture=(8, 4))
+    assert hs.desc.texture_count == 1 and hs.desc.textures[0].width == 8 and hs.desc.textures[0].height == 4
+    assert list(hs.desc.base_color_textures[i] for i in range(2)) == [1, 0]
+
+
+@pytest.mark.gpu
+def test_inverse_loop_albedo_texture(fpt):
+    """C5's albedo texture (RGBA8 sRGB) optimised alone: the loss falls and the
+    texture moves towards the target texture where the views see it."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from falcor_b200.inverse import InverseLoop
+    from falcor_b200.scene import Scene
+    scene = Scene(displaced_grid_scene(res=16, texture=(32, 32)))
+    loop = InverseLoop(scene, 0, orbit_cameras(2), 48, 48, spp=4, max_bounces=2, lr=3e-2, fresh_seeds=False,
+                       optimize=("texture",), use_war=False, texture_index=0)
+    assert loop.texture is not None and tuple(loop.texture.shape) == (32, 32, 3)
+    start = loop.texture.detach().clone()
+    yy, xx = torch.meshgrid(torch.linspace(0, 1, 32, device="cuda"), torch.linspace(0, 1, 32, device="cuda"), indexing="ij")
+    target = torch.stack([0.2 + 0.6 * xx, 0.8 - 0.6 * yy, 0.4 + 0.2 * xx * yy], 2)
+    loop.render_targets(loop.disp, loop.color.detach(), texture_target=target)
+    losses = [loop.step() for _ in range(12)]
+    assert losses[-1] < 0.5 * losses[0], losses
+    moved = (loop.texture.detach() - start).abs().sum(2) > 1e-3
+    assert moved.float().mean() > 0.2
+    closer = ((loop.texture.detach() - target).abs() < (start - target).abs()).all(2)
+    assert float(closer[moved].float().mean()) > 0.6
