@@ -61,7 +61,7 @@ def test_ragged_frames_match_oracle(fpt, oracle, size):
     assert np.array_equal(vb.view(np.uint32), ref_vb)
     ref, _, _, _ = osc.path_tracer(ref_vb, H.pt_params(w, h, 4, seed=1, max_bounces=3))
     ok = H.rel_close(got[..., :3], ref[..., :3], rtol=1e-4).all(axis=-1)
-    assert ok.mean() >= 0.99 or ok.size == 1 and ok.all()
+    assert ok.all(), f"{int((~ok).sum())} of {ok.size} pixels differ"
     assert st.device_error == 0
 
 
@@ -75,7 +75,8 @@ def test_single_triangle_and_background(fpt, oracle):
     assert 0 < hit.mean() < 1  # both hit and background pixels
     osc = H.oracle_scene(host)
     ref, _, _, _ = osc.path_tracer(osc.vbuffer(48, 48), H.pt_params(48, 48, 4, seed=1, max_bounces=3))
-    assert H.rel_close(got[..., :3], ref[..., :3], rtol=1e-4).all(axis=-1).mean() >= 0.99
+    ok = H.rel_close(got[..., :3], ref[..., :3], rtol=1e-4).all(axis=-1)
+    assert ok.all(), f"{int((~ok).sum())} of {ok.size} pixels differ"
     # Background pixels show the constant environment map (through LogLuv, ~1 % chroma error).
     assert np.allclose(got[~hit][:, :3], 0.25, rtol=2e-2)
     assert st.device_error == 0

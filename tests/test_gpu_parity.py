@@ -41,7 +41,7 @@ def test_vbuffer_bit_exact_box_icosphere(torch_cuda, oracle):
     edge = _edge_mask(orc) | _edge_mask(gpu)
     same = np.all(gpu == orc, axis=-1)
     assert np.all(same | edge), f"{np.sum(~same & ~edge)} non-edge primary hits differ"
-    assert np.mean(same) > 0.999
+    assert np.sum(~same) <= max(1, 1e-3 * same.size)  # listed edge pixels
     assert np.mean(orc[..., 0] != 0) > 0.9  # the camera sees the room
 
 
@@ -68,12 +68,17 @@ def test_minimal_path_tracer_parity(torch_cuda, oracle):
     mpt = MinimalPathTracer({"maxBounces": 3})
     mpt.set_scene(scene)
     color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
-    mpt.execute({"vbuffer": vb, "color": color}, frame=0)
+    trace = torch.zeros((Hh, W, 1, 5, 4), dtype=torch.int32, device="cuda")
+    mpt.execute({"vbuffer": vb, "color": color}, frame=0, hit_trace=trace)
     torch.cuda.synchronize()
     g = color.cpu().numpy()
-    o, _, _ = H.oracle_scene(host).minimal_pt(vb.cpu().numpy().view(np.uint32), H.minimal_params(W, Hh))
-    ok = np.all(H.rel_close(g[..., :3], o[..., :3], rtol=1e-4, atol=1e-6), axis=-1)
-    assert np.mean(ok) > 0.995, f"{np.sum(~ok)} of {ok.size} pixels differ"
+    o, _, _, ot = H.oracle_scene(host).minimal_pt(vb.cpu().numpy().view(np.uint32), H.minimal_params(W, Hh), trace=True)
+    # Both sides start from the same V-buffer; every later hit is compared
+    # bit for bit and a path whose hits first differ at an edge ray is listed.
+    differs, listed = H.compare_hit_traces(trace.cpu().numpy().view(np.uint32)[:, :, 0], ot)
+    assert not (differs & ~listed).any()
+    exact, _ = H.check_per_sample(g[..., :3], o[..., :3], listed, "MinimalPathTracer 128x128")
+    print(f"MinimalPathTracer 128x128: {exact:.6f} bit-exact")
     assert np.all(np.isfinite(g))
     assert g[..., :3].mean() > 0.01
 
@@ -90,16 +95,19 @@ def test_path_tracer_per_sample_parity(torch_cuda, oracle):
     pt.set_scene(scene)
     color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
     samples = torch.zeros((Hh, W, spp, 3), dtype=torch.float32, device="cuda")
-    pt.execute({"vbuffer": vb, "color": color}, sample_color=samples)
+    tr = torch.zeros((Hh, W, spp, 6, 4), dtype=torch.int32, device="cuda")
+    pt.execute({"vbuffer": vb, "color": color}, sample_color=samples, hit_trace=tr)
     torch.cuda.synchronize()
     gs = samples.cpu().numpy()
     gc = color.cpu().numpy()
-    o, osmp, cnt, _ = H.oracle_scene(host).path_tracer(vb.cpu().numpy().view(np.uint32), H.pt_params(W, Hh, spp, seed=3, max_bounces=4),
-                                                      samples=True)
-    ok = np.all(H.rel_close(gs, osmp, rtol=1e-4, atol=1e-6), axis=-1)
-    assert np.mean(ok) > 0.995, f"{np.sum(~ok)} of {ok.size} samples differ"
-    okc = np.all(H.rel_close(gc[..., :3], o[..., :3], rtol=1e-4, atol=1e-6), axis=-1)
-    assert np.mean(okc) > 0.99
+    o, osmp, cnt, _, otr = H.oracle_scene(host).path_tracer(vb.cpu().numpy().view(np.uint32),
+                                                           H.pt_params(W, Hh, spp, seed=3, max_bounces=4), samples=True, trace=True)
+    differs, listed = H.compare_hit_traces(tr.cpu().numpy().view(np.uint32), otr)
+    assert not (differs & ~listed).any()
+    exact, _ = H.check_per_sample(gs, osmp, listed, "PathTracer samples")
+    print(f"PathTracer 64x48x4: {exact:.6f} bit-exact")
+    # The pixel colour (LogLuv per sample, averaged) of every pixel without a listed sample.
+    H.check_per_sample(gc[..., :3], o[..., :3], listed.any(axis=-1), "PathTracer colour")
     st = pt.stats()
     assert st.paths == cnt.paths
     assert st.device_error == 0

@@ -252,7 +252,7 @@ def test_vbuffer_extra_channels(torch_cuda, oracle):
     vb = ch["vbuffer"].cpu().numpy().view(np.uint32)
     orc = oracle.OracleScene(C.pointer(host.desc), cd).vbuffer(W, Hh)
     same = np.all(vb == orc, axis=-1)
-    assert np.mean(same) > 0.999
+    assert np.all(same | H.edge_pixels(vb) | H.edge_pixels(orc)), f"{int(np.sum(~same))} primary hits differ"
     pos, valid = _hit_positions(host, vb)
     np.testing.assert_array_equal(ch["mask"].cpu().numpy(), valid.astype(np.float32))
     depth = ch["depth"].cpu().numpy()
@@ -300,7 +300,8 @@ def test_vbuffer_jitter_patterns(torch_cuda, oracle, pattern, count):
             torch.cuda.synchronize()
             g = out.cpu().numpy().view(np.uint32)
             o = oracle.OracleScene(C.pointer(host.desc), cd).vbuffer(W, Hh)
-            assert np.mean(np.all(g == o, axis=-1)) > 0.999
+            same = np.all(g == o, axis=-1)
+            assert np.all(same | H.edge_pixels(g) | H.edge_pixels(o)), f"{int(np.sum(~same))} primary hits differ"
     vbp.set_properties({"samplePattern": "Center"})
     vbp.execute({"vbuffer": out})
     cd = scene.camera_data()
@@ -352,7 +353,7 @@ def test_graph_script_end_to_end(torch_cuda, oracle):
         a = acc.execute(col.astype(np.float32))
         ga = g.get_output("AccumulatePass.output").cpu().numpy()
         ok = np.all(H.rel_close(ga[..., :3], a[..., :3], rtol=1e-4, atol=1e-6), axis=-1)
-        assert np.mean(ok) > 0.995, f"frame {frame}: {np.sum(~ok)} pixels differ"
+        assert ok.all(), f"frame {frame}: {np.sum(~ok)} pixels differ"
     gt = g.get_output("ToneMapper.dst").cpu().numpy()
     ot = tone_map(ga, {"operator": "Reinhard"})  # the tone mapper applied to the device accumulation
     np.testing.assert_allclose(gt, ot, rtol=TM_RTOL, atol=TM_ATOL)

@@ -85,13 +85,17 @@ def test_path_tracer_light_bvh_parity(fpt, oracle, scheduler):
     pt.set_scene(scene)
     color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
     samples = torch.zeros((Hh, W, spp, 3), dtype=torch.float32, device="cuda")
-    pt.execute({"vbuffer": vb, "color": color}, sample_color=samples)
+    tr = torch.zeros((Hh, W, spp, 6, 4), dtype=torch.int32, device="cuda")
+    pt.execute({"vbuffer": vb, "color": color}, sample_color=samples, hit_trace=tr)
     torch.cuda.synchronize()
     gs = samples.cpu().numpy()
-    o, osmp, _, _ = H.oracle_scene(host).path_tracer(vb.cpu().numpy().view(np.uint32),
-                                                       H.pt_params(W, Hh, spp, seed=3, max_bounces=4, sampler=1), samples=True)
-    ok = np.all(H.rel_close(gs, osmp, rtol=1e-4, atol=1e-6), axis=-1)
-    assert np.mean(ok) > 0.995, f"{np.sum(~ok)} of {ok.size} samples differ"
+    o, osmp, _, _, otr = H.oracle_scene(host).path_tracer(vb.cpu().numpy().view(np.uint32),
+                                                            H.pt_params(W, Hh, spp, seed=3, max_bounces=4, sampler=1), samples=True,
+                                                            trace=True)
+    differs, listed = H.compare_hit_traces(tr.cpu().numpy().view(np.uint32), otr)
+    assert not (differs & ~listed).any()
+    exact, _ = H.check_per_sample(gs, osmp, listed, f"LightBVH {scheduler}")
+    print(f"LightBVH {scheduler}: {exact:.6f} bit-exact")
     assert gs.mean() > 0
 
 

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from tests import helpers as H
-from tests.test_wardiff import check_projections, war_params, war_props
+from tests.test_wardiff import check_projections, mesh_vertex_count, war_params, war_props
 
 
 def _texel_tangents(host, osc, rng, k):
@@ -129,7 +129,7 @@ def test_texture_adjoint_matches_oracle_forward_mode(torch_cuda, oracle, war, sc
     pt.set_scene(scene)
     color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
     gt = torch.zeros(3 * scene.texel_count, dtype=torch.float32, device="cuda")
-    gp = torch.zeros(3 * H.mesh_vertex_count(host, 13), dtype=torch.float32, device="cuda")
+    gp = torch.zeros(3 * mesh_vertex_count(host, 13), dtype=torch.float32, device="cuda")
     pt.backward({"color": color}, torch.from_numpy(dLdI).cuda(), position_grad=gp if war else None, texture_grad=gt)
     torch.cuda.synchronize()
     got = gt.cpu().numpy().astype(np.float64)

@@ -141,7 +141,7 @@ def test_primal_matches_oracle(fpt, oracle, scene, scheduler):
         torch.cuda.synchronize()
         got = out.cpu().numpy()
         ok = H.rel_close(got[..., :3], ref[..., :3], rtol=1e-4, atol=1e-6).all(axis=-1)
-        assert ok.mean() >= 0.99, (scene, seed, ok.mean())
+        assert ok.all(), (scene, seed, int((~ok).sum()))
         assert got[..., :3].mean() > 0
 
 
@@ -500,10 +500,13 @@ def test_forward_diff_debug_image_matches_oracle(fpt, oracle, war):
         torch.cuda.synchronize()
         d = dcolor.cpu().numpy()
         assert np.all(d[..., 1:3] == 0) and np.all(d[..., 3] == 1)
+        # FP32 kernel against the FP64 oracle derivative: at most 1e-3 of the
+        # pixels may miss the 1 % bar (cancellation in a pixel's derivative sum).
         ok = np.abs(d[..., 0] - dref[..., 0]) <= 1e-2 * np.maximum(np.abs(dref[..., 0]), 1e-2)
-        assert ok.mean() >= 0.99, (var, war, ok.mean())
+        assert (~ok).sum() <= max(1, 1e-3 * ok.size), (var, war, int((~ok).sum()))
         assert np.abs(dref[..., 0]).max() > 0
-        assert H.rel_close(color.cpu().numpy()[..., :3], ref_color[..., :3], rtol=1e-4, atol=1e-6).all(axis=-1).mean() >= 0.99
+        okc = H.rel_close(color.cpu().numpy()[..., :3], ref_color[..., :3], rtol=1e-4, atol=1e-6).all(axis=-1)
+        assert okc.all(), (var, war, int((~okc).sum()))
 
 
 @pytest.mark.gpu
