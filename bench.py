@@ -498,12 +498,30 @@ def batched_bench(dev) -> dict:
     b.launch()
     t_bat = max_over_ranks(_time_ms(b.launch, 3), dev)
     st = b.stats()
+    # Amdahl bound of batching: every request timed alone (its plain launches),
+    # and the share of the requests large enough to fill the GPU by themselves
+    # (>= 2^22 paths).  Batching cannot speed those up, so even if it made all
+    # other requests free the speedup would stay below t_seq / t_large.
+    t_req = []
+    for i, (si, wdt, hgt, spp, mb) in shard(batch_requests()):
+        one = Batch()
+        one.set_tuning(wave_capacity=tuning[0])
+        one.add(scenes[si], wdt, hgt, spp, mb, seed=i)
+        one.launch_sequential()
+        t_req.append((wdt * hgt * spp, _time_ms(one.launch_sequential, 1)))
+        del one
+    t_alone = max_over_ranks(sum(t for _, t in t_req), dev)
+    t_large = max_over_ranks(sum(t for n, t in t_req if n >= (1 << 22)), dev)
+    amdahl = {"requests_timed_alone_ms": round(t_alone, 2), "large_requests": sum(1 for n, _ in t_req if n >= (1 << 22)),
+              "large_requests_ms": round(t_large, 2), "large_paths_fraction": round(
+                  sum(n for n, _ in t_req if n >= (1 << 22)) / max(1, sum(n for n, _ in t_req)), 4),
+              "max_speedup_if_small_requests_were_free": round(t_seq / max(t_large, 1e-9), 3)}
     return {"workload": "64 requests, 8 scenes of 10k-1M triangles, res {128..1024}^2, spp {1,4,16,32}, bounces 2-8",
             "unit": "Mpaths/s", "paths_per_launch": paths, "batched": round(paths / t_bat / 1e3, 2),
             "sequential": round(paths / t_seq / 1e3, 2), "speedup": round(t_seq / t_bat, 3),
             "ms_batched": round(t_bat, 2), "ms_sequential": round(t_seq, 2),
-            "tuning": {"wave_capacity": tuning[0], "shade_grid_scale": tuning[1]},
-            "graph_kernel_launches": int(st.kernel_launches), "device_error": int(st.device_error)}
+            "tuning": {"wave_capacity": tuning[0], "shade_grid_scale": tuning[1], "fetch_chunk": tuning[2]},
+            "graph_kernel_launches": int(st.kernel_launches), "device_error": int(st.device_error), "amdahl": amdahl}
 
 
 def gpu_rmse(accum, dev) -> dict:

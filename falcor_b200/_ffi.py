@@ -95,6 +95,10 @@ class fpt_frame_io(C.Structure):
                 ("hit_trace", C.c_void_p)]
 
 
+class fpt_batch_tuning(C.Structure):
+    _fields_ = [("wave_capacity", u32), ("shade_grid_scale", u32), ("fetch_chunk", u32)]
+
+
 class fpt_grad_buffers(C.Structure):
     _fields_ = [("material", C.c_void_p), ("mesh_position", C.c_void_p), ("material_dim", u32), ("position_dim", u32),
                 ("mesh_normal", C.c_void_p), ("mesh_tangent", C.c_void_p), ("normal_dim", u32), ("tangent_dim", u32),
@@ -184,6 +188,8 @@ SIGNATURES = {
     "fpt_batch_add": (C.c_int, [_P, C.POINTER(fpt_batch_request)]),
     "fpt_batch_set_tuning": (C.c_int, [_P, u32, u32]),
     "fpt_batch_get_tuning": (C.c_int, [_P, C.POINTER(u32), C.POINTER(u32)]),
+    "fpt_batch_set_tuning_ex": (C.c_int, [_P, C.POINTER(fpt_batch_tuning)]),
+    "fpt_batch_get_tuning_ex": (C.c_int, [_P, C.POINTER(fpt_batch_tuning)]),
     "fpt_batch_autotune": (C.c_int, [_P, _P]),
     "fpt_batch_launch": (C.c_int, [_P, _P]),
     "fpt_batch_launch_sequential": (C.c_int, [_P, _P]),

@@ -47,16 +47,23 @@ class Batch:
         self.requests.append((scene, width, height, spp, max_bounces, seed, color))
         return color
 
-    def set_tuning(self, wave_capacity: int = 0, shade_grid_scale: int = 0) -> None:
-        check(lib().fpt_batch_set_tuning(self._h, wave_capacity, shade_grid_scale))
+    def set_tuning(self, wave_capacity: int = 0, shade_grid_scale: int = 0, fetch_chunk: int | None = None) -> None:
+        """Wave capacity (paths in flight), shade grid multiple and the traversal
+        kernels' queue entries per warp claim (0 or None: unchanged / default)."""
+        if fetch_chunk is None:
+            check(lib().fpt_batch_set_tuning(self._h, wave_capacity, shade_grid_scale))
+            return
+        t = _ffi.fpt_batch_tuning(wave_capacity=wave_capacity, shade_grid_scale=shade_grid_scale, fetch_chunk=fetch_chunk)
+        check(lib().fpt_batch_set_tuning_ex(self._h, C.byref(t)))
 
     @property
-    def tuning(self) -> tuple[int, int]:
-        cap, sc = C.c_uint32(), C.c_uint32()
-        check(lib().fpt_batch_get_tuning(self._h, C.byref(cap), C.byref(sc)))
-        return int(cap.value), int(sc.value)
+    def tuning(self) -> tuple[int, int, int]:
+        """(wave capacity, shade grid scale, fetch chunk)."""
+        t = _ffi.fpt_batch_tuning()
+        check(lib().fpt_batch_get_tuning_ex(self._h, C.byref(t)))
+        return int(t.wave_capacity), int(t.shade_grid_scale), int(t.fetch_chunk)
 
-    def autotune(self) -> tuple[int, int]:
+    def autotune(self) -> tuple[int, int, int]:
         check(lib().fpt_batch_autotune(self._h, C.c_void_p(_stream())))
         return self.tuning
 

@@ -59,6 +59,7 @@ struct fpt_batch {
     // tuning
     uint32_t capacity = 1u << 24;
     int shadeScale = 1;
+    uint32_t fetchChunk = 0;                 // 0: the kernels' default
     bool tuned = false;
     // device state of the batched launch
     DevScene* scenesDev = nullptr;           // one per frame
@@ -172,6 +173,7 @@ fpt_status build_batch(fpt_batch& b, cudaStream_t st) {
     bd.tiles = b.tilesDev;
     bd.slotTile = b.slotTile;
     bd.counters = b.counters;
+    bd.fetchChunk = b.fetchChunk;
     uint32_t launches = 0;
     if ((e = cudaStreamBeginCapture(b.capStream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return cuda_fail("capture", e);
     cudaError_t le = cudaSuccess;
@@ -304,6 +306,25 @@ FPT_API fpt_status fpt_batch_get_tuning(const fpt_batch* b, uint32_t* wave_capac
     return FPT_OK;
 }
 
+FPT_API fpt_status fpt_batch_set_tuning_ex(fpt_batch* b, const fpt_batch_tuning* t) {
+    if (!b || !t) return set_error(FPT_ERR_INVALID_ARG, "fpt_batch_set_tuning_ex: null argument");
+    if (t->fetch_chunk && (t->fetch_chunk > 1024 || (t->fetch_chunk & 31u)))
+        return set_error(FPT_ERR_INVALID_ARG, "fpt_batch_set_tuning_ex: fetch_chunk must be a multiple of 32 up to 1024");
+    if (t->wave_capacity) b->capacity = std::max<uint32_t>(t->wave_capacity, kFrameSpp);
+    if (t->shade_grid_scale) b->shadeScale = int(std::min<uint32_t>(t->shade_grid_scale, 8));
+    b->fetchChunk = t->fetch_chunk;
+    b->free_device();
+    return FPT_OK;
+}
+
+FPT_API fpt_status fpt_batch_get_tuning_ex(const fpt_batch* b, fpt_batch_tuning* t) {
+    if (!b || !t) return set_error(FPT_ERR_INVALID_ARG, "fpt_batch_get_tuning_ex: null argument");
+    t->wave_capacity = b->capacity;
+    t->shade_grid_scale = uint32_t(b->shadeScale);
+    t->fetch_chunk = b->fetchChunk ? b->fetchChunk : 32u;
+    return FPT_OK;
+}
+
 FPT_API fpt_status fpt_batch_autotune(fpt_batch* b, void* stream) {
     if (!b || b->reqs.empty()) return set_error(FPT_ERR_INVALID_ARG, "fpt_batch_autotune: empty batch");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -331,10 +352,26 @@ FPT_API fpt_status fpt_batch_autotune(fpt_batch* b, void* stream) {
             if (s == FPT_OK && ms < best) { best = ms; bestCap = cap; bestScale = sc; }
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    // Then the queue depth per warp claim at the best capacity and grid.
     b->capacity = bestCap;
     b->shadeScale = bestScale;
+    uint32_t bestChunk = b->fetchChunk;
+    for (uint32_t chunk : {32u, 64u, 128u}) {
+        b->fetchChunk = chunk;
+        b->free_device();
+        fpt_status s = run_batched(*b, st);
+        if (s != FPT_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return s; }
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 2 && s == FPT_OK; r++) s = run_batched(*b, st);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (s == FPT_OK && ms < best) { best = ms; bestChunk = chunk; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->fetchChunk = bestChunk;
     b->free_device();
     b->tuned = true;
     return FPT_OK;

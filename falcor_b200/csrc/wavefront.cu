@@ -457,6 +457,7 @@ cudaError_t run_batch(const BatchDevice& bd, const std::vector<BatchWave>& waves
     launches = 0;
     for (const BatchWave& wv : waves) {
         WaveParams wp{};
+        wp.fetchChunk = bd.fetchChunk;
         wp.waveFirstPixel = 0;
         wp.wavePixels = wv.pixels;
         wp.wavePaths = wv.paths;

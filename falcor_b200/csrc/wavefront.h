@@ -95,6 +95,7 @@ struct BatchDevice {
     const BatchTile* tiles = nullptr;
     uint32_t* slotTile = nullptr;
     unsigned long long* counters = nullptr;
+    uint32_t fetchChunk = 0;     // trace-kernel queue entries per warp claim (0: default)
 };
 // Enqueues every wave of the batch (uniform sample generator type and
 // transmission variant across requests); shadeScale multiplies the shade grid.

@@ -45,6 +45,8 @@ struct WaveParams {
     const BatchTile* tiles;
     uint32_t tileCount;
     uint32_t* slotTile;
+    // Queue entries a warp of the trace kernels claims per atomic (0: kFetchChunk).
+    uint32_t fetchChunk;
 };
 
 // Request of wave slot i in a batched wave.
@@ -181,10 +183,11 @@ FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams
         if (idle && !drained) {
             if (chunkNext >= chunkEnd) {
                 uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(fetch, kFetchChunk);
+                const uint32_t chunk = wp.fetchChunk ? wp.fetchChunk : kFetchChunk;
+                if (lane == 0) base = atomicAdd(fetch, chunk);
                 base = __shfl_sync(0xffffffffu, base, 0);
                 if (base >= n) drained = true;
-                else { chunkNext = base; chunkEnd = min(base + kFetchChunk, n); }
+                else { chunkNext = base; chunkEnd = min(base + chunk, n); }
             }
             if (!drained) {
                 const uint32_t avail = chunkEnd - chunkNext;

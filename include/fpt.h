@@ -605,8 +605,20 @@ FPT_API fpt_status fpt_batch_add(fpt_batch* batch, const fpt_batch_request* req)
  * occupancy-sized shade grid; 0 keeps the current value. */
 FPT_API fpt_status fpt_batch_set_tuning(fpt_batch* batch, uint32_t wave_capacity, uint32_t shade_grid_scale);
 FPT_API fpt_status fpt_batch_get_tuning(const fpt_batch* batch, uint32_t* wave_capacity, uint32_t* shade_grid_scale);
+/* All tuning knobs of the batched launch; 0 keeps the current value, except
+ * fetch_chunk where 0 restores the kernels' default (32).  fetch_chunk: queue
+ * entries a warp of the traversal kernels claims per atomic (a multiple of
+ * 32, at most 1024). */
+typedef struct fpt_batch_tuning {
+    uint32_t wave_capacity;
+    uint32_t shade_grid_scale;
+    uint32_t fetch_chunk;
+} fpt_batch_tuning;
+FPT_API fpt_status fpt_batch_set_tuning_ex(fpt_batch* batch, const fpt_batch_tuning* tuning);
+FPT_API fpt_status fpt_batch_get_tuning_ex(const fpt_batch* batch, fpt_batch_tuning* tuning);
 /* Times the batched launch over wave capacities 2^21..2^25 and shade grid
- * scales 1, 2 on the current requests and keeps the fastest. */
+ * scales 1, 2 on the current requests, then traversal fetch chunks 32, 64 and
+ * 128 at the best of those, and keeps the fastest. */
 FPT_API fpt_status fpt_batch_autotune(fpt_batch* batch, void* stream);
 /* All requests as one CUDA graph (built on first call, relaunched after):
  * V-buffers, then waves that pack whole pixel tiles of several requests

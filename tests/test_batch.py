@@ -39,8 +39,23 @@ def test_batched_equals_sequential(fpt):
     st = b.stats()
     assert st.device_error == 0
     assert st.paths > 0
+    # Every traversal fetch chunk (queue entries per warp claim) renders the
+    # same images; invalid chunks are refused.
+    from falcor_b200 import _ffi
+    for chunk in (64, 128):
+        b.set_tuning(fetch_chunk=chunk)
+        assert b.tuning[2] == chunk
+        for o in outs:
+            o.zero_()
+        b.launch()
+        torch.cuda.synchronize()
+        for i, o in enumerate(outs):
+            assert np.array_equal(o.cpu().numpy(), seq[i]), (chunk, i)
+    with pytest.raises(_ffi.FptError):
+        b.set_tuning(fetch_chunk=48)
     # The autotuned configuration renders the same images.
     b.autotune()
+    assert b.tuning[2] in (32, 64, 128)
     for o in outs:
         o.zero_()
     b.launch()
