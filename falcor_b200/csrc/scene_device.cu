@@ -147,14 +147,29 @@ DevMaterial pack_material(const fpt_material& s0, uint32_t baseColorTexture) {
     return o;
 }
 
-fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
-    int devCount = 0;
-    if (cudaGetDeviceCount(&devCount) != cudaSuccess || devCount == 0)
-        return set_error(FPT_ERR_NO_DEVICE, "fpt_scene_create: no CUDA device");
+// Host-side checks of a scene description, before any device work: the
+// arrays exist, positions are finite and within |x| <= 1e15 (the traversal's
+// conservative box test needs |coordinate| * |1/d| to stay finite), every
+// index, material and texture reference is in range.
+fpt_status validate_desc(const fpt_scene_desc& d) {
     if (d.vertex_count && !d.vertices) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: vertices is NULL");
     if (d.index_count && !d.indices) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: indices is NULL");
     if (d.instance_count && !d.instances) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: instances is NULL");
     if (d.material_count == 0 || !d.materials) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: no materials");
+    for (uint32_t i = 0; i < d.vertex_count; i++)
+        for (int a = 0; a < 3; a++)
+            if (!(std::fabs(d.vertices[i].position[a]) <= 1e15f))
+                return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: vertex " + std::to_string(i) +
+                                                          " has a non-finite or out-of-range (|x| > 1e15) position");
+    for (uint32_t i = 0; i < d.instance_count; i++) {
+        const fpt_geometry_instance& in = d.instances[i];
+        if (in.material_id >= d.material_count) return set_error(FPT_ERR_INVALID_ARG, "instance material_id out of range");
+        if (uint64_t(in.ib_offset) + uint64_t(in.triangle_count) * 3 > d.index_count)
+            return set_error(FPT_ERR_INVALID_ARG, "instance index range out of bounds");
+        for (uint64_t k = 0; k < uint64_t(in.triangle_count) * 3; k++)
+            if (uint64_t(d.indices[in.ib_offset + k]) + in.vb_offset >= d.vertex_count)
+                return set_error(FPT_ERR_INVALID_ARG, "vertex index out of bounds");
+    }
     if (d.texture_count && !d.textures) return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: textures is NULL");
     for (uint32_t t = 0; t < d.texture_count; t++) {
         const fpt_texture_desc& td = d.textures[t];
@@ -166,15 +181,15 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
         for (uint32_t m = 0; m < d.material_count; m++)
             if (d.base_color_textures[m] > d.texture_count)
                 return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: material " + std::to_string(m) + " names a missing texture");
-    // The traversal's conservative box test needs |coordinate| * |1/d| to
-    // stay finite (|1/d| <= 1e20): positions are limited to |x| <= 1e15.
-    for (uint32_t i = 0; i < d.vertex_count; i++)
-        for (int a = 0; a < 3; a++) {
-            const float x = d.vertices[i].position[a];
-            if (!(std::fabs(x) <= 1e15f))
-                return set_error(FPT_ERR_INVALID_ARG, "fpt_scene_create: vertex " + std::to_string(i) +
-                                                          " has a non-finite or out-of-range (|x| > 1e15) position");
-        }
+    return FPT_OK;
+}
+
+fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
+    const fpt_status vs = validate_desc(d);
+    if (vs != FPT_OK) return vs;
+    int devCount = 0;
+    if (cudaGetDeviceCount(&devCount) != cudaSuccess || devCount == 0)
+        return set_error(FPT_ERR_NO_DEVICE, "fpt_scene_create: no CUDA device");
     auto sc = std::make_unique<fpt_scene>();
     fpt_scene& s = *sc;
     compute_camera(d.camera, s.info.camera);

@@ -87,8 +87,32 @@ struct SceneArrays {
     std::vector<fpt_material> materials;
     std::vector<float> envRGB;
     fpt_envmap_desc env{};
+    std::vector<std::vector<uint8_t>> texels;     // base-colour textures
+    std::vector<fpt_texture_desc> textures;
+    std::vector<uint32_t> baseColorTextures;      // per material: 1 + texture index, or 0
     fpt_scene_desc desc{};
 };
+
+// A StandardMaterial base-colour texture as fpt texels (mip 0); formats
+// other than RGBA8 (sRGB or linear) and RGBA32Float are left out with a warning.
+uint32_t addBaseColorTexture(RenderContext* pRenderContext, const ref<Texture>& pTex, SceneArrays& out) {
+    uint32_t format;
+    switch (pTex->getFormat()) {
+        case ResourceFormat::RGBA8UnormSrgb: format = FPT_TEXTURE_RGBA8_UNORM_SRGB; break;
+        case ResourceFormat::RGBA8Unorm: format = FPT_TEXTURE_RGBA8_UNORM; break;
+        case ResourceFormat::RGBA32Float: format = FPT_TEXTURE_RGBA32_FLOAT; break;
+        default:
+            logWarning("FalcorB200: base-colour texture format not supported; the material uses its uniform base colour.");
+            return 0;
+    }
+    out.texels.push_back(pRenderContext->readTextureSubresource(pTex.get(), 0));
+    fpt_texture_desc d{};
+    d.width = pTex->getWidth();
+    d.height = pTex->getHeight();
+    d.format = format;
+    out.textures.push_back(d);
+    return uint32_t(out.textures.size());
+}
 
 fpt_material makeMaterial(const ref<Material>& pMaterial) {
     fpt_material m{};
@@ -171,6 +195,9 @@ void makeDescFromScene(RenderContext* pRenderContext, const ref<Device>& pDevice
         const float4x4& M = matrices[gi.globalMatrixID];
         const float3x3 N = float3x3(transpose(inverse(M)));
         const float3x3 T = float3x3(M);
+        // Static meshes are pre-transformed (identity matrix): their vertex data
+        // is passed on bit for bit.
+        const bool identity = M == float4x4::identity();
 
         fpt_geometry_instance inst{};
         inst.vb_offset = uint32_t(out.vertices.size());
@@ -180,9 +207,9 @@ void makeDescFromScene(RenderContext* pRenderContext, const ref<Device>& pDevice
         inst.flags = 0;
         for (uint32_t v = 0; v < nv; v++) {
             fpt_vertex x{};
-            const float3 p = transformPoint(M, pos[v]);
-            const float3 n = normalize(mul(N, nrm[v]));
-            const float3 t = mul(T, tan[v].xyz());
+            const float3 p = identity ? pos[v] : transformPoint(M, pos[v]);
+            const float3 n = identity ? nrm[v] : normalize(mul(N, nrm[v]));
+            const float3 t = identity ? tan[v].xyz() : mul(T, tan[v].xyz());
             x.position[0] = p.x, x.position[1] = p.y, x.position[2] = p.z;
             x.normal[0] = n.x, x.normal[1] = n.y, x.normal[2] = n.z;
             x.tangent[0] = t.x, x.tangent[1] = t.y, x.tangent[2] = t.z, x.tangent[3] = tan[v].w;
@@ -196,7 +223,14 @@ void makeDescFromScene(RenderContext* pRenderContext, const ref<Device>& pDevice
         }
         out.instances.push_back(inst);
     }
-    for (uint32_t m = 0; m < pScene->getMaterialCount(); m++) out.materials.push_back(makeMaterial(pScene->getMaterial(MaterialID(m))));
+    for (uint32_t m = 0; m < pScene->getMaterialCount(); m++) {
+        const ref<Material> pMaterial = pScene->getMaterial(MaterialID(m));
+        out.materials.push_back(makeMaterial(pMaterial));
+        uint32_t tex = 0;
+        if (auto pStd = dynamic_ref_cast<StandardMaterial>(pMaterial))
+            if (const ref<Texture> pTex = pStd->getBaseColorTexture()) tex = addBaseColorTexture(pRenderContext, pTex, out);
+        out.baseColorTextures.push_back(tex);
+    }
 
     const ref<Camera>& pCamera = pScene->getCamera();
     fpt_camera& c = out.desc.camera;
@@ -242,6 +276,10 @@ void makeDescFromScene(RenderContext* pRenderContext, const ref<Device>& pDevice
     out.desc.instance_count = uint32_t(out.instances.size());
     out.desc.materials = out.materials.data();
     out.desc.material_count = uint32_t(out.materials.size());
+    for (size_t t = 0; t < out.textures.size(); t++) out.textures[t].texels = out.texels[t].data();
+    out.desc.textures = out.textures.empty() ? nullptr : out.textures.data();
+    out.desc.texture_count = uint32_t(out.textures.size());
+    out.desc.base_color_textures = out.textures.empty() ? nullptr : out.baseColorTextures.data();
 }
 
 }  // namespace

@@ -72,6 +72,9 @@ struct float4 {
 };
 struct float4x4 {
     float m[4][4] = {{1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};  // row-major, column vectors
+    static float4x4 identity() { return float4x4(); }
+    // matrix::operator== (Utils/Math/MatrixTypes.h:167): bitwise.
+    bool operator==(const float4x4& o) const { return std::memcmp(m, o.m, sizeof(m)) == 0; }
 };
 struct float3x3 {
     float m[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
@@ -124,7 +127,7 @@ inline float3 normalize(const float3& v) {
 }
 
 // ----- Core/API: formats, flags, resources ---------------------------------------
-enum class ResourceFormat { Unknown, RGBA32Float, RGBA32Uint, RG32Float, R32Float, R32Uint };
+enum class ResourceFormat { Unknown, RGBA32Float, RGBA32Uint, RG32Float, R32Float, R32Uint, RGBA8Unorm, RGBA8UnormSrgb };
 inline bool isIntegerFormat(ResourceFormat f) { return f == ResourceFormat::RGBA32Uint || f == ResourceFormat::R32Uint; }
 inline uint32_t getFormatBytesPerBlock(ResourceFormat f) {
     switch (f) {
@@ -404,6 +407,9 @@ public:
     float getSpecularTransmission() const { return specTrans; }
     float getDiffuseTransmission() const { return diffTrans; }
     float3 getTransmissionColor() const { return transmission; }
+    // BasicMaterial::getBaseColorTexture (Scene/Material/BasicMaterial.h).
+    ref<Texture> getBaseColorTexture() const { return baseColorTexture; }
+    ref<Texture> baseColorTexture;
     float4 baseColor, specular;
     float3 emissive, transmission;
     float emissiveFactor = 1.f, specTrans = 0.f, diffTrans = 0.f;

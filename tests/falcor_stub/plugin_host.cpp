@@ -4,7 +4,10 @@
 // channels in textures.  The scene is a procedural workload scene
 // (fpt_procedural_scene) copied into the stand-in Falcor Scene.
 //
-// Usage: plugin_host <out.bin> <width> <height>
+// Usage: plugin_host <out.bin> <width> <height> [textured]
+// With "textured", materials m % 4 == 1 take their base colour from a 32x16
+// RGBA8UnormSrgb texture and materials m % 4 == 2 from an 8x8 RGBA32Float one
+// (texels: plugin_texels below).
 // Writes to out.bin the VBufferRT vbuffer (uint4 per pixel), the PathTracer
 // colour and the MinimalPathTracer colour (float4 per pixel); prints the
 // reflected channels and the PathTracer properties.
@@ -62,9 +65,26 @@ void registerPrograms() {
     };
 }
 
+// The two test textures: byte (x * 37 + y * 11 + c * 53) & 255, and float
+// ((x + 1) * (c + 1) % 7) / 7 + y / 64.
+ref<Texture> makeTexture(const ref<Device>& device, bool srgb8) {
+    const uint32_t W = srgb8 ? 32 : 8, H = srgb8 ? 16 : 8;
+    auto t = device->createTexture2D(W, H, srgb8 ? ResourceFormat::RGBA8UnormSrgb : ResourceFormat::RGBA32Float);
+    std::vector<uint8_t> b(size_t(W) * H * 4);
+    std::vector<float> f(size_t(W) * H * 4);
+    for (uint32_t y = 0; y < H; y++)
+        for (uint32_t x = 0; x < W; x++)
+            for (uint32_t c = 0; c < 4; c++) {
+                b[(size_t(y) * W + x) * 4 + c] = uint8_t((x * 37 + y * 11 + c * 53) & 255);
+                f[(size_t(y) * W + x) * 4 + c] = float((x + 1) * (c + 1) % 7) / 7.f + float(y) / 64.f;
+            }
+    upload(*t, srgb8 ? static_cast<const void*>(b.data()) : static_cast<const void*>(f.data()));
+    return t;
+}
+
 // A Falcor scene holding a procedural workload scene (one mesh per fpt
 // instance, identity transforms, StandardMaterials, camera, env map).
-ref<Scene> makeScene(const ref<Device>& device, const fpt_scene_desc& d) {
+ref<Scene> makeScene(const ref<Device>& device, const fpt_scene_desc& d, bool textured) {
     auto s = make_ref<Scene>();
     s->animation.globalMatrices.push_back(float4x4());
     for (uint32_t i = 0; i < d.vertex_count; i++) {
@@ -105,6 +125,14 @@ ref<Scene> makeScene(const ref<Device>& device, const fpt_scene_desc& d) {
         sm->doubleSided = (m.flags & FPT_MATERIAL_DOUBLE_SIDED) != 0;
         sm->thinSurface = (m.flags & FPT_MATERIAL_THIN_SURFACE) != 0;
         s->materials.push_back(sm);
+    }
+    if (textured) {
+        const ref<Texture> t8 = makeTexture(device, true), t32 = makeTexture(device, false);
+        for (size_t i = 0; i < s->materials.size(); i++) {
+            auto sm = std::dynamic_pointer_cast<StandardMaterial>(s->materials[i]);
+            if (i % 4 == 1) sm->baseColorTexture = t8;
+            if (i % 4 == 2) sm->baseColorTexture = t32;
+        }
     }
     auto cam = make_ref<Camera>();
     const fpt_camera& c = d.camera;
@@ -162,7 +190,8 @@ int main(int argc, char** argv) {
         pp.aspect_ratio = float(W) / float(H);
         fpt_scene_host* host = nullptr;
         if (fpt_procedural_scene(&pp, &host) != FPT_OK) FALCOR_THROW("fpt_procedural_scene: {}", fpt_last_error());
-        ref<Scene> scene = makeScene(device, *fpt_scene_host_desc(host));
+        const bool textured = argc > 4 && std::string(argv[4]) == "textured";
+        ref<Scene> scene = makeScene(device, *fpt_scene_host_desc(host), textured);
 
         Properties vbProps;
         ref<RenderPass> vb = RenderPass::create("VBufferRT", device, vbProps);

@@ -219,3 +219,50 @@ def test_oracle_traverses_library_bvh8_with_identical_hits(fpt, oracle):
     # A strided sample covers every stride^2-th pixel.
     c2, _ = osc.path_tracer_counts(vb, H.pt_params(W, Hh, 4, seed=3, max_bounces=4), stride=4)
     assert 0 < c2.paths <= cnt.paths // 8
+
+
+def test_scene_descriptions_are_validated_on_the_host(fpt):
+    """fpt_scene_create refuses bad host input before any device work
+    (FPT_ERR_INVALID_ARG, no GPU needed): non-finite or out-of-range
+    positions, vertex indices, material IDs and texture references out of
+    range, bad texture descriptors."""
+    import copy
+    from falcor_b200 import _ffi
+    from falcor_b200.scene import HostScene
+    from tests import helpers as H
+    base = H.box_icosphere(2)
+    d = base.desc
+    cam = {name: (list(getattr(d.camera, name)) if not isinstance(getattr(d.camera, name), float) else getattr(d.camera, name))
+           for name, _ in d.camera._fields_}
+    V, I, N, M = base.vertices.copy(), base.indices.copy(), base.instances.copy(), base.materials.copy()
+
+    def create(v=V, i=I, n=N, m=M, **kw):
+        hs = HostScene.from_arrays(v, i, n, m, cam, **kw)
+        h = C.c_void_p()
+        st = fpt.fpt_scene_create(C.byref(hs.desc), C.byref(h))
+        if st == 0:
+            fpt.fpt_scene_destroy(h)
+        return st, fpt.fpt_last_error().decode()
+
+    ok, _ = create()
+    assert ok in (0, 8)  # created, or no CUDA device on this machine
+    for what, val in (("nan", np.nan), ("inf", np.inf), ("huge", 2e15)):
+        v = V.copy()
+        v[7, 1] = val
+        st, msg = create(v=v)
+        assert st == 1 and "vertex 7" in msg, (what, st, msg)
+    i = I.copy()
+    i[5] = 10**6
+    assert create(i=i)[0] == 1
+    n = N.copy()
+    n[3, 3] = len(M)  # material ID out of range
+    assert create(n=n)[0] == 1
+    n = N.copy()
+    n[2, 2] = 10**6  # triangle count past the index buffer
+    assert create(n=n)[0] == 1
+    tex = [np.zeros((4, 4, 4), np.uint8)]
+    assert create(textures=tex, base_color_textures=[0] + [-1] * (len(M) - 1))[0] in (0, 8)
+    st, msg = create(textures=tex, base_color_textures=[3] + [-1] * (len(M) - 1))
+    assert st == 1 and "missing texture" in msg
+    with pytest.raises(ValueError):
+        create(textures=[np.zeros((4, 4, 3), np.uint8)], base_color_textures=[0] * len(M))

@@ -119,3 +119,37 @@ def test_frame_limits(fpt):
     pt.execute({"vbuffer": vb, "color": out})
     torch.cuda.synchronize()
     assert pt.stats().device_error == 0
+
+
+@pytest.mark.gpu
+def test_degenerate_triangles_render_like_the_oracle(fpt, oracle):
+    """Zero-area triangles (coincident and collinear vertices) next to a real
+    one: the watertight test never reports them as hits, the BVH builder keeps
+    them, no device error is raised, and the frame equals the oracle's."""
+    from falcor_b200.scene import HostScene, Scene
+    v = np.zeros((9, 12), np.float32)
+    v[0:3, 0:3] = [[-1, -1, 0], [1, -1, 0], [0, 1, 0]]
+    v[3:6, 0:3] = [[0.2, 0.1, 0.5], [0.2, 0.1, 0.5], [0.2, 0.1, 0.5]]    # one point
+    v[6:9, 0:3] = [[-0.5, 0.0, 0.3], [0.0, 0.0, 0.3], [0.5, 0.0, 0.3]]   # a segment
+    v[:, 3:6] = [0, 0, 1]
+    v[:, 6:10] = [1, 0, 0, 1]
+    mat = np.zeros((1, 19), np.float32)
+    mat[0, 0:4] = [0.7, 0.5, 0.3, 1]
+    mat[0, 4:8] = [0, 0.6, 0, 0]
+    mat[0, 8:11] = [2, 2, 2]
+    mat[0, 11] = 1.0
+    mat[0, 12] = 1.5
+    idx = np.array([0, 1, 2, 0, 1, 2, 0, 1, 2], np.uint32)
+    inst = np.array([[0, 0, 1, 0, 0], [3, 3, 1, 0, 0], [6, 6, 1, 0, 0]], np.uint32)
+    host = HostScene.from_arrays(v, idx, inst, mat, CAM, envmap={"rgb": np.full((8, 16, 3), 0.25, np.float32)})
+    s = Scene(host)
+    vb, got, st = render_pt(s, 40, 40)
+    assert st.device_error == 0
+    hit_inst = vb.view(np.uint32)[..., 0]
+    assert np.any(hit_inst != 0)
+    osc = H.oracle_scene(host)
+    ovb = osc.vbuffer(40, 40)
+    assert np.array_equal(vb.view(np.uint32), ovb)
+    ref, _, _, _ = osc.path_tracer(ovb, H.pt_params(40, 40, 4, seed=1, max_bounces=3))
+    ok = H.rel_close(got[..., :3], ref[..., :3], rtol=1e-4).all(axis=-1)
+    assert ok.all(), f"{int((~ok).sum())} pixels differ"

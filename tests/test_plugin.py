@@ -48,8 +48,32 @@ def test_plugin_compiles_against_falcor_api(fpt, tmp_path):
     assert exe.exists()
 
 
+def _plugin_textures():
+    """The textures plugin_host gives materials m % 4 == 1 and m % 4 == 2."""
+    y, x, c = np.meshgrid(np.arange(16), np.arange(32), np.arange(4), indexing="ij")
+    t8 = ((x * 37 + y * 11 + c * 53) & 255).astype(np.uint8)
+    y, x, c = np.meshgrid(np.arange(8), np.arange(8), np.arange(4), indexing="ij")
+    t32 = (((x + 1) * (c + 1) % 7).astype(np.float32) / np.float32(7.0) + y.astype(np.float32) / np.float32(64.0)).astype(np.float32)
+    return [t8, t32]
+
+
+def _textured_copy(host):
+    from falcor_b200.scene import HostScene
+    d = host.desc
+    cam = {n: (list(getattr(d.camera, n)) if not isinstance(getattr(d.camera, n), float) else getattr(d.camera, n))
+           for n, _ in d.camera._fields_}
+    e = d.envmap.contents
+    env = {"rgb": np.ctypeslib.as_array(e.rgb, shape=(e.height * e.width * 3,)).reshape(e.height, e.width, 3).copy(),
+           "tint": list(e.tint), "intensity": e.intensity}
+    nm = d.material_count
+    bct = [0 if m % 4 == 1 else (1 if m % 4 == 2 else -1) for m in range(nm)]
+    return HostScene.from_arrays(host.vertices.copy(), host.indices.copy(), host.instances.copy(), host.materials.copy(), cam, env,
+                                 textures=_plugin_textures(), base_color_textures=bct)
+
+
 @pytest.mark.gpu
-def test_plugin_passes_render_like_the_library(fpt, tmp_path):
+@pytest.mark.parametrize("textured", [False, True])
+def test_plugin_passes_render_like_the_library(fpt, tmp_path, textured):
     import torch
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
@@ -58,7 +82,8 @@ def test_plugin_passes_render_like_the_library(fpt, tmp_path):
     W, Hh = 64, 48
     exe = _build(tmp_path)
     out = tmp_path / "out.bin"
-    res = subprocess.run([str(exe), str(out), str(W), str(Hh)], capture_output=True, text=True, timeout=300)
+    res = subprocess.run([str(exe), str(out), str(W), str(Hh)] + (["textured"] if textured else []), capture_output=True, text=True,
+                         timeout=300)
     assert res.returncode == 0, res.stdout + res.stderr
     log = res.stdout
     assert "reflect PathTracer: in:vbuffer in:viewW? out:color out:rayCount? out:pathLength?" in log, log
@@ -71,6 +96,8 @@ def test_plugin_passes_render_like_the_library(fpt, tmp_path):
     mpt_plugin = data[2 * n:3 * n].view(np.float32).reshape(Hh, W, 4)
 
     host = H.small_heightfield()  # the scene plugin_host builds (heightfield + soup, env map, 4:3)
+    if textured:
+        host = _textured_copy(host)
     scene = Scene(host)
     vb = H.gpu_vbuffer(scene, W, Hh)
     np.testing.assert_array_equal(vb.cpu().numpy().view(np.uint32), vb_plugin)
