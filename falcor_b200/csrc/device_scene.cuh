@@ -538,21 +538,6 @@ FPT_D ShadingData load_shading_data(const DevScene& s, const HitRec& hit, float3
     return sd;
 }
 
-// Interpolated texture coordinate of a triangle hit (getVertexData's texC,
-// Scene.slang) for code that has the hit but not its ShadingData.
-FPT_D float2 hit_uv(const DevScene& s, uint32_t instanceID, uint32_t primIndex, float bx, float by) {
-    const DevInstance inst = s.instances[instanceID];
-    const uint32_t* ip = s.indices + inst.ibOffset + primIndex * 3;
-    const float b0 = 1.f - bx - by;
-    const PackedVertex v0 = load_vertex(s.vertices, __ldg(ip) + inst.vbOffset);
-    const PackedVertex v1 = load_vertex(s.vertices, __ldg(ip + 1) + inst.vbOffset);
-    const PackedVertex v2 = load_vertex(s.vertices, __ldg(ip + 2) + inst.vbOffset);
-    float2 uv = make_float2(v0.uv[0] * b0, v0.uv[1] * b0);
-    uv.x += v1.uv[0] * bx; uv.y += v1.uv[1] * bx;
-    uv.x += v2.uv[0] * by; uv.y += v2.uv[1] * by;
-    return uv;
-}
-
 // ---------------------------------------------------------------------------
 // Base-colour textures: MaterialSystem::sampleTexture with
 // ExplicitLodTextureSampler(0) (MaterialSystem.slang:308-320), bilinear at mip 0

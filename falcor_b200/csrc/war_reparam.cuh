@@ -587,6 +587,7 @@ FPT_D float2 war_camera_sample(const WarParams& p, uint32_t x, uint32_t y, Unifo
 // One path vertex as the reverse sweep sees it (both schedulers).
 struct WarSweepVertex {
     float3 wiL, wsL, thp, bw, e;
+    float2 uv;                 // texture coordinate of the hit (textured base colours)
     float pdf;
     uint32_t matID, flags;     // flags: 1 front facing, 2 scattered with a valid evaluation
     // WAR only:
@@ -630,8 +631,7 @@ FPT_D void war_sweep_vertex(const DevScene& s, const WarParams& p, uint32_t pid,
     } else {
         sd.frontFacing = (v.flags & 1u) != 0;
         sd.materialID = v.matID;
-        sd.uv = make_float2(0.f, 0.f);
-        if (evalGrad && material_base_texture(s, v.matID) != ~0u) sd.uv = hit_uv(s, v.inst, v.prim, v.b[1], v.b[2]);
+        sd.uv = v.uv;
     }
     if (evalGrad) {
         const MatParams mp = load_mat_params(s, v.matID, sd.uv);

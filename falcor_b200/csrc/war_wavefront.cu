@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_shade(DevSc
             rec_at(ww, vk, 0, i) = make_float4(0.f, 0.f, 0.f, 1.f);  // wiL, pdf
             rec_at(ww, vk, 1, i) = make_float4(0.f, 0.f, 0.f, __uint_as_float(sd.materialID));
             rec_at(ww, vk, 2, i) = make_float4(thp.x, thp.y, thp.z, __uint_as_float(sd.frontFacing ? 1u : 0u));
-            rec_at(ww, vk, 3, i) = make_float4(0.f, 0.f, 0.f, 0.f);  // bw
+            rec_at(ww, vk, 3, i) = make_float4(0.f, 0.f, 0.f, sd.uv.x);  // bw, texture coordinate x
             if (WAR) {
                 rec_at(ww, vk, 5, i) = make_float4(rayDir.x, rayDir.y, rayDir.z, __uint_as_float(is.inst));
                 rec_at(ww, vk, 6, i) = make_float4(0.f, 0.f, 0.f, __uint_as_float(is.prim));
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_shade(DevSc
                     rec_at(ww, vk, 1, i) = make_float4(wsL.x, wsL.y, wsL.z, __uint_as_float(sd.materialID));
                     rec_at(ww, vk, 2, i) = make_float4(thp.x, thp.y, thp.z,
                                                        __uint_as_float((sd.frontFacing ? 1u : 0u) | (valid ? 2u : 0u)));
-                    rec_at(ww, vk, 3, i) = make_float4(bsdfWeight.x, bsdfWeight.y, bsdfWeight.z, 0.f);
+                    rec_at(ww, vk, 3, i) = make_float4(bsdfWeight.x, bsdfWeight.y, bsdfWeight.z, sd.uv.x);
                     if (WAR) {
                         rec_at(ww, vk, 6, i) = make_float4(wo.x, wo.y, wo.z, __uint_as_float(is.prim));
                         store_sg(as_u4(rec_at(ww, vk, 7, i)), sg);
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_shade(DevSc
             }
         }
         push(shadowRay, i, wp.shadowQueue, wp.counts + 2);
-        if (BWD) rec_at(ww, vk, 4, i) = make_float4(e.x, e.y, e.z, 0.f);
+        if (BWD) rec_at(ww, vk, 4, i) = make_float4(e.x, e.y, e.z, sd.uv.y);  // radiance increment, texture coordinate y
         if (BWD && vk + 1 >= ww.maxVertices) cont = false;  // guarded by the host
         w.thpB[i] = make_float4(thp.x, thp.y, thp.z, __uint_as_float(pathLen));
         w.L[i] = make_float4(radiance.x, radiance.y, radiance.z, 0.f);
@@ -432,8 +432,10 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_sweep(DevSc
                 v.matID = __float_as_uint(r1.w);
                 v.thp = xyz(r2);
                 v.flags = __float_as_uint(r2.w);
-                v.bw = xyz(rec_at(ww, k, 3, i));
-                v.e = xyz(rec_at(ww, k, 4, i));
+                const float4 r3 = rec_at(ww, k, 3, i), r4 = rec_at(ww, k, 4, i);
+                v.bw = xyz(r3);
+                v.e = xyz(r4);
+                v.uv = make_float2(r3.w, r4.w);
                 if (WAR) {
                     const float4 r5 = rec_at(ww, k, 5, i), r6 = rec_at(ww, k, 6, i), r8 = rec_at(ww, k, 8, i), r9 = rec_at(ww, k, 9, i);
                     v.inDir = xyz(r5);

@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(kWarBlock) war_kernel(DevScene s, WarParams p)
                     vr->pdf = 1.f;
                     vr->flags = sd.frontFacing ? 1u : 0u;
                     vr->matID = sd.materialID;
+                    vr->uv = sd.uv;
                     if (WAR) {
                         vr->inDir = rayDir;
                         vr->outDir = vr->gV = f3(0.f);
