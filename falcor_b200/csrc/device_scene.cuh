@@ -217,13 +217,47 @@ FPT_D AxisPlanes axis_planes(float p, float s, float o, float inv, uint32_t lo0,
     return a;
 }
 
+// Three-input float min / max (PTX min.f32 / max.f32 with three operands,
+// sm_100): one instruction where two two-input ones would run.  Exact like
+// fminf / fmaxf; the slab distances are never NaN (|1/d| is clamped).
+#ifndef FPT_MINMAX3
+#define FPT_MINMAX3 1
+#endif
+FPT_D float fmax3(float a, float b, float c) {
+#if FPT_MINMAX3
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+#else
+    return fmaxf(fmaxf(a, b), c);
+#endif
+}
+FPT_D float fmin3(float a, float b, float c) {
+#if FPT_MINMAX3
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+#else
+    return fminf(fminf(a, b), c);
+#endif
+}
+
 // Visits one node: tests its 8 child boxes against [tMin, tBest].  Returns
 // the hit internal children as a group (octant order) and the triangles of
 // the hit leaf children as a bit mask relative to the node's triangle base.
+// `top` (shared memory, may be null) holds the first `topCount` nodes of the
+// tree (breadth-first order: its top levels), which are read from there.
 FPT_D void visit_node(const DevScene& s, const TraceRay& r, float tBest, uint32_t nodeIdx, uint32_t& innerHits,
-                      uint32_t& childBase, uint32_t& imask, uint32_t& triBase, uint32_t& triHits) {
-    const uint4* np = s.nodes + size_t(nodeIdx) * 5;
-    const uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+                      uint32_t& childBase, uint32_t& imask, uint32_t& triBase, uint32_t& triHits, const uint4* top = nullptr,
+                      uint32_t topCount = 0) {
+    uint4 w0, w1, w2, w3, w4;
+    if (nodeIdx < topCount) {
+        const uint4* np = top + size_t(nodeIdx) * 5;
+        w0 = np[0]; w1 = np[1]; w2 = np[2]; w3 = np[3]; w4 = np[4];
+    } else {
+        const uint4* np = s.nodes + size_t(nodeIdx) * 5;
+        w0 = __ldg(np + 0); w1 = __ldg(np + 1); w2 = __ldg(np + 2); w3 = __ldg(np + 3); w4 = __ldg(np + 4);
+    }
     const uint32_t ew = w0.w;
     const float sx = __uint_as_float((ew & 0xffu) << 23);
     const float sy = __uint_as_float(((ew >> 8) & 0xffu) << 23);
@@ -246,8 +280,8 @@ FPT_D void visit_node(const DevScene& s, const TraceRay& r, float tBest, uint32_
         const float tfy = fmaf(quant_to_float(k < 4 ? Y.f0 : Y.f1, b), Y.si, Y.bf);
         const float tnz = fmaf(quant_to_float(k < 4 ? Z.n0 : Z.n1, b), Z.si, Z.bn);
         const float tfz = fmaf(quant_to_float(k < 4 ? Z.f0 : Z.f1, b), Z.si, Z.bf);
-        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tMin));
-        const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tBest));
+        const float tn = fmax3(tnx, tny, fmaxf(tnz, r.tMin));
+        const float tf = fmin3(tfx, tfy, fminf(tfz, tBest));
         hits |= (tn <= tf) ? (1u << k) : 0u;
     }
     // Empty slots hold the inverted box [p + 255 s, p], which no ray enters
@@ -282,7 +316,8 @@ constexpr int kPostponeLanes = FPT_POSTPONE_LANES;
 
 // STACK: entries of this thread's stack (at least the tree depth).
 template <bool ANY, int STACK = kStackSize, int TRIS = 0>
-FPT_D void trace_step(const DevScene& s, const TraceRay& r, TraceState& t, uint2* stack, uint32_t stride, int postponeLimit) {
+FPT_D void trace_step(const DevScene& s, const TraceRay& r, TraceState& t, uint2* stack, uint32_t stride, int postponeLimit,
+                      const uint4* top = nullptr, uint32_t topCount = 0) {
     if (t.gHits && (TRIS == 0 || t.tHits == 0)) {
         const uint32_t i = uint32_t(__ffs(t.gHits) - 1);
         t.gHits &= t.gHits - 1u;
@@ -297,7 +332,7 @@ FPT_D void trace_step(const DevScene& s, const TraceRay& r, TraceState& t, uint2
             return;
         }
         uint32_t innerHits, childBase, imask, triBase, triHits;
-        visit_node(s, r, t.tBest, nodeIdx, innerHits, childBase, imask, triBase, triHits);
+        visit_node(s, r, t.tBest, nodeIdx, innerHits, childBase, imask, triBase, triHits, top, topCount);
         if (t.gHits) {
             if (t.sp >= STACK) {
                 atomicOr(s.errorWord, FPT_DEVERR_STACK_OVERFLOW);
@@ -364,6 +399,40 @@ FPT_D void trace_step(const DevScene& s, const TraceRay& r, TraceState& t, uint2
             t.gImask = e.y >> 8;
         }
     }
+}
+
+// Top levels of the BVH in shared memory.  One thread of the block copies the
+// first kTopNodes nodes (5 KB; every ray visits them) with one bulk copy
+// (cp.async.bulk from this GPU's global memory to this CTA's shared memory,
+// no multicast) completing on an mbarrier; the block waits with a bounded
+// number of polls.  Returns the number of staged nodes (0 after a timeout,
+// recorded in the error word: the traversal then reads global memory).
+constexpr uint32_t kTopNodes = 64;
+FPT_D uint32_t stage_top_nodes(const DevScene& s, uint4* dst, unsigned long long* bar) {
+    const uint32_t count = min(s.nodeCount, kTopNodes);
+    if (count == 0) return 0;
+    const uint32_t bytes = count * 80u;  // a multiple of 16; node array and dst are 16-byte aligned
+    const uint32_t barAddr = uint32_t(__cvta_generic_to_shared(bar));
+    const uint32_t dstAddr = uint32_t(__cvta_generic_to_shared(dst));
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared.b64 [%0], 1;" ::"r"(barAddr) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared.b64 _, [%0], %1;" ::"r"(barAddr), "r"(bytes) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(dstAddr), "l"(s.nodes), "r"(bytes), "r"(barAddr) : "memory");
+    }
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < (1u << 20) && !done; it++)
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(done) : "r"(barAddr) : "memory");
+    if (!__syncthreads_and(int(done))) {
+        if (threadIdx.x == 0) atomicOr(s.errorWord, FPT_DEVERR_TIMEOUT);
+        return 0;
+    }
+    return count;
 }
 
 FPT_D void trace_result(const TraceState& t, HitRec& hit) {

@@ -164,11 +164,19 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_SHADE_MIN_BLOCKS) wf_shade(De
 #define FPT_TRACE_MIN_BLOCKS_SHORT 6
 #endif
 constexpr int kShortStack = 16;
+// FPT_TOP_NODES: the trace kernels stage the BVH's top levels in shared memory
+// (stage_top_nodes) and read them from there.
+#ifndef FPT_TOP_NODES
+#define FPT_TOP_NODES 0
+#endif
 template <int STACK>
 __global__ void __launch_bounds__(kTraceBlock, STACK <= kShortStack ? FPT_TRACE_MIN_BLOCKS_SHORT : FPT_TRACE_MIN_BLOCKS)
     wf_shadow(DevScene s, FrameParams p, WaveParams wp, SoA w) {
     __shared__ uint2 stackMem[STACK * kTraceBlock];
-    trace_queue<true, false, false, STACK>(s, p, wp, w, stackMem + threadIdx.x);
+    __shared__ __align__(16) uint4 topMem[FPT_TOP_NODES ? kTopNodes * 5 : 1];
+    __shared__ __align__(8) unsigned long long topBar;
+    const uint32_t topCount = FPT_TOP_NODES ? stage_top_nodes(s, topMem, &topBar) : 0u;
+    trace_queue<true, false, false, STACK>(s, p, wp, w, stackMem + threadIdx.x, topMem, topCount);
 }
 
 // Extension rays: closest hit; the path re-enters the shade queue.
@@ -176,7 +184,10 @@ template <int STACK>
 __global__ void __launch_bounds__(kTraceBlock, STACK <= kShortStack ? FPT_TRACE_MIN_BLOCKS_SHORT : FPT_TRACE_MIN_BLOCKS)
     wf_extend(DevScene s, FrameParams p, WaveParams wp, SoA w) {
     __shared__ uint2 stackMem[STACK * kTraceBlock];
-    trace_queue<false, false, false, STACK>(s, p, wp, w, stackMem + threadIdx.x);
+    __shared__ __align__(16) uint4 topMem[FPT_TOP_NODES ? kTopNodes * 5 : 1];
+    __shared__ __align__(8) unsigned long long topBar;
+    const uint32_t topCount = FPT_TOP_NODES ? stage_top_nodes(s, topMem, &topBar) : 0u;
+    trace_queue<false, false, false, STACK>(s, p, wp, w, stackMem + threadIdx.x, topMem, topCount);
 }
 
 // Batched waves: each ray traced in its own request's scene.

@@ -164,7 +164,8 @@ constexpr int kRefillBelow = FPT_REFILL_BELOW;
 // MULTI: rays of a batched wave, each traced in its own request's scene.
 // STACK: traversal-stack entries per thread (>= the tree depth).
 template <bool SHADOW, bool MARK_VISIBLE = false, bool MULTI = false, int STACK = kStackSize>
-FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams& wp, const SoA& w, uint2* stack) {
+FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams& wp, const SoA& w, uint2* stack,
+                       const uint4* top = nullptr, uint32_t topCount = 0) {
     const uint32_t lane = threadIdx.x & 31u;
     Counters cnt;
     const uint32_t n = wp.counts[SHADOW ? 2 : 1];
@@ -218,7 +219,7 @@ FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams
                         trace_step<SHADOW, STACK, SHADOW ? FPT_SHADOW_TRIS_PER_STEP : FPT_EXTEND_TRIS_PER_STEP>(*S, r, t, stack, kTraceBlock, 0);
                 } else {
                     trace_step<SHADOW, STACK, SHADOW ? FPT_SHADOW_TRIS_PER_STEP : FPT_EXTEND_TRIS_PER_STEP>(s, r, t, stack, kTraceBlock,
-                                                                                                         postponeLimit);
+                                                                                                         postponeLimit, top, topCount);
                 }
                 if (t.status != kTraceRunning) {
                     active = false;
