@@ -553,6 +553,22 @@ def gpu_rmse(accum, dev) -> dict:
             acc += col
         out["c1_64spp"] = round(rmse((acc / 64).cpu().numpy(), g1["rgb"]), 5)
         out["c1_reference_spp"] = int(g1["spp"])
+        # C1 throughput: one MinimalPathTracer frame (256 x 256, 1 spp, maxBounces 3)
+        # per launch, V-buffer included, CUDA events around 64 frames.
+        frame = [0]
+
+        def c1_frame():
+            vbp.execute({"vbuffer": vb})
+            mpt.execute({"vbuffer": vb, "color": col}, frame=frame[0])
+            frame[0] += 1
+        from falcor_b200.passes import VBufferRT
+        vbp = VBufferRT()
+        vbp.set_scene(scene)
+        for _ in range(4):
+            c1_frame()
+        ms = _time_ms(c1_frame, 64)
+        out["c1_ms_per_frame"] = round(ms, 4)
+        out["c1_Mpaths_s"] = round(256 * 256 / (ms / 1e3) / 1e6, 2)
     return out
 
 

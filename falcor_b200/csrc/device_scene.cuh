@@ -217,31 +217,6 @@ FPT_D AxisPlanes axis_planes(float p, float s, float o, float inv, uint32_t lo0,
     return a;
 }
 
-// Three-input float min / max (PTX min.f32 / max.f32 with three operands,
-// sm_100): one instruction where two two-input ones would run.  Exact like
-// fminf / fmaxf; the slab distances are never NaN (|1/d| is clamped).
-#ifndef FPT_MINMAX3
-#define FPT_MINMAX3 1
-#endif
-FPT_D float fmax3(float a, float b, float c) {
-#if FPT_MINMAX3
-    float r;
-    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-#else
-    return fmaxf(fmaxf(a, b), c);
-#endif
-}
-FPT_D float fmin3(float a, float b, float c) {
-#if FPT_MINMAX3
-    float r;
-    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-#else
-    return fminf(fminf(a, b), c);
-#endif
-}
-
 // Visits one node: tests its 8 child boxes against [tMin, tBest].  Returns
 // the hit internal children as a group (octant order) and the triangles of
 // the hit leaf children as a bit mask relative to the node's triangle base.
@@ -280,8 +255,8 @@ FPT_D void visit_node(const DevScene& s, const TraceRay& r, float tBest, uint32_
         const float tfy = fmaf(quant_to_float(k < 4 ? Y.f0 : Y.f1, b), Y.si, Y.bf);
         const float tnz = fmaf(quant_to_float(k < 4 ? Z.n0 : Z.n1, b), Z.si, Z.bn);
         const float tfz = fmaf(quant_to_float(k < 4 ? Z.f0 : Z.f1, b), Z.si, Z.bf);
-        const float tn = fmax3(tnx, tny, fmaxf(tnz, r.tMin));
-        const float tf = fmin3(tfx, tfy, fminf(tfz, tBest));
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tMin));
+        const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tBest));
         hits |= (tn <= tf) ? (1u << k) : 0u;
     }
     // Empty slots hold the inverted box [p + 255 s, p], which no ray enters
@@ -632,7 +607,18 @@ FPT_D DevTexture load_texture(const DevScene& s, uint32_t id) {
     t.width = a.z; t.height = a.w; t.format = b.x; t.texelBase = b.y;
     return t;
 }
-FPT_D float3 tex_sample(const DevScene& s, uint32_t id, float2 uv) {
+// Not inlined (FPT_TEX_INLINE 0): the shading kernels then carry only a call
+// for it, so scenes without textures do not pay for its code in the
+// instruction cache.
+#ifndef FPT_TEX_INLINE
+#define FPT_TEX_INLINE 0
+#endif
+#if FPT_TEX_INLINE
+FPT_D
+#else
+__device__ __noinline__
+#endif
+float3 tex_sample(const DevScene& s, uint32_t id, float2 uv) {
     const DevTexture t = load_texture(s, id);
     const fpt_tex::Bilinear b = fpt_tex::bilinear(uv.x, uv.y, t.width, t.height);
     float3 c = tex_texel(s, t, b.x0, b.y0) * b.w[0];

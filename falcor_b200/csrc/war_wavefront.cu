@@ -67,12 +67,26 @@ struct WarWave {
     float4* rec;        // maxVertices x recArrays x capacity
     uint32_t* nv;       // records per path
     uint32_t maxVertices, recArrays;
+    // Reparameterisation requests of the reverse sweep (WAR), served by
+    // ww_war_requests: scatter rays (kReqArrays x maxVertices * capacity
+    // entries) and screen samples (kScreenReqArrays x capacity), with their
+    // counters in reqCount[0] / reqCount[1].
+    float4* req;
+    float4* sreq;
+    uint32_t* reqCount;
+    uint32_t reqCapacity;
 };
+// Scatter request: origin + gJ, direction + pixel, gDir + b1, sample generator,
+// gradient offsets + b0, b2.  Screen request: sample + gPix, sample generator,
+// gJ + pixel.
+constexpr int kReqArrays = 6, kScreenReqArrays = 3;
 
 FPT_D float4& nee_at(const WarWave& ww, int j, uint32_t i) { return ww.nee[size_t(j) * ww.capacity + i]; }
 FPT_D float4& rec_at(const WarWave& ww, uint32_t k, int j, uint32_t i) {
     return ww.rec[(size_t(k) * ww.recArrays + j) * ww.capacity + i];
 }
+FPT_D float4& req_at(const WarWave& ww, int j, uint32_t k) { return ww.req[size_t(j) * ww.reqCapacity + k]; }
+FPT_D float4& sreq_at(const WarWave& ww, int j, uint32_t k) { return ww.sreq[size_t(j) * ww.capacity + k]; }
 FPT_D uint4& as_u4(float4& v) { return reinterpret_cast<uint4&>(v); }
 FPT_D float3 xyz(const float4& v) { return make_float3(v.x, v.y, v.z); }
 FPT_D bool nonzero(float3 v) { return v.x != 0.f || v.y != 0.f || v.z != 0.f; }
@@ -401,69 +415,149 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_nee_grad(De
 
 // Reverse sweep over each path's records (war_sweep_vertex), then the
 // screen-sample reparameterisation (WAR).
+// Claims one slot of a request queue per lane with want set (warp-aggregated);
+// ~0u when not wanted or when the queue is full (recorded in the error word).
+FPT_D uint32_t claim_slot(const DevScene& s, bool want, uint32_t* count, uint32_t capacity) {
+    const uint32_t group = __activemask();
+    const uint32_t mask = __ballot_sync(group, want);
+    if (mask == 0) return ~0u;
+    const uint32_t lane = threadIdx.x & 31u;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (int(lane) == leader) base = atomicAdd(count, uint32_t(__popc(mask)));
+    base = __shfl_sync(group, base, leader);
+    if (!want) return ~0u;
+    const uint32_t pos = base + uint32_t(__popc(mask & ((1u << lane) - 1u)));
+    if (pos >= capacity) {
+        atomicOr(s.errorWord, FPT_DEVERR_QUEUE);
+        return ~0u;
+    }
+    return pos;
+}
+
+// Reverse sweep over each path's records (war_sweep_vertex).  With WAR the
+// scatter and screen reparameterisations are not evaluated here: they are
+// queued for ww_war_requests, which traces their auxiliary rays with the lanes
+// of a warp cooperating -- a separate, smaller kernel, as the sweep with the
+// cooperative pass inline was bound by instruction fetch.
 template <bool HAS_T, bool WAR>
 __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_sweep(DevScene s, WarParams p, WaveParams wp, WarWave ww) {
-    __shared__ uint2 stackMem[WAR ? kStackSize * kShadeBlock : 1];
-    uint2* stack = stackMem + threadIdx.x;
-    // Warp-uniform trip counts (paths and vertices): the scatter and screen
-    // reparameterisations of the warp's paths are served together (war_coop).
-    const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x - lane; i0 < wp.wavePixels; i0 += gridDim.x * blockDim.x) {
-        const uint32_t i = i0 + lane;
-        const bool valid = i < wp.wavePixels;
-        const uint32_t pid = wp.waveFirstPixel + (valid ? i : 0u);
-        const float3 g = valid ? war_dLdI(p, pid) : f3(0.f);
+    __shared__ uint2 stackMem[1];
+    uint2* stack = stackMem;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < wp.wavePixels; i += gridDim.x * blockDim.x) {
+        const uint32_t pid = wp.waveFirstPixel + i;
+        const float3 g = war_dLdI(p, pid);
         const uint32_t hash = war_hash(pid, p.matHash);
         float3 A = f3(0.f), gV = f3(0.f);
-        const int nv = valid ? int(ww.nv[i]) : 0;
-        const int maxNv = WAR ? __reduce_max_sync(0xffffffffu, uint32_t(nv)) : nv;
-        for (int k = maxNv - 1; k >= 0; k--) {
+        const int nv = int(ww.nv[i]);
+        for (int k = nv - 1; k >= 0; k--) {
+            const float4 r0 = rec_at(ww, k, 0, i), r1 = rec_at(ww, k, 1, i), r2 = rec_at(ww, k, 2, i);
+            WarSweepVertex v;
+            v.wiL = xyz(r0);
+            v.pdf = r0.w;
+            v.wsL = xyz(r1);
+            v.matID = __float_as_uint(r1.w);
+            v.thp = xyz(r2);
+            v.flags = __float_as_uint(r2.w);
+            const float4 r3 = rec_at(ww, k, 3, i), r4 = rec_at(ww, k, 4, i);
+            v.bw = xyz(r3);
+            v.e = xyz(r4);
+            v.uv = make_float2(r3.w, r4.w);
             WarCoopReq rq;
             rq.active = false;
             uint32_t off[3] = {0, 0, 0};
             float bwt[3] = {0.f, 0.f, 0.f};
             bool posT = false;
-            if (k < nv) {
-                const float4 r0 = rec_at(ww, k, 0, i), r1 = rec_at(ww, k, 1, i), r2 = rec_at(ww, k, 2, i);
-                WarSweepVertex v;
-                v.wiL = xyz(r0);
-                v.pdf = r0.w;
-                v.wsL = xyz(r1);
-                v.matID = __float_as_uint(r1.w);
-                v.thp = xyz(r2);
-                v.flags = __float_as_uint(r2.w);
-                const float4 r3 = rec_at(ww, k, 3, i), r4 = rec_at(ww, k, 4, i);
-                v.bw = xyz(r3);
-                v.e = xyz(r4);
-                v.uv = make_float2(r3.w, r4.w);
-                if (WAR) {
-                    const float4 r5 = rec_at(ww, k, 5, i), r6 = rec_at(ww, k, 6, i), r8 = rec_at(ww, k, 8, i), r9 = rec_at(ww, k, 9, i);
-                    v.inDir = xyz(r5);
-                    v.inst = __float_as_uint(r5.w);
-                    v.outDir = xyz(r6);
-                    v.prim = __float_as_uint(r6.w);
-                    v.sg = as_u4(rec_at(ww, k, 7, i));
-                    v.gV = xyz(r8);
-                    v.b[0] = r8.w;
-                    v.b[1] = r9.x;
-                    v.b[2] = r9.y;
-                }
-                war_sweep_vertex<HAS_T, WAR>(s, p, pid, hash, v, g, A, gV, stack, kShadeBlock, WAR ? &rq : nullptr, &off, &bwt,
-                                             &posT);
-            }
             if (WAR) {
-                float3 gO = f3(0.f), gD = f3(0.f);
-                war_coop<3>(s, p, pid, rq, stack, kShadeBlock, gO, gD);
-                if (rq.active && posT) add_position_grad(p, pid, off, bwt, gO);
+                const float4 r5 = rec_at(ww, k, 5, i), r6 = rec_at(ww, k, 6, i), r8 = rec_at(ww, k, 8, i), r9 = rec_at(ww, k, 9, i);
+                v.inDir = xyz(r5);
+                v.inst = __float_as_uint(r5.w);
+                v.outDir = xyz(r6);
+                v.prim = __float_as_uint(r6.w);
+                v.sg = as_u4(rec_at(ww, k, 7, i));
+                v.gV = xyz(r8);
+                v.b[0] = r8.w;
+                v.b[1] = r9.x;
+                v.b[2] = r9.y;
+            }
+            war_sweep_vertex<HAS_T, WAR>(s, p, pid, hash, v, g, A, gV, stack, kShadeBlock, WAR ? &rq : nullptr, &off, &bwt, &posT);
+            if (WAR) {
+                // Queued whenever the warp is wanted: the auxiliary hits can be on
+                // the optimised mesh although this vertex is not (posT).
+                const uint32_t slot = claim_slot(s, rq.active, ww.reqCount, ww.reqCapacity);
+                if (slot != ~0u) {
+                    req_at(ww, 0, slot) = make_float4(rq.origin.x, rq.origin.y, rq.origin.z, rq.gJ);
+                    req_at(ww, 1, slot) = make_float4(rq.dir.x, rq.dir.y, rq.dir.z, __uint_as_float(pid));
+                    req_at(ww, 2, slot) = make_float4(rq.gDir.x, rq.gDir.y, rq.gDir.z, bwt[1]);
+                    as_u4(req_at(ww, 3, slot)) = rq.sg;
+                    req_at(ww, 4, slot) = make_float4(__uint_as_float(off[0]), __uint_as_float(off[1]), __uint_as_float(off[2]), bwt[0]);
+                    req_at(ww, 5, slot) = make_float4(bwt[2], __uint_as_float(posT ? 1u : 0u), 0.f, 0.f);
+                }
             }
         }
-        if (WAR) {
+        if (WAR && p.useWAR && war_wants_pos(p) && nv > 0) {
             WarCoopReq rq;
             rq.active = false;
-            if (valid && p.useWAR && war_wants_pos(p) && nv > 0) war_sweep_screen(s, p, pid, A, gV, stack, kShadeBlock, &rq);
-            float3 gO = f3(0.f), gD = f3(0.f);
-            war_coop<2>(s, p, pid, rq, stack, kShadeBlock, gO, gD);
+            war_sweep_screen(s, p, pid, A, gV, stack, kShadeBlock, &rq);
+            const uint32_t slot = claim_slot(s, rq.active, ww.reqCount + 1, ww.capacity);
+            if (slot != ~0u) {
+                sreq_at(ww, 0, slot) = make_float4(rq.posS.x, rq.posS.y, rq.gPix.x, rq.gPix.y);
+                as_u4(sreq_at(ww, 1, slot)) = rq.sg;
+                sreq_at(ww, 2, slot) = make_float4(rq.gJ, __uint_as_float(pid), 0.f, 0.f);
+            }
         }
+    }
+}
+
+// Serves the queued reparameterisations (J = 3 scatter rays, J = 2 screen
+// samples): each lane loads one request and the warp traces their auxiliary
+// rays together (war_coop); the origin's adjoint of a scatter ray goes to its
+// vertex's position gradient.
+template <int J>
+__global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_war_requests(DevScene s, WarParams p, WarWave ww) {
+    __shared__ uint2 stackMem[kStackSize * kShadeBlock];
+    uint2* stack = stackMem + threadIdx.x;
+    const uint32_t n = min(ww.reqCount[J == 3 ? 0 : 1], J == 3 ? ww.reqCapacity : ww.capacity);
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x - lane; k0 < n; k0 += gridDim.x * blockDim.x) {
+        const uint32_t k = k0 + lane;
+        WarCoopReq rq;
+        rq.active = k < n;
+        rq.needD = false;
+        uint32_t pid = 0;
+        uint32_t off[3] = {0, 0, 0};
+        float bw[3] = {0.f, 0.f, 0.f};
+        bool posT = false;
+        if (rq.active) {
+            if (J == 3) {
+                const float4 a = req_at(ww, 0, k), b = req_at(ww, 1, k), c = req_at(ww, 2, k), d = req_at(ww, 4, k);
+                rq.origin = xyz(a);
+                rq.gJ = a.w;
+                rq.dir = xyz(b);
+                pid = __float_as_uint(b.w);
+                rq.gDir = xyz(c);
+                bw[1] = c.w;
+                rq.sg = as_u4(req_at(ww, 3, k));
+                off[0] = __float_as_uint(d.x);
+                off[1] = __float_as_uint(d.y);
+                off[2] = __float_as_uint(d.z);
+                bw[0] = d.w;
+                const float4 e = req_at(ww, 5, k);
+                bw[2] = e.x;
+                posT = __float_as_uint(e.y) != 0u;
+            } else {
+                const float4 a = sreq_at(ww, 0, k);
+                rq.posS = make_float2(a.x, a.y);
+                rq.gPix = make_float2(a.z, a.w);
+                rq.sg = as_u4(sreq_at(ww, 1, k));
+                const float4 c = sreq_at(ww, 2, k);
+                rq.gJ = c.x;
+                pid = __float_as_uint(c.y);
+            }
+        }
+        float3 gO = f3(0.f), gD = f3(0.f);
+        war_coop<J>(s, p, pid, rq, stack, kShadeBlock, gO, gD);
+        if (J == 3 && rq.active && posT) add_position_grad(p, pid, off, bw, gO);
     }
 }
 
@@ -565,16 +659,31 @@ cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBu
         ww.rec = reinterpret_cast<float4*>(q);
         q += size_t(ww.maxVertices) * ww.recArrays * b.capacity * sizeof(float4);
         ww.nv = reinterpret_cast<uint32_t*>(q);
+        q += size_t(b.capacity) * sizeof(uint32_t);
+        ww.req = ww.sreq = nullptr;
+        ww.reqCount = nullptr;
+        ww.reqCapacity = 0;
+        if (WAR) {
+            q = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(q) + 255) & ~uintptr_t(255));
+            ww.reqCapacity = ww.maxVertices * b.capacity;
+            ww.req = reinterpret_cast<float4*>(q);
+            q += size_t(kReqArrays) * ww.reqCapacity * sizeof(float4);
+            ww.sreq = reinterpret_cast<float4*>(q);
+            q += size_t(kScreenReqArrays) * b.capacity * sizeof(float4);
+            ww.reqCount = reinterpret_cast<uint32_t*>(q);
+        }
     }
     // Trace kernels read the ray counters through FrameParams.
     FrameParams fp{};
     fp.counters = p.counters;
-    static int gShade = 0, gTrace = 0, gSweep = 0, gNee = 0;
+    static int gShade = 0, gTrace = 0, gSweep = 0, gNee = 0, gReq3 = 0, gReq2 = 0;
     if (!gShade) {
         gShade = blocks_for(reinterpret_cast<const void*>(ww_shade<HAS_T, BWD, WAR>), kShadeBlock);
         gTrace = blocks_for(reinterpret_cast<const void*>(ww_extend), kTraceBlock);
         gSweep = BWD ? blocks_for(reinterpret_cast<const void*>(ww_sweep<HAS_T, WAR>), kShadeBlock) : 1;
         gNee = BWD ? blocks_for(reinterpret_cast<const void*>(ww_nee_grad<WAR>), kShadeBlock) : 1;
+        gReq3 = WAR ? blocks_for(reinterpret_cast<const void*>(ww_war_requests<3>), kShadeBlock) : 1;
+        gReq2 = WAR ? blocks_for(reinterpret_cast<const void*>(ww_war_requests<2>), kShadeBlock) : 1;
     }
     const uint32_t pixels = p.width * p.height;
     const uint32_t maxIter = p.maxBounces + 2;
@@ -626,10 +735,21 @@ cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBu
                 launches++;
             }
         }
-        if (BWD)
+        if (BWD) {
+            if (WAR) {
+                e = cudaMemsetAsync(ww.reqCount, 0, 2 * sizeof(uint32_t), st);
+                if (e != cudaSuccess) return e;
+            }
             ww_sweep<HAS_T, WAR><<<std::min<int>(gSweep, int((wp.wavePixels + kShadeBlock - 1) / kShadeBlock)), kShadeBlock, 0, st>>>(
                 s, p, wp, ww);
-        else ww_resolve<<<(wp.wavePixels + 255) / 256, 256, 0, st>>>(p, wp, w);
+            if (WAR) {
+                ww_war_requests<3><<<gReq3, kShadeBlock, 0, st>>>(s, p, ww);
+                ww_war_requests<2><<<gReq2, kShadeBlock, 0, st>>>(s, p, ww);
+                launches += 2;
+            }
+        } else {
+            ww_resolve<<<(wp.wavePixels + 255) / 256, 256, 0, st>>>(p, wp, w);
+        }
         launches++;
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -646,7 +766,10 @@ size_t war_checkpoint_bytes(uint32_t pixels, uint32_t maxBounces) {
 size_t war_adjoint_bytes(uint32_t capacity, uint32_t maxBounces, bool war) {
     const size_t maxVertices = size_t(maxBounces) + 2;
     const size_t nee = war ? kNeeArraysWar : kNeeArrays, rec = war ? kRecArraysWar : kRecArrays;
-    return (nee + maxVertices * rec) * capacity * sizeof(float4) + size_t(capacity) * sizeof(uint32_t);
+    size_t bytes = (nee + maxVertices * rec) * capacity * sizeof(float4) + size_t(capacity) * sizeof(uint32_t);
+    if (war)  // alignment, scatter and screen requests, two counters
+        bytes += 256 + (size_t(kReqArrays) * maxVertices + kScreenReqArrays) * capacity * sizeof(float4) + 2 * sizeof(uint32_t);
+    return bytes;
 }
 
 cudaError_t launch_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBuffers& b, void* adjointScratch, bool backward,
