@@ -616,7 +616,7 @@ FPT_D DevTexture load_texture(const DevScene& s, uint32_t id) {
 #if FPT_TEX_INLINE
 FPT_D
 #else
-__device__ __noinline__
+static __device__ __noinline__
 #endif
 float3 tex_sample(const DevScene& s, uint32_t id, float2 uv) {
     const DevTexture t = load_texture(s, id);
