@@ -45,7 +45,25 @@ struct DevScene {
     const DevTexture* textures;
     const float* srgbDecode;          // 256-entry sRGB decode table
     uint32_t textureCount;
+    float sceneLo[3], sceneInvExtent[3]; // scene bounds at creation (ray binning keys)
 };
+
+// Bin of an extension ray for coherence sorting: the Morton code of its
+// origin's cell in a 4 x 4 x 4 grid over the scene bounds, then its direction
+// octant (512 bins).
+FPT_D uint32_t ray_bin_key(const DevScene& s, float3 o, float3 d) {
+    uint32_t c[3];
+    const float p[3] = {o.x, o.y, o.z};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float f = (p[a] - s.sceneLo[a]) * s.sceneInvExtent[a] * 4.f;
+        c[a] = f >= 3.f ? 3u : (f > 0.f ? uint32_t(f) : 0u);
+    }
+    uint32_t m = 0;
+#pragma unroll
+    for (int b = 1; b >= 0; b--) m = (m << 3) | (((c[0] >> b) & 1u) << 2) | (((c[1] >> b) & 1u) << 1) | ((c[2] >> b) & 1u);
+    return (m << 3) | (d.x < 0.f ? 4u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 1u : 0u);
+}
 
 namespace dev {
 
@@ -607,18 +625,7 @@ FPT_D DevTexture load_texture(const DevScene& s, uint32_t id) {
     t.width = a.z; t.height = a.w; t.format = b.x; t.texelBase = b.y;
     return t;
 }
-// Not inlined (FPT_TEX_INLINE 0): the shading kernels then carry only a call
-// for it, so scenes without textures do not pay for its code in the
-// instruction cache.
-#ifndef FPT_TEX_INLINE
-#define FPT_TEX_INLINE 0
-#endif
-#if FPT_TEX_INLINE
-FPT_D
-#else
-static __device__ __noinline__
-#endif
-float3 tex_sample(const DevScene& s, uint32_t id, float2 uv) {
+FPT_D float3 tex_sample(const DevScene& s, uint32_t id, float2 uv) {
     const DevTexture t = load_texture(s, id);
     const fpt_tex::Bilinear b = fpt_tex::bilinear(uv.x, uv.y, t.width, t.height);
     float3 c = tex_texel(s, t, b.x0, b.y0) * b.w[0];
@@ -716,7 +723,9 @@ struct MaterialInstance {
     }
 };
 
-template <bool HAS_TRANSMISSION>
+// TEX = false: the scene has no textures, and the texture lookup is compiled
+// out (its code would sit in the instruction cache of the shading kernels).
+template <bool HAS_TRANSMISSION, bool TEX = true>
 FPT_D MaterialInstance<HAS_TRANSMISSION> material_instance(const DevScene& s, const ShadingData& sd, bool lambert) {
     const uint4* mp = reinterpret_cast<const uint4*>(s.materials + sd.materialID);
     const uint4 m0 = __ldg(mp), m1 = __ldg(mp + 1), m2 = __ldg(mp + 2);
@@ -735,7 +744,7 @@ FPT_D MaterialInstance<HAS_TRANSMISSION> material_instance(const DevScene& s, co
     const float f = (IoR - 1.f) / (IoR + 1.f);
     const float F0 = f * f;
     float3 baseColor = make_float3(f16(m0.x & 0xffffu), f16(m0.x >> 16), f16(m0.y & 0xffffu));
-    if (flags & kMatFlagBaseColorTexture) baseColor = tex_sample(s, __ldg(reinterpret_cast<const uint32_t*>(mp + 3)), sd.uv);
+    if (TEX && (flags & kMatFlagBaseColorTexture)) baseColor = tex_sample(s, __ldg(reinterpret_cast<const uint32_t*>(mp + 3)), sd.uv);
     const float specG = f16(m0.z >> 16), specB = f16(m0.w & 0xffffu);
     d.diffuse = lerp(baseColor, f3(0.f), specB);
     d.specular = lerp(f3(F0), baseColor, specB);

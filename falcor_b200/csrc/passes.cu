@@ -135,6 +135,7 @@ void set_defaults(fpt_pass& p) {
         // default: on the 1080p heightfield frame shading got 5 % faster but the
         // queue pushes made the extension kernel 10 % slower (net -2 %).
         d["splitMisses"] = PropValue::num(0);
+        d["sortExtensionRays"] = PropValue::num(0);
     } else if (p.type == "VBufferRT") {
         // GBufferBase.h:96-98.
         d["samplePattern"] = PropValue::str("Center");
@@ -418,6 +419,7 @@ void path_tracer_params(fpt_pass& p, FrameParams& fp) {
     fp.lambert = p.str("diffuseBrdf") == "Lambert";
     fp.sortMaterials = p.num("sortShadeQueue") != 0 ? 1u : 0u;
     fp.splitMisses = p.num("splitMisses") != 0 ? 1u : 0u;
+    fp.sortRays = p.num("sortExtensionRays") != 0 ? 1u : 0u;
 }
 
 }  // namespace fpt

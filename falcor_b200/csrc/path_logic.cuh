@@ -143,13 +143,13 @@ FPT_D bool generate_light_sample(const DevScene& s, const FrameParams& p, const 
 }
 
 // PathTracer::handleHit (PathTracer.slang:821-1066).
-template <class SG, bool HAS_T>
+template <class SG, bool HAS_T, bool TEX = true>
 FPT_D void pt_handle_hit(const DevScene& s, const FrameParams& p, PathState<SG>& path, Counters& cnt) {
     const bool isPrimaryHit = path.vertexIndex == 1;
     const bool useEnv = s.hasEnv != 0, useEm = s.hasEmissive != 0;
     const ShadingData sd = load_shading_data(s, path.hit, path.dir);
     cnt.v[6]++;
-    const MaterialInstance<HAS_T> mi = material_instance<HAS_T>(s, sd, p.lambert != 0);
+    const MaterialInstance<HAS_T> mi = material_instance<HAS_T, TEX>(s, sd, p.lambert != 0);
     const float roughness = mi.propRoughness();
     const bool isLightSamplable = path.isLightSamplable();
     const bool computeEmissive =

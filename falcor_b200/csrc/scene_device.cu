@@ -371,6 +371,11 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
     ds.nodeCount = uint32_t(s.bvh.nodes.size());
     ds.triCount = total;
     ds.bvhDepth = s.bvh.maxDepth;
+    for (int a = 0; a < 3; a++) {
+        ds.sceneLo[a] = s.bvh.lo[a];
+        const float ext = s.bvh.hi[a] - s.bvh.lo[a];
+        ds.sceneInvExtent[a] = ext > 0.f ? 1.f / ext : 0.f;
+    }
     ds.materialCount = d.material_count;
     ds.camera = s.info.camera;
     ds.bits = s.info.hit_bits;

@@ -97,15 +97,15 @@ __global__ void __launch_bounds__(kShadeBlock) wf_generate(DevScene s, FramePara
     flush_counters(p.counters, cnt);
 }
 
-template <class SG, bool HAS_T>
+template <class SG, bool HAS_T, bool TEX = true>
 FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uint32_t i, bool& ext, bool& shadow, Counters& cnt,
-                      const WaveParams* wp = nullptr) {
+                      const WaveParams* wp = nullptr, uint32_t* binKey = nullptr) {
     PathState<SG> path;
     load_path(w, i, path);
     if (wp && p.hitTrace)
         record_vertex(p, p.spp, p.maxSurfaceBounces + 2, wp->waveFirstPixel + i % wp->wavePixels, i / wp->wavePixels, path.vertexIndex,
                       (path.flags & 0x2u) != 0, path.hit);
-    if (path.flags & 0x2u) pt_handle_hit<SG, HAS_T>(s, p, path, cnt);
+    if (path.flags & 0x2u) pt_handle_hit<SG, HAS_T, TEX>(s, p, path, cnt);
     else pt_handle_miss<SG>(s, p, path, cnt);
     shadow = path.shadowPending;
     if (shadow) {
@@ -114,6 +114,7 @@ FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uin
         w.sLr[i] = make_float4(path.sLr.x, path.sLr.y, path.sLr.z, 0.f);
     }
     ext = path.has(PF_ACTIVE);
+    if (binKey && ext) *binKey = ray_bin_key(s, path.origin, path.dir);
     store_path(w, i, path);
     if (!ext) cnt.v[0]++;
 }
@@ -133,7 +134,7 @@ FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uin
 #ifndef FPT_SPECIALIZE_SAMPLER
 #define FPT_SPECIALIZE_SAMPLER 1
 #endif
-template <class SG, bool HAS_T, bool MULTI, int ES = -1>
+template <class SG, bool HAS_T, bool MULTI, int ES = -1, bool TEX = true>
 __global__ void __launch_bounds__(kShadeBlock, FPT_SHADE_MIN_BLOCKS) wf_shade(DevScene s, FrameParams pk, WaveParams wp, SoA w) {
     FrameParams p = pk;
     if (ES >= 0) p.emissiveSampler = uint32_t(ES);
@@ -141,18 +142,19 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_SHADE_MIN_BLOCKS) wf_shade(De
     const uint32_t n = wp.counts[0];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k - threadIdx.x < n; k += gridDim.x * blockDim.x) {
         bool ext = false, shadow = false;
-        uint32_t i = 0;
+        uint32_t i = 0, key = 0;
         if (k < n) {
             i = wp.shadeQueue[k];
             if (MULTI) {
                 const uint32_t r = slot_request(wp, i);
                 shade_slot<SG, HAS_T>(wp.scenes[r], wp.frames[r], w, i, ext, shadow, cnt);
             } else {
-                shade_slot<SG, HAS_T>(s, p, w, i, ext, shadow, cnt, &wp);
+                shade_slot<SG, HAS_T, TEX>(s, p, w, i, ext, shadow, cnt, &wp, wp.extKeys ? &key : nullptr);
             }
         }
         push(shadow, i, wp.shadowQueue, wp.counts + 2);
-        push(ext, i, wp.extQueue, wp.counts + 1);
+        const uint32_t pos = push(ext, i, wp.extQueue, wp.counts + 1);
+        if (!MULTI && wp.extKeys && pos != 0xffffffffu) wp.extKeys[pos] = key;
     }
     flush_counters(p.counters, cnt);
 }
@@ -301,6 +303,37 @@ __global__ void wf_sort_scatter(WaveParams wp, uint32_t* bins, uint32_t* out) {
     }
 }
 
+// Counting sort of the extension queue by ray bin (coherence of the next
+// traversal): histogram, scan (wf_sort_scan over nBins), scatter.
+__global__ void wf_bin_count(const uint32_t* keys, const uint32_t* count, uint32_t nBins, uint32_t* bins) {
+    __shared__ uint32_t h[WavefrontBuffers::kMaxSortBins];
+    for (uint32_t b = threadIdx.x; b < nBins; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    const uint32_t n = *count;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        atomicAdd(&h[min(keys[k], nBins - 1u)], 1u);
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < nBins; b += blockDim.x)
+        if (h[b]) atomicAdd(&bins[b], h[b]);
+}
+__global__ void wf_bin_scatter(const uint32_t* keys, const uint32_t* in, const uint32_t* count, uint32_t nBins, uint32_t* bins,
+                               uint32_t* out) {
+    const uint32_t n = *count;
+    uint32_t* cursor = bins + WavefrontBuffers::kMaxSortBins;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k - lane < n; k += gridDim.x * blockDim.x) {
+        const bool valid = k < n;
+        const uint32_t key = valid ? min(keys[k], nBins - 1u) : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        if (!valid) continue;
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (int(lane) == leader) base = atomicAdd(&cursor[key], uint32_t(__popc(peers)));
+        base = __shfl_sync(peers, base, leader);
+        out[base + uint32_t(__popc(peers & ((1u << lane) - 1u)))] = in[k];
+    }
+}
+
 // handleMiss for the paths of the miss queue (hit/miss split): the short
 // environment-light branch of the shade stage, run apart so that the shade
 // kernel's warps hold hits only.
@@ -336,6 +369,16 @@ __global__ void wf_advance(WaveParams wp) {
     wp.counts[kFetchShadow] = 0;
 }
 
+// The shade stage: the kernel specialised for the emissive sampler and for
+// whether the scene has textures.
+template <class SG, bool HAS_T, bool TEX>
+void launch_shade(const DevScene& s, const FrameParams& p, const WaveParams& wp, const SoA& w, int grid, cudaStream_t st) {
+    if (FPT_SPECIALIZE_SAMPLER && p.emissiveSampler == 2) wf_shade<SG, HAS_T, false, 2, TEX><<<grid, kShadeBlock, 0, st>>>(s, p, wp, w);
+    else if (FPT_SPECIALIZE_SAMPLER && p.emissiveSampler == 1) wf_shade<SG, HAS_T, false, 1, TEX><<<grid, kShadeBlock, 0, st>>>(s, p, wp, w);
+    else if (FPT_SPECIALIZE_SAMPLER && p.emissiveSampler == 0) wf_shade<SG, HAS_T, false, 0, TEX><<<grid, kShadeBlock, 0, st>>>(s, p, wp, w);
+    else wf_shade<SG, HAS_T, false, -1, TEX><<<grid, kShadeBlock, 0, st>>>(s, p, wp, w);
+}
+
 template <class SG, bool HAS_T>
 cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st, KernelTimer* kt) {
     auto T0 = [&](int cat) { if (kt && kt->enabled) kt->begin(cat, st); };
@@ -359,7 +402,10 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
     const bool shortStack = s.bvhDepth <= uint32_t(kShortStack);
     // Material sort of the secondary shade queues (primary hits come in pixel
     // order, already coherent).
-    const bool sortQueue = p.sortMaterials && b.owning && b.ensure_sort() == cudaSuccess;
+    // Extension-ray binning (sortExtensionRays) shares the sort buffers and
+    // takes precedence over the material sort.
+    const bool binRays = p.sortRays && !p.splitMisses && b.owning && b.ensure_sort() == cudaSuccess;
+    const bool sortQueue = !binRays && p.sortMaterials && b.owning && b.ensure_sort() == cudaSuccess;
     const uint32_t sortBins = std::min<uint32_t>(std::max<uint32_t>(s.materialCount, 1u), WavefrontBuffers::kMaxSortBins - 1u) + 1u;
     // Hit/miss split of the shade stage.
     const bool split = p.splitMisses && b.owning && b.ensure_split() == cudaSuccess;
@@ -374,11 +420,13 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
         if (e != cudaSuccess) return e;
         uint32_t* qa = b.queueA;
         uint32_t* qb = b.queueB;
+        uint32_t* spare = b.sortQueue;  // binning: scatter target (three distinct buffers rotate within a wave)
         wp.shadeQueue = qa;
         wp.extQueue = qb;
         wp.shadowQueue = b.shadowQueue;
         wp.sortKeys = sortQueue ? b.sortKeys : nullptr;
         wp.sortBins = sortBins;
+        wp.extKeys = binRays ? b.sortKeys : nullptr;
         uint32_t* qHit = qa;
         uint32_t* qMiss = b.missQueue;
         uint32_t* qNextHit = b.nextHitQueue;
@@ -402,16 +450,32 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
                 wp.shadeQueue = b.sortQueue;
             }
             T0(KC_SHADE);
-            if (FPT_SPECIALIZE_SAMPLER && p.emissiveSampler == 2) wf_shade<SG, HAS_T, false, 2><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
-            else if (FPT_SPECIALIZE_SAMPLER && p.emissiveSampler == 1) wf_shade<SG, HAS_T, false, 1><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
-            else if (FPT_SPECIALIZE_SAMPLER && p.emissiveSampler == 0) wf_shade<SG, HAS_T, false, 0><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
-            else wf_shade<SG, HAS_T, false><<<gShade, kShadeBlock, 0, st>>>(s, p, wp, w);
+            if (s.textureCount) launch_shade<SG, HAS_T, true>(s, p, wp, w, gShade, st);
+            else launch_shade<SG, HAS_T, false>(s, p, wp, w, gShade, st);
             if (split && it > 0) wf_miss<SG><<<gGen, kShadeBlock, 0, st>>>(s, p, wp, w);
             T1();
             T0(KC_SHADOW);
             if (shortStack) wf_shadow<kShortStack><<<gTraceShort, kTraceBlock, 0, st>>>(s, p, wp, w);
             else wf_shadow<kStackSize><<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
             T1();
+            if (binRays) {
+                T0(KC_SORT);
+                constexpr uint32_t kRayBins = 512;
+                e = cudaMemsetAsync(b.sortBins, 0, WavefrontBuffers::kMaxSortBins * sizeof(uint32_t), st);
+                if (e != cudaSuccess) return e;
+                wf_bin_count<<<gGen, kShadeBlock, 0, st>>>(b.sortKeys, wp.counts + 1, kRayBins, b.sortBins);
+                WaveParams sp = wp;
+                sp.sortBins = kRayBins;
+                wf_sort_scan<<<1, WavefrontBuffers::kMaxSortBins, 0, st>>>(sp, b.sortBins);
+                wf_bin_scatter<<<gGen, kShadeBlock, 0, st>>>(b.sortKeys, wp.extQueue, wp.counts + 1, kRayBins, b.sortBins, b.sortQueue);
+                T1();
+                // The sorted order becomes the extension queue (and the next shade
+                // queue); the unsorted buffer is the next bounce's scatter target.
+                uint32_t* sorted = spare;
+                spare = qb;
+                qb = sorted;
+                wp.extQueue = sorted;
+            }
             T0(KC_EXTEND);
             if (shortStack) wf_extend<kShortStack><<<gTraceShort, kTraceBlock, 0, st>>>(s, p, wp, w);
             else wf_extend<kStackSize><<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);

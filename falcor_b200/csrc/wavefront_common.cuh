@@ -47,6 +47,9 @@ struct WaveParams {
     uint32_t* slotTile;
     // Queue entries a warp of the trace kernels claims per atomic (0: kFetchChunk).
     uint32_t fetchChunk;
+    // Extension-ray binning: the shade kernel writes the bin key (ray_bin_key)
+    // of extension queue position k to extKeys[k] (null: no binning).
+    uint32_t* extKeys;
 };
 
 // Request of wave slot i in a batched wave.
