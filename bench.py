@@ -49,6 +49,7 @@ def parse_args():
     ap.add_argument("--resolution", default=None, help="WxH override of the workload's frame size (small profiling cases)")
     ap.add_argument("--frames-per-step", type=int, default=FRAMES_PER_STEP, help="16-spp frames per step")
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched secondary metrics")
+    ap.add_argument("--props", default=None, help="JSON object of extra PathTracer properties (tuning experiments)")
     ap.add_argument("--only", choices=["adjoint", "batched", "inverse"], default=None,
                     help="run one secondary metric alone and print it (profiling entry point)")
     return ap.parse_args()
@@ -643,9 +644,11 @@ def main():
     frames = args.frames_per_step
     vb = VBufferRT()
     vb.set_scene(scene)
-    pt = PathTracer({"samplesPerPixel": SPP_PER_FRAME, "maxSurfaceBounces": w.max_bounces,
-                     "maxDiffuseBounces": w.max_bounces, "maxSpecularBounces": w.max_bounces,
-                     "emissiveSampler": "Power", "colorFormat": "LogLuvHDR", "misHeuristic": "Balance"})
+    props = {"samplesPerPixel": SPP_PER_FRAME, "maxSurfaceBounces": w.max_bounces, "maxDiffuseBounces": w.max_bounces,
+             "maxSpecularBounces": w.max_bounces, "emissiveSampler": "Power", "colorFormat": "LogLuvHDR", "misHeuristic": "Balance"}
+    if args.props:
+        props.update(json.loads(args.props))
+    pt = PathTracer(props)
     pt.set_scene(scene)
     vbuf = torch.zeros((Hh, W, 4), dtype=torch.int32, device=dev)
     frame = torch.zeros((Hh, W, 4), dtype=torch.float32, device=dev)
@@ -761,6 +764,8 @@ def main():
         "counters_last_launch": counters,
         "device_error": st.device_error,
     }
+    if args.props:
+        line["config"]["path_tracer_overrides"] = json.loads(args.props)
     if not args.no_extras:
         # Secondary metrics of the same run (every rank does its own replica).
         line["adjoint"] = adjoint_bench(dev)
