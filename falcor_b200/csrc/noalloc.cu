@@ -87,10 +87,12 @@ FPT_API fpt_status fpt_pass_execute_noalloc(fpt_pass* pass, const fpt_frame_io* 
     fp.workCounter = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + kWorkCounterOffset);
     fp.workItems = io->width * io->height;
     path_tracer_params(*pass, fp);
-    // sortShadeQueue and splitMisses need pass-owned queues; they only reorder
-    // work (the samples are the same), so the static layout runs without them.
+    // sortShadeQueue, splitMisses and sortExtensionRays need pass-owned queues;
+    // they only reorder work (the samples are the same), so the static layout
+    // runs without them.
     fp.sortMaterials = false;
     fp.splitMisses = false;
+    fp.sortRays = false;
     // The event counters start at zero; the queue counts are cleared per wave.
     cudaError_t e = cudaMemsetAsync(scratch, 0, kHeaderBytes, st);
     if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, cudaGetErrorString(e));

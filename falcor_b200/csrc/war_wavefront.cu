@@ -689,7 +689,7 @@ cudaError_t run_war_wavefront(const DevScene& s, const WarParams& p, WavefrontBu
     const uint32_t maxIter = p.maxBounces + 2;
     launches = 0;
     for (uint32_t first = 0; first < pixels; first += b.capacity) {
-        WaveParams wp;
+        WaveParams wp{};  // every field not set below stays null / zero (no sort, split, binning)
         wp.waveFirstPixel = first;
         wp.wavePixels = std::min(b.capacity, pixels - first);
         wp.wavePaths = wp.wavePixels;

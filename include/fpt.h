@@ -455,8 +455,8 @@ FPT_API fpt_status fpt_bsdf_probe_run(const fpt_bsdf_probe* probe, uint32_t* his
  * Limits: PathTracer passes with the Wavefront scheduler only (Megakernel is
  * rejected with FPT_ERR_UNSUPPORTED), frames up to 4096 x 4096 (larger sizes
  * are rejected with FPT_ERR_INVALID_ARG).  wavefrontCapacity is replaced by
- * the fixed 16384 paths; sortShadeQueue and splitMisses are not applied (they
- * only reorder work, the samples are the same).  Every call looks up the
+ * the fixed 16384 paths; sortShadeQueue, splitMisses and sortExtensionRays are
+ * not applied (they only reorder work, the samples are the same).  Every call looks up the
  * array's device address (cudaGetSymbolAddress, no stream work) with the
  * calling device current; the first call on a device loads the library's
  * module there and should come before any stream capture.  Calls share the

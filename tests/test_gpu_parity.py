@@ -136,28 +136,34 @@ def test_path_tracer_queue_options_same_samples(torch_cuda, option):
     np.testing.assert_array_equal(out[0], out[1])
 
 
-def test_extension_ray_binning_keeps_every_sample(torch_cuda):
+def test_extension_ray_binning_keeps_every_sample(torch_cuda, oracle):
     """sortExtensionRays reorders each extension queue by origin cell and
-    direction octant; the per-sample radiance, the hits of every vertex and the
-    event counters are unchanged."""
+    direction octant; with and without it every sample matches the oracle (hits
+    of every vertex bit-exact, radiance per sample) and the event counters
+    agree."""
     torch = torch_cuda
     from falcor_b200.scene import Scene
     from falcor_b200.passes import PathTracer
-    scene = Scene(H.small_heightfield())
-    W, Hh, spp = 64, 48, 4
+    host = H.small_heightfield()
+    scene = Scene(host)
+    W, Hh, spp, B = 64, 48, 4, 5
     vb = H.gpu_vbuffer(scene, W, Hh)
-    out = []
+    _, osmp, _, _, otr = H.oracle_scene(host).path_tracer(vb.cpu().numpy().view(np.uint32),
+                                                          H.pt_params(W, Hh, spp, seed=7, max_bounces=B), samples=True, trace=True)
+    counts = []
     for binning in (0, 1):
-        pt = PathTracer(dict(H.pt_props(spp, max_bounces=5, seed=7), sortExtensionRays=binning))
+        pt = PathTracer(dict(H.pt_props(spp, max_bounces=B, seed=7), sortExtensionRays=binning))
         pt.set_scene(scene)
         color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
         smp = torch.zeros((Hh, W, spp, 3), dtype=torch.float32, device="cuda")
-        tr = torch.zeros((Hh, W, spp, 7, 4), dtype=torch.int32, device="cuda")
+        tr = torch.zeros((Hh, W, spp, B + 2, 4), dtype=torch.int32, device="cuda")
         pt.execute({"vbuffer": vb, "color": color}, sample_color=smp, hit_trace=tr)
         torch.cuda.synchronize()
-        out.append((smp.cpu().numpy(), tr.cpu().numpy(), pt.counters(), pt.stats().device_error))
-    (s0, t0, c0, e0), (s1, t1, c1, e1) = out
-    assert np.array_equal(s0.view(np.uint32), s1.view(np.uint32))
-    assert np.array_equal(t0, t1)
-    assert c0["paths"] == c1["paths"] and c0["rays"] == c1["rays"] and c0["hits"] == c1["hits"]
-    assert e0 == 0 and e1 == 0
+        differs, listed = H.compare_hit_traces(tr.cpu().numpy().view(np.uint32), otr)
+        assert not (differs & ~listed).any(), binning
+        exact, _ = H.check_per_sample(smp.cpu().numpy(), osmp, listed, f"binning {binning}")
+        print(f"sortExtensionRays={binning}: {exact:.6f} bit-exact")
+        c = pt.counters()
+        counts.append((c["paths"], c["rays"], c["hits"]))
+        assert pt.stats().device_error == 0
+    assert counts[0] == counts[1]
