@@ -467,7 +467,7 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
                 WaveParams sp = wp;
                 sp.sortBins = kRayBins;
                 wf_sort_scan<<<1, WavefrontBuffers::kMaxSortBins, 0, st>>>(sp, b.sortBins);
-                wf_bin_scatter<<<gGen, kShadeBlock, 0, st>>>(b.sortKeys, wp.extQueue, wp.counts + 1, kRayBins, b.sortBins, b.sortQueue);
+                wf_bin_scatter<<<gGen, kShadeBlock, 0, st>>>(b.sortKeys, wp.extQueue, wp.counts + 1, kRayBins, b.sortBins, spare);
                 T1();
                 // The sorted order becomes the extension queue (and the next shade
                 // queue); the unsorted buffer is the next bounce's scatter target.
