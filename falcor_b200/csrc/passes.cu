@@ -137,11 +137,9 @@ void set_defaults(fpt_pass& p) {
         d["splitMisses"] = PropValue::num(0);
         // Wavefront: counting-sort each extension queue by origin cell (4 x 4 x 4
         // grid over the scene) and direction octant before traversal, so that
-        // the lanes of a warp trace similar rays.  On by default: on the 1080p
-        // heightfield frame extension rays 18.6 -> 15.2 ms and visibility rays
-        // 6.3 -> 5.7 ms per frame for 1.0 ms of sorting (758 -> 814 Mpaths/s).
-        // The bin order also becomes the next shade queue's order.
-        d["sortExtensionRays"] = PropValue::num(1);
+        // the lanes of a warp trace similar rays; the bin order also becomes the
+        // next shade queue's order.
+        d["sortExtensionRays"] = PropValue::num(0);
     } else if (p.type == "VBufferRT") {
         // GBufferBase.h:96-98.
         d["samplePattern"] = PropValue::str("Center");
