@@ -93,6 +93,7 @@ FPT_API fpt_status fpt_pass_execute_noalloc(fpt_pass* pass, const fpt_frame_io* 
     fp.sortMaterials = false;
     fp.splitMisses = false;
     fp.sortRays = false;
+    fp.sortShadowRays = false;
     // The event counters start at zero; the queue counts are cleared per wave.
     cudaError_t e = cudaMemsetAsync(scratch, 0, kHeaderBytes, st);
     if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, cudaGetErrorString(e));

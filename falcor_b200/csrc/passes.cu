@@ -140,6 +140,9 @@ void set_defaults(fpt_pass& p) {
         // the lanes of a warp trace similar rays; the bin order also becomes the
         // next shade queue's order.
         d["sortExtensionRays"] = PropValue::num(0);
+        // The same binning for the visibility rays of NEE (their origin cell and
+        // direction octant), before the shadow kernel.
+        d["sortShadowRays"] = PropValue::num(0);
     } else if (p.type == "VBufferRT") {
         // GBufferBase.h:96-98.
         d["samplePattern"] = PropValue::str("Center");
@@ -424,6 +427,7 @@ void path_tracer_params(fpt_pass& p, FrameParams& fp) {
     fp.sortMaterials = p.num("sortShadeQueue") != 0 ? 1u : 0u;
     fp.splitMisses = p.num("splitMisses") != 0 ? 1u : 0u;
     fp.sortRays = p.num("sortExtensionRays") != 0 ? 1u : 0u;
+    fp.sortShadowRays = p.num("sortShadowRays") != 0 ? 1u : 0u;
 }
 
 }  // namespace fpt
@@ -781,6 +785,7 @@ FPT_API fpt_status fpt_pass_execute(fpt_pass* pass, const fpt_frame_io* io, void
             const bool binRays = fp.sortRays && !fp.splitMisses;
             pass->launches = waves * (4 * (fp.maxSurfaceBounces + 2) + 3 +
                                       (binRays ? 3 * (fp.maxSurfaceBounces + 2) : (fp.sortMaterials ? 3 * (fp.maxSurfaceBounces + 1) : 0)) +
+                                      (fp.sortShadowRays ? 3 * (fp.maxSurfaceBounces + 2) : 0) +
                                       (fp.splitMisses ? fp.maxSurfaceBounces + 1 : 0));
         }
         pass->frameCount++;

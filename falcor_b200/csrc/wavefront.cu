@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(kShadeBlock) wf_generate(DevScene s, FramePara
 
 template <class SG, bool HAS_T, bool TEX = true>
 FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uint32_t i, bool& ext, bool& shadow, Counters& cnt,
-                      const WaveParams* wp = nullptr, uint32_t* binKey = nullptr) {
+                      const WaveParams* wp = nullptr, uint32_t* binKey = nullptr, uint32_t* shadowKey = nullptr) {
     PathState<SG> path;
     load_path(w, i, path);
     if (wp && p.hitTrace)
@@ -109,6 +109,7 @@ FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uin
     else pt_handle_miss<SG>(s, p, path, cnt);
     shadow = path.shadowPending;
     if (shadow) {
+        if (shadowKey) *shadowKey = ray_bin_key(s, path.sOrigin, path.sDir);
         w.sOrigin[i] = make_float4(path.sOrigin.x, path.sOrigin.y, path.sOrigin.z, path.sDist);
         w.sDir[i] = make_float4(path.sDir.x, path.sDir.y, path.sDir.z, 0.f);
         w.sLr[i] = make_float4(path.sLr.x, path.sLr.y, path.sLr.z, 0.f);
@@ -142,17 +143,19 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_SHADE_MIN_BLOCKS) wf_shade(De
     const uint32_t n = wp.counts[0];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k - threadIdx.x < n; k += gridDim.x * blockDim.x) {
         bool ext = false, shadow = false;
-        uint32_t i = 0, key = 0;
+        uint32_t i = 0, key = 0, skey = 0;
         if (k < n) {
             i = wp.shadeQueue[k];
             if (MULTI) {
                 const uint32_t r = slot_request(wp, i);
                 shade_slot<SG, HAS_T>(wp.scenes[r], wp.frames[r], w, i, ext, shadow, cnt);
             } else {
-                shade_slot<SG, HAS_T, TEX>(s, p, w, i, ext, shadow, cnt, &wp, wp.extKeys ? &key : nullptr);
+                shade_slot<SG, HAS_T, TEX>(s, p, w, i, ext, shadow, cnt, &wp, wp.extKeys ? &key : nullptr,
+                                           wp.shadowKeys ? &skey : nullptr);
             }
         }
-        push(shadow, i, wp.shadowQueue, wp.counts + 2);
+        const uint32_t spos = push(shadow, i, wp.shadowQueue, wp.counts + 2);
+        if (!MULTI && wp.shadowKeys && spos != 0xffffffffu) wp.shadowKeys[spos] = skey;
         const uint32_t pos = push(ext, i, wp.extQueue, wp.counts + 1);
         if (!MULTI && wp.extKeys && pos != 0xffffffffu) wp.extKeys[pos] = key;
     }
@@ -405,6 +408,7 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
     // Extension-ray binning (sortExtensionRays) shares the sort buffers and
     // takes precedence over the material sort.
     const bool binRays = p.sortRays && !p.splitMisses && b.owning && b.ensure_sort() == cudaSuccess;
+    const bool binShadow = p.sortShadowRays && b.owning && b.ensure_sort() == cudaSuccess;
     const bool sortQueue = !binRays && p.sortMaterials && b.owning && b.ensure_sort() == cudaSuccess;
     const uint32_t sortBins = std::min<uint32_t>(std::max<uint32_t>(s.materialCount, 1u), WavefrontBuffers::kMaxSortBins - 1u) + 1u;
     // Hit/miss split of the shade stage.
@@ -427,6 +431,7 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
         wp.sortKeys = sortQueue ? b.sortKeys : nullptr;
         wp.sortBins = sortBins;
         wp.extKeys = binRays ? b.sortKeys : nullptr;
+        wp.shadowKeys = binShadow ? b.shadowKeys : nullptr;
         uint32_t* qHit = qa;
         uint32_t* qMiss = b.missQueue;
         uint32_t* qNextHit = b.nextHitQueue;
@@ -454,9 +459,24 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
             else launch_shade<SG, HAS_T, false>(s, p, wp, w, gShade, st);
             if (split && it > 0) wf_miss<SG><<<gGen, kShadeBlock, 0, st>>>(s, p, wp, w);
             T1();
+            WaveParams ws = wp;  // the visibility kernel's view (binned queue)
+            if (binShadow) {
+                T0(KC_SORT);
+                constexpr uint32_t kRayBins = 512;
+                e = cudaMemsetAsync(b.sortBins, 0, WavefrontBuffers::kMaxSortBins * sizeof(uint32_t), st);
+                if (e != cudaSuccess) return e;
+                wf_bin_count<<<gGen, kShadeBlock, 0, st>>>(b.shadowKeys, wp.counts + 2, kRayBins, b.sortBins);
+                WaveParams sp = wp;
+                sp.sortBins = kRayBins;
+                wf_sort_scan<<<1, WavefrontBuffers::kMaxSortBins, 0, st>>>(sp, b.sortBins);
+                wf_bin_scatter<<<gGen, kShadeBlock, 0, st>>>(b.shadowKeys, wp.shadowQueue, wp.counts + 2, kRayBins, b.sortBins,
+                                                             b.shadowSorted);
+                T1();
+                ws.shadowQueue = b.shadowSorted;
+            }
             T0(KC_SHADOW);
-            if (shortStack) wf_shadow<kShortStack><<<gTraceShort, kTraceBlock, 0, st>>>(s, p, wp, w);
-            else wf_shadow<kStackSize><<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
+            if (shortStack) wf_shadow<kShortStack><<<gTraceShort, kTraceBlock, 0, st>>>(s, p, ws, w);
+            else wf_shadow<kStackSize><<<gTrace, kTraceBlock, 0, st>>>(s, p, ws, w);
             T1();
             if (binRays) {
                 T0(KC_SORT);
@@ -641,13 +661,15 @@ cudaError_t WavefrontBuffers::ensure_sort() {
     if (sortBase) cudaFree(sortBase);
     sortBase = nullptr;
     sortCapacity = 0;
-    const size_t bytes = 2 * size_t(capacity) * sizeof(uint32_t) + 2 * kMaxSortBins * sizeof(uint32_t);
+    const size_t bytes = 4 * size_t(capacity) * sizeof(uint32_t) + 2 * kMaxSortBins * sizeof(uint32_t);
     cudaError_t e = cudaMalloc(&sortBase, bytes);
     if (e != cudaSuccess) { sortBase = nullptr; return e; }
     sortCapacity = capacity;
     sortKeys = static_cast<uint32_t*>(sortBase);
     sortQueue = sortKeys + capacity;
-    sortBins = sortQueue + capacity;
+    shadowKeys = sortQueue + capacity;
+    shadowSorted = shadowKeys + capacity;
+    sortBins = shadowSorted + capacity;
     return cudaSuccess;
 }
 

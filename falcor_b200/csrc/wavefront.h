@@ -30,6 +30,8 @@ struct WavefrontBuffers {
     uint32_t* sortKeys = nullptr;
     uint32_t* sortQueue = nullptr;
     uint32_t* sortBins = nullptr;  // kMaxSortBins counts + kMaxSortBins cursors
+    uint32_t* shadowKeys = nullptr;    // visibility-ray binning: keys and the sorted queue
+    uint32_t* shadowSorted = nullptr;
     static constexpr uint32_t kMaxSortBins = 1024;
     // Hit/miss split of the shade stage (owning mode only): the extension
     // kernel pushes hits and misses into separate next-bounce queues.

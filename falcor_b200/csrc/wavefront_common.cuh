@@ -50,6 +50,7 @@ struct WaveParams {
     // Extension-ray binning: the shade kernel writes the bin key (ray_bin_key)
     // of extension queue position k to extKeys[k] (null: no binning).
     uint32_t* extKeys;
+    uint32_t* shadowKeys;  // visibility-ray binning keys at shadow queue positions (null: none)
 };
 
 // Request of wave slot i in a batched wave.

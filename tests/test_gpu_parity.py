@@ -137,10 +137,10 @@ def test_path_tracer_queue_options_same_samples(torch_cuda, option):
 
 
 def test_extension_ray_binning_keeps_every_sample(torch_cuda, oracle):
-    """sortExtensionRays reorders each extension queue by origin cell and
-    direction octant; with and without it every sample matches the oracle (hits
-    of every vertex bit-exact, radiance per sample) and the event counters
-    agree."""
+    """sortExtensionRays / sortShadowRays reorder each extension / visibility
+    queue by origin cell and direction octant; with and without them every
+    sample matches the oracle (hits of every vertex bit-exact, radiance per
+    sample) and the event counters agree."""
     torch = torch_cuda
     from falcor_b200.scene import Scene
     from falcor_b200.passes import PathTracer
@@ -151,8 +151,8 @@ def test_extension_ray_binning_keeps_every_sample(torch_cuda, oracle):
     _, osmp, _, _, otr = H.oracle_scene(host).path_tracer(vb.cpu().numpy().view(np.uint32),
                                                           H.pt_params(W, Hh, spp, seed=7, max_bounces=B), samples=True, trace=True)
     counts = []
-    for binning in (0, 1):
-        pt = PathTracer(dict(H.pt_props(spp, max_bounces=B, seed=7), sortExtensionRays=binning))
+    for binning in ((0, 0), (1, 0), (0, 1), (1, 1)):
+        pt = PathTracer(dict(H.pt_props(spp, max_bounces=B, seed=7), sortExtensionRays=binning[0], sortShadowRays=binning[1]))
         pt.set_scene(scene)
         color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
         smp = torch.zeros((Hh, W, spp, 3), dtype=torch.float32, device="cuda")
@@ -162,8 +162,8 @@ def test_extension_ray_binning_keeps_every_sample(torch_cuda, oracle):
         differs, listed = H.compare_hit_traces(tr.cpu().numpy().view(np.uint32), otr)
         assert not (differs & ~listed).any(), binning
         exact, _ = H.check_per_sample(smp.cpu().numpy(), osmp, listed, f"binning {binning}")
-        print(f"sortExtensionRays={binning}: {exact:.6f} bit-exact")
+        print(f"sortExtensionRays={binning[0]} sortShadowRays={binning[1]}: {exact:.6f} bit-exact")
         c = pt.counters()
         counts.append((c["paths"], c["rays"], c["hits"]))
         assert pt.stats().device_error == 0
-    assert counts[0] == counts[1]
+    assert all(c == counts[0] for c in counts)
