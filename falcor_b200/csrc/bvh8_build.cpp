@@ -2,8 +2,8 @@
 //
 // The reference path has no software triangle BVH (DXR builds the
 // acceleration structures in the driver, Scene::buildBlas Scene.cpp:3376), so
-// this is new work: a binned-SAH binary BVH (leaves of at most 3 triangles),
-// collapsed to 8-wide nodes by repeatedly opening the largest child, with the
+// this is new work: a binned-SAH binary BVH with spatial splits (leaves of at
+// most 3 triangle references), collapsed to 8-wide nodes by repeatedly opening the largest child, with the
 // child slots ordered by direction octant so that traversal can visit them
 // approximately front to back, and the child boxes quantised to 8 bits per
 // plane relative to a per-node origin and power-of-two scale.  Quantisation is
@@ -48,15 +48,62 @@ struct Node2 {
     uint32_t first = 0, count = 0; // leaf (count > 0)
 };
 
-constexpr uint32_t kMaxLeaf = 3;
+// Leaf size limit (the node's leaf meta byte holds a 3-bit count and a 5-bit
+// offset into a 32-triangle window, so 8 leaves of at most 4 triangles fit)
+// and the SAH cost of a binary traversal step relative to one triangle test.
+#ifndef FPT_BVH_MAX_LEAF
+#define FPT_BVH_MAX_LEAF 3
+#endif
+#ifndef FPT_BVH_TRAV_COST
+#define FPT_BVH_TRAV_COST 0.5f
+#endif
+constexpr uint32_t kMaxLeaf = FPT_BVH_MAX_LEAF;
+static_assert(kMaxLeaf >= 1 && kMaxLeaf * 8 <= 32, "leaf triangles of a node must fit the 32-bit window");
 constexpr int kBins = 16;
 
+// Spatial splits (split BVH): a node may also split at a plane through its
+// box, cutting the triangles that straddle the plane into two references
+// whose boxes bound only the triangle's part on each side.  They are tried when
+// the best object split's children overlap by more than kSplitAlpha of the
+// root's area, within a budget of extra references (a fraction of the triangle
+// count, handed down in proportion to the references of each subtree so that
+// the tree does not depend on thread timing).  A triangle can then sit in
+// several leaves; every copy is a full triangle record, so traversal results
+// are unchanged (a repeated test finds the same t and triangle index).
+#ifndef FPT_BVH_SPLIT_BUDGET
+#define FPT_BVH_SPLIT_BUDGET 1.0
+#endif
+constexpr double kSplitBudget = FPT_BVH_SPLIT_BUDGET;
+#ifndef FPT_BVH_SPLIT_ALPHA
+#define FPT_BVH_SPLIT_ALPHA 1e-4f
+#endif
+constexpr float kSplitAlpha = FPT_BVH_SPLIT_ALPHA;
+constexpr int kSpatialBins = 32;
+
+struct Ref {
+    AABB box;
+    uint32_t tri;
+};
+
+// Rounds a double down / up to a float that bounds it.
+inline float round_down(double v) {
+    float f = float(v);
+    if (double(f) > v) f = std::nextafter(f, -std::numeric_limits<float>::infinity());
+    return f;
+}
+inline float round_up(double v) {
+    float f = float(v);
+    if (double(f) < v) f = std::nextafter(f, std::numeric_limits<float>::infinity());
+    return f;
+}
+
 struct Builder2 {
-    std::vector<AABB> triBox;
-    std::vector<float> cen;  // 3 per triangle
-    std::vector<uint32_t> idx;
+    const std::vector<float>* verts = nullptr;  // 9 floats per triangle
     std::vector<Node2> nodes;
+    std::vector<uint32_t> leafTris;  // triangle of each leaf reference
     std::atomic<uint32_t> nextNode{0};
+    std::atomic<uint32_t> nextLeaf{0};
+    float minOverlap = 0.f;
 
     uint32_t alloc() {
         uint32_t n = nextNode.fetch_add(1);
@@ -64,20 +111,68 @@ struct Builder2 {
         return n;
     }
 
-    void build(uint32_t node, uint32_t first, uint32_t count, int depth) {
+    // Bounds of triangle t's part inside lo <= x[a] <= hi (double precision,
+    // rounded outward), intersected with `within`.  Returns false when the
+    // part is empty.
+    bool clip(uint32_t t, int a, float lo, float hi, const AABB& within, AABB& out) const {
+        const float* v = &(*verts)[size_t(t) * 9];
+        double blo[3] = {INFINITY, INFINITY, INFINITY}, bhi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        auto grow = [&](const double* q) {
+            for (int k = 0; k < 3; k++) { blo[k] = std::min(blo[k], q[k]); bhi[k] = std::max(bhi[k], q[k]); }
+        };
+        for (int e = 0; e < 3; e++) {
+            const float* pf = v + e * 3;
+            const float* qf = v + ((e + 1) % 3) * 3;
+            const double P[3] = {pf[0], pf[1], pf[2]}, Q[3] = {qf[0], qf[1], qf[2]};
+            if (P[a] >= lo && P[a] <= hi) grow(P);
+            for (const double c : {double(lo), double(hi)}) {
+                if ((P[a] < c && Q[a] > c) || (P[a] > c && Q[a] < c)) {
+                    const double f = (c - P[a]) / (Q[a] - P[a]);
+                    double X[3];
+                    for (int k = 0; k < 3; k++) X[k] = P[k] + f * (Q[k] - P[k]);
+                    X[a] = c;
+                    grow(X);
+                }
+            }
+        }
+        if (!(blo[0] <= bhi[0])) return false;
+        for (int k = 0; k < 3; k++) {
+            out.lo[k] = std::max(round_down(blo[k]), within.lo[k]);
+            out.hi[k] = std::min(round_up(bhi[k]), within.hi[k]);
+        }
+        out.lo[a] = std::max(out.lo[a], lo);
+        out.hi[a] = std::min(out.hi[a], hi);
+        for (int k = 0; k < 3; k++)
+            if (out.lo[k] > out.hi[k]) return false;
+        return true;
+    }
+
+    void make_leaf(Node2& nd, const std::vector<Ref>& refs) {
+        const uint32_t first = nextLeaf.fetch_add(uint32_t(refs.size()));
+        if (size_t(first) + refs.size() > leafTris.size()) throw std::runtime_error("BVH reference pool exhausted");
+        for (size_t i = 0; i < refs.size(); i++) leafTris[first + i] = refs[i].tri;
+        nd.first = first;
+        nd.count = uint32_t(refs.size());
+    }
+
+    void build(uint32_t node, std::vector<Ref>& refs, int depth, int64_t budget) {
         Node2& nd = nodes[node];
+        const uint32_t count = uint32_t(refs.size());
         AABB box, cbox;
         box.reset();
         cbox.reset();
-        for (uint32_t i = first; i < first + count; i++) {
-            box.grow(triBox[idx[i]]);
-            cbox.grow(&cen[size_t(idx[i]) * 3]);
+        for (const Ref& r : refs) {
+            box.grow(r.box);
+            float c[3];
+            for (int a = 0; a < 3; a++) c[a] = 0.5f * (r.box.lo[a] + r.box.hi[a]);
+            cbox.grow(c);
         }
         nd.box = box;
-        if (count <= 1) { nd.first = first; nd.count = count; return; }
-        // Binned SAH over the three axes.
+        if (count <= 1) { make_leaf(nd, refs); return; }
+        // Binned SAH object split over the three axes.
         float bestCost = std::numeric_limits<float>::max();
         int bestAxis = -1, bestSplit = -1;
+        AABB bestL, bestR;
         for (int a = 0; a < 3; a++) {
             float ext = cbox.hi[a] - cbox.lo[a];
             if (!(ext > 0.f)) continue;
@@ -85,12 +180,12 @@ struct Builder2 {
             uint32_t bc[kBins] = {0};
             for (auto& b : bb) b.reset();
             const float k = float(kBins) * (1.f - 1e-6f) / ext;
-            for (uint32_t i = first; i < first + count; i++) {
-                int b = std::min(kBins - 1, int((cen[size_t(idx[i]) * 3 + a] - cbox.lo[a]) * k));
-                bb[b].grow(triBox[idx[i]]);
+            for (const Ref& r : refs) {
+                int b = std::min(kBins - 1, int((0.5f * (r.box.lo[a] + r.box.hi[a]) - cbox.lo[a]) * k));
+                bb[b].grow(r.box);
                 bc[b]++;
             }
-            float rightArea[kBins];
+            AABB rightBox[kBins];
             uint32_t rightCount[kBins];
             AABB acc;
             acc.reset();
@@ -98,7 +193,7 @@ struct Builder2 {
             for (int b = kBins - 1; b > 0; b--) {
                 acc.grow(bb[b]);
                 n += bc[b];
-                rightArea[b] = acc.area();
+                rightBox[b] = acc;
                 rightCount[b] = n;
             }
             acc.reset();
@@ -107,42 +202,133 @@ struct Builder2 {
                 acc.grow(bb[b]);
                 n += bc[b];
                 if (n == 0 || rightCount[b + 1] == 0) continue;
-                float cost = acc.area() * float(n) + rightArea[b + 1] * float(rightCount[b + 1]);
-                if (cost < bestCost) { bestCost = cost; bestAxis = a; bestSplit = b; }
+                float cost = acc.area() * float(n) + rightBox[b + 1].area() * float(rightCount[b + 1]);
+                if (cost < bestCost) { bestCost = cost; bestAxis = a; bestSplit = b; bestL = acc; bestR = rightBox[b + 1]; }
+            }
+        }
+        // Spatial split, when the object split's children overlap.
+        int spatialAxis = -1;
+        float spatialPos = 0.f;
+        if (budget > 0 && depth < 40) {
+            float overlap = 0.f;
+            if (bestAxis >= 0) {
+                AABB o;
+                for (int a = 0; a < 3; a++) { o.lo[a] = std::max(bestL.lo[a], bestR.lo[a]); o.hi[a] = std::min(bestL.hi[a], bestR.hi[a]); }
+                overlap = (o.lo[0] <= o.hi[0] && o.lo[1] <= o.hi[1] && o.lo[2] <= o.hi[2]) ? o.area() : 0.f;
+            }
+            if (bestAxis < 0 || overlap > minOverlap) {
+                for (int a = 0; a < 3; a++) {
+                    const float ext = box.hi[a] - box.lo[a];
+                    if (!(ext > 0.f)) continue;
+                    float planes[kSpatialBins + 1];
+                    for (int b = 0; b <= kSpatialBins; b++) planes[b] = box.lo[a] + ext * (float(b) / float(kSpatialBins));
+                    planes[kSpatialBins] = box.hi[a];
+                    const float k = float(kSpatialBins) / ext;
+                    auto binOf = [&](float x) { return std::min(kSpatialBins - 1, std::max(0, int((x - box.lo[a]) * k))); };
+                    AABB bb[kSpatialBins];
+                    uint32_t enter[kSpatialBins] = {0}, exit[kSpatialBins] = {0};
+                    for (auto& b : bb) b.reset();
+                    for (const Ref& r : refs) {
+                        const int b0 = binOf(r.box.lo[a]), b1 = binOf(r.box.hi[a]);
+                        if (b0 == b1) {
+                            bb[b0].grow(r.box);
+                        } else {
+                            for (int b = b0; b <= b1; b++) {
+                                AABB c;
+                                if (clip(r.tri, a, planes[b], planes[b + 1], r.box, c)) bb[b].grow(c);
+                            }
+                        }
+                        enter[b0]++;
+                        exit[b1]++;
+                    }
+                    AABB rightBox[kSpatialBins];
+                    uint32_t rightCount[kSpatialBins];
+                    AABB acc;
+                    acc.reset();
+                    uint32_t n = 0;
+                    for (int b = kSpatialBins - 1; b > 0; b--) {
+                        acc.grow(bb[b]);
+                        n += exit[b];
+                        rightBox[b] = acc;
+                        rightCount[b] = n;
+                    }
+                    acc.reset();
+                    n = 0;
+                    for (int b = 0; b < kSpatialBins - 1; b++) {
+                        acc.grow(bb[b]);
+                        n += enter[b];
+                        if (n == 0 || rightCount[b + 1] == 0) continue;
+                        const float cost = acc.area() * float(n) + rightBox[b + 1].area() * float(rightCount[b + 1]);
+                        if (cost < bestCost && int64_t(n) + int64_t(rightCount[b + 1]) - int64_t(count) <= budget) {
+                            bestCost = cost;
+                            spatialAxis = a;
+                            spatialPos = planes[b + 1];
+                        }
+                    }
+                }
             }
         }
         const float leafCost = box.area() * float(count);
-        const float travCost = box.area() * 0.5f;
-        if (count <= kMaxLeaf && (bestAxis < 0 || leafCost <= bestCost + travCost)) {
-            nd.first = first;
-            nd.count = count;
+        const float travCost = box.area() * float(FPT_BVH_TRAV_COST);
+        if (count <= kMaxLeaf && ((bestAxis < 0 && spatialAxis < 0) || leafCost <= bestCost + travCost)) {
+            make_leaf(nd, refs);
             return;
         }
-        uint32_t mid;
-        if (bestAxis < 0) {
-            mid = first + count / 2;  // all centroids equal: split by index
-        } else {
-            const float ext = cbox.hi[bestAxis] - cbox.lo[bestAxis];
-            const float k = float(kBins) * (1.f - 1e-6f) / ext;
-            auto it = std::partition(idx.begin() + first, idx.begin() + first + count, [&](uint32_t t) {
-                int b = std::min(kBins - 1, int((cen[size_t(t) * 3 + bestAxis] - cbox.lo[bestAxis]) * k));
-                return b <= bestSplit;
-            });
-            mid = uint32_t(it - idx.begin());
-            if (mid == first || mid == first + count) mid = first + count / 2;
+        std::vector<Ref> left, right;
+        if (spatialAxis >= 0) {
+            const int a = spatialAxis;
+            for (const Ref& r : refs) {
+                if (r.box.hi[a] <= spatialPos) left.push_back(r);
+                else if (r.box.lo[a] >= spatialPos) right.push_back(r);
+                else {
+                    Ref l{r.box, r.tri}, q{r.box, r.tri};
+                    const bool hasL = clip(r.tri, a, -std::numeric_limits<float>::max(), spatialPos, r.box, l.box);
+                    const bool hasR = clip(r.tri, a, spatialPos, std::numeric_limits<float>::max(), r.box, q.box);
+                    if (hasL) left.push_back(l);
+                    if (hasR) right.push_back(q);
+                    if (!hasL && !hasR) left.push_back(r);  // cannot happen for a straddling box; keep the reference
+                }
+            }
+            if (left.empty() || right.empty() || (left.size() == count && right.size() == count)) {
+                left.clear();
+                right.clear();
+                spatialAxis = -1;
+            }
         }
+        if (spatialAxis < 0) {
+            if (bestAxis < 0) {
+                // All centroids equal: split by position in the list.
+                left.assign(refs.begin(), refs.begin() + count / 2);
+                right.assign(refs.begin() + count / 2, refs.end());
+            } else {
+                const float ext = cbox.hi[bestAxis] - cbox.lo[bestAxis];
+                const float k = float(kBins) * (1.f - 1e-6f) / ext;
+                for (const Ref& r : refs) {
+                    int b = std::min(kBins - 1, int((0.5f * (r.box.lo[bestAxis] + r.box.hi[bestAxis]) - cbox.lo[bestAxis]) * k));
+                    (b <= bestSplit ? left : right).push_back(r);
+                }
+                if (left.empty() || right.empty()) {
+                    left.assign(refs.begin(), refs.begin() + count / 2);
+                    right.assign(refs.begin() + count / 2, refs.end());
+                }
+            }
+        }
+        const int64_t extra = int64_t(left.size() + right.size()) - int64_t(count);
+        const int64_t rest = std::max<int64_t>(0, budget - extra);
+        const int64_t budgetL = int64_t(double(rest) * double(left.size()) / double(left.size() + right.size()));
+        const int64_t budgetR = rest - budgetL;
+        std::vector<Ref>().swap(refs);
         uint32_t l = alloc(), r = alloc();
         nd.left = l;
         nd.right = r;
         nd.count = 0;
-        const uint32_t nl = mid - first, nr = first + count - mid;
         if (count > 200000 && depth < 6) {
-            auto f = std::async(std::launch::async, [&, l, first, nl, depth] { build(l, first, nl, depth + 1); });
-            build(r, mid, nr, depth + 1);
+            auto f = std::async(std::launch::async, [&, l, depth, budgetL] { build(l, left, depth + 1, budgetL); });
+            build(r, right, depth + 1, budgetR);
             f.get();
         } else {
-            build(l, first, nl, depth + 1);
-            build(r, mid, nr, depth + 1);
+            build(l, left, depth + 1, budgetL);
+            build(r, right, depth + 1, budgetR);
         }
     }
 };
@@ -283,7 +469,7 @@ struct Collapse {
                 if (c.count > 0) {
                     if (c.count > kMaxLeaf) throw std::runtime_error("BVH leaf too large");
                     n.meta[k] = uint8_t((c.count << 5) | triOffset);
-                    for (uint32_t t = 0; t < c.count; t++) emitTri(b2.idx[c.first + t]);
+                    for (uint32_t t = 0; t < c.count; t++) emitTri(b2.leafTris[c.first + t]);
                     triOffset += c.count;
                 } else {
                     n.imask |= uint8_t(1u << k);
@@ -326,23 +512,26 @@ void build_bvh8(const std::vector<float>& triVerts, const std::vector<uint32_t>&
         return;
     }
     Builder2 b;
-    b.triBox.resize(n);
-    b.cen.resize(size_t(n) * 3);
-    b.idx.resize(n);
+    b.verts = &triVerts;
+    std::vector<Ref> refs(n);
     for (uint32_t t = 0; t < n; t++) {
-        AABB bx;
-        bx.reset();
-        for (int v = 0; v < 3; v++) bx.grow(&triVerts[size_t(t) * 9 + size_t(v) * 3]);
-        b.triBox[t] = bx;
-        for (int a = 0; a < 3; a++) b.cen[size_t(t) * 3 + a] = 0.5f * (bx.lo[a] + bx.hi[a]);
-        b.idx[t] = t;
+        refs[t].box.reset();
+        for (int v = 0; v < 3; v++) refs[t].box.grow(&triVerts[size_t(t) * 9 + size_t(v) * 3]);
+        refs[t].tri = t;
     }
-    b.nodes.resize(size_t(n) * 2 + 1);
+    const int64_t budget = int64_t(double(n) * kSplitBudget);
+    const size_t maxRefs = size_t(n) + size_t(budget);
+    b.nodes.resize(maxRefs * 2 + 1);
+    b.leafTris.resize(maxRefs);
+    AABB rootBox;
+    rootBox.reset();
+    for (const Ref& r : refs) rootBox.grow(r.box);
+    b.minOverlap = kSplitAlpha * rootBox.area();
     uint32_t root = b.alloc();
-    b.build(root, 0, n, 0);
+    b.build(root, refs, 0, budget);
     for (int a = 0; a < 3; a++) { out.lo[a] = b.nodes[root].box.lo[a]; out.hi[a] = b.nodes[root].box.hi[a]; }
-    out.nodes.reserve(n / 3 + 16);
-    out.tris.reserve(n);
+    out.nodes.reserve(maxRefs / 3 + 16);
+    out.tris.reserve(maxRefs);
     Collapse c{b, triVerts, triInstance, triPrim, out};
     c.run(root);
     out.maxDepth = c.maxDepth;

@@ -129,8 +129,10 @@ struct BVH8 {
     double buildSeconds = 0;
 };
 
-// Builds a binned-SAH binary BVH, collapses it to 8-wide nodes with octant
-// slot ordering and quantises the child boxes conservatively.
+// Builds a binned-SAH binary BVH with spatial splits (a triangle may be
+// referenced by several leaves, each with its own record), collapses it to
+// 8-wide nodes with octant slot ordering and quantises the child boxes
+// conservatively.
 void build_bvh8(const std::vector<float>& triVerts,  // 9 floats per global triangle
                 const std::vector<uint32_t>& triInstance, const std::vector<uint32_t>& triPrim, BVH8& out);
 

@@ -369,7 +369,7 @@ fpt_status create_scene(const fpt_scene_desc& d, fpt_scene*& out) {
     ds.hasEmissive = em.empty() ? 0u : 1u;
     ds.hasTransmission = hasTransmission ? 1u : 0u;
     ds.nodeCount = uint32_t(s.bvh.nodes.size());
-    ds.triCount = total;
+    ds.triCount = uint32_t(s.bvh.tris.size());  // triangle records (spatial splits repeat a triangle)
     ds.bvhDepth = s.bvh.maxDepth;
     for (int a = 0; a < 3; a++) {
         ds.sceneLo[a] = s.bvh.lo[a];
