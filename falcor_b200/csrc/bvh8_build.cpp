@@ -59,7 +59,10 @@ struct Node2 {
 #endif
 constexpr uint32_t kMaxLeaf = FPT_BVH_MAX_LEAF;
 static_assert(kMaxLeaf >= 1 && kMaxLeaf * 8 <= 32, "leaf triangles of a node must fit the 32-bit window");
-constexpr int kBins = 16;
+#ifndef FPT_BVH_BINS
+#define FPT_BVH_BINS 16
+#endif
+constexpr int kBins = FPT_BVH_BINS;
 
 // Spatial splits (split BVH): a node may also split at a plane through its
 // box, cutting the triangles that straddle the plane into two references
@@ -78,7 +81,10 @@ constexpr double kSplitBudget = FPT_BVH_SPLIT_BUDGET;
 #define FPT_BVH_SPLIT_ALPHA 1e-4f
 #endif
 constexpr float kSplitAlpha = FPT_BVH_SPLIT_ALPHA;
-constexpr int kSpatialBins = 32;
+#ifndef FPT_BVH_SPATIAL_BINS
+#define FPT_BVH_SPATIAL_BINS 32
+#endif
+constexpr int kSpatialBins = FPT_BVH_SPATIAL_BINS;
 
 struct Ref {
     AABB box;

@@ -262,9 +262,8 @@ FPT_D void trace_queue(const DevScene& s, const FrameParams& p, const WaveParams
                                 wp.sortKeys[qpos] = key;
                             }
                         }
-                        float4 d = w.dirV[path];
-                        d.w = __uint_as_float(f);
-                        w.dirV[path] = d;
+                        // Only the flags word changes: a 4-byte store, no re-read of the direction.
+                        reinterpret_cast<uint32_t*>(w.dirV + path)[3] = f;
                     }
                 }
             }
