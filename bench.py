@@ -716,6 +716,8 @@ def main():
     breakdown = {k: {"ms_per_frame": round(ktimes[k][0] / frames_timed, 3), "launches_per_frame": ktimes[k][1] / frames_timed,
                      "algorithmic_GBps": round(cat_bytes[k] * frames_timed / max(ktimes[k][0], 1e-9) / 1e6, 2) if k in cat_bytes else None}
                  for k in ktimes}
+    for k, b in breakdown.items():  # each kernel's own fraction of the HBM peak
+        b["frac"] = round(b["algorithmic_GBps"] / hbm, 4) if b["algorithmic_GBps"] is not None and ktimes[k][0] > 0 else None
     alg = algorithmic_bytes(counters, W * Hh)
     rays_per_step = counters["rays"] * frames
 

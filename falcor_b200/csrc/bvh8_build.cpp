@@ -9,6 +9,7 @@
 // plane relative to a per-node origin and power-of-two scale.  Quantisation is
 // conservative with respect to the exact device decoding, fmaf(q, scale, p).
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -81,6 +82,15 @@ constexpr double kSplitBudget = FPT_BVH_SPLIT_BUDGET;
 #define FPT_BVH_SPLIT_ALPHA 1e-4f
 #endif
 constexpr float kSplitAlpha = FPT_BVH_SPLIT_ALPHA;
+// Collapse of the binary tree into 8-wide nodes: 1 = SAH-optimal (dynamic
+// programming, with kPrimCost the cost of a reference test relative to a node
+// visit), 0 = repeatedly open the child of largest area.
+#ifndef FPT_BVH_COLLAPSE_DP
+#define FPT_BVH_COLLAPSE_DP 0
+#endif
+#ifndef FPT_BVH_PRIM_COST
+#define FPT_BVH_PRIM_COST 0.3
+#endif
 #ifndef FPT_BVH_SPATIAL_BINS
 #define FPT_BVH_SPATIAL_BINS 32
 #endif
@@ -403,6 +413,83 @@ struct Collapse {
         out.tris.push_back(r);
     }
 
+    // SAH-optimal collapse (dynamic programming over the binary tree): cost[n][j]
+    // is the least expected cost of covering the subtree of binary node n with
+    // at most j+1 roots, each root an 8-wide node (visit cost kNodeCost times its
+    // area) or a leaf of at most kMaxLeaf references (kPrimCost per reference
+    // times its area).  Children are allocated after their parent, so a reverse
+    // sweep over the node indices sees both children of a node first.
+    std::vector<std::array<float, 8>> cost;
+    std::vector<std::array<uint8_t, 8>> how;  // j > 0: 0 = fewer roots, k = k roots on the left; j = 0: 1 leaf, 2 node
+    std::vector<uint8_t> nodeSplit;           // 8-wide node: (roots on the left) | (all roots << 4)
+    std::vector<uint32_t> refs;
+
+    void optimise(uint32_t nodeCount) {
+        const float kNodeCost = 1.f, kPrimCost = float(FPT_BVH_PRIM_COST);
+        const float inf = std::numeric_limits<float>::infinity();
+        cost.assign(nodeCount, {});
+        how.assign(nodeCount, {});
+        nodeSplit.assign(nodeCount, 0);
+        refs.assign(nodeCount, 0);
+        for (uint32_t n = nodeCount; n-- > 0;) {
+            const Node2& nd = b2.nodes[n];
+            const float A = nd.box.area();
+            auto& C = cost[n];
+            auto& H = how[n];
+            if (nd.count > 0) {
+                refs[n] = nd.count;
+                C.fill(A * kPrimCost * float(nd.count));
+                H.fill(0);
+                H[0] = 1;
+                continue;
+            }
+            refs[n] = refs[nd.left] + refs[nd.right];
+            const auto& L = cost[nd.left];
+            const auto& R = cost[nd.right];
+            float dist[8];
+            uint8_t distK[8];
+            float best = inf;
+            uint8_t bestJ = 0;
+            for (int j = 1; j < 8; j++) {  // j + 1 roots
+                dist[j] = inf;
+                distK[j] = 0;
+                for (int k = 1; k <= j; k++) {  // k roots on the left, j + 1 - k on the right
+                    const float c = L[k - 1] + R[j - k];
+                    if (c < dist[j]) { dist[j] = c; distK[j] = uint8_t(k); }
+                }
+                if (dist[j] < best) { best = dist[j]; bestJ = uint8_t(j); }
+            }
+            nodeSplit[n] = uint8_t(distK[bestJ] | ((bestJ + 1) << 4));
+            const float nodeC = A * kNodeCost + best;
+            const float leafC = refs[n] <= kMaxLeaf ? A * kPrimCost * float(refs[n]) : inf;
+            C[0] = std::min(leafC, nodeC);
+            H[0] = leafC <= nodeC ? 1 : 2;
+            for (int j = 1; j < 8; j++) {
+                if (C[j - 1] <= dist[j]) { C[j] = C[j - 1]; H[j] = 0; }
+                else { C[j] = dist[j]; H[j] = distK[j]; }
+            }
+        }
+    }
+
+    struct Slot { uint32_t node; bool leaf; };
+    void gather(uint32_t n, int roots, std::vector<Slot>& out2) const {
+        const int j = roots - 1;
+        if (j == 0) { out2.push_back({n, how[n][0] == 1}); return; }
+        const uint8_t h = how[n][size_t(j)];
+        if (h == 0) { gather(n, roots - 1, out2); return; }
+        gather(b2.nodes[n].left, h, out2);
+        gather(b2.nodes[n].right, roots - h, out2);
+    }
+    void leaf_refs(uint32_t n, std::vector<uint32_t>& out2) const {
+        const Node2& nd = b2.nodes[n];
+        if (nd.count > 0) {
+            for (uint32_t t = 0; t < nd.count; t++) out2.push_back(b2.leafTris[nd.first + t]);
+            return;
+        }
+        leaf_refs(nd.left, out2);
+        leaf_refs(nd.right, out2);
+    }
+
     // Fills BVH8 node `dst` from binary node `src` (breadth first).
     void run(uint32_t root2) {
         struct Job { uint32_t dst, src, depth; };
@@ -412,23 +499,38 @@ struct Collapse {
         for (size_t qi = 0; qi < queue.size(); qi++) {
             Job job = queue[qi];
             maxDepth = std::max(maxDepth, job.depth);
-            // Gather up to 8 children by opening the largest internal child.
             std::vector<uint32_t> ch;
+            std::vector<bool> chLeaf;
             const Node2& s = b2.nodes[job.src];
-            if (s.count > 0) ch.push_back(job.src);
-            else { ch.push_back(s.left); ch.push_back(s.right); }
-            while (ch.size() < 8) {
-                int best = -1;
-                float bestA = -1.f;
-                for (size_t i = 0; i < ch.size(); i++) {
-                    const Node2& c = b2.nodes[ch[i]];
-                    if (c.count == 0 && c.box.area() > bestA) { bestA = c.box.area(); best = int(i); }
+            if (!cost.empty()) {
+                // Children chosen by the SAH-optimal collapse.
+                std::vector<Slot> slots;
+                if (s.count > 0) slots.push_back({job.src, true});
+                else {
+                    const uint32_t k = nodeSplit[job.src] & 15u, all = nodeSplit[job.src] >> 4;
+                    gather(s.left, int(k), slots);
+                    gather(s.right, int(all - k), slots);
                 }
-                if (best < 0) break;
-                const Node2& c = b2.nodes[ch[size_t(best)]];
-                ch[size_t(best)] = c.left;
-                ch.push_back(c.right);
+                for (const Slot& sl : slots) { ch.push_back(sl.node); chLeaf.push_back(sl.leaf); }
+            } else {
+                // Gather up to 8 children by opening the largest internal child.
+                if (s.count > 0) ch.push_back(job.src);
+                else { ch.push_back(s.left); ch.push_back(s.right); }
+                while (ch.size() < 8) {
+                    int best = -1;
+                    float bestA = -1.f;
+                    for (size_t i = 0; i < ch.size(); i++) {
+                        const Node2& c = b2.nodes[ch[i]];
+                        if (c.count == 0 && c.box.area() > bestA) { bestA = c.box.area(); best = int(i); }
+                    }
+                    if (best < 0) break;
+                    const Node2& c = b2.nodes[ch[size_t(best)]];
+                    ch[size_t(best)] = c.left;
+                    ch.push_back(c.right);
+                }
+                for (uint32_t c : ch) chLeaf.push_back(b2.nodes[c].count > 0);
             }
+            if (ch.size() > 8) throw std::runtime_error("BVH collapse produced more than 8 children");
             // Octant slot assignment: slot k faces corner (k&1 ? +x : -x, k&2 ? +y : -y, k&4 ? +z : -z).
             const Node2& sn = b2.nodes[job.src];
             float pc[3];
@@ -455,11 +557,13 @@ struct Collapse {
                 slotOf[bi] = bs;
             }
             uint32_t slotChild[8];
+            bool slotLeaf[8] = {false};
             bool valid[8] = {false};
             AABB boxes[8];
             for (int k = 0; k < 8; k++) boxes[k].reset();
             for (size_t i = 0; i < ch.size(); i++) {
                 slotChild[slotOf[i]] = ch[i];
+                slotLeaf[slotOf[i]] = chLeaf[i];
                 valid[slotOf[i]] = true;
                 boxes[slotOf[i]] = b2.nodes[ch[i]].box;
             }
@@ -471,12 +575,13 @@ struct Collapse {
             uint32_t triOffset = 0;
             for (int k = 0; k < 8; k++) {
                 if (!valid[k]) continue;
-                const Node2& c = b2.nodes[slotChild[k]];
-                if (c.count > 0) {
-                    if (c.count > kMaxLeaf) throw std::runtime_error("BVH leaf too large");
-                    n.meta[k] = uint8_t((c.count << 5) | triOffset);
-                    for (uint32_t t = 0; t < c.count; t++) emitTri(b2.leafTris[c.first + t]);
-                    triOffset += c.count;
+                if (slotLeaf[k]) {
+                    std::vector<uint32_t> lr;
+                    leaf_refs(slotChild[k], lr);
+                    if (lr.empty() || lr.size() > kMaxLeaf) throw std::runtime_error("BVH leaf too large");
+                    n.meta[k] = uint8_t((lr.size() << 5) | triOffset);
+                    for (uint32_t t : lr) emitTri(t);
+                    triOffset += uint32_t(lr.size());
                 } else {
                     n.imask |= uint8_t(1u << k);
                 }
@@ -539,6 +644,7 @@ void build_bvh8(const std::vector<float>& triVerts, const std::vector<uint32_t>&
     out.nodes.reserve(maxRefs / 3 + 16);
     out.tris.reserve(maxRefs);
     Collapse c{b, triVerts, triInstance, triPrim, out};
+    if (FPT_BVH_COLLAPSE_DP) c.optimise(b.nextNode.load());
     c.run(root);
     out.maxDepth = c.maxDepth;
     out.buildSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
