@@ -321,9 +321,16 @@ FPT_D float3 sample_ggx_vndf(float alpha, float3 wi, float2 u, float& pdf) {
     pdf = eval_pdf_ggx_vndf(alpha, wi, h);
     return h;
 }
-FPT_D float fresnel_schlick(float f0, float f90, float c) { return f0 + (f90 - f0) * fm::pow(hmax(1.f - c, 0.f), 5.f); }
+// Schlick's (1 - cos)^5 (Rendering/Materials/Fresnel.slang:42-51, evalFresnelSchlick
+// writes pow(1 - cosTheta, 5)) as three products, x^2, x^4 and x^4 * x: the
+// same operations in the oracle and in the adjoint's dual numbers.
+FPT_D float pow5(float x) {
+    const float x2 = x * x, x4 = x2 * x2;
+    return x4 * x;
+}
+FPT_D float fresnel_schlick(float f0, float f90, float c) { return f0 + (f90 - f0) * pow5(hmax(1.f - c, 0.f)); }
 FPT_D float3 fresnel_schlick(float3 f0, float c) {
-    float p = fm::pow(hmax(1.f - c, 0.f), 5.f);
+    float p = pow5(hmax(1.f - c, 0.f));
     return f0 + (f3(1.f) - f0) * p;
 }
 FPT_D float fresnel_dielectric(float eta, float ci, float& ct) {

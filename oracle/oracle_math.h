@@ -588,12 +588,20 @@ template <class R> inline V3<R> sample_ggx_vndf(R alpha, V3<R> wi, V2<R> u, R& p
     pdf = eval_pdf_ggx_vndf(alpha, wi, h);
     return h;
 }
+// evalFresnelSchlick (Rendering/Materials/Fresnel.slang:42-51): pow(1 - cosTheta, 5),
+// evaluated as x^2, x^4, x^4 * x (the library does the same, so FP32 results
+// stay bit-identical).
+template <class R> inline R pow5(R x) {
+    R x2 = x * x;
+    R x4 = x2 * x2;
+    return x4 * x;
+}
 template <class R> inline V3<R> fresnel_schlick(V3<R> f0, V3<R> f90, R cosTheta) {
-    R p = pw(vmax(R(1) - cosTheta, R(0)), R(5));
+    R p = pow5(vmax(R(1) - cosTheta, R(0)));
     return f0 + (f90 - f0) * p;
 }
 template <class R> inline R fresnel_schlick(R f0, R f90, R cosTheta) {
-    return f0 + (f90 - f0) * pw(vmax(R(1) - cosTheta, R(0)), R(5));
+    return f0 + (f90 - f0) * pow5(vmax(R(1) - cosTheta, R(0)));
 }
 template <class R> inline R fresnel_dielectric(R eta, R cosThetaI, R& cosThetaT) {
     if (cosThetaI < R(0)) { eta = R(1) / eta; cosThetaI = -cosThetaI; }
