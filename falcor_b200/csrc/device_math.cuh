@@ -452,6 +452,23 @@ struct StandardBSDF {
         float wiDotH = dot(wi, h);
         return eval_pdf_ggx_vndf(alpha, wi, h) / (4.f * wiDotH);
     }
+    // spec_eval and spec_pdf together: the half vector and the NDF are
+    // evaluated once (the same operations, so the same values).
+    FPT_D void spec_eval_pdf(float3 wi, float3 wo, float3& f, float& pdf) const {
+        f = f3(0.f);
+        pdf = 0.f;
+        if (hmin(wi.z, wo.z) < kMinCosTheta) return;
+        if (alpha == 0.f) return;
+        if (!has(L_SPEC_R)) return;
+        float3 h = normalize(wi + wo);
+        float wiDotH = dot(wi, h);
+        float D = eval_ndf_ggx(alpha, h.z);
+        float G = eval_masking_correlated(alpha, wi.z, wo.z);
+        float3 F = fresnel_schlick(specAlbedo, wiDotH);
+        f = F * D * G * 0.25f / wi.z;
+        float G1 = eval_g1_ggx(alpha * alpha, wi.z);
+        pdf = (G1 * D * hmax(0.f, wiDotH) / wi.z) / (4.f * wiDotH);
+    }
     FPT_D float3 st_eval(float3 wi, float3 wo) const {
         if (hmin(wi.z, fabsf(wo.z)) < kMinCosTheta) return f3(0.f);
         if (stAlpha == 0.f) return f3(0.f);
@@ -506,6 +523,31 @@ struct StandardBSDF {
         if (pSR > 0.f) pdf += pSR * spec_pdf(wi, wo);
         if (HAS_TRANSMISSION && pST > 0.f) pdf += pST * st_pdf(wi, wo);
         return pdf;
+    }
+
+    // eval and eval_pdf in one pass (each sum in its own order, as above).
+    FPT_D void eval_with_pdf(float3 wi, float3 wo, float3& r, float& pdf) const {
+        r = f3(0.f);
+        pdf = 0.f;
+        if (pDR > 0.f) {
+            r += (1.f - specTrans) * (1.f - diffTrans) * diffuse_eval(wi, wo);
+            pdf += pDR * diffuse_pdf(wi, wo);
+        }
+        if (HAS_TRANSMISSION && pDT > 0.f) {
+            r += (1.f - specTrans) * diffTrans * difftrans_eval(wi, wo);
+            pdf += pDT * difftrans_pdf(wi, wo);
+        }
+        if (pSR > 0.f) {
+            float3 f;
+            float q;
+            spec_eval_pdf(wi, wo, f, q);
+            r += (1.f - specTrans) * f;
+            pdf += pSR * q;
+        }
+        if (HAS_TRANSMISSION && pST > 0.f) {
+            r += specTrans * (st_eval(wi, wo));
+            pdf += pST * st_pdf(wi, wo);
+        }
     }
 
     template <class SG>

@@ -694,9 +694,35 @@ struct MaterialInstance {
         }
         return bsdf(wiL).eval_pdf(wiL, woL);
     }
+    // eval and evalPdf of one direction, with the BSDF `b` set up for wiL =
+    // toLocal(sd.V) by the caller (shared with sample_with).
+    FPT_D void eval_with_pdf(const ShadingData& sd, const StandardBSDF<HAS_TRANSMISSION>& b, float3 wiL, float3 wo, bool useIS,
+                             float3& f, float& pdf) const {
+        f = f3(0.f);
+        pdf = 0.f;
+        const float3 woL = toLocal(wo);
+        if (!valid_hemisphere(sd, wiL, woL, wo)) return;
+        if (!useIS) {
+            f = b.eval(wiL, woL);
+            if (lobeTypes() & L_TRANSMISSION) {
+                if (hmin(fabsf(wiL.z), fabsf(woL.z)) < kMinCosTheta) return;
+                pdf = 0.5f * woL.z * kInvPi;
+                return;
+            }
+            if (hmin(wiL.z, woL.z) < kMinCosTheta) return;
+            pdf = woL.z * kInvPi;
+            return;
+        }
+        b.eval_with_pdf(wiL, woL, f, pdf);
+    }
     template <class SG>
     FPT_D bool sample(const ShadingData& sd, SG& sg, float3& wo, float3& weight, float& pdf, uint32_t& lobe, bool useIS) const {
         const float3 wiL = toLocal(sd.V);
+        return sample_with(sd, bsdf(wiL), wiL, sg, wo, weight, pdf, lobe, useIS);
+    }
+    template <class SG>
+    FPT_D bool sample_with(const ShadingData& sd, const StandardBSDF<HAS_TRANSMISSION>& b, float3 wiL, SG& sg, float3& wo,
+                           float3& weight, float& pdf, uint32_t& lobe, bool useIS) const {
         float3 woL = f3(0.f);
         if (!useIS) {
             // sampleReference (StandardMaterialInstance.slang:202-230).
@@ -711,10 +737,9 @@ struct MaterialInstance {
             } else {
                 if (hmin(wiL.z, woL.z) < kMinCosTheta || pdf == 0.f) return false;
             }
-            weight = bsdf(wiL).eval(wiL, woL) / pdf;
+            weight = b.eval(wiL, woL) / pdf;
             lobe = woL.z > 0.f ? L_DIFF_R : L_DIFF_T;
         } else {
-            const StandardBSDF<HAS_TRANSMISSION> b = bsdf(wiL);
             if (!b.sample(wiL, woL, pdf, weight, lobe, sg)) return false;
         }
         wo = fromLocal(woL);

@@ -173,6 +173,9 @@ FPT_D void pt_handle_hit(const DevScene& s, const FrameParams& p, PathState<SG>&
     const uint32_t lobeTypes = mi.lobeTypes();
     const bool applyNEE = p.useNEE && (lobeTypes & L_NON_DELTA) != 0;
     path.set(PF_LIGHT_UPPER | PF_LIGHT_LOWER, false);
+    // One BSDF set-up for the light sample's evaluation and the scatter sample.
+    const float3 wiL = mi.toLocal(sd.V);
+    const StandardBSDF<HAS_T> bs = mi.bsdf(wiL);
     if (applyNEE) {
         const bool upper = (lobeTypes & L_NON_DELTA_R) != 0, lower = (lobeTypes & L_NON_DELTA_T) != 0;
         float3 Li, lorigin, ldir;
@@ -181,11 +184,11 @@ FPT_D void pt_handle_hit(const DevScene& s, const FrameParams& p, PathState<SG>&
         path.set(PF_LIGHT_UPPER, upper);
         path.set(PF_LIGHT_LOWER, lower);
         if (validSample) {
-            if (p.useMIS) {
-                const float scatterPdf = mi.evalPdf(sd, ldir, p.useBSDFSampling != 0);
-                Li *= eval_mis(p, lpdf, scatterPdf);
-            }
-            const float3 Lr = mi.eval(sd, ldir) * Li;
+            float3 f;
+            float scatterPdf;
+            mi.eval_with_pdf(sd, bs, wiL, ldir, p.useBSDFSampling != 0, f, scatterPdf);
+            if (p.useMIS) Li *= eval_mis(p, lpdf, scatterPdf);
+            const float3 Lr = f * Li;
             if (any_pos(Lr)) {
                 // The visibility ray is traced by the caller's single traversal
                 // site before the next extension ray; its contribution thp * Lr
@@ -202,7 +205,7 @@ FPT_D void pt_handle_hit(const DevScene& s, const FrameParams& p, PathState<SG>&
     float3 wo, w;
     float bpdf;
     uint32_t lobe;
-    bool valid = mi.sample(sd, path.sg, wo, w, bpdf, lobe, p.useBSDFSampling != 0);
+    bool valid = mi.sample_with(sd, bs, wiL, path.sg, wo, w, bpdf, lobe, p.useBSDFSampling != 0);
     if (valid) {
         path.dir = wo;
         path.thp *= w;
