@@ -116,7 +116,10 @@ FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uin
     }
     ext = path.has(PF_ACTIVE);
     if (binKey && ext) *binKey = ray_bin_key(s, path.origin, path.dir);
-    store_path(w, i, path);
+    // A finished path is read again only for its radiance (its visibility ray
+    // and the collect kernel), so only L is written back.
+    if (ext) store_path(w, i, path);
+    else w.L[i] = make_float4(path.L.x, path.L.y, path.L.z, 0.f);
     if (!ext) cnt.v[0]++;
 }
 
@@ -349,7 +352,7 @@ __global__ void __launch_bounds__(kShadeBlock) wf_miss(DevScene s, FrameParams p
         PathState<SG> path;
         load_path(w, i, path);
         pt_handle_miss<SG>(s, p, path, cnt);
-        store_path(w, i, path);
+        w.L[i] = make_float4(path.L.x, path.L.y, path.L.z, 0.f);  // a miss ends the path: only L is read again
         if (!path.has(PF_ACTIVE)) cnt.v[0]++;
     }
     flush_counters(p.counters, cnt);
