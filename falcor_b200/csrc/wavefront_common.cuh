@@ -134,6 +134,40 @@ FPT_D uint32_t push(bool pred, uint32_t item, uint32_t* q, uint32_t* cnt) {
     return pos;
 }
 
+// Block-aggregated push onto two queues at once: one atomic per queue per
+// block instead of one per warp (every push of a launch goes to the same
+// counter word, whose atomics the L2 serialises).  Every thread of the block
+// must reach the call (block-uniform loops only).  `sh` is 2 * (NW + 1) words
+// of shared memory; positions are returned in posA / posB (0xffffffff: none).
+template <int NW>
+FPT_D void block_push2(bool predA, uint32_t itemA, uint32_t* qA, uint32_t* cntA, bool predB, uint32_t itemB, uint32_t* qB,
+                       uint32_t* cntB, uint32_t* sh, uint32_t& posA, uint32_t& posB) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t mA = __ballot_sync(0xffffffffu, predA), mB = __ballot_sync(0xffffffffu, predB);
+    if (lane == 0) {
+        sh[warp] = __popc(mA);
+        sh[NW + 1 + warp] = __popc(mB);
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        uint32_t* s = sh + threadIdx.x * (NW + 1);
+        uint32_t tot = 0;
+        for (int w = 0; w < NW; w++) {
+            const uint32_t c = s[w];
+            s[w] = tot;
+            tot += c;
+        }
+        s[NW] = tot ? atomicAdd(threadIdx.x ? cntB : cntA, tot) : 0u;
+    }
+    __syncthreads();
+    const uint32_t below = (1u << lane) - 1u;
+    posA = predA ? sh[NW] + sh[warp] + uint32_t(__popc(mA & below)) : 0xffffffffu;
+    posB = predB ? sh[2 * NW + 1] + sh[NW + 1 + warp] + uint32_t(__popc(mB & below)) : 0xffffffffu;
+    __syncthreads();  // the words are reused by the next call
+    if (predA) qA[posA] = itemA;
+    if (predB) qB[posB] = itemB;
+}
+
 // Ray tracing kernels (visibility and extension rays) with per-lane dynamic
 // ray fetch: each warp takes chunks of kFetchChunk queue entries with one
 // atomic and hands them to its idle lanes, and a lane whose ray has finished
