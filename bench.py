@@ -709,7 +709,13 @@ def main():
         cat_bytes["extend"] = oracle_counts["extend"]
         cat_bytes["shadow"] = oracle_counts["shadow"]
     hbm, peak_kind = peaks()
-    dominant = max(("extend", "shadow", "shade"), key=lambda k: ktimes[k][0])
+    # overlapTraces: a bounce's visibility and extension kernels run concurrently on two
+    # streams, so each kernel's event span covers most of their common stage.  The unit is
+    # then the stage ("trace", fork to join), with both kernels' algorithmic bytes.
+    overlapped = ktimes.get("trace", (0.0, 0))[1] > 0
+    if overlapped:
+        cat_bytes["trace"] = cat_bytes["extend"] + cat_bytes["shadow"]
+    dominant = max(("trace", "shade") if overlapped else ("extend", "shadow", "shade"), key=lambda k: ktimes[k][0])
     dom_ms, dom_launches = ktimes[dominant]
     dom_bytes_per_launch = cat_bytes[dominant] * frames_timed / max(dom_launches, 1)
     achieved = cat_bytes[dominant] * frames_timed / (dom_ms / 1e3) / 1e9
@@ -718,6 +724,15 @@ def main():
                  for k in ktimes}
     for k, b in breakdown.items():  # each kernel's own fraction of the HBM peak
         b["frac"] = round(b["algorithmic_GBps"] / hbm, 4) if b["algorithmic_GBps"] is not None and ktimes[k][0] > 0 else None
+        if overlapped and k in ("extend", "shadow"):
+            b["span_overlaps"] = "trace"  # concurrent with the other traversal: the span, not the kernel's own time
+    if dominant == "trace":
+        tr = [None if args.resolution else load_traffic(w.name, k) for k in ("extend", "shadow")]
+        dom_traffic = None if None in tr else tr[0] + tr[1]
+        dom_kernel = "wf_shadow+wf_extend"
+    else:
+        dom_traffic = None if args.resolution else load_traffic(w.name, dominant)
+        dom_kernel = f"wf_{dominant}"
     alg = algorithmic_bytes(counters, W * Hh)
     rays_per_step = counters["rays"] * frames
 
@@ -752,8 +767,8 @@ def main():
                   "bvh_build_s": round(scene.info.bvh_build_seconds, 3)},
         "mrays_per_s": round(rays_per_step * world / (ms_per_step / 1e3) / 1e6, 3),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
-                     "frac": round(achieved / hbm, 4), "traffic": None if args.resolution else load_traffic(w.name, dominant), "peak_kind": peak_kind,
-                     "kernel": f"wf_{dominant}", "kernel_ms_per_launch": round(dom_ms / max(dom_launches, 1), 4),
+                     "frac": round(achieved / hbm, 4), "traffic": dom_traffic, "peak_kind": peak_kind,
+                     "kernel": dom_kernel, "kernel_ms_per_launch": round(dom_ms / max(dom_launches, 1), 4),
                      "algorithmic_bytes_per_launch": int(dom_bytes_per_launch),
                      "frame_algorithmic_bytes": alg, "breakdown": breakdown,
                      "algorithmic_source": oracle_counts["source"] if oracle_counts else "kernel event counters",

@@ -45,6 +45,7 @@ struct FrameParams {
     uint32_t splitMisses;      // wavefront: shade misses in their own kernel
     uint32_t sortRays;         // wavefront: bin each extension queue by origin cell and octant
     uint32_t sortShadowRays;   // wavefront: bin each visibility queue the same way
+    uint32_t overlapTraces;    // wavefront: visibility rays on a second stream, beside the extension rays
     // bookkeeping
     unsigned long long* counters;  // [0] paths, [1] rays
     uint32_t* workCounter;         // persistent scheduling counter (zeroed by the launcher)

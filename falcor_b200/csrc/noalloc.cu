@@ -94,6 +94,7 @@ FPT_API fpt_status fpt_pass_execute_noalloc(fpt_pass* pass, const fpt_frame_io* 
     fp.splitMisses = false;
     fp.sortRays = false;
     fp.sortShadowRays = false;
+    fp.overlapTraces = false;  // the second stream and its events are pass-owned objects
     // The event counters start at zero; the queue counts are cleared per wave.
     cudaError_t e = cudaMemsetAsync(scratch, 0, kHeaderBytes, st);
     if (e != cudaSuccess) return set_error(FPT_ERR_CUDA, cudaGetErrorString(e));

@@ -143,6 +143,11 @@ void set_defaults(fpt_pass& p) {
         // The same binning for the visibility rays of NEE (their origin cell and
         // direction octant), before the shadow kernel.
         d["sortShadowRays"] = PropValue::num(0);
+        // Wavefront: trace a bounce's visibility rays on a second stream while
+        // its extension rays trace on the caller's stream.  The two kernels
+        // touch disjoint path-state fields, so the samples are the same; the
+        // second kernel fills the SMs that the first one's last rays leave idle.
+        d["overlapTraces"] = PropValue::num(1);
     } else if (p.type == "VBufferRT") {
         // GBufferBase.h:96-98.
         d["samplePattern"] = PropValue::str("Center");
@@ -428,6 +433,7 @@ void path_tracer_params(fpt_pass& p, FrameParams& fp) {
     fp.splitMisses = p.num("splitMisses") != 0 ? 1u : 0u;
     fp.sortRays = p.num("sortExtensionRays") != 0 ? 1u : 0u;
     fp.sortShadowRays = p.num("sortShadowRays") != 0 ? 1u : 0u;
+    fp.overlapTraces = p.num("overlapTraces") != 0 ? 1u : 0u;
 }
 
 }  // namespace fpt

@@ -407,8 +407,10 @@ void launch_shade(const DevScene& s, const FrameParams& p, const WaveParams& wp,
 
 template <class SG, bool HAS_T>
 cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st, KernelTimer* kt) {
-    auto T0 = [&](int cat) { if (kt && kt->enabled) kt->begin(cat, st); };
-    auto T1 = [&]() { if (kt && kt->enabled) kt->end(st); };
+    int openPairs[4] = {-1, -1, -1, -1};  // pairs begun by T0 and not yet ended (T0 / T1 nest)
+    int depth = 0;
+    auto T0 = [&](int cat) { const int q = kt && kt->enabled ? kt->begin(cat, st) : -1; if (depth < 4) openPairs[depth] = q; depth++; };
+    auto T1 = [&]() { if (depth > 0 && --depth < 4 && kt) kt->end(openPairs[depth], st); };
     SoA w;
     w.originPdf = b.f4(0); w.dirV = b.f4(1); w.thpB = b.f4(2); w.L = b.f4(3);
     w.sg = reinterpret_cast<uint4*>(b.f4(4)); w.hit = reinterpret_cast<uint4*>(b.f4(5));
@@ -436,6 +438,11 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
     const uint32_t sortBins = std::min<uint32_t>(std::max<uint32_t>(s.materialCount, 1u), WavefrontBuffers::kMaxSortBins - 1u) + 1u;
     // Hit/miss split of the shade stage.
     const bool split = p.splitMisses && b.owning && b.ensure_split() == cudaSuccess;
+    // Visibility rays beside the extension rays: after shading they only add
+    // to L, which the extension kernel neither reads nor writes, and the
+    // extension kernel writes only the hit record and the flags word.
+    const bool overlap = p.overlapTraces && b.owning && b.ensure_aux() == cudaSuccess;
+    const cudaStream_t ss = overlap ? b.aux : st;
     const uint32_t maxIter = p.maxSurfaceBounces + 2;
     for (uint32_t first = 0; first < pixels; first += wavePixels) {
         WaveParams wp{};
@@ -497,10 +504,16 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
                 T1();
                 ws.shadowQueue = b.shadowSorted;
             }
-            T0(KC_SHADOW);
-            if (shortStack) wf_shadow<kShortStack><<<gTraceShort, kTraceBlock, 0, st>>>(s, p, ws, w);
-            else wf_shadow<kStackSize><<<gTrace, kTraceBlock, 0, st>>>(s, p, ws, w);
-            T1();
+            if (overlap) {
+                T0(KC_TRACE);  // ended on the caller's stream after the join
+                if ((e = cudaEventRecord(b.forkEv, st)) != cudaSuccess) return e;
+                if ((e = cudaStreamWaitEvent(b.aux, b.forkEv, 0)) != cudaSuccess) return e;
+            }
+            const int shadowPair = kt && kt->enabled ? kt->begin(KC_SHADOW, ss) : -1;
+            if (shortStack) wf_shadow<kShortStack><<<gTraceShort, kTraceBlock, 0, ss>>>(s, p, ws, w);
+            else wf_shadow<kStackSize><<<gTrace, kTraceBlock, 0, ss>>>(s, p, ws, w);
+            if (kt) kt->end(shadowPair, ss);
+            if (overlap && (e = cudaEventRecord(b.joinEv, b.aux)) != cudaSuccess) return e;
             if (binRays) {
                 T0(KC_SORT);
                 constexpr uint32_t kRayBins = 512;
@@ -523,6 +536,11 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
             if (shortStack) wf_extend<kShortStack><<<gTraceShort, kTraceBlock, 0, st>>>(s, p, wp, w);
             else wf_extend<kStackSize><<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
             T1();
+            // Both traversals of the bounce end before the queues advance.
+            if (overlap) {
+                if ((e = cudaStreamWaitEvent(st, b.joinEv, 0)) != cudaSuccess) return e;
+                T1();
+            }
             wf_advance<<<1, 1, 0, st>>>(wp);
             if (split) {
                 // Hits of this bounce are the next shade queue; the extension
@@ -663,6 +681,29 @@ void WavefrontBuffers::release() {
     missQueue = nextHitQueue = nextMissQueue = nullptr;
 }
 
+cudaError_t WavefrontBuffers::ensure_aux() {
+    if (!owning) return cudaErrorNotSupported;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (aux && auxDevice == dev) return cudaSuccess;
+    release_aux();
+    if ((e = cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking)) != cudaSuccess) { aux = nullptr; return e; }
+    if ((e = cudaEventCreateWithFlags(&forkEv, cudaEventDisableTiming)) != cudaSuccess) { forkEv = nullptr; release_aux(); return e; }
+    if ((e = cudaEventCreateWithFlags(&joinEv, cudaEventDisableTiming)) != cudaSuccess) { joinEv = nullptr; release_aux(); return e; }
+    auxDevice = dev;
+    return cudaSuccess;
+}
+
+void WavefrontBuffers::release_aux() {
+    if (joinEv) cudaEventDestroy(joinEv);
+    if (forkEv) cudaEventDestroy(forkEv);
+    if (aux) cudaStreamDestroy(aux);
+    aux = nullptr;
+    forkEv = joinEv = nullptr;
+    auxDevice = -1;
+}
+
 cudaError_t WavefrontBuffers::ensure_split() {
     if (!owning) return cudaErrorNotSupported;
     if (splitBase && splitCapacity >= capacity) return cudaSuccess;
@@ -724,28 +765,34 @@ cudaError_t launch_path_tracer_wavefront(const DevScene& s, const FrameParams& p
     return uniform ? run_wavefront<UniformSG, false>(s, p, b, st, kt) : run_wavefront<TinyUniformSG, false>(s, p, b, st, kt);
 }
 
-void KernelTimer::begin(int cat, cudaStream_t st) {
+int KernelTimer::begin(int cat, cudaStream_t st) {
+    if (!enabled) return -1;
     if (used + 2 > events.size()) {
         const size_t grow = std::max<size_t>(64, events.size());
         for (size_t i = 0; i < grow; i++) {
             cudaEvent_t e;
-            if (cudaEventCreate(&e) != cudaSuccess) { enabled = false; return; }
+            if (cudaEventCreate(&e) != cudaSuccess) { enabled = false; return -1; }
             events.push_back(e);
         }
     }
+    const int pair = int(used / 2);
     pendingCat.push_back(cat);
+    ended.push_back(0);
     cudaEventRecord(events[used], st);
+    used += 2;
+    return pair;
 }
 
-void KernelTimer::end(cudaStream_t st) {
-    if (!enabled || pendingCat.empty() || used + 1 >= events.size()) return;
-    cudaEventRecord(events[used + 1], st);
-    used += 2;
+void KernelTimer::end(int pair, cudaStream_t st) {
+    if (pair < 0 || size_t(pair) >= ended.size()) return;
+    cudaEventRecord(events[size_t(pair) * 2 + 1], st);
+    ended[size_t(pair)] = 1;
 }
 
 cudaError_t KernelTimer::collect() {
     const size_t pairs = std::min(used / 2, pendingCat.size());
     for (size_t k = 0; k < pairs; k++) {
+        if (!ended[k]) continue;  // a launch sequence that returned early
         cudaError_t e = cudaEventSynchronize(events[k * 2 + 1]);
         if (e != cudaSuccess) return e;
         float t = 0.f;
@@ -756,12 +803,14 @@ cudaError_t KernelTimer::collect() {
     }
     used = 0;
     pendingCat.clear();
+    ended.clear();
     return cudaSuccess;
 }
 
 void KernelTimer::reset() {
     used = 0;
     pendingCat.clear();
+    ended.clear();
     for (int i = 0; i < KC_COUNT; i++) { ms[i] = 0; launches[i] = 0; }
 }
 

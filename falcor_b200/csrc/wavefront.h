@@ -40,12 +40,21 @@ struct WavefrontBuffers {
     uint32_t* missQueue = nullptr;
     uint32_t* nextHitQueue = nullptr;
     uint32_t* nextMissQueue = nullptr;
+    // overlapTraces (owning mode only): the visibility rays' stream
+    // (non-blocking, created on first use on the current device) and the
+    // fork / join events between it and the caller's stream.
+    cudaStream_t aux = nullptr;
+    cudaEvent_t forkEv = nullptr;
+    cudaEvent_t joinEv = nullptr;
+    int auxDevice = -1;
     float4* f4(int k) const { return arrays + size_t(k) * capacity; }
     cudaError_t ensure(uint32_t capacity);
     cudaError_t ensure_sort();
     cudaError_t ensure_split();
+    cudaError_t ensure_aux();
     void release();
-    ~WavefrontBuffers() { release(); }
+    void release_aux();
+    ~WavefrontBuffers() { release(); release_aux(); }
 
     // Bytes needed for `capacity` paths in flight.
     static constexpr size_t bytes_for(uint32_t cap) {
@@ -57,7 +66,10 @@ struct WavefrontBuffers {
 };
 
 // Kernel categories timed by KernelTimer.
-enum KernelCategory { KC_GENERATE = 0, KC_SHADE = 1, KC_SHADOW = 2, KC_EXTEND = 3, KC_RESOLVE = 4, KC_SORT = 5, KC_COUNT = 6 };
+// KC_TRACE (overlapTraces only): the span of a bounce's visibility and
+// extension traversals, from the fork to the join of their two streams; the
+// two kernels' own spans overlap inside it.
+enum KernelCategory { KC_GENERATE = 0, KC_SHADE = 1, KC_SHADOW = 2, KC_EXTEND = 3, KC_RESOLVE = 4, KC_SORT = 5, KC_TRACE = 6, KC_COUNT = 7 };
 
 // Optional CUDA-event timing of each kernel launch, by category (the
 // equivalent of Falcor's FALCOR_PROFILE scopes, Utils/Timing/Profiler.h).
@@ -65,11 +77,15 @@ struct KernelTimer {
     bool enabled = false;
     std::vector<cudaEvent_t> events;   // pool, reused
     std::vector<int> pendingCat;       // category of each recorded pair
+    std::vector<char> ended;           // whether each pair's end was recorded
     size_t used = 0;                   // events in use (pairs * 2)
     double ms[KC_COUNT] = {0};
     uint64_t launches[KC_COUNT] = {0};
-    void begin(int cat, cudaStream_t st);
-    void end(cudaStream_t st);
+    // begin records a pair's start on `st` and returns the pair (-1 when
+    // disabled); end records its end.  Pairs may nest and may be ended on
+    // another stream than the one they began on.
+    int begin(int cat, cudaStream_t st);
+    void end(int pair, cudaStream_t st);
     // Waits for the recorded events and folds them into ms/launches.
     cudaError_t collect();
     void reset();

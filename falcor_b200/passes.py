@@ -185,7 +185,7 @@ class RenderPass:
 
     COUNTER_NAMES = ("paths", "rays", "closest_rays", "shadow_rays", "node_visits", "tri_tests", "hits",
                      "light_samples", "env_samples", "env_evals", "env_pdfs", "shadow_node_visits", "shadow_tri_tests")
-    KERNEL_CATEGORIES = ("generate", "shade", "shadow", "extend", "resolve", "sort")
+    KERNEL_CATEGORIES = ("generate", "shade", "shadow", "extend", "resolve", "sort", "trace")
 
     def kernel_times(self, reset: bool = True) -> dict:
         """GPU ms and launches per wavefront kernel category (needs profileKernels=1)."""

@@ -455,8 +455,9 @@ FPT_API fpt_status fpt_bsdf_probe_run(const fpt_bsdf_probe* probe, uint32_t* his
  * Limits: PathTracer passes with the Wavefront scheduler only (Megakernel is
  * rejected with FPT_ERR_UNSUPPORTED), frames up to 4096 x 4096 (larger sizes
  * are rejected with FPT_ERR_INVALID_ARG).  wavefrontCapacity is replaced by
- * the fixed 16384 paths; sortShadeQueue, splitMisses and sortExtensionRays are
- * not applied (they only reorder work, the samples are the same).  Every call looks up the
+ * the fixed 16384 paths; sortShadeQueue, splitMisses, sortExtensionRays,
+ * sortShadowRays and overlapTraces are not applied (they only reorder work,
+ * the samples are the same).  Every call looks up the
  * array's device address (cudaGetSymbolAddress, no stream work) with the
  * calling device current; the first call on a device loads the library's
  * module there and should come before any stream capture.  Calls share the
@@ -580,7 +581,10 @@ FPT_API fpt_status fpt_pass_get_counters(fpt_pass* pass, uint64_t* out, uint32_t
  * events on the pass's stream when the pass property "profileKernels" is 1
  * (the FALCOR_PROFILE scopes of Utils/Timing/Profiler.h:288-311):
  * [0] generate, [1] shade, [2] visibility traversal, [3] extension traversal,
- * [4] resolve.  Waits for the recorded events; `reset` clears the totals. */
+ * [4] resolve, [5] queue sorts, [6] with "overlapTraces" the span of each
+ * bounce's two concurrent traversals (fork to join; [2] and [3] are then the
+ * overlapping spans of the two kernels).  Waits for the recorded events;
+ * `reset` clears the totals. */
 FPT_API fpt_status fpt_pass_get_kernel_times(fpt_pass* pass, double* ms, uint64_t* launches, uint32_t count, int reset);
 
 /* ------------------------------------------------------------------------ */

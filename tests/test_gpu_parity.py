@@ -113,10 +113,11 @@ def test_path_tracer_per_sample_parity(torch_cuda, oracle):
     assert st.device_error == 0
 
 
-@pytest.mark.parametrize("option", ["sortShadeQueue", "splitMisses"])
+@pytest.mark.parametrize("option", ["sortShadeQueue", "splitMisses", "overlapTraces"])
 def test_path_tracer_queue_options_same_samples(torch_cuda, option):
-    """sortShadeQueue (material sort of the shade queue) and splitMisses (misses
-    shaded by their own kernel) reorder work only: every sample is unchanged."""
+    """sortShadeQueue (material sort of the shade queue), splitMisses (misses
+    shaded by their own kernel) and overlapTraces (visibility rays on a second
+    stream) reorder work only: every sample is unchanged."""
     torch = torch_cuda
     from falcor_b200.scene import Scene
     from falcor_b200.passes import PathTracer
@@ -134,6 +135,41 @@ def test_path_tracer_queue_options_same_samples(torch_cuda, option):
         torch.cuda.synchronize()
         out.append(samples.cpu().numpy())
     np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_overlapped_traces_match_oracle(torch_cuda, oracle):
+    """overlapTraces: each bounce's visibility rays trace on a second stream
+    beside its extension rays.  Every vertex's hit equals the oracle's, every
+    sample's radiance agrees, with the kernel timers on (the visibility
+    kernel is timed on its own stream) and off, over two frames in a row."""
+    torch = torch_cuda
+    from falcor_b200.scene import Scene
+    from falcor_b200.passes import PathTracer
+    host = H.small_heightfield()
+    scene = Scene(host)
+    W, Hh, spp, B = 64, 48, 4, 5
+    vb = H.gpu_vbuffer(scene, W, Hh)
+    _, osmp, ocnt, _, otr = H.oracle_scene(host).path_tracer(vb.cpu().numpy().view(np.uint32),
+                                                             H.pt_params(W, Hh, spp, seed=7, max_bounces=B), samples=True, trace=True)
+    for timers in (0, 1):
+        pt = PathTracer(dict(H.pt_props(spp, max_bounces=B, seed=7), overlapTraces=1, profileKernels=timers))
+        pt.set_scene(scene)
+        pt.kernel_times(reset=True)
+        for frame in range(2):
+            color = torch.zeros((Hh, W, 4), dtype=torch.float32, device="cuda")
+            smp = torch.zeros((Hh, W, spp, 3), dtype=torch.float32, device="cuda")
+            tr = torch.zeros((Hh, W, spp, B + 2, 4), dtype=torch.int32, device="cuda")
+            pt.execute({"vbuffer": vb, "color": color}, sample_color=smp, hit_trace=tr)
+            torch.cuda.synchronize()
+            differs, listed = H.compare_hit_traces(tr.cpu().numpy().view(np.uint32), otr)
+            assert not (differs & ~listed).any(), (timers, frame)
+            exact, _ = H.check_per_sample(smp.cpu().numpy(), osmp, listed, f"overlapTraces timers={timers} frame={frame}")
+            print(f"overlapTraces timers={timers} frame={frame}: {exact:.6f} bit-exact")
+            assert pt.stats().paths == ocnt.paths
+            assert pt.stats().device_error == 0
+        kt = pt.kernel_times(reset=True)
+        if timers:
+            assert kt["shadow"][1] > 0 and kt["extend"][1] == kt["shadow"][1]
 
 
 def test_extension_ray_binning_keeps_every_sample(torch_cuda, oracle):
