@@ -164,6 +164,13 @@ fpt_status build_batch(fpt_batch& b, cudaStream_t st) {
     cudaMemcpy(b.framesDev, b.frames.data(), b.frames.size() * sizeof(FrameParams), cudaMemcpyHostToDevice);
     if (!tiles.empty()) cudaMemcpy(b.tilesDev, tiles.data(), tiles.size() * sizeof(BatchTile), cudaMemcpyHostToDevice);
     if ((e = b.wb.ensure(b.capacity)) != cudaSuccess) return cuda_fail("wavefront buffers", e);
+    // overlapTraces (the requests' PathTracer property): the visibility rays'
+    // stream exists before the capture starts; without it the traversals stay
+    // sequential.
+    bool overlap = false;
+    for (const FrameParams& f : b.frames) overlap = overlap || f.overlapTraces != 0;
+    if (overlap && b.wb.ensure_aux() != cudaSuccess) cudaGetLastError();
+    if (!overlap) b.wb.release_aux();
     if (!b.capStream && (e = cudaStreamCreateWithFlags(&b.capStream, cudaStreamNonBlocking)) != cudaSuccess)
         return cuda_fail("stream", e);
     // Capture V-buffers, all waves and the frame averaging in one graph.

@@ -405,6 +405,16 @@ void launch_shade(const DevScene& s, const FrameParams& p, const WaveParams& wp,
     else wf_shade<SG, HAS_T, false, -1, TEX><<<grid, kShadeBlock, 0, st>>>(s, p, wp, w);
 }
 
+// overlapTraces launch order: 0 enqueues the visibility kernel (second
+// stream) before the extension kernel, 1 after it.  FPT_OVERLAP_AUX_PRIORITY 1
+// gives the visibility stream the device's highest priority.
+#ifndef FPT_OVERLAP_EXTEND_FIRST
+#define FPT_OVERLAP_EXTEND_FIRST 0
+#endif
+#ifndef FPT_OVERLAP_AUX_PRIORITY
+#define FPT_OVERLAP_AUX_PRIORITY 0
+#endif
+
 template <class SG, bool HAS_T>
 cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuffers& b, cudaStream_t st, KernelTimer* kt) {
     int openPairs[4] = {-1, -1, -1, -1};  // pairs begun by T0 and not yet ended (T0 / T1 nest)
@@ -509,11 +519,15 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
                 if ((e = cudaEventRecord(b.forkEv, st)) != cudaSuccess) return e;
                 if ((e = cudaStreamWaitEvent(b.aux, b.forkEv, 0)) != cudaSuccess) return e;
             }
-            const int shadowPair = kt && kt->enabled ? kt->begin(KC_SHADOW, ss) : -1;
-            if (shortStack) wf_shadow<kShortStack><<<gTraceShort, kTraceBlock, 0, ss>>>(s, p, ws, w);
-            else wf_shadow<kStackSize><<<gTrace, kTraceBlock, 0, ss>>>(s, p, ws, w);
-            if (kt) kt->end(shadowPair, ss);
-            if (overlap && (e = cudaEventRecord(b.joinEv, b.aux)) != cudaSuccess) return e;
+            auto shadowStage = [&]() -> cudaError_t {
+                const int shadowPair = kt && kt->enabled ? kt->begin(KC_SHADOW, ss) : -1;
+                if (shortStack) wf_shadow<kShortStack><<<gTraceShort, kTraceBlock, 0, ss>>>(s, p, ws, w);
+                else wf_shadow<kStackSize><<<gTrace, kTraceBlock, 0, ss>>>(s, p, ws, w);
+                if (kt) kt->end(shadowPair, ss);
+                return overlap ? cudaEventRecord(b.joinEv, b.aux) : cudaSuccess;
+            };
+            const bool extendFirst = overlap && FPT_OVERLAP_EXTEND_FIRST;
+            if (!extendFirst && (e = shadowStage()) != cudaSuccess) return e;
             if (binRays) {
                 T0(KC_SORT);
                 constexpr uint32_t kRayBins = 512;
@@ -536,6 +550,7 @@ cudaError_t run_wavefront(const DevScene& s, const FrameParams& p, WavefrontBuff
             if (shortStack) wf_extend<kShortStack><<<gTraceShort, kTraceBlock, 0, st>>>(s, p, wp, w);
             else wf_extend<kStackSize><<<gTrace, kTraceBlock, 0, st>>>(s, p, wp, w);
             T1();
+            if (extendFirst && (e = shadowStage()) != cudaSuccess) return e;
             // Both traversals of the bounce end before the queues advance.
             if (overlap) {
                 if ((e = cudaStreamWaitEvent(st, b.joinEv, 0)) != cudaSuccess) return e;
@@ -590,6 +605,10 @@ cudaError_t run_batch(const BatchDevice& bd, const std::vector<BatchWave>& waves
         gGen = blocks_for(reinterpret_cast<const void*>(wf_generate<SG, true>), kShadeBlock);
     }
     const int shadeBlocks = gShade * std::max(1, shadeScale);
+    // overlapTraces: the caller created the second stream before any capture
+    // (ensure_aux); in a captured graph the two traversals become parallel
+    // branches between the shade and advance nodes.
+    const bool overlap = b.owning && b.aux && b.forkEv && b.joinEv;
     launches = 0;
     for (const BatchWave& wv : waves) {
         WaveParams wp{};
@@ -615,8 +634,14 @@ cudaError_t run_batch(const BatchDevice& bd, const std::vector<BatchWave>& waves
         launches++;
         for (uint32_t it = 0; it < wv.maxIter; it++) {
             wf_shade<SG, HAS_T, true><<<shadeBlocks, kShadeBlock, 0, st>>>(none, fp, wp, w);
-            wf_shadow_batch<<<gTrace, kTraceBlock, 0, st>>>(none, fp, wp, w);
+            if (overlap) {
+                if ((e = cudaEventRecord(b.forkEv, st)) != cudaSuccess) return e;
+                if ((e = cudaStreamWaitEvent(b.aux, b.forkEv, 0)) != cudaSuccess) return e;
+            }
+            wf_shadow_batch<<<gTrace, kTraceBlock, 0, overlap ? b.aux : st>>>(none, fp, wp, w);
+            if (overlap && (e = cudaEventRecord(b.joinEv, b.aux)) != cudaSuccess) return e;
             wf_extend_batch<<<gTrace, kTraceBlock, 0, st>>>(none, fp, wp, w);
+            if (overlap && (e = cudaStreamWaitEvent(st, b.joinEv, 0)) != cudaSuccess) return e;
             wf_advance<<<1, 1, 0, st>>>(wp);
             launches += 4;
             std::swap(qa, qb);
@@ -688,7 +713,12 @@ cudaError_t WavefrontBuffers::ensure_aux() {
     if (e != cudaSuccess) return e;
     if (aux && auxDevice == dev) return cudaSuccess;
     release_aux();
-    if ((e = cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking)) != cudaSuccess) { aux = nullptr; return e; }
+    int least = 0, greatest = 0;
+    if (FPT_OVERLAP_AUX_PRIORITY && cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) greatest = 0;
+    if ((e = cudaStreamCreateWithPriority(&aux, cudaStreamNonBlocking, FPT_OVERLAP_AUX_PRIORITY ? greatest : 0)) != cudaSuccess) {
+        aux = nullptr;
+        return e;
+    }
     if ((e = cudaEventCreateWithFlags(&forkEv, cudaEventDisableTiming)) != cudaSuccess) { forkEv = nullptr; release_aux(); return e; }
     if ((e = cudaEventCreateWithFlags(&joinEv, cudaEventDisableTiming)) != cudaSuccess) { joinEv = nullptr; release_aux(); return e; }
     auxDevice = dev;

@@ -14,7 +14,12 @@ namespace {
 using namespace dev;
 
 constexpr int kTraceBlock = 128;
-constexpr int kShadeBlock = 128;
+// Threads per block of the generate and shade kernels (each grid-stride
+// iteration of the shade kernel ends in a block-wide queue push).
+#ifndef FPT_SHADE_BLOCK
+#define FPT_SHADE_BLOCK 128
+#endif
+constexpr int kShadeBlock = FPT_SHADE_BLOCK;
 
 // Counts: [0] shade queue, [1] extension queue, [2] shadow queue, [4] and [5]
 // the fetch counters of the extension and visibility ray kernels.
