@@ -513,16 +513,28 @@ __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_sweep(DevSc
 // samples): each lane loads one request and the warp traces their auxiliary
 // rays together (war_coop); the origin's adjoint of a scatter ray goes to its
 // vertex's position gradient.
+// FPT_WAR_REQ_ROUND 1: a warp takes only the requests that war_coop serves in
+// one round (32 / G for G lanes per request), so that a launch with few
+// requests spreads them over all resident warps instead of giving a few warps
+// many sequential rounds; 0: one request per lane.
+#ifndef FPT_WAR_REQ_ROUND
+#define FPT_WAR_REQ_ROUND 1
+#endif
 template <int J>
 __global__ void __launch_bounds__(kShadeBlock, FPT_WW_MIN_BLOCKS) ww_war_requests(DevScene s, WarParams p, WarWave ww) {
     __shared__ uint2 stackMem[kStackSize * kShadeBlock];
     uint2* stack = stackMem + threadIdx.x;
     const uint32_t n = min(ww.reqCount[J == 3 ? 0 : 1], J == 3 ? ww.reqCapacity : ww.capacity);
     const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x - lane; k0 < n; k0 += gridDim.x * blockDim.x) {
+    uint32_t G = 1;
+    while (G < p.auxCount) G <<= 1;
+    const uint32_t perWarp = FPT_WAR_REQ_ROUND ? 32u / G : 32u;  // G <= 32 (auxCount <= kMaxAux)
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t k0 = warp * perWarp; k0 < n; k0 += warps * perWarp) {
         const uint32_t k = k0 + lane;
         WarCoopReq rq;
-        rq.active = k < n;
+        rq.active = lane < perWarp && k < n;
         rq.needD = false;
         uint32_t pid = 0;
         uint32_t off[3] = {0, 0, 0};

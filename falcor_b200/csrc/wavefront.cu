@@ -19,6 +19,15 @@
 #include "kernels.cuh"
 #include "path_logic.cuh"
 #include "wavefront.h"
+// The PathTracer's generate and shade kernels run 512-thread blocks (the
+// adjoint's kernels keep the 128 of wavefront_common.cuh).  Every queue push
+// of a launch is an atomic on the same counter word, which the L2 serialises;
+// one push per block per grid-stride iteration makes bigger blocks cheaper.
+// Measured on the 1080p heightfield frame (shading ms per 16-spp frame): 15.97
+// with 64-thread blocks, 15.07 with 128, 14.62 with 256, 13.49 with 512.
+#ifndef FPT_SHADE_BLOCK
+#define FPT_SHADE_BLOCK 512
+#endif
 #include "wavefront_common.cuh"
 
 namespace fpt {
@@ -140,10 +149,11 @@ FPT_D void shade_slot(const DevScene& s, const FrameParams& p, const SoA& w, uin
 // handleHit / handleMiss for every path of the shade queue.  The hit flag of
 // a path is PF_HIT (0x2) in its flags.
 #ifndef FPT_SHADE_MIN_BLOCKS
-// 8 resident blocks (64 registers, spills to L1) measured best on the 1080p
-// heightfield frame with the sampler-specialised kernel: shading 18.77 ms per
-// frame at 6 blocks (80 registers), 17.88 at 7, 17.68 at 8, 19.51 at 5.
-#define FPT_SHADE_MIN_BLOCKS 8
+// 1024 resident threads per SM (64 registers, spills to L1) measured best on
+// the 1080p heightfield frame with the sampler-specialised kernel, as 128-thread
+// blocks: shading 18.77 ms per frame at 6 blocks (80 registers), 17.88 at 7,
+// 17.68 at 8, 19.51 at 5; after later shading changes 14.94 at 7, 15.05 at 8.
+#define FPT_SHADE_MIN_BLOCKS (1024 / FPT_SHADE_BLOCK)
 #endif
 // ES >= 0: the emissive sampler (0 Uniform, 1 LightBVH, 2 Power) fixed at
 // compile time, so that the code of the other two samplers is not in the
