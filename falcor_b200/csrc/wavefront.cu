@@ -19,14 +19,15 @@
 #include "kernels.cuh"
 #include "path_logic.cuh"
 #include "wavefront.h"
-// The PathTracer's generate and shade kernels run 512-thread blocks (the
-// adjoint's kernels keep the 128 of wavefront_common.cuh).  Every queue push
-// of a launch is an atomic on the same counter word, which the L2 serialises;
-// one push per block per grid-stride iteration makes bigger blocks cheaper.
-// Measured on the 1080p heightfield frame (shading ms per 16-spp frame): 15.97
-// with 64-thread blocks, 15.07 with 128, 14.62 with 256, 13.49 with 512.
+// The PathTracer's generate and shade kernels run 1024-thread blocks, one per
+// SM (the adjoint's kernels keep the 128 of wavefront_common.cuh).  Every
+// queue push of a launch is an atomic on the same counter word, which the L2
+// serialises; one push per block per grid-stride iteration makes bigger blocks
+// cheaper.  Measured on the 1080p heightfield frame (shading ms per 16-spp
+// frame): 15.97 with 64-thread blocks, 15.07 with 128, 14.62 with 256, 13.43
+// with 512, 12.69 with 1024 (generate 0.72 -> 0.79 ms from 512 to 1024).
 #ifndef FPT_SHADE_BLOCK
-#define FPT_SHADE_BLOCK 512
+#define FPT_SHADE_BLOCK 1024
 #endif
 #include "wavefront_common.cuh"
 
